@@ -1,0 +1,785 @@
+"""Host-side problem setup: builds the tables GGI_TLM's setup stage leaves in
+its modules before ``run_TLM`` is called (SRC/GGI_TLM.F90:100-154).
+
+This is the part of the reference that stays on the host (layer L3): mesh
+parameters, cell update codes, volume-material Z-filter coefficients, the PML
+parameter table, excitation-function tables, Huygens-surface data, output
+points and frequency-domain output surfaces.  The same tables feed both the
+GPU path (through the C-ABI in ``include/tlm_gpu.h``) and the CPU oracle.
+
+Geometry is restricted to what the hot path needs and what can be voxelised
+exactly without the reference's triangle/tet mesher: axis-aligned blocks and
+spheres (cell-centre-inside test), planar Huygens patches and planar output
+patches on cell faces, point sources and point probes at cell centres.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+# SRC/CONSTANTS/constants.F90:27-39
+PI = 3.141592653589793
+Z0 = 376.73031346177
+Y0 = 1.0 / Z0
+EPS0 = 8.8541878176e-12
+MU0 = 3.141592653589793 * 4e-7
+C0 = 2.99792458e8
+
+MAX_ORDER = 8  # max Z-filter order carried in the coefficient tables
+
+# field components, SRC/TLM_MODULES/TLM_Modules.F90:164-176
+COMPONENTS = {"Ex": 1, "Ey": 2, "Ez": 3, "Hx": 4, "Hy": 5, "Hz": 6, "Jx": 7, "Jy": 8, "Jz": 9}
+# faces, SRC/TLM_MODULES/Mesh_Modules.F90:40-46
+FACE_XMIN, FACE_YMIN, FACE_ZMIN, FACE_XMAX, FACE_YMAX, FACE_ZMAX, CENTRE = 1, 2, 3, 4, 5, 6, 7
+# volume material types, SRC/TLM_MODULES/TLM_material_modules.F90:72-78
+MAT_PEC, MAT_PMC, MAT_DISPERSIVE = 1, 2, 3
+SOURCE_HARD, SOURCE_SOFT = 0, 1  # TLM_excitation_modules.F90:162-163
+
+
+class UnsupportedFeature(ValueError):
+    """A feature outside the GPU path (cables, Ngspice, thin layers, ...)."""
+
+
+def nint(x: float) -> int:
+    """Fortran NINT: round half away from zero."""
+    return int(math.floor(x + 0.5)) if x >= 0 else -int(math.floor(-x + 0.5))
+
+
+# ---------------------------------------------------------------------------
+# Filters (SRC/FILTER)
+# ---------------------------------------------------------------------------
+@dataclass
+class Sfilter:
+    """Laplace-domain rational filter a(s/wnorm)/b(s/wnorm), FILTER/filter_types.F90:37-43."""
+
+    wnorm: float
+    a: List[float]
+    b: List[float]
+
+
+def _poly_mul(p: Sequence[float], q: Sequence[float]) -> List[float]:
+    out = [0.0] * (len(p) + len(q) - 1)
+    for i, pi in enumerate(p):
+        for j, qj in enumerate(q):
+            out[i + j] = out[i + j] + pi * qj
+    return out
+
+
+def _findroots(coeff: Sequence[float]) -> List[complex]:
+    """Roots of a polynomial via the eigenvalues of its companion (upper
+    Hessenberg) matrix, POLYNOMIAL/root_finding.F90:40-100.  The reference
+    calls EISPACK hqr; numpy's LAPACK eigensolver returns the same roots to
+    rounding (~1e-16 relative)."""
+    n = len(coeff) - 1
+    if n <= 0:
+        return []
+    h = np.zeros((n, n))
+    for i in range(n):
+        h[0, i] = -coeff[n - 1 - i] / coeff[n]
+        if i != n - 1:
+            h[i + 1, i] = 1.0
+    w = np.linalg.eigvals(h)
+    roots = []
+    for r in w:
+        wr, wi = float(r.real), float(r.imag)
+        if abs(wi) <= abs(1e-10 * wr):
+            wi = 0.0
+        roots.append(complex(wr, wi))
+    return roots
+
+
+def _rootsort(roots: List[complex]) -> Tuple[List[complex], List[complex]]:
+    """Split roots into real roots and conjugate-paired complex roots,
+    POLYNOMIAL/root_finding.F90:135-230."""
+    rroots, croots = [], []
+    for r in roots:
+        if abs(r) == 0.0 or abs((r * complex(0, -1)).real) / abs(r) <= 1e-8:
+            rroots.append(r)
+        else:
+            croots.append(r)
+    ncomplex = len(croots) // 2
+    for i in range(ncomplex):
+        fpair = 2 * i
+        c0 = croots[fpair]
+        tangle = abs((complex(0, -1) * c0 / c0.real).real) if c0.real != 0.0 else 1e10
+        for k in range(fpair + 1, 2 * ncomplex):
+            ssum = croots[fpair] + croots[k]
+            tanglesum = abs((complex(0, -1) * ssum / abs(ssum)).real) if abs(ssum) != 0.0 else 0.0
+            if tanglesum / tangle < 1e-5:
+                croots[fpair + 1], croots[k] = croots[k], croots[fpair + 1]
+    return rroots, croots[: 2 * ncomplex]
+
+
+def _trim(coeff: Sequence[float]) -> List[float]:
+    """Order reduction used at the start of bilinear_s_to_z
+    (filter_subroutines.F90:640-660): the order stays the declared one if any
+    coefficient is non-zero, else it drops to 0."""
+    if any(c != 0.0 for c in coeff):
+        return list(coeff)
+    return [coeff[0]]
+
+
+def bilinear_s_to_z(fs: Sfilter, dt: float) -> Tuple[List[float], List[float]]:
+    """Bilinear s->z transform, FILTER/filter_subroutines.F90:601-886.
+    Returns (a, b) coefficients of the z^-1 polynomials with b[0]=1."""
+    a_s = _trim(fs.a)
+    b_s = _trim(fs.b)
+    aorder, border = len(a_s) - 1, len(b_s) - 1
+    max_order = max(aorder, border)
+    dt2 = 2.0 / (dt * fs.wnorm)
+    roots = _findroots(a_s)
+    poles = _findroots(b_s)
+    if b_s[border] == 0.0:
+        raise ValueError("bilinear_s_to_z: zero leading denominator coefficient")
+    gain = a_s[aorder] / b_s[border]
+    zpolys = []
+    for loop, rts in ((1, roots), (2, poles)):
+        rr, cr = _rootsort(rts)
+        a = [1.0]
+        for i in range(len(cr) // 2):
+            modc = (cr[2 * i] * cr[2 * i + 1]).real
+            rec2 = (cr[2 * i] + cr[2 * i + 1]).real
+            b2 = [dt2 * dt2 - rec2 * dt2 + modc, -2.0 * dt2 * dt2 + 2.0 * modc, dt2 * dt2 + rec2 * dt2 + modc]
+            a = _poly_mul(a, b2)
+        for r in rr:
+            b1 = [dt2 - r.real, -dt2 - r.real]
+            a = _poly_mul(a, b1)
+        zpolys.append(a)
+    znum = [c * gain for c in zpolys[0]]
+    zden = list(zpolys[1])
+    ztemp = [1.0, 1.0]
+    if aorder > border:
+        for _ in range(aorder - border):
+            zden = _poly_mul(zden, ztemp)
+    elif border > aorder:
+        for _ in range(border - aorder):
+            znum = _poly_mul(znum, ztemp)
+    b0 = zden[0]
+    if b0 != 0.0:
+        znum = [c / b0 for c in znum[: max_order + 1]]
+        zden = [c / b0 for c in zden[: max_order + 1]]
+    return znum, zden
+
+
+def z_fast_slow_decomposition(a: List[float], b: List[float]) -> Tuple[float, List[float], List[float]]:
+    """FILTER/filter_subroutines.F90:1145-1213."""
+    if len(a) != len(b):
+        raise ValueError("Z_fast_slow_decomposition: aorder != border")
+    f_fast = a[0] / b[0]
+    out = list(a)
+    out[0] = 0.0
+    for i in range(1, len(b)):
+        out[i] = out[i] - b[i] * f_fast
+    return f_fast, out, list(b)
+
+
+def electric_susceptibility_impedance(eps: Sfilter, K: float) -> Sfilter:
+    """Z(s)=1/(s*K*(eps_r(s)-1)), FILTER/filter_subroutines.F90:1379-1431."""
+    border = len(eps.a) - 1 + 1
+    bc = [0.0] * (border + 1)
+    for i, c in enumerate(eps.a):
+        bc[i + 1] = K * eps.wnorm * c
+    for i, c in enumerate(eps.b):
+        bc[i + 1] = bc[i + 1] - K * eps.wnorm * c
+    op = 0
+    for i, c in enumerate(bc):
+        if c != 0.0:
+            op = i
+    return Sfilter(eps.wnorm, list(eps.b), bc[: op + 1])
+
+
+def magnetic_susceptibility_impedance(mu: Sfilter, K: float) -> Sfilter:
+    """Z(s)=s*K*(mu_r(s)-1), FILTER/filter_subroutines.F90:1309-1360."""
+    aorder = len(mu.a) - 1 + 1
+    ac = [0.0] * (aorder + 1)
+    for i, c in enumerate(mu.a):
+        ac[i + 1] = K * mu.wnorm * c
+    for i, c in enumerate(mu.b):
+        ac[i + 1] = ac[i + 1] - K * mu.wnorm * c
+    op = 0
+    for i, c in enumerate(ac):
+        if c != 0.0:
+            op = i
+    return Sfilter(mu.wnorm, ac[: op + 1], list(mu.b))
+
+
+@dataclass
+class VolumeMaterial:
+    """One entry of volume_material_list (TLM_material_modules.F90)."""
+
+    type: int = MAT_DISPERSIVE
+    eps: Sfilter = field(default_factory=lambda: Sfilter(1.0, [1.0], [1.0]))
+    sigma_e: float = 0.0
+    mu: Sfilter = field(default_factory=lambda: Sfilter(1.0, [1.0], [1.0]))
+    sigma_m: float = 0.0
+
+    @staticmethod
+    def dielectric(eps_r: float, sigma: float = 0.0, mu_r: float = 1.0) -> "VolumeMaterial":
+        return VolumeMaterial(MAT_DISPERSIVE, Sfilter(1.0, [eps_r], [1.0]), sigma, Sfilter(1.0, [mu_r], [1.0]), 0.0)
+
+    @staticmethod
+    def debye(eps_inf: float, delta_eps: Sequence[float], tau: Sequence[float], sigma: float = 0.0,
+              wnorm: float = 1e9) -> "VolumeMaterial":
+        """Multi-pole Debye eps(s)=eps_inf+sum d_i/(1+s tau_i) as a rational in
+        s/wnorm (the .vmat format, e.g. TEST_DATA/MATERIAL_DATA/debye_1.vmat)."""
+        den = [1.0]
+        for t in tau:
+            den = _poly_mul(den, [1.0, t * wnorm])
+        num = [eps_inf * c for c in den]
+        for i, (d, t) in enumerate(zip(delta_eps, tau)):
+            other = [1.0]
+            for j, t2 in enumerate(tau):
+                if j != i:
+                    other = _poly_mul(other, [1.0, t2 * wnorm])
+            for k, c in enumerate(other):
+                num[k] += d * c
+        return VolumeMaterial(MAT_DISPERSIVE, Sfilter(wnorm, num, den), sigma, Sfilter(wnorm, [1.0], [1.0]), 0.0)
+
+
+def material_coefficients(mat: VolumeMaterial, dl: float, dt: float, reduced_c: float = 1.0):
+    """calculate_volume_material_filter_coefficients,
+    MATERIALS/TLM_volume_materials.F90:190-385 (bilinear warp, frequency_scale=1)."""
+    out = dict(type=mat.type, eps_exists=0, mu_exists=0, Ys_eps_f=0.0, Zs_mu_f=0.0, Ge=0.0, Rm=0.0,
+               eps_a=[0.0], eps_b=[1.0], mu_a=[0.0], mu_b=[1.0], eps_order=0, mu_order=0)
+    if mat.type != MAT_DISPERSIVE:
+        return out
+    Ge = mat.sigma_e * dl / reduced_c
+    if Ge < 0.0:
+        Ge = 0.0 if Ge >= -1e-12 else float("nan")
+    out["Ge"] = Ge
+    if not (len(mat.eps.a) == 1 and mat.eps.a[0] == 1.0):
+        out["eps_exists"] = 1
+        zs = electric_susceptibility_impedance(mat.eps, (EPS0 * reduced_c) * dl)
+        a, b = bilinear_s_to_z(zs, dt)
+        f_fast, a2, b2 = z_fast_slow_decomposition(a, b)
+        out.update(Ys_eps_f=1.0 / f_fast, eps_a=a2, eps_b=b2, eps_order=max(len(a2), len(b2)) - 1)
+    Rm = mat.sigma_m * dl
+    if Rm < 0.0:
+        Rm = 0.0 if Rm >= -1e-12 else float("nan")
+    out["Rm"] = Rm
+    if not (len(mat.mu.a) == 1 and mat.mu.a[0] == 1.0):
+        out["mu_exists"] = 1
+        zs = magnetic_susceptibility_impedance(mat.mu, (MU0 * reduced_c) * dl)
+        a, b = bilinear_s_to_z(zs, dt)
+        f_fast, a2, b2 = z_fast_slow_decomposition(a, b)
+        out.update(Zs_mu_f=f_fast, mu_a=a2, mu_b=b2, mu_order=max(len(a2), len(b2)) - 1)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Excitation functions (EXCITATION/excitation.F90:155-559)
+# ---------------------------------------------------------------------------
+@dataclass
+class ExcitationFunction:
+    type: str  # impulse | gaussian | gaussian_step | step | sinusoid | gaussian_sinusoid | differential_gaussian
+    parameters: Tuple[float, ...]
+
+
+def excitation_tables(fns: Sequence[ExcitationFunction], n_timesteps: int, dt: float):
+    """Tabulate value(t_n) and value_face(t_n+dt/2), excitation.F90:155-559.
+    Scalar libm calls (math.exp / math.sin) so the tables are bitwise those of
+    a glibc-linked build."""
+    val = np.zeros((len(fns), n_timesteps))
+    valf = np.zeros((len(fns), n_timesteps))
+    for e, fn in enumerate(fns):
+        p = fn.parameters
+        for ts in range(1, n_timesteps + 1):
+            time = (ts - 1) * dt
+            time2 = time + dt / 2.0
+            for k, t in ((0, time), (1, time2)):
+                if fn.type == "impulse":
+                    v = p[0] if ts == 1 else 0.0
+                elif fn.type == "gaussian":
+                    amp, width, delay = p[0], p[1], p[2]
+                    v = amp * (math.exp(-(((t - delay) / width) ** 2))) if abs(t - delay) < width * 5.0 else 0.0
+                elif fn.type == "gaussian_step":
+                    amp, width, delay = p[0], p[1], p[2]
+                    if t < delay:
+                        v = amp * (math.exp(-(((t - delay) / width) ** 2))) if abs(t - delay) < width * 5.0 else 0.0
+                    else:
+                        v = amp
+                elif fn.type == "step":
+                    v = p[0] if t >= p[1] else 0.0
+                elif fn.type == "sinusoid":
+                    phase = p[2] * PI / 180.0
+                    v = p[0] * math.sin(2.0 * PI * p[1] * t - phase)
+                elif fn.type == "gaussian_sinusoid":
+                    amp, width, delay, freq = p[0], p[1], p[2], p[3]
+                    phase = p[4] * PI / 180.0
+                    g = math.exp(-(((t - delay) / width) ** 2)) if abs(t - delay) < width * 5.0 else 0.0
+                    v = amp * g * math.sin(2.0 * PI * freq * (t - delay) - phase)
+                elif fn.type == "differential_gaussian":
+                    amp, width, delay = p[0], p[1], p[2]
+                    if abs(t - delay) < width * 5.0:
+                        v = -amp * 2.0 * ((t - delay) / width) * math.exp(-(((t - delay) / width) ** 2))
+                    else:
+                        v = 0.0
+                else:
+                    raise UnsupportedFeature(f"excitation function type {fn.type}")
+                if k == 0:
+                    val[e, ts - 1] = v
+                else:
+                    valf[e, ts - 1] = v
+    return val, valf
+
+
+# ---------------------------------------------------------------------------
+# Problem specification (the .inp + .mesh content this path consumes)
+# ---------------------------------------------------------------------------
+@dataclass
+class Block:
+    """Axis-aligned block of cells, 1-based inclusive cell ranges."""
+
+    i0: int
+    i1: int
+    j0: int
+    j1: int
+    k0: int
+    k1: int
+
+
+@dataclass
+class Sphere:
+    """Cells whose centres lie inside a sphere (centre and radius in cells,
+    cell centres at integer+0.5 in 0-based cell coordinates)."""
+
+    cx: float
+    cy: float
+    cz: float
+    r: float
+
+
+@dataclass
+class PointExcitation:
+    cell: Tuple[int, int, int]  # 1-based
+    component: str
+    function: int  # 1-based function number
+    source_type: int = SOURCE_SOFT
+
+
+@dataclass
+class HuygensPlane:
+    """A planar Huygens patch on cell faces.  ``axis`` 1..3 is the face
+    normal; the patch lies on the boundary between cells ``index`` and
+    ``index+1`` along that axis and covers the 1-based inclusive transverse
+    cell ranges ``r0``, ``r1``.  ``side`` is the side flag of the
+    Huygens_surface packet (1 or -1).  For a planar rectangle the reference's
+    surface mesher records each face as the min face of the cell on the +axis
+    side (outward normal -axis); side 1 keeps that face, side -1 moves the
+    excitation to the max face of the cell below (huygens_surface.F90:420-460).
+    This convention is pinned by TEST_DATA/TEM_PML_TEST Ey.tout_ref, where a
+    +z plane wave launched from such a patch with side 1 reproduces the golden
+    series.  Angles in degrees as in the .inp packet."""
+
+    axis: int
+    index: int
+    r0: Tuple[int, int]
+    r1: Tuple[int, int]
+    function: int
+    ktheta: float
+    kphi: float
+    etheta: float
+    ephi: float
+    side: int = 1
+
+
+@dataclass
+class OutputPoint:
+    cell: Tuple[int, int, int]
+    component: str
+
+
+@dataclass
+class DFTSurface:
+    """Frequency-domain output surface: a planar face patch (same convention
+    as HuygensPlane) and a list of frequencies for one field component."""
+
+    axis: int
+    index: int
+    r0: Tuple[int, int]
+    r1: Tuple[int, int]
+    frequencies: Sequence[float]
+    component: str
+
+
+@dataclass
+class ProblemSpec:
+    nx: int
+    ny: int
+    nz: int
+    dl: float
+    n_timesteps: int
+    R: Tuple[float, float, float, float, float, float] = (0.0,) * 6
+    origin: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    pml_cells: Tuple[int, int, int, int, int, int] = (0,) * 6
+    pml_r: Tuple[float, ...] = (1e-4,) * 6
+    pml_order: int = 2
+    materials: List[VolumeMaterial] = field(default_factory=list)
+    material_regions: List[Tuple[int, object]] = field(default_factory=list)  # (material number, Block|Sphere)
+    functions: List[ExcitationFunction] = field(default_factory=list)
+    point_excitations: List[PointExcitation] = field(default_factory=list)
+    huygens: Optional[HuygensPlane] = None
+    outputs: List[OutputPoint] = field(default_factory=list)
+    dft_surfaces: List[DFTSurface] = field(default_factory=list)
+    reduced_c: float = 1.0
+    # features rejected up front by the GPU path
+    cables: int = 0
+    ngspice: bool = False
+    surface_materials: int = 0
+
+
+def _region_mask(spec: ProblemSpec, region) -> np.ndarray:
+    """Boolean [nz, ny, nx] mask of the cells of a region."""
+    m = np.zeros((spec.nz, spec.ny, spec.nx), dtype=bool)
+    if isinstance(region, Block):
+        m[region.k0 - 1:region.k1, region.j0 - 1:region.j1, region.i0 - 1:region.i1] = True
+    elif isinstance(region, Sphere):
+        z, y, x = np.meshgrid(np.arange(spec.nz) + 0.5, np.arange(spec.ny) + 0.5, np.arange(spec.nx) + 0.5,
+                              indexing="ij")
+        m = (x - region.cx) ** 2 + (y - region.cy) ** 2 + (z - region.cz) ** 2 <= region.r ** 2
+    else:
+        raise TypeError(region)
+    return m
+
+
+def _plane_faces(axis: int, index: int, r0, r1):
+    """Cell faces of a planar patch: list of (cx,cy,cz) of the cell on the +
+    side of each face (the cell whose *min* face it is), in connect order."""
+    faces = []
+    if axis == 1:
+        for k in range(r1[0], r1[1] + 1):
+            for j in range(r0[0], r0[1] + 1):
+                faces.append((index + 1, j, k))
+    elif axis == 2:
+        for k in range(r1[0], r1[1] + 1):
+            for i in range(r0[0], r0[1] + 1):
+                faces.append((i, index + 1, k))
+    else:
+        for j in range(r1[0], r1[1] + 1):
+            for i in range(r0[0], r0[1] + 1):
+                faces.append((i, j, index + 1))
+    return faces
+
+
+def calc_pml_dist(c: int, n: int, t_min: int, t_max: int) -> Tuple[int, int]:
+    """MATERIALS/TLM_PML_volume_materials.F90:446-481."""
+    d_min = c
+    d_max = n - c + 1
+    dist_min = d_min - (t_min + 1)
+    if dist_min > 0:
+        dist_min = 0
+    dist_max = t_max - d_max + 1
+    if dist_max < 0:
+        dist_max = 0
+    return dist_min, dist_max
+
+
+def calc_sigma_0(r: float, N: int, order: int, dl: float) -> float:
+    """MATERIALS/TLM_PML_volume_materials.F90:498-513."""
+    if N == 0:
+        return float("inf")
+    return -(EPS0 * C0 / 2.0) * math.log(r) / (dl * float(abs(N) ** (order + 1)))
+
+
+def pml_conductivity(d: int, n_min: int, n_max: int, s0_min: float, s0_max: float, order: int) -> float:
+    """MATERIALS/TLM_PML_volume_materials.F90:531-581."""
+    if d == 0:
+        return 0.0
+    L = abs(d) - 1
+    s0 = s0_min if d < 0 else s0_max
+    return s0 * float((L + 1) ** (order + 1) - L ** (order + 1))
+
+
+def pml_parameter_row(sx: float, sy: float, sz: float, dt: float) -> List[float]:
+    """One PML_parameters row, TLM_PML_volume_materials.F90:333-351."""
+    return [
+        4.0 / (4.0 + (sy + sz) * dt), 4.0 / (4.0 + (sz + sx) * dt), 4.0 / (4.0 + (sx + sy) * dt),
+        math.exp(-dt * sx / 2.0), math.exp(-dt * sy / 2.0), math.exp(-dt * sz / 2.0),
+        sx * dt / 4.0, sy * dt / 4.0, sz * dt / 4.0,
+        sx * dt / 2.0, sy * dt / 2.0, sz * dt / 2.0,
+        1.0 - (sy + sz) * dt / 4.0, 1.0 - (sz + sx) * dt / 4.0, 1.0 - (sx + sy) * dt / 4.0,
+    ]
+
+
+def huygens_vectors(ktheta_deg: float, kphi_deg: float, etheta: float, ephi: float, hs_z0: float = Z0):
+    """K, Ei, Hi of set_huygens_surface_data, EXCITATION/huygens_surface.F90:300-360."""
+    theta = (PI / 180.0) * ktheta_deg
+    phi = (PI / 180.0) * kphi_deg
+    r = 1.0
+    # rthetaphi_to_xyz_point
+    kx = r * math.sin(theta) * math.cos(phi)
+    ky = r * math.sin(theta) * math.sin(phi)
+    kz = r * math.cos(theta)
+    dxdt = r * math.cos(theta) * math.cos(phi)
+    dxdp = -r * math.sin(phi)
+    dydt = r * math.cos(theta) * math.sin(phi)
+    dydp = r * math.cos(phi)
+    dzdt = -r * math.sin(theta)
+    dzdp = 0.0
+    vx = etheta * dxdt + ephi * dxdp
+    vy = etheta * dydt + ephi * dydp
+    vz = etheta * dzdt + ephi * dzdp
+    norm = math.sqrt(vx * vx + vy * vy + vz * vz)
+    Ei = [vx / norm, vy / norm, vz / norm]
+    Hi = [ky * Ei[2] - kz * Ei[1], kz * Ei[0] - kx * Ei[2], kx * Ei[1] - ky * Ei[0]]
+    Hi = [h / hs_z0 for h in Hi]
+    return (kx, ky, kz), Ei, Hi
+
+
+def build_tables(spec: ProblemSpec) -> dict:
+    """Produce the full table set for one problem (everything the C-ABI
+    ``tlm_gpu_set_*`` entry points and the oracle consume)."""
+    if spec.cables:
+        raise UnsupportedFeature("cable models are not supported by the GPU path")
+    if spec.ngspice:
+        raise UnsupportedFeature("Ngspice co-simulation is not supported by the GPU path")
+    if spec.surface_materials:
+        raise UnsupportedFeature("surface (thin-layer) materials are not supported by the GPU path")
+    nx, ny, nz, dl = spec.nx, spec.ny, spec.nz, spec.dl
+    dt = dl / (2.0 * C0 / spec.reduced_c)  # set_TLM_solver_parameters.F90:94
+    nsteps = spec.n_timesteps
+    ncell = nx * ny * nz
+
+    # local_cell_material / local_cell_PML / local_cell_excitation / local_cell_output
+    cell_mat = np.zeros((nz, ny, nx), dtype=np.int32)
+    for mnum, region in spec.material_regions:
+        cell_mat[_region_mask(spec, region)] = mnum
+    t = spec.pml_cells
+    dxa = np.zeros(nx, dtype=np.int32)
+    dya = np.zeros(ny, dtype=np.int32)
+    dza = np.zeros(nz, dtype=np.int32)
+    for arr, n, tmin, tmax in ((dxa, nx, t[0], t[1]), (dya, ny, t[2], t[3]), (dza, nz, t[4], t[5])):
+        for c in range(1, n + 1):
+            dmin, dmax = calc_pml_dist(c, n, tmin, tmax)
+            arr[c - 1] = dmin if dmin != 0 else dmax
+    in_pml = (dza[:, None, None] != 0) | (dya[None, :, None] != 0) | (dxa[None, None, :] != 0)
+    cell_exc = np.zeros((nz, ny, nx), dtype=bool)
+    for pe in spec.point_excitations:
+        i, j, k = pe.cell
+        cell_exc[k - 1, j - 1, i - 1] = True
+    cell_out = np.zeros((nz, ny, nx), dtype=bool)
+    for op in spec.outputs:
+        i, j, k = op.cell
+        cell_out[k - 1, j - 1, i - 1] = True
+    if np.any(in_pml & cell_exc):
+        raise UnsupportedFeature("Excitation intersects PML")  # set_update_codes.F90:347-354
+    special = (cell_mat != 0) | in_pml | cell_exc | cell_out
+    for m in np.unique(cell_mat[in_pml & (cell_mat != 0)]):
+        raise UnsupportedFeature("material intersects PML: the PML-material update is not supported")
+
+    # set_cell_update_codes, set_update_codes.F90:38-363 (traversal order cz,cy,cx)
+    flat_special = special.reshape(-1)
+    n_special = int(flat_special.sum())
+    cell_code = np.zeros(ncell, dtype=np.int32)
+    cell_code[flat_special] = np.arange(1, n_special + 1, dtype=np.int32)
+    sp_material = cell_mat.reshape(-1)[flat_special].astype(np.int32)
+    exc_flat = cell_exc.reshape(-1)[flat_special]
+    out_flat = cell_out.reshape(-1)[flat_special]
+    sp_excitation = exc_flat.astype(np.int32)
+    sp_output = out_flat.astype(np.int32)
+    # excitation / output cell numbers in traversal order
+    exc_number = np.zeros(ncell, dtype=np.int32)
+    exc_number[cell_exc.reshape(-1)] = np.arange(1, int(cell_exc.sum()) + 1)
+    out_number = np.zeros(ncell, dtype=np.int32)
+    out_number[cell_out.reshape(-1)] = np.arange(1, int(cell_out.sum()) + 1)
+
+    # PML cell numbering and parameter table, TLM_PML_volume_materials.F90:41-428
+    pml_flat = in_pml.reshape(-1)
+    n_pml = int(pml_flat.sum())
+    pml_number = np.zeros(ncell, dtype=np.int32)
+    pml_number[pml_flat] = np.arange(1, n_pml + 1, dtype=np.int32)
+    sp_pml = pml_number[flat_special].astype(np.int32)
+    pml_params = np.zeros((0, 15))
+    pml_cell_param = np.zeros(0, dtype=np.int32)
+    if n_pml:
+        zz, yy, xx = np.nonzero(in_pml)
+        dx_c, dy_c, dz_c = dxa[xx], dya[yy], dza[zz]
+        pml_xmin, pml_xmax = min(0, int(dx_c.min())), max(0, int(dx_c.max()))
+        pml_ymin, pml_ymax = min(0, int(dy_c.min())), max(0, int(dy_c.max()))
+        pml_zmin, pml_zmax = min(0, int(dz_c.min())), max(0, int(dz_c.max()))
+        o = spec.pml_order
+        r = spec.pml_r
+        s0 = [calc_sigma_0(r[0], pml_xmin, o, dl) / EPS0, calc_sigma_0(r[1], pml_xmax, o, dl) / EPS0,
+              calc_sigma_0(r[2], pml_ymin, o, dl) / EPS0, calc_sigma_0(r[3], pml_ymax, o, dl) / EPS0,
+              calc_sigma_0(r[4], pml_zmin, o, dl) / EPS0, calc_sigma_0(r[5], pml_zmax, o, dl) / EPS0]
+        keys = np.stack([dx_c, dy_c, dz_c], axis=1)
+        uniq, first_idx, inverse = np.unique(keys, axis=0, return_index=True, return_inverse=True)
+        order = np.argsort(first_idx)  # parameters numbered in first-seen traversal order
+        rank = np.empty_like(order)
+        rank[order] = np.arange(len(order))
+        pml_cell_param = (rank[inverse.reshape(-1)] + 1).astype(np.int32)
+        pml_params = np.zeros((len(uniq), 15))
+        for u in range(len(uniq)):
+            ddx, ddy, ddz = (int(v) for v in uniq[u])
+            sx = pml_conductivity(ddx, pml_xmin, pml_xmax, s0[0], s0[1], o)
+            sy = pml_conductivity(ddy, pml_ymin, pml_ymax, s0[2], s0[3], o)
+            sz = pml_conductivity(ddz, pml_zmin, pml_zmax, s0[4], s0[5], o)
+            pml_params[rank[u]] = pml_parameter_row(sx, sy, sz, dt)
+
+    # volume materials
+    mats = [material_coefficients(m, dl, dt, spec.reduced_c) for m in spec.materials]
+    nm = len(mats)
+    MO = MAX_ORDER + 1
+
+    def coef(key):
+        arr = np.zeros((max(nm, 1), MO))
+        for i, m in enumerate(mats):
+            c = m[key]
+            arr[i, : len(c)] = c
+        return arr
+
+    tables = dict(
+        nx=nx, ny=ny, nz=nz, dl=dl, dt=dt, n_timesteps=nsteps, R=np.array(spec.R, dtype=np.float64),
+        cell_code=cell_code, n_special=n_special, sp_material=sp_material, sp_pml=sp_pml,
+        sp_excitation=sp_excitation, sp_output=sp_output,
+        n_materials=nm,
+        mat_type=np.array([m["type"] for m in mats] or [0], dtype=np.int32),
+        mat_eps_exists=np.array([m["eps_exists"] for m in mats] or [0], dtype=np.int32),
+        mat_mu_exists=np.array([m["mu_exists"] for m in mats] or [0], dtype=np.int32),
+        mat_eps_order=np.array([m["eps_order"] for m in mats] or [0], dtype=np.int32),
+        mat_mu_order=np.array([m["mu_order"] for m in mats] or [0], dtype=np.int32),
+        mat_Ys_eps_f=np.array([m["Ys_eps_f"] for m in mats] or [0.0]),
+        mat_Zs_mu_f=np.array([m["Zs_mu_f"] for m in mats] or [0.0]),
+        mat_Ge=np.array([m["Ge"] for m in mats] or [0.0]),
+        mat_Rm=np.array([m["Rm"] for m in mats] or [0.0]),
+        mat_eps_a=coef("eps_a"), mat_eps_b=coef("eps_b"), mat_mu_a=coef("mu_a"), mat_mu_b=coef("mu_b"),
+        n_pml_params=len(pml_params), pml_params=np.ascontiguousarray(pml_params, dtype=np.float64),
+        n_pml_cells=n_pml, pml_cell_param=pml_cell_param,
+    )
+    if nm and max(max(m["eps_order"], m["mu_order"]) for m in mats) > MAX_ORDER:
+        raise UnsupportedFeature("Z-filter order above %d" % MAX_ORDER)
+
+    # excitation functions + point excitations
+    val, valf = excitation_tables(spec.functions, nsteps, dt)
+    pts = spec.point_excitations
+    tables.update(
+        n_functions=len(spec.functions), fn_value=val, fn_value_face=valf,
+        n_exc_points=len(pts),
+        pt_cell=np.array([exc_number[(p.cell[2] - 1) * nx * ny + (p.cell[1] - 1) * nx + p.cell[0] - 1] for p in pts],
+                         dtype=np.int32),
+        pt_comp=np.array([COMPONENTS[p.component] for p in pts], dtype=np.int32),
+        pt_fn=np.array([p.function for p in pts], dtype=np.int32),
+        pt_type=np.array([p.source_type for p in pts], dtype=np.int32),
+        n_exc_cells=int(cell_exc.sum()),
+    )
+
+    # special faces: Huygens excitation faces and DFT output faces, in connect order
+    face_exc = {}
+    face_out = {}
+    hs = spec.huygens
+    if hs is not None:
+        for f in _plane_faces(hs.axis, hs.index, hs.r0, hs.r1):
+            face_exc[(f, hs.axis)] = True
+    for ds in spec.dft_surfaces:
+        for f in _plane_faces(ds.axis, ds.index, ds.r0, ds.r1):
+            face_out[(f, ds.axis)] = True
+    keys = set(face_exc) | set(face_out)
+    for (c, axis) in keys:
+        if c[axis - 1] <= 1 or c[axis - 1] > (nx, ny, nz)[axis - 1]:
+            raise UnsupportedFeature("special face on the outer boundary")
+    # connect order: cz, cy, cx, then x-, y-, z-face
+    ordered = sorted(keys, key=lambda k: (k[0][2], k[0][1], k[0][0], k[1]))
+    fexc_num, fout_num = {}, {}
+    ne = no = 0
+    face_cx, face_cy, face_cz, face_dir, face_e, face_o = [], [], [], [], [], []
+    for key in ordered:
+        (cx, cy, cz), axis = key
+        e = o = 0
+        if key in face_exc:
+            ne += 1
+            e = ne
+            fexc_num[key] = ne
+        if key in face_out:
+            no += 1
+            o = no
+            fout_num[key] = no
+        face_cx.append(cx); face_cy.append(cy); face_cz.append(cz); face_dir.append(axis)
+        face_e.append(e); face_o.append(o)
+    tables.update(n_faces=len(ordered), face_cx=np.array(face_cx, dtype=np.int32),
+                  face_cy=np.array(face_cy, dtype=np.int32), face_cz=np.array(face_cz, dtype=np.int32),
+                  face_dir=np.array(face_dir, dtype=np.int32), face_exc=np.array(face_e, dtype=np.int32),
+                  face_out=np.array(face_o, dtype=np.int32), n_exc_faces=ne, n_out_faces=no)
+
+    # Huygens surface data, huygens_surface.F90:247-715
+    if hs is not None:
+        K, Ei, Hi = huygens_vectors(hs.ktheta, hs.kphi, hs.etheta, hs.ephi)
+        faces = _plane_faces(hs.axis, hs.index, hs.r0, hs.r1)
+        norms, offsets, fexc = [], [], []
+        xmin0, ymin0, zmin0 = spec.origin
+        cents = []
+        for (cx, cy, cz) in faces:
+            cell_m = [cx, cy, cz]
+            cell_m[hs.axis - 1] -= 1
+            n = [0, 0, 0]
+            off = [-0.5, -0.5, -0.5]
+            if hs.side == 1:
+                n[hs.axis - 1] = -1
+                off[hs.axis - 1] = -1.0
+                cell_ref = [cx, cy, cz]
+            else:
+                n[hs.axis - 1] = 1
+                off[hs.axis - 1] = 0.0
+                cell_ref = cell_m
+            # get_cell_point_coordinate, general_mesh_subroutines.F90:84-140
+            x = xmin0 + (cell_ref[0] + off[0]) * dl
+            y = ymin0 + (cell_ref[1] + off[1]) * dl
+            z = zmin0 + (cell_ref[2] + off[2]) * dl
+            cents.append((x, y, z))
+            norms.extend(n)
+            offsets.append(K[0] * x + K[1] * y + K[2] * z)
+            fexc.append(fexc_num[((cx, cy, cz), hs.axis)])
+        # surface mesh extents are the face-centre extents of the recorded
+        # faces (build_surface_mesh.F90:120-160); both sides of a face share
+        # one centre
+        cm = np.array(cents)
+        bx = (cm[:, 0].min(), cm[:, 0].max())
+        by = (cm[:, 1].min(), cm[:, 1].max())
+        bz = (cm[:, 2].min(), cm[:, 2].max())
+        offset_min = 1e30
+        for (xx_, yy_, zz_) in ((bx[0], by[0], bz[0]), (bx[1], by[0], bz[0]), (bx[0], by[1], bz[0]),
+                                (bx[1], by[1], bz[0]), (bx[0], by[0], bz[1]), (bx[1], by[0], bz[1]),
+                                (bx[0], by[1], bz[1]), (bx[1], by[1], bz[1])):
+            offset_min = min(K[0] * xx_ + K[1] * yy_ + K[2] * zz_, offset_min)
+        tables.update(hs_n=len(faces), hs_face_exc=np.array(fexc, dtype=np.int32),
+                      hs_norm=np.array(norms, dtype=np.int32), hs_offset=np.array(offsets),
+                      hs_Ei=np.array(Ei), hs_Hi=np.array(Hi), hs_offset_min=offset_min - dl / 2.0,
+                      hs_c=C0 / spec.reduced_c, hs_fn=hs.function)
+    else:
+        tables.update(hs_n=0, hs_face_exc=np.zeros(0, np.int32), hs_norm=np.zeros(0, np.int32),
+                      hs_offset=np.zeros(0), hs_Ei=np.zeros(3), hs_Hi=np.zeros(3), hs_offset_min=0.0,
+                      hs_c=C0 / spec.reduced_c, hs_fn=0)
+
+    # outputs
+    tables["n_out_cells"] = int(cell_out.sum())
+    tables["out_cell"] = np.array(
+        [out_number[(o.cell[2] - 1) * nx * ny + (o.cell[1] - 1) * nx + o.cell[0] - 1] for o in spec.outputs],
+        dtype=np.int32)
+    tables["out_comp"] = np.array([COMPONENTS[o.component] for o in spec.outputs], dtype=np.int32)
+
+    # DFT surfaces: one reference surface entry per frequency
+    freqs, comps, ptr, fo, fs = [], [], [0], [], []
+    for ds in spec.dft_surfaces:
+        faces = _plane_faces(ds.axis, ds.index, ds.r0, ds.r1)
+        side_code = ds.axis  # min face of the + cell: face_xmin/ymin/zmin = 1/2/3
+        for fr in ds.frequencies:
+            freqs.append(fr)
+            comps.append(COMPONENTS[ds.component])
+            for f in faces:
+                fo.append(fout_num[(f, ds.axis)])
+                fs.append(side_code)
+            ptr.append(len(fo))
+    tables.update(n_dft=len(freqs), dft_freq=np.array(freqs, dtype=np.float64),
+                  dft_comp=np.array(comps, dtype=np.int32), dft_face_ptr=np.array(ptr, dtype=np.int32),
+                  dft_face_out=np.array(fo, dtype=np.int32), dft_face_side=np.array(fs, dtype=np.int32))
+    return tables
+
+
+def probe_series(tables: dict, cell_out: np.ndarray) -> np.ndarray:
+    """Pick the output-point time series from cell_output_field snapshots
+    (output_points.F90:463-612): cell_out is [steps, n_out_cells, 6]."""
+    idx = tables["out_cell"] - 1
+    comp = tables["out_comp"] - 1
+    return cell_out[:, idx, comp].T.copy()  # [n_points, steps]

@@ -1,0 +1,147 @@
+"""ctypes binding of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg
+import this module, as the checker.  It runs the plain-C FP64 restatement of
+GGI_TLM's sequential time loop (oracle/tlm_oracle.c) on the same tables the
+GPU path consumes (ggi_tlm_b200.problem.build_tables).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libtlm_oracle.so")
+MAX_ORDER = 8
+
+_i32p = C.POINTER(C.c_int32)
+_f64p = C.POINTER(C.c_double)
+
+
+class _Problem(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("n_timesteps", C.c_int32),
+        ("dl", C.c_double), ("dt", C.c_double), ("R", C.c_double * 6),
+        ("cell_code", _i32p), ("n_special", C.c_int32),
+        ("sp_material", _i32p), ("sp_pml", _i32p), ("sp_excitation", _i32p), ("sp_output", _i32p),
+        ("n_materials", C.c_int32), ("mat_type", _i32p), ("mat_eps_exists", _i32p), ("mat_mu_exists", _i32p),
+        ("mat_eps_order", _i32p), ("mat_mu_order", _i32p),
+        ("mat_Ys_eps_f", _f64p), ("mat_Zs_mu_f", _f64p), ("mat_Ge", _f64p), ("mat_Rm", _f64p),
+        ("mat_eps_a", _f64p), ("mat_eps_b", _f64p), ("mat_mu_a", _f64p), ("mat_mu_b", _f64p),
+        ("n_pml_params", C.c_int32), ("pml_params", _f64p), ("n_pml_cells", C.c_int32), ("pml_cell_param", _i32p),
+        ("n_functions", C.c_int32), ("fn_value", _f64p), ("fn_value_face", _f64p),
+        ("n_exc_points", C.c_int32), ("pt_cell", _i32p), ("pt_comp", _i32p), ("pt_fn", _i32p), ("pt_type", _i32p),
+        ("n_exc_cells", C.c_int32),
+        ("n_faces", C.c_int32), ("face_cx", _i32p), ("face_cy", _i32p), ("face_cz", _i32p), ("face_dir", _i32p),
+        ("face_exc", _i32p), ("face_out", _i32p), ("n_exc_faces", C.c_int32), ("n_out_faces", C.c_int32),
+        ("hs_n", C.c_int32), ("hs_face_exc", _i32p), ("hs_norm", _i32p), ("hs_offset", _f64p),
+        ("hs_Ei", C.c_double * 3), ("hs_Hi", C.c_double * 3), ("hs_offset_min", C.c_double), ("hs_c", C.c_double),
+        ("hs_fn", C.c_int32),
+        ("n_out_cells", C.c_int32),
+        ("n_dft", C.c_int32), ("dft_freq", _f64p), ("dft_comp", _i32p), ("dft_face_ptr", _i32p),
+        ("dft_face_out", _i32p), ("dft_face_side", _i32p),
+    ]
+
+
+def build(force: bool = False) -> str:
+    """Compile oracle/_build/libtlm_oracle.so with the committed Makefile."""
+    src = os.path.join(_HERE, "tlm_oracle.c")
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", _HERE])
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(build())
+        _lib.tlm_oracle_create.restype = C.c_void_p
+        _lib.tlm_oracle_create.argtypes = [C.POINTER(_Problem)]
+        _lib.tlm_oracle_destroy.argtypes = [C.c_void_p]
+        _lib.tlm_oracle_run.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _f64p]
+        _lib.tlm_oracle_get_dft.argtypes = [C.c_void_p, _f64p]
+        _lib.tlm_oracle_get_links.argtypes = [C.c_void_p, _f64p]
+    return _lib
+
+
+class Oracle:
+    """One oracle instance over one problem's tables."""
+
+    def __init__(self, t: dict):
+        lib = _load()
+        self.t = t
+        keep = []
+
+        def arr(key, dtype):
+            a = np.ascontiguousarray(t[key], dtype=dtype).reshape(-1)
+            if a.size == 0:
+                a = np.zeros(1, dtype=dtype)
+            keep.append(a)
+            return a.ctypes.data_as(_i32p if dtype == np.int32 else _f64p)
+
+        p = _Problem()
+        p.nx, p.ny, p.nz, p.n_timesteps = t["nx"], t["ny"], t["nz"], t["n_timesteps"]
+        p.dl, p.dt = t["dl"], t["dt"]
+        p.R[:] = [float(v) for v in t["R"]]
+        p.cell_code = arr("cell_code", np.int32)
+        p.n_special = t["n_special"]
+        for k in ("sp_material", "sp_pml", "sp_excitation", "sp_output", "mat_type", "mat_eps_exists",
+                  "mat_mu_exists", "mat_eps_order", "mat_mu_order", "pml_cell_param", "pt_cell", "pt_comp",
+                  "pt_fn", "pt_type", "face_cx", "face_cy", "face_cz", "face_dir", "face_exc", "face_out",
+                  "hs_face_exc", "hs_norm", "dft_comp", "dft_face_ptr", "dft_face_out", "dft_face_side"):
+            setattr(p, k, arr(k, np.int32))
+        for k in ("mat_Ys_eps_f", "mat_Zs_mu_f", "mat_Ge", "mat_Rm", "mat_eps_a", "mat_eps_b", "mat_mu_a",
+                  "mat_mu_b", "pml_params", "fn_value", "fn_value_face", "hs_offset", "dft_freq"):
+            setattr(p, k, arr(k, np.float64))
+        for k in ("n_materials", "n_pml_params", "n_pml_cells", "n_functions", "n_exc_points", "n_exc_cells",
+                  "n_faces", "n_exc_faces", "n_out_faces", "hs_n", "hs_fn", "n_out_cells", "n_dft"):
+            setattr(p, k, int(t[k]))
+        p.hs_Ei[:] = [float(v) for v in t["hs_Ei"]]
+        p.hs_Hi[:] = [float(v) for v in t["hs_Hi"]]
+        p.hs_offset_min = float(t["hs_offset_min"])
+        p.hs_c = float(t["hs_c"])
+        self._keep = keep
+        self._p = p
+        self._h = lib.tlm_oracle_create(C.byref(p))
+        if not self._h:
+            raise MemoryError("oracle allocation failed")
+        self.step = 0
+
+    def run(self, n_steps: int) -> np.ndarray:
+        """Advance n_steps; returns cell_output_field snapshots [n, n_out_cells, 6]."""
+        n_out = max(int(self.t["n_out_cells"]), 1)
+        out = np.zeros((n_steps, n_out, 6))
+        rc = _load().tlm_oracle_run(self._h, self.step + 1, n_steps, out.ctypes.data_as(_f64p))
+        if rc != 0:
+            raise RuntimeError(f"oracle run failed rc={rc}")
+        self.step += n_steps
+        return out[:, : int(self.t["n_out_cells"]), :]
+
+    def dft(self) -> np.ndarray:
+        n = int(self.t["dft_face_ptr"][-1]) if self.t["n_dft"] else 0
+        out = np.zeros(max(2 * n, 1))
+        _load().tlm_oracle_get_dft(self._h, out.ctypes.data_as(_f64p))
+        return out[: 2 * n].reshape(-1, 2)
+
+    def links(self) -> np.ndarray:
+        t = self.t
+        out = np.zeros(t["nx"] * t["ny"] * t["nz"] * 12)
+        _load().tlm_oracle_get_links(self._h, out.ctypes.data_as(_f64p))
+        return out.reshape(t["nz"], t["ny"], t["nx"], 12)
+
+    def close(self):
+        if self._h:
+            _load().tlm_oracle_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,36 @@
+"""Extract the reference's own golden time series for the in-scope
+known-answer cases into compact fixtures (tests/golden/*.npz).
+
+Reads GGI_TLM's TEST_DATA/*/PROBLEM_SPECIFICATION_FILES/*.tout_ref (text,
+format (E16.7,I5,E16.7), SRC/TLM_MODULES/File_information.F90:235) from the
+reference checkout given on the command line (default /root/reference) and
+stores (time, value) arrays.  Run once where the reference is present; the
+fixtures travel with the repository.
+
+    python tests/golden/make_golden.py [/path/to/reference]
+"""
+import os
+import sys
+
+import numpy as np
+
+CASES = {
+    "tem_pml_Ey": "TEM_PML_TEST/PROBLEM_SPECIFICATION_FILES/Ey.tout_ref",
+    "tem_material_Ey": "TEM_MATERIAL_TEST/PROBLEM_SPECIFICATION_FILES/Ey.tout_ref",
+    "material_stability_Ey": "MATERIAL_STABILITY_TEST/PROBLEM_SPECIFICATION_FILES/cavity.field.tout_ref",
+}
+
+
+def main():
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    here = os.path.dirname(os.path.abspath(__file__))
+    for name, rel in CASES.items():
+        path = os.path.join(ref, "GGI_TLM", "TEST_DATA", rel)
+        d = np.loadtxt(path, comments="#")
+        np.savez_compressed(os.path.join(here, name + ".npz"), time=d[:, 0], point=d[:, 1].astype(np.int32),
+                            value=d[:, 2], source=rel)
+        print(name, d.shape)
+
+
+if __name__ == "__main__":
+    main()
