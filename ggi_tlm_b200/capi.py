@@ -1,0 +1,245 @@
+"""ctypes binding of the C-ABI in include/tlm_gpu.h.
+
+This is the host-side mirror of the reference's time-loop call
+(``CALL run_TLM()``, SRC/GGI_TLM.F90:157): a caller hands over the arrays
+its setup stage produced (see ``ggi_tlm_b200.problem.build_tables``), then
+advances the mesh and reads back probe samples and DFT accumulators.
+
+The CUDA library is required.  There is no CPU fallback: if
+``_lib/libtlm_gpu.so`` is missing or no CUDA device is present, every entry
+point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libtlm_gpu.so")
+
+TLM_PRECISION_FP32 = 32
+TLM_PRECISION_FP64 = 64
+MAX_ORDER = 8
+
+ERRORS = {-1: "TLM_E_BADARG", -2: "TLM_E_UNSUPPORTED", -3: "TLM_E_OOM", -4: "TLM_E_CUDA", -5: "TLM_E_STATE",
+          -6: "TLM_E_TIMEOUT"}
+
+# every symbol include/tlm_gpu.h declares (checked by the CPU test suite)
+EXPORTS = [
+    "tlm_gpu_create", "tlm_gpu_set_cells", "tlm_gpu_set_materials", "tlm_gpu_set_pml", "tlm_gpu_set_excitation",
+    "tlm_gpu_set_faces", "tlm_gpu_set_huygens", "tlm_gpu_set_outputs", "tlm_gpu_set_dft", "tlm_gpu_run",
+    "tlm_gpu_synchronize", "tlm_gpu_fetch_cell_output", "tlm_gpu_fetch_dft", "tlm_gpu_fetch_links",
+    "tlm_gpu_set_stream", "tlm_gpu_set_timing", "tlm_gpu_last_run_time", "tlm_gpu_memory_bytes",
+    "tlm_gpu_last_run_launches", "tlm_gpu_destroy", "tlm_gpu_last_error",
+]
+
+
+class TLMError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("n_timesteps", C.c_int32),
+                ("dl", C.c_double), ("dt", C.c_double), ("R", C.c_double * 6), ("precision", C.c_int32),
+                ("device", C.c_int32)]
+
+
+_i32p = C.POINTER(C.c_int32)
+_f64p = C.POINTER(C.c_double)
+_lib = None
+
+
+def load_library(path: Optional[str] = None):
+    """Load libtlm_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise RuntimeError(f"CUDA library not built: {path} (run python -m ggi_tlm_b200.build)")
+    lib = C.CDLL(path)
+    i64, i32 = C.c_int64, C.c_int32
+    sig = {
+        "tlm_gpu_create": [C.POINTER(MeshDesc), C.POINTER(i64)],
+        "tlm_gpu_set_cells": [i64, _i32p, i32, _i32p, _i32p, _i32p, _i32p],
+        "tlm_gpu_set_materials": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _f64p, _f64p, _f64p, _f64p, _f64p,
+                                  _f64p, _f64p, _f64p, i32],
+        "tlm_gpu_set_pml": [i64, i32, _f64p, i32, _i32p],
+        "tlm_gpu_set_excitation": [i64, i32, i32, _f64p, _f64p, i32, _i32p, _i32p, _i32p, _i32p, i32],
+        "tlm_gpu_set_faces": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, i32, i32],
+        "tlm_gpu_set_huygens": [i64, i32, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double, C.c_double, i32],
+        "tlm_gpu_set_outputs": [i64, i32],
+        "tlm_gpu_set_dft": [i64, i32, _f64p, _i32p, _i32p, _i32p, _i32p],
+        "tlm_gpu_run": [i64, i32, i32],
+        "tlm_gpu_synchronize": [i64],
+        "tlm_gpu_fetch_cell_output": [i64, i32, i32, _f64p],
+        "tlm_gpu_fetch_dft": [i64, _f64p],
+        "tlm_gpu_fetch_links": [i64, _f64p],
+        "tlm_gpu_set_stream": [i64, C.c_void_p],
+        "tlm_gpu_set_timing": [i64, i32],
+        "tlm_gpu_last_run_time": [i64, C.POINTER(C.c_float), C.POINTER(C.c_float)],
+        "tlm_gpu_memory_bytes": [i64, C.POINTER(i64)],
+        "tlm_gpu_last_run_launches": [i64, C.POINTER(i64)],
+        "tlm_gpu_destroy": [i64],
+        "tlm_gpu_last_error": [C.c_char_p, i32],
+    }
+    for name, args in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        buf = C.create_string_buffer(512)
+        _lib.tlm_gpu_last_error(buf, 512)
+        raise TLMError(rc, buf.value.decode(errors="replace"))
+
+
+def _i32(a) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.int32).reshape(-1)
+    return a if a.size else np.zeros(1, np.int32)
+
+
+def _f64(a) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+    return a if a.size else np.zeros(1, np.float64)
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_i32p if a.dtype == np.int32 else _f64p)
+
+
+class GpuMesh:
+    """One mesh on the GPU, driven through the C-ABI exactly as the Fortran
+    shim would drive it (create -> set_* -> run -> fetch -> destroy)."""
+
+    def __init__(self, tables: dict, precision: int = TLM_PRECISION_FP64, device: int = 0):
+        lib = load_library()
+        t = tables
+        self.t = t
+        d = MeshDesc()
+        d.nx, d.ny, d.nz, d.n_timesteps = t["nx"], t["ny"], t["nz"], t["n_timesteps"]
+        d.dl, d.dt = t["dl"], t["dt"]
+        d.R[:] = [float(v) for v in t["R"]]
+        d.precision = precision
+        d.device = device
+        h = C.c_int64(0)
+        _check(lib.tlm_gpu_create(C.byref(d), C.byref(h)))
+        self.h = h.value
+        self.precision = precision
+        self.step = 0
+        try:
+            self._upload(t)
+        except Exception:
+            self.close()
+            raise
+
+    def _upload(self, t: dict):
+        lib = _lib
+        a = [_i32(t["cell_code"]), _i32(t["sp_material"]), _i32(t["sp_pml"]), _i32(t["sp_excitation"]),
+             _i32(t["sp_output"])]
+        _check(lib.tlm_gpu_set_cells(self.h, _p(a[0]), int(t["n_special"]), _p(a[1]), _p(a[2]), _p(a[3]), _p(a[4])))
+        nm = int(t["n_materials"])
+        if nm:
+            m = [_i32(t[k]) for k in ("mat_type", "mat_eps_exists", "mat_mu_exists", "mat_eps_order", "mat_mu_order")]
+            f = [_f64(t[k]) for k in ("mat_Ys_eps_f", "mat_Zs_mu_f", "mat_Ge", "mat_Rm", "mat_eps_a", "mat_eps_b",
+                                      "mat_mu_a", "mat_mu_b")]
+            stride = np.asarray(t["mat_eps_a"]).reshape(nm, -1).shape[1]
+            _check(lib.tlm_gpu_set_materials(self.h, nm, *[_p(x) for x in m], *[_p(x) for x in f], stride))
+        pp, pc = _f64(t["pml_params"]), _i32(t["pml_cell_param"])
+        _check(lib.tlm_gpu_set_pml(self.h, int(t["n_pml_params"]), _p(pp), int(t["n_pml_cells"]), _p(pc)))
+        v, vf = _f64(t["fn_value"]), _f64(t["fn_value_face"])
+        pts = [_i32(t[k]) for k in ("pt_cell", "pt_comp", "pt_fn", "pt_type")]
+        _check(lib.tlm_gpu_set_excitation(self.h, int(t["n_functions"]), int(t["n_timesteps"]), _p(v), _p(vf),
+                                          int(t["n_exc_points"]), *[_p(x) for x in pts], int(t["n_exc_cells"])))
+        fa = [_i32(t[k]) for k in ("face_cx", "face_cy", "face_cz", "face_dir", "face_exc", "face_out")]
+        _check(lib.tlm_gpu_set_faces(self.h, int(t["n_faces"]), *[_p(x) for x in fa], int(t["n_exc_faces"]),
+                                     int(t["n_out_faces"])))
+        if int(t["hs_n"]):
+            hf, hn, ho, Ei, Hi = (_i32(t["hs_face_exc"]), _i32(t["hs_norm"]), _f64(t["hs_offset"]), _f64(t["hs_Ei"]),
+                                  _f64(t["hs_Hi"]))
+            _check(lib.tlm_gpu_set_huygens(self.h, int(t["hs_n"]), _p(hf), _p(hn), _p(ho), _p(Ei), _p(Hi),
+                                           float(t["hs_offset_min"]), float(t["hs_c"]), int(t["hs_fn"])))
+        _check(lib.tlm_gpu_set_outputs(self.h, int(t["n_out_cells"])))
+        if int(t["n_dft"]):
+            df = [_f64(t["dft_freq"]), _i32(t["dft_comp"]), _i32(t["dft_face_ptr"]), _i32(t["dft_face_out"]),
+                  _i32(t["dft_face_side"])]
+            _check(lib.tlm_gpu_set_dft(self.h, int(t["n_dft"]), *[_p(x) for x in df]))
+
+    # -- time stepping -----------------------------------------------------
+    def run(self, n_steps: int, sync: bool = True):
+        _check(_lib.tlm_gpu_run(self.h, self.step + 1, n_steps))
+        self.step += n_steps
+        if sync:
+            self.synchronize()
+
+    def synchronize(self):
+        _check(_lib.tlm_gpu_synchronize(self.h))
+
+    def set_timing(self, enable: bool):
+        _check(_lib.tlm_gpu_set_timing(self.h, 1 if enable else 0))
+
+    def set_stream(self, stream_ptr: int):
+        _check(_lib.tlm_gpu_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def last_run_time(self):
+        a, b = C.c_float(0), C.c_float(0)
+        _check(_lib.tlm_gpu_last_run_time(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def last_run_launches(self) -> int:
+        n = C.c_int64(0)
+        _check(_lib.tlm_gpu_last_run_launches(self.h, C.byref(n)))
+        return n.value
+
+    def memory_bytes(self) -> int:
+        n = C.c_int64(0)
+        _check(_lib.tlm_gpu_memory_bytes(self.h, C.byref(n)))
+        return n.value
+
+    # -- results -----------------------------------------------------------
+    def cell_output(self, first: int = 1, n: Optional[int] = None) -> np.ndarray:
+        """cell_output_field snapshots [n, n_out_cells, 6] of steps first.."""
+        if n is None:
+            n = self.step - first + 1
+        no = int(self.t["n_out_cells"])
+        out = np.zeros((n, max(no, 1), 6))
+        _check(_lib.tlm_gpu_fetch_cell_output(self.h, first, n, out.ctypes.data_as(_f64p)))
+        return out[:, :no, :]
+
+    def dft(self) -> np.ndarray:
+        n = int(self.t["dft_face_ptr"][-1]) if int(self.t["n_dft"]) else 0
+        out = np.zeros(max(2 * n, 2))
+        _check(_lib.tlm_gpu_fetch_dft(self.h, out.ctypes.data_as(_f64p)))
+        return out[: 2 * n].reshape(-1, 2)
+
+    def links(self) -> np.ndarray:
+        t = self.t
+        out = np.zeros(t["nx"] * t["ny"] * t["nz"] * 12)
+        _check(_lib.tlm_gpu_fetch_links(self.h, out.ctypes.data_as(_f64p)))
+        return out.reshape(t["nz"], t["ny"], t["nx"], 12)
+
+    def close(self):
+        if getattr(self, "h", 0):
+            _check(_lib.tlm_gpu_destroy(self.h))
+            self.h = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,246 @@
+"""Seeded synthetic problems for the SCN-TLM core.
+
+* Known-answer cases restated from the reference's own regression tests
+  (TEST_DATA/TEM_PML_TEST, TEM_MATERIAL_TEST, MATERIAL_STABILITY_TEST): their
+  geometry is a 1x1xN TEM cell or a 20^3 box with rectangular blocks and a
+  planar Huygens patch, which voxelise exactly without the reference mesher.
+* The benchmark configurations (PEC box, PML box with dielectric spheres,
+  Debye slabs, batches of uneven boxes, the 512^3 PML target), generated from
+  a seed.  No public dataset is involved; these stand in for the reference's
+  .inp/.mesh inputs with the sizes and value ranges of the workloads.
+"""
+from __future__ import annotations
+
+import math
+from typing import List, Optional, Tuple
+
+import numpy as np
+
+from .problem import (C0, MAT_DISPERSIVE, Block, DFTSurface, ExcitationFunction, HuygensPlane, OutputPoint,
+                      PointExcitation, ProblemSpec, Sfilter, Sphere, VolumeMaterial, nint)
+
+
+def _dt(dl: float) -> float:
+    return dl / (2.0 * C0)
+
+
+# ---------------------------------------------------------------------------
+# Known-answer cases (reference regression tests)
+# ---------------------------------------------------------------------------
+def _tem_cell(nz: int, pml: bool, material: Optional[VolumeMaterial]) -> ProblemSpec:
+    """TEM cell of TEST_DATA/TEM_PML_TEST and TEM_MATERIAL_TEST: one cell of
+    0.1 m cross-section with PMC/PEC side walls, a +z Gaussian plane wave
+    launched from a Huygens patch at z=0.1 m, Ey/Hx probes at z=9.95/10.05 m."""
+    dl = 0.1
+    n = nint(30e-8 / _dt(dl))
+    spec = ProblemSpec(
+        nx=1, ny=1, nz=nz, dl=dl, n_timesteps=n,
+        R=(1.0, 1.0, -1.0, -1.0, 0.0, -1.0 if pml else 0.0), origin=(-0.05, -0.05, 0.0),
+        pml_cells=(0, 0, 0, 0, 0, 20) if pml else (0,) * 6, pml_r=(0.1, 0.1, 0.1, 0.1, 0.1, 1e-4), pml_order=2,
+        functions=[ExcitationFunction("gaussian", (1.0, 2e-9, 8e-9))],
+        huygens=HuygensPlane(axis=3, index=1, r0=(1, 1), r1=(1, 1), function=1, ktheta=0.0, kphi=90.0,
+                             etheta=1.0, ephi=0.0, side=1),
+        outputs=[OutputPoint((1, 1, 100), "Ey"), OutputPoint((1, 1, 100), "Hx"), OutputPoint((1, 1, 101), "Ey"),
+                 OutputPoint((1, 1, 101), "Hx")])
+    if material is not None:
+        spec.materials = [material]
+        spec.material_regions = [(1, Block(1, 1, 1, 1, 201, 600))]
+    return spec
+
+
+def debye_2() -> VolumeMaterial:
+    """TEST_DATA/MATERIAL_DATA/debye_2.vmat: eps(s)=(4+0.75 s/w)/(1+0.5 s/w), w=1e7."""
+    return VolumeMaterial(MAT_DISPERSIVE, Sfilter(1e7, [4.0, 0.75], [1.0, 0.5]), 0.0, Sfilter(1e7, [1.0], [1.0]), 0.0)
+
+
+def kat_tem_pml() -> ProblemSpec:
+    """TEST_DATA/TEM_PML_TEST/PROBLEM_SPECIFICATION_FILES/TEM_cell.inp."""
+    return _tem_cell(200, True, None)
+
+
+def kat_tem_material() -> ProblemSpec:
+    """TEST_DATA/TEM_MATERIAL_TEST/PROBLEM_SPECIFICATION_FILES/TEM_cell.inp."""
+    return _tem_cell(600, False, debye_2())
+
+
+def kat_material_stability() -> ProblemSpec:
+    """TEST_DATA/MATERIAL_STABILITY_TEST/PROBLEM_SPECIFICATION_FILES/cavity.inp:
+    20^3 box, Debye block 0.6^3 m, impulse plane wave from a 1 m^2 patch."""
+    dl = 0.1
+    n = nint(1e-6 / _dt(dl))
+    return ProblemSpec(
+        nx=20, ny=20, nz=20, dl=dl, n_timesteps=n, R=(1.0, 1.0, -1.0, -1.0, -1.0, -1.0), origin=(-1.0, -1.0, -1.0),
+        materials=[debye_2()], material_regions=[(1, Block(8, 13, 8, 13, 8, 13))],
+        functions=[ExcitationFunction("impulse", (1.0, 0.0))],
+        huygens=HuygensPlane(axis=3, index=5, r0=(6, 15), r1=(6, 15), function=1, ktheta=0.0, kphi=90.0,
+                             etheta=1.0, ephi=0.0, side=1),
+        outputs=[OutputPoint((11, 11, 11), "Ey")])
+
+
+KAT_CASES = {
+    "tem_pml_Ey": kat_tem_pml,
+    "tem_material_Ey": kat_tem_material,
+    "material_stability_Ey": kat_material_stability,
+}
+
+
+# ---------------------------------------------------------------------------
+# Benchmark configurations
+# ---------------------------------------------------------------------------
+def pec_box(n: int = 40, steps: int = 2000, seed: int = 1, dl: float = 0.01) -> ProblemSpec:
+    """PEC-walled free-space box, Gaussian (0.2 ns, 1 ns) soft Ex point source
+    at the centre cell, Ex/Ey/Ez probes at 4 seeded cells."""
+    rng = np.random.default_rng(seed)
+    src = (n // 2, n // 2, n // 2)
+    probes: List[Tuple[int, int, int]] = []
+    while len(probes) < 4:
+        c = tuple(int(v) for v in rng.integers(1, n + 1, size=3))
+        if c != src and c not in probes:
+            probes.append(c)
+    outs = [OutputPoint(c, comp) for c in probes for comp in ("Ex", "Ey", "Ez")]
+    return ProblemSpec(nx=n, ny=n, nz=n, dl=dl, n_timesteps=steps, R=(-1.0,) * 6,
+                       functions=[ExcitationFunction("gaussian", (1.0, 0.2e-9, 1e-9))],
+                       point_excitations=[PointExcitation(src, "Ex", 1)], outputs=outs)
+
+
+def _spheres(rng, n_spheres, dims, pml, rmin, rmax, eps_range=(2.0, 8.0), sigma_range=(0.0, 0.05)):
+    mats, regions = [], []
+    for i in range(n_spheres):
+        r = float(rng.uniform(rmin, rmax))
+        lo = [pml + r + 1 for _ in range(3)]
+        hi = [d - pml - r - 1 for d in dims]
+        if any(h <= l for l, h in zip(lo, hi)):
+            continue
+        c = [float(rng.uniform(l, h)) for l, h in zip(lo, hi)]
+        eps = float(rng.uniform(*eps_range))
+        sig = float(rng.uniform(*sigma_range))
+        mats.append(VolumeMaterial.dielectric(eps, sig))
+        regions.append((len(mats), Sphere(c[0], c[1], c[2], r)))
+    return mats, regions
+
+
+def pml_spheres(n: int = 256, pml: int = 8, n_spheres: int = 32, steps: int = 4000, seed: int = 2,
+                dl: float = 5e-3, n_probes: int = 16, n_freq: int = 64, dft_size: int = 64,
+                rmin: float = 5.0, rmax: float = 20.0) -> ProblemSpec:
+    """PML-bounded box with seeded dielectric spheres (eps_r U[2,8], sigma
+    U[0,0.05] S/m, kept out of the PML), a +z Gaussian plane wave from a
+    Huygens patch just inside the z-min PML, probes, and an FP64 DFT surface
+    of dft_size^2 faces at n_freq frequencies."""
+    rng = np.random.default_rng(seed)
+    mats, regions = _spheres(rng, n_spheres, (n, n, n), pml, rmin, rmax)
+    lo, hi = pml + 1, n - pml
+    probes = []
+    while len(probes) < n_probes:
+        c = tuple(int(v) for v in rng.integers(lo + 2, hi - 1, size=3))
+        if c not in probes:
+            probes.append(c)
+    c0 = n // 2 - dft_size // 2 + 1
+    dft_z = min(n - pml - 2, (3 * n) // 4)
+    fmax = 0.3 * C0 / (10 * dl) * 10 / 3  # up to c/(10 dl): 10 cells per wavelength
+    freqs = list(np.linspace(0.05 * fmax, fmax, n_freq)) if n_freq else []
+    spec = ProblemSpec(
+        nx=n, ny=n, nz=n, dl=dl, n_timesteps=steps, R=(0.0,) * 6, pml_cells=(pml,) * 6, pml_r=(1e-4,) * 6,
+        pml_order=2, materials=mats, material_regions=regions,
+        functions=[ExcitationFunction("gaussian", (1.0, 0.2e-9, 1e-9))],
+        huygens=HuygensPlane(axis=3, index=pml + 1, r0=(lo, hi), r1=(lo, hi), function=1, ktheta=0.0, kphi=90.0,
+                             etheta=1.0, ephi=0.0, side=1),
+        outputs=[OutputPoint(c, "Ey") for c in probes],
+        dft_surfaces=[DFTSurface(axis=3, index=dft_z, r0=(c0, c0 + dft_size - 1), r1=(c0, c0 + dft_size - 1),
+                                 frequencies=freqs, component="Ey")] if n_freq else [])
+    return spec
+
+
+def debye_slabs(nx: int = 384, ny: int = 384, nz: int = 192, pml: int = 10, n_slabs: int = 6, thickness: int = 8,
+                steps: int = 6000, seed: int = 3, dl: float = 2e-3, n_freq: int = 64, dft_size: int = 64,
+                margin: int = 10) -> ProblemSpec:
+    """PML box with z-normal 2-pole Debye slabs (eps_inf U[2,5], delta_eps
+    U[5,40], tau log-U[1e-11,1e-9] s) kept out of the PML, a +z Gaussian plane
+    wave, Ey probes in front of and behind each slab, FP64 DFT surface."""
+    rng = np.random.default_rng(seed)
+    ilo, ihi = pml + 1, nx - pml
+    jlo, jhi = pml + 1, ny - pml
+    zlo, zhi = pml + 1, nz - pml
+    hz = zlo + 3
+    avail = zhi - 3 - (hz + 4)
+    pitch = max(thickness + 6, avail // max(n_slabs, 1))
+    mats, regions, outs = [], [], []
+    ci, cj = nx // 2, ny // 2
+    for s in range(n_slabs):
+        z0 = hz + 4 + s * pitch
+        z1 = z0 + thickness - 1
+        if z1 + 3 > zhi:
+            break
+        eps_inf = float(rng.uniform(2.0, 5.0))
+        de = [float(rng.uniform(5.0, 40.0)) for _ in range(2)]
+        tau = [float(10 ** rng.uniform(-11.0, -9.0)) for _ in range(2)]
+        mats.append(VolumeMaterial.debye(eps_inf, de, tau, wnorm=1e9))
+        regions.append((len(mats), Block(ilo + margin, ihi - margin, jlo + margin, jhi - margin, z0, z1)))
+        outs.append(OutputPoint((ci, cj, z0 - 2), "Ey"))
+        outs.append(OutputPoint((ci, cj, z1 + 2), "Ey"))
+    c0 = nx // 2 - dft_size // 2 + 1
+    d0 = ny // 2 - dft_size // 2 + 1
+    fmax = C0 / (10 * dl)
+    freqs = list(np.linspace(0.05 * fmax, fmax, n_freq)) if n_freq else []
+    return ProblemSpec(
+        nx=nx, ny=ny, nz=nz, dl=dl, n_timesteps=steps, R=(0.0,) * 6, pml_cells=(pml,) * 6, pml_r=(1e-4,) * 6,
+        pml_order=2, materials=mats, material_regions=regions,
+        functions=[ExcitationFunction("gaussian", (1.0, 0.1e-9, 0.5e-9))],
+        huygens=HuygensPlane(axis=3, index=hz, r0=(ilo, ihi), r1=(jlo, jhi), function=1, ktheta=0.0, kphi=90.0,
+                             etheta=1.0, ephi=0.0, side=1),
+        outputs=outs,
+        dft_surfaces=[DFTSurface(axis=3, index=zhi - 2, r0=(c0, c0 + dft_size - 1), r1=(d0, d0 + dft_size - 1),
+                                 frequencies=freqs, component="Ey")] if n_freq else [])
+
+
+def pml_point_source(nx: int = 512, ny: Optional[int] = None, nz: Optional[int] = None, pml: int = 8,
+                     steps: int = 1000, dl: float = 5e-3, n_spheres: int = 0, seed: int = 4,
+                     n_probes: int = 4) -> ProblemSpec:
+    """PML-bounded free-space box (optionally with dielectric spheres), a
+    Gaussian soft Ex point source at a seeded interior cell and Ex probes:
+    the 512^3 roofline target and the boxes of the batched workload."""
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    rng = np.random.default_rng(seed)
+    dims = (nx, ny, nz)
+    rmax = max(2.0, min(d - 2 * pml for d in dims) / 4.0)
+    mats, regions = _spheres(rng, n_spheres, dims, pml, min(2.0, rmax), rmax)
+    inside_sphere = lambda c: any(  # noqa: E731
+        (c[0] - 0.5 - r.cx) ** 2 + (c[1] - 0.5 - r.cy) ** 2 + (c[2] - 0.5 - r.cz) ** 2 <= r.r ** 2 for _, r in regions)
+    lo = [pml + 1 for _ in dims]
+    hi = [d - pml for d in dims]
+
+    def pick():
+        for _ in range(1000):
+            c = tuple(int(rng.integers(l, h + 1)) for l, h in zip(lo, hi))
+            if not inside_sphere(c):
+                return c
+        return tuple((l + h) // 2 for l, h in zip(lo, hi))
+
+    src = ((nx + 1) // 2, (ny + 1) // 2, (nz + 1) // 2) if not n_spheres else pick()
+    if inside_sphere(src):
+        src = pick()
+    probes = []
+    for _ in range(n_probes):
+        c = pick()
+        if c != src and c not in probes:
+            probes.append(c)
+    return ProblemSpec(
+        nx=nx, ny=ny, nz=nz, dl=dl, n_timesteps=steps, R=(0.0,) * 6, pml_cells=(pml,) * 6, pml_r=(1e-4,) * 6,
+        pml_order=2, materials=mats, material_regions=regions,
+        functions=[ExcitationFunction("gaussian", (1.0, 0.2e-9, 1e-9))],
+        point_excitations=[PointExcitation(src, "Ex", 1)], outputs=[OutputPoint(c, "Ex") for c in probes])
+
+
+def batch_boxes(n_boxes: int = 96, edge: Tuple[int, int] = (24, 160), steps: Tuple[int, int] = (1500, 5000),
+                pml: int = 8, max_spheres: int = 8, seed: int = 5, dl: float = 5e-3) -> List[ProblemSpec]:
+    """The batched workload: uneven PML boxes, edges U[24,160] per axis, 0-8
+    dielectric spheres, a seeded Gaussian point source, steps U[1500,5000]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for b in range(n_boxes):
+        nx, ny, nz = (int(v) for v in rng.integers(edge[0], edge[1] + 1, size=3))
+        st = int(rng.integers(steps[0], steps[1] + 1))
+        ns = int(rng.integers(0, max_spheres + 1))
+        out.append(pml_point_source(nx, ny, nz, pml=pml, steps=st, dl=dl, n_spheres=ns,
+                                    seed=int(rng.integers(0, 2 ** 31)), n_probes=2))
+    return out

@@ -1,0 +1,876 @@
+// tlm_gpu.cu -- C-ABI (include/tlm_gpu.h) over the sm_100a SCN-TLM kernels.
+//
+// A handle owns one mesh: the ping-pong reflected-pulse planes, the compact
+// special-cell tables (per-32-cell bit masks + prefix counts + one int4
+// record per special cell), the PML and Z-filter state, the per-step cell
+// excitation table, the cell-output ring and the DFT accumulators.  Tables
+// are assembled on the host from the reference's module arrays at the first
+// run (or explicit finalisation) and uploaded once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/tlm_gpu.h"
+#include "tlm_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess) return fail(TLM_E_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                       __FILE__, __LINE__);                                       \
+  } while (0)
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+struct Mesh {
+  tlm_gpu_mesh_desc desc{};
+  int Px = 0, Py = 0, Pz = 0;
+  long long plane = 0;
+  bool fp64 = false;
+  bool finalized = false;
+  int next_step = 1;  // next timestep to run (1-based)
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  bool timing = false;
+  float last_total_ms = 0.f, last_cell_ms = 0.f;
+  int timed_steps = 0;
+  long long last_launches = 0;
+  size_t dev_bytes = 0;
+
+  // host copies of the reference arrays
+  std::vector<int32_t> cell_code, sp_material, sp_pml, sp_exc, sp_out;
+  int n_special = 0;
+  bool have_cells = false;
+  std::vector<tlm::MatDev> mats;
+  std::vector<double> pml_params;
+  int n_pml_params = 0;
+  std::vector<int32_t> pml_cell_param;
+  int n_pml_cells = 0;
+  int n_fn = 0, n_fn_steps = 0;
+  std::vector<double> fn_value, fn_value_face;
+  std::vector<int32_t> pt_cell, pt_comp, pt_fn, pt_type;
+  int n_exc_cells = 0;
+  std::vector<int32_t> f_cx, f_cy, f_cz, f_dir, f_exc, f_out;
+  int n_exc_faces = 0, n_out_faces = 0;
+  int hs_n = 0;
+  std::vector<int32_t> hs_face_exc, hs_norm;
+  std::vector<double> hs_offset;
+  double hs_Ei[3] = {0, 0, 0}, hs_Hi[3] = {0, 0, 0}, hs_offset_min = 0, hs_c = 0;
+  int hs_fn = 0;
+  int n_out_cells = 0;
+  int n_dft = 0;
+  std::vector<double> dft_freq;
+  std::vector<int32_t> dft_comp, dft_ptr, dft_fout, dft_fcode;
+
+  // device buffers
+  DevBuf links, seg_mask, seg_base, sp_rec, sp_pos, pml_state, pml_par, pml_ixt, filt, mats_d, exc_field, exc_type,
+      cell_out, faces, face_io, face_hs, value_face, face_field, dft_entry, dft_phasor, dft_acc, d_base;
+  int n_filt = 0, filt_eo = 0, filt_mo = 0;
+  int dft_entries = 0;
+  int n_sp_dev = 0;  // special cells on the device list
+
+  // graph of kGraphSteps steps
+  static constexpr int kGraphSteps = 8;
+  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> kev;
+
+  ~Mesh() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    for (auto e : kev) cudaEventDestroy(e);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+  }
+};
+
+std::mutex g_mu;
+std::map<int64_t, std::unique_ptr<Mesh>> g_meshes;
+int64_t g_next = 1;
+
+Mesh *get(int64_t h) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_meshes.find(h);
+  return it == g_meshes.end() ? nullptr : it->second.get();
+}
+
+int dalloc(Mesh *m, DevBuf &b, size_t bytes) {
+  if (b.p) {
+    cudaFree(b.p);
+    m->dev_bytes -= b.bytes;
+    b.p = nullptr;
+  }
+  b.bytes = std::max<size_t>(bytes, 16);
+  cudaError_t e = cudaMalloc(&b.p, b.bytes);
+  if (e != cudaSuccess) {
+    b.p = nullptr;
+    return fail(TLM_E_OOM, "cudaMalloc(%zu) failed: %s", b.bytes, cudaGetErrorString(e));
+  }
+  m->dev_bytes += b.bytes;
+  return TLM_OK;
+}
+
+template <typename V>
+int upload(Mesh *m, DevBuf &b, const std::vector<V> &v) {
+  int rc = dalloc(m, b, v.size() * sizeof(V));
+  if (rc) return rc;
+  if (!v.empty()) CK(cudaMemcpy(b.p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice));
+  return TLM_OK;
+}
+
+template <typename T>
+tlm::MeshDev<T> mesh_dev(Mesh *m) {
+  tlm::MeshDev<T> d{};
+  d.nx = m->desc.nx;
+  d.ny = m->desc.ny;
+  d.nz = m->desc.nz;
+  d.Px = m->Px;
+  d.Py = m->Py;
+  d.PxPy = (long long)m->Px * m->Py;
+  d.plane = m->plane;
+  const int VEC = sizeof(T) == 4 ? 4 : 2;
+  d.chunks_per_plane = (m->desc.ny * m->Px) / VEC;
+  d.segs_per_plane = (m->desc.ny * m->Px + 31) / 32;
+  T *base = (T *)m->links.p;
+  d.links0 = base;
+  d.links1 = base + 12 * m->plane;
+  for (int i = 0; i < 6; i++) d.R[i] = T(m->desc.R[i]);
+  d.seg_mask = (const uint32_t *)m->seg_mask.p;
+  d.seg_base = (const uint32_t *)m->seg_base.p;
+  d.sp_rec = (const int4 *)m->sp_rec.p;
+  d.sp_pos = (const int4 *)m->sp_pos.p;
+  d.pml_state = (T *)m->pml_state.p;
+  d.n_pml = m->n_pml_cells;
+  d.pml_par = (const T *)m->pml_par.p;
+  d.pml_ixt = (T *)m->pml_ixt.p;
+  d.filt = (double *)m->filt.p;
+  d.n_filt = m->n_filt;
+  d.filt_eo = m->filt_eo;
+  d.filt_mo = m->filt_mo;
+  d.mats = (const tlm::MatDev *)m->mats_d.p;
+  d.exc_field = (const double *)m->exc_field.p;
+  d.exc_type = (const int8_t *)m->exc_type.p;
+  d.n_exc = m->n_exc_cells;
+  d.cell_out = (double *)m->cell_out.p;
+  d.n_out = m->n_out_cells;
+  d.dl = m->desc.dl;
+  d.d_base = (const int *)m->d_base.p;
+  return d;
+}
+
+tlm::FaceDev face_dev(Mesh *m) {
+  tlm::FaceDev f{};
+  f.face = (const int4 *)m->faces.p;
+  f.face_io = (const int2 *)m->face_io.p;
+  f.hs = (const double4 *)m->face_hs.p;
+  f.n_faces = (int)m->f_cx.size();
+  for (int i = 0; i < 3; i++) {
+    f.Ei[i] = m->hs_Ei[i];
+    f.Hi[i] = m->hs_Hi[i];
+  }
+  f.offset_min = m->hs_offset_min;
+  f.c = m->hs_c;
+  f.dt = m->desc.dt;
+  f.dl = m->desc.dl;
+  f.value_face = (const double *)m->value_face.p;
+  f.n_timesteps = m->desc.n_timesteps;
+  f.face_field = (double *)m->face_field.p;
+  return f;
+}
+
+tlm::DftDev dft_dev(Mesh *m) {
+  tlm::DftDev d{};
+  d.n_entries = m->dft_entries;
+  d.n_dft = m->n_dft;
+  d.entry = (const int4 *)m->dft_entry.p;
+  d.phasor = (const double2 *)m->dft_phasor.p;
+  d.face_field = (const double *)m->face_field.p;
+  d.acc = (double2 *)m->dft_acc.p;
+  return d;
+}
+
+// Build and upload all device tables.
+int finalize(Mesh *m) {
+  if (m->finalized) return TLM_OK;
+  const auto &D = m->desc;
+  const int nx = D.nx, ny = D.ny, nz = D.nz;
+  const long long ncell = (long long)nx * ny * nz;
+  const int nsteps = D.n_timesteps;
+  CK(cudaSetDevice(D.device));
+  if (!m->have_cells) {
+    m->cell_code.assign(ncell, 0);
+    m->n_special = 0;
+  }
+  // ---- validate cross references
+  for (int s = 0; s < m->n_special; s++) {
+    const int mat = m->sp_material[s], pml = m->sp_pml[s];
+    if (mat < 0 || mat > (int)m->mats.size()) return fail(TLM_E_BADARG, "special cell %d: material %d out of range", s + 1, mat);
+    if (pml < 0 || pml > m->n_pml_cells) return fail(TLM_E_BADARG, "special cell %d: PML cell %d out of range", s + 1, pml);
+    if (pml && mat) {
+      const int type = m->mats[mat - 1].type;
+      if (type == 1 || type == 2) return fail(TLM_E_UNSUPPORTED, "PEC/PMC volume material in PML (scatter.F90:559-567)");
+      return fail(TLM_E_UNSUPPORTED, "PML cell inside a dispersive material is not supported by the GPU path");
+    }
+    if (pml && m->sp_exc[s]) return fail(TLM_E_UNSUPPORTED, "Excitation intersects PML (set_update_codes.F90:347-354)");
+  }
+  // ---- special cell tables: masks, prefix bases, records
+  const int VEC = m->fp64 ? 2 : 4;
+  (void)VEC;
+  const int per_plane = ny * m->Px;
+  const int segs_pp = (per_plane + 31) / 32;
+  std::vector<uint32_t> mask((size_t)segs_pp * nz, 0u), base((size_t)segs_pp * nz, 0u);
+  std::vector<int4> rec, pos;
+  rec.reserve(m->n_special + 1);
+  pos.reserve(m->n_special + 1);
+  // filter storage per dispersive cell (allocate_volume_material_filter_data)
+  int eo = 0, mo = 0;
+  for (auto &md : m->mats) {
+    if (md.type == 3) {
+      if (md.eps_exists) eo = std::max(eo, md.eps_order);
+      if (md.mu_exists) mo = std::max(mo, md.mu_order);
+    }
+  }
+  m->filt_eo = eo;
+  m->filt_mo = mo;
+  int n_filt = 0, exc_no = 0, out_no = 0;
+  long long cell = 0;
+  uint32_t running = 0;
+  for (int z = 0; z < nz; z++) {
+    for (int y = 0; y < ny; y++) {
+      for (int x = 0; x < nx; x++, cell++) {
+        const int code = m->cell_code[cell];
+        if (code == 0) continue;
+        if (code < 0 || code > m->n_special) return fail(TLM_E_BADARG, "cell_centre_update_code out of range at cell %lld", cell + 1);
+        const int s = code - 1;
+        const int e = y * m->Px + x;
+        const size_t sg = (size_t)z * segs_pp + (e >> 5);
+        mask[sg] |= 1u << (e & 31);
+        int flags = 0;
+        const int mat = m->sp_material[s];
+        int4 r{0, -1, -1, -1};
+        if (m->sp_pml[s]) {
+          flags |= tlm::SP_PML;
+          r.y = m->sp_pml[s] - 1;
+          const int par = m->pml_cell_param[r.y];
+          if (par < 1 || par > m->n_pml_params) return fail(TLM_E_BADARG, "PML cell %d: parameter %d out of range", r.y + 1, par);
+          r.z = par - 1;
+        } else {
+          if (mat) {
+            flags |= tlm::SP_MAT;
+            if (m->mats[mat - 1].type == 3) r.y = n_filt++;
+          }
+          if (m->sp_exc[s]) {
+            flags |= tlm::SP_EXC;
+            r.z = exc_no++;
+          }
+        }
+        if (m->sp_out[s]) {
+          flags |= tlm::SP_OUT;
+          r.w = out_no++;
+        }
+        r.x = flags | (mat << 8);
+        rec.push_back(r);
+        pos.push_back(int4{x, y, z, 0});
+      }
+    }
+  }
+  // the records are pushed in traversal order, which is also mask order
+  // within (z, e): rebuild bases as exclusive prefix counts of mask bits
+  running = 0;
+  for (size_t i = 0; i < mask.size(); i++) {
+    base[i] = running;
+    running += __builtin_popcount(mask[i]);
+  }
+  if ((int)running != (int)rec.size()) return fail(TLM_E_BADARG, "special cell count mismatch");
+  if (exc_no != m->n_exc_cells) return fail(TLM_E_BADARG, "excitation cells: %d flagged, %d declared", exc_no, m->n_exc_cells);
+  if (out_no != m->n_out_cells) return fail(TLM_E_BADARG, "output cells: %d flagged, %d declared", out_no, m->n_out_cells);
+  m->n_filt = n_filt;
+  m->n_sp_dev = (int)rec.size();
+  int rc;
+  if ((rc = upload(m, m->seg_mask, mask)) || (rc = upload(m, m->seg_base, base)) || (rc = upload(m, m->sp_rec, rec)) ||
+      (rc = upload(m, m->sp_pos, pos)))
+    return rc;
+  // ---- links (zeroed, allocate_mesh.F90:120)
+  const size_t esz = m->fp64 ? 8 : 4;
+  if ((rc = dalloc(m, m->links, 2 * 12 * (size_t)m->plane * esz))) return rc;
+  CK(cudaMemset(m->links.p, 0, m->links.bytes));
+  // ---- PML
+  if ((rc = dalloc(m, m->pml_state, (size_t)tlm::kPmlState * std::max(m->n_pml_cells, 1) * esz))) return rc;
+  CK(cudaMemset(m->pml_state.p, 0, m->pml_state.bytes));
+  {
+    if (m->fp64) {
+      std::vector<double> par((size_t)std::max(m->n_pml_params, 1) * 16, 0.0);
+      for (int i = 0; i < m->n_pml_params; i++)
+        for (int k = 0; k < 15; k++) par[(size_t)i * 16 + k] = m->pml_params[(size_t)i * 15 + k];
+      if ((rc = upload(m, m->pml_par, par))) return rc;
+    } else {
+      std::vector<float> par((size_t)std::max(m->n_pml_params, 1) * 16, 0.f);
+      for (int i = 0; i < m->n_pml_params; i++)
+        for (int k = 0; k < 15; k++) par[(size_t)i * 16 + k] = (float)m->pml_params[(size_t)i * 15 + k];
+      if ((rc = upload(m, m->pml_par, par))) return rc;
+    }
+  }
+  if ((rc = dalloc(m, m->pml_ixt, (size_t)std::max(m->n_out_cells, 1) * 3 * esz))) return rc;
+  CK(cudaMemset(m->pml_ixt.p, 0, m->pml_ixt.bytes));
+  // ---- filters + materials
+  const size_t J = 3 * (size_t)(eo + mo);
+  if ((rc = dalloc(m, m->filt, std::max<size_t>(J, 1) * std::max(n_filt, 1) * sizeof(double)))) return rc;
+  CK(cudaMemset(m->filt.p, 0, m->filt.bytes));
+  {
+    std::vector<tlm::MatDev> md = m->mats;
+    if (md.empty()) md.resize(1);
+    if ((rc = upload(m, m->mats_d, md))) return rc;
+  }
+  // ---- per-step cell excitation (excitation() + Point_excitation)
+  {
+    const int ne = m->n_exc_cells;
+    std::vector<double> field((size_t)std::max(ne, 1) * 9 * nsteps, 0.0);
+    std::vector<int8_t> type((size_t)std::max(ne, 1) * 6, 1);
+    for (size_t p = 0; p < m->pt_cell.size(); p++) {
+      const int c = m->pt_cell[p] - 1, comp = m->pt_comp[p] - 1, fn = m->pt_fn[p] - 1;
+      if (c < 0 || c >= ne || comp < 0 || comp >= 9 || fn < 0 || fn >= m->n_fn)
+        return fail(TLM_E_BADARG, "point excitation %zu: bad cell/component/function", p + 1);
+      if (comp < 6) type[(size_t)c * 6 + comp] = (int8_t)m->pt_type[p];
+    }
+    for (int t = 0; t < nsteps; t++) {
+      double *row = field.data() + (size_t)t * std::max(ne, 1) * 9;
+      for (size_t p = 0; p < m->pt_cell.size(); p++) {
+        const int c = m->pt_cell[p] - 1, comp = m->pt_comp[p] - 1, fn = m->pt_fn[p] - 1;
+        const double v = t < m->n_fn_steps ? m->fn_value[(size_t)fn * m->n_fn_steps + t] : 0.0;
+        row[(size_t)c * 9 + comp] = row[(size_t)c * 9 + comp] + v;
+      }
+    }
+    if ((rc = upload(m, m->exc_field, field)) || (rc = upload(m, m->exc_type, type))) return rc;
+  }
+  // ---- cell outputs
+  if ((rc = dalloc(m, m->cell_out, (size_t)std::max(m->n_out_cells, 1) * 6 * nsteps * sizeof(double)))) return rc;
+  CK(cudaMemset(m->cell_out.p, 0, m->cell_out.bytes));
+  // ---- special faces
+  {
+    const int nf = (int)m->f_cx.size();
+    std::vector<int4> fc(std::max(nf, 1));
+    std::vector<int2> io(std::max(nf, 1));
+    std::vector<double4> hs(std::max(nf, 1), double4{0, 0, 0, 0});
+    std::vector<int> exc_to_face(m->n_exc_faces + 1, -1);
+    for (int f = 0; f < nf; f++) {
+      const int x = m->f_cx[f] - 1, y = m->f_cy[f] - 1, z = m->f_cz[f] - 1, d = m->f_dir[f];
+      if (d < 1 || d > 3 || x < 0 || x >= nx || y < 0 || y >= ny || z < 0 || z >= nz)
+        return fail(TLM_E_BADARG, "special face %d out of range", f + 1);
+      if ((d == 1 && x == 0) || (d == 2 && y == 0) || (d == 3 && z == 0))
+        return fail(TLM_E_BADARG, "special face %d lies on the outer boundary", f + 1);
+      fc[f] = int4{x, y, z, d};
+      io[f] = int2{m->f_exc[f] ? m->f_exc[f] - 1 : -1, m->f_out[f] ? m->f_out[f] - 1 : -1};
+      if (m->f_exc[f]) {
+        if (m->f_exc[f] > m->n_exc_faces) return fail(TLM_E_BADARG, "face excitation number out of range");
+        exc_to_face[m->f_exc[f]] = f;
+      }
+      if (m->f_out[f] > m->n_out_faces) return fail(TLM_E_BADARG, "face output number out of range");
+    }
+    std::vector<int> covered(m->n_exc_faces + 1, 0);
+    for (int h = 0; h < m->hs_n; h++) {
+      const int e = m->hs_face_exc[h];
+      if (e < 1 || e > m->n_exc_faces || exc_to_face[e] < 0) return fail(TLM_E_BADARG, "Huygens patch %d: bad face excitation number", h + 1);
+      if (covered[e]++) return fail(TLM_E_UNSUPPORTED, "two Huygens patches on one face");
+      hs[exc_to_face[e]] = double4{m->hs_offset[h], (double)m->hs_norm[3 * h], (double)m->hs_norm[3 * h + 1],
+                                   (double)m->hs_norm[3 * h + 2]};
+    }
+    for (int e = 1; e <= m->n_exc_faces; e++)
+      if (!covered[e]) return fail(TLM_E_UNSUPPORTED, "face excitation %d is not a Huygens patch (face point sources are not supported)", e);
+    if ((rc = upload(m, m->faces, fc)) || (rc = upload(m, m->face_io, io)) || (rc = upload(m, m->face_hs, hs))) return rc;
+    std::vector<double> vf(std::max(nsteps, 1), 0.0);
+    if (m->hs_n) {
+      if (m->hs_fn < 1 || m->hs_fn > m->n_fn) return fail(TLM_E_BADARG, "Huygens function number out of range");
+      for (int t = 0; t < nsteps && t < m->n_fn_steps; t++) vf[t] = m->fn_value_face[(size_t)(m->hs_fn - 1) * m->n_fn_steps + t];
+    }
+    if ((rc = upload(m, m->value_face, vf))) return rc;
+    if ((rc = dalloc(m, m->face_field, (size_t)std::max(m->n_out_faces, 1) * 12 * sizeof(double)))) return rc;
+    CK(cudaMemset(m->face_field.p, 0, m->face_field.bytes));
+  }
+  // ---- DFT
+  {
+    std::vector<int4> ent;
+    for (int d = 0; d < m->n_dft; d++) {
+      for (int k = m->dft_ptr[d]; k < m->dft_ptr[d + 1]; k++) {
+        const int fo = m->dft_fout[k];
+        if (fo < 1 || fo > m->n_out_faces) return fail(TLM_E_BADARG, "DFT face output number out of range");
+        const int comp = m->dft_comp[d];
+        if (comp < 1 || comp > 9) return fail(TLM_E_BADARG, "DFT component out of range");
+        ent.push_back(int4{d, fo - 1, m->dft_fcode[k], comp});
+      }
+    }
+    m->dft_entries = (int)ent.size();
+    if (ent.empty()) ent.resize(1);
+    std::vector<double2> ph((size_t)std::max(m->n_dft, 1) * nsteps, double2{0, 0});
+    const double pi = 3.141592653589793;
+    for (int t = 0; t < nsteps; t++) {
+      double time = (double)t * D.dt;  // (timestep-1)*dt
+      time = time + D.dt / 2.0;
+      for (int d = 0; d < m->n_dft; d++) {
+        const double arg = -2.0 * pi * m->dft_freq[d] * time;
+        ph[(size_t)t * m->n_dft + d] = double2{cos(arg), sin(arg)};
+      }
+    }
+    if ((rc = upload(m, m->dft_entry, ent)) || (rc = upload(m, m->dft_phasor, ph))) return rc;
+    if ((rc = dalloc(m, m->dft_acc, ent.size() * sizeof(double2)))) return rc;
+    CK(cudaMemset(m->dft_acc.p, 0, m->dft_acc.bytes));
+  }
+  if ((rc = dalloc(m, m->d_base, sizeof(int)))) return rc;
+  {
+    int one = 1;
+    CK(cudaMemcpy(m->d_base.p, &one, sizeof(int), cudaMemcpyHostToDevice));
+  }
+  if (!m->stream) {
+    CK(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+    m->own_stream = true;
+  }
+  CK(cudaEventCreate(&m->ev0));
+  CK(cudaEventCreate(&m->ev1));
+  m->finalized = true;
+  return TLM_OK;
+}
+
+// Enqueue relative steps [0, n) of one step bundle (kernels only, the base
+// counter is advanced by the caller).
+template <typename T, int VEC>
+int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
+  const tlm::MeshDev<T> md = mesh_dev<T>(m);
+  const int threads = 256;
+  dim3 grid((md.chunks_per_plane + threads - 1) / threads, m->desc.nz);
+  const tlm::FaceDev fd = face_dev(m);
+  const tlm::DftDev dd = dft_dev(m);
+  for (int k = 0; k < n; k++) {
+    if (kev) cudaEventRecord(kev[2 * k], m->stream);
+    tlm::tlm_cell_kernel<T, VEC><<<grid, threads, 0, m->stream>>>(md, k);
+    if (kev) cudaEventRecord(kev[2 * k + 1], m->stream);
+    m->last_launches++;
+    if (m->n_sp_dev) {
+      tlm::tlm_special_kernel<T><<<(m->n_sp_dev + 127) / 128, 128, 0, m->stream>>>(md, m->n_sp_dev, k);
+      m->last_launches++;
+    }
+    if (fd.n_faces) {
+      tlm::tlm_face_kernel<T><<<(fd.n_faces + 127) / 128, 128, 0, m->stream>>>(md, fd, k);
+      m->last_launches++;
+    }
+    if (dd.n_entries) {
+      tlm::tlm_dft_kernel<<<(dd.n_entries + 255) / 256, 256, 0, m->stream>>>(dd, md.d_base, k);
+      m->last_launches++;
+    }
+  }
+  CK(cudaGetLastError());
+  return TLM_OK;
+}
+
+int enqueue(Mesh *m, int n, cudaEvent_t *kev) {
+  return m->fp64 ? enqueue_steps<double, 2>(m, n, kev) : enqueue_steps<float, 4>(m, n, kev);
+}
+
+int run_steps(Mesh *m, int n) {
+  int rc;
+  m->last_launches = 0;
+  CK(cudaEventRecord(m->ev0, m->stream));
+  if (m->timing) {
+    // per-step launches with an event pair around every cell kernel; the
+    // durations are summed once the run has finished (last_run_time)
+    const size_t need = 2 * (size_t)n;
+    while (m->kev.size() < need) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      m->kev.push_back(e);
+    }
+    for (int s = 0; s < n; s++) {
+      if ((rc = enqueue(m, 1, m->kev.data() + 2 * s))) return rc;
+      tlm::tlm_advance_base<<<1, 1, 0, m->stream>>>((int *)m->d_base.p, 1);
+      m->last_launches++;
+    }
+    m->timed_steps = n;
+  } else {
+    const int G = Mesh::kGraphSteps;
+    int full = n / G, rem = n % G;
+    if (full > 0 && !m->graph) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+      long long saved = m->last_launches;
+      rc = enqueue(m, G, nullptr);
+      tlm::tlm_advance_base<<<1, 1, 0, m->stream>>>((int *)m->d_base.p, G);
+      cudaError_t ce = cudaStreamEndCapture(m->stream, &g);
+      if (rc) return rc;
+      if (ce != cudaSuccess) return fail(TLM_E_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&m->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) return fail(TLM_E_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+      m->last_launches = saved;
+    }
+    const long long per_graph =
+        (long long)G * (1 + (m->n_sp_dev ? 1 : 0) + (m->f_cx.empty() ? 0 : 1) + (m->dft_entries ? 1 : 0)) + 1;
+    for (int i = 0; i < full; i++) {
+      CK(cudaGraphLaunch(m->graph, m->stream));
+      m->last_launches += per_graph;
+    }
+    for (int i = 0; i < rem; i++) {
+      if ((rc = enqueue(m, 1, nullptr))) return rc;
+      tlm::tlm_advance_base<<<1, 1, 0, m->stream>>>((int *)m->d_base.p, 1);
+      m->last_launches++;
+    }
+    m->timed_steps = 0;
+  }
+  CK(cudaEventRecord(m->ev1, m->stream));
+  CK(cudaGetLastError());
+  return TLM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tlm_gpu_create(const tlm_gpu_mesh_desc *desc, int64_t *handle) {
+  if (!desc || !handle) return fail(TLM_E_BADARG, "null argument");
+  if (desc->nx < 1 || desc->ny < 1 || desc->nz < 1) return fail(TLM_E_BADARG, "mesh dimensions must be >= 1");
+  if (desc->n_timesteps < 1) return fail(TLM_E_BADARG, "n_timesteps must be >= 1");
+  if (!(desc->dl > 0) || !(desc->dt > 0)) return fail(TLM_E_BADARG, "dl and dt must be positive");
+  if (desc->precision != TLM_PRECISION_FP32 && desc->precision != TLM_PRECISION_FP64)
+    return fail(TLM_E_BADARG, "precision must be TLM_PRECISION_FP32 or TLM_PRECISION_FP64");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(TLM_E_CUDA, "no CUDA device available");
+  if (desc->device < 0 || desc->device >= ndev) return fail(TLM_E_BADARG, "device %d out of range", desc->device);
+  auto m = std::make_unique<Mesh>();
+  m->desc = *desc;
+  m->fp64 = desc->precision == TLM_PRECISION_FP64;
+  m->Px = ((desc->nx + 1 + 3) / 4) * 4;
+  m->Py = desc->ny + 2;
+  m->Pz = desc->nz + 2;
+  m->plane = (long long)m->Px * m->Py * m->Pz;
+  if ((long long)desc->ny * m->Px >= (1LL << 31) / 4) return fail(TLM_E_BADARG, "mesh plane too large");
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int64_t h = g_next++;
+  g_meshes[h] = std::move(m);
+  *handle = h;
+  return TLM_OK;
+}
+
+int tlm_gpu_set_cells(int64_t h, const int32_t *code, int32_t n_special, const int32_t *sp_material,
+                      const int32_t *sp_pml, const int32_t *sp_excitation, const int32_t *sp_output) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (!code || n_special < 0 || (n_special && (!sp_material || !sp_pml || !sp_excitation || !sp_output)))
+    return fail(TLM_E_BADARG, "null argument");
+  const long long ncell = (long long)m->desc.nx * m->desc.ny * m->desc.nz;
+  m->cell_code.assign(code, code + ncell);
+  m->n_special = n_special;
+  m->sp_material.assign(sp_material, sp_material + n_special);
+  m->sp_pml.assign(sp_pml, sp_pml + n_special);
+  m->sp_exc.assign(sp_excitation, sp_excitation + n_special);
+  m->sp_out.assign(sp_output, sp_output + n_special);
+  m->have_cells = true;
+  return TLM_OK;
+}
+
+int tlm_gpu_set_materials(int64_t h, int32_t n, const int32_t *type, const int32_t *eps_exists, const int32_t *mu_exists,
+                          const int32_t *eps_order, const int32_t *mu_order, const double *Ys_eps_f,
+                          const double *Zs_mu_f, const double *Ge, const double *Rm, const double *eps_a,
+                          const double *eps_b, const double *mu_a, const double *mu_b, int32_t stride) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0) return fail(TLM_E_BADARG, "negative material count");
+  m->mats.assign(n, tlm::MatDev{});
+  for (int i = 0; i < n; i++) {
+    tlm::MatDev &d = m->mats[i];
+    d.type = type[i];
+    if (d.type < 1 || d.type > 3) return fail(TLM_E_UNSUPPORTED, "volume material %d: type %d not supported", i + 1, d.type);
+    d.eps_exists = eps_exists[i];
+    d.mu_exists = mu_exists[i];
+    d.eps_order = eps_order[i];
+    d.mu_order = mu_order[i];
+    if (d.eps_order < 0 || d.eps_order > tlm::kMaxOrder || d.mu_order < 0 || d.mu_order > tlm::kMaxOrder ||
+        d.eps_order + 1 > stride || d.mu_order + 1 > stride)
+      return fail(TLM_E_UNSUPPORTED, "volume material %d: filter order above %d", i + 1, tlm::kMaxOrder);
+    d.Ys_eps_f = Ys_eps_f[i];
+    d.Zs_mu_f = Zs_mu_f[i];
+    d.Ge = Ge[i];
+    d.Rm = Rm[i];
+    for (int k = 0; k <= tlm::kMaxOrder; k++) {
+      d.eps_a[k] = k <= d.eps_order ? eps_a[(size_t)i * stride + k] : 0.0;
+      d.eps_b[k] = k <= d.eps_order ? eps_b[(size_t)i * stride + k] : 0.0;
+      d.mu_a[k] = k <= d.mu_order ? mu_a[(size_t)i * stride + k] : 0.0;
+      d.mu_b[k] = k <= d.mu_order ? mu_b[(size_t)i * stride + k] : 0.0;
+    }
+    if (d.type == 3 && ((d.eps_exists && d.eps_b[0] == 0.0) || (d.mu_exists && d.mu_b[0] == 0.0)))
+      return fail(TLM_E_BADARG, "volume material %d: filter b(0) is zero", i + 1);
+  }
+  return TLM_OK;
+}
+
+int tlm_gpu_set_pml(int64_t h, int32_t n_params, const double *params, int32_t n_pml_cells, const int32_t *cell_param) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n_params < 0 || n_pml_cells < 0 || (n_params && !params) || (n_pml_cells && !cell_param))
+    return fail(TLM_E_BADARG, "bad PML arguments");
+  m->n_pml_params = n_params;
+  m->pml_params.assign(params, params + (size_t)n_params * 15);
+  m->n_pml_cells = n_pml_cells;
+  m->pml_cell_param.assign(cell_param, cell_param + n_pml_cells);
+  return TLM_OK;
+}
+
+int tlm_gpu_set_excitation(int64_t h, int32_t n_fn, int32_t n_steps, const double *value, const double *value_face,
+                           int32_t n_points, const int32_t *pt_cell, const int32_t *pt_comp, const int32_t *pt_fn,
+                           const int32_t *pt_type, int32_t n_exc_cells) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n_fn < 0 || n_steps < 0 || n_points < 0 || n_exc_cells < 0) return fail(TLM_E_BADARG, "negative count");
+  m->n_fn = n_fn;
+  m->n_fn_steps = n_steps;
+  m->fn_value.assign(value, value + (size_t)n_fn * n_steps);
+  m->fn_value_face.assign(value_face, value_face + (size_t)n_fn * n_steps);
+  m->pt_cell.assign(pt_cell, pt_cell + n_points);
+  m->pt_comp.assign(pt_comp, pt_comp + n_points);
+  m->pt_fn.assign(pt_fn, pt_fn + n_points);
+  m->pt_type.assign(pt_type, pt_type + n_points);
+  for (int i = 0; i < n_points; i++)
+    if (pt_type[i] != 0 && pt_type[i] != 1) return fail(TLM_E_BADARG, "point excitation %d: bad source type", i + 1);
+  m->n_exc_cells = n_exc_cells;
+  return TLM_OK;
+}
+
+int tlm_gpu_set_faces(int64_t h, int32_t n, const int32_t *cx, const int32_t *cy, const int32_t *cz, const int32_t *dir,
+                      const int32_t *exc, const int32_t *out, int32_t n_exc_faces, int32_t n_out_faces) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0) return fail(TLM_E_BADARG, "negative face count");
+  m->f_cx.assign(cx, cx + n);
+  m->f_cy.assign(cy, cy + n);
+  m->f_cz.assign(cz, cz + n);
+  m->f_dir.assign(dir, dir + n);
+  m->f_exc.assign(exc, exc + n);
+  m->f_out.assign(out, out + n);
+  m->n_exc_faces = n_exc_faces;
+  m->n_out_faces = n_out_faces;
+  return TLM_OK;
+}
+
+int tlm_gpu_set_huygens(int64_t h, int32_t n, const int32_t *face_exc, const int32_t *norm, const double *offset,
+                        const double *Ei, const double *Hi, double offset_min, double c, int32_t function) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && (!face_exc || !norm || !offset || !Ei || !Hi))) return fail(TLM_E_BADARG, "bad Huygens arguments");
+  m->hs_n = n;
+  m->hs_face_exc.assign(face_exc, face_exc + n);
+  m->hs_norm.assign(norm, norm + 3 * (size_t)n);
+  m->hs_offset.assign(offset, offset + n);
+  for (int i = 0; i < 3 && n; i++) {
+    m->hs_Ei[i] = Ei[i];
+    m->hs_Hi[i] = Hi[i];
+  }
+  m->hs_offset_min = offset_min;
+  m->hs_c = c;
+  m->hs_fn = function;
+  if (n && !(c > 0)) return fail(TLM_E_BADARG, "Huygens wave speed must be positive");
+  return TLM_OK;
+}
+
+int tlm_gpu_set_outputs(int64_t h, int32_t n_out_cells) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n_out_cells < 0) return fail(TLM_E_BADARG, "negative output count");
+  m->n_out_cells = n_out_cells;
+  return TLM_OK;
+}
+
+int tlm_gpu_set_dft(int64_t h, int32_t n, const double *freq, const int32_t *comp, const int32_t *ptr,
+                    const int32_t *fout, const int32_t *fcode) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0) return fail(TLM_E_BADARG, "negative surface count");
+  m->n_dft = n;
+  m->dft_freq.assign(freq, freq + n);
+  m->dft_comp.assign(comp, comp + n);
+  m->dft_ptr.assign(ptr, ptr + n + 1);
+  const int ne = n ? ptr[n] : 0;
+  m->dft_fout.assign(fout, fout + ne);
+  m->dft_fcode.assign(fcode, fcode + ne);
+  for (int k = 0; k < ne; k++)
+    if (fcode[k] < 1 || fcode[k] > 6) return fail(TLM_E_BADARG, "DFT face code out of range");
+  return TLM_OK;
+}
+
+int tlm_gpu_set_stream(int64_t h, void *stream) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->graph) {
+    cudaGraphExecDestroy(m->graph);
+    m->graph = nullptr;
+  }
+  if (m->own_stream && m->stream) cudaStreamDestroy(m->stream);
+  m->own_stream = false;
+  m->stream = (cudaStream_t)stream;
+  if (!stream) {
+    CK(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+    m->own_stream = true;
+  }
+  return TLM_OK;
+}
+
+int tlm_gpu_set_timing(int64_t h, int32_t enable) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  m->timing = enable != 0;
+  return TLM_OK;
+}
+
+int tlm_gpu_run(int64_t h, int32_t first_step, int32_t n_steps) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  CK(cudaSetDevice(m->desc.device));
+  int rc = finalize(m);
+  if (rc) return rc;
+  if (first_step != m->next_step) return fail(TLM_E_STATE, "expected first_step %d, got %d", m->next_step, first_step);
+  if (n_steps < 0 || first_step + n_steps - 1 > m->desc.n_timesteps)
+    return fail(TLM_E_BADARG, "steps %d..%d beyond n_timesteps %d", first_step, first_step + n_steps - 1, m->desc.n_timesteps);
+  if (n_steps == 0) return TLM_OK;
+  rc = run_steps(m, n_steps);
+  if (rc) return rc;
+  m->next_step += n_steps;
+  return TLM_OK;
+}
+
+int tlm_gpu_synchronize(int64_t h) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->stream) CK(cudaStreamSynchronize(m->stream));
+  return TLM_OK;
+}
+
+int tlm_gpu_last_run_time(int64_t h, float *ms_total, float *ms_cell) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
+  CK(cudaEventSynchronize(m->ev1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, m->ev0, m->ev1));
+  float cell = 0.f;
+  for (int s = 0; s < m->timed_steps; s++) {
+    float k = 0.f;
+    CK(cudaEventElapsedTime(&k, m->kev[2 * s], m->kev[2 * s + 1]));
+    cell += k;
+  }
+  if (ms_total) *ms_total = ms;
+  if (ms_cell) *ms_cell = cell;
+  return TLM_OK;
+}
+
+int tlm_gpu_last_run_launches(int64_t h, int64_t *launches) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  *launches = m->last_launches;
+  return TLM_OK;
+}
+
+int tlm_gpu_memory_bytes(int64_t h, int64_t *bytes) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  *bytes = (int64_t)m->dev_bytes;
+  return TLM_OK;
+}
+
+int tlm_gpu_fetch_cell_output(int64_t h, int32_t first, int32_t n, double *out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
+  if (first < 1 || n < 0 || first + n - 1 >= m->next_step) return fail(TLM_E_BADARG, "steps not yet computed");
+  if (m->n_out_cells == 0 || n == 0) return TLM_OK;
+  CK(cudaStreamSynchronize(m->stream));
+  const size_t row = (size_t)m->n_out_cells * 6;
+  CK(cudaMemcpy(out, (double *)m->cell_out.p + (size_t)(first - 1) * row, (size_t)n * row * sizeof(double),
+                cudaMemcpyDeviceToHost));
+  return TLM_OK;
+}
+
+int tlm_gpu_fetch_dft(int64_t h, double *out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
+  if (!m->dft_entries) return TLM_OK;
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(out, m->dft_acc.p, (size_t)m->dft_entries * 2 * sizeof(double), cudaMemcpyDeviceToHost));
+  return TLM_OK;
+}
+
+int tlm_gpu_fetch_links(int64_t h, double *out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  CK(cudaSetDevice(m->desc.device));
+  int rc = finalize(m);
+  if (rc) return rc;
+  const long long n = (long long)m->desc.nx * m->desc.ny * m->desc.nz;
+  DevBuf tmp;
+  if ((rc = dalloc(m, tmp, (size_t)n * 12 * sizeof(double)))) return rc;
+  const int t_done = m->next_step - 1;
+  const int threads = 256;
+  const unsigned blocks = (unsigned)((n + threads - 1) / threads);
+  if (m->fp64)
+    tlm::tlm_gather_links<double><<<blocks, threads, 0, m->stream>>>(mesh_dev<double>(m), t_done, (double *)tmp.p);
+  else
+    tlm::tlm_gather_links<float><<<blocks, threads, 0, m->stream>>>(mesh_dev<float>(m), t_done, (double *)tmp.p);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(out, tmp.p, (size_t)n * 12 * sizeof(double), cudaMemcpyDeviceToHost));
+  m->dev_bytes -= tmp.bytes;
+  return TLM_OK;
+}
+
+int tlm_gpu_destroy(int64_t h) {
+  std::unique_ptr<Mesh> m;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_meshes.find(h);
+    if (it == g_meshes.end()) return fail(TLM_E_BADARG, "bad handle");
+    m = std::move(it->second);
+    g_meshes.erase(it);
+  }
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  return TLM_OK;
+}
+
+int tlm_gpu_last_error(char *buf, int32_t len) {
+  if (!buf || len <= 0) return TLM_E_BADARG;
+  std::snprintf(buf, (size_t)len, "%s", g_last_error.c_str());
+  return TLM_OK;
+}
+
+}  // extern "C"

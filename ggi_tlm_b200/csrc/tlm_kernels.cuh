@@ -1,0 +1,788 @@
+// tlm_kernels.cuh -- sm_100a kernels of the SCN-TLM time step.
+//
+// One time step of GGI_TLM (SRC/TLM_SOLVER/run_TLM.F90:240-293) is
+//   excitation -> scatter -> cell_output -> connect -> face_output -> outer_boundary.
+// Here it is re-formulated as a "pull" step over structure-of-arrays
+// reflected-pulse planes held in a ping-pong pair of buffers:
+//
+//   tlm_cell_kernel   : for every cell, gather the 12 incident pulses from the
+//                       neighbours' reflected pulses of the previous step (this
+//                       *is* the free-space connect, connect_normal_to_*.F90:1-10,
+//                       and the outer-boundary reflection, outer_boundary.F90:71-131,
+//                       read through ghost slots), scatter (scatter.F90,
+//                       scatter_PML.F90) and write the 12 reflected pulses.
+//                       12 plane reads + 12 plane writes per cell: one HBM pass.
+//   tlm_face_kernel   : the few special faces (Huygens excitation faces, output
+//                       faces) re-do their connect with the reference's formulas
+//                       (connect_normal_to_*.F90:287-360) in place on the
+//                       reflected planes and record face fields.
+//   tlm_dft_kernel    : FP64 frequency-domain accumulation on output faces
+//                       (frequency_output_surfaces.F90:405-406).
+//
+// Plane layout: element (x,y,z) of every port plane lives at
+//   ((z+1)*Py + (y+1))*Px + x,   Px = roundup(nx+1, 4), Py = ny+2, Pz = nz+2,
+// so x=-1 / x=nx, y=-1 / y=ny and z=-1 / z=nz are ghost slots.  A ghost slot
+// holds R * (the boundary cell's own reflected pulse), written by that cell,
+// which is exactly what the reference's outer_boundary leaves in the boundary
+// port before the next scatter.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tlm {
+
+// SRC/CONSTANTS/constants.F90:27-39
+constexpr double kZ0 = 376.73031346177;
+constexpr double kY0 = 1.0 / 376.73031346177;
+
+// port numbering, SRC/TLM_MODULES/Mesh_Modules.F90:83-94 (0-based)
+enum Port {
+  Vy_xmin = 0, Vz_xmin, Vy_xmax, Vz_xmax, Vx_ymin, Vz_ymin,
+  Vx_ymax, Vz_ymax, Vx_zmin, Vy_zmin, Vx_zmax, Vy_zmax
+};
+// PML paper notation, SRC/TLM_MODULES/PML_module.F90:59-70
+enum PmlPort {
+  Vxny = 0, Vxnz, Vxpy, Vxpz, Vynx, Vynz, Vypx, Vypz, Vznx, Vzny, Vzpx, Vzpy
+};
+
+enum SpecialFlags : int { SP_PML = 1, SP_MAT = 2, SP_EXC = 4, SP_OUT = 8 };
+
+constexpr int kMaxOrder = 8;
+constexpr int kPmlState = 24;  // Ix,Iy,Iz, Vi(12), Vxt,Vyt,Vzt, Vxyt,Vyxt,Vzxt,Vxzt,Vyzt,Vzyt
+
+// One volume material after calculate_volume_material_filter_coefficients.
+struct MatDev {
+  int type, eps_exists, mu_exists, eps_order, mu_order, pad0, pad1, pad2;
+  double Ys_eps_f, Zs_mu_f, Ge, Rm;
+  double eps_a[kMaxOrder + 1], eps_b[kMaxOrder + 1], mu_a[kMaxOrder + 1], mu_b[kMaxOrder + 1];
+};
+
+template <typename T>
+struct MeshDev {
+  int nx, ny, nz, Px, Py;
+  long long PxPy;           // elements per z-plane (incl. ghost rows)
+  long long plane;          // elements per port plane
+  int chunks_per_plane;     // ny*Px/VEC
+  int segs_per_plane;       // ceil(ny*Px/32)
+  T *links0, *links1;       // 12 planes each
+  T R[6];
+  const uint32_t *seg_mask;
+  const uint32_t *seg_base;
+  const int4 *sp_rec;
+  const int4 *sp_pos;       // (x, y, z) 0-based of each special cell
+  T *pml_state;             // [24][n_pml]
+  int n_pml;
+  const T *pml_par;         // [n_par][16]
+  T *pml_ixt;               // [n_out][3]
+  double *filt;             // [J][n_filt]
+  int n_filt, filt_eo, filt_mo;  // eps/mu max orders (state taps per component)
+  const MatDev *mats;
+  const double *exc_field;  // [n_timesteps][n_exc][9]
+  const int8_t *exc_type;   // [n_exc][6]
+  int n_exc;
+  double *cell_out;         // [n_timesteps][n_out][6]
+  int n_out;
+  double dl;
+  const int *d_base;        // device step counter (1-based step of relative step 0)
+};
+
+template <typename T, int VEC> struct VecT;
+template <> struct VecT<float, 4> { using type = float4; };
+template <> struct VecT<double, 2> { using type = double2; };
+
+template <typename T, int VEC>
+__device__ __forceinline__ void load_vec(const T *__restrict__ p, T (&v)[VEC]) {
+  using V = typename VecT<T, VEC>::type;
+  V q = __ldcs(reinterpret_cast<const V *>(p));
+  if constexpr (VEC == 4) { v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w; }
+  else { v[0] = q.x; v[1] = q.y; }
+}
+
+template <typename T, int VEC>
+__device__ __forceinline__ void store_vec(T *__restrict__ p, const T (&v)[VEC]) {
+  using V = typename VecT<T, VEC>::type;
+  V q;
+  if constexpr (VEC == 4) { q.x = v[0]; q.y = v[1]; q.z = v[2]; q.w = v[3]; }
+  else { q.x = v[0]; q.y = v[1]; }
+  __stcs(reinterpret_cast<V *>(p), q);
+}
+
+// ---------------------------------------------------------------------------
+// Free-space scatter, scatter.F90:222-272 (pull form: inc -> out)
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void scatter_pulses(const T *inc, T *out, T Vx, T Vy, T Vz, T Ix, T Iy, T Iz) {
+  const T Z0 = T(kZ0);
+  out[Vx_ymin] = Vx - Z0 * Iz - inc[Vx_ymax];
+  out[Vx_ymax] = Vx + Z0 * Iz - inc[Vx_ymin];
+  out[Vx_zmin] = Vx + Z0 * Iy - inc[Vx_zmax];
+  out[Vx_zmax] = Vx - Z0 * Iy - inc[Vx_zmin];
+  out[Vy_zmin] = Vy - Z0 * Ix - inc[Vy_zmax];
+  out[Vy_zmax] = Vy + Z0 * Ix - inc[Vy_zmin];
+  out[Vy_xmin] = Vy + Z0 * Iz - inc[Vy_xmax];
+  out[Vy_xmax] = Vy - Z0 * Iz - inc[Vy_xmin];
+  out[Vz_xmin] = Vz - Z0 * Iy - inc[Vz_xmax];
+  out[Vz_xmax] = Vz + Z0 * Iy - inc[Vz_xmin];
+  out[Vz_ymin] = Vz + Z0 * Ix - inc[Vz_ymax];
+  out[Vz_ymax] = Vz - Z0 * Ix - inc[Vz_ymin];
+}
+
+template <typename T>
+__device__ __forceinline__ void free_space_cell(const T *inc, T *out) {
+  T Vx = (inc[Vx_ymin] + inc[Vx_ymax] + inc[Vx_zmin] + inc[Vx_zmax]) / T(2);
+  T Vy = (inc[Vy_xmin] + inc[Vy_xmax] + inc[Vy_zmin] + inc[Vy_zmax]) / T(2);
+  T Vz = (inc[Vz_xmin] + inc[Vz_xmax] + inc[Vz_ymin] + inc[Vz_ymax]) / T(2);
+  T Ix, Iy, Iz;
+  if constexpr (sizeof(T) == 8) {
+    Ix = (inc[Vz_ymax] - inc[Vy_zmax] - inc[Vz_ymin] + inc[Vy_zmin]) / (2.0 * kZ0);
+    Iy = (inc[Vx_zmax] - inc[Vz_xmax] - inc[Vx_zmin] + inc[Vz_xmin]) / (2.0 * kZ0);
+    Iz = (inc[Vy_xmax] - inc[Vx_ymax] - inc[Vy_xmin] + inc[Vx_ymin]) / (2.0 * kZ0);
+  } else {
+    const float r = float(1.0 / (2.0 * kZ0));
+    Ix = (inc[Vz_ymax] - inc[Vy_zmax] - inc[Vz_ymin] + inc[Vy_zmin]) * r;
+    Iy = (inc[Vx_zmax] - inc[Vz_xmax] - inc[Vx_zmin] + inc[Vz_xmin]) * r;
+    Iz = (inc[Vy_xmax] - inc[Vx_ymax] - inc[Vy_xmin] + inc[Vx_ymin]) * r;
+  }
+  scatter_pulses<T>(inc, out, Vx, Vy, Vz, Ix, Iy, Iz);
+}
+
+// ---------------------------------------------------------------------------
+// PML free-space cell, scatter_PML.F90:22-313
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par, int out_no, const T *inc_in, T *out,
+                                      double *cell_out_row) {
+  const T Z0 = T(kZ0);
+  const T *P = m.pml_par + (size_t)par * 16;
+  const T ax = P[0], ay = P[1], az = P[2];
+  const T exp_x = P[3], exp_y = P[4], exp_z = P[5];
+  const T Csx = P[6], Csy = P[7], Csz = P[8];
+  const T Csx2 = P[9], Csy2 = P[10], Csz2 = P[11];
+  const T Csy_sz = P[12], Csz_sx = P[13], Csx_sy = P[14];
+  T *S = m.pml_state;
+  const int n = m.n_pml;
+  const T last_Ix = S[0 * n + pidx], last_Iy = S[1 * n + pidx], last_Iz = S[2 * n + pidx];
+  T last_Vi[12];
+#pragma unroll
+  for (int k = 0; k < 12; k++) last_Vi[k] = S[(3 + k) * n + pidx];
+  const T last_Vxt = S[15 * n + pidx], last_Vyt = S[16 * n + pidx], last_Vzt = S[17 * n + pidx];
+  const T last_Vxyt = S[18 * n + pidx], last_Vyxt = S[19 * n + pidx], last_Vzxt = S[20 * n + pidx];
+  const T last_Vxzt = S[21 * n + pidx], last_Vyzt = S[22 * n + pidx], last_Vzyt = S[23 * n + pidx];
+
+  // STAGE 3: half-cell loss on incident pulses
+  T V[12];
+  V[Vynx] = inc_in[Vynx] * exp_y; V[Vypx] = inc_in[Vypx] * exp_y;
+  V[Vznx] = inc_in[Vznx] * exp_z; V[Vzpx] = inc_in[Vzpx] * exp_z;
+  V[Vxny] = inc_in[Vxny] * exp_x; V[Vxpy] = inc_in[Vxpy] * exp_x;
+  V[Vzny] = inc_in[Vzny] * exp_z; V[Vzpy] = inc_in[Vzpy] * exp_z;
+  V[Vxnz] = inc_in[Vxnz] * exp_x; V[Vxpz] = inc_in[Vxpz] * exp_x;
+  V[Vynz] = inc_in[Vynz] * exp_y; V[Vypz] = inc_in[Vypz] * exp_y;
+  // STAGE 4
+  const T Vx = (V[Vynx] + V[Vypx] + V[Vznx] + V[Vzpx]) / T(2);
+  const T Vy = (V[Vxny] + V[Vxpy] + V[Vzny] + V[Vzpy]) / T(2);
+  const T Vz = (V[Vxnz] + V[Vxpz] + V[Vynz] + V[Vypz]) / T(2);
+  const T Ix = (V[Vypz] - V[Vzpy] - V[Vynz] + V[Vzny]) / (T(2) * Z0);
+  const T Iy = (V[Vzpx] - V[Vxpz] - V[Vznx] + V[Vxnz]) / (T(2) * Z0);
+  const T Iz = (V[Vxpy] - V[Vypx] - V[Vxny] + V[Vynx]) / (T(2) * Z0);
+  // STAGE 5
+  const T Vx_sh = ax * (-(last_Vi[Vznx] + last_Vi[Vzpx] + last_Vi[Vynx] + last_Vi[Vypx]) / T(2) +
+                        Csy * ((V[Vznx] + V[Vzpx]) + (last_Vi[Vznx] + last_Vi[Vzpx])) +
+                        Csz * ((V[Vynx] + V[Vypx]) + (last_Vi[Vynx] + last_Vi[Vypx])) + Csy_sz * last_Vxt);
+  const T Vy_sh = ay * (-(last_Vi[Vxny] + last_Vi[Vxpy] + last_Vi[Vzny] + last_Vi[Vzpy]) / T(2) +
+                        Csz * ((V[Vxny] + V[Vxpy]) + (last_Vi[Vxny] + last_Vi[Vxpy])) +
+                        Csx * ((V[Vzny] + V[Vzpy]) + (last_Vi[Vzny] + last_Vi[Vzpy])) + Csz_sx * last_Vyt);
+  const T Vz_sh = az * (-(last_Vi[Vynz] + last_Vi[Vypz] + last_Vi[Vxnz] + last_Vi[Vxpz]) / T(2) +
+                        Csx * ((V[Vynz] + V[Vypz]) + (last_Vi[Vynz] + last_Vi[Vypz])) +
+                        Csy * ((V[Vxnz] + V[Vxpz]) + (last_Vi[Vxnz] + last_Vi[Vxpz])) + Csx_sy * last_Vzt);
+  // STAGE 6
+  const T Vxt = ax * Vx + Vx_sh, Vyt = ay * Vy + Vy_sh, Vzt = az * Vz + Vz_sh;
+  // STAGE 7a (output cells only)
+  T Ixt = T(0), Iyt = T(0), Izt = T(0);
+  if (out_no >= 0) {
+    T *X = m.pml_ixt + (size_t)out_no * 3;
+    Ixt = ax * (Ix - last_Ix + Csx2 * (Ix + last_Ix) + Csy_sz * X[0]);
+    Iyt = ay * (Iy - last_Iy + Csy2 * (Iy + last_Iy) + Csz_sx * X[1]);
+    Izt = az * (Iz - last_Iz + Csz2 * (Iz + last_Iz) + Csx_sy * X[2]);
+    X[0] = Ixt; X[1] = Iyt; X[2] = Izt;
+  }
+  // STAGE 7
+  const T Vxy_se = az * (Z0 * (-last_Iz + Csy2 * (Iz + last_Iz)) + Csx_sy * last_Vxyt);
+  const T Vyx_se = az * (Z0 * (-last_Iz + Csx2 * (Iz + last_Iz)) + Csx_sy * last_Vyxt);
+  const T Vzx_se = ay * (Z0 * (-last_Iy + Csx2 * (Iy + last_Iy)) + Csz_sx * last_Vzxt);
+  const T Vxz_se = ay * (Z0 * (-last_Iy + Csz2 * (Iy + last_Iy)) + Csz_sx * last_Vxzt);
+  const T Vyz_se = ax * (Z0 * (-last_Ix + Csz2 * (Ix + last_Ix)) + Csy_sz * last_Vyzt);
+  const T Vzy_se = ax * (Z0 * (-last_Ix + Csy2 * (Ix + last_Ix)) + Csy_sz * last_Vzyt);
+  // STAGE 8 + 9: save state
+  S[0 * n + pidx] = Ix; S[1 * n + pidx] = Iy; S[2 * n + pidx] = Iz;
+#pragma unroll
+  for (int k = 0; k < 12; k++) S[(3 + k) * n + pidx] = V[k];
+  S[15 * n + pidx] = Vxt; S[16 * n + pidx] = Vyt; S[17 * n + pidx] = Vzt;
+  S[18 * n + pidx] = az * Iz * Z0 + Vxy_se;
+  S[19 * n + pidx] = az * Iz * Z0 + Vyx_se;
+  S[20 * n + pidx] = ay * Iy * Z0 + Vzx_se;
+  S[21 * n + pidx] = ay * Iy * Z0 + Vxz_se;
+  S[22 * n + pidx] = ax * Ix * Z0 + Vyz_se;
+  S[23 * n + pidx] = ax * Ix * Z0 + Vzy_se;
+  // STAGE 10
+  const T Vynx_P = Vx_sh - Vyx_se, Vypx_P = Vx_sh + Vyx_se;
+  const T Vznx_P = Vx_sh + Vzx_se, Vzpx_P = Vx_sh - Vzx_se;
+  const T Vxny_P = Vy_sh + Vxy_se, Vxpy_P = Vy_sh - Vxy_se;
+  const T Vzny_P = Vy_sh - Vzy_se, Vzpy_P = Vy_sh + Vzy_se;
+  const T Vynz_P = Vz_sh + Vyz_se, Vypz_P = Vz_sh - Vyz_se;
+  const T Vxnz_P = Vz_sh - Vxz_se, Vxpz_P = Vz_sh + Vxz_se;
+  // STAGE 11 + 13: scattered pulses with half-cell loss
+  out[Vynx] = (ax * Vx - az * Z0 * Iz - V[Vypx] + Vynx_P) * exp_y;
+  out[Vypx] = (ax * Vx + az * Z0 * Iz - V[Vynx] + Vypx_P) * exp_y;
+  out[Vznx] = (ax * Vx + ay * Z0 * Iy - V[Vzpx] + Vznx_P) * exp_z;
+  out[Vzpx] = (ax * Vx - ay * Z0 * Iy - V[Vznx] + Vzpx_P) * exp_z;
+  out[Vzny] = (ay * Vy - ax * Z0 * Ix - V[Vzpy] + Vzny_P) * exp_z;
+  out[Vzpy] = (ay * Vy + ax * Z0 * Ix - V[Vzny] + Vzpy_P) * exp_z;
+  out[Vxny] = (ay * Vy + az * Z0 * Iz - V[Vxpy] + Vxny_P) * exp_x;
+  out[Vxpy] = (ay * Vy - az * Z0 * Iz - V[Vxny] + Vxpy_P) * exp_x;
+  out[Vxnz] = (az * Vz - ay * Z0 * Iy - V[Vxpz] + Vxnz_P) * exp_x;
+  out[Vxpz] = (az * Vz + ay * Z0 * Iy - V[Vxnz] + Vxpz_P) * exp_x;
+  out[Vynz] = (az * Vz + ax * Z0 * Ix - V[Vypz] + Vynz_P) * exp_y;
+  out[Vypz] = (az * Vz - ax * Z0 * Ix - V[Vynz] + Vypz_P) * exp_y;
+  // STAGE 12: output
+  if (out_no >= 0) {
+    const double dl = m.dl;
+    cell_out_row[0] = -double(Vxt) / dl; cell_out_row[1] = -double(Vyt) / dl; cell_out_row[2] = -double(Vzt) / dl;
+    cell_out_row[3] = double(Ixt) / dl; cell_out_row[4] = double(Iyt) / dl; cell_out_row[5] = double(Izt) / dl;
+  }
+}
+
+// evaluate_Zfilter (filter_subroutines.F90:510-540) on a state whose taps
+// w(1..order) are given; returns f and sets w0.
+__device__ __forceinline__ double zfilter_eval(const double *a, const double *b, int order, const double *w, double G,
+                                               double &w0) {
+  double W0 = G;
+  for (int i = 1; i <= order; i++) W0 = W0 - b[i] * w[i];
+  W0 = W0 / b[0];
+  w0 = W0;
+  double F0 = 0.0;
+  F0 = F0 + a[0] * W0;
+  for (int i = 1; i <= order; i++) F0 = F0 + a[i] * w[i];
+  return F0;
+}
+
+// ---------------------------------------------------------------------------
+// Material / excitation / output cell (not PML), scatter.F90:274-547, in FP64
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void special_cell(const MeshDev<T> &m, int4 rec, int t, const T *incT, T *outT) {
+  const int flags = rec.x & 0xff;
+  const int material = rec.x >> 8;
+  double inc[12];
+#pragma unroll
+  for (int k = 0; k < 12; k++) inc[k] = double(incT[k]);
+  const double Z04 = kZ0 * 4.0, Y04 = kY0 * 4.0;
+  double VEx = (inc[Vx_ymin] + inc[Vx_ymax] + inc[Vx_zmin] + inc[Vx_zmax]) / 2.0;
+  double VEy = (inc[Vy_xmin] + inc[Vy_xmax] + inc[Vy_zmin] + inc[Vy_zmax]) / 2.0;
+  double VEz = (inc[Vz_xmin] + inc[Vz_xmax] + inc[Vz_ymin] + inc[Vz_ymax]) / 2.0;
+  double Yx = Y04, Yy = Y04, Yz = Y04;
+  double VHx = 2.0 * (inc[Vz_ymax] - inc[Vy_zmax] - inc[Vz_ymin] + inc[Vy_zmin]);
+  double VHy = 2.0 * (inc[Vx_zmax] - inc[Vz_xmax] - inc[Vx_zmin] + inc[Vz_xmin]);
+  double VHz = 2.0 * (inc[Vy_xmax] - inc[Vx_ymax] - inc[Vy_xmin] + inc[Vx_ymin]);
+  double Zx = Z04, Zy = Z04, Zz = Z04;
+  double Vo[3] = {0, 0, 0}, Ys = 0.0;
+  double we[3][kMaxOrder + 1], wm[3][kMaxOrder + 1];
+  const MatDev *M = nullptr;
+  int type = 0;
+  const int fidx = rec.y;
+  if (flags & SP_MAT) {
+    M = m.mats + (material - 1);
+    type = M->type;
+  }
+  if (type == 1) {
+    VEx = 0.0; VEy = 0.0; VEz = 0.0;
+  } else if (type == 2) {
+    VHx = 0.0; VHy = 0.0; VHz = 0.0;
+  } else if (type == 3) {
+    if (M->eps_exists) {
+      Ys = M->Ys_eps_f;
+      const int o = M->eps_order;
+      for (int c = 0; c < 3; c++) {
+        // timeshift_Zfilter: w(i) <- w(i-1)
+        for (int k = 0; k < o; k++) we[c][k + 1] = m.filt[(size_t)(c * m.filt_eo + k) * m.n_filt + fidx];
+        Vo[c] = zfilter_eval(M->eps_a, M->eps_b, o, we[c], 0.0, we[c][0]);
+      }
+      double V1, Y1;
+      V1 = (VEx * Yx + Vo[0] * Ys) / (Yx + Ys); Y1 = Yx + Ys; VEx = V1; Yx = Y1;
+      V1 = (VEy * Yy + Vo[1] * Ys) / (Yy + Ys); Y1 = Yy + Ys; VEy = V1; Yy = Y1;
+      V1 = (VEz * Yz + Vo[2] * Ys) / (Yz + Ys); Y1 = Yz + Ys; VEz = V1; Yz = Y1;
+    }
+    const double Ge = M->Ge;
+    double V1, Y1;
+    V1 = (VEx * Yx + 0.0 * Ge) / (Yx + Ge); Y1 = Yx + Ge; VEx = V1; Yx = Y1;
+    V1 = (VEy * Yy + 0.0 * Ge) / (Yy + Ge); Y1 = Yy + Ge; VEy = V1; Yy = Y1;
+    V1 = (VEz * Yz + 0.0 * Ge) / (Yz + Ge); Y1 = Yz + Ge; VEz = V1; Yz = Y1;
+    if (M->mu_exists) {
+      const double Zs = M->Zs_mu_f;
+      const int o = M->mu_order;
+      double Vs[3];
+      for (int c = 0; c < 3; c++) {
+        for (int k = 0; k < o; k++)
+          wm[c][k + 1] = m.filt[(size_t)(3 * m.filt_eo + c * m.filt_mo + k) * m.n_filt + fidx];
+        Vs[c] = zfilter_eval(M->mu_a, M->mu_b, o, wm[c], 0.0, wm[c][0]);
+      }
+      VHx = VHx + Vs[0]; Zx = Zx + Zs;
+      VHy = VHy + Vs[1]; Zy = Zy + Zs;
+      VHz = VHz + Vs[2]; Zz = Zz + Zs;
+    }
+    const double Rm = M->Rm;
+    VHx = VHx + 0.0; Zx = Zx + Rm;
+    VHy = VHy + 0.0; Zy = Zy + Rm;
+    VHz = VHz + 0.0; Zz = Zz + Rm;
+  }
+  double Vx = VEx, Vy = VEy, Vz = VEz;
+  double Ix = VHx / Zx, Iy = VHy / Zy, Iz = VHz / Zz;
+  if (flags & SP_EXC) {
+    // scatter.F90:429-450
+    const int e = rec.z;
+    const double *field = m.exc_field + ((size_t)(t - 1) * m.n_exc + e) * 9;
+    const int8_t *h = m.exc_type + (size_t)e * 6;
+    const double dl = m.dl;
+    const double Isx = field[6] * dl * dl, Isy = field[7] * dl * dl, Isz = field[8] * dl * dl;
+    Vx = double(h[0]) * Vx - field[0] * dl / 2.0 + Isx / Yx;
+    Vy = double(h[1]) * Vy - field[1] * dl / 2.0 + Isy / Yy;
+    Vz = double(h[2]) * Vz - field[2] * dl / 2.0 + Isz / Yz;
+    Ix = double(h[3]) * Ix + field[3] * dl / 2.0;
+    Iy = double(h[4]) * Iy + field[4] * dl / 2.0;
+    Iz = double(h[5]) * Iz + field[5] * dl / 2.0;
+  }
+  if (flags & SP_OUT) {
+    // scatter.F90:465-480
+    const double dl = m.dl;
+    double *f = m.cell_out + ((size_t)(t - 1) * m.n_out + rec.w) * 6;
+    f[0] = -Vx / dl; f[1] = -Vy / dl; f[2] = -Vz / dl;
+    f[3] = Ix / dl; f[4] = Iy / dl; f[5] = Iz / dl;
+  }
+  if (type == 3) {
+    // filter update, scatter.F90:483-515; store taps w(0..order-1)
+    if (M->eps_exists) {
+      const int o = M->eps_order;
+      const double Io[3] = {(Vx - Vo[0]) * Ys, (Vy - Vo[1]) * Ys, (Vz - Vo[2]) * Ys};
+      for (int c = 0; c < 3; c++) {
+        zfilter_eval(M->eps_a, M->eps_b, o, we[c], Io[c], we[c][0]);
+        for (int k = 0; k < o; k++) m.filt[(size_t)(c * m.filt_eo + k) * m.n_filt + fidx] = we[c][k];
+      }
+    }
+    if (M->mu_exists) {
+      const int o = M->mu_order;
+      const double G[3] = {-Ix, -Iy, -Iz};
+      for (int c = 0; c < 3; c++) {
+        zfilter_eval(M->mu_a, M->mu_b, o, wm[c], G[c], wm[c][0]);
+        for (int k = 0; k < o; k++) m.filt[(size_t)(3 * m.filt_eo + c * m.filt_mo + k) * m.n_filt + fidx] = wm[c][k];
+      }
+    }
+  }
+  // scatter.F90:519-547
+  double out[12];
+  const double Z0 = kZ0;
+  out[Vx_ymin] = Vx - Z0 * Iz - inc[Vx_ymax];
+  out[Vx_ymax] = Vx + Z0 * Iz - inc[Vx_ymin];
+  out[Vx_zmin] = Vx + Z0 * Iy - inc[Vx_zmax];
+  out[Vx_zmax] = Vx - Z0 * Iy - inc[Vx_zmin];
+  out[Vy_zmin] = Vy - Z0 * Ix - inc[Vy_zmax];
+  out[Vy_zmax] = Vy + Z0 * Ix - inc[Vy_zmin];
+  out[Vy_xmin] = Vy + Z0 * Iz - inc[Vy_xmax];
+  out[Vy_xmax] = Vy - Z0 * Iz - inc[Vy_xmin];
+  out[Vz_xmin] = Vz - Z0 * Iy - inc[Vz_xmax];
+  out[Vz_xmax] = Vz + Z0 * Iy - inc[Vz_xmin];
+  out[Vz_ymin] = Vz + Z0 * Ix - inc[Vz_ymax];
+  out[Vz_ymax] = Vz - Z0 * Ix - inc[Vz_ymin];
+#pragma unroll
+  for (int k = 0; k < 12; k++) outT[k] = T(out[k]);
+}
+
+// ---------------------------------------------------------------------------
+// Bulk kernel: gather (connect + outer boundary) + free-space scatter for all
+// non-special cells.  grid = (ceil(chunks_per_plane/blockDim), nz); one thread
+// = VEC consecutive x-cells.  Special cells are skipped (their stores are
+// masked out; warps made only of special or out-of-range cells return early)
+// and are done by tlm_special_kernel from the same input buffer.
+// ---------------------------------------------------------------------------
+template <typename T, int VEC>
+__global__ void __launch_bounds__(256) tlm_cell_kernel(const MeshDev<T> m, int rel_step) {
+  const int z = blockIdx.y;
+  const int chunk = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = chunk < m.chunks_per_plane;
+  const int lane = threadIdx.x & 31;
+  const int e = chunk * VEC;  // element offset in the plane interior
+  uint32_t mine = 0;
+  int nvalid = 0, y = 0, x0 = 0;
+  if (valid) {
+    y = e / m.Px;
+    x0 = e - y * m.Px;
+    nvalid = min(VEC, m.nx - x0);
+    const uint32_t mask = __ldg(m.seg_mask + (size_t)z * m.segs_per_plane + (e >> 5));
+    mine = (mask >> (e & 31)) & ((1u << VEC) - 1u);
+  }
+  const uint32_t need = (nvalid > 0) ? (((1u << nvalid) - 1u) & ~mine) : 0u;  // cells to write
+  if (__all_sync(0xffffffffu, need == 0)) return;
+  const int t = *m.d_base + rel_step;  // 1-based timestep
+  const T *__restrict__ in = (t & 1) ? m.links0 : m.links1;   // R_{t-1}
+  T *__restrict__ out = (t & 1) ? m.links1 : m.links0;        // R_t
+  const long long P = m.plane;
+  const long long idx = (long long)(z + 1) * m.PxPy + (long long)m.Px + e;
+  const long long dy = m.Px, dz = m.PxPy;
+
+  T inc[12][VEC];
+  if (valid) {
+    load_vec<T, VEC>(in + Vx_ymax * P + idx - dy, inc[Vx_ymin]);
+    load_vec<T, VEC>(in + Vz_ymax * P + idx - dy, inc[Vz_ymin]);
+    load_vec<T, VEC>(in + Vx_ymin * P + idx + dy, inc[Vx_ymax]);
+    load_vec<T, VEC>(in + Vz_ymin * P + idx + dy, inc[Vz_ymax]);
+    load_vec<T, VEC>(in + Vx_zmax * P + idx - dz, inc[Vx_zmin]);
+    load_vec<T, VEC>(in + Vy_zmax * P + idx - dz, inc[Vy_zmin]);
+    load_vec<T, VEC>(in + Vx_zmin * P + idx + dz, inc[Vx_zmax]);
+    load_vec<T, VEC>(in + Vy_zmin * P + idx + dz, inc[Vy_zmax]);
+  }
+  {
+    // x neighbours: own aligned chunk + one element from the neighbouring lane
+    T a[VEC], b[VEC], c[VEC], d[VEC];
+#pragma unroll
+    for (int j = 0; j < VEC; j++) { a[j] = T(0); b[j] = T(0); c[j] = T(0); d[j] = T(0); }
+    if (valid) {
+      load_vec<T, VEC>(in + Vy_xmax * P + idx, a);
+      load_vec<T, VEC>(in + Vz_xmax * P + idx, b);
+      load_vec<T, VEC>(in + Vy_xmin * P + idx, c);
+      load_vec<T, VEC>(in + Vz_xmin * P + idx, d);
+    }
+    T pa = __shfl_up_sync(0xffffffffu, a[VEC - 1], 1);
+    T pb = __shfl_up_sync(0xffffffffu, b[VEC - 1], 1);
+    T nc = __shfl_down_sync(0xffffffffu, c[0], 1);
+    T nd = __shfl_down_sync(0xffffffffu, d[0], 1);
+    if (valid && lane == 0) {
+      pa = in[Vy_xmax * P + idx - 1];
+      pb = in[Vz_xmax * P + idx - 1];
+    }
+    if (valid && lane == 31) {
+      nc = in[Vy_xmin * P + idx + VEC];
+      nd = in[Vz_xmin * P + idx + VEC];
+    }
+    inc[Vy_xmin][0] = pa;
+    inc[Vz_xmin][0] = pb;
+#pragma unroll
+    for (int j = 1; j < VEC; j++) { inc[Vy_xmin][j] = a[j - 1]; inc[Vz_xmin][j] = b[j - 1]; }
+#pragma unroll
+    for (int j = 0; j < VEC - 1; j++) { inc[Vy_xmax][j] = c[j + 1]; inc[Vz_xmax][j] = d[j + 1]; }
+    inc[Vy_xmax][VEC - 1] = nc;
+    inc[Vz_xmax][VEC - 1] = nd;
+  }
+  if (need == 0) return;
+
+  // free-space scatter; results overwrite the cell's own incident slots
+#pragma unroll
+  for (int j = 0; j < VEC; j++) {
+    T ci[12], co[12];
+#pragma unroll
+    for (int p = 0; p < 12; p++) ci[p] = inc[p][j];
+    free_space_cell<T>(ci, co);
+#pragma unroll
+    for (int p = 0; p < 12; p++) inc[p][j] = co[p];
+  }
+#define res inc
+
+  if (need == (1u << VEC) - 1u) {
+#pragma unroll
+    for (int p = 0; p < 12; p++) store_vec<T, VEC>(out + p * P + idx, res[p]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < VEC; j++)
+      if (need & (1u << j))
+#pragma unroll
+        for (int p = 0; p < 12; p++) out[p * P + idx + j] = res[p][j];
+  }
+  // ghost slots: R * own reflected pulse (outer_boundary.F90:71-131)
+  if (x0 == 0 && (need & 1u)) {
+    out[Vy_xmax * P + idx - 1] = m.R[0] * res[Vy_xmin][0];
+    out[Vz_xmax * P + idx - 1] = m.R[0] * res[Vz_xmin][0];
+  }
+  if (x0 + nvalid == m.nx) {
+    const int j = nvalid - 1;  // last cell of the row (selected without dynamic register indexing)
+    T vy = res[Vy_xmax][0], vz = res[Vz_xmax][0];
+#pragma unroll
+    for (int k = 1; k < VEC; k++)
+      if (j == k) { vy = res[Vy_xmax][k]; vz = res[Vz_xmax][k]; }
+    if (need & (1u << j)) {
+      out[Vy_xmin * P + idx + j + 1] = m.R[1] * vy;
+      out[Vz_xmin * P + idx + j + 1] = m.R[1] * vz;
+    }
+  }
+  if (y == 0) {
+#pragma unroll
+    for (int j = 0; j < VEC; j++)
+      if (need & (1u << j)) {
+        out[Vx_ymax * P + idx - dy + j] = m.R[2] * res[Vx_ymin][j];
+        out[Vz_ymax * P + idx - dy + j] = m.R[2] * res[Vz_ymin][j];
+      }
+  }
+  if (y == m.ny - 1) {
+#pragma unroll
+    for (int j = 0; j < VEC; j++)
+      if (need & (1u << j)) {
+        out[Vx_ymin * P + idx + dy + j] = m.R[3] * res[Vx_ymax][j];
+        out[Vz_ymin * P + idx + dy + j] = m.R[3] * res[Vz_ymax][j];
+      }
+  }
+  if (z == 0) {
+#pragma unroll
+    for (int j = 0; j < VEC; j++)
+      if (need & (1u << j)) {
+        out[Vx_zmax * P + idx - dz + j] = m.R[4] * res[Vx_zmin][j];
+        out[Vy_zmax * P + idx - dz + j] = m.R[4] * res[Vy_zmin][j];
+      }
+  }
+  if (z == m.nz - 1) {
+#pragma unroll
+    for (int j = 0; j < VEC; j++)
+      if (need & (1u << j)) {
+        out[Vx_zmin * P + idx + dz + j] = m.R[5] * res[Vx_zmax][j];
+        out[Vy_zmin * P + idx + dz + j] = m.R[5] * res[Vy_zmax][j];
+      }
+  }
+}
+
+#undef res
+
+// ---------------------------------------------------------------------------
+// Special-cell kernel: one thread per special cell (traversal order, so PML
+// state and links coalesce along x): gather, PML / material / excitation /
+// output scatter, reflected pulses + ghost slots.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128) tlm_special_kernel(const MeshDev<T> m, int n_special, int rel_step) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_special) return;
+  const int t = *m.d_base + rel_step;
+  const T *__restrict__ in = (t & 1) ? m.links0 : m.links1;
+  T *__restrict__ out = (t & 1) ? m.links1 : m.links0;
+  const long long P = m.plane;
+  const int4 pos = m.sp_pos[s];
+  const int4 rec = m.sp_rec[s];
+  const long long idx = (long long)(pos.z + 1) * m.PxPy + (long long)(pos.y + 1) * m.Px + pos.x;
+  const long long dy = m.Px, dz = m.PxPy;
+  T ci[12], co[12];
+  ci[Vy_xmin] = in[Vy_xmax * P + idx - 1];
+  ci[Vz_xmin] = in[Vz_xmax * P + idx - 1];
+  ci[Vy_xmax] = in[Vy_xmin * P + idx + 1];
+  ci[Vz_xmax] = in[Vz_xmin * P + idx + 1];
+  ci[Vx_ymin] = in[Vx_ymax * P + idx - dy];
+  ci[Vz_ymin] = in[Vz_ymax * P + idx - dy];
+  ci[Vx_ymax] = in[Vx_ymin * P + idx + dy];
+  ci[Vz_ymax] = in[Vz_ymin * P + idx + dy];
+  ci[Vx_zmin] = in[Vx_zmax * P + idx - dz];
+  ci[Vy_zmin] = in[Vy_zmax * P + idx - dz];
+  ci[Vx_zmax] = in[Vx_zmin * P + idx + dz];
+  ci[Vy_zmax] = in[Vy_zmin * P + idx + dz];
+  if (rec.x & SP_PML) {
+    double *row = (rec.w >= 0) ? m.cell_out + ((size_t)(t - 1) * m.n_out + rec.w) * 6 : nullptr;
+    pml_cell<T>(m, rec.y, rec.z, rec.w, ci, co, row);
+  } else {
+    special_cell<T>(m, rec, t, ci, co);
+  }
+#pragma unroll
+  for (int p = 0; p < 12; p++) out[p * P + idx] = co[p];
+  if (pos.x == 0) {
+    out[Vy_xmax * P + idx - 1] = m.R[0] * co[Vy_xmin];
+    out[Vz_xmax * P + idx - 1] = m.R[0] * co[Vz_xmin];
+  }
+  if (pos.x == m.nx - 1) {
+    out[Vy_xmin * P + idx + 1] = m.R[1] * co[Vy_xmax];
+    out[Vz_xmin * P + idx + 1] = m.R[1] * co[Vz_xmax];
+  }
+  if (pos.y == 0) {
+    out[Vx_ymax * P + idx - dy] = m.R[2] * co[Vx_ymin];
+    out[Vz_ymax * P + idx - dy] = m.R[2] * co[Vz_ymin];
+  }
+  if (pos.y == m.ny - 1) {
+    out[Vx_ymin * P + idx + dy] = m.R[3] * co[Vx_ymax];
+    out[Vz_ymin * P + idx + dy] = m.R[3] * co[Vz_ymax];
+  }
+  if (pos.z == 0) {
+    out[Vx_zmax * P + idx - dz] = m.R[4] * co[Vx_zmin];
+    out[Vy_zmax * P + idx - dz] = m.R[4] * co[Vy_zmin];
+  }
+  if (pos.z == m.nz - 1) {
+    out[Vx_zmin * P + idx + dz] = m.R[5] * co[Vx_zmax];
+    out[Vy_zmin * P + idx + dz] = m.R[5] * co[Vy_zmax];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Special faces: Huygens excitation + face outputs, connect_normal_to_*.F90
+// ---------------------------------------------------------------------------
+struct FaceDev {
+  const int4 *face;        // (x, y, z) 0-based of the + cell, dir 1..3
+  const int2 *face_io;     // (exc index or -1, out index or -1)
+  const double4 *hs;       // per special face: (offset, nx, ny, nz) when exc
+  int n_faces;
+  double Ei[3], Hi[3];
+  double offset_min, c, dt, dl;
+  const double *value_face;  // [n_timesteps] of the Huygens function
+  int n_timesteps;
+  double *face_field;      // [n_out_faces][2][6]
+};
+
+template <typename T>
+__global__ void tlm_face_kernel(const MeshDev<T> m, const FaceDev fd, int rel_step) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= fd.n_faces) return;
+  const int t = *m.d_base + rel_step;
+  T *R = (t & 1) ? m.links1 : m.links0;  // R_t just written by the cell kernel
+  const long long P = m.plane;
+  const int4 fc = fd.face[f];
+  const int2 io = fd.face_io[f];
+  const int dir = fc.w;
+  const long long ip = (long long)(fc.z + 1) * m.PxPy + (long long)(fc.y + 1) * m.Px + fc.x;  // + cell
+  const long long step = dir == 1 ? 1 : (dir == 2 ? (long long)m.Px : m.PxPy);
+  const long long im = ip - step;  // - cell
+  int pmin1, pmax1, pmin2, pmax2;
+  if (dir == 1) { pmin1 = Vy_xmin; pmax1 = Vy_xmax; pmin2 = Vz_xmin; pmax2 = Vz_xmax; }
+  else if (dir == 2) { pmin1 = Vx_ymin; pmax1 = Vx_ymax; pmin2 = Vz_ymin; pmax2 = Vz_ymax; }
+  else { pmin1 = Vx_zmin; pmax1 = Vx_zmax; pmin2 = Vy_zmin; pmax2 = Vy_zmax; }
+  // reflected pulses at the face: a = from the + cell (its min port), b = from the - cell
+  const double a1 = double(R[pmin1 * P + ip]), b1 = double(R[pmax1 * P + im]);
+  const double a2 = double(R[pmin2 * P + ip]), b2 = double(R[pmax2 * P + im]);
+  double A_min = a1 + b1, A_max = A_min;
+  double B_min = a2 + b2, B_max = B_min;
+  if (io.x >= 0) {
+    // Huygens_surface_excitation (huygens_surface.F90:734-848) with
+    // get_interpolated_excitation_value (excitation.F90:645-690)
+    const double4 h = fd.hs[f];
+    const double dt = fd.dt;
+    const double t_offset = (h.x - fd.offset_min) / fd.c;
+    const double local_time = (double(t - 1)) * dt - t_offset;
+    const int ts1 = (int)round(local_time / dt);
+    const int ts2 = ts1 + 1;
+    const double delta_t = local_time - double(ts1) * dt;
+    const double v1 = (ts1 >= 1 && ts1 <= fd.n_timesteps) ? fd.value_face[ts1 - 1] : 0.0;
+    const double v2 = (ts2 >= 1 && ts2 <= fd.n_timesteps) ? fd.value_face[ts2 - 1] : 0.0;
+    const double value = v1 + delta_t * (v2 - v1) / dt;
+    const double nx_ = h.y, ny_ = h.z, nz_ = h.w;
+    const double *Hi = fd.Hi, *Ei = fd.Ei;
+    double Js[3], Ms[3];
+    Js[0] = (ny_ * value * (Hi[2]) - nz_ * value * (Hi[1]));
+    Js[1] = (nz_ * value * (Hi[0]) - nx_ * value * (Hi[2]));
+    Js[2] = (nx_ * value * (Hi[1]) - ny_ * value * (Hi[0]));
+    Ms[0] = -(ny_ * value * (Ei[2]) - nz_ * value * (Ei[1]));
+    Ms[1] = -(nz_ * value * (Ei[0]) - nx_ * value * (Ei[2]));
+    Ms[2] = -(nx_ * value * (Ei[1]) - ny_ * value * (Ei[0]));
+    const double dl = fd.dl, Z0 = kZ0;
+    // soft source (hard_source_factor = 1), only J and M terms are non-zero
+    if (dir == 1) {  // connect_normal_to_x.F90:301-305
+      A_min = A_min * 1.0 + Js[1] * dl * Z0 / 2.0 + Ms[2] * dl / 2.0;
+      A_max = A_max * 1.0 + Js[1] * dl * Z0 / 2.0 - Ms[2] * dl / 2.0;
+      B_min = B_min * 1.0 + Js[2] * dl * Z0 / 2.0 - Ms[1] * dl / 2.0;
+      B_max = B_max * 1.0 + Js[2] * dl * Z0 / 2.0 + Ms[1] * dl / 2.0;
+    } else if (dir == 2) {  // connect_normal_to_y.F90:304-308
+      A_min = A_min * 1.0 + Js[0] * dl * Z0 / 2.0 - Ms[2] * dl / 2.0;
+      A_max = A_max * 1.0 + Js[0] * dl * Z0 / 2.0 + Ms[2] * dl / 2.0;
+      B_min = B_min * 1.0 + Js[2] * dl * Z0 / 2.0 + Ms[0] * dl / 2.0;
+      B_max = B_max * 1.0 + Js[2] * dl * Z0 / 2.0 - Ms[0] * dl / 2.0;
+    } else {  // connect_normal_to_z.F90:302-306
+      A_min = A_min * 1.0 + Js[0] * dl * Z0 / 2.0 + Ms[1] * dl / 2.0;
+      A_max = A_max * 1.0 + Js[0] * dl * Z0 / 2.0 - Ms[1] * dl / 2.0;
+      B_min = B_min * 1.0 + Js[1] * dl * Z0 / 2.0 - Ms[0] * dl / 2.0;
+      B_max = B_max * 1.0 + Js[1] * dl * Z0 / 2.0 + Ms[0] * dl / 2.0;
+    }
+  }
+  // new incident pulses: + cell pulls its min port from the - cell's max-port
+  // slot, the - cell pulls its max port from the + cell's min-port slot
+  const double inc_p1 = A_min - a1, inc_m1 = A_max - b1;
+  const double inc_p2 = B_min - a2, inc_m2 = B_max - b2;
+  R[pmax1 * P + im] = T(inc_p1);
+  R[pmin1 * P + ip] = T(inc_m1);
+  R[pmax2 * P + im] = T(inc_p2);
+  R[pmin2 * P + ip] = T(inc_m2);
+  if (io.y >= 0) {
+    const double dl = fd.dl, Z0 = kZ0;
+    double *fo = fd.face_field + (size_t)io.y * 12;
+    for (int side = 0; side < 2; side++) {
+      // side 1: positive = incident into + cell, negative = reflected from + cell
+      const double pa = side ? b1 : inc_p1, na = side ? inc_m1 : a1;
+      const double pb = side ? b2 : inc_p2, nb = side ? inc_m2 : a2;
+      double *fl = fo + side * 6;
+      if (dir == 1) {
+        fl[0] = 0.0; fl[1] = -(pa + na) / dl; fl[2] = -(pb + nb) / dl;
+        fl[3] = 0.0; fl[4] = (pb - nb) / (Z0 * dl); fl[5] = -(pa - na) / (Z0 * dl);
+      } else if (dir == 2) {
+        fl[0] = -(pa + na) / dl; fl[1] = 0.0; fl[2] = -(pb + nb) / dl;
+        fl[3] = -(pb - nb) / (Z0 * dl); fl[4] = 0.0; fl[5] = (pa - na) / (Z0 * dl);
+      } else {
+        fl[0] = -(pa + na) / dl; fl[1] = -(pb + nb) / dl; fl[2] = 0.0;
+        fl[3] = (pb - nb) / (Z0 * dl); fl[4] = -(pa - na) / (Z0 * dl); fl[5] = 0.0;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 DFT accumulation, frequency_output_surfaces.F90:343-410
+// ---------------------------------------------------------------------------
+struct DftDev {
+  int n_entries, n_dft;
+  const int4 *entry;        // (surface, out face index, face code 1..6, component 1..9)
+  const double2 *phasor;    // [n_timesteps][n_dft] exp(-j 2 pi f t)
+  const double *face_field; // [n_out_faces][2][6]
+  double2 *acc;             // [n_entries]
+};
+
+__global__ void tlm_dft_kernel(const DftDev d, const int *d_base, int rel_step) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.n_entries) return;
+  const int t = *d_base + rel_step;
+  const int4 en = d.entry[k];
+  const int face = en.z;
+  const int side = face <= 3 ? 0 : 1;
+  double normx = 0, normy = 0, normz = 0;
+  if (face == 1) normx = 1; else if (face == 4) normx = -1;
+  else if (face == 2) normy = 1; else if (face == 5) normy = -1;
+  else if (face == 3) normz = 1; else normz = -1;
+  const double *fl = d.face_field + (size_t)en.y * 12 + side * 6;
+  double value;
+  if (en.w <= 6) value = fl[en.w - 1];
+  else if (en.w == 7) value = (normy * fl[5] - normz * fl[4]);
+  else if (en.w == 8) value = (normz * fl[3] - normx * fl[5]);
+  else value = (normx * fl[4] - normy * fl[3]);
+  const double2 ph = d.phasor[(size_t)(t - 1) * d.n_dft + en.x];
+  double2 a = d.acc[k];
+  a.x = a.x + value * ph.x;
+  a.y = a.y + value * ph.y;
+  d.acc[k] = a;
+}
+
+__global__ void tlm_advance_base(int *d_base, int n) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *d_base += n;
+}
+
+// Incident pulses of the next step in the reference layout V(12,nx,ny,nz):
+// the same gather as the cell kernel, from the last written buffer.
+template <typename T>
+__global__ void tlm_gather_links(const MeshDev<T> m, int t_done, double *out) {
+  const long long n = (long long)m.nx * m.ny * m.nz;
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const int x = (int)(c % m.nx);
+  const int y = (int)((c / m.nx) % m.ny);
+  const int z = (int)(c / ((long long)m.nx * m.ny));
+  const T *R = (t_done & 1) ? m.links1 : m.links0;
+  const long long P = m.plane;
+  const long long i = (long long)(z + 1) * m.PxPy + (long long)(y + 1) * m.Px + x;
+  double *o = out + c * 12;
+  o[Vy_xmin] = double(R[Vy_xmax * P + i - 1]);
+  o[Vz_xmin] = double(R[Vz_xmax * P + i - 1]);
+  o[Vy_xmax] = double(R[Vy_xmin * P + i + 1]);
+  o[Vz_xmax] = double(R[Vz_xmin * P + i + 1]);
+  o[Vx_ymin] = double(R[Vx_ymax * P + i - m.Px]);
+  o[Vz_ymin] = double(R[Vz_ymax * P + i - m.Px]);
+  o[Vx_ymax] = double(R[Vx_ymin * P + i + m.Px]);
+  o[Vz_ymax] = double(R[Vz_ymin * P + i + m.Px]);
+  o[Vx_zmin] = double(R[Vx_zmax * P + i - m.PxPy]);
+  o[Vy_zmin] = double(R[Vy_zmax * P + i - m.PxPy]);
+  o[Vx_zmax] = double(R[Vx_zmin * P + i + m.PxPy]);
+  o[Vy_zmax] = double(R[Vy_zmin * P + i + m.PxPy]);
+}
+
+}  // namespace tlm

@@ -437,9 +437,13 @@ def _region_mask(spec: ProblemSpec, region) -> np.ndarray:
     if isinstance(region, Block):
         m[region.k0 - 1:region.k1, region.j0 - 1:region.j1, region.i0 - 1:region.i1] = True
     elif isinstance(region, Sphere):
-        z, y, x = np.meshgrid(np.arange(spec.nz) + 0.5, np.arange(spec.ny) + 0.5, np.arange(spec.nx) + 0.5,
-                              indexing="ij")
-        m = (x - region.cx) ** 2 + (y - region.cy) ** 2 + (z - region.cz) ** 2 <= region.r ** 2
+        lo = [max(0, int(math.floor(c - region.r)) - 1) for c in (region.cz, region.cy, region.cx)]
+        hi = [min(n, int(math.ceil(c + region.r)) + 1) for c, n in
+              ((region.cz, spec.nz), (region.cy, spec.ny), (region.cx, spec.nx))]
+        z, y, x = np.meshgrid(np.arange(lo[0], hi[0]) + 0.5, np.arange(lo[1], hi[1]) + 0.5,
+                              np.arange(lo[2], hi[2]) + 0.5, indexing="ij")
+        m[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = (
+            (x - region.cx) ** 2 + (y - region.cy) ** 2 + (z - region.cz) ** 2 <= region.r ** 2)
     else:
         raise TypeError(region)
     return m

@@ -1,0 +1,186 @@
+/*
+ * tlm_gpu.h -- C-ABI of the B200 (sm_100a) SCN-TLM time-stepping core.
+ *
+ * Drop-in boundary for GGI_TLM's time loop: the unchanged Fortran driver
+ * (SRC/GGI_TLM.F90) runs all of its setup (input parsing, .mesh reading,
+ * materials, PML, excitation and output set-up) and then, in place of
+ * `CALL run_TLM()` (SRC/GGI_TLM.F90:157), hands the module arrays below to
+ * this library and advances the mesh on the GPU.  The pattern follows the
+ * reference's only existing Fortran->C binding, MODULE ngspice_F90
+ * (SRC/NGSPICE_LINK/run_ngspice_TLM.F90:40-110): ISO_C_BINDING interfaces,
+ * scalars and arrays by reference, an integer return code.
+ *
+ * Conventions
+ *  - All pointers are caller-owned host memory.  The library copies what it
+ *    needs at set-time and never keeps a caller pointer.
+ *  - Indices inside the arrays are the reference's 1-based numbers
+ *    (special cell codes, material numbers, PML cell numbers, excitation and
+ *    output numbers), so the Fortran arrays pass through unchanged.
+ *  - Every entry point returns TLM_OK (0) or a negative TLM_E_* code;
+ *    tlm_gpu_last_error() returns the message of the last failure on the
+ *    calling thread.  The Fortran shim maps a non-zero code to
+ *    `write(*,*) msg; STOP 1`, the reference's own convention
+ *    (set_update_codes.F90:316, scatter.F90:561-567).
+ *  - One host thread per handle.  The library launches on its own CUDA
+ *    stream unless tlm_gpu_set_stream() gives it one.
+ *  - Features outside the GPU path (cables, Ngspice, surface/thin-layer
+ *    materials, diodes/switches, periodic or wrapping boundaries, mode
+ *    stirring, MPI np>1, PML cells inside dispersive materials) are rejected
+ *    with TLM_E_UNSUPPORTED at set-time.
+ */
+#ifndef TLM_GPU_H
+#define TLM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TLM_OK 0
+#define TLM_E_BADARG (-1)
+#define TLM_E_UNSUPPORTED (-2)
+#define TLM_E_OOM (-3)
+#define TLM_E_CUDA (-4)
+#define TLM_E_STATE (-5)
+#define TLM_E_TIMEOUT (-6)
+
+#define TLM_PRECISION_FP32 32 /* FP32 links + FP32 scatter; FP64 filters, sources, DFT */
+#define TLM_PRECISION_FP64 64 /* plain FP64 everywhere (parity path) */
+
+#define TLM_MAX_FILTER_ORDER 8
+
+/* Mesh and solver parameters: nx,ny,nz (TLM_general), dl, dt
+   (set_TLM_solver_parameters.F90:94), n_timesteps (:96) and the outer
+   boundary reflection coefficients R_xmin..R_zmax (outer_boundary.F90). */
+typedef struct tlm_gpu_mesh_desc {
+  int32_t nx, ny, nz;
+  int32_t n_timesteps;
+  double dl, dt;
+  double R[6];
+  int32_t precision; /* TLM_PRECISION_FP32 or TLM_PRECISION_FP64 */
+  int32_t device;    /* CUDA device ordinal */
+} tlm_gpu_mesh_desc;
+
+/* Allocate device state for one mesh; replaces allocate_mesh
+   (SRC/TLM_SOLVER/allocate_mesh.F90:106-134).  Links start at zero. */
+int tlm_gpu_create(const tlm_gpu_mesh_desc *desc, int64_t *handle);
+
+/* Cell classification: cell_centre_update_code(1:nx*ny*nz) in (cz,cy,cx)
+   order and the lookup tables cell_update_code_to_material_data(:,1),
+   cell_update_code_to_PML_data, cell_update_code_to_excitation_number,
+   cell_update_code_to_output_number (SRC/TLM_MODULES/Mesh_Modules.F90:121-150,
+   built by set_cell_update_codes, SRC/TLM_SOLVER/set_update_codes.F90:38-363).
+   Cable numbers must be zero. */
+int tlm_gpu_set_cells(int64_t handle, const int32_t *cell_centre_update_code, int32_t n_special,
+                      const int32_t *sp_material, const int32_t *sp_pml, const int32_t *sp_excitation,
+                      const int32_t *sp_output);
+
+/* Volume materials: volume_material_list(1:n) after
+   calculate_volume_material_filter_coefficients
+   (SRC/MATERIALS/TLM_volume_materials.F90:190-385): type (1 PEC, 2 PMC,
+   3 DISPERSIVE), filter existence flags, Zfilter_response orders, Ys_eps_f,
+   Zs_mu_f, Ge, Rm and the Zs_eps_Z / Zs_mu_Z coefficient rows a(0:order),
+   b(0:order) laid out with row stride `coeff_stride` (>= order+1). */
+int tlm_gpu_set_materials(int64_t handle, int32_t n_materials, const int32_t *type, const int32_t *eps_exists,
+                          const int32_t *mu_exists, const int32_t *eps_order, const int32_t *mu_order,
+                          const double *Ys_eps_f, const double *Zs_mu_f, const double *Ge, const double *Rm,
+                          const double *eps_a, const double *eps_b, const double *mu_a, const double *mu_b,
+                          int32_t coeff_stride);
+
+/* PML: PML_parameters(1:n_params) as 15 doubles per row in the order
+   ax,ay,az,exp_x,exp_y,exp_z,Csx,Csy,Csz,Csx2,Csy2,Csz2,Csy_sz,Csz_sx,Csx_sy
+   (SRC/TLM_MODULES/PML_module.F90:100-113, filled at
+   SRC/MATERIALS/TLM_PML_volume_materials.F90:325-351) and
+   PML_cell_data(1:n_pml_cells)%PML_parameter_array_pos. */
+int tlm_gpu_set_pml(int64_t handle, int32_t n_params, const double *params, int32_t n_pml_cells,
+                    const int32_t *pml_cell_param);
+
+/* Excitation: excitation_functions(1:n_fn)%value(1:n_steps) and
+   %value_face(1:n_steps) (SRC/EXCITATION/excitation.F90:155-559), and the
+   cell-centre point excitations (excitation cell number, field component
+   1..9, function number, source type 0 hard / 1 soft) of
+   SRC/EXCITATION/excitation_points.F90:231-335. */
+int tlm_gpu_set_excitation(int64_t handle, int32_t n_functions, int32_t n_steps, const double *value,
+                           const double *value_face, int32_t n_points, const int32_t *pt_cell,
+                           const int32_t *pt_comp, const int32_t *pt_fn, const int32_t *pt_type,
+                           int32_t n_exc_cells);
+
+/* Special faces, the non-zero entries of face_update_code compacted in
+   connect order (SRC/TLM_SOLVER/connect.F90:180-214): 1-based cell
+   (cx,cy,cz) on the + side of the face, normal axis 1..3, 1-based face
+   excitation number (or 0) and face output number (or 0).  Surface
+   materials are not part of the GPU path. */
+int tlm_gpu_set_faces(int64_t handle, int32_t n_faces, const int32_t *cx, const int32_t *cy, const int32_t *cz,
+                      const int32_t *dir, const int32_t *exc, const int32_t *out, int32_t n_exc_faces,
+                      int32_t n_out_faces);
+
+/* Huygens surface (SRC/EXCITATION/huygens_surface.F90:247-848): per patch
+   the face excitation number, normal (3 ints) and offset; the incident
+   field vectors Ei, Hi; offset_min, the wave speed c0/reduced_c and the
+   excitation function number. */
+int tlm_gpu_set_huygens(int64_t handle, int32_t n_patches, const int32_t *face_exc, const int32_t *norm,
+                        const double *offset, const double *Ei, const double *Hi, double offset_min, double c,
+                        int32_t function);
+
+/* Number of output cells; cell_output_field(1:n,1:6) is recorded every
+   step (SRC/TLM_SOLVER/scatter.F90:465-480, scatter_PML.F90 STAGE 12). */
+int tlm_gpu_set_outputs(int64_t handle, int32_t n_out_cells);
+
+/* Frequency-domain output surfaces (one entry per frequency, as
+   frequency_output_surface(:) in SRC/OUTPUT/frequency_output_surfaces.F90:
+   297-421): frequency, field component (1..6 E/H, 7..9 J=nxH), and a CSR
+   list (face_ptr[n_surfaces+1]) of output face numbers and face codes
+   (1..6 = face_xmin,ymin,zmin,xmax,ymax,zmax). */
+int tlm_gpu_set_dft(int64_t handle, int32_t n_surfaces, const double *frequency, const int32_t *component,
+                    const int32_t *face_ptr, const int32_t *face_out, const int32_t *face_code);
+
+/* Advance timesteps first_step..first_step+n_steps-1 (1-based, run_TLM
+   numbering, SRC/TLM_SOLVER/run_TLM.F90:191-295).  Steps must be
+   contiguous across calls.  Asynchronous on the library stream. */
+int tlm_gpu_run(int64_t handle, int32_t first_step, int32_t n_steps);
+
+/* Block until all work of the handle has finished. */
+int tlm_gpu_synchronize(int64_t handle);
+
+/* cell_output_field snapshots of steps first..first+n-1:
+   out[n][n_out_cells][6] doubles. */
+int tlm_gpu_fetch_cell_output(int64_t handle, int32_t first_step, int32_t n_steps, double *out);
+
+/* DFT accumulators (re, im) per surface face in set_dft order. */
+int tlm_gpu_fetch_dft(int64_t handle, double *out);
+
+/* Incident link voltages of the next step in the reference layout
+   V(1:12,1:nx,1:ny,1:nz) (port fastest), i.e. the content of the
+   reference's V array after outer_boundary. */
+int tlm_gpu_fetch_links(int64_t handle, double *out);
+
+/* Use a caller CUDA stream (cudaStream_t passed as void*; NULL = own). */
+int tlm_gpu_set_stream(int64_t handle, void *stream);
+
+/* Kernel timing mode: when enabled, tlm_gpu_run launches step by step
+   (no graph replay) and brackets every fused cell kernel with CUDA events on
+   the launch stream, so tlm_gpu_last_run_time can report the summed cell
+   kernel time of the run. */
+int tlm_gpu_set_timing(int64_t handle, int32_t enable);
+
+/* Device time of the last tlm_gpu_run (CUDA events on the launch stream):
+   whole run, and the summed duration of the fused cell kernel alone. */
+int tlm_gpu_last_run_time(int64_t handle, float *ms_total, float *ms_cell_kernel);
+
+/* Device memory held by the handle, bytes. */
+int tlm_gpu_memory_bytes(int64_t handle, int64_t *bytes);
+
+/* Number of kernel launches issued by the last tlm_gpu_run. */
+int tlm_gpu_last_run_launches(int64_t handle, int64_t *launches);
+
+int tlm_gpu_destroy(int64_t handle);
+
+/* Message of the last failure on this thread (NUL-terminated, truncated
+   to len-1 characters). */
+int tlm_gpu_last_error(char *buf, int32_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TLM_GPU_H */

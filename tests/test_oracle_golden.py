@@ -1,0 +1,61 @@
+"""The CPU oracle against the reference's own golden time series.
+
+The fixtures in tests/golden/ are the reference's TEST_DATA *.tout_ref files
+(extracted by tests/golden/make_golden.py), printed with 8 significant digits
+(format E16.7), so agreement is expected at ~1e-7 relative L2.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from ggi_tlm_b200 import cases
+from ggi_tlm_b200.problem import build_tables, probe_series
+
+import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL = 5e-7  # E16.7 print precision accumulated over the series
+
+
+def golden(name):
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
+    return d["time"], d["value"]
+
+
+@pytest.mark.parametrize("name", sorted(cases.KAT_CASES))
+def test_oracle_matches_reference_golden(name):
+    spec = cases.KAT_CASES[name]()
+    t = build_tables(spec)
+    o = O.Oracle(t)
+    ps = probe_series(t, o.run(t["n_timesteps"]))
+    tr, vr = golden(name)
+    v = np.where(np.abs(ps[0]) < 1e-30, 0.0, ps[0])  # output_points.F90:596-597
+    assert len(v) == len(vr) == t["n_timesteps"]
+    # output time stamps: time=(timestep-1)*dt
+    np.testing.assert_allclose((np.arange(len(v))) * t["dt"], tr, rtol=1e-6, atol=1e-18)
+    rel = np.linalg.norm(v - vr) / np.linalg.norm(vr)
+    assert rel < TOL, rel
+
+
+def test_material_changes_the_known_answer():
+    """Without the Debye slab the TEM_MATERIAL series is far from golden, so
+    the known answer pins the dispersive Z-filter path."""
+    spec = cases.kat_tem_material()
+    spec.materials, spec.material_regions = [], []
+    t = build_tables(spec)
+    ps = probe_series(t, O.Oracle(t).run(t["n_timesteps"]))
+    _, vr = golden("tem_material_Ey")
+    assert np.linalg.norm(ps[0] - vr) / np.linalg.norm(vr) > 0.05
+
+
+def test_oracle_step_split_is_identical():
+    """Running 2 x n steps equals one run of 2n steps (state carried exactly)."""
+    spec = cases.pml_spheres(n=20, pml=4, n_spheres=2, steps=60, n_probes=3, n_freq=3, dft_size=6, rmin=2, rmax=3)
+    t = build_tables(spec)
+    a = O.Oracle(t)
+    ca = np.concatenate([a.run(30), a.run(30)])
+    b = O.Oracle(t)
+    cb = b.run(60)
+    assert np.array_equal(ca, cb)
+    assert np.array_equal(a.dft(), b.dft())
