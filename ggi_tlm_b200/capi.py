@@ -33,7 +33,8 @@ EXPORTS = [
     "tlm_gpu_set_faces", "tlm_gpu_set_huygens", "tlm_gpu_set_outputs", "tlm_gpu_set_dft", "tlm_gpu_run",
     "tlm_gpu_synchronize", "tlm_gpu_fetch_cell_output", "tlm_gpu_fetch_dft", "tlm_gpu_fetch_links",
     "tlm_gpu_set_stream", "tlm_gpu_set_timing", "tlm_gpu_last_run_time", "tlm_gpu_memory_bytes",
-    "tlm_gpu_last_run_launches", "tlm_gpu_destroy", "tlm_gpu_last_error",
+    "tlm_gpu_last_run_launches", "tlm_gpu_destroy", "tlm_gpu_last_error", "tlm_gpu_set_variant",
+    "tlm_gpu_num_variants",
 ]
 
 
@@ -86,6 +87,8 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_memory_bytes": [i64, C.POINTER(i64)],
         "tlm_gpu_last_run_launches": [i64, C.POINTER(i64)],
         "tlm_gpu_destroy": [i64],
+        "tlm_gpu_set_variant": [i64, i32],
+        "tlm_gpu_num_variants": [C.POINTER(i32)],
         "tlm_gpu_last_error": [C.c_char_p, i32],
     }
     for name, args in sig.items():
@@ -94,6 +97,12 @@ def load_library(path: Optional[str] = None):
         f.restype = C.c_int
     _lib = lib
     return lib
+
+
+def num_variants() -> int:
+    n = C.c_int32(0)
+    _check(load_library().tlm_gpu_num_variants(C.byref(n)))
+    return n.value
 
 
 def _check(rc: int):
@@ -186,6 +195,9 @@ class GpuMesh:
 
     def set_timing(self, enable: bool):
         _check(_lib.tlm_gpu_set_timing(self.h, 1 if enable else 0))
+
+    def set_variant(self, variant: int):
+        _check(_lib.tlm_gpu_set_variant(self.h, variant))
 
     def set_stream(self, stream_ptr: int):
         _check(_lib.tlm_gpu_set_stream(self.h, C.c_void_p(stream_ptr)))

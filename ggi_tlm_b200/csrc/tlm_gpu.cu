@@ -96,7 +96,17 @@ struct Mesh {
       cell_out, faces, face_io, face_hs, value_face, face_field, dft_entry, dft_phasor, dft_acc, d_base;
   int n_filt = 0, filt_eo = 0, filt_mo = 0;
   int dft_entries = 0;
-  int n_sp_dev = 0;  // special cells on the device list
+  int n_sp_dev = 0;  // non-PML special cells on the device list
+  int n_pml_list = 0, n_pml_out = 0;
+  DevBuf pml_pos, pml_par16, pml_outmap;
+  // bulk-kernel variant: 0 = register-pipelined kernel, 1..kNumVariants-1 = TMA-staged configurations
+  int variant = 1;
+  int n_sms = 148;
+  std::vector<uint32_t> host_mask;  // per-32-element special-cell masks (for tile lists)
+  DevBuf tiles, d_err;
+  int tiles_tile = 0;  // TILE the current list was built for
+  int n_tiles = 0;
+  bool dry_launch = false;
 
   // graph of kGraphSteps steps
   static constexpr int kGraphSteps = 8;
@@ -251,6 +261,12 @@ int finalize(Mesh *m) {
   std::vector<int4> rec, pos;
   rec.reserve(m->n_special + 1);
   pos.reserve(m->n_special + 1);
+  std::vector<unsigned long long> pml_pos;
+  std::vector<uint16_t> pml_par;
+  std::vector<int2> pml_out;
+  pml_pos.reserve(m->n_pml_cells + 1);
+  pml_par.reserve(m->n_pml_cells + 1);
+  int mask_count = 0;
   // filter storage per dispersive cell (allocate_volume_material_filter_data)
   int eo = 0, mo = 0;
   for (auto &md : m->mats) {
@@ -274,15 +290,26 @@ int finalize(Mesh *m) {
         const int e = y * m->Px + x;
         const size_t sg = (size_t)z * segs_pp + (e >> 5);
         mask[sg] |= 1u << (e & 31);
+        mask_count++;
         int flags = 0;
         const int mat = m->sp_material[s];
         int4 r{0, -1, -1, -1};
         if (m->sp_pml[s]) {
-          flags |= tlm::SP_PML;
-          r.y = m->sp_pml[s] - 1;
-          const int par = m->pml_cell_param[r.y];
-          if (par < 1 || par > m->n_pml_params) return fail(TLM_E_BADARG, "PML cell %d: parameter %d out of range", r.y + 1, par);
-          r.z = par - 1;
+          // PML cells go to the packed PML list; PML cell numbers follow traversal order
+          const int pidx = m->sp_pml[s] - 1;
+          if (pidx != (int)pml_pos.size())
+            return fail(TLM_E_BADARG, "PML cell numbers must follow (cz,cy,cx) traversal order (cell %lld)", cell + 1);
+          const int par = m->pml_cell_param[pidx];
+          if (par < 1 || par > m->n_pml_params || par > 65536)
+            return fail(TLM_E_BADARG, "PML cell %d: parameter %d out of range", pidx + 1, par);
+          unsigned long long pk = (unsigned long long)x | ((unsigned long long)y << 21) | ((unsigned long long)z << 42);
+          if (m->sp_out[s]) {
+            pk |= 1ull << 63;
+            pml_out.push_back(int2{pidx, out_no++});
+          }
+          pml_pos.push_back(pk);
+          pml_par.push_back((uint16_t)(par - 1));
+          continue;
         } else {
           if (mat) {
             flags |= tlm::SP_MAT;
@@ -310,12 +337,25 @@ int finalize(Mesh *m) {
     base[i] = running;
     running += __builtin_popcount(mask[i]);
   }
-  if ((int)running != (int)rec.size()) return fail(TLM_E_BADARG, "special cell count mismatch");
+  if ((int)running != mask_count || (int)(rec.size() + pml_pos.size()) != mask_count)
+    return fail(TLM_E_BADARG, "special cell count mismatch");
+  if ((int)pml_pos.size() != m->n_pml_cells) return fail(TLM_E_BADARG, "PML cells: %zu flagged, %d declared", pml_pos.size(), m->n_pml_cells);
+  if (nx >= (1 << 21) || ny >= (1 << 21) || nz >= (1 << 21)) return fail(TLM_E_BADARG, "mesh too large for packed positions");
+  m->n_pml_list = (int)pml_pos.size();
+  m->n_pml_out = (int)pml_out.size();
+  if (pml_out.empty()) pml_out.resize(1);
+  {
+    int rc2;
+    if ((rc2 = upload(m, m->pml_pos, pml_pos)) || (rc2 = upload(m, m->pml_par16, pml_par)) ||
+        (rc2 = upload(m, m->pml_outmap, pml_out)))
+      return rc2;
+  }
   if (exc_no != m->n_exc_cells) return fail(TLM_E_BADARG, "excitation cells: %d flagged, %d declared", exc_no, m->n_exc_cells);
   if (out_no != m->n_out_cells) return fail(TLM_E_BADARG, "output cells: %d flagged, %d declared", out_no, m->n_out_cells);
   m->n_filt = n_filt;
   m->n_sp_dev = (int)rec.size();
   int rc;
+  m->host_mask = mask;
   if ((rc = upload(m, m->seg_mask, mask)) || (rc = upload(m, m->seg_base, base)) || (rc = upload(m, m->sp_rec, rec)) ||
       (rc = upload(m, m->sp_pos, pos)))
     return rc;
@@ -444,6 +484,13 @@ int finalize(Mesh *m) {
     CK(cudaMemset(m->dft_acc.p, 0, m->dft_acc.bytes));
   }
   if ((rc = dalloc(m, m->d_base, sizeof(int)))) return rc;
+  if ((rc = dalloc(m, m->d_err, sizeof(int)))) return rc;
+  CK(cudaMemset(m->d_err.p, 0, sizeof(int)));
+  {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&m->n_sms, cudaDevAttrMultiProcessorCount, dev));
+  }
   {
     int one = 1;
     CK(cudaMemcpy(m->d_base.p, &one, sizeof(int), cudaMemcpyHostToDevice));
@@ -458,20 +505,142 @@ int finalize(Mesh *m) {
   return TLM_OK;
 }
 
+// TMA-staged bulk kernel configurations (the autotuner's search space):
+// tile elements per work item and shared-memory ring depth.
+struct Variant {
+  int tile32, stages32, tile64, stages64;
+};
+constexpr Variant kVariants[] = {
+    {0, 0, 0, 0},        // 0: register-pipelined kernel (no TMA)
+    {1024, 2, 512, 2},   // 1
+    {512, 3, 256, 3},    // 2
+    {512, 4, 256, 4},    // 3
+    {1024, 3, 512, 3},   // 4
+    {256, 6, 128, 6},    // 5
+};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+// Tiles of TILE elements of each plane interior that hold at least one
+// free-space cell.
+int build_tiles(Mesh *m, int TILE) {
+  if (m->tiles_tile == TILE) return TLM_OK;
+  const int nx = m->desc.nx, ny = m->desc.ny, nz = m->desc.nz;
+  const int per_plane = ny * m->Px;
+  const int segs_pp = (per_plane + 31) / 32;
+  std::vector<int4> tl;
+  for (int z = 0; z < nz; z++) {
+    for (int e0 = 0; e0 < per_plane; e0 += TILE) {
+      const int len = std::min(TILE, per_plane - e0);
+      bool any = false;
+      for (int e = e0; e < e0 + len && !any; e += 32) {
+        const uint32_t mk = m->host_mask[(size_t)z * segs_pp + (e >> 5)];
+        for (int k = 0; k < 32 && e + k < e0 + len; k++) {
+          const int x = (e + k) % m->Px;
+          if (x < nx && !((mk >> k) & 1u)) {
+            any = true;
+            break;
+          }
+        }
+      }
+      if (any) tl.push_back(int4{z, e0, len, 0});
+    }
+  }
+  m->n_tiles = (int)tl.size();
+  if (tl.empty()) tl.resize(1);
+  int rc = upload(m, m->tiles, tl);
+  if (rc) return rc;
+  m->tiles_tile = TILE;
+  return TLM_OK;
+}
+
+template <typename T, int VEC, int TILE, int NSTAGE>
+int launch_tma(Mesh *m, const tlm::MeshDev<T> &md, int k) {
+  using Cfg = tlm::TmaCfg<T, VEC, TILE, NSTAGE>;
+  auto kern = tlm::tlm_bulk_tma_kernel<T, VEC, TILE, NSTAGE>;
+  // the shared-memory opt-in is per device; the occupancy query is cached per device too
+  static int per_sm_cache[64] = {0};
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  int per_sm = dev < 64 ? per_sm_cache[dev] : 0;
+  if (per_sm == 0) {
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Cfg::THREADS, Cfg::SMEM));
+    if (per_sm < 1) per_sm = 1;
+    if (dev < 64) per_sm_cache[dev] = per_sm;
+  }
+  const int grid = std::max(1, std::min(m->n_tiles, per_sm * m->n_sms));
+  tlm::TileList tl{(const int4 *)m->tiles.p, m->n_tiles, (int *)m->d_err.p};
+  if (m->dry_launch) return TLM_OK;  // configuration only (outside stream capture)
+  if (m->n_tiles) kern<<<grid, Cfg::THREADS, Cfg::SMEM, m->stream>>>(md, tl, k);
+  return TLM_OK;
+}
+
+// Everything a bulk launch needs that must not happen inside stream
+// capture (allocation of the tile list, kernel attributes).
+template <typename T, int VEC>
+int launch_bulk(Mesh *m, const tlm::MeshDev<T> &md, int k);
+
+int prepare_variant(Mesh *m) {
+  if (m->variant == 0) return TLM_OK;
+  const Variant &cf = kVariants[m->variant];
+  int rc = build_tiles(m, m->fp64 ? cf.tile64 : cf.tile32);
+  if (rc) return rc;
+  m->dry_launch = true;
+  rc = m->fp64 ? launch_bulk<double, 2>(m, mesh_dev<double>(m), 0) : launch_bulk<float, 4>(m, mesh_dev<float>(m), 0);
+  m->dry_launch = false;
+  return rc;
+}
+
+template <typename T, int VEC>
+int launch_bulk(Mesh *m, const tlm::MeshDev<T> &md, int k) {
+  const int v = m->variant;
+  if (v == 0) {
+    const int threads = 256;
+    dim3 grid((md.chunks_per_plane + threads - 1) / threads, m->desc.nz);
+    tlm::tlm_cell_kernel<T, VEC><<<grid, threads, 0, m->stream>>>(md, k);
+    return TLM_OK;
+  }
+  const Variant &cf = kVariants[v];
+  const int TILE = sizeof(T) == 4 ? cf.tile32 : cf.tile64;
+  if (m->tiles_tile != TILE) return fail(TLM_E_STATE, "tile list not prepared for variant %d", v);
+  if constexpr (sizeof(T) == 4) {
+    switch (v) {
+      case 1: return launch_tma<T, VEC, 1024, 2>(m, md, k);
+      case 2: return launch_tma<T, VEC, 512, 3>(m, md, k);
+      case 3: return launch_tma<T, VEC, 512, 4>(m, md, k);
+      case 4: return launch_tma<T, VEC, 1024, 3>(m, md, k);
+      default: return launch_tma<T, VEC, 256, 6>(m, md, k);
+    }
+  } else {
+    switch (v) {
+      case 1: return launch_tma<T, VEC, 512, 2>(m, md, k);
+      case 2: return launch_tma<T, VEC, 256, 3>(m, md, k);
+      case 3: return launch_tma<T, VEC, 256, 4>(m, md, k);
+      case 4: return launch_tma<T, VEC, 512, 3>(m, md, k);
+      default: return launch_tma<T, VEC, 128, 6>(m, md, k);
+    }
+  }
+}
+
 // Enqueue relative steps [0, n) of one step bundle (kernels only, the base
 // counter is advanced by the caller).
 template <typename T, int VEC>
 int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
   const tlm::MeshDev<T> md = mesh_dev<T>(m);
-  const int threads = 256;
-  dim3 grid((md.chunks_per_plane + threads - 1) / threads, m->desc.nz);
   const tlm::FaceDev fd = face_dev(m);
   const tlm::DftDev dd = dft_dev(m);
   for (int k = 0; k < n; k++) {
     if (kev) cudaEventRecord(kev[2 * k], m->stream);
-    tlm::tlm_cell_kernel<T, VEC><<<grid, threads, 0, m->stream>>>(md, k);
+    int rc = launch_bulk<T, VEC>(m, md, k);
+    if (rc) return rc;
     if (kev) cudaEventRecord(kev[2 * k + 1], m->stream);
     m->last_launches++;
+    if (m->n_pml_list) {
+      tlm::PmlList pl{(const unsigned long long *)m->pml_pos.p, (const uint16_t *)m->pml_par16.p,
+                      (const int2 *)m->pml_outmap.p, m->n_pml_list, m->n_pml_out};
+      tlm::tlm_pml_kernel<T><<<(m->n_pml_list + 127) / 128, 128, 0, m->stream>>>(md, pl, k);
+      m->last_launches++;
+    }
     if (m->n_sp_dev) {
       tlm::tlm_special_kernel<T><<<(m->n_sp_dev + 127) / 128, 128, 0, m->stream>>>(md, m->n_sp_dev, k);
       m->last_launches++;
@@ -495,6 +664,7 @@ int enqueue(Mesh *m, int n, cudaEvent_t *kev) {
 
 int run_steps(Mesh *m, int n) {
   int rc;
+  if ((rc = prepare_variant(m))) return rc;
   m->last_launches = 0;
   CK(cudaEventRecord(m->ev0, m->stream));
   if (m->timing) {
@@ -530,7 +700,8 @@ int run_steps(Mesh *m, int n) {
       m->last_launches = saved;
     }
     const long long per_graph =
-        (long long)G * (1 + (m->n_sp_dev ? 1 : 0) + (m->f_cx.empty() ? 0 : 1) + (m->dft_entries ? 1 : 0)) + 1;
+        (long long)G * (1 + (m->n_pml_list ? 1 : 0) + (m->n_sp_dev ? 1 : 0) + (m->f_cx.empty() ? 0 : 1) +
+                          (m->dft_entries ? 1 : 0)) + 1;
     for (int i = 0; i < full; i++) {
       CK(cudaGraphLaunch(m->graph, m->stream));
       m->last_launches += per_graph;
@@ -769,10 +940,37 @@ int tlm_gpu_run(int64_t h, int32_t first_step, int32_t n_steps) {
   return TLM_OK;
 }
 
+static int check_device_error(Mesh *m) {
+  if (!m->d_err.p) return TLM_OK;
+  int err = 0;
+  CK(cudaMemcpy(&err, m->d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err == tlm::kErrTimeout) return fail(TLM_E_TIMEOUT, "a bulk-copy wait in the cell kernel timed out");
+  if (err) return fail(TLM_E_CUDA, "device error word %d", err);
+  return TLM_OK;
+}
+
 int tlm_gpu_synchronize(int64_t h) {
   Mesh *m = get(h);
   if (!m) return fail(TLM_E_BADARG, "bad handle");
   if (m->stream) CK(cudaStreamSynchronize(m->stream));
+  return check_device_error(m);
+}
+
+int tlm_gpu_set_variant(int64_t h, int32_t variant) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (variant < 0 || variant >= kNumVariants) return fail(TLM_E_BADARG, "variant %d out of range", variant);
+  if (m->graph) {
+    cudaGraphExecDestroy(m->graph);
+    m->graph = nullptr;
+  }
+  m->variant = variant;
+  return TLM_OK;
+}
+
+int tlm_gpu_num_variants(int32_t *n) {
+  if (!n) return fail(TLM_E_BADARG, "null argument");
+  *n = kNumVariants;
   return TLM_OK;
 }
 

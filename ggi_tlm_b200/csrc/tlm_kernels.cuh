@@ -161,13 +161,15 @@ __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par,
   const T Csy_sz = P[12], Csz_sx = P[13], Csx_sy = P[14];
   T *S = m.pml_state;
   const int n = m.n_pml;
-  const T last_Ix = S[0 * n + pidx], last_Iy = S[1 * n + pidx], last_Iz = S[2 * n + pidx];
+  const T last_Ix = __ldcs(S + 0 * n + pidx), last_Iy = __ldcs(S + 1 * n + pidx), last_Iz = __ldcs(S + 2 * n + pidx);
   T last_Vi[12];
 #pragma unroll
-  for (int k = 0; k < 12; k++) last_Vi[k] = S[(3 + k) * n + pidx];
-  const T last_Vxt = S[15 * n + pidx], last_Vyt = S[16 * n + pidx], last_Vzt = S[17 * n + pidx];
-  const T last_Vxyt = S[18 * n + pidx], last_Vyxt = S[19 * n + pidx], last_Vzxt = S[20 * n + pidx];
-  const T last_Vxzt = S[21 * n + pidx], last_Vyzt = S[22 * n + pidx], last_Vzyt = S[23 * n + pidx];
+  for (int k = 0; k < 12; k++) last_Vi[k] = __ldcs(S + (size_t)(3 + k) * n + pidx);
+  const T last_Vxt = __ldcs(S + (size_t)15 * n + pidx), last_Vyt = __ldcs(S + (size_t)16 * n + pidx);
+  const T last_Vzt = __ldcs(S + (size_t)17 * n + pidx);
+  const T last_Vxyt = __ldcs(S + (size_t)18 * n + pidx), last_Vyxt = __ldcs(S + (size_t)19 * n + pidx);
+  const T last_Vzxt = __ldcs(S + (size_t)20 * n + pidx), last_Vxzt = __ldcs(S + (size_t)21 * n + pidx);
+  const T last_Vyzt = __ldcs(S + (size_t)22 * n + pidx), last_Vzyt = __ldcs(S + (size_t)23 * n + pidx);
 
   // STAGE 3: half-cell loss on incident pulses
   T V[12];
@@ -213,16 +215,16 @@ __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par,
   const T Vyz_se = ax * (Z0 * (-last_Ix + Csz2 * (Ix + last_Ix)) + Csy_sz * last_Vyzt);
   const T Vzy_se = ax * (Z0 * (-last_Ix + Csy2 * (Ix + last_Ix)) + Csy_sz * last_Vzyt);
   // STAGE 8 + 9: save state
-  S[0 * n + pidx] = Ix; S[1 * n + pidx] = Iy; S[2 * n + pidx] = Iz;
+  __stcs(S + 0 * n + pidx, Ix); __stcs(S + 1 * n + pidx, Iy); __stcs(S + 2 * n + pidx, Iz);
 #pragma unroll
-  for (int k = 0; k < 12; k++) S[(3 + k) * n + pidx] = V[k];
-  S[15 * n + pidx] = Vxt; S[16 * n + pidx] = Vyt; S[17 * n + pidx] = Vzt;
-  S[18 * n + pidx] = az * Iz * Z0 + Vxy_se;
-  S[19 * n + pidx] = az * Iz * Z0 + Vyx_se;
-  S[20 * n + pidx] = ay * Iy * Z0 + Vzx_se;
-  S[21 * n + pidx] = ay * Iy * Z0 + Vxz_se;
-  S[22 * n + pidx] = ax * Ix * Z0 + Vyz_se;
-  S[23 * n + pidx] = ax * Ix * Z0 + Vzy_se;
+  for (int k = 0; k < 12; k++) __stcs(S + (size_t)(3 + k) * n + pidx, V[k]);
+  __stcs(S + (size_t)15 * n + pidx, Vxt); __stcs(S + (size_t)16 * n + pidx, Vyt); __stcs(S + (size_t)17 * n + pidx, Vzt);
+  __stcs(S + (size_t)18 * n + pidx, az * Iz * Z0 + Vxy_se);
+  __stcs(S + (size_t)19 * n + pidx, az * Iz * Z0 + Vyx_se);
+  __stcs(S + (size_t)20 * n + pidx, ay * Iy * Z0 + Vzx_se);
+  __stcs(S + (size_t)21 * n + pidx, ay * Iy * Z0 + Vxz_se);
+  __stcs(S + (size_t)22 * n + pidx, ax * Ix * Z0 + Vyz_se);
+  __stcs(S + (size_t)23 * n + pidx, ax * Ix * Z0 + Vzy_se);
   // STAGE 10
   const T Vynx_P = Vx_sh - Vyx_se, Vypx_P = Vx_sh + Vyx_se;
   const T Vznx_P = Vx_sh + Vzx_se, Vzpx_P = Vx_sh - Vzx_se;
@@ -547,6 +549,259 @@ __global__ void __launch_bounds__(256) tlm_cell_kernel(const MeshDev<T> m, int r
 #undef res
 
 // ---------------------------------------------------------------------------
+// TMA-staged persistent bulk kernel.
+//
+// Work item = a tile of up to TILE consecutive elements of one z-plane's
+// interior (rows y=0..ny-1).  One elected thread per block issues 12
+// cp.async.bulk copies (one per source plane segment, shifted by the pull
+// offset of that port) into an NSTAGE-deep shared-memory ring completed on an
+// mbarrier; the block computes tile i from its stage while the copies of
+// tiles i+1.. are in flight.  Results go straight to global memory with
+// streaming vector stores.  All mbarrier waits are bounded by %globaltimer;
+// on expiry the block records an error code and returns.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// Wait for phase `parity` of an mbarrier, giving up after ~2 s.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (unsigned it = 1;; it++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 255u) == 0u && global_ns() - t0 > 2000000000ull) return false;
+  }
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+constexpr int kErrTimeout = 1;
+
+struct TileList {
+  const int4 *tile;  // (z, e0, len, 0)
+  int n;
+  int *err;          // device error word (0 = ok)
+};
+
+template <typename T, int VEC, int TILE, int NSTAGE>
+struct TmaCfg {
+  static constexpr int H = 16 / (int)sizeof(T);       // halo elements (16 B) on each side of x-planes
+  static constexpr int SEG = TILE + 2 * H;             // elements per plane buffer
+  static constexpr int THREADS = TILE / VEC;
+  static constexpr size_t STAGE_BYTES = (size_t)12 * SEG * sizeof(T);
+  static constexpr size_t SMEM = NSTAGE * STAGE_BYTES + 64;
+};
+
+template <typename T, int VEC, int TILE, int NSTAGE>
+__device__ __forceinline__ void tma_issue(const MeshDev<T> &m, const T *in, const int4 tile, T *stage, uint64_t *bar) {
+  using C = TmaCfg<T, VEC, TILE, NSTAGE>;
+  const long long P = m.plane;
+  const long long idx0 = (long long)(tile.x + 1) * m.PxPy + (long long)m.Px + tile.y;
+  const int len = tile.z;
+  const uint32_t xb = (uint32_t)((len + 2 * C::H) * sizeof(T));
+  const uint32_t yb = (uint32_t)(len * sizeof(T));
+  mbar_expect_tx(bar, 4 * xb + 8 * yb);
+  // buffer b holds the source plane of incident port b (plane of the opposite port)
+  const long long dy = m.Px, dz = m.PxPy;
+  // x-planes, with a 16-byte halo on both sides
+  bulk_g2s(stage + Vy_xmin * C::SEG, in + Vy_xmax * P + idx0 - C::H, xb, bar);
+  bulk_g2s(stage + Vz_xmin * C::SEG, in + Vz_xmax * P + idx0 - C::H, xb, bar);
+  bulk_g2s(stage + Vy_xmax * C::SEG, in + Vy_xmin * P + idx0 - C::H, xb, bar);
+  bulk_g2s(stage + Vz_xmax * C::SEG, in + Vz_xmin * P + idx0 - C::H, xb, bar);
+  // y and z planes: the shifted rows/planes, stored at offset H
+  bulk_g2s(stage + Vx_ymin * C::SEG + C::H, in + Vx_ymax * P + idx0 - dy, yb, bar);
+  bulk_g2s(stage + Vz_ymin * C::SEG + C::H, in + Vz_ymax * P + idx0 - dy, yb, bar);
+  bulk_g2s(stage + Vx_ymax * C::SEG + C::H, in + Vx_ymin * P + idx0 + dy, yb, bar);
+  bulk_g2s(stage + Vz_ymax * C::SEG + C::H, in + Vz_ymin * P + idx0 + dy, yb, bar);
+  bulk_g2s(stage + Vx_zmin * C::SEG + C::H, in + Vx_zmax * P + idx0 - dz, yb, bar);
+  bulk_g2s(stage + Vy_zmin * C::SEG + C::H, in + Vy_zmax * P + idx0 - dz, yb, bar);
+  bulk_g2s(stage + Vx_zmax * C::SEG + C::H, in + Vx_zmin * P + idx0 + dz, yb, bar);
+  bulk_g2s(stage + Vy_zmax * C::SEG + C::H, in + Vy_zmin * P + idx0 + dz, yb, bar);
+}
+
+template <typename T, int VEC>
+__device__ __forceinline__ void lds_vec(const T *p, T (&v)[VEC]) {
+  using V = typename VecT<T, VEC>::type;
+  const V q = *reinterpret_cast<const V *>(p);
+  if constexpr (VEC == 4) { v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w; }
+  else { v[0] = q.x; v[1] = q.y; }
+}
+
+template <typename T, int VEC, int TILE, int NSTAGE>
+__global__ void __launch_bounds__(TILE / VEC) tlm_bulk_tma_kernel(const MeshDev<T> m, const TileList tl, int rel_step) {
+  using C = TmaCfg<T, VEC, TILE, NSTAGE>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T *stages = reinterpret_cast<T *>(smem_raw);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + NSTAGE * C::STAGE_BYTES);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < NSTAGE; s++) mbar_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const int t = *m.d_base + rel_step;
+  const T *__restrict__ in = (t & 1) ? m.links0 : m.links1;
+  T *__restrict__ out = (t & 1) ? m.links1 : m.links0;
+  const long long P = m.plane;
+  const long long dy = m.Px, dz = m.PxPy;
+  const int first = blockIdx.x, stride = gridDim.x;
+  int n_mine = (tl.n - first + stride - 1) / stride;
+  if (n_mine < 0) n_mine = 0;
+  // prologue: fill the ring
+  if (tid == 0)
+    for (int s = 0; s < NSTAGE && s < n_mine; s++)
+      tma_issue<T, VEC, TILE, NSTAGE>(m, in, tl.tile[first + s * stride], stages + s * 12 * C::SEG, &bars[s]);
+  for (int i = 0; i < n_mine; i++) {
+    const int s = i % NSTAGE;
+    const uint32_t parity = (uint32_t)((i / NSTAGE) & 1);
+    const int4 tile = tl.tile[first + i * stride];
+    if (!mbar_wait_bounded(&bars[s], parity)) {
+      if (tid == 0) atomicExch(tl.err, kErrTimeout);
+      return;
+    }
+    const T *st = stages + s * 12 * C::SEG;
+    const int z = tile.x;
+    const int el = tid * VEC;  // element offset inside the tile
+    const int e = tile.y + el;
+    const bool valid = el < tile.z;
+    if (valid) {
+      const int y = e / m.Px;
+      const int x0 = e - y * m.Px;
+      const int nvalid = min(VEC, m.nx - x0);
+      const uint32_t mask = __ldg(m.seg_mask + (size_t)z * m.segs_per_plane + (e >> 5));
+      const uint32_t mine = (mask >> (e & 31)) & ((1u << VEC) - 1u);
+      const uint32_t need = (nvalid > 0) ? (((1u << nvalid) - 1u) & ~mine) : 0u;
+      if (need) {
+        T inc[12][VEC];
+        const int o = C::H + el;
+        lds_vec<T, VEC>(st + Vx_ymin * C::SEG + o, inc[Vx_ymin]);
+        lds_vec<T, VEC>(st + Vz_ymin * C::SEG + o, inc[Vz_ymin]);
+        lds_vec<T, VEC>(st + Vx_ymax * C::SEG + o, inc[Vx_ymax]);
+        lds_vec<T, VEC>(st + Vz_ymax * C::SEG + o, inc[Vz_ymax]);
+        lds_vec<T, VEC>(st + Vx_zmin * C::SEG + o, inc[Vx_zmin]);
+        lds_vec<T, VEC>(st + Vy_zmin * C::SEG + o, inc[Vy_zmin]);
+        lds_vec<T, VEC>(st + Vx_zmax * C::SEG + o, inc[Vx_zmax]);
+        lds_vec<T, VEC>(st + Vy_zmax * C::SEG + o, inc[Vy_zmax]);
+        {
+          T a[VEC], b[VEC], c[VEC], d[VEC];
+          lds_vec<T, VEC>(st + Vy_xmin * C::SEG + o, a);  // source plane Vy_xmax at x
+          lds_vec<T, VEC>(st + Vz_xmin * C::SEG + o, b);
+          lds_vec<T, VEC>(st + Vy_xmax * C::SEG + o, c);  // source plane Vy_xmin at x
+          lds_vec<T, VEC>(st + Vz_xmax * C::SEG + o, d);
+          inc[Vy_xmin][0] = st[Vy_xmin * C::SEG + o - 1];
+          inc[Vz_xmin][0] = st[Vz_xmin * C::SEG + o - 1];
+#pragma unroll
+          for (int j = 1; j < VEC; j++) { inc[Vy_xmin][j] = a[j - 1]; inc[Vz_xmin][j] = b[j - 1]; }
+#pragma unroll
+          for (int j = 0; j < VEC - 1; j++) { inc[Vy_xmax][j] = c[j + 1]; inc[Vz_xmax][j] = d[j + 1]; }
+          inc[Vy_xmax][VEC - 1] = st[Vy_xmax * C::SEG + o + VEC];
+          inc[Vz_xmax][VEC - 1] = st[Vz_xmax * C::SEG + o + VEC];
+        }
+#pragma unroll
+        for (int j = 0; j < VEC; j++) {
+          T ci[12], co[12];
+#pragma unroll
+          for (int p = 0; p < 12; p++) ci[p] = inc[p][j];
+          free_space_cell<T>(ci, co);
+#pragma unroll
+          for (int p = 0; p < 12; p++) inc[p][j] = co[p];
+        }
+        const long long idx = (long long)(z + 1) * m.PxPy + (long long)m.Px + e;
+        if (need == (1u << VEC) - 1u) {
+#pragma unroll
+          for (int p = 0; p < 12; p++) store_vec<T, VEC>(out + p * P + idx, inc[p]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < VEC; j++)
+            if (need & (1u << j)) {
+#pragma unroll
+              for (int p = 0; p < 12; p++) out[p * P + idx + j] = inc[p][j];
+            }
+        }
+        if (x0 == 0 && (need & 1u)) {
+          out[Vy_xmax * P + idx - 1] = m.R[0] * inc[Vy_xmin][0];
+          out[Vz_xmax * P + idx - 1] = m.R[0] * inc[Vz_xmin][0];
+        }
+        if (x0 + nvalid == m.nx) {
+          const int j = nvalid - 1;
+          T vy = inc[Vy_xmax][0], vz = inc[Vz_xmax][0];
+#pragma unroll
+          for (int k = 1; k < VEC; k++)
+            if (j == k) { vy = inc[Vy_xmax][k]; vz = inc[Vz_xmax][k]; }
+          if (need & (1u << j)) {
+            out[Vy_xmin * P + idx + j + 1] = m.R[1] * vy;
+            out[Vz_xmin * P + idx + j + 1] = m.R[1] * vz;
+          }
+        }
+        if (y == 0) {
+#pragma unroll
+          for (int j = 0; j < VEC; j++)
+            if (need & (1u << j)) {
+              out[Vx_ymax * P + idx - dy + j] = m.R[2] * inc[Vx_ymin][j];
+              out[Vz_ymax * P + idx - dy + j] = m.R[2] * inc[Vz_ymin][j];
+            }
+        }
+        if (y == m.ny - 1) {
+#pragma unroll
+          for (int j = 0; j < VEC; j++)
+            if (need & (1u << j)) {
+              out[Vx_ymin * P + idx + dy + j] = m.R[3] * inc[Vx_ymax][j];
+              out[Vz_ymin * P + idx + dy + j] = m.R[3] * inc[Vz_ymax][j];
+            }
+        }
+        if (z == 0) {
+#pragma unroll
+          for (int j = 0; j < VEC; j++)
+            if (need & (1u << j)) {
+              out[Vx_zmax * P + idx - dz + j] = m.R[4] * inc[Vx_zmin][j];
+              out[Vy_zmax * P + idx - dz + j] = m.R[4] * inc[Vy_zmin][j];
+            }
+        }
+        if (z == m.nz - 1) {
+#pragma unroll
+          for (int j = 0; j < VEC; j++)
+            if (need & (1u << j)) {
+              out[Vx_zmin * P + idx + dz + j] = m.R[5] * inc[Vx_zmax][j];
+              out[Vy_zmin * P + idx + dz + j] = m.R[5] * inc[Vy_zmax][j];
+            }
+        }
+      }
+    }
+    __syncthreads();  // every thread is done reading stage s
+    if (tid == 0 && i + NSTAGE < n_mine) {
+      fence_proxy_async();
+      tma_issue<T, VEC, TILE, NSTAGE>(m, in, tl.tile[first + (i + NSTAGE) * stride], stages + s * 12 * C::SEG,
+                                      &bars[s]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Special-cell kernel: one thread per special cell (traversal order, so PML
 // state and links coalesce along x): gather, PML / material / excitation /
 // output scatter, reflected pulses + ghost slots.
@@ -605,6 +860,79 @@ __global__ void __launch_bounds__(128) tlm_special_kernel(const MeshDev<T> m, in
     out[Vy_zmax * P + idx - dz] = m.R[4] * co[Vy_zmin];
   }
   if (pos.z == m.nz - 1) {
+    out[Vx_zmin * P + idx + dz] = m.R[5] * co[Vx_zmax];
+    out[Vy_zmin * P + idx + dz] = m.R[5] * co[Vy_zmax];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PML kernel: one thread per PML cell, in the reference's PML cell numbering
+// (traversal order), so the thread index is the PML state index.  Per cell
+// it reads an 8-byte packed position (x | y<<21 | z<<42 | output<<63) and a
+// 2-byte PML parameter index.
+// ---------------------------------------------------------------------------
+struct PmlList {
+  const unsigned long long *pos;
+  const uint16_t *par;
+  const int2 *out_map;  // (pml index, output number) of PML output cells
+  int n, n_out_map;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(128) tlm_pml_kernel(const MeshDev<T> m, const PmlList pl, int rel_step) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= pl.n) return;
+  const int t = *m.d_base + rel_step;
+  const T *__restrict__ in = (t & 1) ? m.links0 : m.links1;
+  T *__restrict__ out = (t & 1) ? m.links1 : m.links0;
+  const long long P = m.plane;
+  const unsigned long long pk = __ldcs(pl.pos + s);
+  const int x = (int)(pk & 0x1fffffull), y = (int)((pk >> 21) & 0x1fffffull), z = (int)((pk >> 42) & 0x1fffffull);
+  const int par = __ldcs(pl.par + s);
+  int out_no = -1;
+  if (pk >> 63)
+    for (int k = 0; k < pl.n_out_map; k++)
+      if (pl.out_map[k].x == s) out_no = pl.out_map[k].y;
+  const long long idx = (long long)(z + 1) * m.PxPy + (long long)(y + 1) * m.Px + x;
+  const long long dy = m.Px, dz = m.PxPy;
+  T ci[12], co[12];
+  ci[Vy_xmin] = __ldcs(in + Vy_xmax * P + idx - 1);
+  ci[Vz_xmin] = __ldcs(in + Vz_xmax * P + idx - 1);
+  ci[Vy_xmax] = __ldcs(in + Vy_xmin * P + idx + 1);
+  ci[Vz_xmax] = __ldcs(in + Vz_xmin * P + idx + 1);
+  ci[Vx_ymin] = __ldcs(in + Vx_ymax * P + idx - dy);
+  ci[Vz_ymin] = __ldcs(in + Vz_ymax * P + idx - dy);
+  ci[Vx_ymax] = __ldcs(in + Vx_ymin * P + idx + dy);
+  ci[Vz_ymax] = __ldcs(in + Vz_ymin * P + idx + dy);
+  ci[Vx_zmin] = __ldcs(in + Vx_zmax * P + idx - dz);
+  ci[Vy_zmin] = __ldcs(in + Vy_zmax * P + idx - dz);
+  ci[Vx_zmax] = __ldcs(in + Vx_zmin * P + idx + dz);
+  ci[Vy_zmax] = __ldcs(in + Vy_zmin * P + idx + dz);
+  double *row = (out_no >= 0) ? m.cell_out + ((size_t)(t - 1) * m.n_out + out_no) * 6 : nullptr;
+  pml_cell<T>(m, s, par, out_no, ci, co, row);
+#pragma unroll
+  for (int p = 0; p < 12; p++) __stcs(out + p * P + idx, co[p]);
+  if (x == 0) {
+    out[Vy_xmax * P + idx - 1] = m.R[0] * co[Vy_xmin];
+    out[Vz_xmax * P + idx - 1] = m.R[0] * co[Vz_xmin];
+  }
+  if (x == m.nx - 1) {
+    out[Vy_xmin * P + idx + 1] = m.R[1] * co[Vy_xmax];
+    out[Vz_xmin * P + idx + 1] = m.R[1] * co[Vz_xmax];
+  }
+  if (y == 0) {
+    out[Vx_ymax * P + idx - dy] = m.R[2] * co[Vx_ymin];
+    out[Vz_ymax * P + idx - dy] = m.R[2] * co[Vz_ymin];
+  }
+  if (y == m.ny - 1) {
+    out[Vx_ymin * P + idx + dy] = m.R[3] * co[Vx_ymax];
+    out[Vz_ymin * P + idx + dy] = m.R[3] * co[Vz_ymax];
+  }
+  if (z == 0) {
+    out[Vx_zmax * P + idx - dz] = m.R[4] * co[Vx_zmin];
+    out[Vy_zmax * P + idx - dz] = m.R[4] * co[Vy_zmin];
+  }
+  if (z == m.nz - 1) {
     out[Vx_zmin * P + idx + dz] = m.R[5] * co[Vx_zmax];
     out[Vy_zmin * P + idx + dz] = m.R[5] * co[Vy_zmax];
   }

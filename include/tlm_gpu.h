@@ -164,6 +164,13 @@ int tlm_gpu_set_stream(int64_t handle, void *stream);
    kernel time of the run. */
 int tlm_gpu_set_timing(int64_t handle, int32_t enable);
 
+/* Tuning: select the configuration of the bulk (free-space) cell kernel,
+   0 = register-pipelined kernel, 1..n-1 = TMA-staged persistent kernel
+   with different tile sizes and shared-memory ring depths.  Numerics are
+   identical for every variant; the autotuner picks the fastest. */
+int tlm_gpu_set_variant(int64_t handle, int32_t variant);
+int tlm_gpu_num_variants(int32_t *n_variants);
+
 /* Device time of the last tlm_gpu_run (CUDA events on the launch stream):
    whole run, and the summed duration of the fused cell kernel alone. */
 int tlm_gpu_last_run_time(int64_t handle, float *ms_total, float *ms_cell_kernel);
