@@ -34,7 +34,7 @@ EXPORTS = [
     "tlm_gpu_synchronize", "tlm_gpu_fetch_cell_output", "tlm_gpu_fetch_dft", "tlm_gpu_fetch_links",
     "tlm_gpu_set_stream", "tlm_gpu_set_timing", "tlm_gpu_last_run_time", "tlm_gpu_memory_bytes",
     "tlm_gpu_last_run_launches", "tlm_gpu_destroy", "tlm_gpu_last_error", "tlm_gpu_set_variant",
-    "tlm_gpu_num_variants",
+    "tlm_gpu_num_variants", "tlm_gpu_fetch_links_noalloc",
 ]
 
 
@@ -81,6 +81,7 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_fetch_cell_output": [i64, i32, i32, _f64p],
         "tlm_gpu_fetch_dft": [i64, _f64p],
         "tlm_gpu_fetch_links": [i64, _f64p],
+        "tlm_gpu_fetch_links_noalloc": [i64, _f64p],
         "tlm_gpu_set_stream": [i64, C.c_void_p],
         "tlm_gpu_set_timing": [i64, i32],
         "tlm_gpu_last_run_time": [i64, C.POINTER(C.c_float), C.POINTER(C.c_float)],

@@ -1052,6 +1052,65 @@ int tlm_gpu_fetch_links(int64_t h, double *out) {
   return TLM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free link read-back.
+//
+// The gather of tlm_gpu_fetch_links needs a device buffer of nx*ny*nz*12
+// doubles and gets it with cudaMalloc.  tlm_gpu_fetch_links_noalloc does the
+// same gather into a fixed scratch array that lives in the library image
+// (file-scope __device__ storage, kNoAllocScratchDoubles doubles = 8 MiB on
+// every device that loads the library, held until the process exits), so it
+// makes no cudaMalloc/cudaFree call.  In host code the array's name is only a
+// host-side stand-in; the device address is looked up once per device with
+// cudaGetSymbolAddress, by the first call made on that device.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kNoAllocScratchDoubles = (size_t)1 << 20;  // 8 MiB
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[64] = {nullptr};
+}  // namespace
+
+int tlm_gpu_fetch_links_noalloc(int64_t h, double *out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (!out) return fail(TLM_E_BADARG, "null output");
+  if (!m->finalized)
+    return fail(TLM_E_STATE, "the mesh has no device state yet: call tlm_gpu_run at least once first");
+  const long long n = (long long)m->desc.nx * m->desc.ny * m->desc.nz;
+  if ((size_t)n * 12 > kNoAllocScratchDoubles)
+    return fail(TLM_E_BADARG, "mesh of %lld cells exceeds the allocation-free read-back limit of %zu cells", n,
+                kNoAllocScratchDoubles / 12);
+  const int dev = m->desc.device;
+  if (dev < 0 || dev >= 64) return fail(TLM_E_BADARG, "device %d out of range", dev);
+  CK(cudaSetDevice(dev));
+  double *scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void *p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p)
+        return fail(TLM_E_CUDA, "cudaGetSymbolAddress(scratch) failed on device %d: %s", dev, cudaGetErrorString(e));
+      g_noalloc_ptr[dev] = (double *)p;
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  const int t_done = m->next_step - 1;
+  const int threads = 256;
+  const unsigned blocks = (unsigned)((n + threads - 1) / threads);
+  // every scratch element the caller receives is written by this gather, so
+  // nothing has to be cleared first
+  if (m->fp64)
+    tlm::tlm_gather_links<double><<<blocks, threads, 0, m->stream>>>(mesh_dev<double>(m), t_done, scratch);
+  else
+    tlm::tlm_gather_links<float><<<blocks, threads, 0, m->stream>>>(mesh_dev<float>(m), t_done, scratch);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, scratch, (size_t)n * 12 * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  CK(cudaStreamSynchronize(m->stream));
+  return TLM_OK;
+}
+
 int tlm_gpu_destroy(int64_t h) {
   std::unique_ptr<Mesh> m;
   {

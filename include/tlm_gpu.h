@@ -155,6 +155,22 @@ int tlm_gpu_fetch_dft(int64_t handle, double *out);
    reference's V array after outer_boundary. */
 int tlm_gpu_fetch_links(int64_t handle, double *out);
 
+/* Allocation-free variant of tlm_gpu_fetch_links.  It has no counterpart in
+   the reference.  It exists for callers that cannot call cudaMalloc: code
+   that must not grow device memory it does not own (a host framework with a
+   fixed device budget or pool), or that must not trigger the implicit device
+   synchronisation of cudaMalloc/cudaFree while other GPU work is in flight.
+   The gather runs into a fixed scratch array inside the library (8 MiB per
+   device that loads the library, kept until the process exits), so the mesh
+   may have at most 87381 cells (nx*ny*nz*12 <= 2^20 doubles); larger meshes
+   are rejected with TLM_E_BADARG.  The mesh must already have device state
+   (at least one tlm_gpu_run).  The first call on a device looks up the
+   scratch address (cudaGetSymbolAddress) and should come before any stream
+   capture.  All calls share the one scratch array, which keeps the last
+   call's contents: calls that overlap on the GPU (other host threads, other
+   handles) race on it. */
+int tlm_gpu_fetch_links_noalloc(int64_t handle, double *out);
+
 /* Use a caller CUDA stream (cudaStream_t passed as void*; NULL = own). */
 int tlm_gpu_set_stream(int64_t handle, void *stream);
 
