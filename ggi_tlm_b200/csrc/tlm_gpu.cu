@@ -178,10 +178,10 @@ tlm::MeshDev<T> mesh_dev(Mesh *m) {
   d.seg_base = (const uint32_t *)m->seg_base.p;
   d.sp_rec = (const int4 *)m->sp_rec.p;
   d.sp_pos = (const int4 *)m->sp_pos.p;
-  d.pml_state = (T *)m->pml_state.p;
+  d.pml_state = (typename tlm::PmlTypes<T>::state *)m->pml_state.p;
   d.n_pml = m->n_pml_cells;
-  d.pml_par = (const T *)m->pml_par.p;
-  d.pml_ixt = (T *)m->pml_ixt.p;
+  d.pml_par = (const double *)m->pml_par.p;
+  d.pml_ixt = (typename tlm::PmlTypes<T>::state *)m->pml_ixt.p;
   d.filt = (double *)m->filt.p;
   d.n_filt = m->n_filt;
   d.filt_eo = m->filt_eo;
@@ -364,22 +364,16 @@ int finalize(Mesh *m) {
   if ((rc = dalloc(m, m->links, 2 * 12 * (size_t)m->plane * esz))) return rc;
   CK(cudaMemset(m->links.p, 0, m->links.bytes));
   // ---- PML
-  if ((rc = dalloc(m, m->pml_state, (size_t)tlm::kPmlState * std::max(m->n_pml_cells, 1) * esz))) return rc;
+  const size_t pesz = m->fp64 ? sizeof(tlm::PmlTypes<double>::state) : sizeof(tlm::PmlTypes<float>::state);
+  if ((rc = dalloc(m, m->pml_state, (size_t)tlm::kPmlState * std::max(m->n_pml_cells, 1) * pesz))) return rc;
   CK(cudaMemset(m->pml_state.p, 0, m->pml_state.bytes));
   {
-    if (m->fp64) {
-      std::vector<double> par((size_t)std::max(m->n_pml_params, 1) * 16, 0.0);
-      for (int i = 0; i < m->n_pml_params; i++)
-        for (int k = 0; k < 15; k++) par[(size_t)i * 16 + k] = m->pml_params[(size_t)i * 15 + k];
-      if ((rc = upload(m, m->pml_par, par))) return rc;
-    } else {
-      std::vector<float> par((size_t)std::max(m->n_pml_params, 1) * 16, 0.f);
-      for (int i = 0; i < m->n_pml_params; i++)
-        for (int k = 0; k < 15; k++) par[(size_t)i * 16 + k] = (float)m->pml_params[(size_t)i * 15 + k];
-      if ((rc = upload(m, m->pml_par, par))) return rc;
-    }
+    std::vector<double> par((size_t)std::max(m->n_pml_params, 1) * 16, 0.0);
+    for (int i = 0; i < m->n_pml_params; i++)
+      for (int k = 0; k < 15; k++) par[(size_t)i * 16 + k] = m->pml_params[(size_t)i * 15 + k];
+    if ((rc = upload(m, m->pml_par, par))) return rc;
   }
-  if ((rc = dalloc(m, m->pml_ixt, (size_t)std::max(m->n_out_cells, 1) * 3 * esz))) return rc;
+  if ((rc = dalloc(m, m->pml_ixt, (size_t)std::max(m->n_out_cells, 1) * 3 * pesz))) return rc;
   CK(cudaMemset(m->pml_ixt.p, 0, m->pml_ixt.bytes));
   // ---- filters + materials
   const size_t J = 3 * (size_t)(eo + mo);

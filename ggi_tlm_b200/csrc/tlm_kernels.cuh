@@ -57,6 +57,17 @@ struct MatDev {
   double eps_a[kMaxOrder + 1], eps_b[kMaxOrder + 1], mu_a[kMaxOrder + 1], mu_b[kMaxOrder + 1];
 };
 
+// Storage and arithmetic types of the PML update for a link type T.
+template <typename T> struct PmlTypes { using state = T; using arith = T; };
+template <> struct PmlTypes<float> {
+  using state = float;
+  // The PML recursions run in FP64 with FP64 coefficients: with FP32
+  // coefficients (exp(-s dt/2), 1-(s_i+s_j)dt/4, ...) the quasi-static field a
+  // DC-carrying source leaves inside the PML drifts, and the late-time probe
+  // error grows 100x.  The state stays FP32 in storage.
+  using arith = double;
+};
+
 template <typename T>
 struct MeshDev {
   int nx, ny, nz, Px, Py;
@@ -70,10 +81,10 @@ struct MeshDev {
   const uint32_t *seg_base;
   const int4 *sp_rec;
   const int4 *sp_pos;       // (x, y, z) 0-based of each special cell
-  T *pml_state;             // [24][n_pml]
+  typename PmlTypes<T>::state *pml_state;  // [24][n_pml]
   int n_pml;
-  const T *pml_par;         // [n_par][16]
-  T *pml_ixt;               // [n_out][3]
+  const double *pml_par;    // [n_par][16], FP64 in both precisions
+  typename PmlTypes<T>::state *pml_ixt;    // [n_out][3]
   double *filt;             // [J][n_filt]
   int n_filt, filt_eo, filt_mo;  // eps/mu max orders (state taps per component)
   const MatDev *mats;
@@ -127,23 +138,37 @@ __device__ __forceinline__ void scatter_pulses(const T *inc, T *out, T Vx, T Vy,
   out[Vz_ymax] = Vz - Z0 * Ix - inc[Vz_ymin];
 }
 
+// In FP64 the formulas follow scatter.F90 literally (I = (...)/(2 Z0), then
+// Z0*I).  In FP32 the currents are carried scaled by Z0 (U = Z0*I = (...)/2):
+// algebraically identical, one rounding less per current, and halving is
+// exact in both precisions.
 template <typename T>
 __device__ __forceinline__ void free_space_cell(const T *inc, T *out) {
-  T Vx = (inc[Vx_ymin] + inc[Vx_ymax] + inc[Vx_zmin] + inc[Vx_zmax]) / T(2);
-  T Vy = (inc[Vy_xmin] + inc[Vy_xmax] + inc[Vy_zmin] + inc[Vy_zmax]) / T(2);
-  T Vz = (inc[Vz_xmin] + inc[Vz_xmax] + inc[Vz_ymin] + inc[Vz_ymax]) / T(2);
-  T Ix, Iy, Iz;
+  const T Vx = (inc[Vx_ymin] + inc[Vx_ymax] + inc[Vx_zmin] + inc[Vx_zmax]) / T(2);
+  const T Vy = (inc[Vy_xmin] + inc[Vy_xmax] + inc[Vy_zmin] + inc[Vy_zmax]) / T(2);
+  const T Vz = (inc[Vz_xmin] + inc[Vz_xmax] + inc[Vz_ymin] + inc[Vz_ymax]) / T(2);
   if constexpr (sizeof(T) == 8) {
-    Ix = (inc[Vz_ymax] - inc[Vy_zmax] - inc[Vz_ymin] + inc[Vy_zmin]) / (2.0 * kZ0);
-    Iy = (inc[Vx_zmax] - inc[Vz_xmax] - inc[Vx_zmin] + inc[Vz_xmin]) / (2.0 * kZ0);
-    Iz = (inc[Vy_xmax] - inc[Vx_ymax] - inc[Vy_xmin] + inc[Vx_ymin]) / (2.0 * kZ0);
+    const double Ix = (inc[Vz_ymax] - inc[Vy_zmax] - inc[Vz_ymin] + inc[Vy_zmin]) / (2.0 * kZ0);
+    const double Iy = (inc[Vx_zmax] - inc[Vz_xmax] - inc[Vx_zmin] + inc[Vz_xmin]) / (2.0 * kZ0);
+    const double Iz = (inc[Vy_xmax] - inc[Vx_ymax] - inc[Vy_xmin] + inc[Vx_ymin]) / (2.0 * kZ0);
+    scatter_pulses<T>(inc, out, Vx, Vy, Vz, Ix, Iy, Iz);
   } else {
-    const float r = float(1.0 / (2.0 * kZ0));
-    Ix = (inc[Vz_ymax] - inc[Vy_zmax] - inc[Vz_ymin] + inc[Vy_zmin]) * r;
-    Iy = (inc[Vx_zmax] - inc[Vz_xmax] - inc[Vx_zmin] + inc[Vz_xmin]) * r;
-    Iz = (inc[Vy_xmax] - inc[Vx_ymax] - inc[Vy_xmin] + inc[Vx_ymin]) * r;
+    const T Ux = (inc[Vz_ymax] - inc[Vy_zmax] - inc[Vz_ymin] + inc[Vy_zmin]) / T(2);
+    const T Uy = (inc[Vx_zmax] - inc[Vz_xmax] - inc[Vx_zmin] + inc[Vz_xmin]) / T(2);
+    const T Uz = (inc[Vy_xmax] - inc[Vx_ymax] - inc[Vy_xmin] + inc[Vx_ymin]) / T(2);
+    out[Vx_ymin] = Vx - Uz - inc[Vx_ymax];
+    out[Vx_ymax] = Vx + Uz - inc[Vx_ymin];
+    out[Vx_zmin] = Vx + Uy - inc[Vx_zmax];
+    out[Vx_zmax] = Vx - Uy - inc[Vx_zmin];
+    out[Vy_zmin] = Vy - Ux - inc[Vy_zmax];
+    out[Vy_zmax] = Vy + Ux - inc[Vy_zmin];
+    out[Vy_xmin] = Vy + Uz - inc[Vy_xmax];
+    out[Vy_xmax] = Vy - Uz - inc[Vy_xmin];
+    out[Vz_xmin] = Vz - Uy - inc[Vz_xmax];
+    out[Vz_xmax] = Vz + Uy - inc[Vz_xmin];
+    out[Vz_ymin] = Vz + Ux - inc[Vz_ymax];
+    out[Vz_ymax] = Vz - Ux - inc[Vz_ymin];
   }
-  scatter_pulses<T>(inc, out, Vx, Vy, Vz, Ix, Iy, Iz);
 }
 
 // ---------------------------------------------------------------------------
@@ -152,27 +177,31 @@ __device__ __forceinline__ void free_space_cell(const T *inc, T *out) {
 template <typename T>
 __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par, int out_no, const T *inc_in, T *out,
                                       double *cell_out_row) {
-  const T Z0 = T(kZ0);
-  const T *P = m.pml_par + (size_t)par * 16;
-  const T ax = P[0], ay = P[1], az = P[2];
-  const T exp_x = P[3], exp_y = P[4], exp_z = P[5];
-  const T Csx = P[6], Csy = P[7], Csz = P[8];
-  const T Csx2 = P[9], Csy2 = P[10], Csz2 = P[11];
-  const T Csy_sz = P[12], Csz_sx = P[13], Csx_sy = P[14];
-  T *S = m.pml_state;
+  using A = typename PmlTypes<T>::arith;
+  using ST = typename PmlTypes<T>::state;
+  // FP64: literal scatter_PML.F90 arithmetic.  FP32: currents (and the
+  // series-term state) carried scaled by Z0, i.e. Z0 = 1 below.
+  const A Z0 = sizeof(T) == 8 ? A(kZ0) : A(1);
+  const double *P = m.pml_par + (size_t)par * 16;
+  const A ax = A(P[0]), ay = A(P[1]), az = A(P[2]);
+  const A exp_x = A(P[3]), exp_y = A(P[4]), exp_z = A(P[5]);
+  const A Csx = A(P[6]), Csy = A(P[7]), Csz = A(P[8]);
+  const A Csx2 = A(P[9]), Csy2 = A(P[10]), Csz2 = A(P[11]);
+  const A Csy_sz = A(P[12]), Csz_sx = A(P[13]), Csx_sy = A(P[14]);
+  ST *S = m.pml_state;
   const int n = m.n_pml;
-  const T last_Ix = __ldcs(S + 0 * n + pidx), last_Iy = __ldcs(S + 1 * n + pidx), last_Iz = __ldcs(S + 2 * n + pidx);
-  T last_Vi[12];
+  const A last_Ix = __ldcs(S + 0 * n + pidx), last_Iy = __ldcs(S + 1 * n + pidx), last_Iz = __ldcs(S + 2 * n + pidx);
+  A last_Vi[12];
 #pragma unroll
   for (int k = 0; k < 12; k++) last_Vi[k] = __ldcs(S + (size_t)(3 + k) * n + pidx);
-  const T last_Vxt = __ldcs(S + (size_t)15 * n + pidx), last_Vyt = __ldcs(S + (size_t)16 * n + pidx);
-  const T last_Vzt = __ldcs(S + (size_t)17 * n + pidx);
-  const T last_Vxyt = __ldcs(S + (size_t)18 * n + pidx), last_Vyxt = __ldcs(S + (size_t)19 * n + pidx);
-  const T last_Vzxt = __ldcs(S + (size_t)20 * n + pidx), last_Vxzt = __ldcs(S + (size_t)21 * n + pidx);
-  const T last_Vyzt = __ldcs(S + (size_t)22 * n + pidx), last_Vzyt = __ldcs(S + (size_t)23 * n + pidx);
+  const A last_Vxt = __ldcs(S + (size_t)15 * n + pidx), last_Vyt = __ldcs(S + (size_t)16 * n + pidx);
+  const A last_Vzt = __ldcs(S + (size_t)17 * n + pidx);
+  const A last_Vxyt = __ldcs(S + (size_t)18 * n + pidx), last_Vyxt = __ldcs(S + (size_t)19 * n + pidx);
+  const A last_Vzxt = __ldcs(S + (size_t)20 * n + pidx), last_Vxzt = __ldcs(S + (size_t)21 * n + pidx);
+  const A last_Vyzt = __ldcs(S + (size_t)22 * n + pidx), last_Vzyt = __ldcs(S + (size_t)23 * n + pidx);
 
   // STAGE 3: half-cell loss on incident pulses
-  T V[12];
+  A V[12];
   V[Vynx] = inc_in[Vynx] * exp_y; V[Vypx] = inc_in[Vypx] * exp_y;
   V[Vznx] = inc_in[Vznx] * exp_z; V[Vzpx] = inc_in[Vzpx] * exp_z;
   V[Vxny] = inc_in[Vxny] * exp_x; V[Vxpy] = inc_in[Vxpy] * exp_x;
@@ -180,76 +209,77 @@ __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par,
   V[Vxnz] = inc_in[Vxnz] * exp_x; V[Vxpz] = inc_in[Vxpz] * exp_x;
   V[Vynz] = inc_in[Vynz] * exp_y; V[Vypz] = inc_in[Vypz] * exp_y;
   // STAGE 4
-  const T Vx = (V[Vynx] + V[Vypx] + V[Vznx] + V[Vzpx]) / T(2);
-  const T Vy = (V[Vxny] + V[Vxpy] + V[Vzny] + V[Vzpy]) / T(2);
-  const T Vz = (V[Vxnz] + V[Vxpz] + V[Vynz] + V[Vypz]) / T(2);
-  const T Ix = (V[Vypz] - V[Vzpy] - V[Vynz] + V[Vzny]) / (T(2) * Z0);
-  const T Iy = (V[Vzpx] - V[Vxpz] - V[Vznx] + V[Vxnz]) / (T(2) * Z0);
-  const T Iz = (V[Vxpy] - V[Vypx] - V[Vxny] + V[Vynx]) / (T(2) * Z0);
+  const A Vx = (V[Vynx] + V[Vypx] + V[Vznx] + V[Vzpx]) / A(2);
+  const A Vy = (V[Vxny] + V[Vxpy] + V[Vzny] + V[Vzpy]) / A(2);
+  const A Vz = (V[Vxnz] + V[Vxpz] + V[Vynz] + V[Vypz]) / A(2);
+  const A Ix = (V[Vypz] - V[Vzpy] - V[Vynz] + V[Vzny]) / (A(2) * Z0);
+  const A Iy = (V[Vzpx] - V[Vxpz] - V[Vznx] + V[Vxnz]) / (A(2) * Z0);
+  const A Iz = (V[Vxpy] - V[Vypx] - V[Vxny] + V[Vynx]) / (A(2) * Z0);
   // STAGE 5
-  const T Vx_sh = ax * (-(last_Vi[Vznx] + last_Vi[Vzpx] + last_Vi[Vynx] + last_Vi[Vypx]) / T(2) +
+  const A Vx_sh = ax * (-(last_Vi[Vznx] + last_Vi[Vzpx] + last_Vi[Vynx] + last_Vi[Vypx]) / A(2) +
                         Csy * ((V[Vznx] + V[Vzpx]) + (last_Vi[Vznx] + last_Vi[Vzpx])) +
                         Csz * ((V[Vynx] + V[Vypx]) + (last_Vi[Vynx] + last_Vi[Vypx])) + Csy_sz * last_Vxt);
-  const T Vy_sh = ay * (-(last_Vi[Vxny] + last_Vi[Vxpy] + last_Vi[Vzny] + last_Vi[Vzpy]) / T(2) +
+  const A Vy_sh = ay * (-(last_Vi[Vxny] + last_Vi[Vxpy] + last_Vi[Vzny] + last_Vi[Vzpy]) / A(2) +
                         Csz * ((V[Vxny] + V[Vxpy]) + (last_Vi[Vxny] + last_Vi[Vxpy])) +
                         Csx * ((V[Vzny] + V[Vzpy]) + (last_Vi[Vzny] + last_Vi[Vzpy])) + Csz_sx * last_Vyt);
-  const T Vz_sh = az * (-(last_Vi[Vynz] + last_Vi[Vypz] + last_Vi[Vxnz] + last_Vi[Vxpz]) / T(2) +
+  const A Vz_sh = az * (-(last_Vi[Vynz] + last_Vi[Vypz] + last_Vi[Vxnz] + last_Vi[Vxpz]) / A(2) +
                         Csx * ((V[Vynz] + V[Vypz]) + (last_Vi[Vynz] + last_Vi[Vypz])) +
                         Csy * ((V[Vxnz] + V[Vxpz]) + (last_Vi[Vxnz] + last_Vi[Vxpz])) + Csx_sy * last_Vzt);
   // STAGE 6
-  const T Vxt = ax * Vx + Vx_sh, Vyt = ay * Vy + Vy_sh, Vzt = az * Vz + Vz_sh;
+  const A Vxt = ax * Vx + Vx_sh, Vyt = ay * Vy + Vy_sh, Vzt = az * Vz + Vz_sh;
   // STAGE 7a (output cells only)
-  T Ixt = T(0), Iyt = T(0), Izt = T(0);
+  A Ixt = A(0), Iyt = A(0), Izt = A(0);
   if (out_no >= 0) {
-    T *X = m.pml_ixt + (size_t)out_no * 3;
+    ST *X = m.pml_ixt + (size_t)out_no * 3;
     Ixt = ax * (Ix - last_Ix + Csx2 * (Ix + last_Ix) + Csy_sz * X[0]);
     Iyt = ay * (Iy - last_Iy + Csy2 * (Iy + last_Iy) + Csz_sx * X[1]);
     Izt = az * (Iz - last_Iz + Csz2 * (Iz + last_Iz) + Csx_sy * X[2]);
-    X[0] = Ixt; X[1] = Iyt; X[2] = Izt;
+    X[0] = ST(Ixt); X[1] = ST(Iyt); X[2] = ST(Izt);
   }
   // STAGE 7
-  const T Vxy_se = az * (Z0 * (-last_Iz + Csy2 * (Iz + last_Iz)) + Csx_sy * last_Vxyt);
-  const T Vyx_se = az * (Z0 * (-last_Iz + Csx2 * (Iz + last_Iz)) + Csx_sy * last_Vyxt);
-  const T Vzx_se = ay * (Z0 * (-last_Iy + Csx2 * (Iy + last_Iy)) + Csz_sx * last_Vzxt);
-  const T Vxz_se = ay * (Z0 * (-last_Iy + Csz2 * (Iy + last_Iy)) + Csz_sx * last_Vxzt);
-  const T Vyz_se = ax * (Z0 * (-last_Ix + Csz2 * (Ix + last_Ix)) + Csy_sz * last_Vyzt);
-  const T Vzy_se = ax * (Z0 * (-last_Ix + Csy2 * (Ix + last_Ix)) + Csy_sz * last_Vzyt);
+  const A Vxy_se = az * (Z0 * (-last_Iz + Csy2 * (Iz + last_Iz)) + Csx_sy * last_Vxyt);
+  const A Vyx_se = az * (Z0 * (-last_Iz + Csx2 * (Iz + last_Iz)) + Csx_sy * last_Vyxt);
+  const A Vzx_se = ay * (Z0 * (-last_Iy + Csx2 * (Iy + last_Iy)) + Csz_sx * last_Vzxt);
+  const A Vxz_se = ay * (Z0 * (-last_Iy + Csz2 * (Iy + last_Iy)) + Csz_sx * last_Vxzt);
+  const A Vyz_se = ax * (Z0 * (-last_Ix + Csz2 * (Ix + last_Ix)) + Csy_sz * last_Vyzt);
+  const A Vzy_se = ax * (Z0 * (-last_Ix + Csy2 * (Ix + last_Ix)) + Csy_sz * last_Vzyt);
   // STAGE 8 + 9: save state
-  __stcs(S + 0 * n + pidx, Ix); __stcs(S + 1 * n + pidx, Iy); __stcs(S + 2 * n + pidx, Iz);
+  __stcs(S + 0 * n + pidx, ST(Ix)); __stcs(S + 1 * n + pidx, ST(Iy)); __stcs(S + 2 * n + pidx, ST(Iz));
 #pragma unroll
-  for (int k = 0; k < 12; k++) __stcs(S + (size_t)(3 + k) * n + pidx, V[k]);
-  __stcs(S + (size_t)15 * n + pidx, Vxt); __stcs(S + (size_t)16 * n + pidx, Vyt); __stcs(S + (size_t)17 * n + pidx, Vzt);
-  __stcs(S + (size_t)18 * n + pidx, az * Iz * Z0 + Vxy_se);
-  __stcs(S + (size_t)19 * n + pidx, az * Iz * Z0 + Vyx_se);
-  __stcs(S + (size_t)20 * n + pidx, ay * Iy * Z0 + Vzx_se);
-  __stcs(S + (size_t)21 * n + pidx, ay * Iy * Z0 + Vxz_se);
-  __stcs(S + (size_t)22 * n + pidx, ax * Ix * Z0 + Vyz_se);
-  __stcs(S + (size_t)23 * n + pidx, ax * Ix * Z0 + Vzy_se);
+  for (int k = 0; k < 12; k++) __stcs(S + (size_t)(3 + k) * n + pidx, ST(V[k]));
+  __stcs(S + (size_t)15 * n + pidx, ST(Vxt)); __stcs(S + (size_t)16 * n + pidx, ST(Vyt)); __stcs(S + (size_t)17 * n + pidx, ST(Vzt));
+  __stcs(S + (size_t)18 * n + pidx, ST(az * Iz * Z0 + Vxy_se));
+  __stcs(S + (size_t)19 * n + pidx, ST(az * Iz * Z0 + Vyx_se));
+  __stcs(S + (size_t)20 * n + pidx, ST(ay * Iy * Z0 + Vzx_se));
+  __stcs(S + (size_t)21 * n + pidx, ST(ay * Iy * Z0 + Vxz_se));
+  __stcs(S + (size_t)22 * n + pidx, ST(ax * Ix * Z0 + Vyz_se));
+  __stcs(S + (size_t)23 * n + pidx, ST(ax * Ix * Z0 + Vzy_se));
   // STAGE 10
-  const T Vynx_P = Vx_sh - Vyx_se, Vypx_P = Vx_sh + Vyx_se;
-  const T Vznx_P = Vx_sh + Vzx_se, Vzpx_P = Vx_sh - Vzx_se;
-  const T Vxny_P = Vy_sh + Vxy_se, Vxpy_P = Vy_sh - Vxy_se;
-  const T Vzny_P = Vy_sh - Vzy_se, Vzpy_P = Vy_sh + Vzy_se;
-  const T Vynz_P = Vz_sh + Vyz_se, Vypz_P = Vz_sh - Vyz_se;
-  const T Vxnz_P = Vz_sh - Vxz_se, Vxpz_P = Vz_sh + Vxz_se;
+  const A Vynx_P = Vx_sh - Vyx_se, Vypx_P = Vx_sh + Vyx_se;
+  const A Vznx_P = Vx_sh + Vzx_se, Vzpx_P = Vx_sh - Vzx_se;
+  const A Vxny_P = Vy_sh + Vxy_se, Vxpy_P = Vy_sh - Vxy_se;
+  const A Vzny_P = Vy_sh - Vzy_se, Vzpy_P = Vy_sh + Vzy_se;
+  const A Vynz_P = Vz_sh + Vyz_se, Vypz_P = Vz_sh - Vyz_se;
+  const A Vxnz_P = Vz_sh - Vxz_se, Vxpz_P = Vz_sh + Vxz_se;
   // STAGE 11 + 13: scattered pulses with half-cell loss
-  out[Vynx] = (ax * Vx - az * Z0 * Iz - V[Vypx] + Vynx_P) * exp_y;
-  out[Vypx] = (ax * Vx + az * Z0 * Iz - V[Vynx] + Vypx_P) * exp_y;
-  out[Vznx] = (ax * Vx + ay * Z0 * Iy - V[Vzpx] + Vznx_P) * exp_z;
-  out[Vzpx] = (ax * Vx - ay * Z0 * Iy - V[Vznx] + Vzpx_P) * exp_z;
-  out[Vzny] = (ay * Vy - ax * Z0 * Ix - V[Vzpy] + Vzny_P) * exp_z;
-  out[Vzpy] = (ay * Vy + ax * Z0 * Ix - V[Vzny] + Vzpy_P) * exp_z;
-  out[Vxny] = (ay * Vy + az * Z0 * Iz - V[Vxpy] + Vxny_P) * exp_x;
-  out[Vxpy] = (ay * Vy - az * Z0 * Iz - V[Vxny] + Vxpy_P) * exp_x;
-  out[Vxnz] = (az * Vz - ay * Z0 * Iy - V[Vxpz] + Vxnz_P) * exp_x;
-  out[Vxpz] = (az * Vz + ay * Z0 * Iy - V[Vxnz] + Vxpz_P) * exp_x;
-  out[Vynz] = (az * Vz + ax * Z0 * Ix - V[Vypz] + Vynz_P) * exp_y;
-  out[Vypz] = (az * Vz - ax * Z0 * Ix - V[Vynz] + Vypz_P) * exp_y;
+  out[Vynx] = T((ax * Vx - az * Z0 * Iz - V[Vypx] + Vynx_P) * exp_y);
+  out[Vypx] = T((ax * Vx + az * Z0 * Iz - V[Vynx] + Vypx_P) * exp_y);
+  out[Vznx] = T((ax * Vx + ay * Z0 * Iy - V[Vzpx] + Vznx_P) * exp_z);
+  out[Vzpx] = T((ax * Vx - ay * Z0 * Iy - V[Vznx] + Vzpx_P) * exp_z);
+  out[Vzny] = T((ay * Vy - ax * Z0 * Ix - V[Vzpy] + Vzny_P) * exp_z);
+  out[Vzpy] = T((ay * Vy + ax * Z0 * Ix - V[Vzny] + Vzpy_P) * exp_z);
+  out[Vxny] = T((ay * Vy + az * Z0 * Iz - V[Vxpy] + Vxny_P) * exp_x);
+  out[Vxpy] = T((ay * Vy - az * Z0 * Iz - V[Vxny] + Vxpy_P) * exp_x);
+  out[Vxnz] = T((az * Vz - ay * Z0 * Iy - V[Vxpz] + Vxnz_P) * exp_x);
+  out[Vxpz] = T((az * Vz + ay * Z0 * Iy - V[Vxnz] + Vxpz_P) * exp_x);
+  out[Vynz] = T((az * Vz + ax * Z0 * Ix - V[Vypz] + Vynz_P) * exp_y);
+  out[Vypz] = T((az * Vz - ax * Z0 * Ix - V[Vynz] + Vypz_P) * exp_y);
   // STAGE 12: output
   if (out_no >= 0) {
     const double dl = m.dl;
     cell_out_row[0] = -double(Vxt) / dl; cell_out_row[1] = -double(Vyt) / dl; cell_out_row[2] = -double(Vzt) / dl;
-    cell_out_row[3] = double(Ixt) / dl; cell_out_row[4] = double(Iyt) / dl; cell_out_row[5] = double(Izt) / dl;
+    const double hs = sizeof(T) == 8 ? dl : dl * kZ0;  // FP32 carries Z0*I
+    cell_out_row[3] = double(Ixt) / hs; cell_out_row[4] = double(Iyt) / hs; cell_out_row[5] = double(Izt) / hs;
   }
 }
 
