@@ -34,7 +34,8 @@ EXPORTS = [
     "tlm_gpu_synchronize", "tlm_gpu_fetch_cell_output", "tlm_gpu_fetch_dft", "tlm_gpu_fetch_links",
     "tlm_gpu_set_stream", "tlm_gpu_set_timing", "tlm_gpu_last_run_time", "tlm_gpu_memory_bytes",
     "tlm_gpu_last_run_launches", "tlm_gpu_destroy", "tlm_gpu_last_error", "tlm_gpu_set_variant",
-    "tlm_gpu_num_variants", "tlm_gpu_fetch_links_noalloc",
+    "tlm_gpu_num_variants", "tlm_gpu_fetch_links_noalloc", "tlm_gpu_batch_create", "tlm_gpu_batch_set_variant",
+    "tlm_gpu_batch_run", "tlm_gpu_batch_synchronize", "tlm_gpu_batch_last_run", "tlm_gpu_batch_destroy",
 ]
 
 
@@ -91,6 +92,12 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_variant": [i64, i32],
         "tlm_gpu_num_variants": [C.POINTER(i32)],
         "tlm_gpu_last_error": [C.c_char_p, i32],
+        "tlm_gpu_batch_create": [C.POINTER(i64), i32, C.POINTER(i64)],
+        "tlm_gpu_batch_set_variant": [i64, i32],
+        "tlm_gpu_batch_run": [i64, i32],
+        "tlm_gpu_batch_synchronize": [i64],
+        "tlm_gpu_batch_last_run": [i64, C.POINTER(C.c_float), C.POINTER(i64), C.POINTER(i64)],
+        "tlm_gpu_batch_destroy": [i64],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -243,6 +250,55 @@ class GpuMesh:
     def close(self):
         if getattr(self, "h", 0):
             _check(_lib.tlm_gpu_destroy(self.h))
+            self.h = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class GpuBatch:
+    """Several GpuMesh objects advanced together (one launch per kernel type
+    per step, graph-replayed).  The meshes keep their own results."""
+
+    def __init__(self, meshes):
+        lib = load_library()
+        self.meshes = list(meshes)
+        arr = (C.c_int64 * len(self.meshes))(*[m.h for m in self.meshes])
+        h = C.c_int64(0)
+        _check(lib.tlm_gpu_batch_create(arr, len(self.meshes), C.byref(h)))
+        self.h = h.value
+
+    def set_variant(self, v: int):
+        _check(_lib.tlm_gpu_batch_set_variant(self.h, v))
+
+    def run(self, n_steps: int, sync: bool = True):
+        _check(_lib.tlm_gpu_batch_run(self.h, n_steps))
+        before = {id(m): m.step for m in self.meshes}
+        for m in self.meshes:
+            m.step = min(m.t["n_timesteps"], before[id(m)] + n_steps)
+        if sync:
+            self.synchronize()
+
+    def synchronize(self):
+        _check(_lib.tlm_gpu_batch_synchronize(self.h))
+
+    def last_run(self):
+        ms, cu, la = C.c_float(0), C.c_int64(0), C.c_int64(0)
+        _check(_lib.tlm_gpu_batch_last_run(self.h, C.byref(ms), C.byref(cu), C.byref(la)))
+        return ms.value, cu.value, la.value
+
+    def close(self):
+        if getattr(self, "h", 0):
+            _check(_lib.tlm_gpu_batch_destroy(self.h))
             self.h = 0
 
     def __del__(self):

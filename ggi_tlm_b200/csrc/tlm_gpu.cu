@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -104,9 +105,12 @@ struct Mesh {
   int n_sms = 148;
   std::vector<uint32_t> host_mask;  // per-32-element special-cell masks (for tile lists)
   DevBuf tiles, d_err;
+  std::vector<int4> host_tiles;
+  cudaStream_t batch_stream = nullptr;  // set while the mesh belongs to a batch
   int tiles_tile = 0;  // TILE the current list was built for
   int n_tiles = 0;
   bool dry_launch = false;
+  int pml_prefetch = 1200;  // blocks ahead for the PML state L2 prefetch (0 = off)
 
   // graph of kGraphSteps steps
   static constexpr int kGraphSteps = 8;
@@ -346,6 +350,7 @@ int finalize(Mesh *m) {
   if (pml_out.empty()) pml_out.resize(1);
   {
     int rc2;
+    pml_pos.resize(pml_pos.size() + 8, 0ull);  // 64 bytes of padding for the widened L2 prefetch
     if ((rc2 = upload(m, m->pml_pos, pml_pos)) || (rc2 = upload(m, m->pml_par16, pml_par)) ||
         (rc2 = upload(m, m->pml_outmap, pml_out)))
       return rc2;
@@ -365,7 +370,7 @@ int finalize(Mesh *m) {
   CK(cudaMemset(m->links.p, 0, m->links.bytes));
   // ---- PML
   const size_t pesz = m->fp64 ? sizeof(tlm::PmlTypes<double>::state) : sizeof(tlm::PmlTypes<float>::state);
-  if ((rc = dalloc(m, m->pml_state, (size_t)tlm::kPmlState * std::max(m->n_pml_cells, 1) * pesz))) return rc;
+  if ((rc = dalloc(m, m->pml_state, (size_t)tlm::kPmlState * std::max(m->n_pml_cells, 1) * pesz + 64))) return rc;
   CK(cudaMemset(m->pml_state.p, 0, m->pml_state.bytes));
   {
     std::vector<double> par((size_t)std::max(m->n_pml_params, 1) * 16, 0.0);
@@ -495,6 +500,7 @@ int finalize(Mesh *m) {
   }
   CK(cudaEventCreate(&m->ev0));
   CK(cudaEventCreate(&m->ev1));
+  if (const char *pf = getenv("TLM_PML_PREFETCH_BLOCKS")) m->pml_prefetch = atoi(pf);
   m->finalized = true;
   return TLM_OK;
 }
@@ -540,6 +546,7 @@ int build_tiles(Mesh *m, int TILE) {
     }
   }
   m->n_tiles = (int)tl.size();
+  m->host_tiles = tl;
   if (tl.empty()) tl.resize(1);
   int rc = upload(m, m->tiles, tl);
   if (rc) return rc;
@@ -565,7 +572,7 @@ int launch_tma(Mesh *m, const tlm::MeshDev<T> &md, int k) {
   const int grid = std::max(1, std::min(m->n_tiles, per_sm * m->n_sms));
   tlm::TileList tl{(const int4 *)m->tiles.p, m->n_tiles, (int *)m->d_err.p};
   if (m->dry_launch) return TLM_OK;  // configuration only (outside stream capture)
-  if (m->n_tiles) kern<<<grid, Cfg::THREADS, Cfg::SMEM, m->stream>>>(md, tl, k);
+  if (m->n_tiles) kern<<<grid, Cfg::THREADS, Cfg::SMEM, m->stream>>>(md, nullptr, tl, k);
   return TLM_OK;
 }
 
@@ -632,7 +639,7 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
     if (m->n_pml_list) {
       tlm::PmlList pl{(const unsigned long long *)m->pml_pos.p, (const uint16_t *)m->pml_par16.p,
                       (const int2 *)m->pml_outmap.p, m->n_pml_list, m->n_pml_out};
-      tlm::tlm_pml_kernel<T><<<(m->n_pml_list + 127) / 128, 128, 0, m->stream>>>(md, pl, k);
+      tlm::tlm_pml_kernel<T><<<(m->n_pml_list + 127) / 128, 128, 0, m->stream>>>(md, pl, k, m->pml_prefetch);
       m->last_launches++;
     }
     if (m->n_sp_dev) {
@@ -1003,6 +1010,7 @@ int tlm_gpu_memory_bytes(int64_t h, int64_t *bytes) {
 int tlm_gpu_fetch_cell_output(int64_t h, int32_t first, int32_t n, double *out) {
   Mesh *m = get(h);
   if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
   if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
   if (first < 1 || n < 0 || first + n - 1 >= m->next_step) return fail(TLM_E_BADARG, "steps not yet computed");
   if (m->n_out_cells == 0 || n == 0) return TLM_OK;
@@ -1016,6 +1024,7 @@ int tlm_gpu_fetch_cell_output(int64_t h, int32_t first, int32_t n, double *out) 
 int tlm_gpu_fetch_dft(int64_t h, double *out) {
   Mesh *m = get(h);
   if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
   if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
   if (!m->dft_entries) return TLM_OK;
   CK(cudaStreamSynchronize(m->stream));
@@ -1026,6 +1035,7 @@ int tlm_gpu_fetch_dft(int64_t h, double *out) {
 int tlm_gpu_fetch_links(int64_t h, double *out) {
   Mesh *m = get(h);
   if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
   CK(cudaSetDevice(m->desc.device));
   int rc = finalize(m);
   if (rc) return rc;
@@ -1121,6 +1131,331 @@ int tlm_gpu_destroy(int64_t h) {
 int tlm_gpu_last_error(char *buf, int32_t len) {
   if (!buf || len <= 0) return TLM_E_BADARG;
   std::snprintf(buf, (size_t)len, "%s", g_last_error.c_str());
+  return TLM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batches: many meshes advanced together by one launch per kernel type.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Batch {
+  std::vector<int64_t> handles;
+  bool fp64 = false;
+  int device = 0;
+  int variant = 1;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  std::vector<int> active;  // indices into handles of the current segment
+  DevBuf meshes_d, pml_d, faces_d, dfts_d, nsp_d, tiles_d, pmlb_d, spb_d, faceb_d, dftb_d, dbases_d, err_d;
+  int n_tiles = 0, n_pmlb = 0, n_spb = 0, n_faceb = 0, n_dftb = 0;
+  long long last_cell_updates = 0;
+  long long last_launches = 0;
+  long long graph_launches = 0;
+  size_t dev_bytes = 0;
+  ~Batch() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+std::map<int64_t, std::unique_ptr<Batch>> g_batches;
+int64_t g_next_batch = 1;
+
+Batch *get_batch(int64_t h) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_batches.find(h);
+  return it == g_batches.end() ? nullptr : it->second.get();
+}
+
+template <typename V>
+int bupload(Batch *b, DevBuf &buf, const std::vector<V> &v) {
+  if (buf.p) {
+    cudaFree(buf.p);
+    b->dev_bytes -= buf.bytes;
+    buf.p = nullptr;
+  }
+  buf.bytes = std::max<size_t>(v.size() * sizeof(V), 16);
+  cudaError_t e = cudaMalloc(&buf.p, buf.bytes);
+  if (e != cudaSuccess) {
+    buf.p = nullptr;
+    return fail(TLM_E_OOM, "cudaMalloc(%zu) failed: %s", buf.bytes, cudaGetErrorString(e));
+  }
+  b->dev_bytes += buf.bytes;
+  if (!v.empty()) CK(cudaMemcpy(buf.p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice));
+  return TLM_OK;
+}
+
+// Build the device work lists of the active meshes.
+template <typename T>
+int build_batch_lists(Batch *b) {
+  const Variant &cf = kVariants[b->variant];
+  const int TILE = sizeof(T) == 4 ? cf.tile32 : cf.tile64;
+  std::vector<tlm::MeshDev<T>> md;
+  std::vector<tlm::PmlList> pl;
+  std::vector<tlm::FaceDev> fd;
+  std::vector<tlm::DftDev> dd;
+  std::vector<int> nsp;
+  std::vector<int4> tiles;
+  std::vector<int2> pmlb, spb, faceb, dftb;
+  std::vector<int *> bases;
+  for (size_t a = 0; a < b->active.size(); a++) {
+    Mesh *m = get(b->handles[b->active[a]]);
+    int rc = build_tiles(m, TILE);
+    if (rc) return rc;
+    md.push_back(mesh_dev<T>(m));
+    pl.push_back(tlm::PmlList{(const unsigned long long *)m->pml_pos.p, (const uint16_t *)m->pml_par16.p,
+                              (const int2 *)m->pml_outmap.p, m->n_pml_list, m->n_pml_out});
+    fd.push_back(face_dev(m));
+    dd.push_back(dft_dev(m));
+    nsp.push_back(m->n_sp_dev);
+    for (const int4 &tl : m->host_tiles) tiles.push_back(int4{tl.x, tl.y, tl.z, (int)a});
+    for (int s0 = 0; s0 < m->n_pml_list; s0 += 128) pmlb.push_back(int2{(int)a, s0});
+    for (int s0 = 0; s0 < m->n_sp_dev; s0 += 128) spb.push_back(int2{(int)a, s0});
+    for (int s0 = 0; s0 < (int)m->f_cx.size(); s0 += 128) faceb.push_back(int2{(int)a, s0});
+    for (int s0 = 0; s0 < m->dft_entries; s0 += 256) dftb.push_back(int2{(int)a, s0});
+    bases.push_back((int *)m->d_base.p);
+  }
+  b->n_tiles = (int)tiles.size();
+  b->n_pmlb = (int)pmlb.size();
+  b->n_spb = (int)spb.size();
+  b->n_faceb = (int)faceb.size();
+  b->n_dftb = (int)dftb.size();
+  int rc;
+  if ((rc = bupload(b, b->meshes_d, md)) || (rc = bupload(b, b->pml_d, pl)) || (rc = bupload(b, b->faces_d, fd)) ||
+      (rc = bupload(b, b->dfts_d, dd)) || (rc = bupload(b, b->nsp_d, nsp)) || (rc = bupload(b, b->tiles_d, tiles)) ||
+      (rc = bupload(b, b->pmlb_d, pmlb)) || (rc = bupload(b, b->spb_d, spb)) || (rc = bupload(b, b->faceb_d, faceb)) ||
+      (rc = bupload(b, b->dftb_d, dftb)) || (rc = bupload(b, b->dbases_d, bases)))
+    return rc;
+  return TLM_OK;
+}
+
+template <typename T, int VEC, int TILE, int NSTAGE>
+int launch_batch_tma(Batch *b, bool dry) {
+  using Cfg = tlm::TmaCfg<T, VEC, TILE, NSTAGE>;
+  auto kern = tlm::tlm_bulk_tma_kernel<T, VEC, TILE, NSTAGE>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM));
+  int per_sm = 0, n_sms = 148;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Cfg::THREADS, Cfg::SMEM));
+  CK(cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, b->device));
+  if (per_sm < 1) per_sm = 1;
+  if (dry || !b->n_tiles) return TLM_OK;
+  const int grid = std::max(1, std::min(b->n_tiles, per_sm * n_sms));
+  tlm::TileList tl{(const int4 *)b->tiles_d.p, b->n_tiles, (int *)b->err_d.p};
+  tlm::MeshDev<T> none{};
+  kern<<<grid, Cfg::THREADS, Cfg::SMEM, b->stream>>>(none, (const tlm::MeshDev<T> *)b->meshes_d.p, tl, 0);
+  b->last_launches++;
+  return TLM_OK;
+}
+
+template <typename T, int VEC>
+int batch_step(Batch *b, bool dry) {
+  int rc = TLM_OK;
+  if constexpr (sizeof(T) == 4) {
+    switch (b->variant) {
+      case 1: rc = launch_batch_tma<T, VEC, 1024, 2>(b, dry); break;
+      case 2: rc = launch_batch_tma<T, VEC, 512, 3>(b, dry); break;
+      case 3: rc = launch_batch_tma<T, VEC, 512, 4>(b, dry); break;
+      case 4: rc = launch_batch_tma<T, VEC, 1024, 3>(b, dry); break;
+      default: rc = launch_batch_tma<T, VEC, 256, 6>(b, dry); break;
+    }
+  } else {
+    switch (b->variant) {
+      case 1: rc = launch_batch_tma<T, VEC, 512, 2>(b, dry); break;
+      case 2: rc = launch_batch_tma<T, VEC, 256, 3>(b, dry); break;
+      case 3: rc = launch_batch_tma<T, VEC, 256, 4>(b, dry); break;
+      case 4: rc = launch_batch_tma<T, VEC, 512, 3>(b, dry); break;
+      default: rc = launch_batch_tma<T, VEC, 128, 6>(b, dry); break;
+    }
+  }
+  if (rc || dry) return rc;
+  tlm::BatchDev<T> bd{};
+  bd.meshes = (const tlm::MeshDev<T> *)b->meshes_d.p;
+  bd.pml = (const tlm::PmlList *)b->pml_d.p;
+  bd.faces = (const tlm::FaceDev *)b->faces_d.p;
+  bd.dfts = (const tlm::DftDev *)b->dfts_d.p;
+  bd.n_special = (const int *)b->nsp_d.p;
+  bd.pml_blocks = (const int2 *)b->pmlb_d.p;
+  bd.special_blocks = (const int2 *)b->spb_d.p;
+  bd.face_blocks = (const int2 *)b->faceb_d.p;
+  bd.dft_blocks = (const int2 *)b->dftb_d.p;
+  bd.n_pml_blocks = b->n_pmlb;
+  bd.n_special_blocks = b->n_spb;
+  bd.n_face_blocks = b->n_faceb;
+  bd.n_dft_blocks = b->n_dftb;
+  bd.d_bases = (int *const *)b->dbases_d.p;
+  bd.n_active = (int)b->active.size();
+  if (b->n_pmlb) { tlm::tlm_pml_batch_kernel<T><<<b->n_pmlb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
+  if (b->n_spb) { tlm::tlm_special_batch_kernel<T><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
+  if (b->n_faceb) { tlm::tlm_face_batch_kernel<T><<<b->n_faceb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
+  if (b->n_dftb) { tlm::tlm_dft_batch_kernel<T><<<b->n_dftb, 256, 0, b->stream>>>(bd, 0); b->last_launches++; }
+  tlm::tlm_advance_batch<<<(bd.n_active + 127) / 128, 128, 0, b->stream>>>(bd.d_bases, bd.n_active, 1);
+  b->last_launches++;
+  CK(cudaGetLastError());
+  return TLM_OK;
+}
+
+int batch_step_any(Batch *b, bool dry) { return b->fp64 ? batch_step<double, 2>(b, dry) : batch_step<float, 4>(b, dry); }
+
+}  // namespace
+
+extern "C" {
+
+int tlm_gpu_batch_create(const int64_t *handles, int32_t n, int64_t *batch) {
+  if (!handles || n < 1 || !batch) return fail(TLM_E_BADARG, "bad batch arguments");
+  auto b = std::make_unique<Batch>();
+  for (int i = 0; i < n; i++) {
+    Mesh *m = get(handles[i]);
+    if (!m) return fail(TLM_E_BADARG, "bad handle at position %d", i);
+    if (m->batch_stream) return fail(TLM_E_STATE, "mesh %d already belongs to a batch", i);
+    if (i == 0) {
+      b->fp64 = m->fp64;
+      b->device = m->desc.device;
+    } else if (m->fp64 != b->fp64 || m->desc.device != b->device) {
+      return fail(TLM_E_BADARG, "all meshes of a batch need the same precision and device");
+    }
+    for (int j = 0; j < i; j++)
+      if (handles[j] == handles[i]) return fail(TLM_E_BADARG, "mesh listed twice");
+  }
+  CK(cudaSetDevice(b->device));
+  for (int i = 0; i < n; i++) {
+    Mesh *m = get(handles[i]);
+    int rc = finalize(m);
+    if (rc) return rc;
+    if (m->stream) CK(cudaStreamSynchronize(m->stream));
+  }
+  b->handles.assign(handles, handles + n);
+  CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&b->ev0));
+  CK(cudaEventCreate(&b->ev1));
+  {
+    std::vector<int> zero(1, 0);
+    int rc = bupload(b.get(), b->err_d, zero);
+    if (rc) return rc;
+  }
+  for (int i = 0; i < n; i++) get(handles[i])->batch_stream = b->stream;
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int64_t h = g_next_batch++;
+  g_batches[h] = std::move(b);
+  *batch = h;
+  return TLM_OK;
+}
+
+int tlm_gpu_batch_set_variant(int64_t bh, int32_t variant) {
+  Batch *b = get_batch(bh);
+  if (!b) return fail(TLM_E_BADARG, "bad batch handle");
+  if (variant < 1 || variant >= kNumVariants) return fail(TLM_E_BADARG, "batch variant must be a TMA variant (1..%d)", kNumVariants - 1);
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->variant = variant;
+  b->active.clear();  // forces a rebuild of the work lists
+  return TLM_OK;
+}
+
+int tlm_gpu_batch_run(int64_t bh, int32_t n_steps) {
+  Batch *b = get_batch(bh);
+  if (!b) return fail(TLM_E_BADARG, "bad batch handle");
+  if (n_steps < 0) return fail(TLM_E_BADARG, "negative step count");
+  CK(cudaSetDevice(b->device));
+  b->last_launches = 0;
+  b->last_cell_updates = 0;
+  CK(cudaEventRecord(b->ev0, b->stream));
+  int left = n_steps;
+  while (left > 0) {
+    std::vector<int> act;
+    int seg = left;
+    for (size_t i = 0; i < b->handles.size(); i++) {
+      Mesh *m = get(b->handles[i]);
+      const int rem = m->desc.n_timesteps - m->next_step + 1;
+      if (rem > 0) {
+        act.push_back((int)i);
+        seg = std::min(seg, rem);
+      }
+    }
+    if (act.empty()) break;
+    if (act != b->active) {
+      b->active = act;
+      int rc = b->fp64 ? build_batch_lists<double>(b) : build_batch_lists<float>(b);
+      if (rc) return rc;
+      if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+      }
+    }
+    if (!b->graph) {
+      int rc = batch_step_any(b, true);  // kernel attributes outside capture
+      if (rc) return rc;
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      const long long saved = b->last_launches;
+      rc = batch_step_any(b, false);
+      cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+      if (rc) return rc;
+      if (ce != cudaSuccess) return fail(TLM_E_CUDA, "batch graph capture: %s", cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&b->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) return fail(TLM_E_CUDA, "batch graph instantiate: %s", cudaGetErrorString(ce));
+      b->graph_launches = b->last_launches - saved;
+      b->last_launches = saved;
+    }
+    for (int k = 0; k < seg; k++) {
+      CK(cudaGraphLaunch(b->graph, b->stream));
+      b->last_launches += b->graph_launches;
+    }
+    for (int i : b->active) {
+      Mesh *m = get(b->handles[i]);
+      m->next_step += seg;
+      b->last_cell_updates += (long long)seg * m->desc.nx * m->desc.ny * m->desc.nz;
+    }
+    left -= seg;
+  }
+  CK(cudaEventRecord(b->ev1, b->stream));
+  return TLM_OK;
+}
+
+int tlm_gpu_batch_synchronize(int64_t bh) {
+  Batch *b = get_batch(bh);
+  if (!b) return fail(TLM_E_BADARG, "bad batch handle");
+  CK(cudaStreamSynchronize(b->stream));
+  int err = 0;
+  CK(cudaMemcpy(&err, b->err_d.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err == tlm::kErrTimeout) return fail(TLM_E_TIMEOUT, "a bulk-copy wait in the batched cell kernel timed out");
+  return TLM_OK;
+}
+
+int tlm_gpu_batch_last_run(int64_t bh, float *ms, int64_t *cell_updates, int64_t *launches) {
+  Batch *b = get_batch(bh);
+  if (!b) return fail(TLM_E_BADARG, "bad batch handle");
+  CK(cudaEventSynchronize(b->ev1));
+  float t = 0.f;
+  CK(cudaEventElapsedTime(&t, b->ev0, b->ev1));
+  if (ms) *ms = t;
+  if (cell_updates) *cell_updates = b->last_cell_updates;
+  if (launches) *launches = b->last_launches;
+  return TLM_OK;
+}
+
+int tlm_gpu_batch_destroy(int64_t bh) {
+  std::unique_ptr<Batch> b;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_batches.find(bh);
+    if (it == g_batches.end()) return fail(TLM_E_BADARG, "bad batch handle");
+    b = std::move(it->second);
+    g_batches.erase(it);
+  }
+  cudaStreamSynchronize(b->stream);
+  for (int64_t h : b->handles) {
+    Mesh *m = get(h);
+    if (m) m->batch_stream = nullptr;
+  }
   return TLM_OK;
 }
 

@@ -682,8 +682,10 @@ __device__ __forceinline__ void lds_vec(const T *p, T (&v)[VEC]) {
   else { v[0] = q.x; v[1] = q.y; }
 }
 
+// meshes == nullptr: one mesh (m0); otherwise a batch, tile.w indexes meshes[]
 template <typename T, int VEC, int TILE, int NSTAGE>
-__global__ void __launch_bounds__(TILE / VEC) tlm_bulk_tma_kernel(const MeshDev<T> m, const TileList tl, int rel_step) {
+__global__ void __launch_bounds__(TILE / VEC) tlm_bulk_tma_kernel(const MeshDev<T> m0, const MeshDev<T> *meshes,
+                                                                  const TileList tl, int rel_step) {
   using C = TmaCfg<T, VEC, TILE, NSTAGE>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T *stages = reinterpret_cast<T *>(smem_raw);
@@ -694,22 +696,26 @@ __global__ void __launch_bounds__(TILE / VEC) tlm_bulk_tma_kernel(const MeshDev<
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  const int t = *m.d_base + rel_step;
-  const T *__restrict__ in = (t & 1) ? m.links0 : m.links1;
-  T *__restrict__ out = (t & 1) ? m.links1 : m.links0;
-  const long long P = m.plane;
-  const long long dy = m.Px, dz = m.PxPy;
   const int first = blockIdx.x, stride = gridDim.x;
   int n_mine = (tl.n - first + stride - 1) / stride;
   if (n_mine < 0) n_mine = 0;
   // prologue: fill the ring
   if (tid == 0)
-    for (int s = 0; s < NSTAGE && s < n_mine; s++)
-      tma_issue<T, VEC, TILE, NSTAGE>(m, in, tl.tile[first + s * stride], stages + s * 12 * C::SEG, &bars[s]);
+    for (int s = 0; s < NSTAGE && s < n_mine; s++) {
+      const int4 tw = tl.tile[first + s * stride];
+      const MeshDev<T> &mw = meshes ? meshes[tw.w] : m0;
+      const int tt = *mw.d_base + rel_step;
+      tma_issue<T, VEC, TILE, NSTAGE>(mw, (tt & 1) ? mw.links0 : mw.links1, tw, stages + s * 12 * C::SEG, &bars[s]);
+    }
   for (int i = 0; i < n_mine; i++) {
     const int s = i % NSTAGE;
     const uint32_t parity = (uint32_t)((i / NSTAGE) & 1);
     const int4 tile = tl.tile[first + i * stride];
+    const MeshDev<T> &m = meshes ? meshes[tile.w] : m0;
+    const int t = *m.d_base + rel_step;
+    T *__restrict__ out = (t & 1) ? m.links1 : m.links0;
+    const long long P = m.plane;
+    const long long dy = m.Px, dz = m.PxPy;
     if (!mbar_wait_bounded(&bars[s], parity)) {
       if (tid == 0) atomicExch(tl.err, kErrTimeout);
       return;
@@ -825,8 +831,10 @@ __global__ void __launch_bounds__(TILE / VEC) tlm_bulk_tma_kernel(const MeshDev<
     __syncthreads();  // every thread is done reading stage s
     if (tid == 0 && i + NSTAGE < n_mine) {
       fence_proxy_async();
-      tma_issue<T, VEC, TILE, NSTAGE>(m, in, tl.tile[first + (i + NSTAGE) * stride], stages + s * 12 * C::SEG,
-                                      &bars[s]);
+      const int4 tw = tl.tile[first + (i + NSTAGE) * stride];
+      const MeshDev<T> &mw = meshes ? meshes[tw.w] : m0;
+      const int tt = *mw.d_base + rel_step;
+      tma_issue<T, VEC, TILE, NSTAGE>(mw, (tt & 1) ? mw.links0 : mw.links1, tw, stages + s * 12 * C::SEG, &bars[s]);
     }
   }
 }
@@ -837,9 +845,17 @@ __global__ void __launch_bounds__(TILE / VEC) tlm_bulk_tma_kernel(const MeshDev<
 // output scatter, reflected pulses + ghost slots.
 // ---------------------------------------------------------------------------
 template <typename T>
+__device__ __forceinline__ void special_body(const MeshDev<T> &m, int s, int rel_step);
+
+template <typename T>
 __global__ void __launch_bounds__(128) tlm_special_kernel(const MeshDev<T> m, int n_special, int rel_step) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_special) return;
+  special_body<T>(m, s, rel_step);
+}
+
+template <typename T>
+__device__ __forceinline__ void special_body(const MeshDev<T> &m, int s, int rel_step) {
   const int t = *m.d_base + rel_step;
   const T *__restrict__ in = (t & 1) ? m.links0 : m.links1;
   T *__restrict__ out = (t & 1) ? m.links1 : m.links0;
@@ -908,10 +924,42 @@ struct PmlList {
   int n, n_out_map;
 };
 
+__device__ __forceinline__ void bulk_prefetch_l2(const void *p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 template <typename T>
-__global__ void __launch_bounds__(128) tlm_pml_kernel(const MeshDev<T> m, const PmlList pl, int rel_step) {
+__device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl, int s, int rel_step);
+
+template <typename T>
+__global__ void __launch_bounds__(128) tlm_pml_kernel(const MeshDev<T> m, const PmlList pl, int rel_step,
+                                                      int prefetch_blocks) {
+  // one elected thread per block pulls the PML state of the block that runs
+  // prefetch_blocks later into L2 (24 contiguous 512-byte ranges + metadata),
+  // so that block's state loads hit L2.  Ranges are widened to 16-byte
+  // boundaries; the state and position buffers carry 64 bytes of padding so
+  // the widened ranges stay inside their allocations.
+  if (threadIdx.x == 0 && prefetch_blocks > 0) {
+    const long long s0 = (long long)(blockIdx.x + prefetch_blocks) * blockDim.x;
+    if (s0 < pl.n) {
+      const int cnt = (int)min((long long)blockDim.x, (long long)pl.n - s0);
+      const uint32_t sb = (uint32_t)(((cnt * (int)sizeof(typename PmlTypes<T>::state)) + 15) & ~15);
+      for (int k = 0; k < kPmlState; k++) {
+        const char *a = reinterpret_cast<const char *>(m.pml_state + (size_t)k * m.n_pml + s0);
+        const char *al = reinterpret_cast<const char *>(reinterpret_cast<uintptr_t>(a) & ~(uintptr_t)15);
+        bulk_prefetch_l2(al, sb + 16);
+      }
+      const char *pa = reinterpret_cast<const char *>(reinterpret_cast<uintptr_t>(pl.pos + s0) & ~(uintptr_t)15);
+      bulk_prefetch_l2(pa, (uint32_t)((cnt * 8 + 15) & ~15) + 16);
+    }
+  }
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= pl.n) return;
+  pml_body<T>(m, pl, s, rel_step);
+}
+
+template <typename T>
+__device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl, int s, int rel_step) {
   const int t = *m.d_base + rel_step;
   const T *__restrict__ in = (t & 1) ? m.links0 : m.links1;
   T *__restrict__ out = (t & 1) ? m.links1 : m.links0;
@@ -984,9 +1032,17 @@ struct FaceDev {
 };
 
 template <typename T>
+__device__ __forceinline__ void face_body(const MeshDev<T> &m, const FaceDev &fd, int f, int rel_step);
+
+template <typename T>
 __global__ void tlm_face_kernel(const MeshDev<T> m, const FaceDev fd, int rel_step) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= fd.n_faces) return;
+  face_body<T>(m, fd, f, rel_step);
+}
+
+template <typename T>
+__device__ __forceinline__ void face_body(const MeshDev<T> &m, const FaceDev &fd, int f, int rel_step) {
   const int t = *m.d_base + rel_step;
   T *R = (t & 1) ? m.links1 : m.links0;  // R_t just written by the cell kernel
   const long long P = m.plane;
@@ -1087,9 +1143,15 @@ struct DftDev {
   double2 *acc;             // [n_entries]
 };
 
+__device__ __forceinline__ void dft_body(const DftDev &d, const int *d_base, int k, int rel_step);
+
 __global__ void tlm_dft_kernel(const DftDev d, const int *d_base, int rel_step) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= d.n_entries) return;
+  dft_body(d, d_base, k, rel_step);
+}
+
+__device__ __forceinline__ void dft_body(const DftDev &d, const int *d_base, int k, int rel_step) {
   const int t = *d_base + rel_step;
   const int4 en = d.entry[k];
   const int face = en.z;
@@ -1113,6 +1175,64 @@ __global__ void tlm_dft_kernel(const DftDev d, const int *d_base, int rel_step) 
 
 __global__ void tlm_advance_base(int *d_base, int n) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *d_base += n;
+}
+
+// ---------------------------------------------------------------------------
+// Batched execution: many meshes (of one precision) advanced together.  Each
+// kernel walks a block list of (mesh, first item) pairs; block b does items
+// first..first+blockDim-1 of mesh b.x.  Per-mesh tables live in device arrays.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct BatchDev {
+  const MeshDev<T> *meshes;
+  const PmlList *pml;
+  const FaceDev *faces;
+  const DftDev *dfts;
+  const int *n_special;
+  const int2 *pml_blocks, *special_blocks, *face_blocks, *dft_blocks;
+  int n_pml_blocks, n_special_blocks, n_face_blocks, n_dft_blocks;
+  int *const *d_bases;  // step counter of each active mesh
+  int n_active;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(128) tlm_pml_batch_kernel(const BatchDev<T> b, int rel_step) {
+  const int2 w = b.pml_blocks[blockIdx.x];
+  const int s = w.y + threadIdx.x;
+  const PmlList &pl = b.pml[w.x];
+  if (s >= pl.n) return;
+  pml_body<T>(b.meshes[w.x], pl, s, rel_step);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) tlm_special_batch_kernel(const BatchDev<T> b, int rel_step) {
+  const int2 w = b.special_blocks[blockIdx.x];
+  const int s = w.y + threadIdx.x;
+  if (s >= b.n_special[w.x]) return;
+  special_body<T>(b.meshes[w.x], s, rel_step);
+}
+
+template <typename T>
+__global__ void tlm_face_batch_kernel(const BatchDev<T> b, int rel_step) {
+  const int2 w = b.face_blocks[blockIdx.x];
+  const int f = w.y + threadIdx.x;
+  const FaceDev &fd = b.faces[w.x];
+  if (f >= fd.n_faces) return;
+  face_body<T>(b.meshes[w.x], fd, f, rel_step);
+}
+
+template <typename T>
+__global__ void tlm_dft_batch_kernel(const BatchDev<T> b, int rel_step) {
+  const int2 w = b.dft_blocks[blockIdx.x];
+  const int k = w.y + threadIdx.x;
+  const DftDev &d = b.dfts[w.x];
+  if (k >= d.n_entries) return;
+  dft_body(d, b.meshes[w.x].d_base, k, rel_step);
+}
+
+__global__ void tlm_advance_batch(int *const *d_bases, int n_active, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_active) *d_bases[i] += n;
 }
 
 // Incident pulses of the next step in the reference layout V(12,nx,ny,nz):

@@ -199,6 +199,25 @@ int tlm_gpu_last_run_launches(int64_t handle, int64_t *launches);
 
 int tlm_gpu_destroy(int64_t handle);
 
+/* Batches (no counterpart in the reference, which runs one mesh per
+   process): advance many meshes of one precision together.  Every batch
+   step is one persistent TMA-staged launch over the concatenated tile lists
+   of all active meshes plus one launch each for their PML cells, other
+   special cells, special faces and DFT entries, captured once as a CUDA
+   graph and replayed.  Each mesh runs until its own n_timesteps; a mesh that
+   finishes drops out and the work lists are rebuilt.  Results are read per
+   mesh with the tlm_gpu_fetch_* calls (after tlm_gpu_batch_synchronize).
+   A mesh may belong to one batch at a time and must not be run on its own
+   while it does. */
+int tlm_gpu_batch_create(const int64_t *handles, int32_t n_meshes, int64_t *batch);
+int tlm_gpu_batch_set_variant(int64_t batch, int32_t variant);
+/* Advance every unfinished mesh by up to n_steps steps (asynchronous). */
+int tlm_gpu_batch_run(int64_t batch, int32_t n_steps);
+int tlm_gpu_batch_synchronize(int64_t batch);
+/* Device time, cell updates and kernel launches of the last batch run. */
+int tlm_gpu_batch_last_run(int64_t batch, float *ms, int64_t *cell_updates, int64_t *launches);
+int tlm_gpu_batch_destroy(int64_t batch);
+
 /* Message of the last failure on this thread (NUL-terminated, truncated
    to len-1 characters). */
 int tlm_gpu_last_error(char *buf, int32_t len);
