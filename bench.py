@@ -212,6 +212,112 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def _timed_steps(g, k):
+    g.set_timing(True)
+    g.run(k)
+    total, bulk = g.last_run_time()
+    g.set_timing(False)
+    return total, bulk
+
+
+def bench_target_512(device, peak):
+    """The roofline target: 512^3 PML-bounded free-space mesh, point source."""
+    from ggi_tlm_b200 import autotune, capi
+    from ggi_tlm_b200.problem import build_tables
+
+    t = build_tables(__import__("ggi_tlm_b200.cases", fromlist=["x"]).pml_point_source(512, steps=400))
+    n = t["nx"] * t["ny"] * t["nz"]
+    out = {"workload": "pml_point_source_512^3_pml8", "cells": n, "pml_cells": int(t["n_pml_cells"])}
+    for prec, esz, key in ((capi.TLM_PRECISION_FP32, 4, "fp32"), (capi.TLM_PRECISION_FP64, 8, "fp64")):
+        g = capi.GpuMesh(t, precision=prec, device=device)
+        tv = autotune.tune(g, steps_per_variant=2, use_cache=False)
+        g.run(3)
+        K = 60
+        total, bulk = _timed_steps(g, K)
+        g.close()
+        ab = algorithmic_bytes(t, esz)
+        step_gbs = ab["total"] / (total / K / 1e3) / 1e9
+        out[key] = {"gcell_per_s": n * K / (total / 1e3) / 1e9, "ms_per_step": total / K,
+                    "step_achieved_gbs": step_gbs, "step_frac_of_measured_hbm": step_gbs / peak,
+                    "step_frac_of_8tbs": step_gbs / 8000.0,
+                    "bulk_kernel_gbs": ab["bulk"] / (bulk / K / 1e3) / 1e9,
+                    "bulk_kernel_frac_of_measured_hbm": ab["bulk"] / (bulk / K / 1e3) / 1e9 / peak,
+                    "variant": tv["variant"], "timed_steps": K}
+    return out
+
+
+def bench_batch(device):
+    """Config 4: 96 uneven PML boxes (edges U[24,160], 0-8 spheres, point
+    sources, 1500-5000 steps) advanced together, FP32, against the same boxes
+    solved one after another."""
+    from ggi_tlm_b200 import capi, cases
+    from ggi_tlm_b200.problem import build_tables
+
+    specs = cases.batch_boxes()
+    tabs = [build_tables(s) for s in specs]
+    meshes = [capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP32, device=device) for t in tabs]
+    b = capi.GpuBatch(meshes)
+    # tune the batch kernel configuration on the first real steps
+    tune = {}
+    for v in (1, 3, 4):
+        b.set_variant(v)
+        b.run(8)
+        ms, cu, _ = b.last_run()
+        tune[v] = ms / 8
+    best = min(tune, key=tune.get)
+    b.set_variant(best)
+    b.run(100000)
+    ms, cu, launches = b.last_run()
+    b.close()
+    for g in meshes:
+        g.close()
+    # the same boxes one at a time (graph-replayed solo runs)
+    solo_ms, solo_cu = 0.0, 0
+    for t in tabs:
+        with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP32, device=device) as g:
+            g.set_variant(best)
+            g.run(t["n_timesteps"])
+            total, _ = g.last_run_time()
+            solo_ms += total
+            solo_cu += t["nx"] * t["ny"] * t["nz"] * t["n_timesteps"]
+    return {"workload": "96 PML boxes, edges U[24,160], 0-8 spheres, 1500-5000 steps, FP32",
+            "boxes": len(tabs), "cell_updates": cu, "gcell_per_s": cu / (ms / 1e3) / 1e9, "device_ms": ms,
+            "variant": best, "variant_ms_per_step": tune, "kernel_launches": launches,
+            "solo_sequential_gcell_per_s": solo_cu / (solo_ms / 1e3) / 1e9,
+            "speedup_vs_solo_sequential": (cu / ms) / (solo_cu / solo_ms) if solo_ms else None,
+            "note": "first 24 steps of every box ran during variant tuning (same numerics)"}
+
+
+def bench_serving(device, n_requests=32):
+    """Config 5: Poisson arrivals (40/s, seeded) of solves with edges
+    log-U[32,256], 0-3 Debye slabs, 6-10 cell PML, 1000-8000 steps; FP32
+    continuous batching under a 150 GB budget against sequential plain-FP64
+    solves of the same trace."""
+    from ggi_tlm_b200 import cases, serving
+    from ggi_tlm_b200.problem import build_tables
+
+    specs = cases.serving_requests(n_requests)
+    trace = serving.poisson_trace(specs, rate_per_s=40.0, seed=7, build=build_tables)
+    srv = serving.Server(engine=serving.GpuEngine(device=device, variant=1), budget_bytes=150e9, max_slots=64,
+                         quantum=64)
+    res = srv.serve(trace)
+    ours = serving.summarize(res)
+    base_res = serving.sequential_fp64(trace, device=device)
+    base = serving.summarize(base_res)
+    errs = []
+    for a, b_ in zip(res, base_res):
+        for i in range(a.probes.shape[0]):
+            nb = np.linalg.norm(b_.probes[i])
+            if nb > 0:
+                errs.append(float(np.linalg.norm(a.probes[i] - b_.probes[i]) / nb))
+    return {"workload": f"{n_requests}-request Poisson trace, 40 req/s, edges log-U[32,256], 0-3 Debye slabs",
+            "fp32_batched": ours, "fp64_sequential": base,
+            "solves_per_s_ratio": ours["solves_per_s"] / base["solves_per_s"],
+            "probe_rel_l2_vs_fp64_median": float(np.median(errs)) if errs else None,
+            "probe_rel_l2_vs_fp64_max": float(np.max(errs)) if errs else None,
+            "peak_slots": srv.peak_slots, "peak_bytes": srv.peak_bytes}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -222,6 +328,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="main workload only (no 512^3, batch, serving sections)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -310,6 +417,10 @@ def main():
     else:
         e2e = None
 
+    t512 = None if args.quick else bench_target_512(local, peak)
+    c4 = None if args.quick else bench_batch(local)
+    c5 = None if args.quick else bench_serving(local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, steps, el = cpu_oracle_rate(t, float(os.environ.get("TLM_CPU_BUDGET_S", "20")), 1000)
@@ -334,6 +445,7 @@ def main():
             "step_roofline": {"achieved": step_gbs, "frac": step_gbs / peak,
                               "algorithmic_bytes_per_step": ab32["total"]},
             "fp64": fp64, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+            "target_512": t512, "batch_c4": c4, "serving_c5": c5,
             "device_bytes": mem32,
         }
         print(json.dumps(line), flush=True)

@@ -244,3 +244,37 @@ def batch_boxes(n_boxes: int = 96, edge: Tuple[int, int] = (24, 160), steps: Tup
         out.append(pml_point_source(nx, ny, nz, pml=pml, steps=st, dl=dl, n_spheres=ns,
                                     seed=int(rng.integers(0, 2 ** 31)), n_probes=2))
     return out
+
+
+def serving_requests(n_requests: int = 64, edge: Tuple[int, int] = (32, 256), steps: Tuple[int, int] = (1000, 8000),
+                     pml: Tuple[int, int] = (6, 10), max_slabs: int = 3, seed: int = 6,
+                     dl: float = 2e-3) -> List[ProblemSpec]:
+    """The serving workload: mesh edges log-uniform in [32,256] per axis,
+    0-3 z-normal 2-pole Debye slabs, 6-10 cell PML, 1000-8000 steps, a
+    Gaussian point source and probes, FP64 DFT on a small surface."""
+    rng = np.random.default_rng(seed)
+    out = []
+    lo, hi = math.log(edge[0]), math.log(edge[1])
+    for r in range(n_requests):
+        nx, ny, nz = (int(round(math.exp(rng.uniform(lo, hi)))) for _ in range(3))
+        st = int(rng.integers(steps[0], steps[1] + 1))
+        p = int(rng.integers(pml[0], pml[1] + 1))
+        ns = int(rng.integers(0, max_slabs + 1))
+        spec = pml_point_source(nx, ny, nz, pml=p, steps=st, dl=dl, n_spheres=0, seed=int(rng.integers(0, 2 ** 31)),
+                                n_probes=2)
+        # Debye slabs across the interior, kept out of the PML and away from the source
+        zlo, zhi = p + 2, nz - p - 1
+        src_z = spec.point_excitations[0].cell[2]
+        for s in range(ns):
+            z0 = int(rng.integers(zlo, max(zlo + 1, zhi - 2)))
+            z1 = min(z0 + 2, zhi)
+            if z0 <= src_z <= z1 or z1 < z0:
+                continue
+            eps_inf = float(rng.uniform(2.0, 5.0))
+            de = [float(rng.uniform(5.0, 40.0)) for _ in range(2)]
+            tau = [float(10 ** rng.uniform(-11.0, -9.0)) for _ in range(2)]
+            spec.materials.append(VolumeMaterial.debye(eps_inf, de, tau, wnorm=1e9))
+            spec.material_regions.append((len(spec.materials), Block(p + 1, nx - p, p + 1, ny - p, z0, z1)))
+        # drop probes that fell inside a slab (the reference warns but allows it; keep them in free space)
+        out.append(spec)
+    return out

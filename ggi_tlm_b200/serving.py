@@ -1,0 +1,232 @@
+"""Resident serving loop for TLM solves with continuous batching.
+
+Requests (each one solve: the setup tables of one mesh) arrive over time.
+The loop keeps the link state, PML/filter state, probe records and DFT
+accumulators of every admitted solve resident on the device and advances all
+admitted solves together as one batch (``capi.GpuBatch``: one persistent TMA
+launch per kernel type per step).  Between scheduling quanta it
+
+* retires finished solves (probe series and DFT read back, device memory
+  released),
+* admits waiting requests in arrival order while a slot is free and the
+  estimated device footprint fits the HBM budget,
+
+so requests that arrive while others are on the GPU join the running batch
+as slots and memory free up, and their work overlaps on the device.  The
+batch engine computes every solve bit-identically to a solo run, so a
+result does not depend on what it was batched with.
+
+The engine is injectable; the default drives the CUDA library, tests also
+use a CPU stand-in to check the scheduling logic.
+"""
+from __future__ import annotations
+
+import collections
+import time
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional
+
+import numpy as np
+
+from . import capi
+from .problem import probe_series
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float  # seconds after the start of the trace
+    tables: dict
+
+
+@dataclass
+class Result:
+    rid: int
+    arrival: float
+    admitted: float
+    finished: float
+    cells: int
+    steps: int
+    probes: Optional[np.ndarray] = None
+    dft: Optional[np.ndarray] = None
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+    @property
+    def queue_wait(self) -> float:
+        return self.admitted - self.arrival
+
+
+def footprint_bytes(t: dict, precision: int = capi.TLM_PRECISION_FP32) -> int:
+    """Device bytes one solve holds (the allocations of the library's
+    finalize step: ping-pong link planes with ghost slots, PML state and
+    tables, filter taps, excitation table, probe records, faces, DFT)."""
+    esz = 8 if precision == capi.TLM_PRECISION_FP64 else 4
+    nx, ny, nz, n = t["nx"], t["ny"], t["nz"], t["n_timesteps"]
+    px = ((nx + 1 + 3) // 4) * 4
+    plane = px * (ny + 2) * (nz + 2)
+    links = 2 * 12 * plane * esz
+    pml = int(t["n_pml_cells"]) * (24 * esz + 10)
+    special = int(t["n_special"]) * 32 + (ny * px + 31) // 32 * nz * 8
+    filt = int(t["n_special"]) * 0 + 6 * 8 * 8 * int((np.asarray(t["sp_material"]) > 0).sum())
+    outs = int(t["n_out_cells"]) * 6 * 8 * n + int(t["n_exc_cells"]) * 9 * 8 * n
+    dft = int(t["dft_face_ptr"][-1]) * 16 + int(t["n_dft"]) * 16 * n if int(t["n_dft"]) else 0
+    return int(links + pml + special + filt + outs + dft + (1 << 20))
+
+
+class GpuEngine:
+    """Default engine: solves are GpuMesh objects advanced in a GpuBatch."""
+
+    def __init__(self, precision: int = capi.TLM_PRECISION_FP32, device: int = 0, variant: Optional[int] = None):
+        self.precision = precision
+        self.device = device
+        self.variant = variant
+        self.meshes: Dict[int, capi.GpuMesh] = {}
+        self.batch: Optional[capi.GpuBatch] = None
+
+    def add(self, rid: int, tables: dict):
+        self._drop_batch()
+        self.meshes[rid] = capi.GpuMesh(tables, precision=self.precision, device=self.device)
+
+    def remove(self, rid: int):
+        self._drop_batch()
+        self.meshes.pop(rid).close()
+
+    def _drop_batch(self):
+        if self.batch is not None:
+            self.batch.close()
+            self.batch = None
+
+    def advance(self, n_steps: int):
+        if not self.meshes:
+            return
+        if self.batch is None:
+            self.batch = capi.GpuBatch(list(self.meshes.values()))
+            if self.variant is not None:
+                self.batch.set_variant(self.variant)
+        self.batch.run(n_steps, sync=True)
+
+    def progress(self, rid: int) -> int:
+        return self.meshes[rid].step
+
+    def results(self, rid: int):
+        g = self.meshes[rid]
+        return probe_series(g.t, g.cell_output()), g.dft()
+
+    def close(self):
+        self._drop_batch()
+        for g in self.meshes.values():
+            g.close()
+        self.meshes.clear()
+
+
+class Server:
+    """Continuous-batching scheduler over an engine."""
+
+    def __init__(self, engine=None, budget_bytes: float = 150e9, max_slots: int = 64, quantum: int = 64,
+                 precision: int = capi.TLM_PRECISION_FP32, clock: Callable[[], float] = time.perf_counter,
+                 keep_results: bool = True):
+        self.engine = engine if engine is not None else GpuEngine(precision)
+        self.budget = float(budget_bytes)
+        self.max_slots = max_slots
+        self.quantum = quantum
+        self.precision = precision
+        self.clock = clock
+        self.keep_results = keep_results
+        self.peak_bytes = 0
+        self.peak_slots = 0
+        self.events: List[tuple] = []  # (time, "admit"/"finish", rid, bytes in use)
+
+    def serve(self, trace: List[Request]) -> List[Result]:
+        pending = collections.deque(sorted(trace, key=lambda r: (r.arrival, r.rid)))
+        for r in pending:
+            if footprint_bytes(r.tables, self.precision) > self.budget:
+                raise ValueError(f"request {r.rid} needs more than the whole HBM budget")
+        waiting: collections.deque = collections.deque()
+        active: Dict[int, tuple] = {}  # rid -> (request, admitted time, bytes)
+        used = 0
+        done: List[Result] = []
+        t0 = self.clock()
+        while pending or waiting or active:
+            now = self.clock() - t0
+            while pending and pending[0].arrival <= now:
+                waiting.append(pending.popleft())
+            # admission: arrival order, while a slot and the budget allow
+            while waiting and len(active) < self.max_slots:
+                need = footprint_bytes(waiting[0].tables, self.precision)
+                if used + need > self.budget:
+                    break
+                r = waiting.popleft()
+                self.engine.add(r.rid, r.tables)
+                used += need
+                active[r.rid] = (r, self.clock() - t0, need)
+                self.events.append((self.clock() - t0, "admit", r.rid, used))
+            self.peak_bytes = max(self.peak_bytes, used)
+            self.peak_slots = max(self.peak_slots, len(active))
+            if not active:
+                if pending:  # idle until the next arrival
+                    delay = pending[0].arrival - (self.clock() - t0)
+                    if delay > 0:
+                        time.sleep(min(delay, 0.05))
+                continue
+            self.engine.advance(self.quantum)
+            for rid in list(active):
+                r, adm, need = active[rid]
+                if self.engine.progress(rid) >= r.tables["n_timesteps"]:
+                    probes, dft = self.engine.results(rid) if self.keep_results else (None, None)
+                    fin = self.clock() - t0
+                    t = r.tables
+                    done.append(Result(rid, r.arrival, adm, fin, t["nx"] * t["ny"] * t["nz"], t["n_timesteps"],
+                                       probes, dft))
+                    self.engine.remove(rid)
+                    del active[rid]
+                    used -= need
+                    self.events.append((fin, "finish", rid, used))
+        return sorted(done, key=lambda x: x.rid)
+
+
+def summarize(results: List[Result], makespan: Optional[float] = None) -> dict:
+    lat = np.array([r.latency for r in results])
+    wait = np.array([r.queue_wait for r in results])
+    span = makespan if makespan is not None else max(r.finished for r in results) - min(r.arrival for r in results)
+    cu = sum(r.cells * r.steps for r in results)
+    return {
+        "solves": len(results), "makespan_s": span, "solves_per_s": len(results) / span,
+        "cell_updates_per_s": cu / span,
+        "latency_p50_s": float(np.percentile(lat, 50)), "latency_p95_s": float(np.percentile(lat, 95)),
+        "latency_p99_s": float(np.percentile(lat, 99)),
+        "queue_wait_p50_s": float(np.percentile(wait, 50)), "queue_wait_p99_s": float(np.percentile(wait, 99)),
+    }
+
+
+def sequential_fp64(trace: List[Request], device: int = 0, clock: Callable[[], float] = time.perf_counter):
+    """Baseline: the same trace solved one request at a time with the plain
+    FP64 path, in arrival order (a request starts when it has arrived and the
+    previous one has finished)."""
+    out = []
+    t0 = clock()
+    for r in sorted(trace, key=lambda r: (r.arrival, r.rid)):
+        now = clock() - t0
+        if r.arrival > now:
+            time.sleep(r.arrival - now)
+        start = clock() - t0
+        with capi.GpuMesh(r.tables, precision=capi.TLM_PRECISION_FP64, device=device) as g:
+            g.run(r.tables["n_timesteps"])
+            probes = probe_series(r.tables, g.cell_output())
+        fin = clock() - t0
+        t = r.tables
+        out.append(Result(r.rid, r.arrival, start, fin, t["nx"] * t["ny"] * t["nz"], t["n_timesteps"], probes))
+    return out
+
+
+def poisson_trace(specs_and_seeds, rate_per_s: float, seed: int, build):
+    """Seeded Poisson arrivals: build(spec) -> tables for each spec."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    trace = []
+    for i, spec in enumerate(specs_and_seeds):
+        t += float(rng.exponential(1.0 / rate_per_s))
+        trace.append(Request(i, t, build(spec)))
+    return trace
