@@ -77,10 +77,40 @@ def kat_material_stability() -> ProblemSpec:
         outputs=[OutputPoint((11, 11, 11), "Ey")])
 
 
+def point_to_cell(p: float, xmin: float, dl: float) -> int:
+    """MESH/general_mesh_subroutines.F90:345-383, int((p-xmin)/dl)+1, with the
+    division evaluated as a multiplication by 1/dl, as the reference's build
+    flags (-funsafe-math-optimizations, make_configuration_data:39) compile
+    it.  The distinction matters for points on cell boundaries; the
+    MATERIAL_TEST2 golden series pins it."""
+    return int((p - xmin) * (1.0 / dl)) + 1
+
+
+def kat_material_test2() -> ProblemSpec:
+    """TEST_DATA/MATERIAL_TEST2/PROBLEM_SPECIFICATION_FILES/mat_test.inp: 60^3
+    cells over 6 mm, a 1 mm cube of a Lorentz material (mur_lorentz.vmat: the
+    same 2nd-order rational for eps_r and mu_r, complex poles), soft Ex
+    Gaussian point source and an Ex probe 2.4 mm apart, R=0."""
+    xmin, xmax, n = -3.0e-3, 3.0e-3, 60
+    dlx = (xmax - xmin) / float(n)
+    dl = (dlx + dlx + dlx) / 3.0  # set_mesh_parameters.F90:61-66
+    steps = nint(10e-10 / _dt(dl))
+    f = Sfilter(1e10, [2.0, 3.1827e-1, 4.0518e-1], [1.0, 3.1827e-1, 4.0518e-1])
+    lorentz = VolumeMaterial(MAT_DISPERSIVE, f, 0.0, Sfilter(f.wnorm, list(f.a), list(f.b)), 0.0)
+    c = lambda p: point_to_cell(p, xmin, dl)  # noqa: E731
+    return ProblemSpec(
+        nx=n, ny=n, nz=n, dl=dl, n_timesteps=steps, R=(0.0,) * 6, origin=(xmin,) * 3,
+        materials=[lorentz], material_regions=[(1, Block(26, 35, 26, 35, 26, 35))],
+        functions=[ExcitationFunction("gaussian", (1.0, 1e-10, 3e-10))],
+        point_excitations=[PointExcitation((c(1.2e-3), c(0.0), c(0.0)), "Ex", 1)],
+        outputs=[OutputPoint((c(-1.2e-3), c(0.0), c(0.0)), "Ex")])
+
+
 KAT_CASES = {
     "tem_pml_Ey": kat_tem_pml,
     "tem_material_Ey": kat_tem_material,
     "material_stability_Ey": kat_material_stability,
+    "material_test2_Ex": kat_material_test2,
 }
 
 

@@ -18,6 +18,7 @@ CASES = {
     "tem_pml_Ey": "TEM_PML_TEST/PROBLEM_SPECIFICATION_FILES/Ey.tout_ref",
     "tem_material_Ey": "TEM_MATERIAL_TEST/PROBLEM_SPECIFICATION_FILES/Ey.tout_ref",
     "material_stability_Ey": "MATERIAL_STABILITY_TEST/PROBLEM_SPECIFICATION_FILES/cavity.field.tout_ref",
+    "material_test2_Ex": "MATERIAL_TEST2/PROBLEM_SPECIFICATION_FILES/mat_test.field.tout_ref",
 }
 
 

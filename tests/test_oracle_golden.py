@@ -59,3 +59,15 @@ def test_oracle_step_split_is_identical():
     cb = b.run(60)
     assert np.array_equal(ca, cb)
     assert np.array_equal(a.dft(), b.dft())
+
+
+def test_point_mapping_uses_reciprocal_multiply():
+    """The MATERIAL_TEST2 source sits 4.2 mm from xmin, exactly on a cell
+    boundary of 0.1 mm cells: int(4.2e-3/1e-4) is 41 but int(4.2e-3*(1/1e-4))
+    is 42, and only the second one (cell 43) reproduces the golden series."""
+    xmin, dl = -3.0e-3, (6.0e-3 / 60 * 3) / 3.0
+    assert int((1.2e-3 - xmin) / dl) + 1 == 42
+    assert cases.point_to_cell(1.2e-3, xmin, dl) == 43
+    spec = cases.kat_material_test2()
+    assert spec.point_excitations[0].cell == (43, 31, 31)
+    assert spec.outputs[0].cell == (19, 31, 31)
