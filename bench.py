@@ -35,6 +35,29 @@ UNIT = "Gcell-updates/s"
 FALLBACK_HBM_GBS = 6650.0
 
 
+# Bulk (free-space) cell-kernel configurations of the library, by variant
+# index: (cells per tile, staging depth) for FP32 and FP64; 0 = the
+# register-pipelined kernel without TMA staging.
+BULK_VARIANTS = [(0, 0, 0, 0), (1024, 2, 512, 2), (512, 3, 256, 3), (512, 4, 256, 4), (1024, 3, 512, 3),
+                 (256, 6, 128, 6)]
+
+# DRAM bytes per launch of the bulk kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum) from one ncu --set full capture of the same workload.
+NCU_TRAFFIC = {
+    "pml_spheres_256^3_pml8_32spheres_huygens_dft64x64x64": {
+        "bytes": 756.039168e6 + 608.934400e6,
+        "source": "profiles/tlm_bulk_tma_kernel_pml_spheres_256_fp32.md (tlm_bulk_tma_kernel<float,4,512,3>)"},
+}
+
+
+def bulk_kernel_name(variant: int, vec: int) -> str:
+    t32, s32, t64, s64 = BULK_VARIANTS[variant]
+    if variant == 0:
+        return f"tlm_cell_kernel<{'float' if vec == 4 else 'double'},{vec}>"
+    tile, st = (t32, s32) if vec == 4 else (t64, s64)
+    return f"tlm_bulk_tma_kernel<{'float' if vec == 4 else 'double'},{vec},{tile},{st}>"
+
+
 def measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -136,18 +159,26 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+def dist_env():
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def dist_setup(backend: str = ""):
+    """One process per GPU (torchrun env).  NCCL on GPUs; gloo when no GPU is
+    visible (the host-side replica logic is tested that way)."""
+    world, rank, local = dist_env()
     if world > 1:
         import datetime
 
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if not backend:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local
 
 
@@ -164,9 +195,18 @@ def max_over_ranks(x: float, world: int) -> float:
     import torch
     import torch.distributed as dist
 
-    v = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    v = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(v, op=dist.ReduceOp.MAX)
     return float(v.item())
+
+
+def replica_rate(cells: int, steps: int, world: int, local_ms: float) -> tuple:
+    """Whole-job rate of ``world`` replicas that each advance ``cells`` for
+    ``steps``: total cell updates / the slowest rank's time.  Returns
+    (Gcell-updates/s, max ms)."""
+    ms = max_over_ranks(local_ms, world)
+    return cells * steps * world / (ms / 1e3) / 1e9, ms
 
 
 def cpu_oracle_rate(t, budget_s: float, max_steps: int):
@@ -330,10 +370,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--quick", action="store_true", help="main workload only (no 512^3, batch, serving sections)")
     args = ap.parse_args()
-    world, rank, local = dist_setup()
-    if args.impl == "reference":
+    if args.impl == "reference":  # rank 0 alone; no process group, no collective
+        world, rank, _ = dist_env()
         run_reference_arm(args, world, rank)
         return
+    world, rank, local = dist_setup()
 
     from ggi_tlm_b200 import autotune, build, capi
     from ggi_tlm_b200.problem import build_tables, probe_series
@@ -374,8 +415,7 @@ def main():
         return total_ms, bulk_ms, launches, clocks, probes, mem
 
     total32, bulk32, launches, clocks, p32, mem32 = timed_run(capi.TLM_PRECISION_FP32, not args.no_fp64)
-    ms_max = max_over_ranks(total32, world)
-    value = n * K * world / (ms_max / 1e3) / 1e9
+    value, ms_max = replica_rate(n, K, world, total32)
     ab32 = algorithmic_bytes(t, 4)
     bulk_gbs = ab32["bulk"] / (bulk32 / K / 1e3) / 1e9
     step_gbs = ab32["total"] / (total32 / K / 1e3) / 1e9
@@ -386,7 +426,7 @@ def main():
         ab64 = algorithmic_bytes(t, 8)
         norms = [np.linalg.norm(p64[i]) for i in range(len(p64))]
         rel = max(np.linalg.norm(p32[i] - p64[i]) / norms[i] for i in range(len(p64)) if norms[i] > 0)
-        fp64 = {"value": n * K * world / (max_over_ranks(total64, world) / 1e3) / 1e9, "unit": UNIT,
+        fp64 = {"value": replica_rate(n, K, world, total64)[0], "unit": UNIT,
                 "ms_per_step": total64 / K,
                 "step_achieved_gbs": ab64["total"] / (total64 / K / 1e3) / 1e9,
                 "step_frac_of_measured_hbm": ab64["total"] / (total64 / K / 1e3) / 1e9 / peak,
@@ -417,9 +457,10 @@ def main():
     else:
         e2e = None
 
-    t512 = None if args.quick else bench_target_512(local, peak)
-    c4 = None if args.quick else bench_batch(local)
-    c5 = None if args.quick else bench_serving(local)
+    sections = not args.quick and world == 1  # per-GPU sections, reported at N=1
+    t512 = bench_target_512(local, peak) if sections else None
+    c4 = bench_batch(local) if sections else None
+    c5 = bench_serving(local) if sections else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -437,9 +478,11 @@ def main():
                        "bulk_variant_fp32": tuned[capi.TLM_PRECISION_FP32]["variant"],
                        "bulk_variant_fp64": tuned.get(capi.TLM_PRECISION_FP64, {}).get("variant"),
                        "l2": "state (%.2f GB) larger than L2 (126 MB)" % (ab32["total"] / 1e9)},
-            "roofline": {"bound": "hbm", "kernel": "tlm_cell_kernel<float,4>", "achieved": bulk_gbs, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": bulk_kernel_name(tuned[capi.TLM_PRECISION_FP32]["variant"], 4),
+                         "achieved": bulk_gbs, "peak": peak,
                          "unit": "GB/s", "frac": bulk_gbs / peak, "peak_kind": peak_kind,
-                         "traffic": None,
+                         "traffic": NCU_TRAFFIC.get(wname, {}).get("bytes"),
+                         "traffic_source": NCU_TRAFFIC.get(wname, {}).get("source"),
                          "algorithmic_bytes_per_launch": ab32["bulk"],
                          "avg_launch_ms": bulk32 / K},
             "step_roofline": {"achieved": step_gbs, "frac": step_gbs / peak,
