@@ -24,6 +24,7 @@ TLM_PRECISION_FP32 = 32
 TLM_PRECISION_FP64 = 64
 MAX_ORDER = 8
 
+TLM_OK, TLM_E_BADARG, TLM_E_UNSUPPORTED, TLM_E_OOM, TLM_E_CUDA, TLM_E_STATE, TLM_E_TIMEOUT = 0, -1, -2, -3, -4, -5, -6
 ERRORS = {-1: "TLM_E_BADARG", -2: "TLM_E_UNSUPPORTED", -3: "TLM_E_OOM", -4: "TLM_E_CUDA", -5: "TLM_E_STATE",
           -6: "TLM_E_TIMEOUT"}
 
@@ -36,6 +37,7 @@ EXPORTS = [
     "tlm_gpu_last_run_launches", "tlm_gpu_destroy", "tlm_gpu_last_error", "tlm_gpu_set_variant",
     "tlm_gpu_num_variants", "tlm_gpu_fetch_links_noalloc", "tlm_gpu_batch_create", "tlm_gpu_batch_set_variant",
     "tlm_gpu_batch_run", "tlm_gpu_batch_synchronize", "tlm_gpu_batch_last_run", "tlm_gpu_batch_destroy",
+    "tlm_gpu_set_small_to_zero",
 ]
 
 
@@ -76,6 +78,7 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_faces": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, i32, i32],
         "tlm_gpu_set_huygens": [i64, i32, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double, C.c_double, i32],
         "tlm_gpu_set_outputs": [i64, i32],
+        "tlm_gpu_set_small_to_zero": [i64, i32, C.c_double],
         "tlm_gpu_set_dft": [i64, i32, _f64p, _i32p, _i32p, _i32p, _i32p],
         "tlm_gpu_run": [i64, i32, i32],
         "tlm_gpu_synchronize": [i64],
@@ -190,6 +193,8 @@ class GpuMesh:
             df = [_f64(t["dft_freq"]), _i32(t["dft_comp"]), _i32(t["dft_face_ptr"]), _i32(t["dft_face_out"]),
                   _i32(t["dft_face_side"])]
             _check(lib.tlm_gpu_set_dft(self.h, int(t["n_dft"]), *[_p(x) for x in df]))
+        if int(t.get("n_small_to_zero", 0)):
+            _check(lib.tlm_gpu_set_small_to_zero(self.h, int(t["n_small_to_zero"]), float(t["small_to_zero_value"])))
 
     # -- time stepping -----------------------------------------------------
     def run(self, n_steps: int, sync: bool = True):

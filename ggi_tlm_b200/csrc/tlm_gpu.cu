@@ -110,6 +110,8 @@ struct Mesh {
   int tiles_tile = 0;  // TILE the current list was built for
   int n_tiles = 0;
   bool dry_launch = false;
+  int small_every = 0;       // set_small_to_zero: period in steps (0 = off)
+  double small_value = 0.0;
   int pml_prefetch = 1200;  // blocks ahead for the PML state L2 prefetch (0 = off)
 
   // graph of kGraphSteps steps
@@ -631,6 +633,10 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
   const tlm::FaceDev fd = face_dev(m);
   const tlm::DftDev dd = dft_dev(m);
   for (int k = 0; k < n; k++) {
+    if (m->small_every > 0) {
+      tlm::tlm_flush_small_kernel<T><<<4 * m->n_sms, 256, 0, m->stream>>>(md, k, m->small_every, m->small_value);
+      m->last_launches++;
+    }
     if (kev) cudaEventRecord(kev[2 * k], m->stream);
     int rc = launch_bulk<T, VEC>(m, md, k);
     if (rc) return rc;
@@ -880,6 +886,16 @@ int tlm_gpu_set_outputs(int64_t h, int32_t n_out_cells) {
   if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
   if (n_out_cells < 0) return fail(TLM_E_BADARG, "negative output count");
   m->n_out_cells = n_out_cells;
+  return TLM_OK;
+}
+
+int tlm_gpu_set_small_to_zero(int64_t h, int32_t n_small, double small) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n_small < 0 || !(small >= 0.0)) return fail(TLM_E_BADARG, "set_small_to_zero needs n >= 0 and value >= 0");
+  m->small_every = n_small;
+  m->small_value = small;
   return TLM_OK;
 }
 
@@ -1256,6 +1272,16 @@ int launch_batch_tma(Batch *b, bool dry) {
 template <typename T, int VEC>
 int batch_step(Batch *b, bool dry) {
   int rc = TLM_OK;
+  if (!dry) {
+    for (int i : b->active) {  // set_small_to_zero of the members that ask for it
+      Mesh *m = get(b->handles[i]);
+      if (m && m->small_every > 0) {
+        tlm::tlm_flush_small_kernel<T><<<4 * m->n_sms, 256, 0, b->stream>>>(mesh_dev<T>(m), 0, m->small_every,
+                                                                           m->small_value);
+        b->last_launches++;
+      }
+    }
+  }
   if constexpr (sizeof(T) == 4) {
     switch (b->variant) {
       case 1: rc = launch_batch_tma<T, VEC, 1024, 2>(b, dry); break;

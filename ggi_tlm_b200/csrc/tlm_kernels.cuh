@@ -1235,6 +1235,37 @@ __global__ void tlm_advance_batch(int *const *d_bases, int n_active, int n) {
   if (i < n_active) *d_bases[i] += n;
 }
 
+// TLM_set_small_to_zero (TLM_SOLVER/TLM_set_small_to_zero.F90:34-68), called
+// before the excitation of every timestep that is a multiple of `every`
+// (run_TLM.F90:236-238): incident pulses with |V| < small become 0.  Every
+// slot of the buffer that step t reads holds exactly one cell's incident
+// pulse (a neighbour's reflection, a face update written in place, or R times
+// the cell's own reflection in a ghost slot), so the flush runs element-wise
+// over that buffer; slots that no cell reads are padding.  The step number
+// comes from the device counter, so the launch can sit in a replayed graph.
+template <typename T>
+__global__ void tlm_flush_small_kernel(const MeshDev<T> m, int rel_step, int every, double small) {
+  const int t = *m.d_base + rel_step;
+  if (t % every != 0) return;
+  T *R = (t & 1) ? m.links0 : m.links1;  // written by step t-1
+  const long long n4 = 12 * m.plane * (long long)sizeof(T) / 16;  // plane is a multiple of 4 elements
+  uint4 *q = reinterpret_cast<uint4 *>(R);
+  constexpr int E = 16 / sizeof(T);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+    uint4 w = q[i];
+    T v[E];
+    memcpy(v, &w, 16);
+    bool hit = false;
+#pragma unroll
+    for (int e = 0; e < E; e++)
+      if (fabs(double(v[e])) < small) { hit = hit || v[e] != T(0); v[e] = T(0); }
+    if (hit) {
+      memcpy(&w, v, 16);
+      q[i] = w;
+    }
+  }
+}
+
 // Incident pulses of the next step in the reference layout V(12,nx,ny,nz):
 // the same gather as the cell kernel, from the last written buffer.
 template <typename T>

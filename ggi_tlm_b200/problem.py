@@ -425,6 +425,8 @@ class ProblemSpec:
     outputs: List[OutputPoint] = field(default_factory=list)
     dft_surfaces: List[DFTSurface] = field(default_factory=list)
     reduced_c: float = 1.0
+    # set_small_to_zero packet (read_small_to_zero.F90:55-59): (n_small_to_zero, small_to_zero_value)
+    small_to_zero: Optional[Tuple[int, float]] = None
     # features rejected up front by the GPU path
     cables: int = 0
     ngspice: bool = False
@@ -778,6 +780,10 @@ def build_tables(spec: ProblemSpec) -> dict:
     tables.update(n_dft=len(freqs), dft_freq=np.array(freqs, dtype=np.float64),
                   dft_comp=np.array(comps, dtype=np.int32), dft_face_ptr=np.array(ptr, dtype=np.int32),
                   dft_face_out=np.array(fo, dtype=np.int32), dft_face_side=np.array(fs, dtype=np.int32))
+    n_small, small = spec.small_to_zero if spec.small_to_zero else (0, 0.0)
+    if n_small < 0 or small < 0.0:
+        raise ValueError("set_small_to_zero needs n >= 0 and a value >= 0")
+    tables.update(n_small_to_zero=int(n_small), small_to_zero_value=float(small))
     return tables
 
 

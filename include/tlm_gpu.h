@@ -135,6 +135,13 @@ int tlm_gpu_set_outputs(int64_t handle, int32_t n_out_cells);
 int tlm_gpu_set_dft(int64_t handle, int32_t n_surfaces, const double *frequency, const int32_t *component,
                     const int32_t *face_ptr, const int32_t *face_out, const int32_t *face_code);
 
+/* set_small_to_zero packet (SRC/PROCESS_INPUT_FILE/read_small_to_zero.F90:
+   55-59): before the excitation of every timestep that is a multiple of
+   n_small_to_zero, incident link pulses with |V| < small_to_zero_value
+   become 0 (SRC/TLM_SOLVER/TLM_set_small_to_zero.F90:34-68, called at
+   run_TLM.F90:236-238).  n_small_to_zero = 0 switches it off (the default). */
+int tlm_gpu_set_small_to_zero(int64_t handle, int32_t n_small_to_zero, double small_to_zero_value);
+
 /* Advance timesteps first_step..first_step+n_steps-1 (1-based, run_TLM
    numbering, SRC/TLM_SOLVER/run_TLM.F90:191-295).  Steps must be
    contiguous across calls.  Asynchronous on the library stream. */

@@ -674,11 +674,24 @@ static void dft_surfaces(tlm_oracle_state *s, double time) {
 }
 
 /* run_TLM.F90:191-295 for timesteps first..first+n-1 */
+/* TLM_set_small_to_zero (TLM_SOLVER/TLM_set_small_to_zero.F90:34-68): the 12
+   incident pulses of every cell with |V| below the threshold become 0 */
+static void set_small_to_zero(tlm_oracle_state *s) {
+  const double small = s->p.small_to_zero_value;
+  for (int cz = 1; cz <= s->nz; cz++)
+    for (int cy = 1; cy <= s->ny; cy++)
+      for (int cx = 1; cx <= s->nx; cx++)
+        for (int port = 0; port < 12; port++)
+          if (fabs(V_(port, cx, cy, cz)) < small) V_(port, cx, cy, cz) = 0.0;
+}
+
 int tlm_oracle_run(tlm_oracle_state *s, int32_t first_step, int32_t n_steps, double *cell_out) {
   const tlm_oracle_problem *p = &s->p;
   if (first_step != s->timestep + 1) return -10;
   for (int k = 0; k < n_steps; k++) {
     int timestep = first_step + k;
+    /* run_TLM.F90:236-238, before the excitation of the step */
+    if (p->n_small_to_zero > 0 && timestep % p->n_small_to_zero == 0) set_small_to_zero(s);
     double time = (timestep - 1) * p->dt;
     excitation(s, timestep);
     int rc = scatter(s);

@@ -98,6 +98,11 @@ typedef struct {
   const int32_t *dft_face_ptr; /* CSR [n_dft+1] into dft_face_out / dft_face_side */
   const int32_t *dft_face_out; /* 1-based output face number */
   const int32_t *dft_face_side;/* 1..6 face code (face_xmin..face_zmax) */
+
+  /* set_small_to_zero (read_small_to_zero.F90:55-59): every n_small_to_zero
+     timesteps, |V| < small_to_zero_value -> 0; n_small_to_zero 0 = off */
+  int32_t n_small_to_zero;
+  double small_to_zero_value;
 } tlm_oracle_problem;
 
 typedef struct tlm_oracle_state tlm_oracle_state;
