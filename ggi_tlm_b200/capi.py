@@ -37,7 +37,7 @@ EXPORTS = [
     "tlm_gpu_last_run_launches", "tlm_gpu_destroy", "tlm_gpu_last_error", "tlm_gpu_set_variant",
     "tlm_gpu_num_variants", "tlm_gpu_fetch_links_noalloc", "tlm_gpu_batch_create", "tlm_gpu_batch_set_variant",
     "tlm_gpu_batch_run", "tlm_gpu_batch_synchronize", "tlm_gpu_batch_last_run", "tlm_gpu_batch_destroy",
-    "tlm_gpu_set_small_to_zero",
+    "tlm_gpu_set_small_to_zero", "tlm_gpu_set_pml_sigma",
 ]
 
 
@@ -74,6 +74,7 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_materials": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _f64p, _f64p, _f64p, _f64p, _f64p,
                                   _f64p, _f64p, _f64p, i32],
         "tlm_gpu_set_pml": [i64, i32, _f64p, i32, _i32p],
+        "tlm_gpu_set_pml_sigma": [i64, i32, _f64p],
         "tlm_gpu_set_excitation": [i64, i32, i32, _f64p, _f64p, i32, _i32p, _i32p, _i32p, _i32p, i32],
         "tlm_gpu_set_faces": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, i32, i32],
         "tlm_gpu_set_huygens": [i64, i32, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double, C.c_double, i32],
@@ -176,6 +177,9 @@ class GpuMesh:
             _check(lib.tlm_gpu_set_materials(self.h, nm, *[_p(x) for x in m], *[_p(x) for x in f], stride))
         pp, pc = _f64(t["pml_params"]), _i32(t["pml_cell_param"])
         _check(lib.tlm_gpu_set_pml(self.h, int(t["n_pml_params"]), _p(pp), int(t["n_pml_cells"]), _p(pc)))
+        if int(t.get("n_pml_material_cells", 0)):
+            sg = _f64(t["pml_sigma"])
+            _check(lib.tlm_gpu_set_pml_sigma(self.h, int(t["n_pml_params"]), _p(sg)))
         v, vf = _f64(t["fn_value"]), _f64(t["fn_value_face"])
         pts = [_i32(t[k]) for k in ("pt_cell", "pt_comp", "pt_fn", "pt_type")]
         _check(lib.tlm_gpu_set_excitation(self.h, int(t["n_functions"]), int(t["n_timesteps"]), _p(v), _p(vf),

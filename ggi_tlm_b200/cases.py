@@ -106,6 +106,27 @@ def kat_material_test2() -> ProblemSpec:
         outputs=[OutputPoint((c(-1.2e-3), c(0.0), c(0.0)), "Ex")])
 
 
+def pml_dielectric_slab(n: int = 40, pml: int = 8, steps: int = 300, eps_r: float = 4.0, sigma: float = 0.01,
+                        slab_top: int = 15, pad: int = 0, dl: float = 5e-3) -> ProblemSpec:
+    """A lossy dielectric substrate (cells z <= slab_top, every x and y) that
+    runs into the PML on five sides, so its PML cells take the PML-material
+    update (scatter_PML_material.F90); Gaussian Ez source in the free space
+    above, Ez probes in the slab and above it, an Ex probe near the interface.
+    ``pad`` > 0 surrounds the same geometry by ``pad`` free cells on every side
+    and drops the PML (a reference domain whose boundary is too far away to be
+    seen within ``steps``)."""
+    N = n + 2 * pad
+    c = N // 2 + 1
+    return ProblemSpec(
+        nx=N, ny=N, nz=N, dl=dl, n_timesteps=steps, pml_cells=(pml,) * 6 if pad == 0 else (0,) * 6,
+        materials=[VolumeMaterial.dielectric(eps_r, sigma)],
+        material_regions=[(1, Block(1, N, 1, N, 1, pad + slab_top))],
+        functions=[ExcitationFunction("gaussian", (1.0, 0.05e-9, 0.2e-9))],
+        point_excitations=[PointExcitation((c, c, pad + slab_top + 6), "Ez", 1)],
+        outputs=[OutputPoint((c, c, pad + slab_top - 3), "Ez"), OutputPoint((c, c, pad + slab_top + 9), "Ez"),
+                 OutputPoint((c + 4, c, pad + slab_top + 2), "Ex")])
+
+
 KAT_CASES = {
     "tem_pml_Ey": kat_tem_pml,
     "tem_material_Ey": kat_tem_material,

@@ -73,6 +73,7 @@ struct Mesh {
   bool have_cells = false;
   std::vector<tlm::MatDev> mats;
   std::vector<double> pml_params;
+  std::vector<double> pml_sigma;  // [n_pml_params][3] sx, sy, sz (PML cells in a material)
   int n_pml_params = 0;
   std::vector<int32_t> pml_cell_param;
   int n_pml_cells = 0;
@@ -94,7 +95,9 @@ struct Mesh {
 
   // device buffers
   DevBuf links, seg_mask, seg_base, sp_rec, sp_pos, pml_state, pml_par, pml_ixt, filt, mats_d, exc_field, exc_type,
-      cell_out, faces, face_io, face_hs, value_face, face_field, dft_entry, dft_phasor, dft_acc, d_base;
+      cell_out, faces, face_io, face_hs, value_face, face_field, dft_entry, dft_phasor, dft_acc, d_base,
+      pmm_pos, pmm_parmat, pmm_state, pmm_sigma;
+  int n_pmm = 0;  // PML cells inside a volume material
   int n_filt = 0, filt_eo = 0, filt_mo = 0;
   int dft_entries = 0;
   int n_sp_dev = 0;  // non-PML special cells on the device list
@@ -199,6 +202,7 @@ tlm::MeshDev<T> mesh_dev(Mesh *m) {
   d.cell_out = (double *)m->cell_out.p;
   d.n_out = m->n_out_cells;
   d.dl = m->desc.dl;
+  d.dt = m->desc.dt;
   d.d_base = (const int *)m->d_base.p;
   return d;
 }
@@ -254,7 +258,8 @@ int finalize(Mesh *m) {
     if (pml && mat) {
       const int type = m->mats[mat - 1].type;
       if (type == 1 || type == 2) return fail(TLM_E_UNSUPPORTED, "PEC/PMC volume material in PML (scatter.F90:559-567)");
-      return fail(TLM_E_UNSUPPORTED, "PML cell inside a dispersive material is not supported by the GPU path");
+      if (m->pml_sigma.empty())
+        return fail(TLM_E_BADARG, "PML cell %d lies in material %d: tlm_gpu_set_pml_sigma is required", pml, mat);
     }
     if (pml && m->sp_exc[s]) return fail(TLM_E_UNSUPPORTED, "Excitation intersects PML (set_update_codes.F90:347-354)");
   }
@@ -270,6 +275,8 @@ int finalize(Mesh *m) {
   std::vector<unsigned long long> pml_pos;
   std::vector<uint16_t> pml_par;
   std::vector<int2> pml_out;
+  std::vector<int4> pmm_pos;
+  std::vector<int2> pmm_parmat;
   pml_pos.reserve(m->n_pml_cells + 1);
   pml_par.reserve(m->n_pml_cells + 1);
   int mask_count = 0;
@@ -306,9 +313,16 @@ int finalize(Mesh *m) {
           if (pidx != (int)pml_pos.size())
             return fail(TLM_E_BADARG, "PML cell numbers must follow (cz,cy,cx) traversal order (cell %lld)", cell + 1);
           const int par = m->pml_cell_param[pidx];
-          if (par < 1 || par > m->n_pml_params || par > 65536)
+          if (par < 1 || par > m->n_pml_params || par > 65535)
             return fail(TLM_E_BADARG, "PML cell %d: parameter %d out of range", pidx + 1, par);
           unsigned long long pk = (unsigned long long)x | ((unsigned long long)y << 21) | ((unsigned long long)z << 42);
+          if (mat) {  // PML cell in a volume material: own list, own kernel
+            pmm_pos.push_back(int4{x, y, z, m->sp_out[s] ? out_no++ : -1});
+            pmm_parmat.push_back(int2{par - 1, mat});
+            pml_pos.push_back(pk);
+            pml_par.push_back(tlm::kPmlMaterialSlot);
+            continue;
+          }
           if (m->sp_out[s]) {
             pk |= 1ull << 63;
             pml_out.push_back(int2{pidx, out_no++});
@@ -348,6 +362,18 @@ int finalize(Mesh *m) {
   if ((int)pml_pos.size() != m->n_pml_cells) return fail(TLM_E_BADARG, "PML cells: %zu flagged, %d declared", pml_pos.size(), m->n_pml_cells);
   if (nx >= (1 << 21) || ny >= (1 << 21) || nz >= (1 << 21)) return fail(TLM_E_BADARG, "mesh too large for packed positions");
   m->n_pml_list = (int)pml_pos.size();
+  m->n_pmm = (int)pmm_pos.size();
+  if (m->n_pmm) {
+    int rc2;
+    std::vector<double> sg((size_t)m->n_pml_params * 4, 0.0);
+    for (int i = 0; i < m->n_pml_params; i++)
+      for (int k = 0; k < 3; k++) sg[(size_t)i * 4 + k] = m->pml_sigma[(size_t)i * 3 + k];
+    if ((rc2 = upload(m, m->pmm_pos, pmm_pos)) || (rc2 = upload(m, m->pmm_parmat, pmm_parmat)) ||
+        (rc2 = upload(m, m->pmm_sigma, sg)) ||
+        (rc2 = dalloc(m, m->pmm_state, (size_t)tlm::kPmmState * m->n_pmm * sizeof(double))))
+      return rc2;
+    CK(cudaMemset(m->pmm_state.p, 0, m->pmm_state.bytes));  // allocate_PML_material_data: all zero
+  }
   m->n_pml_out = (int)pml_out.size();
   if (pml_out.empty()) pml_out.resize(1);
   {
@@ -627,6 +653,11 @@ int launch_bulk(Mesh *m, const tlm::MeshDev<T> &md, int k) {
 
 // Enqueue relative steps [0, n) of one step bundle (kernels only, the base
 // counter is advanced by the caller).
+tlm::PmmList pmm_list(Mesh *m) {
+  return tlm::PmmList{(const int4 *)m->pmm_pos.p, (const int2 *)m->pmm_parmat.p, (double *)m->pmm_state.p,
+                      (const double *)m->pmm_sigma.p, m->n_pmm};
+}
+
 template <typename T, int VEC>
 int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
   const tlm::MeshDev<T> md = mesh_dev<T>(m);
@@ -646,6 +677,10 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
       tlm::PmlList pl{(const unsigned long long *)m->pml_pos.p, (const uint16_t *)m->pml_par16.p,
                       (const int2 *)m->pml_outmap.p, m->n_pml_list, m->n_pml_out};
       tlm::tlm_pml_kernel<T><<<(m->n_pml_list + 127) / 128, 128, 0, m->stream>>>(md, pl, k, m->pml_prefetch);
+      m->last_launches++;
+    }
+    if (m->n_pmm) {
+      tlm::tlm_pml_material_kernel<T><<<(m->n_pmm + 127) / 128, 128, 0, m->stream>>>(md, pmm_list(m), k);
       m->last_launches++;
     }
     if (m->n_sp_dev) {
@@ -818,6 +853,16 @@ int tlm_gpu_set_pml(int64_t h, int32_t n_params, const double *params, int32_t n
   m->pml_params.assign(params, params + (size_t)n_params * 15);
   m->n_pml_cells = n_pml_cells;
   m->pml_cell_param.assign(cell_param, cell_param + n_pml_cells);
+  return TLM_OK;
+}
+
+int tlm_gpu_set_pml_sigma(int64_t h, int32_t n_params, const double *sigma) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n_params != m->n_pml_params || (n_params && !sigma))
+    return fail(TLM_E_BADARG, "PML sigma rows: %d given, %d PML parameter rows set", n_params, m->n_pml_params);
+  m->pml_sigma.assign(sigma, sigma + (size_t)n_params * 3);
   return TLM_OK;
 }
 
@@ -1317,6 +1362,13 @@ int batch_step(Batch *b, bool dry) {
   bd.d_bases = (int *const *)b->dbases_d.p;
   bd.n_active = (int)b->active.size();
   if (b->n_pmlb) { tlm::tlm_pml_batch_kernel<T><<<b->n_pmlb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
+  for (int i : b->active) {  // PML cells inside materials of the members that have them
+    Mesh *m = get(b->handles[i]);
+    if (m && m->n_pmm) {
+      tlm::tlm_pml_material_kernel<T><<<(m->n_pmm + 127) / 128, 128, 0, b->stream>>>(mesh_dev<T>(m), pmm_list(m), 0);
+      b->last_launches++;
+    }
+  }
   if (b->n_spb) { tlm::tlm_special_batch_kernel<T><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
   if (b->n_faceb) { tlm::tlm_face_batch_kernel<T><<<b->n_faceb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
   if (b->n_dftb) { tlm::tlm_dft_batch_kernel<T><<<b->n_dftb, 256, 0, b->stream>>>(bd, 0); b->last_launches++; }

@@ -48,6 +48,9 @@ enum PmlPort {
 enum SpecialFlags : int { SP_PML = 1, SP_MAT = 2, SP_EXC = 4, SP_OUT = 8 };
 
 constexpr int kMaxOrder = 8;
+// PML-list parameter index of a PML cell inside a volume material (those
+// cells take tlm_pml_material_kernel)
+constexpr uint16_t kPmlMaterialSlot = 0xFFFF;
 constexpr int kPmlState = 24;  // Ix,Iy,Iz, Vi(12), Vxt,Vyt,Vzt, Vxyt,Vyxt,Vzxt,Vxzt,Vyzt,Vzyt
 
 // One volume material after calculate_volume_material_filter_coefficients.
@@ -93,7 +96,7 @@ struct MeshDev {
   int n_exc;
   double *cell_out;         // [n_timesteps][n_out][6]
   int n_out;
-  double dl;
+  double dl, dt;
   const int *d_base;        // device step counter (1-based step of relative step 0)
 };
 
@@ -967,6 +970,7 @@ __device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl,
   const unsigned long long pk = __ldcs(pl.pos + s);
   const int x = (int)(pk & 0x1fffffull), y = (int)((pk >> 21) & 0x1fffffull), z = (int)((pk >> 42) & 0x1fffffull);
   const int par = __ldcs(pl.par + s);
+  if (par == kPmlMaterialSlot) return;  // PML cell in a material: tlm_pml_material_kernel
   int out_no = -1;
   if (pk >> 63)
     for (int k = 0; k < pl.n_out_map; k++)
@@ -1014,6 +1018,229 @@ __device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl,
     out[Vx_zmin * P + idx + dz] = m.R[5] * co[Vx_zmax];
     out[Vy_zmin * P + idx + dz] = m.R[5] * co[Vy_zmax];
   }
+}
+
+// ---------------------------------------------------------------------------
+// PML cells inside a non-dispersive volume material,
+// TLM_SOLVER/scatter_PML_material.F90:22-534.  One thread per cell; the
+// cells keep their slot in the PML numbering (the PML kernel skips them) and
+// carry their own FP64 state, 66 values per cell in SoA order:
+//   0-11 Vi, 12-23 Vi one step older, 24-26 Vxt..Vzt, 27-29 one step older,
+//   30-32 Ixt..Izt, 33-35 one step older, 36-41 series terms (xy yx yz zy zx
+//   xz), 42-44 capacitive stub reflected, 45-47 its incident, 48-50 one step
+//   older, 51-53 inductive stub reflected, 54-56 voltage across its
+//   impedance, 57-59 one step older, 60-62 Vc, 63-65 one step older.
+// The coefficients are rebuilt from sx,sy,sz and the material every step, as
+// in the reference.  Axis a = x,y,z has partners (j,k) = (y,z),(z,x),(x,y).
+// ---------------------------------------------------------------------------
+constexpr int kPmmState = 66;
+
+struct PmmList {
+  const int4 *pos;      // (x, y, z, output number or -1)
+  const int2 *par_mat;  // (PML parameter row, 0-based; material, 1-based)
+  double *state;        // [kPmmState][n]
+  const double *sigma;  // [n_par][4]: sx, sy, sz, 0
+  int n;
+};
+
+template <typename T>
+__device__ __forceinline__ void pml_material_body(const MeshDev<T> &m, const PmmList &pl, int s, int rel_step) {
+  const int t = *m.d_base + rel_step;
+  const T *__restrict__ in = (t & 1) ? m.links0 : m.links1;
+  T *__restrict__ out = (t & 1) ? m.links1 : m.links0;
+  const long long P = m.plane;
+  const int4 ps = pl.pos[s];
+  const int2 pm = pl.par_mat[s];
+  const int x = ps.x, y = ps.y, z = ps.z;
+  const long long idx = (long long)(z + 1) * m.PxPy + (long long)(y + 1) * m.Px + x;
+  const long long dy = m.Px, dz = m.PxPy;
+  double V[12];
+  V[Vy_xmin] = double(in[Vy_xmax * P + idx - 1]);
+  V[Vz_xmin] = double(in[Vz_xmax * P + idx - 1]);
+  V[Vy_xmax] = double(in[Vy_xmin * P + idx + 1]);
+  V[Vz_xmax] = double(in[Vz_xmin * P + idx + 1]);
+  V[Vx_ymin] = double(in[Vx_ymax * P + idx - dy]);
+  V[Vz_ymin] = double(in[Vz_ymax * P + idx - dy]);
+  V[Vx_ymax] = double(in[Vx_ymin * P + idx + dy]);
+  V[Vz_ymax] = double(in[Vz_ymin * P + idx + dy]);
+  V[Vx_zmin] = double(in[Vx_zmax * P + idx - dz]);
+  V[Vy_zmin] = double(in[Vy_zmax * P + idx - dz]);
+  V[Vx_zmax] = double(in[Vx_zmin * P + idx + dz]);
+  V[Vy_zmax] = double(in[Vy_zmin * P + idx + dz]);
+
+  const double *Pr = m.pml_par + (size_t)pm.x * 16;
+  const double *Sg = pl.sigma + (size_t)pm.x * 4;
+  const MatDev &mt = m.mats[pm.y - 1];
+  const double dt = m.dt, Z0 = kZ0;
+  const double Ys = mt.Ys_eps_f / kY0, Ge = mt.Ge / kY0, Zs = mt.Zs_mu_f, Rm = mt.Rm;
+  const double sg[3] = {Sg[0], Sg[1], Sg[2]};
+  const double ex[3] = {Pr[3], Pr[4], Pr[5]};
+  double *S = pl.state;
+  const int n = pl.n;
+  auto ld = [&](int k) { return S[(size_t)k * n + s]; };
+  auto st = [&](int k, double v) { S[(size_t)k * n + s] = v; };
+
+  // STAGE 3
+  V[Vynx] = V[Vynx] * ex[1]; V[Vypx] = V[Vypx] * ex[1];
+  V[Vznx] = V[Vznx] * ex[2]; V[Vzpx] = V[Vzpx] * ex[2];
+  V[Vxny] = V[Vxny] * ex[0]; V[Vxpy] = V[Vxpy] * ex[0];
+  V[Vzny] = V[Vzny] * ex[2]; V[Vzpy] = V[Vzpy] * ex[2];
+  V[Vxnz] = V[Vxnz] * ex[0]; V[Vxpz] = V[Vxpz] * ex[0];
+  V[Vynz] = V[Vynz] * ex[1]; V[Vypz] = V[Vypz] * ex[1];
+
+  double Vss[3], It_m1[3], It_m2[3], Vt[3], Vc[3], It[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    Vss[a] = -ld(51 + a);
+    It_m1[a] = ld(30 + a);
+    It_m2[a] = ld(33 + a);
+  }
+  // STAGE 4: stretched V with the capacitive stub
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double sj = sg[(a + 1) % 3], sk = sg[(a + 2) % 3];
+    const double GpY2 = (Ge + Ys) / 2.0;
+    const double A0 = 8.0 + 4.0 * GpY2 + 2.0 * dt * (sj + sk) * (1.0 + GpY2) + dt * dt * sj * sk * GpY2;
+    const double A1 = -2.0 * (8.0 + 4.0 * GpY2) + 2.0 * (dt * dt * sj * sk * GpY2);
+    const double A2 = 8.0 + 4.0 * GpY2 - 2.0 * dt * (sj + sk) * (1.0 + GpY2) + dt * dt * sj * sk * GpY2;
+    const double B0 = 4.0 + 2.0 * dt * sj, B1 = -8.0, B2 = 4.0 - 2.0 * dt * sj;
+    const double C0 = 4.0 + 2.0 * dt * sk, C1 = -8.0, C2 = 4.0 - 2.0 * dt * sk;
+    const double D0 = 4.0 * Ys + 2.0 * dt * (sj + sk) * Ys + 1.0 * (dt * dt * sj * sk * Ys);
+    const double D1 = -8.0 * Ys + 2.0 * (dt * dt * sj * sk * Ys);
+    const double D2 = 4.0 * Ys - 2.0 * dt * (sj + sk) * Ys + 1.0 * (dt * dt * sj * sk * Ys);
+    // port pairs: B (x: Vznx,Vzpx  y: Vxny,Vxpy  z: Vynz,Vypz), C the others
+    const int b0 = a == 0 ? Vznx : (a == 1 ? Vxny : Vynz), b1 = a == 0 ? Vzpx : (a == 1 ? Vxpy : Vypz);
+    const int c0 = a == 0 ? Vynx : (a == 1 ? Vzny : Vxnz), c1 = a == 0 ? Vypx : (a == 1 ? Vzpy : Vxpz);
+    const double Vos = ld(42 + a);
+    Vt[a] = (1.0 / A0) * (B0 * (V[b0] + V[b1]) + C0 * (V[c0] + V[c1]) + D0 * (Vos) +
+                          B1 * (ld(b0) + ld(b1)) + C1 * (ld(c0) + ld(c1)) + D1 * (ld(45 + a)) +
+                          B2 * (ld(12 + b0) + ld(12 + b1)) + C2 * (ld(12 + c0) + ld(12 + c1)) + D2 * (ld(48 + a)) -
+                          A1 * ld(24 + a) - A2 * ld(27 + a));
+  }
+  // STAGE 5: stretched I through the series impedance
+  Vc[0] = V[Vypz] - V[Vzpy] - V[Vynz] + V[Vzny] - Vss[0];
+  Vc[1] = V[Vzpx] - V[Vxpz] - V[Vznx] + V[Vxnz] - Vss[1];
+  Vc[2] = V[Vxpy] - V[Vypx] - V[Vxny] + V[Vynx] - Vss[2];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double sj = sg[(a + 1) % 3], sk = sg[(a + 2) % 3], sa = sg[a];
+    const double ZpR = Zs + Rm;
+    const double S0 = 16.0 * Z0 + 4.0 * ZpR + 2.0 * dt * (sj + sk) * (2.0 * Z0 + ZpR) + dt * dt * sj * sk * ZpR;
+    const double S1 = -32.0 * Z0 - 8.0 * ZpR + 2.0 * dt * dt * sj * sk * ZpR;
+    const double S2 = 16.0 * Z0 + 4.0 * ZpR - 2.0 * dt * (sj + sk) * (2.0 * Z0 + ZpR) + dt * dt * sj * sk * ZpR;
+    const double T0 = 8.0 + 4.0 * dt * sa, T1 = -16.0, T2 = 8.0 - 4.0 * dt * sa;
+    It[a] = (1.0 / S0) * (T0 * Vc[a] + T1 * ld(60 + a) + T2 * ld(63 + a) - S1 * It_m1[a] - S2 * It_m2[a]);
+  }
+  // series terms V_{ab}t, driven by the current of the third axis c; U uses
+  // sigma_c, W sigma_b (order xy yx yz zy zx xz)
+  double Vabt[6];
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    const int a = (q == 0 || q == 5) ? 0 : ((q == 1 || q == 2) ? 1 : 2);
+    const int b = (q == 1 || q == 4) ? 0 : ((q == 0 || q == 3) ? 1 : 2);
+    const int c = 3 - a - b;
+    const double U0 = 2.0 + dt * sg[c], U1 = -2.0 + dt * sg[c];
+    const double W0 = Z0 * (2.0 + dt * sg[b]), W1 = Z0 * (-2.0 + dt * sg[b]);
+    Vabt[q] = (1.0 / U0) * (W0 * It[c] + W1 * It_m1[c] - U1 * ld(36 + q));
+  }
+  const double Vxyt = Vabt[0], Vyxt = Vabt[1], Vyzt = Vabt[2], Vzyt = Vabt[3], Vzxt = Vabt[4], Vxzt = Vabt[5];
+  // STAGE 9: state for the next step
+#pragma unroll
+  for (int k = 0; k < 12; k++) {
+    st(12 + k, ld(k));
+    st(k, V[k]);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    st(27 + a, ld(24 + a));
+    st(24 + a, Vt[a]);
+    st(33 + a, It_m1[a]);
+    st(30 + a, It[a]);
+    st(63 + a, ld(60 + a));
+    st(60 + a, Vc[a]);
+  }
+#pragma unroll
+  for (int q = 0; q < 6; q++) st(36 + q, Vabt[q]);
+  // STAGE 11: scattered pulses
+  double R[12];
+  R[Vynx] = Vt[0] - Vyxt - V[Vypx]; R[Vypx] = Vt[0] + Vyxt - V[Vynx];
+  R[Vznx] = Vt[0] + Vzxt - V[Vzpx]; R[Vzpx] = Vt[0] - Vzxt - V[Vznx];
+  R[Vzny] = Vt[1] - Vzyt - V[Vzpy]; R[Vzpy] = Vt[1] + Vzyt - V[Vzny];
+  R[Vxny] = Vt[1] + Vxyt - V[Vxpy]; R[Vxpy] = Vt[1] - Vxyt - V[Vxny];
+  R[Vxnz] = Vt[2] - Vxzt - V[Vxpz]; R[Vxpz] = Vt[2] + Vxzt - V[Vxnz];
+  R[Vynz] = Vt[2] + Vyzt - V[Vypz]; R[Vypz] = Vt[2] - Vyzt - V[Vynz];
+  // capacitive stub: reflect and keep the incident history
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double Vos = ld(42 + a);
+    st(42 + a, Vt[a] - Vos);
+    st(48 + a, ld(45 + a));
+    st(45 + a, Vos);
+  }
+  // inductive stub: voltage across the stub impedance, then its reflection
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double sj = sg[(a + 1) % 3], sk = sg[(a + 2) % 3], sa = sg[a];
+    const double P0 = 4.0 + 2.0 * dt * sa, P1 = -8.0, P2 = 4.0 - 2.0 * dt * sa;
+    const double Q0 = 4.0 * Zs + 2.0 * dt * (sj + sk) * Zs + 1.0 * (dt * dt * sj * sk * Zs);
+    const double Q1 = -8.0 * Zs + 2.0 * (dt * dt * sj * sk * Zs);
+    const double Q2 = 4.0 * Zs - 2.0 * dt * (sj + sk) * Zs + 1.0 * (dt * dt * sj * sk * Zs);
+    const double Vs = (1.0 / P0) * (Q0 * It[a] + Q1 * It_m1[a] + Q2 * It_m2[a] - P1 * ld(54 + a) - P2 * ld(57 + a));
+    st(51 + a, (Vs + Vss[a]));
+    st(57 + a, ld(54 + a));
+    st(54 + a, Vs);
+  }
+  // STAGE 12: output
+  if (ps.w >= 0) {
+    double *row = m.cell_out + ((size_t)(t - 1) * m.n_out + ps.w) * 6;
+    const double dl = m.dl;
+    row[0] = -Vt[0] / dl; row[1] = -Vt[1] / dl; row[2] = -Vt[2] / dl;
+    row[3] = It[0] / dl; row[4] = It[1] / dl; row[5] = It[2] / dl;
+  }
+  // STAGE 13: half-cell loss on the scattered pulses, then the pulses leave
+  R[Vynx] = R[Vynx] * ex[1]; R[Vypx] = R[Vypx] * ex[1];
+  R[Vznx] = R[Vznx] * ex[2]; R[Vzpx] = R[Vzpx] * ex[2];
+  R[Vxny] = R[Vxny] * ex[0]; R[Vxpy] = R[Vxpy] * ex[0];
+  R[Vzny] = R[Vzny] * ex[2]; R[Vzpy] = R[Vzpy] * ex[2];
+  R[Vxnz] = R[Vxnz] * ex[0]; R[Vxpz] = R[Vxpz] * ex[0];
+  R[Vynz] = R[Vynz] * ex[1]; R[Vypz] = R[Vypz] * ex[1];
+  T co[12];
+#pragma unroll
+  for (int p = 0; p < 12; p++) {
+    co[p] = T(R[p]);
+    out[p * P + idx] = co[p];
+  }
+  if (x == 0) {
+    out[Vy_xmax * P + idx - 1] = m.R[0] * co[Vy_xmin];
+    out[Vz_xmax * P + idx - 1] = m.R[0] * co[Vz_xmin];
+  }
+  if (x == m.nx - 1) {
+    out[Vy_xmin * P + idx + 1] = m.R[1] * co[Vy_xmax];
+    out[Vz_xmin * P + idx + 1] = m.R[1] * co[Vz_xmax];
+  }
+  if (y == 0) {
+    out[Vx_ymax * P + idx - dy] = m.R[2] * co[Vx_ymin];
+    out[Vz_ymax * P + idx - dy] = m.R[2] * co[Vz_ymin];
+  }
+  if (y == m.ny - 1) {
+    out[Vx_ymin * P + idx + dy] = m.R[3] * co[Vx_ymax];
+    out[Vz_ymin * P + idx + dy] = m.R[3] * co[Vz_ymax];
+  }
+  if (z == 0) {
+    out[Vx_zmax * P + idx - dz] = m.R[4] * co[Vx_zmin];
+    out[Vy_zmax * P + idx - dz] = m.R[4] * co[Vy_zmin];
+  }
+  if (z == m.nz - 1) {
+    out[Vx_zmin * P + idx + dz] = m.R[5] * co[Vx_zmax];
+    out[Vy_zmin * P + idx + dz] = m.R[5] * co[Vy_zmax];
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) tlm_pml_material_kernel(const MeshDev<T> m, const PmmList pl, int rel_step) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= pl.n) return;
+  pml_material_body<T>(m, pl, s, rel_step);
 }
 
 // ---------------------------------------------------------------------------

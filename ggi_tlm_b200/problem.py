@@ -573,8 +573,16 @@ def build_tables(spec: ProblemSpec) -> dict:
     if np.any(in_pml & cell_exc):
         raise UnsupportedFeature("Excitation intersects PML")  # set_update_codes.F90:347-354
     special = (cell_mat != 0) | in_pml | cell_exc | cell_out
-    for m in np.unique(cell_mat[in_pml & (cell_mat != 0)]):
-        raise UnsupportedFeature("material intersects PML: the PML-material update is not supported")
+    # materials in the PML (set_update_codes.F90:290-331, scatter.F90:552-567):
+    # PEC/PMC stop the reference, so do dispersive ones (any S-domain order
+    # above 0); a constant eps_r, mu_r, sigma material takes the PML-material
+    # update (scatter_PML_material.F90)
+    for mnum in np.unique(cell_mat[in_pml & (cell_mat != 0)]):
+        vm = spec.materials[int(mnum) - 1]
+        if vm.type != MAT_DISPERSIVE:
+            raise UnsupportedFeature("PEC/PMC volume material in PML")
+        if len(vm.eps.a) > 1 or len(vm.eps.b) > 1 or len(vm.mu.a) > 1 or len(vm.mu.b) > 1:
+            raise UnsupportedFeature(f"PML fatal error: dispersive material found, material number {int(mnum)}")
 
     # set_cell_update_codes, set_update_codes.F90:38-363 (traversal order cz,cy,cx)
     flat_special = special.reshape(-1)
@@ -599,6 +607,7 @@ def build_tables(spec: ProblemSpec) -> dict:
     pml_number[pml_flat] = np.arange(1, n_pml + 1, dtype=np.int32)
     sp_pml = pml_number[flat_special].astype(np.int32)
     pml_params = np.zeros((0, 15))
+    pml_sigma = np.zeros((0, 3))
     pml_cell_param = np.zeros(0, dtype=np.int32)
     if n_pml:
         zz, yy, xx = np.nonzero(in_pml)
@@ -618,12 +627,14 @@ def build_tables(spec: ProblemSpec) -> dict:
         rank[order] = np.arange(len(order))
         pml_cell_param = (rank[inverse.reshape(-1)] + 1).astype(np.int32)
         pml_params = np.zeros((len(uniq), 15))
+        pml_sigma = np.zeros((len(uniq), 3))
         for u in range(len(uniq)):
             ddx, ddy, ddz = (int(v) for v in uniq[u])
             sx = pml_conductivity(ddx, pml_xmin, pml_xmax, s0[0], s0[1], o)
             sy = pml_conductivity(ddy, pml_ymin, pml_ymax, s0[2], s0[3], o)
             sz = pml_conductivity(ddz, pml_zmin, pml_zmax, s0[4], s0[5], o)
             pml_params[rank[u]] = pml_parameter_row(sx, sy, sz, dt)
+            pml_sigma[rank[u]] = (sx, sy, sz)
 
     # volume materials
     mats = [material_coefficients(m, dl, dt, spec.reduced_c) for m in spec.materials]
@@ -654,6 +665,8 @@ def build_tables(spec: ProblemSpec) -> dict:
         mat_eps_a=coef("eps_a"), mat_eps_b=coef("eps_b"), mat_mu_a=coef("mu_a"), mat_mu_b=coef("mu_b"),
         n_pml_params=len(pml_params), pml_params=np.ascontiguousarray(pml_params, dtype=np.float64),
         n_pml_cells=n_pml, pml_cell_param=pml_cell_param,
+        pml_sigma=np.ascontiguousarray(pml_sigma, dtype=np.float64),
+        n_pml_material_cells=int(np.count_nonzero(in_pml & (cell_mat != 0))),
     )
     if nm and max(max(m["eps_order"], m["mu_order"]) for m in mats) > MAX_ORDER:
         raise UnsupportedFeature("Z-filter order above %d" % MAX_ORDER)

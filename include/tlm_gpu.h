@@ -96,6 +96,16 @@ int tlm_gpu_set_materials(int64_t handle, int32_t n_materials, const int32_t *ty
 int tlm_gpu_set_pml(int64_t handle, int32_t n_params, const double *params, int32_t n_pml_cells,
                     const int32_t *pml_cell_param);
 
+/* PML_parameters(1:n_params)%sx,sy,sz: the layer conductivities divided by
+   eps0 (SRC/MATERIALS/TLM_PML_volume_materials.F90:321-331), 3 doubles per
+   row.  Required (after tlm_gpu_set_pml) when a PML cell lies inside a
+   volume material: those cells take the PML-material update
+   (SRC/TLM_SOLVER/scatter_PML_material.F90:22-534), which rebuilds its
+   recursion coefficients from them.  The caller keeps the reference's
+   precondition (SRC/TLM_SOLVER/set_update_codes.F90:290-331): such a
+   material has eps_r and mu_r of S-domain order 0. */
+int tlm_gpu_set_pml_sigma(int64_t handle, int32_t n_params, const double *sigma);
+
 /* Excitation: excitation_functions(1:n_fn)%value(1:n_steps) and
    %value_face(1:n_steps) (SRC/EXCITATION/excitation.F90:155-559), and the
    cell-centre point excitations (excitation cell number, field component

@@ -44,6 +44,7 @@ class _Problem(C.Structure):
         ("n_dft", C.c_int32), ("dft_freq", _f64p), ("dft_comp", _i32p), ("dft_face_ptr", _i32p),
         ("dft_face_out", _i32p), ("dft_face_side", _i32p),
         ("n_small_to_zero", C.c_int32), ("small_to_zero_value", C.c_double),
+        ("pml_sigma", _f64p),
     ]
 
 
@@ -107,6 +108,8 @@ class Oracle:
         p.hs_Hi[:] = [float(v) for v in t["hs_Hi"]]
         p.hs_offset_min = float(t["hs_offset_min"])
         p.hs_c = float(t["hs_c"])
+        if int(t.get("n_pml_material_cells", 0)):
+            p.pml_sigma = arr("pml_sigma", np.float64)
         p.n_small_to_zero = int(t.get("n_small_to_zero", 0))
         p.small_to_zero_value = float(t.get("small_to_zero_value", 0.0))
         self._keep = keep

@@ -33,6 +33,20 @@ typedef struct {
   double Vyxt, Vzxt, Vxyt, Vzyt, Vyzt, Vxzt;
 } pml_cell_t; /* PML_data_type, PML_module.F90:116-128 */
 
+/* PML_material_data_type (PML_module.F90:131-155): the values one step older
+   than those in pml_cell_t, plus the capacitive / inductive stub state.
+   Index 0,1,2 = x,y,z.  The reference also stores Ix_m1.. and Vyxt_m1..,
+   which its update never reads; they are left out. */
+typedef struct {
+  double Vt_m1[3];   /* Vxt_m1, Vyt_m1, Vzt_m1 */
+  double It_m1[3];   /* Ixt_m1, Iyt_m1, Izt_m1 */
+  double Vi_m1[12];
+  double Vosr[3], Vos[3], Vos_m1[3];
+  double Vssr[3];
+  double Vs[3], Vs_m1[3];
+  double Vc[3], Vc_m1[3];
+} pml_mat_t;
+
 typedef struct {
   int order;
   double f;
@@ -47,6 +61,8 @@ struct tlm_oracle_state {
   int32_t *sp_filter;  /* cell_update_code_to_material_data(:,2), 1-based */
   zresp_t *eps_f, *mu_f;
   pml_cell_t *pml;
+  pml_mat_t *pml_mat;  /* PML cells inside a volume material, traversal order */
+  int32_t *pml_mat_pos; /* PML_material_array_pos per PML cell, 1-based or 0 */
   double *cell_exc;    /* [n_exc_cells][9] */
   int32_t *cell_exc_type; /* [n_exc_cells][6] */
   double *cell_out;    /* [n_out_cells][6] */
@@ -126,6 +142,18 @@ tlm_oracle_state *tlm_oracle_create(const tlm_oracle_problem *p) {
     }
   }
   s->pml = (pml_cell_t *)calloc((size_t)p->n_pml_cells + 1, sizeof(pml_cell_t));
+  /* allocate_PML_material_data, TLM_PML_volume_materials.F90:590-740: a
+     PML cell whose special cell has a DISPERSIVE-type material gets the next
+     PML material record, in special-cell (traversal) order; all zero */
+  s->pml_mat_pos = (int32_t *)calloc((size_t)p->n_pml_cells + 1, sizeof(int32_t));
+  {
+    int n_pm = 0;
+    for (int c = 0; c < p->n_special; c++) {
+      int pc = p->sp_pml[c], m = p->sp_material[c];
+      if (pc && m && p->mat_type[m - 1] == 3) s->pml_mat_pos[pc - 1] = ++n_pm;
+    }
+    s->pml_mat = (pml_mat_t *)calloc((size_t)n_pm + 1, sizeof(pml_mat_t));
+  }
   s->cell_exc = (double *)calloc((size_t)p->n_exc_cells * 9 + 1, sizeof(double));
   s->cell_exc_type = (int32_t *)calloc((size_t)p->n_exc_cells * 6 + 1, sizeof(int32_t));
   for (int i = 0; i < p->n_exc_cells * 6; i++) s->cell_exc_type[i] = 1; /* soft, set_update_codes.F90:195 */
@@ -147,7 +175,7 @@ tlm_oracle_state *tlm_oracle_create(const tlm_oracle_problem *p) {
 
 void tlm_oracle_destroy(tlm_oracle_state *s) {
   if (!s) return;
-  free(s->V); free(s->sp_filter); free(s->eps_f); free(s->mu_f); free(s->pml);
+  free(s->V); free(s->sp_filter); free(s->eps_f); free(s->mu_f); free(s->pml); free(s->pml_mat); free(s->pml_mat_pos);
   free(s->cell_exc); free(s->cell_exc_type); free(s->cell_out); free(s->face_exc);
   free(s->face_exc_type); free(s->face_out); free(s->face_code); free(s->dft);
   free(s);
@@ -344,6 +372,194 @@ static void scatter_pml_cell(tlm_oracle_state *s, int cx, int cy, int cz, int pm
   V_(Vypz, cx, cy, cz) = V_(Vypz, cx, cy, cz) * exp_yr;
 }
 
+/* PML cell inside a non-dispersive volume material,
+   TLM_SOLVER/scatter_PML_material.F90:22-534.  Second-order recursions in
+   time for the stretched voltages (with the capacitive stub), the stretched
+   currents (with the inductive stub) and the series PML terms; the
+   coefficients are rebuilt from sx,sy,sz and the material every call, as the
+   reference does.  Axis a = x,y,z has partners (j,k) = (y,z),(z,x),(x,y). */
+static void scatter_pml_material_cell(tlm_oracle_state *s, int cx, int cy, int cz, int pml_cell, int material_number,
+                                      int output, int *output_cell_number) {
+  const tlm_oracle_problem *p = &s->p;
+  const int prow = p->pml_cell_param[pml_cell - 1] - 1;
+  const double *P = p->pml_params + (size_t)prow * 15;
+  const double *S = p->pml_sigma + (size_t)prow * 3;
+  const int m = material_number - 1;
+  const double dt = p->dt;
+  pml_cell_t *pc = &s->pml[pml_cell - 1];
+  pml_mat_t *pm = &s->pml_mat[s->pml_mat_pos[pml_cell - 1] - 1];
+
+  /* STAGE 1 (:24-221): the same Ys, Ge, Zs, Rm on the three axes */
+  const double Ys = p->mat_Ys_eps_f[m] / Y0, Ge = p->mat_Ge[m] / Y0;
+  const double Zs = p->mat_Zs_mu_f[m], Rm = p->mat_Rm[m];
+  const double sg[3] = {S[0], S[1], S[2]};
+  const double ex[3] = {P[3], P[4], P[5]}; /* exp_x, exp_y, exp_z */
+  double A[3][3], B[3][3], Cc[3][3], D[3][3], Sc[3][3], T[3][3], Pc[3][3], Q[3][3];
+  for (int a = 0; a < 3; a++) {
+    const double sj = sg[(a + 1) % 3], sk = sg[(a + 2) % 3], sa = sg[a];
+    const double GpY2 = (Ge + Ys) / 2.0;
+    A[a][0] = 8.0 + 4.0 * GpY2 + 2.0 * dt * (sj + sk) * (1.0 + GpY2) + dt * dt * sj * sk * GpY2;
+    A[a][1] = -2.0 * (8.0 + 4.0 * GpY2) + 2.0 * (dt * dt * sj * sk * GpY2);
+    A[a][2] = 8.0 + 4.0 * GpY2 - 2.0 * dt * (sj + sk) * (1.0 + GpY2) + dt * dt * sj * sk * GpY2;
+    B[a][0] = 4.0 + 2.0 * dt * sj; B[a][1] = -8.0; B[a][2] = 4.0 - 2.0 * dt * sj;
+    Cc[a][0] = 4.0 + 2.0 * dt * sk; Cc[a][1] = -8.0; Cc[a][2] = 4.0 - 2.0 * dt * sk;
+    D[a][0] = 4.0 * Ys + 2.0 * dt * (sj + sk) * Ys + 1.0 * (dt * dt * sj * sk * Ys);
+    D[a][1] = -8.0 * Ys + 2.0 * (dt * dt * sj * sk * Ys);
+    D[a][2] = 4.0 * Ys - 2.0 * dt * (sj + sk) * Ys + 1.0 * (dt * dt * sj * sk * Ys);
+    const double ZpR = Zs + Rm;
+    Sc[a][0] = 16.0 * Z0 + 4.0 * ZpR + 2.0 * dt * (sj + sk) * (2.0 * Z0 + ZpR) + dt * dt * sj * sk * ZpR;
+    Sc[a][1] = -32.0 * Z0 - 8.0 * ZpR + 2.0 * dt * dt * sj * sk * ZpR;
+    Sc[a][2] = 16.0 * Z0 + 4.0 * ZpR - 2.0 * dt * (sj + sk) * (2.0 * Z0 + ZpR) + dt * dt * sj * sk * ZpR;
+    T[a][0] = 8.0 + 4.0 * dt * sa; T[a][1] = -16.0; T[a][2] = 8.0 - 4.0 * dt * sa;
+    Pc[a][0] = 4.0 + 2.0 * dt * sa; Pc[a][1] = -8.0; Pc[a][2] = 4.0 - 2.0 * dt * sa;
+    Q[a][0] = 4.0 * Zs + 2.0 * dt * (sj + sk) * Zs + 1.0 * (dt * dt * sj * sk * Zs);
+    Q[a][1] = -8.0 * Zs + 2.0 * (dt * dt * sj * sk * Zs);
+    Q[a][2] = 4.0 * Zs - 2.0 * dt * (sj + sk) * Zs + 1.0 * (dt * dt * sj * sk * Zs);
+  }
+  /* series terms V_{ab}t: U uses the third axis c, W the axis b (:169-195) */
+  const int sab[6][2] = {{0, 1}, {1, 0}, {1, 2}, {2, 1}, {2, 0}, {0, 2}}; /* xy yx yz zy zx xz */
+  double U0[6], U1[6], W0[6], W1[6];
+  for (int q = 0; q < 6; q++) {
+    const int a = sab[q][0], b = sab[q][1], c = 3 - a - b;
+    U0[q] = 2.0 + dt * sg[c];
+    U1[q] = -2.0 + dt * sg[c];
+    W0[q] = Z0 * (2.0 + dt * sg[b]);
+    W1[q] = Z0 * (-2.0 + dt * sg[b]);
+  }
+
+  /* STAGE 2: previous values */
+  double Vi_m1[12], Vi_m2[12];
+  memcpy(Vi_m1, pc->Vi, sizeof(Vi_m1));
+  memcpy(Vi_m2, pm->Vi_m1, sizeof(Vi_m2));
+  const double Vt_m1[3] = {pc->Vxt, pc->Vyt, pc->Vzt};
+  const double It_m1[3] = {pc->Ixt, pc->Iyt, pc->Izt};
+  const double It_m2[3] = {pm->It_m1[0], pm->It_m1[1], pm->It_m1[2]};
+  const double Vabt_m1[6] = {pc->Vxyt, pc->Vyxt, pc->Vyzt, pc->Vzyt, pc->Vzxt, pc->Vxzt};
+  double Vos[3], Vss[3];
+  for (int a = 0; a < 3; a++) {
+    Vos[a] = pm->Vosr[a];  /* capacitive stub incident = last reflected */
+    Vss[a] = -pm->Vssr[a]; /* inductive stub incident = -last reflected */
+  }
+
+  /* STAGE 3: half-cell loss on the incident pulses */
+  V_(Vynx, cx, cy, cz) = V_(Vynx, cx, cy, cz) * ex[1];
+  V_(Vypx, cx, cy, cz) = V_(Vypx, cx, cy, cz) * ex[1];
+  V_(Vznx, cx, cy, cz) = V_(Vznx, cx, cy, cz) * ex[2];
+  V_(Vzpx, cx, cy, cz) = V_(Vzpx, cx, cy, cz) * ex[2];
+  V_(Vxny, cx, cy, cz) = V_(Vxny, cx, cy, cz) * ex[0];
+  V_(Vxpy, cx, cy, cz) = V_(Vxpy, cx, cy, cz) * ex[0];
+  V_(Vzny, cx, cy, cz) = V_(Vzny, cx, cy, cz) * ex[2];
+  V_(Vzpy, cx, cy, cz) = V_(Vzpy, cx, cy, cz) * ex[2];
+  V_(Vxnz, cx, cy, cz) = V_(Vxnz, cx, cy, cz) * ex[0];
+  V_(Vxpz, cx, cy, cz) = V_(Vxpz, cx, cy, cz) * ex[0];
+  V_(Vynz, cx, cy, cz) = V_(Vynz, cx, cy, cz) * ex[1];
+  V_(Vypz, cx, cy, cz) = V_(Vypz, cx, cy, cz) * ex[1];
+
+  /* STAGE 4: stretched Vt.  Port pairs: B multiplies (x: z-ports on x faces,
+     y: x-ports on y faces, z: y-ports on z faces), C the other pair */
+  const int pb[3][2] = {{Vznx, Vzpx}, {Vxny, Vxpy}, {Vynz, Vypz}};
+  const int pcp[3][2] = {{Vynx, Vypx}, {Vzny, Vzpy}, {Vxnz, Vxpz}};
+  double Vt[3];
+  for (int a = 0; a < 3; a++) {
+    const int b0 = pb[a][0], b1 = pb[a][1], c0 = pcp[a][0], c1 = pcp[a][1];
+    Vt[a] = (1.0 / A[a][0]) * (B[a][0] * (V_(b0, cx, cy, cz) + V_(b1, cx, cy, cz)) +
+                               Cc[a][0] * (V_(c0, cx, cy, cz) + V_(c1, cx, cy, cz)) + D[a][0] * (Vos[a]) +
+                               B[a][1] * (Vi_m1[b0] + Vi_m1[b1]) + Cc[a][1] * (Vi_m1[c0] + Vi_m1[c1]) +
+                               D[a][1] * (pm->Vos[a]) + B[a][2] * (Vi_m2[b0] + Vi_m2[b1]) +
+                               Cc[a][2] * (Vi_m2[c0] + Vi_m2[c1]) + D[a][2] * (pm->Vos_m1[a]) -
+                               A[a][1] * Vt_m1[a] - A[a][2] * pm->Vt_m1[a]);
+  }
+
+  /* STAGE 5: stretched It through the series impedance */
+  double Vc[3];
+  Vc[0] = V_(Vypz, cx, cy, cz) - V_(Vzpy, cx, cy, cz) - V_(Vynz, cx, cy, cz) + V_(Vzny, cx, cy, cz) - Vss[0];
+  Vc[1] = V_(Vzpx, cx, cy, cz) - V_(Vxpz, cx, cy, cz) - V_(Vznx, cx, cy, cz) + V_(Vxnz, cx, cy, cz) - Vss[1];
+  Vc[2] = V_(Vxpy, cx, cy, cz) - V_(Vypx, cx, cy, cz) - V_(Vxny, cx, cy, cz) + V_(Vynx, cx, cy, cz) - Vss[2];
+  double It[3];
+  for (int a = 0; a < 3; a++)
+    It[a] = (1.0 / Sc[a][0]) * (T[a][0] * Vc[a] + T[a][1] * pm->Vc[a] + T[a][2] * pm->Vc_m1[a] -
+                                Sc[a][1] * It_m1[a] - Sc[a][2] * It_m2[a]);
+  /* V_{ab}t is driven by the current of the third axis c */
+  double Vabt[6];
+  for (int q = 0; q < 6; q++) {
+    const int c = 3 - sab[q][0] - sab[q][1];
+    Vabt[q] = (1.0 / U0[q]) * (W0[q] * It[c] + W1[q] * It_m1[c] - U1[q] * Vabt_m1[q]);
+  }
+  const double Vxyt = Vabt[0], Vyxt = Vabt[1], Vyzt = Vabt[2], Vzyt = Vabt[3], Vzxt = Vabt[4], Vxzt = Vabt[5];
+
+  /* STAGE 9: save for the next step */
+  memcpy(pm->Vi_m1, pc->Vi, sizeof(pm->Vi_m1));
+  for (int k = 0; k < 12; k++) pc->Vi[k] = V_(k, cx, cy, cz);
+  for (int a = 0; a < 3; a++) {
+    pm->Vt_m1[a] = Vt_m1[a];
+    pm->It_m1[a] = It_m1[a];
+    pm->Vc_m1[a] = pm->Vc[a];
+    pm->Vc[a] = Vc[a];
+  }
+  pc->Vxt = Vt[0]; pc->Vyt = Vt[1]; pc->Vzt = Vt[2];
+  pc->Ixt = It[0]; pc->Iyt = It[1]; pc->Izt = It[2];
+  pc->Vxyt = Vxyt; pc->Vyxt = Vyxt; pc->Vyzt = Vyzt; pc->Vzyt = Vzyt; pc->Vzxt = Vzxt; pc->Vxzt = Vxzt;
+
+  /* STAGE 11: scattered pulses */
+  double V_max, V_min;
+  V_max = V_(Vypx, cx, cy, cz); V_min = V_(Vynx, cx, cy, cz);
+  V_(Vynx, cx, cy, cz) = Vt[0] - Vyxt - V_max;
+  V_(Vypx, cx, cy, cz) = Vt[0] + Vyxt - V_min;
+  V_max = V_(Vzpx, cx, cy, cz); V_min = V_(Vznx, cx, cy, cz);
+  V_(Vznx, cx, cy, cz) = Vt[0] + Vzxt - V_max;
+  V_(Vzpx, cx, cy, cz) = Vt[0] - Vzxt - V_min;
+  V_max = V_(Vzpy, cx, cy, cz); V_min = V_(Vzny, cx, cy, cz);
+  V_(Vzny, cx, cy, cz) = Vt[1] - Vzyt - V_max;
+  V_(Vzpy, cx, cy, cz) = Vt[1] + Vzyt - V_min;
+  V_max = V_(Vxpy, cx, cy, cz); V_min = V_(Vxny, cx, cy, cz);
+  V_(Vxny, cx, cy, cz) = Vt[1] + Vxyt - V_max;
+  V_(Vxpy, cx, cy, cz) = Vt[1] - Vxyt - V_min;
+  V_max = V_(Vxpz, cx, cy, cz); V_min = V_(Vxnz, cx, cy, cz);
+  V_(Vxnz, cx, cy, cz) = Vt[2] - Vxzt - V_max;
+  V_(Vxpz, cx, cy, cz) = Vt[2] + Vxzt - V_min;
+  V_max = V_(Vypz, cx, cy, cz); V_min = V_(Vynz, cx, cy, cz);
+  V_(Vynz, cx, cy, cz) = Vt[2] + Vyzt - V_max;
+  V_(Vypz, cx, cy, cz) = Vt[2] - Vyzt - V_min;
+
+  /* capacitive stub scatter and history */
+  for (int a = 0; a < 3; a++) {
+    pm->Vosr[a] = Vt[a] - Vos[a];
+    pm->Vos_m1[a] = pm->Vos[a];
+    pm->Vos[a] = Vos[a];
+  }
+  /* inductive stub: voltage across the stub impedance, then its reflection */
+  for (int a = 0; a < 3; a++) {
+    const double Vs = (1.0 / Pc[a][0]) * (Q[a][0] * It[a] + Q[a][1] * It_m1[a] + Q[a][2] * It_m2[a] -
+                                          Pc[a][1] * pm->Vs[a] - Pc[a][2] * pm->Vs_m1[a]);
+    pm->Vssr[a] = (Vs + Vss[a]);
+    pm->Vs_m1[a] = pm->Vs[a];
+    pm->Vs[a] = Vs;
+  }
+
+  /* STAGE 12: output */
+  if (output) {
+    double dl = p->dl;
+    double *f = s->cell_out + (size_t)(*output_cell_number) * 6;
+    (*output_cell_number)++;
+    f[Ex] = -Vt[0] / dl; f[Ey] = -Vt[1] / dl; f[Ez] = -Vt[2] / dl;
+    f[Hx] = It[0] / dl; f[Hy] = It[1] / dl; f[Hz] = It[2] / dl;
+  }
+
+  /* STAGE 13: half-cell loss on the scattered pulses */
+  V_(Vynx, cx, cy, cz) = V_(Vynx, cx, cy, cz) * ex[1];
+  V_(Vypx, cx, cy, cz) = V_(Vypx, cx, cy, cz) * ex[1];
+  V_(Vznx, cx, cy, cz) = V_(Vznx, cx, cy, cz) * ex[2];
+  V_(Vzpx, cx, cy, cz) = V_(Vzpx, cx, cy, cz) * ex[2];
+  V_(Vxny, cx, cy, cz) = V_(Vxny, cx, cy, cz) * ex[0];
+  V_(Vxpy, cx, cy, cz) = V_(Vxpy, cx, cy, cz) * ex[0];
+  V_(Vzny, cx, cy, cz) = V_(Vzny, cx, cy, cz) * ex[2];
+  V_(Vzpy, cx, cy, cz) = V_(Vzpy, cx, cy, cz) * ex[2];
+  V_(Vxnz, cx, cy, cz) = V_(Vxnz, cx, cy, cz) * ex[0];
+  V_(Vxpz, cx, cy, cz) = V_(Vxpz, cx, cy, cz) * ex[0];
+  V_(Vynz, cx, cy, cz) = V_(Vynz, cx, cy, cz) * ex[1];
+  V_(Vypz, cx, cy, cz) = V_(Vypz, cx, cy, cz) * ex[1];
+}
+
 /* final scatter of the pulses, scatter.F90:519-547 (also :247-272) */
 static void scatter_pulses(tlm_oracle_state *s, int cx, int cy, int cz, double Vx, double Vy, double Vz,
                            double Ix, double Iy, double Iz) {
@@ -397,7 +613,11 @@ static int scatter(tlm_oracle_state *s) {
         int output_number = p->sp_output[sc];
         if (pml_cell != 0) {
           if (material_type == 1 || material_type == 2) return -1; /* scatter.F90:559-567 */
-          if (material_type == 3) return -2; /* PML in material: not restated */
+          if (material_type == 3) { /* scatter.F90:570-571 */
+            if (!p->pml_sigma) return -2;
+            scatter_pml_material_cell(s, cx, cy, cz, pml_cell, material_number, output_number, &output_cell_number);
+            continue;
+          }
           scatter_pml_cell(s, cx, cy, cz, pml_cell, output_number, &output_cell_number);
           continue;
         }

@@ -103,6 +103,10 @@ typedef struct {
      timesteps, |V| < small_to_zero_value -> 0; n_small_to_zero 0 = off */
   int32_t n_small_to_zero;
   double small_to_zero_value;
+
+  /* PML_parameters(:)%sx,sy,sz (TLM_PML_volume_materials.F90:329-331), 3 per
+     parameter row; needed by PML cells inside a volume material, else NULL */
+  const double *pml_sigma;
 } tlm_oracle_problem;
 
 typedef struct tlm_oracle_state tlm_oracle_state;

@@ -154,7 +154,7 @@ def test_gpu_rejects_unsupported_and_bad_calls(gpu_lib):
         assert e.value.code == -5
         with pytest.raises(capi.TLMError):
             g.run(11)  # beyond n_timesteps
-    # a PML cell inside a dispersive material is rejected up front
+    # a PML cell inside a PEC volume material is rejected up front (scatter.F90:559-567)
     bad = dict(t)
     bad["sp_pml"] = np.array(t["sp_pml"]).copy()
     bad["n_pml_params"] = 1
@@ -163,7 +163,7 @@ def test_gpu_rejects_unsupported_and_bad_calls(gpu_lib):
     bad["pml_cell_param"] = np.array([1], np.int32)
     bad["n_materials"] = 1
     for k in ("mat_type",):
-        bad[k] = np.array([3], np.int32)
+        bad[k] = np.array([1], np.int32)
     bad["sp_material"] = np.ones_like(np.array(t["sp_material"]))
     bad["sp_pml"][0] = 1
     with pytest.raises(capi.TLMError) as e:
