@@ -37,7 +37,8 @@ EXPORTS = [
     "tlm_gpu_last_run_launches", "tlm_gpu_destroy", "tlm_gpu_last_error", "tlm_gpu_set_variant",
     "tlm_gpu_num_variants", "tlm_gpu_fetch_links_noalloc", "tlm_gpu_batch_create", "tlm_gpu_batch_set_variant",
     "tlm_gpu_batch_run", "tlm_gpu_batch_synchronize", "tlm_gpu_batch_last_run", "tlm_gpu_batch_destroy",
-    "tlm_gpu_set_small_to_zero", "tlm_gpu_set_pml_sigma",
+    "tlm_gpu_set_small_to_zero", "tlm_gpu_set_pml_sigma", "tlm_gpu_set_face_excitation",
+    "tlm_gpu_set_face_outputs", "tlm_gpu_fetch_face_output",
 ]
 
 
@@ -75,6 +76,9 @@ def load_library(path: Optional[str] = None):
                                   _f64p, _f64p, _f64p, i32],
         "tlm_gpu_set_pml": [i64, i32, _f64p, i32, _i32p],
         "tlm_gpu_set_pml_sigma": [i64, i32, _f64p],
+        "tlm_gpu_set_face_excitation": [i64, i32, _i32p, _i32p, _i32p, _i32p],
+        "tlm_gpu_set_face_outputs": [i64, i32, _i32p, _i32p, _i32p],
+        "tlm_gpu_fetch_face_output": [i64, i32, i32, _f64p],
         "tlm_gpu_set_excitation": [i64, i32, i32, _f64p, _f64p, i32, _i32p, _i32p, _i32p, _i32p, i32],
         "tlm_gpu_set_faces": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, i32, i32],
         "tlm_gpu_set_huygens": [i64, i32, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double, C.c_double, i32],
@@ -197,6 +201,12 @@ class GpuMesh:
             df = [_f64(t["dft_freq"]), _i32(t["dft_comp"]), _i32(t["dft_face_ptr"]), _i32(t["dft_face_out"]),
                   _i32(t["dft_face_side"])]
             _check(lib.tlm_gpu_set_dft(self.h, int(t["n_dft"]), *[_p(x) for x in df]))
+        if int(t.get("n_face_points", 0)):
+            fp = [_i32(t[k]) for k in ("fpt_face", "fpt_comp", "fpt_fn", "fpt_type")]
+            _check(lib.tlm_gpu_set_face_excitation(self.h, int(t["n_face_points"]), *[_p(x) for x in fp]))
+        if int(t.get("n_face_probes", 0)):
+            fq = [_i32(t[k]) for k in ("fprobe_face", "fprobe_side", "fprobe_comp")]
+            _check(lib.tlm_gpu_set_face_outputs(self.h, int(t["n_face_probes"]), *[_p(x) for x in fq]))
         if int(t.get("n_small_to_zero", 0)):
             _check(lib.tlm_gpu_set_small_to_zero(self.h, int(t["n_small_to_zero"]), float(t["small_to_zero_value"])))
 
@@ -243,6 +253,15 @@ class GpuMesh:
         out = np.zeros((n, max(no, 1), 6))
         _check(_lib.tlm_gpu_fetch_cell_output(self.h, first, n, out.ctypes.data_as(_f64p)))
         return out[:, :no, :]
+
+    def face_output(self, first: int = 1, n: Optional[int] = None) -> np.ndarray:
+        """Face output point series [n_face_probes, n] of steps first.."""
+        if n is None:
+            n = self.step - first + 1
+        nq = int(self.t.get("n_face_probes", 0))
+        out = np.zeros((max(n, 1), max(nq, 1)))
+        _check(_lib.tlm_gpu_fetch_face_output(self.h, first, n, out.ctypes.data_as(_f64p)))
+        return out[:n, :nq].T.copy()
 
     def dft(self) -> np.ndarray:
         n = int(self.t["dft_face_ptr"][-1]) if int(self.t["n_dft"]) else 0

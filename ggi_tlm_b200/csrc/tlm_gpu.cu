@@ -82,6 +82,10 @@ struct Mesh {
   std::vector<int32_t> pt_cell, pt_comp, pt_fn, pt_type;
   int n_exc_cells = 0;
   std::vector<int32_t> f_cx, f_cy, f_cz, f_dir, f_exc, f_out;
+  // point sources on faces (excitation face number, component 1..12, function, type)
+  std::vector<int32_t> fpt_face, fpt_comp, fpt_fn, fpt_type;
+  // output points on faces (output face number, side 1/2, component 1..6)
+  std::vector<int32_t> fpr_face, fpr_side, fpr_comp;
   int n_exc_faces = 0, n_out_faces = 0;
   int hs_n = 0;
   std::vector<int32_t> hs_face_exc, hs_norm;
@@ -96,7 +100,8 @@ struct Mesh {
   // device buffers
   DevBuf links, seg_mask, seg_base, sp_rec, sp_pos, pml_state, pml_par, pml_ixt, filt, mats_d, exc_field, exc_type,
       cell_out, faces, face_io, face_hs, value_face, face_field, dft_entry, dft_phasor, dft_acc, d_base,
-      pmm_pos, pmm_parmat, pmm_state, pmm_sigma;
+      pmm_pos, pmm_parmat, pmm_state, pmm_sigma, face_src, fpt_field_d, fpt_type_d, fprobe, fprobe_rec;
+  int n_pt_rows = 0;
   int n_pmm = 0;  // PML cells inside a volume material
   int n_filt = 0, filt_eo = 0, filt_mo = 0;
   int dft_entries = 0;
@@ -224,7 +229,15 @@ tlm::FaceDev face_dev(Mesh *m) {
   f.value_face = (const double *)m->value_face.p;
   f.n_timesteps = m->desc.n_timesteps;
   f.face_field = (double *)m->face_field.p;
+  f.face_src = (const int2 *)m->face_src.p;
+  f.pt_field = (const double *)m->fpt_field_d.p;
+  f.pt_type = (const int8_t *)m->fpt_type_d.p;
+  f.n_pt_rows = m->n_pt_rows;
   return f;
+}
+
+tlm::FaceProbeDev face_probe_dev(Mesh *m) {
+  return tlm::FaceProbeDev{(const int4 *)m->fprobe.p, (double *)m->fprobe_rec.p, (int)m->fpr_face.size()};
 }
 
 tlm::DftDev dft_dev(Mesh *m) {
@@ -463,15 +476,63 @@ int finalize(Mesh *m) {
       if (m->f_out[f] > m->n_out_faces) return fail(TLM_E_BADARG, "face output number out of range");
     }
     std::vector<int> covered(m->n_exc_faces + 1, 0);
+    std::vector<int2> src(std::max(nf, 1), int2{0, -1});
     for (int h = 0; h < m->hs_n; h++) {
       const int e = m->hs_face_exc[h];
       if (e < 1 || e > m->n_exc_faces || exc_to_face[e] < 0) return fail(TLM_E_BADARG, "Huygens patch %d: bad face excitation number", h + 1);
       if (covered[e]++) return fail(TLM_E_UNSUPPORTED, "two Huygens patches on one face");
       hs[exc_to_face[e]] = double4{m->hs_offset[h], (double)m->hs_norm[3 * h], (double)m->hs_norm[3 * h + 1],
                                    (double)m->hs_norm[3 * h + 2]};
+      src[exc_to_face[e]].x = 1;
     }
-    for (int e = 1; e <= m->n_exc_faces; e++)
-      if (!covered[e]) return fail(TLM_E_UNSUPPORTED, "face excitation %d is not a Huygens patch (face point sources are not supported)", e);
+    // face point sources: one row of summed fields per excitation face that
+    // has any, tabulated for every step from the functions' value_face
+    std::vector<int> row_of(m->n_exc_faces + 1, -1);
+    const int npt = (int)m->fpt_face.size();
+    m->n_pt_rows = 0;
+    for (int e = 0; e < npt; e++) {
+      const int fe = m->fpt_face[e], comp = m->fpt_comp[e], fn = m->fpt_fn[e], ty = m->fpt_type[e];
+      if (fe < 1 || fe > m->n_exc_faces || exc_to_face[fe] < 0) return fail(TLM_E_BADARG, "face point source %d: bad face excitation number", e + 1);
+      if (comp < 1 || comp > 12) return fail(TLM_E_BADARG, "face point source %d: component %d out of range", e + 1, comp);
+      if (fn < 1 || fn > m->n_fn) return fail(TLM_E_BADARG, "face point source %d: function out of range", e + 1);
+      if (ty != 0 && ty != 1) return fail(TLM_E_BADARG, "face point source %d: source type must be 0 (hard) or 1 (soft)", e + 1);
+      if (row_of[fe] < 0) row_of[fe] = m->n_pt_rows++;
+      covered[fe]++;
+    }
+    for (int e = 1; e <= m->n_exc_faces; e++) {
+      if (!covered[e]) return fail(TLM_E_BADARG, "face excitation %d has neither a Huygens patch nor a point source", e);
+      if (row_of[e] >= 0) src[exc_to_face[e]].y = row_of[e];
+    }
+    {
+      const int R = std::max(m->n_pt_rows, 1);
+      std::vector<double> ptf((size_t)nsteps * R * 12, 0.0);
+      std::vector<int8_t> ptt((size_t)R * 6, 1);  // set_update_codes.F90:593, soft
+      for (int e = 0; e < npt; e++) {
+        const int r = row_of[m->fpt_face[e]], c = m->fpt_comp[e] - 1, fn = m->fpt_fn[e] - 1;
+        for (int t = 0; t < nsteps && t < m->n_fn_steps; t++) {
+          double &v = ptf[((size_t)t * R + r) * 12 + c];
+          v = v + m->fn_value_face[(size_t)fn * m->n_fn_steps + t];
+        }
+        if (c < 6) ptt[(size_t)r * 6 + c] = (int8_t)m->fpt_type[e];
+      }
+      if ((rc = upload(m, m->fpt_field_d, ptf)) || (rc = upload(m, m->fpt_type_d, ptt)) || (rc = upload(m, m->face_src, src)))
+        return rc;
+    }
+    // face output points
+    {
+      const int nq = (int)m->fpr_face.size();
+      std::vector<int4> pq(std::max(nq, 1), int4{0, 0, 0, 0});
+      for (int q = 0; q < nq; q++) {
+        if (m->fpr_face[q] < 1 || m->fpr_face[q] > m->n_out_faces || m->fpr_side[q] < 1 || m->fpr_side[q] > 2 ||
+            m->fpr_comp[q] < 1 || m->fpr_comp[q] > 6)
+          return fail(TLM_E_BADARG, "face output point %d: face, side or component out of range", q + 1);
+        pq[q] = int4{m->fpr_face[q] - 1, m->fpr_side[q] - 1, m->fpr_comp[q] - 1, 0};
+      }
+      if ((rc = upload(m, m->fprobe, pq)) ||
+          (rc = dalloc(m, m->fprobe_rec, (size_t)std::max(nq, 1) * nsteps * sizeof(double))))
+        return rc;
+      CK(cudaMemset(m->fprobe_rec.p, 0, m->fprobe_rec.bytes));
+    }
     if ((rc = upload(m, m->faces, fc)) || (rc = upload(m, m->face_io, io)) || (rc = upload(m, m->face_hs, hs))) return rc;
     std::vector<double> vf(std::max(nsteps, 1), 0.0);
     if (m->hs_n) {
@@ -691,6 +752,11 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
       tlm::tlm_face_kernel<T><<<(fd.n_faces + 127) / 128, 128, 0, m->stream>>>(md, fd, k);
       m->last_launches++;
     }
+    if (!m->fpr_face.empty()) {
+      const tlm::FaceProbeDev pd = face_probe_dev(m);
+      tlm::tlm_face_probe_kernel<<<(pd.n + 127) / 128, 128, 0, m->stream>>>(pd, fd.face_field, md.d_base, k);
+      m->last_launches++;
+    }
     if (dd.n_entries) {
       tlm::tlm_dft_kernel<<<(dd.n_entries + 255) / 256, 256, 0, m->stream>>>(dd, md.d_base, k);
       m->last_launches++;
@@ -904,6 +970,30 @@ int tlm_gpu_set_faces(int64_t h, int32_t n, const int32_t *cx, const int32_t *cy
   return TLM_OK;
 }
 
+int tlm_gpu_set_face_excitation(int64_t h, int32_t n, const int32_t *face_exc, const int32_t *comp,
+                                const int32_t *function, const int32_t *type) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && (!face_exc || !comp || !function || !type))) return fail(TLM_E_BADARG, "bad face excitation arguments");
+  m->fpt_face.assign(face_exc, face_exc + n);
+  m->fpt_comp.assign(comp, comp + n);
+  m->fpt_fn.assign(function, function + n);
+  m->fpt_type.assign(type, type + n);
+  return TLM_OK;
+}
+
+int tlm_gpu_set_face_outputs(int64_t h, int32_t n, const int32_t *face_out, const int32_t *side, const int32_t *comp) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && (!face_out || !side || !comp))) return fail(TLM_E_BADARG, "bad face output arguments");
+  m->fpr_face.assign(face_out, face_out + n);
+  m->fpr_side.assign(side, side + n);
+  m->fpr_comp.assign(comp, comp + n);
+  return TLM_OK;
+}
+
 int tlm_gpu_set_huygens(int64_t h, int32_t n, const int32_t *face_exc, const int32_t *norm, const double *offset,
                         const double *Ei, const double *Hi, double offset_min, double c, int32_t function) {
   Mesh *m = get(h);
@@ -1078,6 +1168,20 @@ int tlm_gpu_fetch_cell_output(int64_t h, int32_t first, int32_t n, double *out) 
   CK(cudaStreamSynchronize(m->stream));
   const size_t row = (size_t)m->n_out_cells * 6;
   CK(cudaMemcpy(out, (double *)m->cell_out.p + (size_t)(first - 1) * row, (size_t)n * row * sizeof(double),
+                cudaMemcpyDeviceToHost));
+  return TLM_OK;
+}
+
+int tlm_gpu_fetch_face_output(int64_t h, int32_t first, int32_t n, double *out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
+  if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
+  if (first < 1 || n < 0 || first + n - 1 >= m->next_step) return fail(TLM_E_BADARG, "steps not yet computed");
+  const size_t nq = m->fpr_face.size();
+  if (nq == 0 || n == 0) return TLM_OK;
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(out, (double *)m->fprobe_rec.p + (size_t)(first - 1) * nq, (size_t)n * nq * sizeof(double),
                 cudaMemcpyDeviceToHost));
   return TLM_OK;
 }
@@ -1371,6 +1475,15 @@ int batch_step(Batch *b, bool dry) {
   }
   if (b->n_spb) { tlm::tlm_special_batch_kernel<T><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
   if (b->n_faceb) { tlm::tlm_face_batch_kernel<T><<<b->n_faceb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
+  for (int i : b->active) {  // face output points of the members that have them
+    Mesh *m = get(b->handles[i]);
+    if (m && !m->fpr_face.empty()) {
+      const tlm::FaceProbeDev pd = face_probe_dev(m);
+      tlm::tlm_face_probe_kernel<<<(pd.n + 127) / 128, 128, 0, b->stream>>>(pd, (const double *)m->face_field.p,
+                                                                             (const int *)m->d_base.p, 0);
+      b->last_launches++;
+    }
+  }
   if (b->n_dftb) { tlm::tlm_dft_batch_kernel<T><<<b->n_dftb, 256, 0, b->stream>>>(bd, 0); b->last_launches++; }
   tlm::tlm_advance_batch<<<(bd.n_active + 127) / 128, 128, 0, b->stream>>>(bd.d_bases, bd.n_active, 1);
   b->last_launches++;

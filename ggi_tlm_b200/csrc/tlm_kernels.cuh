@@ -1256,6 +1256,10 @@ struct FaceDev {
   const double *value_face;  // [n_timesteps] of the Huygens function
   int n_timesteps;
   double *face_field;      // [n_out_faces][2][6]
+  const int2 *face_src;    // per special face: (Huygens patch 0/1, face point-source row or -1)
+  const double *pt_field;  // [n_timesteps][n_pt_rows][12] summed face point sources (E, H, J, M)
+  const int8_t *pt_type;   // [n_pt_rows][6] hard (0) / soft (1) source factor of E, H
+  int n_pt_rows;
 };
 
 template <typename T>
@@ -1266,6 +1270,23 @@ __global__ void tlm_face_kernel(const MeshDev<T> m, const FaceDev fd, int rel_st
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= fd.n_faces) return;
   face_body<T>(m, fd, f, rel_step);
+}
+
+// face_output_points (output_points.F90:255-444): one thread per face output
+// point copies its side and component of face_output_field, after connect.
+struct FaceProbeDev {
+  const int4 *probe;  // (output face 0-based, side 0/1, component 0..5, 0)
+  double *rec;        // [n_timesteps][n]
+  int n;
+};
+
+__global__ void tlm_face_probe_kernel(const FaceProbeDev pd, const double *face_field, const int *d_base,
+                                      int rel_step) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= pd.n) return;
+  const int t = *d_base + rel_step;
+  const int4 pr = pd.probe[q];
+  pd.rec[(size_t)(t - 1) * pd.n + q] = face_field[(size_t)pr.x * 12 + pr.y * 6 + pr.z];
 }
 
 template <typename T>
@@ -1289,44 +1310,65 @@ __device__ __forceinline__ void face_body(const MeshDev<T> &m, const FaceDev &fd
   double A_min = a1 + b1, A_max = A_min;
   double B_min = a2 + b2, B_max = B_min;
   if (io.x >= 0) {
-    // Huygens_surface_excitation (huygens_surface.F90:734-848) with
-    // get_interpolated_excitation_value (excitation.F90:645-690)
-    const double4 h = fd.hs[f];
-    const double dt = fd.dt;
-    const double t_offset = (h.x - fd.offset_min) / fd.c;
-    const double local_time = (double(t - 1)) * dt - t_offset;
-    const int ts1 = (int)round(local_time / dt);
-    const int ts2 = ts1 + 1;
-    const double delta_t = local_time - double(ts1) * dt;
-    const double v1 = (ts1 >= 1 && ts1 <= fd.n_timesteps) ? fd.value_face[ts1 - 1] : 0.0;
-    const double v2 = (ts2 >= 1 && ts2 <= fd.n_timesteps) ? fd.value_face[ts2 - 1] : 0.0;
-    const double value = v1 + delta_t * (v2 - v1) / dt;
-    const double nx_ = h.y, ny_ = h.z, nz_ = h.w;
-    const double *Hi = fd.Hi, *Ei = fd.Ei;
-    double Js[3], Ms[3];
-    Js[0] = (ny_ * value * (Hi[2]) - nz_ * value * (Hi[1]));
-    Js[1] = (nz_ * value * (Hi[0]) - nx_ * value * (Hi[2]));
-    Js[2] = (nx_ * value * (Hi[1]) - ny_ * value * (Hi[0]));
-    Ms[0] = -(ny_ * value * (Ei[2]) - nz_ * value * (Ei[1]));
-    Ms[1] = -(nz_ * value * (Ei[0]) - nx_ * value * (Ei[2]));
-    Ms[2] = -(nx_ * value * (Ei[1]) - ny_ * value * (Ei[0]));
+    // face_excitation_field / face_excitation_type of this face: point
+    // sources first (excitation_points.F90:286-323, the same value on both
+    // sides), then the Huygens J, M (huygens_surface.F90:734-848)
+    const int2 src = fd.face_src[f];
+    double fld[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double hsf[6] = {1.0, 1.0, 1.0, 1.0, 1.0, 1.0};
+    double Js[3] = {0.0, 0.0, 0.0}, Ms[3] = {0.0, 0.0, 0.0};
+    if (src.y >= 0) {
+      const double *pf = fd.pt_field + ((size_t)(t - 1) * fd.n_pt_rows + src.y) * 12;
+      const int8_t *ty = fd.pt_type + (size_t)src.y * 6;
+#pragma unroll
+      for (int k = 0; k < 6; k++) {
+        fld[k] = pf[k];
+        hsf[k] = double(ty[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        Js[k] = pf[6 + k];
+        Ms[k] = pf[9 + k];
+      }
+    }
+    if (src.x) {
+      // get_interpolated_excitation_value (excitation.F90:645-690)
+      const double4 h = fd.hs[f];
+      const double dt = fd.dt;
+      const double t_offset = (h.x - fd.offset_min) / fd.c;
+      const double local_time = (double(t - 1)) * dt - t_offset;
+      const int ts1 = (int)round(local_time / dt);
+      const int ts2 = ts1 + 1;
+      const double delta_t = local_time - double(ts1) * dt;
+      const double v1 = (ts1 >= 1 && ts1 <= fd.n_timesteps) ? fd.value_face[ts1 - 1] : 0.0;
+      const double v2 = (ts2 >= 1 && ts2 <= fd.n_timesteps) ? fd.value_face[ts2 - 1] : 0.0;
+      const double value = v1 + delta_t * (v2 - v1) / dt;
+      const double nx_ = h.y, ny_ = h.z, nz_ = h.w;
+      const double *Hi = fd.Hi, *Ei = fd.Ei;
+      Js[0] = Js[0] + (ny_ * value * (Hi[2]) - nz_ * value * (Hi[1]));
+      Js[1] = Js[1] + (nz_ * value * (Hi[0]) - nx_ * value * (Hi[2]));
+      Js[2] = Js[2] + (nx_ * value * (Hi[1]) - ny_ * value * (Hi[0]));
+      Ms[0] = Ms[0] + -(ny_ * value * (Ei[2]) - nz_ * value * (Ei[1]));
+      Ms[1] = Ms[1] + -(nz_ * value * (Ei[0]) - nx_ * value * (Ei[2]));
+      Ms[2] = Ms[2] + -(nx_ * value * (Ei[1]) - ny_ * value * (Ei[0]));
+    }
     const double dl = fd.dl, Z0 = kZ0;
-    // soft source (hard_source_factor = 1), only J and M terms are non-zero
+    // connect_normal_to_{x,y,z}.F90: the side-1 source types act on both sides
     if (dir == 1) {  // connect_normal_to_x.F90:301-305
-      A_min = A_min * 1.0 + Js[1] * dl * Z0 / 2.0 + Ms[2] * dl / 2.0;
-      A_max = A_max * 1.0 + Js[1] * dl * Z0 / 2.0 - Ms[2] * dl / 2.0;
-      B_min = B_min * 1.0 + Js[2] * dl * Z0 / 2.0 - Ms[1] * dl / 2.0;
-      B_max = B_max * 1.0 + Js[2] * dl * Z0 / 2.0 + Ms[1] * dl / 2.0;
+      A_min = A_min * hsf[1] - fld[1] * dl - fld[5] * Z0 * dl + Js[1] * dl * Z0 / 2.0 + Ms[2] * dl / 2.0;
+      A_max = A_max * hsf[1] - fld[1] * dl + fld[5] * Z0 * dl + Js[1] * dl * Z0 / 2.0 - Ms[2] * dl / 2.0;
+      B_min = B_min * hsf[2] - fld[2] * dl + fld[4] * Z0 * dl + Js[2] * dl * Z0 / 2.0 - Ms[1] * dl / 2.0;
+      B_max = B_max * hsf[2] - fld[2] * dl - fld[4] * Z0 * dl + Js[2] * dl * Z0 / 2.0 + Ms[1] * dl / 2.0;
     } else if (dir == 2) {  // connect_normal_to_y.F90:304-308
-      A_min = A_min * 1.0 + Js[0] * dl * Z0 / 2.0 - Ms[2] * dl / 2.0;
-      A_max = A_max * 1.0 + Js[0] * dl * Z0 / 2.0 + Ms[2] * dl / 2.0;
-      B_min = B_min * 1.0 + Js[2] * dl * Z0 / 2.0 + Ms[0] * dl / 2.0;
-      B_max = B_max * 1.0 + Js[2] * dl * Z0 / 2.0 - Ms[0] * dl / 2.0;
+      A_min = A_min * hsf[0] - fld[0] * dl + fld[5] * Z0 * dl + Js[0] * dl * Z0 / 2.0 - Ms[2] * dl / 2.0;
+      A_max = A_max * hsf[0] - fld[0] * dl - fld[5] * Z0 * dl + Js[0] * dl * Z0 / 2.0 + Ms[2] * dl / 2.0;
+      B_min = B_min * hsf[2] - fld[2] * dl - fld[3] * Z0 * dl + Js[2] * dl * Z0 / 2.0 + Ms[0] * dl / 2.0;
+      B_max = B_max * hsf[2] - fld[2] * dl + fld[3] * Z0 * dl + Js[2] * dl * Z0 / 2.0 - Ms[0] * dl / 2.0;
     } else {  // connect_normal_to_z.F90:302-306
-      A_min = A_min * 1.0 + Js[0] * dl * Z0 / 2.0 + Ms[1] * dl / 2.0;
-      A_max = A_max * 1.0 + Js[0] * dl * Z0 / 2.0 - Ms[1] * dl / 2.0;
-      B_min = B_min * 1.0 + Js[1] * dl * Z0 / 2.0 - Ms[0] * dl / 2.0;
-      B_max = B_max * 1.0 + Js[1] * dl * Z0 / 2.0 + Ms[0] * dl / 2.0;
+      A_min = A_min * hsf[0] - fld[0] * dl - fld[4] * Z0 * dl + Js[0] * dl * Z0 / 2.0 + Ms[1] * dl / 2.0;
+      A_max = A_max * hsf[0] - fld[0] * dl + fld[4] * Z0 * dl + Js[0] * dl * Z0 / 2.0 - Ms[1] * dl / 2.0;
+      B_min = B_min * hsf[1] - fld[1] * dl + fld[3] * Z0 * dl + Js[1] * dl * Z0 / 2.0 - Ms[0] * dl / 2.0;
+      B_max = B_max * hsf[1] - fld[1] * dl - fld[3] * Z0 * dl + Js[1] * dl * Z0 / 2.0 + Ms[0] * dl / 2.0;
     }
   }
   // new incident pulses: + cell pulls its min port from the - cell's max-port

@@ -31,7 +31,13 @@ C0 = 2.99792458e8
 MAX_ORDER = 8  # max Z-filter order carried in the coefficient tables
 
 # field components, SRC/TLM_MODULES/TLM_Modules.F90:164-176
-COMPONENTS = {"Ex": 1, "Ey": 2, "Ez": 3, "Hx": 4, "Hy": 5, "Hz": 6, "Jx": 7, "Jy": 8, "Jz": 9}
+COMPONENTS = {"Ex": 1, "Ey": 2, "Ez": 3, "Hx": 4, "Hy": 5, "Hz": 6, "Jx": 7, "Jy": 8, "Jz": 9,
+              "Mx": 10, "My": 11, "Mz": 12}
+# a point on a cell face -> (offset of the cell whose min face it is, axis, side 1/2),
+# get_min_face (MESH/general_mesh_subroutines.F90) and the side rule of
+# excitation_points.F90:295-307 / output_points.F90:386-399
+FACE_POINT = {"xmin": ((0, 0, 0), 1, 1), "xmax": ((1, 0, 0), 1, 2), "ymin": ((0, 0, 0), 2, 1),
+              "ymax": ((0, 1, 0), 2, 2), "zmin": ((0, 0, 0), 3, 1), "zmax": ((0, 0, 1), 3, 2)}
 # faces, SRC/TLM_MODULES/Mesh_Modules.F90:40-46
 FACE_XMIN, FACE_YMIN, FACE_ZMIN, FACE_XMAX, FACE_YMAX, FACE_ZMAX, CENTRE = 1, 2, 3, 4, 5, 6, 7
 # volume material types, SRC/TLM_MODULES/TLM_material_modules.F90:72-78
@@ -358,6 +364,7 @@ class PointExcitation:
     component: str
     function: int  # 1-based function number
     source_type: int = SOURCE_SOFT
+    face: str = "centre"  # or xmin, xmax, ymin, ymax, zmin, zmax: a point source on that face of the cell
 
 
 @dataclass
@@ -390,6 +397,7 @@ class HuygensPlane:
 class OutputPoint:
     cell: Tuple[int, int, int]
     component: str
+    face: str = "centre"  # or a face of the cell (field on that side of the face, after connect)
 
 
 @dataclass
@@ -562,12 +570,19 @@ def build_tables(spec: ProblemSpec) -> dict:
             dmin, dmax = calc_pml_dist(c, n, tmin, tmax)
             arr[c - 1] = dmin if dmin != 0 else dmax
     in_pml = (dza[:, None, None] != 0) | (dya[None, :, None] != 0) | (dxa[None, None, :] != 0)
+    for q in list(spec.point_excitations) + list(spec.outputs):
+        if q.face != "centre" and q.face not in FACE_POINT:
+            raise ValueError(f"unknown face {q.face!r}")
+    centre_pts = [q for q in spec.point_excitations if q.face == "centre"]
+    centre_outs = [q for q in spec.outputs if q.face == "centre"]
     cell_exc = np.zeros((nz, ny, nx), dtype=bool)
-    for pe in spec.point_excitations:
+    for pe in centre_pts:
+        if COMPONENTS[pe.component] > 9:
+            raise ValueError("a cell-centre source drives E, H or J (components 1..9)")
         i, j, k = pe.cell
         cell_exc[k - 1, j - 1, i - 1] = True
     cell_out = np.zeros((nz, ny, nx), dtype=bool)
-    for op in spec.outputs:
+    for op in centre_outs:
         i, j, k = op.cell
         cell_out[k - 1, j - 1, i - 1] = True
     if np.any(in_pml & cell_exc):
@@ -673,7 +688,7 @@ def build_tables(spec: ProblemSpec) -> dict:
 
     # excitation functions + point excitations
     val, valf = excitation_tables(spec.functions, nsteps, dt)
-    pts = spec.point_excitations
+    pts = centre_pts
     tables.update(
         n_functions=len(spec.functions), fn_value=val, fn_value_face=valf,
         n_exc_points=len(pts),
@@ -685,9 +700,21 @@ def build_tables(spec: ProblemSpec) -> dict:
         n_exc_cells=int(cell_exc.sum()),
     )
 
-    # special faces: Huygens excitation faces and DFT output faces, in connect order
+    # special faces: Huygens and face-point excitation faces, DFT and
+    # face-point output faces, in connect order
     face_exc = {}
     face_out = {}
+
+    def face_key(q):
+        (ox, oy, oz), axis, side = FACE_POINT[q.face]
+        return ((q.cell[0] + ox, q.cell[1] + oy, q.cell[2] + oz), axis), side
+
+    face_pts = [(q, *face_key(q)) for q in spec.point_excitations if q.face != "centre"]
+    face_probes = [(q, *face_key(q)) for q in spec.outputs if q.face != "centre"]
+    for _, key, _ in face_pts:
+        face_exc[key] = True
+    for _, key, _ in face_probes:
+        face_out[key] = True
     hs = spec.huygens
     if hs is not None:
         for f in _plane_faces(hs.axis, hs.index, hs.r0, hs.r1):
@@ -717,6 +744,19 @@ def build_tables(spec: ProblemSpec) -> dict:
             fout_num[key] = no
         face_cx.append(cx); face_cy.append(cy); face_cz.append(cz); face_dir.append(axis)
         face_e.append(e); face_o.append(o)
+    tables.update(
+        n_face_points=len(face_pts),
+        fpt_face=np.array([fexc_num[k] for _, k, _ in face_pts], dtype=np.int32),
+        fpt_comp=np.array([COMPONENTS[q.component] for q, _, _ in face_pts], dtype=np.int32),
+        fpt_fn=np.array([q.function for q, _, _ in face_pts], dtype=np.int32),
+        fpt_type=np.array([q.source_type for q, _, _ in face_pts], dtype=np.int32),
+        n_face_probes=len(face_probes),
+        fprobe_face=np.array([fout_num[k] for _, k, _ in face_probes], dtype=np.int32),
+        fprobe_side=np.array([sd for _, _, sd in face_probes], dtype=np.int32),
+        fprobe_comp=np.array([COMPONENTS[q.component] for q, _, _ in face_probes], dtype=np.int32))
+    for q, _, _ in face_probes:
+        if COMPONENTS[q.component] > 6:
+            raise ValueError("a face output point records E or H (components 1..6)")
     tables.update(n_faces=len(ordered), face_cx=np.array(face_cx, dtype=np.int32),
                   face_cy=np.array(face_cy, dtype=np.int32), face_cz=np.array(face_cz, dtype=np.int32),
                   face_dir=np.array(face_dir, dtype=np.int32), face_exc=np.array(face_e, dtype=np.int32),
@@ -726,6 +766,8 @@ def build_tables(spec: ProblemSpec) -> dict:
     if hs is not None:
         K, Ei, Hi = huygens_vectors(hs.ktheta, hs.kphi, hs.etheta, hs.ephi)
         faces = _plane_faces(hs.axis, hs.index, hs.r0, hs.r1)
+        if not faces:
+            raise ValueError("empty Huygens patch: r0 and r1 are (min, max) cell ranges")
         norms, offsets, fexc = [], [], []
         xmin0, ymin0, zmin0 = spec.origin
         cents = []
@@ -774,9 +816,9 @@ def build_tables(spec: ProblemSpec) -> dict:
     # outputs
     tables["n_out_cells"] = int(cell_out.sum())
     tables["out_cell"] = np.array(
-        [out_number[(o.cell[2] - 1) * nx * ny + (o.cell[1] - 1) * nx + o.cell[0] - 1] for o in spec.outputs],
+        [out_number[(o.cell[2] - 1) * nx * ny + (o.cell[1] - 1) * nx + o.cell[0] - 1] for o in centre_outs],
         dtype=np.int32)
-    tables["out_comp"] = np.array([COMPONENTS[o.component] for o in spec.outputs], dtype=np.int32)
+    tables["out_comp"] = np.array([COMPONENTS[o.component] for o in centre_outs], dtype=np.int32)
 
     # DFT surfaces: one reference surface entry per frequency
     freqs, comps, ptr, fo, fs = [], [], [0], [], []

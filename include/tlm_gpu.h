@@ -133,6 +133,24 @@ int tlm_gpu_set_huygens(int64_t handle, int32_t n_patches, const int32_t *face_e
                         const double *offset, const double *Ei, const double *Hi, double offset_min, double c,
                         int32_t function);
 
+/* Point sources on cell faces (SRC/EXCITATION/excitation_points.F90:
+   135-211 numbering, :286-323 per step): 1-based excitation face number of
+   the face (the min face of the cell on its + side, as in set_faces),
+   component 1..12 (Ex..Hz, Jx..Jz, Mx..Mz), excitation function, source type
+   (0 hard, 1 soft).  value_face(timestep) of the function is added on both
+   sides of the face, and the type of the E/H component set there; connect
+   then applies them (SRC/TLM_SOLVER/connect_normal_to_x.F90:287-307 and the
+   y, z analogues).  Every excitation face needs a Huygens patch or a point. */
+int tlm_gpu_set_face_excitation(int64_t handle, int32_t n_points, const int32_t *face_exc, const int32_t *component,
+                                const int32_t *function, const int32_t *source_type);
+
+/* Output points on cell faces (SRC/OUTPUT/output_points.F90:255-444):
+   1-based output face number, side (1 = the min-side field, face_xmin/ymin/
+   zmin; 2 = the max side) and component 1..6 of face_output_field after
+   connect, recorded every step. */
+int tlm_gpu_set_face_outputs(int64_t handle, int32_t n_points, const int32_t *face_out, const int32_t *side,
+                             const int32_t *component);
+
 /* Number of output cells; cell_output_field(1:n,1:6) is recorded every
    step (SRC/TLM_SOLVER/scatter.F90:465-480, scatter_PML.F90 STAGE 12). */
 int tlm_gpu_set_outputs(int64_t handle, int32_t n_out_cells);
@@ -163,6 +181,10 @@ int tlm_gpu_synchronize(int64_t handle);
 /* cell_output_field snapshots of steps first..first+n-1:
    out[n][n_out_cells][6] doubles. */
 int tlm_gpu_fetch_cell_output(int64_t handle, int32_t first_step, int32_t n_steps, double *out);
+
+/* Face output point values of steps first..first+n-1: out[n][n_points]
+   (the time of step k is (k-1)*dt + dt/2, output_points.F90:441). */
+int tlm_gpu_fetch_face_output(int64_t handle, int32_t first_step, int32_t n_steps, double *out);
 
 /* DFT accumulators (re, im) per surface face in set_dft order. */
 int tlm_gpu_fetch_dft(int64_t handle, double *out);

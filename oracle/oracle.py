@@ -45,6 +45,9 @@ class _Problem(C.Structure):
         ("dft_face_out", _i32p), ("dft_face_side", _i32p),
         ("n_small_to_zero", C.c_int32), ("small_to_zero_value", C.c_double),
         ("pml_sigma", _f64p),
+        ("n_face_points", C.c_int32), ("fpt_face", _i32p), ("fpt_comp", _i32p), ("fpt_fn", _i32p),
+        ("fpt_type", _i32p),
+        ("n_face_probes", C.c_int32), ("fprobe_face", _i32p), ("fprobe_side", _i32p), ("fprobe_comp", _i32p),
     ]
 
 
@@ -69,6 +72,7 @@ def _load():
         _lib.tlm_oracle_run.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _f64p]
         _lib.tlm_oracle_get_dft.argtypes = [C.c_void_p, _f64p]
         _lib.tlm_oracle_get_links.argtypes = [C.c_void_p, _f64p]
+        _lib.tlm_oracle_get_face_probes.argtypes = [C.c_void_p, _f64p]
     return _lib
 
 
@@ -79,6 +83,11 @@ class Oracle:
         lib = _load()
         self.t = t
         keep = []
+
+        def arr_empty():
+            a = np.zeros(1, dtype=np.int32)
+            keep.append(a)
+            return a.ctypes.data_as(_i32p)
 
         def arr(key, dtype):
             a = np.ascontiguousarray(t[key], dtype=dtype).reshape(-1)
@@ -108,6 +117,10 @@ class Oracle:
         p.hs_Hi[:] = [float(v) for v in t["hs_Hi"]]
         p.hs_offset_min = float(t["hs_offset_min"])
         p.hs_c = float(t["hs_c"])
+        p.n_face_points = int(t.get("n_face_points", 0))
+        p.n_face_probes = int(t.get("n_face_probes", 0))
+        for k in ("fpt_face", "fpt_comp", "fpt_fn", "fpt_type", "fprobe_face", "fprobe_side", "fprobe_comp"):
+            setattr(p, k, arr(k, np.int32) if k in t else arr_empty())
         if int(t.get("n_pml_material_cells", 0)):
             p.pml_sigma = arr("pml_sigma", np.float64)
         p.n_small_to_zero = int(t.get("n_small_to_zero", 0))
@@ -134,6 +147,13 @@ class Oracle:
         out = np.zeros(max(2 * n, 1))
         _load().tlm_oracle_get_dft(self._h, out.ctypes.data_as(_f64p))
         return out[: 2 * n].reshape(-1, 2)
+
+    def face_probes(self) -> np.ndarray:
+        """Face output point values [n_face_probes, steps run so far]."""
+        n = int(self.t.get("n_face_probes", 0))
+        out = np.zeros(max(self.step * n, 1))
+        _load().tlm_oracle_get_face_probes(self._h, out.ctypes.data_as(_f64p))
+        return out[: self.step * n].reshape(self.step, n).T.copy()
 
     def links(self) -> np.ndarray:
         t = self.t

@@ -63,6 +63,7 @@ struct tlm_oracle_state {
   pml_cell_t *pml;
   pml_mat_t *pml_mat;  /* PML cells inside a volume material, traversal order */
   int32_t *pml_mat_pos; /* PML_material_array_pos per PML cell, 1-based or 0 */
+  double *face_probe_rec; /* [n_timesteps][n_face_probes] */
   double *cell_exc;    /* [n_exc_cells][9] */
   int32_t *cell_exc_type; /* [n_exc_cells][6] */
   double *cell_out;    /* [n_out_cells][6] */
@@ -142,6 +143,7 @@ tlm_oracle_state *tlm_oracle_create(const tlm_oracle_problem *p) {
     }
   }
   s->pml = (pml_cell_t *)calloc((size_t)p->n_pml_cells + 1, sizeof(pml_cell_t));
+  s->face_probe_rec = (double *)calloc((size_t)p->n_timesteps * p->n_face_probes + 1, sizeof(double));
   /* allocate_PML_material_data, TLM_PML_volume_materials.F90:590-740: a
      PML cell whose special cell has a DISPERSIVE-type material gets the next
      PML material record, in special-cell (traversal) order; all zero */
@@ -175,7 +177,7 @@ tlm_oracle_state *tlm_oracle_create(const tlm_oracle_problem *p) {
 
 void tlm_oracle_destroy(tlm_oracle_state *s) {
   if (!s) return;
-  free(s->V); free(s->sp_filter); free(s->eps_f); free(s->mu_f); free(s->pml); free(s->pml_mat); free(s->pml_mat_pos);
+  free(s->V); free(s->sp_filter); free(s->eps_f); free(s->mu_f); free(s->pml); free(s->pml_mat); free(s->pml_mat_pos); free(s->face_probe_rec);
   free(s->cell_exc); free(s->cell_exc_type); free(s->cell_out); free(s->face_exc);
   free(s->face_exc_type); free(s->face_out); free(s->face_code); free(s->dft);
   free(s);
@@ -207,6 +209,17 @@ static void excitation(tlm_oracle_state *s, int timestep) {
     double value = p->fn_value[(size_t)(p->pt_fn[e] - 1) * p->n_timesteps + (timestep - 1)];
     s->cell_exc[cell * 9 + comp] = s->cell_exc[cell * 9 + comp] + value;
     if (comp < 6) s->cell_exc_type[cell * 6 + comp] = p->pt_type[e];
+  }
+  /* Point_excitation, face points (excitation_points.F90:286-323): the value
+     goes to both sides of the face, the source type too (components 1..6) */
+  for (int e = 0; e < p->n_face_points; e++) {
+    int face = p->fpt_face[e] - 1, comp = p->fpt_comp[e] - 1;
+    double value = p->fn_value_face[(size_t)(p->fpt_fn[e] - 1) * p->n_timesteps + (timestep - 1)];
+    for (int side = 0; side < 2; side++) {
+      double *fe = s->face_exc + (size_t)face * 24 + side * 12;
+      fe[comp] = fe[comp] + value;
+      if (comp < 6) s->face_exc_type[(size_t)face * 12 + side * 6 + comp] = p->fpt_type[e];
+    }
   }
   for (int h = 0; h < p->hs_n; h++) {
     double value = interp_face_value(s, p->hs_offset[h], timestep);
@@ -920,6 +933,10 @@ int tlm_oracle_run(tlm_oracle_state *s, int32_t first_step, int32_t n_steps, dou
       memcpy(cell_out + (size_t)k * p->n_out_cells * 6, s->cell_out, sizeof(double) * p->n_out_cells * 6);
     time = time + p->dt / 2.0;
     connect(s);
+    /* face_output_points (output_points.F90:255-444): side 1/2 of the output face */
+    for (int q = 0; q < p->n_face_probes; q++)
+      s->face_probe_rec[(size_t)(timestep - 1) * p->n_face_probes + q] =
+          s->face_out[(size_t)(p->fprobe_face[q] - 1) * 12 + (p->fprobe_side[q] - 1) * 6 + (p->fprobe_comp[q] - 1)];
     dft_surfaces(s, time);
     outer_boundary(s);
     s->timestep = timestep;
@@ -930,6 +947,11 @@ int tlm_oracle_run(tlm_oracle_state *s, int32_t first_step, int32_t n_steps, dou
 int tlm_oracle_get_dft(tlm_oracle_state *s, double *out) {
   int n = s->p.n_dft ? s->p.dft_face_ptr[s->p.n_dft] : 0;
   memcpy(out, s->dft, sizeof(double) * 2 * (size_t)n);
+  return 0;
+}
+
+int tlm_oracle_get_face_probes(tlm_oracle_state *s, double *out) {
+  memcpy(out, s->face_probe_rec, sizeof(double) * (size_t)s->timestep * s->p.n_face_probes);
   return 0;
 }
 

@@ -107,6 +107,15 @@ typedef struct {
   /* PML_parameters(:)%sx,sy,sz (TLM_PML_volume_materials.F90:329-331), 3 per
      parameter row; needed by PML cells inside a volume material, else NULL */
   const double *pml_sigma;
+
+  /* point sources on cell faces (EXCITATION/excitation_points.F90:286-323):
+     1-based excitation face number, component 1..12, function, source type */
+  int32_t n_face_points;
+  const int32_t *fpt_face, *fpt_comp, *fpt_fn, *fpt_type;
+  /* output points on cell faces (OUTPUT/output_points.F90:255-444): 1-based
+     output face number, side 1 (min) / 2 (max), component 1..6 */
+  int32_t n_face_probes;
+  const int32_t *fprobe_face, *fprobe_side, *fprobe_comp;
 } tlm_oracle_problem;
 
 typedef struct tlm_oracle_state tlm_oracle_state;
@@ -118,6 +127,8 @@ void tlm_oracle_destroy(tlm_oracle_state *s);
 int tlm_oracle_run(tlm_oracle_state *s, int32_t first_step, int32_t n_steps, double *cell_out);
 /* DFT accumulators: per surface, per face, (re,im) */
 int tlm_oracle_get_dft(tlm_oracle_state *s, double *out);
+/* face output point values of every completed timestep: [timestep][n_face_probes] */
+int tlm_oracle_get_face_probes(tlm_oracle_state *s, double *out);
 /* link array dump in the reference layout V(12, nx, ny, nz) interior only */
 int tlm_oracle_get_links(tlm_oracle_state *s, double *out);
 
