@@ -16,7 +16,8 @@ from typing import List, Optional, Tuple
 
 import numpy as np
 
-from .problem import (C0, MAT_DISPERSIVE, Block, DFTSurface, ExcitationFunction, HuygensPlane, OutputPoint,
+from .problem import (C0, MAT_DISPERSIVE, Block, DFTSurface, ExcitationFunction, HuygensBox, HuygensPlane,
+                      OutputPoint,
                       PointExcitation, ProblemSpec, Sfilter, Sphere, VolumeMaterial, nint)
 
 
@@ -77,6 +78,17 @@ def kat_material_stability() -> ProblemSpec:
         outputs=[OutputPoint((11, 11, 11), "Ey")])
 
 
+def cubic_mesh_dl(xmin: float, xmax: float, n: int) -> float:
+    """MESH/set_mesh_parameters.F90:61-66, dl=(dlx+dly+dlz)/3 on a cubic
+    mesh, with the division by 3 evaluated as a multiplication by 1/3 as the
+    reference's build flags (-funsafe-math-optimizations) compile it: for a
+    4 m / 40-cell mesh this gives dl = 0.1 exactly where a true division
+    gives 0.1 + 1 ulp, and the TEST_DATA/HUYGENS_SURFACE output point
+    (0,0,0) then lands in cell 21 as in the golden series."""
+    dlx = (xmax - xmin) / float(n)
+    return (dlx + dlx + dlx) * (1.0 / 3.0)
+
+
 def point_to_cell(p: float, xmin: float, dl: float) -> int:
     """MESH/general_mesh_subroutines.F90:345-383, int((p-xmin)/dl)+1, with the
     division evaluated as a multiplication by 1/dl, as the reference's build
@@ -92,8 +104,7 @@ def kat_material_test2() -> ProblemSpec:
     same 2nd-order rational for eps_r and mu_r, complex poles), soft Ex
     Gaussian point source and an Ex probe 2.4 mm apart, R=0."""
     xmin, xmax, n = -3.0e-3, 3.0e-3, 60
-    dlx = (xmax - xmin) / float(n)
-    dl = (dlx + dlx + dlx) / 3.0  # set_mesh_parameters.F90:61-66
+    dl = cubic_mesh_dl(xmin, xmax, n)
     steps = nint(10e-10 / _dt(dl))
     f = Sfilter(1e10, [2.0, 3.1827e-1, 4.0518e-1], [1.0, 3.1827e-1, 4.0518e-1])
     lorentz = VolumeMaterial(MAT_DISPERSIVE, f, 0.0, Sfilter(f.wnorm, list(f.a), list(f.b)), 0.0)
@@ -127,11 +138,31 @@ def pml_dielectric_slab(n: int = 40, pml: int = 8, steps: int = 300, eps_r: floa
                  OutputPoint((c + 4, c, pad + slab_top + 2), "Ex")])
 
 
+def kat_huygens_box(component: str = "Ex") -> ProblemSpec:
+    """TEST_DATA/HUYGENS_SURFACE/PROBLEM_SPECIFICATION_FILES/huygens_test.inp:
+    40^3 cells over 4 m, R=0, a closed Huygens surface on the 2 m cube at the
+    centre (cells 11..30 on each axis, side 1) launching a Gaussian plane
+    wave along the cube diagonal (theta 54.73, phi 45 degrees, polarisation
+    (1.0, 0.5)); the fields at the centre point (0,0,0) -> cell (21,21,21).
+    The reference's volume and output surfaces of that input are
+    post-processing only and are left out."""
+    xmin, n = -2.0, 40
+    dl = cubic_mesh_dl(xmin, 2.0, n)
+    steps = nint(2e-8 / _dt(dl))
+    c = point_to_cell(0.0, xmin, dl)
+    return ProblemSpec(
+        nx=n, ny=n, nz=n, dl=dl, n_timesteps=steps, R=(0.0,) * 6, origin=(xmin,) * 3,
+        functions=[ExcitationFunction("gaussian", (1.0, 2e-9, 6e-9))],
+        huygens=HuygensBox((11, 30), (11, 30), (11, 30), 1, 54.73, 45.0, 1.0, 0.5),
+        outputs=[OutputPoint((c, c, c), component)])
+
+
 KAT_CASES = {
     "tem_pml_Ey": kat_tem_pml,
     "tem_material_Ey": kat_tem_material,
     "material_stability_Ey": kat_material_stability,
     "material_test2_Ex": kat_material_test2,
+    **{f"huygens_box_{f}": (lambda f=f: kat_huygens_box(f)) for f in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")},
 }
 
 

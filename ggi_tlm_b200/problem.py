@@ -394,6 +394,32 @@ class HuygensPlane:
 
 
 @dataclass
+class HuygensBox:
+    """A closed Huygens surface on the boundary faces of the block of cells
+    i0..i1, j0..j1, k0..k1 (1-based, inclusive): the reference's
+    rectangular_block surface aligned with the mesh.  Its triangles
+    (GEOMETRY/build_surface_rectangular_block.F90) have normals that point
+    into the block under triangle_normal's (v3-v1)x(v2-v1)
+    (GEOMETRY/functions.F90:241-262), and the surface mesher
+    (MESH/mesh_triangle.F90) records each face on the cell behind the
+    triangle, facing along that normal: with side 1 the patches sit on the
+    neighbouring outside cells with inward normals, and the incident field
+    appears inside the block.  Side -1 moves every patch to the block's own
+    boundary cell with an outward normal.  Pinned by TEST_DATA/HUYGENS_SURFACE
+    (*_centre.tout_ref)."""
+
+    i: Tuple[int, int]
+    j: Tuple[int, int]
+    k: Tuple[int, int]
+    function: int
+    ktheta: float
+    kphi: float
+    etheta: float
+    ephi: float
+    side: int = 1
+
+
+@dataclass
 class OutputPoint:
     cell: Tuple[int, int, int]
     component: str
@@ -429,7 +455,7 @@ class ProblemSpec:
     material_regions: List[Tuple[int, object]] = field(default_factory=list)  # (material number, Block|Sphere)
     functions: List[ExcitationFunction] = field(default_factory=list)
     point_excitations: List[PointExcitation] = field(default_factory=list)
-    huygens: Optional[HuygensPlane] = None
+    huygens: Optional[object] = None  # HuygensPlane or HuygensBox
     outputs: List[OutputPoint] = field(default_factory=list)
     dft_surfaces: List[DFTSurface] = field(default_factory=list)
     reduced_c: float = 1.0
@@ -541,6 +567,42 @@ def huygens_vectors(ktheta_deg: float, kphi_deg: float, etheta: float, ephi: flo
     Hi = [ky * Ei[2] - kz * Ei[1], kz * Ei[0] - kx * Ei[2], kx * Ei[1] - ky * Ei[0]]
     Hi = [h / hs_z0 for h in Hi]
     return (kx, ky, kz), Ei, Hi
+
+
+def _huygens_patches(hs) -> List[Tuple[Tuple[int, int, int], int]]:
+    """(cell, face code 1..6) of every Huygens patch after the side flip
+    (huygens_surface.F90:412-450), in the surface mesher's face_list order
+    (face code, then cz, cy, cx; MESH/build_surface_mesh.F90:100-150)."""
+    rec = []
+    if isinstance(hs, HuygensPlane):
+        # recorded as the min face of the cell on the + side (normal -axis)
+        for c in _plane_faces(hs.axis, hs.index, hs.r0, hs.r1):
+            rec.append((c, hs.axis))
+    else:
+        (i0, i1), (j0, j1), (k0, k1) = hs.i, hs.j, hs.k
+        if i0 > i1 or j0 > j1 or k0 > k1:
+            raise ValueError("empty Huygens box")
+        # min faces of the cells just past the block's max planes, max faces
+        # of the cells just before its min planes (inward normals)
+        for code in (FACE_XMIN, FACE_YMIN, FACE_ZMIN, FACE_XMAX, FACE_YMAX, FACE_ZMAX):
+            axis = (code - 1) % 3
+            at = (i1 + 1, j1 + 1, k1 + 1)[axis] if code <= 3 else (i0 - 1, j0 - 1, k0 - 1)[axis]
+            rng = [range(i0, i1 + 1), range(j0, j1 + 1), range(k0, k1 + 1)]
+            rng[axis] = range(at, at + 1)
+            for cz in rng[2]:
+                for cy in rng[1]:
+                    for cx in rng[0]:
+                        rec.append(((cx, cy, cz), code))
+    out = []
+    for c, code in rec:
+        if hs.side != 1:  # excitation on the other side of the face
+            axis = (code - 1) % 3
+            c = list(c)
+            c[axis] += -1 if code <= 3 else 1
+            code = code + 3 if code <= 3 else code - 3
+            c = tuple(c)
+        out.append((c, code))
+    return out
 
 
 def build_tables(spec: ProblemSpec) -> dict:
@@ -716,9 +778,20 @@ def build_tables(spec: ProblemSpec) -> dict:
     for _, key, _ in face_probes:
         face_out[key] = True
     hs = spec.huygens
-    if hs is not None:
-        for f in _plane_faces(hs.axis, hs.index, hs.r0, hs.r1):
-            face_exc[(f, hs.axis)] = True
+    hs_patches = _huygens_patches(hs) if hs is not None else []
+    if hs is not None and not hs_patches:
+        raise ValueError("empty Huygens patch: r0 and r1 are (min, max) cell ranges")
+
+    def connect_key(c, code):  # a cell face -> (cell whose min face it is, axis)
+        axis = (code - 1) % 3
+        if code <= 3:
+            return (tuple(c), axis + 1)
+        c = list(c)
+        c[axis] += 1
+        return (tuple(c), axis + 1)
+
+    for c, code in hs_patches:
+        face_exc[connect_key(c, code)] = True
     for ds in spec.dft_surfaces:
         for f in _plane_faces(ds.axis, ds.index, ds.r0, ds.r1):
             face_out[(f, ds.axis)] = True
@@ -765,33 +838,23 @@ def build_tables(spec: ProblemSpec) -> dict:
     # Huygens surface data, huygens_surface.F90:247-715
     if hs is not None:
         K, Ei, Hi = huygens_vectors(hs.ktheta, hs.kphi, hs.etheta, hs.ephi)
-        faces = _plane_faces(hs.axis, hs.index, hs.r0, hs.r1)
-        if not faces:
-            raise ValueError("empty Huygens patch: r0 and r1 are (min, max) cell ranges")
         norms, offsets, fexc = [], [], []
         xmin0, ymin0, zmin0 = spec.origin
         cents = []
-        for (cx, cy, cz) in faces:
-            cell_m = [cx, cy, cz]
-            cell_m[hs.axis - 1] -= 1
+        for (c, code) in hs_patches:
+            axis = (code - 1) % 3
             n = [0, 0, 0]
-            off = [-0.5, -0.5, -0.5]
-            if hs.side == 1:
-                n[hs.axis - 1] = -1
-                off[hs.axis - 1] = -1.0
-                cell_ref = [cx, cy, cz]
-            else:
-                n[hs.axis - 1] = 1
-                off[hs.axis - 1] = 0.0
-                cell_ref = cell_m
+            n[axis] = -1 if code <= 3 else 1
             # get_cell_point_coordinate, general_mesh_subroutines.F90:84-140
-            x = xmin0 + (cell_ref[0] + off[0]) * dl
-            y = ymin0 + (cell_ref[1] + off[1]) * dl
-            z = zmin0 + (cell_ref[2] + off[2]) * dl
+            off = [-0.5, -0.5, -0.5]
+            off[axis] = -1.0 if code <= 3 else 0.0
+            x = xmin0 + (c[0] + off[0]) * dl
+            y = ymin0 + (c[1] + off[1]) * dl
+            z = zmin0 + (c[2] + off[2]) * dl
             cents.append((x, y, z))
             norms.extend(n)
             offsets.append(K[0] * x + K[1] * y + K[2] * z)
-            fexc.append(fexc_num[((cx, cy, cz), hs.axis)])
+            fexc.append(fexc_num[connect_key(c, code)])
         # surface mesh extents are the face-centre extents of the recorded
         # faces (build_surface_mesh.F90:120-160); both sides of a face share
         # one centre
@@ -804,7 +867,7 @@ def build_tables(spec: ProblemSpec) -> dict:
                                 (bx[1], by[1], bz[0]), (bx[0], by[0], bz[1]), (bx[1], by[0], bz[1]),
                                 (bx[0], by[1], bz[1]), (bx[1], by[1], bz[1])):
             offset_min = min(K[0] * xx_ + K[1] * yy_ + K[2] * zz_, offset_min)
-        tables.update(hs_n=len(faces), hs_face_exc=np.array(fexc, dtype=np.int32),
+        tables.update(hs_n=len(hs_patches), hs_face_exc=np.array(fexc, dtype=np.int32),
                       hs_norm=np.array(norms, dtype=np.int32), hs_offset=np.array(offsets),
                       hs_Ei=np.array(Ei), hs_Hi=np.array(Hi), hs_offset_min=offset_min - dl / 2.0,
                       hs_c=C0 / spec.reduced_c, hs_fn=hs.function)

@@ -19,6 +19,8 @@ CASES = {
     "tem_material_Ey": "TEM_MATERIAL_TEST/PROBLEM_SPECIFICATION_FILES/Ey.tout_ref",
     "material_stability_Ey": "MATERIAL_STABILITY_TEST/PROBLEM_SPECIFICATION_FILES/cavity.field.tout_ref",
     "material_test2_Ex": "MATERIAL_TEST2/PROBLEM_SPECIFICATION_FILES/mat_test.field.tout_ref",
+    **{f"huygens_box_{f}": f"HUYGENS_SURFACE/PROBLEM_SPECIFICATION_FILES/{f}_centre.tout_ref"
+       for f in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")},
 }
 
 

@@ -65,9 +65,20 @@ def test_point_mapping_uses_reciprocal_multiply():
     """The MATERIAL_TEST2 source sits 4.2 mm from xmin, exactly on a cell
     boundary of 0.1 mm cells: int(4.2e-3/1e-4) is 41 but int(4.2e-3*(1/1e-4))
     is 42, and only the second one (cell 43) reproduces the golden series."""
-    xmin, dl = -3.0e-3, (6.0e-3 / 60 * 3) / 3.0
+    xmin, dl = -3.0e-3, cases.cubic_mesh_dl(-3.0e-3, 3.0e-3, 60)
     assert int((1.2e-3 - xmin) / dl) + 1 == 42
     assert cases.point_to_cell(1.2e-3, xmin, dl) == 43
     spec = cases.kat_material_test2()
     assert spec.point_excitations[0].cell == (43, 31, 31)
     assert spec.outputs[0].cell == (19, 31, 31)
+
+
+def test_mesh_dl_uses_reciprocal_of_three():
+    """On the HUYGENS_SURFACE mesh (4 m, 40 cells) (dlx+dly+dlz)/3 is one ulp
+    above 0.1 and would put the output point (0,0,0) in cell 20; the
+    reference's (dlx+dly+dlz)*(1/3) gives 0.1 and cell 21, which the golden
+    series confirms."""
+    dlx = 4.0 / 40
+    assert (dlx + dlx + dlx) / 3.0 != 0.1
+    assert cases.cubic_mesh_dl(-2.0, 2.0, 40) == 0.1
+    assert cases.kat_huygens_box().outputs[0].cell == (21, 21, 21)
