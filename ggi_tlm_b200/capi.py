@@ -38,7 +38,7 @@ EXPORTS = [
     "tlm_gpu_num_variants", "tlm_gpu_fetch_links_noalloc", "tlm_gpu_batch_create", "tlm_gpu_batch_set_variant",
     "tlm_gpu_batch_run", "tlm_gpu_batch_synchronize", "tlm_gpu_batch_last_run", "tlm_gpu_batch_destroy",
     "tlm_gpu_set_small_to_zero", "tlm_gpu_set_pml_sigma", "tlm_gpu_set_face_excitation",
-    "tlm_gpu_set_face_outputs", "tlm_gpu_fetch_face_output",
+    "tlm_gpu_set_face_outputs", "tlm_gpu_fetch_face_output", "tlm_gpu_set_outer_huygens",
 ]
 
 
@@ -78,6 +78,7 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_pml_sigma": [i64, i32, _f64p],
         "tlm_gpu_set_face_excitation": [i64, i32, _i32p, _i32p, _i32p, _i32p],
         "tlm_gpu_set_face_outputs": [i64, i32, _i32p, _i32p, _i32p],
+        "tlm_gpu_set_outer_huygens": [i64, i32, _i32p, _f64p, _f64p, _f64p, C.c_double, C.c_double, i32],
         "tlm_gpu_fetch_face_output": [i64, i32, i32, _f64p],
         "tlm_gpu_set_excitation": [i64, i32, i32, _f64p, _f64p, i32, _i32p, _i32p, _i32p, _i32p, i32],
         "tlm_gpu_set_faces": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, i32, i32],
@@ -191,7 +192,11 @@ class GpuMesh:
         fa = [_i32(t[k]) for k in ("face_cx", "face_cy", "face_cz", "face_dir", "face_exc", "face_out")]
         _check(lib.tlm_gpu_set_faces(self.h, int(t["n_faces"]), *[_p(x) for x in fa], int(t["n_exc_faces"]),
                                      int(t["n_out_faces"])))
-        if int(t["hs_n"]):
+        if int(t["hs_n"]) and int(t.get("hs_outer", 0)):
+            hc, ho, Ei, Hi = _i32(t["hs_cell"]), _f64(t["hs_offset"]), _f64(t["hs_Ei"]), _f64(t["hs_Hi"])
+            _check(lib.tlm_gpu_set_outer_huygens(self.h, int(t["hs_n"]), _p(hc), _p(ho), _p(Ei), _p(Hi),
+                                                 float(t["hs_offset_min"]), float(t["hs_c"]), int(t["hs_fn"])))
+        elif int(t["hs_n"]):
             hf, hn, ho, Ei, Hi = (_i32(t["hs_face_exc"]), _i32(t["hs_norm"]), _f64(t["hs_offset"]), _f64(t["hs_Ei"]),
                                   _f64(t["hs_Hi"]))
             _check(lib.tlm_gpu_set_huygens(self.h, int(t["hs_n"]), _p(hf), _p(hn), _p(ho), _p(Ei), _p(Hi),

@@ -92,6 +92,8 @@ struct Mesh {
   std::vector<double> hs_offset;
   double hs_Ei[3] = {0, 0, 0}, hs_Hi[3] = {0, 0, 0}, hs_offset_min = 0, hs_c = 0;
   int hs_fn = 0;
+  bool hs_outer = false;             // the Huygens surface is the outer boundary
+  std::vector<int32_t> hs_cell;      // outer: 4 per patch (cx, cy, cz 1-based, face code)
   int n_out_cells = 0;
   int n_dft = 0;
   std::vector<double> dft_freq;
@@ -100,7 +102,8 @@ struct Mesh {
   // device buffers
   DevBuf links, seg_mask, seg_base, sp_rec, sp_pos, pml_state, pml_par, pml_ixt, filt, mats_d, exc_field, exc_type,
       cell_out, faces, face_io, face_hs, value_face, face_field, dft_entry, dft_phasor, dft_acc, d_base,
-      pmm_pos, pmm_parmat, pmm_state, pmm_sigma, face_src, fpt_field_d, fpt_type_d, fprobe, fprobe_rec;
+      pmm_pos, pmm_parmat, pmm_state, pmm_sigma, face_src, fpt_field_d, fpt_type_d, fprobe, fprobe_rec,
+      ohs_face, ohs_offset;
   int n_pt_rows = 0;
   int n_pmm = 0;  // PML cells inside a volume material
   int n_filt = 0, filt_eo = 0, filt_mo = 0;
@@ -234,6 +237,24 @@ tlm::FaceDev face_dev(Mesh *m) {
   f.pt_type = (const int8_t *)m->fpt_type_d.p;
   f.n_pt_rows = m->n_pt_rows;
   return f;
+}
+
+tlm::OuterHsDev outer_hs_dev(Mesh *m) {
+  tlm::OuterHsDev o{};
+  o.face = (const int4 *)m->ohs_face.p;
+  o.offset = (const double *)m->ohs_offset.p;
+  o.n = m->hs_outer ? m->hs_n : 0;
+  for (int i = 0; i < 3; i++) {
+    o.Ei[i] = m->hs_Ei[i];
+    o.Hi[i] = m->hs_Hi[i];
+  }
+  o.offset_min = m->hs_offset_min;
+  o.c = m->hs_c;
+  o.dt = m->desc.dt;
+  o.dl = m->desc.dl;
+  o.value_face = (const double *)m->value_face.p;
+  o.n_timesteps = m->desc.n_timesteps;
+  return o;
 }
 
 tlm::FaceProbeDev face_probe_dev(Mesh *m) {
@@ -477,7 +498,7 @@ int finalize(Mesh *m) {
     }
     std::vector<int> covered(m->n_exc_faces + 1, 0);
     std::vector<int2> src(std::max(nf, 1), int2{0, -1});
-    for (int h = 0; h < m->hs_n; h++) {
+    for (int h = 0; h < (m->hs_outer ? 0 : m->hs_n); h++) {
       const int e = m->hs_face_exc[h];
       if (e < 1 || e > m->n_exc_faces || exc_to_face[e] < 0) return fail(TLM_E_BADARG, "Huygens patch %d: bad face excitation number", h + 1);
       if (covered[e]++) return fail(TLM_E_UNSUPPORTED, "two Huygens patches on one face");
@@ -540,6 +561,22 @@ int finalize(Mesh *m) {
       for (int t = 0; t < nsteps && t < m->n_fn_steps; t++) vf[t] = m->fn_value_face[(size_t)(m->hs_fn - 1) * m->n_fn_steps + t];
     }
     if ((rc = upload(m, m->value_face, vf))) return rc;
+    // outer-boundary Huygens patches
+    if (m->hs_outer) {
+      std::vector<int4> of(std::max(m->hs_n, 1));
+      for (int h = 0; h < m->hs_n; h++) {
+        const int x = m->hs_cell[4 * h] - 1, y = m->hs_cell[4 * h + 1] - 1, z = m->hs_cell[4 * h + 2] - 1;
+        const int code = m->hs_cell[4 * h + 3];
+        const bool ok = x >= 0 && x < nx && y >= 0 && y < ny && z >= 0 && z < nz && code >= 1 && code <= 6 &&
+                        ((code == 1 && x == 0) || (code == 4 && x == nx - 1) || (code == 2 && y == 0) ||
+                         (code == 5 && y == ny - 1) || (code == 3 && z == 0) || (code == 6 && z == nz - 1));
+        if (!ok) return fail(TLM_E_BADARG, "outer Huygens patch %d is not a boundary face of the mesh", h + 1);
+        of[h] = int4{x, y, z, code};
+      }
+      std::vector<double> oo(m->hs_offset.begin(), m->hs_offset.end());
+      if (oo.empty()) oo.resize(1);
+      if ((rc = upload(m, m->ohs_face, of)) || (rc = upload(m, m->ohs_offset, oo))) return rc;
+    }
     if ((rc = dalloc(m, m->face_field, (size_t)std::max(m->n_out_faces, 1) * 12 * sizeof(double)))) return rc;
     CK(cudaMemset(m->face_field.p, 0, m->face_field.bytes));
   }
@@ -755,6 +792,10 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
     if (!m->fpr_face.empty()) {
       const tlm::FaceProbeDev pd = face_probe_dev(m);
       tlm::tlm_face_probe_kernel<<<(pd.n + 127) / 128, 128, 0, m->stream>>>(pd, fd.face_field, md.d_base, k);
+      m->last_launches++;
+    }
+    if (m->hs_outer && m->hs_n) {
+      tlm::tlm_outer_huygens_kernel<T><<<(m->hs_n + 127) / 128, 128, 0, m->stream>>>(md, outer_hs_dev(m), k);
       m->last_launches++;
     }
     if (dd.n_entries) {
@@ -1012,6 +1053,29 @@ int tlm_gpu_set_huygens(int64_t h, int32_t n, const int32_t *face_exc, const int
   m->hs_c = c;
   m->hs_fn = function;
   if (n && !(c > 0)) return fail(TLM_E_BADARG, "Huygens wave speed must be positive");
+  return TLM_OK;
+}
+
+int tlm_gpu_set_outer_huygens(int64_t h, int32_t n, const int32_t *cell_face, const double *offset, const double *Ei,
+                              const double *Hi, double offset_min, double c, int32_t function) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && (!cell_face || !offset || !Ei || !Hi))) return fail(TLM_E_BADARG, "bad outer Huygens arguments");
+  if (n && !(c > 0)) return fail(TLM_E_BADARG, "Huygens wave speed must be positive");
+  m->hs_outer = n > 0;
+  m->hs_n = n;
+  m->hs_cell.assign(cell_face, cell_face + 4 * (size_t)n);
+  m->hs_offset.assign(offset, offset + n);
+  m->hs_face_exc.assign(n, 0);
+  m->hs_norm.assign(3 * (size_t)n, 0);
+  for (int i = 0; i < 3; i++) {
+    m->hs_Ei[i] = Ei[i];
+    m->hs_Hi[i] = Hi[i];
+  }
+  m->hs_offset_min = offset_min;
+  m->hs_c = c;
+  m->hs_fn = function;
   return TLM_OK;
 }
 
@@ -1475,6 +1539,13 @@ int batch_step(Batch *b, bool dry) {
   }
   if (b->n_spb) { tlm::tlm_special_batch_kernel<T><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
   if (b->n_faceb) { tlm::tlm_face_batch_kernel<T><<<b->n_faceb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
+  for (int i : b->active) {  // outer-boundary Huygens surfaces of the members that have them
+    Mesh *m = get(b->handles[i]);
+    if (m && m->hs_outer && m->hs_n) {
+      tlm::tlm_outer_huygens_kernel<T><<<(m->hs_n + 127) / 128, 128, 0, b->stream>>>(mesh_dev<T>(m), outer_hs_dev(m), 0);
+      b->last_launches++;
+    }
+  }
   for (int i : b->active) {  // face output points of the members that have them
     Mesh *m = get(b->handles[i]);
     if (m && !m->fpr_face.empty()) {

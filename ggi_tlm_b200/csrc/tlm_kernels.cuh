@@ -1272,6 +1272,74 @@ __global__ void tlm_face_kernel(const MeshDev<T> m, const FaceDev fd, int rel_st
   face_body<T>(m, fd, f, rel_step);
 }
 
+// Outer-boundary Huygens surface (TLM_SOLVER/outer_boundary.F90:133-318):
+// one thread per boundary face adds the surface's J, M to the two ghost
+// slots that hold R times the boundary cell's reflected pulses (written by
+// the cell kernels this step):
+//   V - J dl Z0/2 + sg M dl/2 + R (-J dl Z0/2 - sg M dl/2)
+// with the excitation value interpolated as for the connect faces
+// (excitation.F90:645-690).
+struct OuterHsDev {
+  const int4 *face;      // (x, y, z) 0-based boundary cell, face code 1..6
+  const double *offset;  // per face
+  int n;
+  double Ei[3], Hi[3];
+  double offset_min, c, dt, dl;
+  const double *value_face;  // [n_timesteps]
+  int n_timesteps;
+};
+
+template <typename T>
+__global__ void tlm_outer_huygens_kernel(const MeshDev<T> m, const OuterHsDev od, int rel_step) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= od.n) return;
+  const int t = *m.d_base + rel_step;
+  T *R = (t & 1) ? m.links1 : m.links0;
+  const long long P = m.plane;
+  const int4 fc = od.face[f];
+  const int code = fc.w;
+  const long long idx = (long long)(fc.z + 1) * m.PxPy + (long long)(fc.y + 1) * m.Px + fc.x;
+  const double dt = od.dt;
+  const double t_offset = (od.offset[f] - od.offset_min) / od.c;
+  const double local_time = (double(t - 1)) * dt - t_offset;
+  const int ts1 = (int)round(local_time / dt);
+  const int ts2 = ts1 + 1;
+  const double delta_t = local_time - double(ts1) * dt;
+  const double v1 = (ts1 >= 1 && ts1 <= od.n_timesteps) ? od.value_face[ts1 - 1] : 0.0;
+  const double v2 = (ts2 >= 1 && ts2 <= od.n_timesteps) ? od.value_face[ts2 - 1] : 0.0;
+  const double value = v1 + delta_t * (v2 - v1) / dt;
+  const int axis = (code - 1) % 3;
+  const double nrm = code <= 3 ? -1.0 : 1.0;
+  const double nx_ = axis == 0 ? nrm : 0.0, ny_ = axis == 1 ? nrm : 0.0, nz_ = axis == 2 ? nrm : 0.0;
+  const double *Hi = od.Hi, *Ei = od.Ei;
+  double Js[3], Ms[3];
+  Js[0] = (ny_ * value * (Hi[2]) - nz_ * value * (Hi[1]));
+  Js[1] = (nz_ * value * (Hi[0]) - nx_ * value * (Hi[2]));
+  Js[2] = (nx_ * value * (Hi[1]) - ny_ * value * (Hi[0]));
+  Ms[0] = -(ny_ * value * (Ei[2]) - nz_ * value * (Ei[1]));
+  Ms[1] = -(nz_ * value * (Ei[0]) - nx_ * value * (Ei[2]));
+  Ms[2] = -(nx_ * value * (Ei[1]) - ny_ * value * (Ei[0]));
+  // ghost slot of each tangential port, its J and M components, and the
+  // sign of M on the first port (the second port takes the opposite sign)
+  long long g0, g1;
+  int j0, m0, j1, m1;
+  double s0;
+  const long long dy = m.Px, dz = m.PxPy;
+  switch (code) {
+    case 1: g0 = Vy_xmax * P + idx - 1; g1 = Vz_xmax * P + idx - 1; j0 = 1; m0 = 2; j1 = 2; m1 = 1; s0 = -1.0; break;
+    case 2: g0 = Vx_ymax * P + idx - dy; g1 = Vz_ymax * P + idx - dy; j0 = 0; m0 = 2; j1 = 2; m1 = 0; s0 = 1.0; break;
+    case 3: g0 = Vx_zmax * P + idx - dz; g1 = Vy_zmax * P + idx - dz; j0 = 0; m0 = 1; j1 = 1; m1 = 0; s0 = -1.0; break;
+    case 4: g0 = Vy_xmin * P + idx + 1; g1 = Vz_xmin * P + idx + 1; j0 = 1; m0 = 2; j1 = 2; m1 = 1; s0 = 1.0; break;
+    case 5: g0 = Vx_ymin * P + idx + dy; g1 = Vz_ymin * P + idx + dy; j0 = 0; m0 = 2; j1 = 2; m1 = 0; s0 = -1.0; break;
+    default: g0 = Vx_zmin * P + idx + dz; g1 = Vy_zmin * P + idx + dz; j0 = 0; m0 = 1; j1 = 1; m1 = 0; s0 = 1.0; break;
+  }
+  const double Rf = double(m.R[code <= 3 ? 2 * (code - 1) : 2 * (code - 4) + 1]);
+  const double dl = od.dl, Z0 = kZ0;
+  const double v0 = double(R[g0]), w0 = double(R[g1]);
+  R[g0] = T(v0 - Js[j0] * dl * Z0 / 2.0 + s0 * Ms[m0] * dl / 2.0 + Rf * (-Js[j0] * dl * Z0 / 2.0 - s0 * Ms[m0] * dl / 2.0));
+  R[g1] = T(w0 - Js[j1] * dl * Z0 / 2.0 - s0 * Ms[m1] * dl / 2.0 + Rf * (-Js[j1] * dl * Z0 / 2.0 + s0 * Ms[m1] * dl / 2.0));
+}
+
 // face_output_points (output_points.F90:255-444): one thread per face output
 // point copies its side and component of face_output_field, after connect.
 struct FaceProbeDev {

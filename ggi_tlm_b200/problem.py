@@ -420,6 +420,21 @@ class HuygensBox:
 
 
 @dataclass
+class HuygensOuter:
+    """The Huygens surface on the outer boundary of the mesh (surface number
+    0 in the Huygens_surface packet, huygens_surface%outer_surface_flag):
+    every boundary face is a patch with the outward normal of the mesh
+    (huygens_surface.F90:517-612), and its J, M enter the boundary ports in
+    outer_boundary (TLM_SOLVER/outer_boundary.F90:133-318)."""
+
+    function: int
+    ktheta: float
+    kphi: float
+    etheta: float
+    ephi: float
+
+
+@dataclass
 class OutputPoint:
     cell: Tuple[int, int, int]
     component: str
@@ -455,7 +470,7 @@ class ProblemSpec:
     material_regions: List[Tuple[int, object]] = field(default_factory=list)  # (material number, Block|Sphere)
     functions: List[ExcitationFunction] = field(default_factory=list)
     point_excitations: List[PointExcitation] = field(default_factory=list)
-    huygens: Optional[object] = None  # HuygensPlane or HuygensBox
+    huygens: Optional[object] = None  # HuygensPlane, HuygensBox or HuygensOuter
     outputs: List[OutputPoint] = field(default_factory=list)
     dft_surfaces: List[DFTSurface] = field(default_factory=list)
     reduced_c: float = 1.0
@@ -574,6 +589,8 @@ def _huygens_patches(hs) -> List[Tuple[Tuple[int, int, int], int]]:
     (huygens_surface.F90:412-450), in the surface mesher's face_list order
     (face code, then cz, cy, cx; MESH/build_surface_mesh.F90:100-150)."""
     rec = []
+    if isinstance(hs, HuygensOuter):
+        raise TypeError("the outer-boundary surface has no connect faces")
     if isinstance(hs, HuygensPlane):
         # recorded as the min face of the cell on the + side (normal -axis)
         for c in _plane_faces(hs.axis, hs.index, hs.r0, hs.r1):
@@ -778,8 +795,9 @@ def build_tables(spec: ProblemSpec) -> dict:
     for _, key, _ in face_probes:
         face_out[key] = True
     hs = spec.huygens
-    hs_patches = _huygens_patches(hs) if hs is not None else []
-    if hs is not None and not hs_patches:
+    outer = isinstance(hs, HuygensOuter)
+    hs_patches = _huygens_patches(hs) if hs is not None and not outer else []
+    if hs is not None and not outer and not hs_patches:
         raise ValueError("empty Huygens patch: r0 and r1 are (min, max) cell ranges")
 
     def connect_key(c, code):  # a cell face -> (cell whose min face it is, axis)
@@ -836,7 +854,43 @@ def build_tables(spec: ProblemSpec) -> dict:
                   face_out=np.array(face_o, dtype=np.int32), n_exc_faces=ne, n_out_faces=no)
 
     # Huygens surface data, huygens_surface.F90:247-715
-    if hs is not None:
+    if outer:
+        K, Ei, Hi = huygens_vectors(hs.ktheta, hs.kphi, hs.etheta, hs.ephi)
+        cells = []  # huygens_surface.F90:517-612 order
+        for cz in range(1, nz + 1):
+            for cy in range(1, ny + 1):
+                cells += [(1, cy, cz, FACE_XMIN), (nx, cy, cz, FACE_XMAX)]
+        for cz in range(1, nz + 1):
+            for cx in range(1, nx + 1):
+                cells += [(cx, 1, cz, FACE_YMIN), (cx, ny, cz, FACE_YMAX)]
+        cells += [(cx, cy, 1, FACE_ZMIN) for cy in range(1, ny + 1) for cx in range(1, nx + 1)]
+        cells += [(cx, cy, nz, FACE_ZMAX) for cy in range(1, ny + 1) for cx in range(1, nx + 1)]
+        xmin0, ymin0, zmin0 = spec.origin
+        norms, offsets = [], []
+        for (cx, cy, cz, code) in cells:
+            axis = (code - 1) % 3
+            n = [0, 0, 0]
+            n[axis] = -1 if code <= 3 else 1
+            off = [-0.5, -0.5, -0.5]
+            off[axis] = -1.0 if code <= 3 else 0.0
+            x = xmin0 + (cx + off[0]) * dl
+            y = ymin0 + (cy + off[1]) * dl
+            z = zmin0 + (cz + off[2]) * dl
+            norms.extend(n)
+            offsets.append(K[0] * x + K[1] * y + K[2] * z)
+        # the extents are the mesh's own (huygens_surface.F90:508-515)
+        bx, by, bz = (xmin0, xmin0 + nx * dl), (ymin0, ymin0 + ny * dl), (zmin0, zmin0 + nz * dl)
+        offset_min = 1e30
+        for (xx_, yy_, zz_) in ((bx[0], by[0], bz[0]), (bx[1], by[0], bz[0]), (bx[0], by[1], bz[0]),
+                                (bx[1], by[1], bz[0]), (bx[0], by[0], bz[1]), (bx[1], by[0], bz[1]),
+                                (bx[0], by[1], bz[1]), (bx[1], by[1], bz[1])):
+            offset_min = min(K[0] * xx_ + K[1] * yy_ + K[2] * zz_, offset_min)
+        tables.update(hs_n=len(cells), hs_face_exc=np.zeros(len(cells), np.int32),
+                      hs_norm=np.array(norms, dtype=np.int32), hs_offset=np.array(offsets),
+                      hs_Ei=np.array(Ei), hs_Hi=np.array(Hi), hs_offset_min=offset_min - dl / 2.0,
+                      hs_c=C0 / spec.reduced_c, hs_fn=hs.function, hs_outer=1,
+                      hs_cell=np.array(cells, dtype=np.int32).reshape(-1))
+    elif hs is not None:
         K, Ei, Hi = huygens_vectors(hs.ktheta, hs.kphi, hs.etheta, hs.ephi)
         norms, offsets, fexc = [], [], []
         xmin0, ymin0, zmin0 = spec.origin

@@ -133,6 +133,17 @@ int tlm_gpu_set_huygens(int64_t handle, int32_t n_patches, const int32_t *face_e
                         const double *offset, const double *Ei, const double *Hi, double offset_min, double c,
                         int32_t function);
 
+/* The Huygens surface on the outer boundary of the mesh (surface number 0
+   of the Huygens_surface packet; SRC/EXCITATION/huygens_surface.F90:508-612):
+   n boundary faces, 4 ints each (cx, cy, cz 1-based, face code 1..6 with
+   the outward normal of the mesh), their offsets K.r, the field vectors,
+   offset_min, c0/reduced_c and the excitation function.  Their J, M are
+   added to the boundary ports after the R reflection
+   (SRC/TLM_SOLVER/outer_boundary.F90:133-318).  Use it in place of
+   tlm_gpu_set_huygens: the reference has one Huygens surface. */
+int tlm_gpu_set_outer_huygens(int64_t handle, int32_t n_faces, const int32_t *cell_face, const double *offset,
+                              const double *Ei, const double *Hi, double offset_min, double c, int32_t function);
+
 /* Point sources on cell faces (SRC/EXCITATION/excitation_points.F90:
    135-211 numbering, :286-323 per step): 1-based excitation face number of
    the face (the min face of the cell on its + side, as in set_faces),

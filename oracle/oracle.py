@@ -48,6 +48,7 @@ class _Problem(C.Structure):
         ("n_face_points", C.c_int32), ("fpt_face", _i32p), ("fpt_comp", _i32p), ("fpt_fn", _i32p),
         ("fpt_type", _i32p),
         ("n_face_probes", C.c_int32), ("fprobe_face", _i32p), ("fprobe_side", _i32p), ("fprobe_comp", _i32p),
+        ("hs_outer", C.c_int32), ("hs_cell", _i32p),
     ]
 
 
@@ -119,7 +120,9 @@ class Oracle:
         p.hs_c = float(t["hs_c"])
         p.n_face_points = int(t.get("n_face_points", 0))
         p.n_face_probes = int(t.get("n_face_probes", 0))
-        for k in ("fpt_face", "fpt_comp", "fpt_fn", "fpt_type", "fprobe_face", "fprobe_side", "fprobe_comp"):
+        p.hs_outer = int(t.get("hs_outer", 0))
+        for k in ("fpt_face", "fpt_comp", "fpt_fn", "fpt_type", "fprobe_face", "fprobe_side", "fprobe_comp",
+                  "hs_cell"):
             setattr(p, k, arr(k, np.int32) if k in t else arr_empty())
         if int(t.get("n_pml_material_cells", 0)):
             p.pml_sigma = arr("pml_sigma", np.float64)

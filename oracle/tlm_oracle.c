@@ -221,7 +221,7 @@ static void excitation(tlm_oracle_state *s, int timestep) {
       if (comp < 6) s->face_exc_type[(size_t)face * 12 + side * 6 + comp] = p->fpt_type[e];
     }
   }
-  for (int h = 0; h < p->hs_n; h++) {
+  for (int h = 0; h < (p->hs_outer ? 0 : p->hs_n); h++) {
     double value = interp_face_value(s, p->hs_offset[h], timestep);
     double nxx = p->hs_norm[3 * h], nyy = p->hs_norm[3 * h + 1], nzz = p->hs_norm[3 * h + 2];
     const double *Hi = p->hs_Hi, *Ei = p->hs_Ei;
@@ -850,8 +850,9 @@ static void connect(tlm_oracle_state *s) {
 }
 
 /* outer_boundary(), TLM_SOLVER/outer_boundary.F90:71-131 */
-static void outer_boundary(tlm_oracle_state *s) {
+static void outer_boundary(tlm_oracle_state *s, int timestep) {
   const double *R = s->p.R;
+  const tlm_oracle_problem *p = &s->p;
   int nx = s->nx, ny = s->ny, nz = s->nz;
   for (int cz = 1; cz <= nz; cz++)
     for (int cy = 1; cy <= ny; cy++) {
@@ -877,6 +878,42 @@ static void outer_boundary(tlm_oracle_state *s) {
       V_(Vx_zmax, cx, cy, nz) = V_(Vx_zmax, cx, cy, nz) * R[5];
       V_(Vy_zmax, cx, cy, nz) = V_(Vy_zmax, cx, cy, nz) * R[5];
     }
+  if (!p->hs_outer) return;
+  /* outer-boundary Huygens surface (outer_boundary.F90:133-318): per
+     boundary face, the two tangential ports get
+     V - J dl Z0/2 + sg M dl/2 + R (-J dl Z0/2 - sg M dl/2)
+     with (port, J component, M component, sg) per face code below */
+  static const int tab[7][2][4] = {
+      {{0}},
+      {{Vy_xmin, 1, 2, -1}, {Vz_xmin, 2, 1, +1}}, /* face_xmin */
+      {{Vx_ymin, 0, 2, +1}, {Vz_ymin, 2, 0, -1}}, /* face_ymin */
+      {{Vx_zmin, 0, 1, -1}, {Vy_zmin, 1, 0, +1}}, /* face_zmin */
+      {{Vy_xmax, 1, 2, +1}, {Vz_xmax, 2, 1, -1}}, /* face_xmax */
+      {{Vx_ymax, 0, 2, -1}, {Vz_ymax, 2, 0, +1}}, /* face_ymax */
+      {{Vx_zmax, 0, 1, +1}, {Vy_zmax, 1, 0, -1}}, /* face_zmax */
+  };
+  const double dl = p->dl;
+  for (int h = 0; h < p->hs_n; h++) {
+    const int32_t *c = p->hs_cell + 4 * h;
+    double value = interp_face_value(s, p->hs_offset[h], timestep);
+    double normx = p->hs_norm[3 * h], normy = p->hs_norm[3 * h + 1], normz = p->hs_norm[3 * h + 2];
+    const double *Hi = p->hs_Hi, *Ei = p->hs_Ei;
+    double Js[3], Ms[3];
+    Js[0] = (normy * value * (Hi[2]) - normz * value * (Hi[1]));
+    Js[1] = (normz * value * (Hi[0]) - normx * value * (Hi[2]));
+    Js[2] = (normx * value * (Hi[1]) - normy * value * (Hi[0]));
+    Ms[0] = -(normy * value * (Ei[2]) - normz * value * (Ei[1]));
+    Ms[1] = -(normz * value * (Ei[0]) - normx * value * (Ei[2]));
+    Ms[2] = -(normx * value * (Ei[1]) - normy * value * (Ei[0]));
+    const int code = c[3];
+    const double Rf = R[code <= 3 ? 2 * (code - 1) : 2 * (code - 4) + 1];
+    for (int q = 0; q < 2; q++) {
+      const int port = tab[code][q][0];
+      const double J = Js[tab[code][q][1]], M = Ms[tab[code][q][2]], sg = tab[code][q][3];
+      double *v = &V_(port, c[0], c[1], c[2]);
+      *v = *v - J * dl * Z0 / 2.0 + sg * M * dl / 2.0 + Rf * (-J * dl * Z0 / 2.0 - sg * M * dl / 2.0);
+    }
+  }
 }
 
 /* face_output_frequency_output_surfaces, frequency_output_surfaces.F90:297-421 */
@@ -938,7 +975,7 @@ int tlm_oracle_run(tlm_oracle_state *s, int32_t first_step, int32_t n_steps, dou
       s->face_probe_rec[(size_t)(timestep - 1) * p->n_face_probes + q] =
           s->face_out[(size_t)(p->fprobe_face[q] - 1) * 12 + (p->fprobe_side[q] - 1) * 6 + (p->fprobe_comp[q] - 1)];
     dft_surfaces(s, time);
-    outer_boundary(s);
+    outer_boundary(s, timestep);
     s->timestep = timestep;
   }
   return 0;

@@ -116,6 +116,13 @@ typedef struct {
      output face number, side 1 (min) / 2 (max), component 1..6 */
   int32_t n_face_probes;
   const int32_t *fprobe_face, *fprobe_side, *fprobe_comp;
+
+  /* the Huygens surface is the outer boundary (huygens_surface%outer_surface_flag):
+     its hs_n patches are boundary faces, 4 ints each in hs_cell (cx,cy,cz
+     1-based, face code 1..6), and their sources enter in outer_boundary
+     (TLM_SOLVER/outer_boundary.F90:133-318) instead of connect */
+  int32_t hs_outer;
+  const int32_t *hs_cell;
 } tlm_oracle_problem;
 
 typedef struct tlm_oracle_state tlm_oracle_state;
