@@ -39,6 +39,7 @@ EXPORTS = [
     "tlm_gpu_batch_run", "tlm_gpu_batch_synchronize", "tlm_gpu_batch_last_run", "tlm_gpu_batch_destroy",
     "tlm_gpu_set_small_to_zero", "tlm_gpu_set_pml_sigma", "tlm_gpu_set_face_excitation",
     "tlm_gpu_set_face_outputs", "tlm_gpu_fetch_face_output", "tlm_gpu_set_outer_huygens",
+    "tlm_gpu_set_far_field", "tlm_gpu_fetch_far_field",
 ]
 
 
@@ -79,6 +80,8 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_face_excitation": [i64, i32, _i32p, _i32p, _i32p, _i32p],
         "tlm_gpu_set_face_outputs": [i64, i32, _i32p, _i32p, _i32p],
         "tlm_gpu_set_outer_huygens": [i64, i32, _i32p, _f64p, _f64p, _f64p, C.c_double, C.c_double, i32],
+        "tlm_gpu_set_far_field": [i64, i32, _f64p, _i32p, _i32p, _i32p],
+        "tlm_gpu_fetch_far_field": [i64, _f64p],
         "tlm_gpu_fetch_face_output": [i64, i32, i32, _f64p],
         "tlm_gpu_set_excitation": [i64, i32, i32, _f64p, _f64p, i32, _i32p, _i32p, _i32p, _i32p, i32],
         "tlm_gpu_set_faces": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, i32, i32],
@@ -206,6 +209,9 @@ class GpuMesh:
             df = [_f64(t["dft_freq"]), _i32(t["dft_comp"]), _i32(t["dft_face_ptr"]), _i32(t["dft_face_out"]),
                   _i32(t["dft_face_side"])]
             _check(lib.tlm_gpu_set_dft(self.h, int(t["n_dft"]), *[_p(x) for x in df]))
+        if int(t.get("n_ff", 0)):
+            ff = [_f64(t["ff_freq"]), _i32(t["ff_face_ptr"]), _i32(t["ff_face_out"]), _i32(t["ff_face_code"])]
+            _check(lib.tlm_gpu_set_far_field(self.h, int(t["n_ff"]), *[_p(x) for x in ff]))
         if int(t.get("n_face_points", 0)):
             fp = [_i32(t[k]) for k in ("fpt_face", "fpt_comp", "fpt_fn", "fpt_type")]
             _check(lib.tlm_gpu_set_face_excitation(self.h, int(t["n_face_points"]), *[_p(x) for x in fp]))
@@ -267,6 +273,14 @@ class GpuMesh:
         out = np.zeros((max(n, 1), max(nq, 1)))
         _check(_lib.tlm_gpu_fetch_face_output(self.h, first, n, out.ctypes.data_as(_f64p)))
         return out[:n, :nq].T.copy()
+
+    def far_field(self) -> np.ndarray:
+        """Far-field accumulators [entries, 6] complex: Jx, Jy, Jz, Mx, My, Mz."""
+        n = int(self.t["ff_face_ptr"][-1]) if int(self.t.get("n_ff", 0)) else 0
+        out = np.zeros(max(12 * n, 12))
+        _check(_lib.tlm_gpu_fetch_far_field(self.h, out.ctypes.data_as(_f64p)))
+        v = out[: 12 * n].reshape(n, 6, 2)
+        return v[..., 0] + 1j * v[..., 1]
 
     def dft(self) -> np.ndarray:
         n = int(self.t["dft_face_ptr"][-1]) if int(self.t["n_dft"]) else 0

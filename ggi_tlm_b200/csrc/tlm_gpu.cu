@@ -103,11 +103,14 @@ struct Mesh {
   DevBuf links, seg_mask, seg_base, sp_rec, sp_pos, pml_state, pml_par, pml_ixt, filt, mats_d, exc_field, exc_type,
       cell_out, faces, face_io, face_hs, value_face, face_field, dft_entry, dft_phasor, dft_acc, d_base,
       pmm_pos, pmm_parmat, pmm_state, pmm_sigma, face_src, fpt_field_d, fpt_type_d, fprobe, fprobe_rec,
-      ohs_face, ohs_offset;
+      ohs_face, ohs_offset, ff_entry, ff_phasor, ff_acc;
   int n_pt_rows = 0;
   int n_pmm = 0;  // PML cells inside a volume material
   int n_filt = 0, filt_eo = 0, filt_mo = 0;
   int dft_entries = 0;
+  std::vector<double> ff_freq;                       // far-field surfaces, one per frequency
+  std::vector<int32_t> ff_ptr, ff_fout, ff_fcode;
+  int ff_entries = 0;
   int n_sp_dev = 0;  // non-PML special cells on the device list
   int n_pml_list = 0, n_pml_out = 0;
   DevBuf pml_pos, pml_par16, pml_outmap;
@@ -255,6 +258,17 @@ tlm::OuterHsDev outer_hs_dev(Mesh *m) {
   o.value_face = (const double *)m->value_face.p;
   o.n_timesteps = m->desc.n_timesteps;
   return o;
+}
+
+tlm::FarFieldDev far_field_dev(Mesh *m) {
+  tlm::FarFieldDev d{};
+  d.n_entries = m->ff_entries;
+  d.n_ff = (int)m->ff_freq.size();
+  d.entry = (const int4 *)m->ff_entry.p;
+  d.phasor = (const double2 *)m->ff_phasor.p;
+  d.face_field = (const double *)m->face_field.p;
+  d.acc = (double2 *)m->ff_acc.p;
+  return d;
 }
 
 tlm::FaceProbeDev face_probe_dev(Mesh *m) {
@@ -608,6 +622,34 @@ int finalize(Mesh *m) {
     if ((rc = dalloc(m, m->dft_acc, ent.size() * sizeof(double2)))) return rc;
     CK(cudaMemset(m->dft_acc.p, 0, m->dft_acc.bytes));
   }
+  // ---- far-field surfaces
+  {
+    const int nff = (int)m->ff_freq.size();
+    std::vector<int4> ent;
+    for (int d = 0; d < nff; d++) {
+      for (int k = m->ff_ptr[d]; k < m->ff_ptr[d + 1]; k++) {
+        const int fo = m->ff_fout[k], code = m->ff_fcode[k];
+        if (fo < 1 || fo > m->n_out_faces) return fail(TLM_E_BADARG, "far-field face output number out of range");
+        if (code < 1 || code > 6) return fail(TLM_E_BADARG, "far-field face code out of range");
+        ent.push_back(int4{d, fo - 1, code, 0});
+      }
+    }
+    m->ff_entries = (int)ent.size();
+    if (ent.empty()) ent.resize(1);
+    std::vector<double2> ph((size_t)std::max(nff, 1) * nsteps, double2{0, 0});
+    const double pi = 3.141592653589793;
+    for (int t = 0; t < nsteps; t++) {
+      double time = (double)t * D.dt;  // (timestep-1)*dt
+      time = time + D.dt / 2.0;
+      for (int d = 0; d < nff; d++) {
+        const double arg = -2.0 * pi * m->ff_freq[d] * time;
+        ph[(size_t)t * nff + d] = double2{cos(arg) * D.dt, sin(arg) * D.dt};
+      }
+    }
+    if ((rc = upload(m, m->ff_entry, ent)) || (rc = upload(m, m->ff_phasor, ph))) return rc;
+    if ((rc = dalloc(m, m->ff_acc, ent.size() * 6 * sizeof(double2)))) return rc;
+    CK(cudaMemset(m->ff_acc.p, 0, m->ff_acc.bytes));
+  }
   if ((rc = dalloc(m, m->d_base, sizeof(int)))) return rc;
   if ((rc = dalloc(m, m->d_err, sizeof(int)))) return rc;
   CK(cudaMemset(m->d_err.p, 0, sizeof(int)));
@@ -796,6 +838,11 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
     }
     if (m->hs_outer && m->hs_n) {
       tlm::tlm_outer_huygens_kernel<T><<<(m->hs_n + 127) / 128, 128, 0, m->stream>>>(md, outer_hs_dev(m), k);
+      m->last_launches++;
+    }
+    if (m->ff_entries) {
+      const tlm::FarFieldDev fdv = far_field_dev(m);
+      tlm::tlm_far_field_kernel<<<(fdv.n_entries + 255) / 256, 256, 0, m->stream>>>(fdv, md.d_base, k);
       m->last_launches++;
     }
     if (dd.n_entries) {
@@ -1250,6 +1297,33 @@ int tlm_gpu_fetch_face_output(int64_t h, int32_t first, int32_t n, double *out) 
   return TLM_OK;
 }
 
+int tlm_gpu_set_far_field(int64_t h, int32_t n, const double *freq, const int32_t *ptr, const int32_t *fout,
+                          const int32_t *fcode) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && (!freq || !ptr || !fout || !fcode))) return fail(TLM_E_BADARG, "bad far-field arguments");
+  m->ff_freq.assign(freq, freq + n);
+  m->ff_ptr.assign(ptr, ptr + (n ? n + 1 : 0));
+  const int ne = n ? ptr[n] : 0;
+  for (int d = 0; d < n; d++)
+    if (ptr[d] < 0 || ptr[d + 1] < ptr[d]) return fail(TLM_E_BADARG, "far-field face pointers must be non-decreasing");
+  m->ff_fout.assign(fout, fout + ne);
+  m->ff_fcode.assign(fcode, fcode + ne);
+  return TLM_OK;
+}
+
+int tlm_gpu_fetch_far_field(int64_t h, double *out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
+  if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
+  if (!m->ff_entries) return TLM_OK;
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(out, m->ff_acc.p, (size_t)m->ff_entries * 12 * sizeof(double), cudaMemcpyDeviceToHost));
+  return TLM_OK;
+}
+
 int tlm_gpu_fetch_dft(int64_t h, double *out) {
   Mesh *m = get(h);
   if (!m) return fail(TLM_E_BADARG, "bad handle");
@@ -1543,6 +1617,14 @@ int batch_step(Batch *b, bool dry) {
     Mesh *m = get(b->handles[i]);
     if (m && m->hs_outer && m->hs_n) {
       tlm::tlm_outer_huygens_kernel<T><<<(m->hs_n + 127) / 128, 128, 0, b->stream>>>(mesh_dev<T>(m), outer_hs_dev(m), 0);
+      b->last_launches++;
+    }
+  }
+  for (int i : b->active) {  // far-field surfaces of the members that have them
+    Mesh *m = get(b->handles[i]);
+    if (m && m->ff_entries) {
+      const tlm::FarFieldDev fdv = far_field_dev(m);
+      tlm::tlm_far_field_kernel<<<(fdv.n_entries + 255) / 256, 256, 0, b->stream>>>(fdv, (const int *)m->d_base.p, 0);
       b->last_launches++;
     }
   }

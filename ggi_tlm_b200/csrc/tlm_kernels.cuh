@@ -1510,6 +1510,50 @@ __device__ __forceinline__ void dft_body(const DftDev &d, const int *d_base, int
   d.acc[k] = a;
 }
 
+// face_output_far_field (far_field_surfaces.F90:252-351): one thread per
+// (surface, face) entry accumulates J += e^{-jwt} dt (n x H) and
+// M -= e^{-jwt} dt (n x E) from the entry's side of face_output_field.
+struct FarFieldDev {
+  int n_entries, n_ff;
+  const int4 *entry;        // (surface, out face index, face code 1..6, 0)
+  const double2 *phasor;    // [n_timesteps][n_ff] exp(-j 2 pi f t) dt
+  const double *face_field; // [n_out_faces][2][6]
+  double2 *acc;             // [n_entries][6]: Jx, Jy, Jz, Mx, My, Mz
+};
+
+__global__ void tlm_far_field_kernel(const FarFieldDev d, const int *d_base, int rel_step) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.n_entries) return;
+  const int t = *d_base + rel_step;
+  const int4 en = d.entry[k];
+  const int face = en.z;
+  const int side = face <= 3 ? 0 : 1;
+  double normx = 0, normy = 0, normz = 0;
+  if (face == 1) normx = 1; else if (face == 4) normx = -1;
+  else if (face == 2) normy = 1; else if (face == 5) normy = -1;
+  else if (face == 3) normz = 1; else normz = -1;
+  const double *fl = d.face_field + (size_t)en.y * 12 + side * 6;
+  double v[6];
+  v[0] = (normy * fl[5] - normz * fl[4]);
+  v[1] = (normz * fl[3] - normx * fl[5]);
+  v[2] = (normx * fl[4] - normy * fl[3]);
+  v[3] = (normy * fl[2] - normz * fl[1]);
+  v[4] = (normz * fl[0] - normx * fl[2]);
+  v[5] = (normx * fl[1] - normy * fl[0]);
+  const double2 ph = d.phasor[(size_t)(t - 1) * d.n_ff + en.x];
+  double2 *a = d.acc + (size_t)k * 6;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    double2 j = a[c], m = a[3 + c];
+    j.x = j.x + ph.x * v[c];
+    j.y = j.y + ph.y * v[c];
+    m.x = m.x - ph.x * v[3 + c];
+    m.y = m.y - ph.y * v[3 + c];
+    a[c] = j;
+    a[3 + c] = m;
+  }
+}
+
 __global__ void tlm_advance_base(int *d_base, int n) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *d_base += n;
 }

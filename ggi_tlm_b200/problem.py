@@ -435,6 +435,33 @@ class HuygensOuter:
 
 
 @dataclass
+class FarFieldSurface:
+    """A far-field surface (Far_field_surface packet, OUTPUT/far_field_surfaces.F90):
+    per frequency the accumulators J += e^{-jwt} dt (n x H) and
+    M -= e^{-jwt} dt (n x E) of every face of a closed box of cells
+    ``box`` = ((i0, i1), (j0, j1), (k0, k1)) or of a planar patch ``plane`` =
+    (axis, index, r0, r1).  The faces are those the surface mesher records
+    (as for HuygensBox / HuygensPlane), flipped to the other side of each
+    face when ``side`` is -1; n is +1 on a min face and -1 on a max face,
+    i.e. it points into the cell whose face is sampled."""
+
+    frequencies: List[float]
+    box: Optional[Tuple[Tuple[int, int], Tuple[int, int], Tuple[int, int]]] = None
+    plane: Optional[Tuple[int, int, Tuple[int, int], Tuple[int, int]]] = None
+    side: int = 1
+
+    def faces(self) -> List[Tuple[Tuple[int, int, int], int]]:
+        if (self.box is None) == (self.plane is None):
+            raise ValueError("a far-field surface is either a box or a plane")
+        if self.box is not None:
+            g = HuygensBox(self.box[0], self.box[1], self.box[2], 0, 0.0, 0.0, 1.0, 0.0, side=self.side)
+        else:
+            ax, ix, r0, r1 = self.plane
+            g = HuygensPlane(ax, ix, r0, r1, 0, 0.0, 0.0, 1.0, 0.0, side=self.side)
+        return _huygens_patches(g)
+
+
+@dataclass
 class OutputPoint:
     cell: Tuple[int, int, int]
     component: str
@@ -473,6 +500,7 @@ class ProblemSpec:
     huygens: Optional[object] = None  # HuygensPlane, HuygensBox or HuygensOuter
     outputs: List[OutputPoint] = field(default_factory=list)
     dft_surfaces: List[DFTSurface] = field(default_factory=list)
+    far_field_surfaces: List["FarFieldSurface"] = field(default_factory=list)
     reduced_c: float = 1.0
     # set_small_to_zero packet (read_small_to_zero.F90:55-59): (n_small_to_zero, small_to_zero_value)
     small_to_zero: Optional[Tuple[int, float]] = None
@@ -810,6 +838,10 @@ def build_tables(spec: ProblemSpec) -> dict:
 
     for c, code in hs_patches:
         face_exc[connect_key(c, code)] = True
+    ff_faces = [ff.faces() for ff in spec.far_field_surfaces]
+    for fl in ff_faces:
+        for c, code in fl:
+            face_out[connect_key(c, code)] = True
     for ds in spec.dft_surfaces:
         for f in _plane_faces(ds.axis, ds.index, ds.r0, ds.r1):
             face_out[(f, ds.axis)] = True
@@ -952,6 +984,18 @@ def build_tables(spec: ProblemSpec) -> dict:
     tables.update(n_dft=len(freqs), dft_freq=np.array(freqs, dtype=np.float64),
                   dft_comp=np.array(comps, dtype=np.int32), dft_face_ptr=np.array(ptr, dtype=np.int32),
                   dft_face_out=np.array(fo, dtype=np.int32), dft_face_side=np.array(fs, dtype=np.int32))
+    # far-field surfaces: one reference surface entry per frequency
+    ffreq, fptr, ffo, ffc = [], [0], [], []
+    for ff, fl in zip(spec.far_field_surfaces, ff_faces):
+        for fr in ff.frequencies:
+            ffreq.append(fr)
+            for c, code in fl:
+                ffo.append(fout_num[connect_key(c, code)])
+                ffc.append(code)
+            fptr.append(len(ffo))
+    tables.update(n_ff=len(ffreq), ff_freq=np.array(ffreq, dtype=np.float64),
+                  ff_face_ptr=np.array(fptr, dtype=np.int32), ff_face_out=np.array(ffo, dtype=np.int32),
+                  ff_face_code=np.array(ffc, dtype=np.int32))
     n_small, small = spec.small_to_zero if spec.small_to_zero else (0, 0.0)
     if n_small < 0 or small < 0.0:
         raise ValueError("set_small_to_zero needs n >= 0 and a value >= 0")

@@ -181,6 +181,20 @@ int tlm_gpu_set_dft(int64_t handle, int32_t n_surfaces, const double *frequency,
    run_TLM.F90:236-238).  n_small_to_zero = 0 switches it off (the default). */
 int tlm_gpu_set_small_to_zero(int64_t handle, int32_t n_small_to_zero, double small_to_zero_value);
 
+/* Far-field surfaces (SRC/OUTPUT/far_field_surfaces.F90:36-351), one entry
+   per frequency as far_field_surface(:): frequency and a CSR list
+   (face_ptr[n_surfaces+1]) of output face numbers and face codes 1..6 of
+   the surface's faces after the side flip.  Every step each face
+   accumulates J += exp(-j 2 pi f t) dt (n x H) and M -= exp(-j 2 pi f t) dt
+   (n x E) on its side of face_output_field, n = +1 on a min face, -1 on a
+   max face. */
+int tlm_gpu_set_far_field(int64_t handle, int32_t n_surfaces, const double *frequency, const int32_t *face_ptr,
+                          const int32_t *face_out, const int32_t *face_code);
+
+/* Far-field accumulators per surface face in set_far_field order: Jx, Jy,
+   Jz, Mx, My, Mz as (re, im) pairs, 12 doubles per face. */
+int tlm_gpu_fetch_far_field(int64_t handle, double *out);
+
 /* Advance timesteps first_step..first_step+n_steps-1 (1-based, run_TLM
    numbering, SRC/TLM_SOLVER/run_TLM.F90:191-295).  Steps must be
    contiguous across calls.  Asynchronous on the library stream. */

@@ -49,6 +49,8 @@ class _Problem(C.Structure):
         ("fpt_type", _i32p),
         ("n_face_probes", C.c_int32), ("fprobe_face", _i32p), ("fprobe_side", _i32p), ("fprobe_comp", _i32p),
         ("hs_outer", C.c_int32), ("hs_cell", _i32p),
+        ("n_ff", C.c_int32), ("ff_freq", _f64p), ("ff_face_ptr", _i32p), ("ff_face_out", _i32p),
+        ("ff_face_code", _i32p),
     ]
 
 
@@ -74,6 +76,7 @@ def _load():
         _lib.tlm_oracle_get_dft.argtypes = [C.c_void_p, _f64p]
         _lib.tlm_oracle_get_links.argtypes = [C.c_void_p, _f64p]
         _lib.tlm_oracle_get_face_probes.argtypes = [C.c_void_p, _f64p]
+        _lib.tlm_oracle_get_far_field.argtypes = [C.c_void_p, _f64p]
     return _lib
 
 
@@ -89,6 +92,11 @@ class Oracle:
             a = np.zeros(1, dtype=np.int32)
             keep.append(a)
             return a.ctypes.data_as(_i32p)
+
+        def arr_empty_f():
+            a = np.zeros(1)
+            keep.append(a)
+            return a.ctypes.data_as(_f64p)
 
         def arr(key, dtype):
             a = np.ascontiguousarray(t[key], dtype=dtype).reshape(-1)
@@ -121,6 +129,10 @@ class Oracle:
         p.n_face_points = int(t.get("n_face_points", 0))
         p.n_face_probes = int(t.get("n_face_probes", 0))
         p.hs_outer = int(t.get("hs_outer", 0))
+        p.n_ff = int(t.get("n_ff", 0))
+        p.ff_freq = arr("ff_freq", np.float64) if "ff_freq" in t else arr_empty_f()
+        for k in ("ff_face_ptr", "ff_face_out", "ff_face_code"):
+            setattr(p, k, arr(k, np.int32) if k in t else arr_empty())
         for k in ("fpt_face", "fpt_comp", "fpt_fn", "fpt_type", "fprobe_face", "fprobe_side", "fprobe_comp",
                   "hs_cell"):
             setattr(p, k, arr(k, np.int32) if k in t else arr_empty())
@@ -150,6 +162,14 @@ class Oracle:
         out = np.zeros(max(2 * n, 1))
         _load().tlm_oracle_get_dft(self._h, out.ctypes.data_as(_f64p))
         return out[: 2 * n].reshape(-1, 2)
+
+    def far_field(self) -> np.ndarray:
+        """Far-field accumulators [entries, 6] complex: Jx, Jy, Jz, Mx, My, Mz."""
+        n = int(self.t["ff_face_ptr"][-1]) if int(self.t.get("n_ff", 0)) else 0
+        out = np.zeros(max(12 * n, 1))
+        _load().tlm_oracle_get_far_field(self._h, out.ctypes.data_as(_f64p))
+        v = out[: 12 * n].reshape(n, 6, 2)
+        return v[..., 0] + 1j * v[..., 1]
 
     def face_probes(self) -> np.ndarray:
         """Face output point values [n_face_probes, steps run so far]."""

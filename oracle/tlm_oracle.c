@@ -64,6 +64,7 @@ struct tlm_oracle_state {
   pml_mat_t *pml_mat;  /* PML cells inside a volume material, traversal order */
   int32_t *pml_mat_pos; /* PML_material_array_pos per PML cell, 1-based or 0 */
   double *face_probe_rec; /* [n_timesteps][n_face_probes] */
+  double *ff_acc;         /* far field, per surface face: J(3), M(3) complex */
   double *cell_exc;    /* [n_exc_cells][9] */
   int32_t *cell_exc_type; /* [n_exc_cells][6] */
   double *cell_out;    /* [n_out_cells][6] */
@@ -144,6 +145,7 @@ tlm_oracle_state *tlm_oracle_create(const tlm_oracle_problem *p) {
   }
   s->pml = (pml_cell_t *)calloc((size_t)p->n_pml_cells + 1, sizeof(pml_cell_t));
   s->face_probe_rec = (double *)calloc((size_t)p->n_timesteps * p->n_face_probes + 1, sizeof(double));
+  s->ff_acc = (double *)calloc((size_t)(p->n_ff ? p->ff_face_ptr[p->n_ff] : 0) * 12 + 1, sizeof(double));
   /* allocate_PML_material_data, TLM_PML_volume_materials.F90:590-740: a
      PML cell whose special cell has a DISPERSIVE-type material gets the next
      PML material record, in special-cell (traversal) order; all zero */
@@ -177,7 +179,7 @@ tlm_oracle_state *tlm_oracle_create(const tlm_oracle_problem *p) {
 
 void tlm_oracle_destroy(tlm_oracle_state *s) {
   if (!s) return;
-  free(s->V); free(s->sp_filter); free(s->eps_f); free(s->mu_f); free(s->pml); free(s->pml_mat); free(s->pml_mat_pos); free(s->face_probe_rec);
+  free(s->V); free(s->sp_filter); free(s->eps_f); free(s->mu_f); free(s->pml); free(s->pml_mat); free(s->pml_mat_pos); free(s->face_probe_rec); free(s->ff_acc);
   free(s->cell_exc); free(s->cell_exc_type); free(s->cell_out); free(s->face_exc);
   free(s->face_exc_type); free(s->face_out); free(s->face_code); free(s->dft);
   free(s);
@@ -943,6 +945,41 @@ static void dft_surfaces(tlm_oracle_state *s, double time) {
   }
 }
 
+/* face_output_far_field, far_field_surfaces.F90:252-351: J += e^{-jwt} dt (n x H),
+   M -= e^{-jwt} dt (n x E) on the face side of each entry, n = +1 on a min
+   face and -1 on a max face */
+static void far_field_surfaces(tlm_oracle_state *s, double time) {
+  const tlm_oracle_problem *p = &s->p;
+  const double pi = 3.141592653589793;
+  for (int d = 0; d < p->n_ff; d++) {
+    double arg = -2.0 * pi * p->ff_freq[d] * time;
+    double er = cos(arg) * p->dt, ei = sin(arg) * p->dt; /* exp(-j*2*pi*f*t)*dt */
+    for (int k = p->ff_face_ptr[d]; k < p->ff_face_ptr[d + 1]; k++) {
+      int face = p->ff_face_code[k];
+      int side = (face <= 3) ? 0 : 1;
+      double normx = 0, normy = 0, normz = 0;
+      if (face == 1) normx = 1; else if (face == 4) normx = -1;
+      else if (face == 2) normy = 1; else if (face == 5) normy = -1;
+      else if (face == 3) normz = 1; else normz = -1;
+      const double *fld = s->face_out + (size_t)(p->ff_face_out[k] - 1) * 12 + side * 6;
+      double v[6];
+      v[0] = (normy * fld[Hz] - normz * fld[Hy]);
+      v[1] = (normz * fld[Hx] - normx * fld[Hz]);
+      v[2] = (normx * fld[Hy] - normy * fld[Hx]);
+      v[3] = (normy * fld[Ez] - normz * fld[Ey]);
+      v[4] = (normz * fld[Ex] - normx * fld[Ez]);
+      v[5] = (normx * fld[Ey] - normy * fld[Ex]);
+      double *a = s->ff_acc + (size_t)k * 12;
+      for (int c = 0; c < 3; c++) {
+        a[2 * c] = a[2 * c] + er * v[c];
+        a[2 * c + 1] = a[2 * c + 1] + ei * v[c];
+        a[6 + 2 * c] = a[6 + 2 * c] - er * v[3 + c];
+        a[6 + 2 * c + 1] = a[6 + 2 * c + 1] - ei * v[3 + c];
+      }
+    }
+  }
+}
+
 /* run_TLM.F90:191-295 for timesteps first..first+n-1 */
 /* TLM_set_small_to_zero (TLM_SOLVER/TLM_set_small_to_zero.F90:34-68): the 12
    incident pulses of every cell with |V| below the threshold become 0 */
@@ -975,6 +1012,7 @@ int tlm_oracle_run(tlm_oracle_state *s, int32_t first_step, int32_t n_steps, dou
       s->face_probe_rec[(size_t)(timestep - 1) * p->n_face_probes + q] =
           s->face_out[(size_t)(p->fprobe_face[q] - 1) * 12 + (p->fprobe_side[q] - 1) * 6 + (p->fprobe_comp[q] - 1)];
     dft_surfaces(s, time);
+    far_field_surfaces(s, time);
     outer_boundary(s, timestep);
     s->timestep = timestep;
   }
@@ -984,6 +1022,11 @@ int tlm_oracle_run(tlm_oracle_state *s, int32_t first_step, int32_t n_steps, dou
 int tlm_oracle_get_dft(tlm_oracle_state *s, double *out) {
   int n = s->p.n_dft ? s->p.dft_face_ptr[s->p.n_dft] : 0;
   memcpy(out, s->dft, sizeof(double) * 2 * (size_t)n);
+  return 0;
+}
+
+int tlm_oracle_get_far_field(tlm_oracle_state *s, double *out) {
+  memcpy(out, s->ff_acc, sizeof(double) * 12 * (size_t)(s->p.n_ff ? s->p.ff_face_ptr[s->p.n_ff] : 0));
   return 0;
 }
 

@@ -123,6 +123,13 @@ typedef struct {
      (TLM_SOLVER/outer_boundary.F90:133-318) instead of connect */
   int32_t hs_outer;
   const int32_t *hs_cell;
+
+  /* far-field surfaces (OUTPUT/far_field_surfaces.F90:252-351), one entry
+     per frequency: CSR list (ff_face_ptr[n_ff+1]) of 1-based output face
+     numbers and face codes 1..6 of the face-list entry after the side flip */
+  int32_t n_ff;
+  const double *ff_freq;
+  const int32_t *ff_face_ptr, *ff_face_out, *ff_face_code;
 } tlm_oracle_problem;
 
 typedef struct tlm_oracle_state tlm_oracle_state;
@@ -134,6 +141,8 @@ void tlm_oracle_destroy(tlm_oracle_state *s);
 int tlm_oracle_run(tlm_oracle_state *s, int32_t first_step, int32_t n_steps, double *cell_out);
 /* DFT accumulators: per surface, per face, (re,im) */
 int tlm_oracle_get_dft(tlm_oracle_state *s, double *out);
+/* far-field accumulators per surface face: J(3), M(3) as (re, im) pairs */
+int tlm_oracle_get_far_field(tlm_oracle_state *s, double *out);
 /* face output point values of every completed timestep: [timestep][n_face_probes] */
 int tlm_oracle_get_face_probes(tlm_oracle_state *s, double *out);
 /* link array dump in the reference layout V(12, nx, ny, nz) interior only */
