@@ -793,6 +793,20 @@ int launch_bulk(Mesh *m, const tlm::MeshDev<T> &md, int k) {
 
 // Enqueue relative steps [0, n) of one step bundle (kernels only, the base
 // counter is advanced by the caller).
+// Compile-time bound on the Z-filter orders of a mesh's special-cell kernel
+// (1, 2, 4 or the library maximum): the smallest that covers every material.
+int special_order_bound(int maxo) { return maxo <= 1 ? 1 : (maxo <= 2 ? 2 : (maxo <= 4 ? 4 : tlm::kMaxOrder)); }
+
+template <typename T>
+void launch_special(int bound, int blocks, cudaStream_t st, const tlm::MeshDev<T> &md, int n, int k) {
+  switch (bound) {
+    case 1: tlm::tlm_special_kernel<T, 1><<<blocks, 128, 0, st>>>(md, n, k); break;
+    case 2: tlm::tlm_special_kernel<T, 2><<<blocks, 128, 0, st>>>(md, n, k); break;
+    case 4: tlm::tlm_special_kernel<T, 4><<<blocks, 128, 0, st>>>(md, n, k); break;
+    default: tlm::tlm_special_kernel<T, tlm::kMaxOrder><<<blocks, 128, 0, st>>>(md, n, k); break;
+  }
+}
+
 tlm::PmmList pmm_list(Mesh *m) {
   return tlm::PmmList{(const int4 *)m->pmm_pos.p, (const int2 *)m->pmm_parmat.p, (double *)m->pmm_state.p,
                       (const double *)m->pmm_sigma.p, m->n_pmm};
@@ -824,7 +838,8 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
       m->last_launches++;
     }
     if (m->n_sp_dev) {
-      tlm::tlm_special_kernel<T><<<(m->n_sp_dev + 127) / 128, 128, 0, m->stream>>>(md, m->n_sp_dev, k);
+      launch_special<T>(special_order_bound(std::max(m->filt_eo, m->filt_mo)), (m->n_sp_dev + 127) / 128, m->stream,
+                        md, m->n_sp_dev, k);
       m->last_launches++;
     }
     if (fd.n_faces) {
@@ -1611,7 +1626,20 @@ int batch_step(Batch *b, bool dry) {
       b->last_launches++;
     }
   }
-  if (b->n_spb) { tlm::tlm_special_batch_kernel<T><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
+  if (b->n_spb) {
+    int maxo = 0;
+    for (int i : b->active) {
+      Mesh *m = get(b->handles[i]);
+      if (m) maxo = std::max(maxo, std::max(m->filt_eo, m->filt_mo));
+    }
+    switch (special_order_bound(maxo)) {
+      case 1: tlm::tlm_special_batch_kernel<T, 1><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
+      case 2: tlm::tlm_special_batch_kernel<T, 2><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
+      case 4: tlm::tlm_special_batch_kernel<T, 4><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
+      default: tlm::tlm_special_batch_kernel<T, tlm::kMaxOrder><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
+    }
+    b->last_launches++;
+  }
   if (b->n_faceb) { tlm::tlm_face_batch_kernel<T><<<b->n_faceb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
   for (int i : b->active) {  // outer-boundary Huygens surfaces of the members that have them
     Mesh *m = get(b->handles[i]);

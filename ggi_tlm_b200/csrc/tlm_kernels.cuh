@@ -45,7 +45,7 @@ enum PmlPort {
   Vxny = 0, Vxnz, Vxpy, Vxpz, Vynx, Vynz, Vypx, Vypz, Vznx, Vzny, Vzpx, Vzpy
 };
 
-enum SpecialFlags : int { SP_PML = 1, SP_MAT = 2, SP_EXC = 4, SP_OUT = 8 };
+enum SpecialFlags : int { SP_MAT = 2, SP_EXC = 4, SP_OUT = 8 };
 
 constexpr int kMaxOrder = 8;
 // PML-list parameter index of a PML cell inside a volume material (those
@@ -288,22 +288,30 @@ __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par,
 
 // evaluate_Zfilter (filter_subroutines.F90:510-540) on a state whose taps
 // w(1..order) are given; returns f and sets w0.
+// MAXO is a compile-time bound on the order: the loops unroll with the
+// runtime order as a predicate, so the taps stay in registers.
+template <int MAXO>
 __device__ __forceinline__ double zfilter_eval(const double *a, const double *b, int order, const double *w, double G,
                                                double &w0) {
   double W0 = G;
-  for (int i = 1; i <= order; i++) W0 = W0 - b[i] * w[i];
+#pragma unroll
+  for (int i = 1; i <= MAXO; i++)
+    if (i <= order) W0 = W0 - b[i] * w[i];
   W0 = W0 / b[0];
   w0 = W0;
   double F0 = 0.0;
   F0 = F0 + a[0] * W0;
-  for (int i = 1; i <= order; i++) F0 = F0 + a[i] * w[i];
+#pragma unroll
+  for (int i = 1; i <= MAXO; i++)
+    if (i <= order) F0 = F0 + a[i] * w[i];
   return F0;
 }
 
 // ---------------------------------------------------------------------------
 // Material / excitation / output cell (not PML), scatter.F90:274-547, in FP64
 // ---------------------------------------------------------------------------
-template <typename T>
+// MAXO: compile-time bound on every material's eps and mu filter order in the mesh.
+template <typename T, int MAXO>
 __device__ __forceinline__ void special_cell(const MeshDev<T> &m, int4 rec, int t, const T *incT, T *outT) {
   const int flags = rec.x & 0xff;
   const int material = rec.x >> 8;
@@ -320,7 +328,7 @@ __device__ __forceinline__ void special_cell(const MeshDev<T> &m, int4 rec, int 
   double VHz = 2.0 * (inc[Vy_xmax] - inc[Vx_ymax] - inc[Vy_xmin] + inc[Vx_ymin]);
   double Zx = Z04, Zy = Z04, Zz = Z04;
   double Vo[3] = {0, 0, 0}, Ys = 0.0;
-  double we[3][kMaxOrder + 1], wm[3][kMaxOrder + 1];
+  double we[3][MAXO + 1], wm[3][MAXO + 1];
   const MatDev *M = nullptr;
   int type = 0;
   const int fidx = rec.y;
@@ -338,8 +346,10 @@ __device__ __forceinline__ void special_cell(const MeshDev<T> &m, int4 rec, int 
       const int o = M->eps_order;
       for (int c = 0; c < 3; c++) {
         // timeshift_Zfilter: w(i) <- w(i-1)
-        for (int k = 0; k < o; k++) we[c][k + 1] = m.filt[(size_t)(c * m.filt_eo + k) * m.n_filt + fidx];
-        Vo[c] = zfilter_eval(M->eps_a, M->eps_b, o, we[c], 0.0, we[c][0]);
+#pragma unroll
+        for (int k = 0; k < MAXO; k++)
+          if (k < o) we[c][k + 1] = m.filt[(size_t)(c * m.filt_eo + k) * m.n_filt + fidx];
+        Vo[c] = zfilter_eval<MAXO>(M->eps_a, M->eps_b, o, we[c], 0.0, we[c][0]);
       }
       double V1, Y1;
       V1 = (VEx * Yx + Vo[0] * Ys) / (Yx + Ys); Y1 = Yx + Ys; VEx = V1; Yx = Y1;
@@ -356,9 +366,10 @@ __device__ __forceinline__ void special_cell(const MeshDev<T> &m, int4 rec, int 
       const int o = M->mu_order;
       double Vs[3];
       for (int c = 0; c < 3; c++) {
-        for (int k = 0; k < o; k++)
-          wm[c][k + 1] = m.filt[(size_t)(3 * m.filt_eo + c * m.filt_mo + k) * m.n_filt + fidx];
-        Vs[c] = zfilter_eval(M->mu_a, M->mu_b, o, wm[c], 0.0, wm[c][0]);
+#pragma unroll
+        for (int k = 0; k < MAXO; k++)
+          if (k < o) wm[c][k + 1] = m.filt[(size_t)(3 * m.filt_eo + c * m.filt_mo + k) * m.n_filt + fidx];
+        Vs[c] = zfilter_eval<MAXO>(M->mu_a, M->mu_b, o, wm[c], 0.0, wm[c][0]);
       }
       VHx = VHx + Vs[0]; Zx = Zx + Zs;
       VHy = VHy + Vs[1]; Zy = Zy + Zs;
@@ -398,16 +409,20 @@ __device__ __forceinline__ void special_cell(const MeshDev<T> &m, int4 rec, int 
       const int o = M->eps_order;
       const double Io[3] = {(Vx - Vo[0]) * Ys, (Vy - Vo[1]) * Ys, (Vz - Vo[2]) * Ys};
       for (int c = 0; c < 3; c++) {
-        zfilter_eval(M->eps_a, M->eps_b, o, we[c], Io[c], we[c][0]);
-        for (int k = 0; k < o; k++) m.filt[(size_t)(c * m.filt_eo + k) * m.n_filt + fidx] = we[c][k];
+        zfilter_eval<MAXO>(M->eps_a, M->eps_b, o, we[c], Io[c], we[c][0]);
+#pragma unroll
+        for (int k = 0; k < MAXO; k++)
+          if (k < o) m.filt[(size_t)(c * m.filt_eo + k) * m.n_filt + fidx] = we[c][k];
       }
     }
     if (M->mu_exists) {
       const int o = M->mu_order;
       const double G[3] = {-Ix, -Iy, -Iz};
       for (int c = 0; c < 3; c++) {
-        zfilter_eval(M->mu_a, M->mu_b, o, wm[c], G[c], wm[c][0]);
-        for (int k = 0; k < o; k++) m.filt[(size_t)(3 * m.filt_eo + c * m.filt_mo + k) * m.n_filt + fidx] = wm[c][k];
+        zfilter_eval<MAXO>(M->mu_a, M->mu_b, o, wm[c], G[c], wm[c][0]);
+#pragma unroll
+        for (int k = 0; k < MAXO; k++)
+          if (k < o) m.filt[(size_t)(3 * m.filt_eo + c * m.filt_mo + k) * m.n_filt + fidx] = wm[c][k];
       }
     }
   }
@@ -847,17 +862,17 @@ __global__ void __launch_bounds__(TILE / VEC) tlm_bulk_tma_kernel(const MeshDev<
 // state and links coalesce along x): gather, PML / material / excitation /
 // output scatter, reflected pulses + ghost slots.
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, int MAXO>
 __device__ __forceinline__ void special_body(const MeshDev<T> &m, int s, int rel_step);
 
-template <typename T>
+template <typename T, int MAXO>
 __global__ void __launch_bounds__(128) tlm_special_kernel(const MeshDev<T> m, int n_special, int rel_step) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_special) return;
-  special_body<T>(m, s, rel_step);
+  special_body<T, MAXO>(m, s, rel_step);
 }
 
-template <typename T>
+template <typename T, int MAXO>
 __device__ __forceinline__ void special_body(const MeshDev<T> &m, int s, int rel_step) {
   const int t = *m.d_base + rel_step;
   const T *__restrict__ in = (t & 1) ? m.links0 : m.links1;
@@ -880,12 +895,8 @@ __device__ __forceinline__ void special_body(const MeshDev<T> &m, int s, int rel
   ci[Vy_zmin] = in[Vy_zmax * P + idx - dz];
   ci[Vx_zmax] = in[Vx_zmin * P + idx + dz];
   ci[Vy_zmax] = in[Vy_zmin * P + idx + dz];
-  if (rec.x & SP_PML) {
-    double *row = (rec.w >= 0) ? m.cell_out + ((size_t)(t - 1) * m.n_out + rec.w) * 6 : nullptr;
-    pml_cell<T>(m, rec.y, rec.z, rec.w, ci, co, row);
-  } else {
-    special_cell<T>(m, rec, t, ci, co);
-  }
+  // PML cells never reach this list: they take tlm_pml_kernel
+  special_cell<T, MAXO>(m, rec, t, ci, co);
 #pragma unroll
   for (int p = 0; p < 12; p++) out[p * P + idx] = co[p];
   if (pos.x == 0) {
@@ -920,6 +931,15 @@ __device__ __forceinline__ void special_body(const MeshDev<T> &m, int s, int rel
 // it reads an 8-byte packed position (x | y<<21 | z<<42 | output<<63) and a
 // 2-byte PML parameter index.
 // ---------------------------------------------------------------------------
+// Resident 128-thread blocks per SM the PML kernel is compiled for (caps its
+// registers at 65536 / (128 x this)).  Measured on B200, 256^3 PML-spheres
+// and 512^3 point-source meshes: 3 is 1-5% faster per step than no bound
+// (FP64 drops from 184 registers to 170 without spills), 4 and 5 spill and
+// are no faster or slower.
+#ifndef TLM_PML_MIN_BLOCKS
+#define TLM_PML_MIN_BLOCKS 3
+#endif
+
 struct PmlList {
   const unsigned long long *pos;
   const uint16_t *par;
@@ -935,7 +955,7 @@ template <typename T>
 __device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl, int s, int rel_step);
 
 template <typename T>
-__global__ void __launch_bounds__(128) tlm_pml_kernel(const MeshDev<T> m, const PmlList pl, int rel_step,
+__global__ void __launch_bounds__(128, TLM_PML_MIN_BLOCKS) tlm_pml_kernel(const MeshDev<T> m, const PmlList pl, int rel_step,
                                                       int prefetch_blocks) {
   // one elected thread per block pulls the PML state of the block that runs
   // prefetch_blocks later into L2 (24 contiguous 512-byte ranges + metadata),
@@ -1585,12 +1605,12 @@ __global__ void __launch_bounds__(128) tlm_pml_batch_kernel(const BatchDev<T> b,
   pml_body<T>(b.meshes[w.x], pl, s, rel_step);
 }
 
-template <typename T>
+template <typename T, int MAXO>
 __global__ void __launch_bounds__(128) tlm_special_batch_kernel(const BatchDev<T> b, int rel_step) {
   const int2 w = b.special_blocks[blockIdx.x];
   const int s = w.y + threadIdx.x;
   if (s >= b.n_special[w.x]) return;
-  special_body<T>(b.meshes[w.x], s, rel_step);
+  special_body<T, MAXO>(b.meshes[w.x], s, rel_step);
 }
 
 template <typename T>
