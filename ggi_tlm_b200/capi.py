@@ -39,7 +39,7 @@ EXPORTS = [
     "tlm_gpu_batch_run", "tlm_gpu_batch_synchronize", "tlm_gpu_batch_last_run", "tlm_gpu_batch_destroy",
     "tlm_gpu_set_small_to_zero", "tlm_gpu_set_pml_sigma", "tlm_gpu_set_face_excitation",
     "tlm_gpu_set_face_outputs", "tlm_gpu_fetch_face_output", "tlm_gpu_set_outer_huygens",
-    "tlm_gpu_set_far_field", "tlm_gpu_fetch_far_field",
+    "tlm_gpu_set_far_field", "tlm_gpu_fetch_far_field", "tlm_gpu_pool_release", "tlm_gpu_pool_cached_bytes",
 ]
 
 
@@ -82,6 +82,8 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_outer_huygens": [i64, i32, _i32p, _f64p, _f64p, _f64p, C.c_double, C.c_double, i32],
         "tlm_gpu_set_far_field": [i64, i32, _f64p, _i32p, _i32p, _i32p],
         "tlm_gpu_fetch_far_field": [i64, _f64p],
+        "tlm_gpu_pool_release": [],
+        "tlm_gpu_pool_cached_bytes": [C.POINTER(i64)],
         "tlm_gpu_fetch_face_output": [i64, i32, i32, _f64p],
         "tlm_gpu_set_excitation": [i64, i32, i32, _f64p, _f64p, i32, _i32p, _i32p, _i32p, _i32p, i32],
         "tlm_gpu_set_faces": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, i32, i32],
@@ -117,6 +119,18 @@ def load_library(path: Optional[str] = None):
         f.restype = C.c_int
     _lib = lib
     return lib
+
+
+def pool_cached_bytes() -> int:
+    """Bytes the library's device-memory cache holds for reuse."""
+    v = C.c_int64(0)
+    _check(load_library().tlm_gpu_pool_cached_bytes(C.byref(v)))
+    return int(v.value)
+
+
+def pool_release():
+    """Return every cached device block to the driver."""
+    _check(load_library().tlm_gpu_pool_release())
 
 
 def num_variants() -> int:

@@ -44,13 +44,128 @@ int fail(int code, const char *fmt, ...) {
                                        __FILE__, __LINE__);                                       \
   } while (0)
 
+// ---------------------------------------------------------------------------
+// Device-memory cache.  Buffers released by destroyed meshes and by rebuilt
+// batch lists are kept per device and handed out again to later allocations
+// of a similar size, so a serving loop that creates and destroys meshes all
+// the time stops paying for cudaMalloc/cudaFree (a single cudaFree of a
+// large buffer took up to 0.6 s on B200).  A released block may still be read
+// by kernels in flight, so the first reuse after any release synchronises
+// the device first (cudaFree synchronised implicitly too).  The cache holds
+// at most TLM_POOL_CACHE_BYTES (default 16 GiB) per device; beyond that, and
+// on tlm_gpu_pool_release, blocks go back to the driver.
+// ---------------------------------------------------------------------------
+namespace pool {
+std::mutex mu;
+std::map<int, std::multimap<size_t, void *>> blocks;  // device -> (capacity, pointer)
+std::map<int, size_t> cached;                         // device -> cached bytes
+std::map<int, bool> released_since_sync;              // device -> a release happened since the last sync
+
+size_t cache_limit() {
+  static size_t lim = [] {
+    const char *e = getenv("TLM_POOL_CACHE_BYTES");
+    return e ? (size_t)strtoull(e, nullptr, 10) : ((size_t)16 << 30);
+  }();
+  return lim;
+}
+
+size_t round_up(size_t b) {
+  const size_t g = b <= ((size_t)1 << 20) ? 4096 : ((size_t)2 << 20);
+  return (b + g - 1) / g * g;
+}
+
+// A block of at least `bytes` on the current device; its capacity in *cap.
+cudaError_t alloc(size_t bytes, void **p, size_t *cap) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const size_t want = round_up(bytes);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto &bl = blocks[dev];
+    auto it = bl.lower_bound(want);
+    if (it != bl.end() && it->first <= want + want / 4) {
+      if (released_since_sync[dev]) {
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) return e;
+        released_since_sync[dev] = false;
+      }
+      *p = it->second;
+      *cap = it->first;
+      cached[dev] -= it->first;
+      bl.erase(it);
+      return cudaSuccess;
+    }
+  }
+  cudaError_t e = cudaMalloc(p, want);
+  if (e == cudaErrorMemoryAllocation) {  // give the cache back to the driver and retry
+    cudaGetLastError();
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto &kv : blocks[dev]) cudaFree(kv.second);
+    blocks[dev].clear();
+    cached[dev] = 0;
+    e = cudaMalloc(p, want);
+  }
+  *cap = want;
+  return e;
+}
+
+void release(int dev, void *p, size_t cap) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(mu);
+  if (cached[dev] + cap > cache_limit()) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != dev) cudaSetDevice(dev);
+    cudaFree(p);
+    if (cur != dev) cudaSetDevice(cur);
+    return;
+  }
+  blocks[dev].emplace(cap, p);
+  cached[dev] += cap;
+  released_since_sync[dev] = true;
+}
+
+void release_all() {
+  std::lock_guard<std::mutex> lk(mu);
+  int cur = 0;
+  cudaGetDevice(&cur);
+  for (auto &dv : blocks) {
+    cudaSetDevice(dv.first);
+    for (auto &kv : dv.second) cudaFree(kv.second);
+    dv.second.clear();
+    cached[dv.first] = 0;
+  }
+  cudaSetDevice(cur);
+}
+
+size_t cached_bytes() {
+  std::lock_guard<std::mutex> lk(mu);
+  size_t t = 0;
+  for (auto &kv : cached) t += kv.second;
+  return t;
+}
+}  // namespace pool
+
 struct DevBuf {
   void *p = nullptr;
-  size_t bytes = 0;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
+  size_t bytes = 0;  // requested
+  size_t cap = 0;    // capacity of the cached block
+  int dev = 0;
+  ~DevBuf() { pool::release(dev, p, cap); }
 };
+
+// Allocate `bytes` into b from the device cache (the current device).
+cudaError_t buf_alloc(DevBuf &b, size_t bytes) {
+  if (b.p) {
+    pool::release(b.dev, b.p, b.cap);
+    b.p = nullptr;
+  }
+  b.bytes = bytes;
+  cudaGetDevice(&b.dev);
+  cudaError_t e = pool::alloc(bytes, &b.p, &b.cap);
+  if (e != cudaSuccess) b.p = nullptr;
+  return e;
+}
 
 struct Mesh {
   tlm_gpu_mesh_desc desc{};
@@ -154,17 +269,9 @@ Mesh *get(int64_t h) {
 }
 
 int dalloc(Mesh *m, DevBuf &b, size_t bytes) {
-  if (b.p) {
-    cudaFree(b.p);
-    m->dev_bytes -= b.bytes;
-    b.p = nullptr;
-  }
-  b.bytes = std::max<size_t>(bytes, 16);
-  cudaError_t e = cudaMalloc(&b.p, b.bytes);
-  if (e != cudaSuccess) {
-    b.p = nullptr;
-    return fail(TLM_E_OOM, "cudaMalloc(%zu) failed: %s", b.bytes, cudaGetErrorString(e));
-  }
+  if (b.p) m->dev_bytes -= b.bytes;
+  cudaError_t e = buf_alloc(b, std::max<size_t>(bytes, 16));
+  if (e != cudaSuccess) return fail(TLM_E_OOM, "device allocation of %zu bytes failed: %s", b.bytes, cudaGetErrorString(e));
   m->dev_bytes += b.bytes;
   return TLM_OK;
 }
@@ -1446,6 +1553,17 @@ int tlm_gpu_destroy(int64_t h) {
   return TLM_OK;
 }
 
+int tlm_gpu_pool_release(void) {
+  pool::release_all();
+  return TLM_OK;
+}
+
+int tlm_gpu_pool_cached_bytes(int64_t *bytes) {
+  if (!bytes) return fail(TLM_E_BADARG, "null output");
+  *bytes = (int64_t)pool::cached_bytes();
+  return TLM_OK;
+}
+
 int tlm_gpu_last_error(char *buf, int32_t len) {
   if (!buf || len <= 0) return TLM_E_BADARG;
   std::snprintf(buf, (size_t)len, "%s", g_last_error.c_str());
@@ -1493,17 +1611,9 @@ Batch *get_batch(int64_t h) {
 
 template <typename V>
 int bupload(Batch *b, DevBuf &buf, const std::vector<V> &v) {
-  if (buf.p) {
-    cudaFree(buf.p);
-    b->dev_bytes -= buf.bytes;
-    buf.p = nullptr;
-  }
-  buf.bytes = std::max<size_t>(v.size() * sizeof(V), 16);
-  cudaError_t e = cudaMalloc(&buf.p, buf.bytes);
-  if (e != cudaSuccess) {
-    buf.p = nullptr;
-    return fail(TLM_E_OOM, "cudaMalloc(%zu) failed: %s", buf.bytes, cudaGetErrorString(e));
-  }
+  if (buf.p) b->dev_bytes -= buf.bytes;
+  cudaError_t e = buf_alloc(buf, std::max<size_t>(v.size() * sizeof(V), 16));
+  if (e != cudaSuccess) return fail(TLM_E_OOM, "device allocation of %zu bytes failed: %s", buf.bytes, cudaGetErrorString(e));
   b->dev_bytes += buf.bytes;
   if (!v.empty()) CK(cudaMemcpy(buf.p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice));
   return TLM_OK;

@@ -284,6 +284,16 @@ int tlm_gpu_batch_destroy(int64_t batch);
 
 /* Message of the last failure on this thread (NUL-terminated, truncated
    to len-1 characters). */
+/* Device-memory cache of the library (no counterpart in the reference,
+   whose arrays are allocated once per run): buffers of destroyed meshes and
+   batches are kept per device, up to TLM_POOL_CACHE_BYTES (default 16 GiB),
+   and reused by later meshes, so creating and destroying meshes in a
+   serving loop does not call cudaMalloc/cudaFree each time.
+   tlm_gpu_pool_release returns every cached block to the driver;
+   tlm_gpu_pool_cached_bytes reports how much is cached. */
+int tlm_gpu_pool_release(void);
+int tlm_gpu_pool_cached_bytes(int64_t *bytes);
+
 int tlm_gpu_last_error(char *buf, int32_t len);
 
 #ifdef __cplusplus
