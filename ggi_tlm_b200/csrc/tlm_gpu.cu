@@ -553,7 +553,7 @@ int finalize(Mesh *m) {
   CK(cudaMemset(m->links.p, 0, m->links.bytes));
   // ---- PML
   const size_t pesz = m->fp64 ? sizeof(tlm::PmlTypes<double>::state) : sizeof(tlm::PmlTypes<float>::state);
-  if ((rc = dalloc(m, m->pml_state, (size_t)tlm::kPmlState * std::max(m->n_pml_cells, 1) * pesz + 64))) return rc;
+  if ((rc = dalloc(m, m->pml_state, tlm::pml_state_elems(std::max(m->n_pml_cells, 1)) * pesz + 64))) return rc;
   CK(cudaMemset(m->pml_state.p, 0, m->pml_state.bytes));
   {
     std::vector<double> par((size_t)std::max(m->n_pml_params, 1) * 16, 0.0);

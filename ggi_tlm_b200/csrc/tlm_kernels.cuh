@@ -48,6 +48,14 @@ enum PmlPort {
 enum SpecialFlags : int { SP_MAT = 2, SP_EXC = 4, SP_OUT = 8 };
 
 constexpr int kMaxOrder = 8;
+// PML state layout: tiles of 32 cells, each holding the 24 values as 24
+// runs of 32 words ([n/32][24][32]), so a warp's state is one contiguous
+// 3 KB (FP32) or 6 KB (FP64) block instead of 24 separate streams.
+__host__ __device__ __forceinline__ size_t pml_sidx(int k, long long s) {
+  return ((size_t)(s >> 5) * 24 + (size_t)k) * 32 + (size_t)(s & 31);
+}
+__host__ __device__ __forceinline__ size_t pml_state_elems(long long n) { return (size_t)((n + 31) / 32) * 24 * 32; }
+
 // PML-list parameter index of a PML cell inside a volume material (those
 // cells take tlm_pml_material_kernel)
 constexpr uint16_t kPmlMaterialSlot = 0xFFFF;
@@ -193,15 +201,15 @@ __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par,
   const A Csy_sz = A(P[12]), Csz_sx = A(P[13]), Csx_sy = A(P[14]);
   ST *S = m.pml_state;
   const int n = m.n_pml;
-  const A last_Ix = __ldcs(S + 0 * n + pidx), last_Iy = __ldcs(S + 1 * n + pidx), last_Iz = __ldcs(S + 2 * n + pidx);
+  const A last_Ix = __ldcs(S + pml_sidx(0, pidx)), last_Iy = __ldcs(S + pml_sidx(1, pidx)), last_Iz = __ldcs(S + pml_sidx(2, pidx));
   A last_Vi[12];
 #pragma unroll
-  for (int k = 0; k < 12; k++) last_Vi[k] = __ldcs(S + (size_t)(3 + k) * n + pidx);
-  const A last_Vxt = __ldcs(S + (size_t)15 * n + pidx), last_Vyt = __ldcs(S + (size_t)16 * n + pidx);
-  const A last_Vzt = __ldcs(S + (size_t)17 * n + pidx);
-  const A last_Vxyt = __ldcs(S + (size_t)18 * n + pidx), last_Vyxt = __ldcs(S + (size_t)19 * n + pidx);
-  const A last_Vzxt = __ldcs(S + (size_t)20 * n + pidx), last_Vxzt = __ldcs(S + (size_t)21 * n + pidx);
-  const A last_Vyzt = __ldcs(S + (size_t)22 * n + pidx), last_Vzyt = __ldcs(S + (size_t)23 * n + pidx);
+  for (int k = 0; k < 12; k++) last_Vi[k] = __ldcs(S + pml_sidx(3 + k, pidx));
+  const A last_Vxt = __ldcs(S + pml_sidx(15, pidx)), last_Vyt = __ldcs(S + pml_sidx(16, pidx));
+  const A last_Vzt = __ldcs(S + pml_sidx(17, pidx));
+  const A last_Vxyt = __ldcs(S + pml_sidx(18, pidx)), last_Vyxt = __ldcs(S + pml_sidx(19, pidx));
+  const A last_Vzxt = __ldcs(S + pml_sidx(20, pidx)), last_Vxzt = __ldcs(S + pml_sidx(21, pidx));
+  const A last_Vyzt = __ldcs(S + pml_sidx(22, pidx)), last_Vzyt = __ldcs(S + pml_sidx(23, pidx));
 
   // STAGE 3: half-cell loss on incident pulses
   A V[12];
@@ -247,16 +255,16 @@ __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par,
   const A Vyz_se = ax * (Z0 * (-last_Ix + Csz2 * (Ix + last_Ix)) + Csy_sz * last_Vyzt);
   const A Vzy_se = ax * (Z0 * (-last_Ix + Csy2 * (Ix + last_Ix)) + Csy_sz * last_Vzyt);
   // STAGE 8 + 9: save state
-  __stcs(S + 0 * n + pidx, ST(Ix)); __stcs(S + 1 * n + pidx, ST(Iy)); __stcs(S + 2 * n + pidx, ST(Iz));
+  __stcs(S + pml_sidx(0, pidx), ST(Ix)); __stcs(S + pml_sidx(1, pidx), ST(Iy)); __stcs(S + pml_sidx(2, pidx), ST(Iz));
 #pragma unroll
-  for (int k = 0; k < 12; k++) __stcs(S + (size_t)(3 + k) * n + pidx, ST(V[k]));
-  __stcs(S + (size_t)15 * n + pidx, ST(Vxt)); __stcs(S + (size_t)16 * n + pidx, ST(Vyt)); __stcs(S + (size_t)17 * n + pidx, ST(Vzt));
-  __stcs(S + (size_t)18 * n + pidx, ST(az * Iz * Z0 + Vxy_se));
-  __stcs(S + (size_t)19 * n + pidx, ST(az * Iz * Z0 + Vyx_se));
-  __stcs(S + (size_t)20 * n + pidx, ST(ay * Iy * Z0 + Vzx_se));
-  __stcs(S + (size_t)21 * n + pidx, ST(ay * Iy * Z0 + Vxz_se));
-  __stcs(S + (size_t)22 * n + pidx, ST(ax * Ix * Z0 + Vyz_se));
-  __stcs(S + (size_t)23 * n + pidx, ST(ax * Ix * Z0 + Vzy_se));
+  for (int k = 0; k < 12; k++) __stcs(S + pml_sidx(3 + k, pidx), ST(V[k]));
+  __stcs(S + pml_sidx(15, pidx), ST(Vxt)); __stcs(S + pml_sidx(16, pidx), ST(Vyt)); __stcs(S + pml_sidx(17, pidx), ST(Vzt));
+  __stcs(S + pml_sidx(18, pidx), ST(az * Iz * Z0 + Vxy_se));
+  __stcs(S + pml_sidx(19, pidx), ST(az * Iz * Z0 + Vyx_se));
+  __stcs(S + pml_sidx(20, pidx), ST(ay * Iy * Z0 + Vzx_se));
+  __stcs(S + pml_sidx(21, pidx), ST(ay * Iy * Z0 + Vxz_se));
+  __stcs(S + pml_sidx(22, pidx), ST(ax * Ix * Z0 + Vyz_se));
+  __stcs(S + pml_sidx(23, pidx), ST(ax * Ix * Z0 + Vzy_se));
   // STAGE 10
   const A Vynx_P = Vx_sh - Vyx_se, Vypx_P = Vx_sh + Vyx_se;
   const A Vznx_P = Vx_sh + Vzx_se, Vzpx_P = Vx_sh - Vzx_se;
@@ -958,20 +966,17 @@ template <typename T>
 __global__ void __launch_bounds__(128, TLM_PML_MIN_BLOCKS) tlm_pml_kernel(const MeshDev<T> m, const PmlList pl, int rel_step,
                                                       int prefetch_blocks) {
   // one elected thread per block pulls the PML state of the block that runs
-  // prefetch_blocks later into L2 (24 contiguous 512-byte ranges + metadata),
-  // so that block's state loads hit L2.  Ranges are widened to 16-byte
-  // boundaries; the state and position buffers carry 64 bytes of padding so
-  // the widened ranges stay inside their allocations.
+  // prefetch_blocks later into L2 (one contiguous range of whole 32-cell
+  // tiles + metadata), so that block's state loads hit L2.  The position
+  // range is widened to 16-byte boundaries; the position buffer carries 64
+  // bytes of padding so the widened range stays inside its allocation.
   if (threadIdx.x == 0 && prefetch_blocks > 0) {
     const long long s0 = (long long)(blockIdx.x + prefetch_blocks) * blockDim.x;
     if (s0 < pl.n) {
       const int cnt = (int)min((long long)blockDim.x, (long long)pl.n - s0);
-      const uint32_t sb = (uint32_t)(((cnt * (int)sizeof(typename PmlTypes<T>::state)) + 15) & ~15);
-      for (int k = 0; k < kPmlState; k++) {
-        const char *a = reinterpret_cast<const char *>(m.pml_state + (size_t)k * m.n_pml + s0);
-        const char *al = reinterpret_cast<const char *>(reinterpret_cast<uintptr_t>(a) & ~(uintptr_t)15);
-        bulk_prefetch_l2(al, sb + 16);
-      }
+      const long long tiles = ((long long)cnt + 31) / 32;  // s0 is a multiple of 128
+      const char *a = reinterpret_cast<const char *>(m.pml_state + pml_sidx(0, s0));
+      bulk_prefetch_l2(a, (uint32_t)(tiles * 24 * 32 * sizeof(typename PmlTypes<T>::state)));
       const char *pa = reinterpret_cast<const char *>(reinterpret_cast<uintptr_t>(pl.pos + s0) & ~(uintptr_t)15);
       bulk_prefetch_l2(pa, (uint32_t)((cnt * 8 + 15) & ~15) + 16);
     }
