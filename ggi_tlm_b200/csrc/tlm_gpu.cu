@@ -488,7 +488,7 @@ int finalize(Mesh *m) {
         } else {
           if (mat) {
             flags |= tlm::SP_MAT;
-            if (m->mats[mat - 1].type == 3) r.y = n_filt++;
+            if (m->mats[mat - 1].type == 3) r.y = (int)rec.size();  // taps slot = record index
           }
           if (m->sp_exc[s]) {
             flags |= tlm::SP_EXC;
@@ -540,6 +540,7 @@ int finalize(Mesh *m) {
   }
   if (exc_no != m->n_exc_cells) return fail(TLM_E_BADARG, "excitation cells: %d flagged, %d declared", exc_no, m->n_exc_cells);
   if (out_no != m->n_out_cells) return fail(TLM_E_BADARG, "output cells: %d flagged, %d declared", out_no, m->n_out_cells);
+  n_filt = (int)rec.size();  // one tap slot per record (special_cell loads taps by record index)
   m->n_filt = n_filt;
   m->n_sp_dev = (int)rec.size();
   int rc;
@@ -902,13 +903,16 @@ int launch_bulk(Mesh *m, const tlm::MeshDev<T> &md, int k) {
 // counter is advanced by the caller).
 // Compile-time bound on the Z-filter orders of a mesh's special-cell kernel
 // (1, 2, 4 or the library maximum): the smallest that covers every material.
-int special_order_bound(int maxo) { return maxo <= 1 ? 1 : (maxo <= 2 ? 2 : (maxo <= 4 ? 4 : tlm::kMaxOrder)); }
+int special_order_bound(int maxo) {
+  return maxo <= 1 ? 1 : (maxo <= 2 ? 2 : (maxo <= 3 ? 3 : (maxo <= 4 ? 4 : tlm::kMaxOrder)));
+}
 
 template <typename T>
 void launch_special(int bound, int blocks, cudaStream_t st, const tlm::MeshDev<T> &md, int n, int k) {
   switch (bound) {
     case 1: tlm::tlm_special_kernel<T, 1><<<blocks, 128, 0, st>>>(md, n, k); break;
     case 2: tlm::tlm_special_kernel<T, 2><<<blocks, 128, 0, st>>>(md, n, k); break;
+    case 3: tlm::tlm_special_kernel<T, 3><<<blocks, 128, 0, st>>>(md, n, k); break;
     case 4: tlm::tlm_special_kernel<T, 4><<<blocks, 128, 0, st>>>(md, n, k); break;
     default: tlm::tlm_special_kernel<T, tlm::kMaxOrder><<<blocks, 128, 0, st>>>(md, n, k); break;
   }
@@ -1745,6 +1749,7 @@ int batch_step(Batch *b, bool dry) {
     switch (special_order_bound(maxo)) {
       case 1: tlm::tlm_special_batch_kernel<T, 1><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
       case 2: tlm::tlm_special_batch_kernel<T, 2><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
+      case 3: tlm::tlm_special_batch_kernel<T, 3><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
       case 4: tlm::tlm_special_batch_kernel<T, 4><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
       default: tlm::tlm_special_batch_kernel<T, tlm::kMaxOrder><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
     }

@@ -319,8 +319,11 @@ __device__ __forceinline__ double zfilter_eval(const double *a, const double *b,
 // Material / excitation / output cell (not PML), scatter.F90:274-547, in FP64
 // ---------------------------------------------------------------------------
 // MAXO: compile-time bound on every material's eps and mu filter order in the mesh.
+// s: the record index, which is also the cell's slot in the filter-tap
+// arrays (one slot per record), so the taps can be loaded before the
+// record and its material are known.
 template <typename T, int MAXO>
-__device__ __forceinline__ void special_cell(const MeshDev<T> &m, int4 rec, int t, const T *incT, T *outT) {
+__device__ __forceinline__ void special_cell(const MeshDev<T> &m, int s, int4 rec, int t, const T *incT, T *outT) {
   const int flags = rec.x & 0xff;
   const int material = rec.x >> 8;
   double inc[12];
@@ -339,7 +342,18 @@ __device__ __forceinline__ void special_cell(const MeshDev<T> &m, int4 rec, int 
   double we[3][MAXO + 1], wm[3][MAXO + 1];
   const MatDev *M = nullptr;
   int type = 0;
-  const int fidx = rec.y;
+  const int fidx = s;
+  // taps w(1..order) of every filter up to the mesh's largest orders
+  // (timeshift_Zfilter: w(i) <- w(i-1)); slots past a material's own order
+  // are loaded but not used
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+#pragma unroll
+    for (int k = 0; k < MAXO; k++) {
+      if (k < m.filt_eo) we[c][k + 1] = m.filt[(size_t)(c * m.filt_eo + k) * m.n_filt + fidx];
+      if (k < m.filt_mo) wm[c][k + 1] = m.filt[(size_t)(3 * m.filt_eo + c * m.filt_mo + k) * m.n_filt + fidx];
+    }
+  }
   if (flags & SP_MAT) {
     M = m.mats + (material - 1);
     type = M->type;
@@ -352,13 +366,7 @@ __device__ __forceinline__ void special_cell(const MeshDev<T> &m, int4 rec, int 
     if (M->eps_exists) {
       Ys = M->Ys_eps_f;
       const int o = M->eps_order;
-      for (int c = 0; c < 3; c++) {
-        // timeshift_Zfilter: w(i) <- w(i-1)
-#pragma unroll
-        for (int k = 0; k < MAXO; k++)
-          if (k < o) we[c][k + 1] = m.filt[(size_t)(c * m.filt_eo + k) * m.n_filt + fidx];
-        Vo[c] = zfilter_eval<MAXO>(M->eps_a, M->eps_b, o, we[c], 0.0, we[c][0]);
-      }
+      for (int c = 0; c < 3; c++) Vo[c] = zfilter_eval<MAXO>(M->eps_a, M->eps_b, o, we[c], 0.0, we[c][0]);
       double V1, Y1;
       V1 = (VEx * Yx + Vo[0] * Ys) / (Yx + Ys); Y1 = Yx + Ys; VEx = V1; Yx = Y1;
       V1 = (VEy * Yy + Vo[1] * Ys) / (Yy + Ys); Y1 = Yy + Ys; VEy = V1; Yy = Y1;
@@ -373,12 +381,7 @@ __device__ __forceinline__ void special_cell(const MeshDev<T> &m, int4 rec, int 
       const double Zs = M->Zs_mu_f;
       const int o = M->mu_order;
       double Vs[3];
-      for (int c = 0; c < 3; c++) {
-#pragma unroll
-        for (int k = 0; k < MAXO; k++)
-          if (k < o) wm[c][k + 1] = m.filt[(size_t)(3 * m.filt_eo + c * m.filt_mo + k) * m.n_filt + fidx];
-        Vs[c] = zfilter_eval<MAXO>(M->mu_a, M->mu_b, o, wm[c], 0.0, wm[c][0]);
-      }
+      for (int c = 0; c < 3; c++) Vs[c] = zfilter_eval<MAXO>(M->mu_a, M->mu_b, o, wm[c], 0.0, wm[c][0]);
       VHx = VHx + Vs[0]; Zx = Zx + Zs;
       VHy = VHy + Vs[1]; Zy = Zy + Zs;
       VHz = VHz + Vs[2]; Zz = Zz + Zs;
@@ -904,7 +907,7 @@ __device__ __forceinline__ void special_body(const MeshDev<T> &m, int s, int rel
   ci[Vx_zmax] = in[Vx_zmin * P + idx + dz];
   ci[Vy_zmax] = in[Vy_zmin * P + idx + dz];
   // PML cells never reach this list: they take tlm_pml_kernel
-  special_cell<T, MAXO>(m, rec, t, ci, co);
+  special_cell<T, MAXO>(m, s, rec, t, ci, co);
 #pragma unroll
   for (int p = 0; p < 12; p++) out[p * P + idx] = co[p];
   if (pos.x == 0) {
