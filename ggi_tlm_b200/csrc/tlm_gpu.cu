@@ -228,6 +228,7 @@ struct Mesh {
   int ff_entries = 0;
   int n_sp_dev = 0;  // non-PML special cells on the device list
   int n_pml_list = 0, n_pml_out = 0;
+  tlm::PmlShell pml_shell{};  // .on when the PML cells form a box shell
   DevBuf pml_pos, pml_par16, pml_outmap;
   // bulk-kernel variant: 0 = register-pipelined kernel, 1..kNumVariants-1 = TMA-staged configurations
   int variant = 1;
@@ -394,6 +395,56 @@ tlm::DftDev dft_dev(Mesh *m) {
 }
 
 // Build and upload all device tables.
+// The thicknesses of the box shell that the PML cells form, read off their
+// (traversal-ordered, packed) positions, and checked cell by cell; .on = 0
+// when the cells are not such a shell (the kernels then load positions).
+tlm::PmlShell detect_pml_shell(const std::vector<unsigned long long> &pos, int nx, int ny, int nz) {
+  tlm::PmlShell h{};
+  if (pos.empty() || (long long)nx * ny > (1ll << 30) || pos.size() > (size_t)INT32_MAX) return h;
+  auto X = [](unsigned long long p) { return (int)(p & 0x1fffffull); };
+  auto Y = [](unsigned long long p) { return (int)((p >> 21) & 0x1fffffull); };
+  auto Z = [](unsigned long long p) { return (int)((p >> 42) & 0x1fffffull); };
+  // slab thicknesses: leading / trailing z-planes that are entirely PML,
+  // then, in the first plane between them, leading / trailing full rows,
+  // then the leading / trailing run of x in the first row between those
+  std::vector<long long> per_z(nz, 0);
+  for (auto p : pos) per_z[Z(p)]++;
+  const long long full = (long long)nx * ny;
+  int zl = 0, zh = 0;
+  while (zl < nz && per_z[zl] == full) zl++;
+  while (zh < nz - zl && per_z[nz - 1 - zh] == full) zh++;
+  int yl = 0, yh = 0, xl = 0, xh = 0;
+  if (zl + zh < nz) {
+    const int zm = zl;
+    std::vector<int> per_y(ny, 0);
+    for (auto p : pos)
+      if (Z(p) == zm) per_y[Y(p)]++;
+    while (yl < ny && per_y[yl] == nx) yl++;
+    while (yh < ny - yl && per_y[ny - 1 - yh] == nx) yh++;
+    if (yl + yh < ny) {
+      std::vector<char> xin(nx, 0);
+      for (auto p : pos)
+        if (Z(p) == zm && Y(p) == yl) xin[X(p)] = 1;
+      while (xl < nx && xin[xl]) xl++;
+      while (xh < nx - xl && xin[nx - 1 - xh]) xh++;
+    }
+  }
+  h.nx = nx; h.ny = ny; h.nz = nz;
+  h.xl = xl; h.xh = xh; h.yl = yl; h.yh = yh; h.zl = zl; h.zh = zh;
+  h.full = (int)full;
+  h.partial = (yl + yh) * nx + (ny - yl - yh) * (xl + xh);
+  const long long count = (long long)(zl + zh) * full + (long long)(nz - zl - zh) * h.partial;
+  if (count != (long long)pos.size()) return tlm::PmlShell{};
+  // the decoder the kernels run must reproduce every listed position
+  for (size_t s = 0; s < pos.size(); s++) {
+    int x, y, z;
+    tlm::pml_shell_pos(h, (int)s, x, y, z);
+    if (x != X(pos[s]) || y != Y(pos[s]) || z != Z(pos[s])) return tlm::PmlShell{};
+  }
+  h.on = 1;
+  return h;
+}
+
 int finalize(Mesh *m) {
   if (m->finalized) return TLM_OK;
   const auto &D = m->desc;
@@ -517,6 +568,9 @@ int finalize(Mesh *m) {
   if ((int)pml_pos.size() != m->n_pml_cells) return fail(TLM_E_BADARG, "PML cells: %zu flagged, %d declared", pml_pos.size(), m->n_pml_cells);
   if (nx >= (1 << 21) || ny >= (1 << 21) || nz >= (1 << 21)) return fail(TLM_E_BADARG, "mesh too large for packed positions");
   m->n_pml_list = (int)pml_pos.size();
+  m->pml_shell = detect_pml_shell(pml_pos, nx, ny, nz);
+  if (const char *e = getenv("TLM_PML_SHELL"))  // "0": load positions even for a shell
+    if (e[0] == '0') m->pml_shell = tlm::PmlShell{};
   m->n_pmm = (int)pmm_pos.size();
   if (m->n_pmm) {
     int rc2;
@@ -940,7 +994,7 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
     m->last_launches++;
     if (m->n_pml_list) {
       tlm::PmlList pl{(const unsigned long long *)m->pml_pos.p, (const uint16_t *)m->pml_par16.p,
-                      (const int2 *)m->pml_outmap.p, m->n_pml_list, m->n_pml_out};
+                      (const int2 *)m->pml_outmap.p, m->n_pml_list, m->n_pml_out, m->pml_shell};
       tlm::tlm_pml_kernel<T><<<(m->n_pml_list + 127) / 128, 128, 0, m->stream>>>(md, pl, k, m->pml_prefetch);
       m->last_launches++;
     }
@@ -1642,7 +1696,7 @@ int build_batch_lists(Batch *b) {
     if (rc) return rc;
     md.push_back(mesh_dev<T>(m));
     pl.push_back(tlm::PmlList{(const unsigned long long *)m->pml_pos.p, (const uint16_t *)m->pml_par16.p,
-                              (const int2 *)m->pml_outmap.p, m->n_pml_list, m->n_pml_out});
+                              (const int2 *)m->pml_outmap.p, m->n_pml_list, m->n_pml_out, m->pml_shell});
     fd.push_back(face_dev(m));
     dd.push_back(dft_dev(m));
     nsp.push_back(m->n_sp_dev);

@@ -951,12 +951,70 @@ __device__ __forceinline__ void special_body(const MeshDev<T> &m, int s, int rel
 #define TLM_PML_MIN_BLOCKS 3
 #endif
 
+// The PML cells of the reference's meshes form a box shell: the cells within
+// xl/xh of the x ends, yl/yh of the y ends or zl/zh of the z ends
+// (calc_pml_dist).  Numbered in traversal order, a cell's position then
+// follows from its PML number, so the link addresses do not wait for a
+// position load.
+struct PmlShell {
+  int on;                 // 1: positions from the shell, 0: from `pos`
+  int nx, ny, nz, xl, xh, yl, yh, zl, zh;
+  int full, partial;      // PML cells of a whole z-plane / of a plane between the z slabs
+};
+
 struct PmlList {
   const unsigned long long *pos;
   const uint16_t *par;
-  const int2 *out_map;  // (pml index, output number) of PML output cells
+  const int2 *out_map;  // (pml index, output number) of PML output cells, sorted by pml index
   int n, n_out_map;
+  PmlShell sh;
 };
+
+// Position of PML cell s of a shell (traversal order z, y, x).
+__host__ __device__ __forceinline__ void pml_shell_pos(const PmlShell &h, int s, int &x, int &y, int &z) {
+  const int lo = h.zl * h.full;
+  if (s < lo) {
+    z = s / h.full;
+    const int r = s - z * h.full;
+    y = r / h.nx;
+    x = r - y * h.nx;
+    return;
+  }
+  const int s2 = s - lo;
+  const int mid = h.nz - h.zl - h.zh;
+  if (s2 < mid * h.partial) {
+    const int zz = s2 / h.partial;
+    z = h.zl + zz;
+    const int r = s2 - zz * h.partial;
+    const int rows_lo = h.yl * h.nx;
+    if (r < rows_lo) {
+      y = r / h.nx;
+      x = r - y * h.nx;
+      return;
+    }
+    const int r2 = r - rows_lo;
+    const int w = h.xl + h.xh;
+    const int midrows = h.ny - h.yl - h.yh;
+    if (r2 < midrows * w) {
+      const int yy = r2 / w;
+      y = h.yl + yy;
+      const int c = r2 - yy * w;
+      x = c < h.xl ? c : h.nx - h.xh + (c - h.xl);
+      return;
+    }
+    const int r3 = r2 - midrows * w;
+    const int yy = r3 / h.nx;
+    y = h.ny - h.yh + yy;
+    x = r3 - yy * h.nx;
+    return;
+  }
+  const int s3 = s2 - mid * h.partial;
+  const int zz = s3 / h.full;
+  z = h.nz - h.zh + zz;
+  const int r = s3 - zz * h.full;
+  y = r / h.nx;
+  x = r - y * h.nx;
+}
 
 __device__ __forceinline__ void bulk_prefetch_l2(const void *p, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
@@ -980,8 +1038,10 @@ __global__ void __launch_bounds__(128, TLM_PML_MIN_BLOCKS) tlm_pml_kernel(const 
       const long long tiles = ((long long)cnt + 31) / 32;  // s0 is a multiple of 128
       const char *a = reinterpret_cast<const char *>(m.pml_state + pml_sidx(0, s0));
       bulk_prefetch_l2(a, (uint32_t)(tiles * 24 * 32 * sizeof(typename PmlTypes<T>::state)));
-      const char *pa = reinterpret_cast<const char *>(reinterpret_cast<uintptr_t>(pl.pos + s0) & ~(uintptr_t)15);
-      bulk_prefetch_l2(pa, (uint32_t)((cnt * 8 + 15) & ~15) + 16);
+      if (!pl.sh.on) {
+        const char *pa = reinterpret_cast<const char *>(reinterpret_cast<uintptr_t>(pl.pos + s0) & ~(uintptr_t)15);
+        bulk_prefetch_l2(pa, (uint32_t)((cnt * 8 + 15) & ~15) + 16);
+      }
     }
   }
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -995,14 +1055,27 @@ __device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl,
   const T *__restrict__ in = (t & 1) ? m.links0 : m.links1;
   T *__restrict__ out = (t & 1) ? m.links1 : m.links0;
   const long long P = m.plane;
-  const unsigned long long pk = __ldcs(pl.pos + s);
-  const int x = (int)(pk & 0x1fffffull), y = (int)((pk >> 21) & 0x1fffffull), z = (int)((pk >> 42) & 0x1fffffull);
+  int x, y, z, out_no = -1;
+  if (pl.sh.on) {
+    pml_shell_pos(pl.sh, s, x, y, z);
+    if (pl.n_out_map) {  // binary search of the sorted output map
+      int lo = 0, hi = pl.n_out_map - 1;
+      while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int2 e = pl.out_map[mid];
+        if (e.x == s) { out_no = e.y; break; }
+        if (e.x < s) lo = mid + 1; else hi = mid - 1;
+      }
+    }
+  } else {
+    const unsigned long long pk = __ldcs(pl.pos + s);
+    x = (int)(pk & 0x1fffffull); y = (int)((pk >> 21) & 0x1fffffull); z = (int)((pk >> 42) & 0x1fffffull);
+    if (pk >> 63)
+      for (int k = 0; k < pl.n_out_map; k++)
+        if (pl.out_map[k].x == s) out_no = pl.out_map[k].y;
+  }
   const int par = __ldcs(pl.par + s);
   if (par == kPmlMaterialSlot) return;  // PML cell in a material: tlm_pml_material_kernel
-  int out_no = -1;
-  if (pk >> 63)
-    for (int k = 0; k < pl.n_out_map; k++)
-      if (pl.out_map[k].x == s) out_no = pl.out_map[k].y;
   const long long idx = (long long)(z + 1) * m.PxPy + (long long)(y + 1) * m.Px + x;
   const long long dy = m.Px, dz = m.PxPy;
   T ci[12], co[12];
