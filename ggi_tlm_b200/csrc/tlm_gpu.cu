@@ -1173,6 +1173,21 @@ int tlm_gpu_set_materials(int64_t h, int32_t n, const int32_t *type, const int32
     }
     if (d.type == 3 && ((d.eps_exists && d.eps_b[0] == 0.0) || (d.mu_exists && d.mu_b[0] == 0.0)))
       return fail(TLM_E_BADARG, "volume material %d: filter b(0) is zero", i + 1);
+    // reciprocals of the constant divisors of special_cell, each divisor
+    // formed exactly as the cell update forms it
+    {
+      const double Y04 = tlm::kY0 * 4.0, Z04 = tlm::kZ0 * 4.0;
+      d.inv_eps_b0 = d.eps_b[0] != 0.0 ? 1.0 / d.eps_b[0] : 0.0;
+      d.inv_mu_b0 = d.mu_b[0] != 0.0 ? 1.0 / d.mu_b[0] : 0.0;
+      double Y = Y04;
+      d.inv_Y_eps = 1.0 / (Y + (d.eps_exists ? d.Ys_eps_f : 0.0));
+      if (d.eps_exists) Y = Y + d.Ys_eps_f;
+      d.inv_Y_Ge = 1.0 / (Y + d.Ge);
+      double Z = Z04;
+      if (d.mu_exists) Z = Z + d.Zs_mu_f;
+      Z = Z + d.Rm;
+      d.inv_Z = 1.0 / Z;
+    }
   }
   return TLM_OK;
 }

@@ -65,6 +65,11 @@ constexpr int kPmlState = 24;  // Ix,Iy,Iz, Vi(12), Vxt,Vyt,Vzt, Vxyt,Vyxt,Vzxt,
 struct MatDev {
   int type, eps_exists, mu_exists, eps_order, mu_order, pad0, pad1, pad2;
   double Ys_eps_f, Zs_mu_f, Ge, Rm;
+  // reciprocals of the material's constant divisors (the Thevenin sums and
+  // the filters' b(0)), so the per-cell update multiplies instead of running
+  // IEEE FP64 divisions; the reference's build (-funsafe-math-optimizations)
+  // licenses the same rewrite
+  double inv_eps_b0, inv_mu_b0, inv_Y_eps, inv_Y_Ge, inv_Z;
   double eps_a[kMaxOrder + 1], eps_b[kMaxOrder + 1], mu_a[kMaxOrder + 1], mu_b[kMaxOrder + 1];
 };
 
@@ -299,13 +304,13 @@ __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par,
 // MAXO is a compile-time bound on the order: the loops unroll with the
 // runtime order as a predicate, so the taps stay in registers.
 template <int MAXO>
-__device__ __forceinline__ double zfilter_eval(const double *a, const double *b, int order, const double *w, double G,
-                                               double &w0) {
+__device__ __forceinline__ double zfilter_eval(const double *a, const double *b, double inv_b0, int order,
+                                               const double *w, double G, double &w0) {
   double W0 = G;
 #pragma unroll
   for (int i = 1; i <= MAXO; i++)
     if (i <= order) W0 = W0 - b[i] * w[i];
-  W0 = W0 / b[0];
+  W0 = W0 * inv_b0;
   w0 = W0;
   double F0 = 0.0;
   F0 = F0 + a[0] * W0;
@@ -366,22 +371,24 @@ __device__ __forceinline__ void special_cell(const MeshDev<T> &m, int s, int4 re
     if (M->eps_exists) {
       Ys = M->Ys_eps_f;
       const int o = M->eps_order;
-      for (int c = 0; c < 3; c++) Vo[c] = zfilter_eval<MAXO>(M->eps_a, M->eps_b, o, we[c], 0.0, we[c][0]);
+      for (int c = 0; c < 3; c++) Vo[c] = zfilter_eval<MAXO>(M->eps_a, M->eps_b, M->inv_eps_b0, o, we[c], 0.0, we[c][0]);
       double V1, Y1;
-      V1 = (VEx * Yx + Vo[0] * Ys) / (Yx + Ys); Y1 = Yx + Ys; VEx = V1; Yx = Y1;
-      V1 = (VEy * Yy + Vo[1] * Ys) / (Yy + Ys); Y1 = Yy + Ys; VEy = V1; Yy = Y1;
-      V1 = (VEz * Yz + Vo[2] * Ys) / (Yz + Ys); Y1 = Yz + Ys; VEz = V1; Yz = Y1;
+      const double iY = M->inv_Y_eps;  // 1 / (Y04 + Ys)
+      V1 = (VEx * Yx + Vo[0] * Ys) * iY; Y1 = Yx + Ys; VEx = V1; Yx = Y1;
+      V1 = (VEy * Yy + Vo[1] * Ys) * iY; Y1 = Yy + Ys; VEy = V1; Yy = Y1;
+      V1 = (VEz * Yz + Vo[2] * Ys) * iY; Y1 = Yz + Ys; VEz = V1; Yz = Y1;
     }
     const double Ge = M->Ge;
     double V1, Y1;
-    V1 = (VEx * Yx + 0.0 * Ge) / (Yx + Ge); Y1 = Yx + Ge; VEx = V1; Yx = Y1;
-    V1 = (VEy * Yy + 0.0 * Ge) / (Yy + Ge); Y1 = Yy + Ge; VEy = V1; Yy = Y1;
-    V1 = (VEz * Yz + 0.0 * Ge) / (Yz + Ge); Y1 = Yz + Ge; VEz = V1; Yz = Y1;
+    const double iG = M->inv_Y_Ge;  // 1 / (Y + Ge)
+    V1 = (VEx * Yx + 0.0 * Ge) * iG; Y1 = Yx + Ge; VEx = V1; Yx = Y1;
+    V1 = (VEy * Yy + 0.0 * Ge) * iG; Y1 = Yy + Ge; VEy = V1; Yy = Y1;
+    V1 = (VEz * Yz + 0.0 * Ge) * iG; Y1 = Yz + Ge; VEz = V1; Yz = Y1;
     if (M->mu_exists) {
       const double Zs = M->Zs_mu_f;
       const int o = M->mu_order;
       double Vs[3];
-      for (int c = 0; c < 3; c++) Vs[c] = zfilter_eval<MAXO>(M->mu_a, M->mu_b, o, wm[c], 0.0, wm[c][0]);
+      for (int c = 0; c < 3; c++) Vs[c] = zfilter_eval<MAXO>(M->mu_a, M->mu_b, M->inv_mu_b0, o, wm[c], 0.0, wm[c][0]);
       VHx = VHx + Vs[0]; Zx = Zx + Zs;
       VHy = VHy + Vs[1]; Zy = Zy + Zs;
       VHz = VHz + Vs[2]; Zz = Zz + Zs;
@@ -392,7 +399,13 @@ __device__ __forceinline__ void special_cell(const MeshDev<T> &m, int s, int4 re
     VHz = VHz + 0.0; Zz = Zz + Rm;
   }
   double Vx = VEx, Vy = VEy, Vz = VEz;
-  double Ix = VHx / Zx, Iy = VHy / Zy, Iz = VHz / Zz;
+  double Ix, Iy, Iz;
+  if (type == 3) {  // Zx = Zy = Zz, a material constant
+    const double iZ = M->inv_Z;
+    Ix = VHx * iZ; Iy = VHy * iZ; Iz = VHz * iZ;
+  } else {
+    Ix = VHx / Zx; Iy = VHy / Zy; Iz = VHz / Zz;
+  }
   if (flags & SP_EXC) {
     // scatter.F90:429-450
     const int e = rec.z;
@@ -420,7 +433,7 @@ __device__ __forceinline__ void special_cell(const MeshDev<T> &m, int s, int4 re
       const int o = M->eps_order;
       const double Io[3] = {(Vx - Vo[0]) * Ys, (Vy - Vo[1]) * Ys, (Vz - Vo[2]) * Ys};
       for (int c = 0; c < 3; c++) {
-        zfilter_eval<MAXO>(M->eps_a, M->eps_b, o, we[c], Io[c], we[c][0]);
+        zfilter_eval<MAXO>(M->eps_a, M->eps_b, M->inv_eps_b0, o, we[c], Io[c], we[c][0]);
 #pragma unroll
         for (int k = 0; k < MAXO; k++)
           if (k < o) m.filt[(size_t)(c * m.filt_eo + k) * m.n_filt + fidx] = we[c][k];
@@ -430,7 +443,7 @@ __device__ __forceinline__ void special_cell(const MeshDev<T> &m, int s, int4 re
       const int o = M->mu_order;
       const double G[3] = {-Ix, -Iy, -Iz};
       for (int c = 0; c < 3; c++) {
-        zfilter_eval<MAXO>(M->mu_a, M->mu_b, o, wm[c], G[c], wm[c][0]);
+        zfilter_eval<MAXO>(M->mu_a, M->mu_b, M->inv_mu_b0, o, wm[c], G[c], wm[c][0]);
 #pragma unroll
         for (int k = 0; k < MAXO; k++)
           if (k < o) m.filt[(size_t)(3 * m.filt_eo + c * m.filt_mo + k) * m.n_filt + fidx] = wm[c][k];
