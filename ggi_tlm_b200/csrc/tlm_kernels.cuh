@@ -228,9 +228,11 @@ __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par,
   const A Vx = (V[Vynx] + V[Vypx] + V[Vznx] + V[Vzpx]) / A(2);
   const A Vy = (V[Vxny] + V[Vxpy] + V[Vzny] + V[Vzpy]) / A(2);
   const A Vz = (V[Vxnz] + V[Vxpz] + V[Vynz] + V[Vypz]) / A(2);
-  const A Ix = (V[Vypz] - V[Vzpy] - V[Vynz] + V[Vzny]) / (A(2) * Z0);
-  const A Iy = (V[Vzpx] - V[Vxpz] - V[Vznx] + V[Vxnz]) / (A(2) * Z0);
-  const A Iz = (V[Vxpy] - V[Vypx] - V[Vxny] + V[Vynx]) / (A(2) * Z0);
+  // 1/(2 Z0) is a compile-time constant: a multiply, not an FP64 division
+  const A inv2Z0 = A(1) / (A(2) * Z0);
+  const A Ix = (V[Vypz] - V[Vzpy] - V[Vynz] + V[Vzny]) * inv2Z0;
+  const A Iy = (V[Vzpx] - V[Vxpz] - V[Vznx] + V[Vxnz]) * inv2Z0;
+  const A Iz = (V[Vxpy] - V[Vypx] - V[Vxny] + V[Vynx]) * inv2Z0;
   // STAGE 5
   const A Vx_sh = ax * (-(last_Vi[Vznx] + last_Vi[Vzpx] + last_Vi[Vynx] + last_Vi[Vypx]) / A(2) +
                         Csy * ((V[Vznx] + V[Vzpx]) + (last_Vi[Vznx] + last_Vi[Vzpx])) +
