@@ -345,6 +345,7 @@ def bench_serving(device, n_requests=32):
     srv = serving.Server(engine=serving.GpuEngine(device=device, variant=1), budget_bytes=150e9, max_slots=64,
                          quantum=64)
     res = srv.serve(trace)
+    srv.engine.close()
     ours = serving.summarize(res)
     base_res = serving.sequential_fp64(trace, device=device)
     base = serving.summarize(base_res)

@@ -40,6 +40,7 @@ EXPORTS = [
     "tlm_gpu_set_small_to_zero", "tlm_gpu_set_pml_sigma", "tlm_gpu_set_face_excitation",
     "tlm_gpu_set_face_outputs", "tlm_gpu_fetch_face_output", "tlm_gpu_set_outer_huygens",
     "tlm_gpu_set_far_field", "tlm_gpu_fetch_far_field", "tlm_gpu_pool_release", "tlm_gpu_pool_cached_bytes",
+    "tlm_gpu_prepare",
 ]
 
 
@@ -83,6 +84,7 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_far_field": [i64, i32, _f64p, _i32p, _i32p, _i32p],
         "tlm_gpu_fetch_far_field": [i64, _f64p],
         "tlm_gpu_pool_release": [],
+        "tlm_gpu_prepare": [i64],
         "tlm_gpu_pool_cached_bytes": [C.POINTER(i64)],
         "tlm_gpu_fetch_face_output": [i64, i32, i32, _f64p],
         "tlm_gpu_set_excitation": [i64, i32, i32, _f64p, _f64p, i32, _i32p, _i32p, _i32p, _i32p, i32],
@@ -236,6 +238,10 @@ class GpuMesh:
             _check(lib.tlm_gpu_set_small_to_zero(self.h, int(t["n_small_to_zero"]), float(t["small_to_zero_value"])))
 
     # -- time stepping -----------------------------------------------------
+    def prepare(self):
+        """Build the device state now rather than at the first run."""
+        _check(_lib.tlm_gpu_prepare(self.h))
+
     def run(self, n_steps: int, sync: bool = True):
         _check(_lib.tlm_gpu_run(self.h, self.step + 1, n_steps))
         self.step += n_steps

@@ -49,9 +49,12 @@ int fail(int code, const char *fmt, ...) {
 // batch lists are kept per device and handed out again to later allocations
 // of a similar size, so a serving loop that creates and destroys meshes all
 // the time stops paying for cudaMalloc/cudaFree (a single cudaFree of a
-// large buffer took up to 0.6 s on B200).  A released block may still be read
-// by kernels in flight, so the first reuse after any release synchronises
-// the device first (cudaFree synchronised implicitly too).  The cache holds
+// large buffer took up to 0.6 s on B200).  Blocks of destroyed meshes and
+// batches are released after their streams were synchronised and can be
+// reused at once.  A buffer replaced while work may still be in flight (a
+// batch's lists rebuilt between graph launches) may still be read, so the
+// first reuse after such a release synchronises the device first, as
+// cudaFree would have.  The cache holds
 // at most TLM_POOL_CACHE_BYTES (default 16 GiB) per device; beyond that, and
 // on tlm_gpu_pool_release, blocks go back to the driver.
 // ---------------------------------------------------------------------------
@@ -109,7 +112,8 @@ cudaError_t alloc(size_t bytes, void **p, size_t *cap) {
   return e;
 }
 
-void release(int dev, void *p, size_t cap) {
+// idle: no kernel can still use the block (its streams were synchronised)
+void release(int dev, void *p, size_t cap, bool idle) {
   if (!p) return;
   std::lock_guard<std::mutex> lk(mu);
   if (cached[dev] + cap > cache_limit()) {
@@ -122,7 +126,7 @@ void release(int dev, void *p, size_t cap) {
   }
   blocks[dev].emplace(cap, p);
   cached[dev] += cap;
-  released_since_sync[dev] = true;
+  if (!idle) released_since_sync[dev] = true;
 }
 
 void release_all() {
@@ -151,13 +155,14 @@ struct DevBuf {
   size_t bytes = 0;  // requested
   size_t cap = 0;    // capacity of the cached block
   int dev = 0;
-  ~DevBuf() { pool::release(dev, p, cap); }
+  // owners synchronise their streams before they are destroyed
+  ~DevBuf() { pool::release(dev, p, cap, true); }
 };
 
 // Allocate `bytes` into b from the device cache (the current device).
 cudaError_t buf_alloc(DevBuf &b, size_t bytes) {
   if (b.p) {
-    pool::release(b.dev, b.p, b.cap);
+    pool::release(b.dev, b.p, b.cap, false);  // may still be read by work in flight
     b.p = nullptr;
   }
   b.bytes = bytes;
@@ -1623,7 +1628,14 @@ int tlm_gpu_destroy(int64_t h) {
     g_meshes.erase(it);
   }
   if (m->stream) cudaStreamSynchronize(m->stream);
+  if (m->batch_stream) cudaStreamSynchronize(m->batch_stream);
   return TLM_OK;
+}
+
+int tlm_gpu_prepare(int64_t h) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  return finalize(m);
 }
 
 int tlm_gpu_pool_release(void) {

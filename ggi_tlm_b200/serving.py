@@ -77,7 +77,13 @@ def footprint_bytes(t: dict, precision: int = capi.TLM_PRECISION_FP32) -> int:
 
 
 class GpuEngine:
-    """Default engine: solves are GpuMesh objects advanced in a GpuBatch."""
+    """Default engine: solves are GpuMesh objects advanced in a GpuBatch.
+
+    A quantum runs asynchronously: ``advance`` starts it and returns, and
+    ``wait`` blocks until it has finished.  Requests admitted meanwhile get
+    their device state built at once (``GpuMesh.prepare``), overlapping the
+    running quantum; the batch is rebuilt with them, and without retired
+    solves, when the next quantum starts."""
 
     def __init__(self, precision: int = capi.TLM_PRECISION_FP32, device: int = 0, variant: Optional[int] = None):
         self.precision = precision
@@ -85,28 +91,46 @@ class GpuEngine:
         self.variant = variant
         self.meshes: Dict[int, capi.GpuMesh] = {}
         self.batch: Optional[capi.GpuBatch] = None
+        self.retired: List[capi.GpuMesh] = []
+        self.dirty = False
+        self.running = False
 
     def add(self, rid: int, tables: dict):
-        self._drop_batch()
-        self.meshes[rid] = capi.GpuMesh(tables, precision=self.precision, device=self.device)
+        g = capi.GpuMesh(tables, precision=self.precision, device=self.device)
+        g.prepare()
+        self.meshes[rid] = g
+        self.dirty = True
 
     def remove(self, rid: int):
-        self._drop_batch()
-        self.meshes.pop(rid).close()
+        self.retired.append(self.meshes.pop(rid))  # closed once the batch that holds it is gone
+        self.dirty = True
 
     def _drop_batch(self):
         if self.batch is not None:
             self.batch.close()
             self.batch = None
 
+    def wait(self):
+        if self.running:
+            self.batch.synchronize()
+            self.running = False
+
     def advance(self, n_steps: int):
+        self.wait()
+        if self.dirty:
+            self._drop_batch()
+            for g in self.retired:
+                g.close()
+            self.retired.clear()
+            self.dirty = False
         if not self.meshes:
             return
         if self.batch is None:
             self.batch = capi.GpuBatch(list(self.meshes.values()))
             if self.variant is not None:
                 self.batch.set_variant(self.variant)
-        self.batch.run(n_steps, sync=True)
+        self.batch.run(n_steps, sync=False)
+        self.running = True
 
     def progress(self, rid: int) -> int:
         return self.meshes[rid].step
@@ -116,10 +140,12 @@ class GpuEngine:
         return probe_series(g.t, g.cell_output()), g.dft()
 
     def close(self):
+        self.wait()
         self._drop_batch()
-        for g in self.meshes.values():
+        for g in list(self.meshes.values()) + self.retired:
             g.close()
         self.meshes.clear()
+        self.retired.clear()
 
 
 class Server:
@@ -171,7 +197,13 @@ class Server:
                     if delay > 0:
                         time.sleep(min(delay, 0.05))
                 continue
-            self.engine.advance(self.quantum)
+            # the quantum in flight (if any) ends; retire what finished, then
+            # start the next quantum, during which the next admissions happen
+            wait = getattr(self.engine, "wait", None)
+            if wait is not None:
+                wait()
+            else:
+                self.engine.advance(self.quantum)
             for rid in list(active):
                 r, adm, need = active[rid]
                 if self.engine.progress(rid) >= r.tables["n_timesteps"]:
@@ -184,6 +216,8 @@ class Server:
                     del active[rid]
                     used -= need
                     self.events.append((fin, "finish", rid, used))
+            if wait is not None and active:
+                self.engine.advance(self.quantum)  # asynchronous
         return sorted(done, key=lambda x: x.rid)
 
 

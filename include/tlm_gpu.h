@@ -195,6 +195,12 @@ int tlm_gpu_set_far_field(int64_t handle, int32_t n_surfaces, const double *freq
    Jz, Mx, My, Mz as (re, im) pairs, 12 doubles per face. */
 int tlm_gpu_fetch_far_field(int64_t handle, double *out);
 
+/* Build the handle's device state now (allocations, table uploads, masks)
+   instead of at its first run; a serving loop calls it for a new request
+   while other solves are running.  No counterpart in the reference, which
+   sets up once before run_TLM. */
+int tlm_gpu_prepare(int64_t handle);
+
 /* Advance timesteps first_step..first_step+n_steps-1 (1-based, run_TLM
    numbering, SRC/TLM_SOLVER/run_TLM.F90:191-295).  Steps must be
    contiguous across calls.  Asynchronous on the library stream. */

@@ -96,6 +96,7 @@ def test_results_same_alone_and_in_the_mix(gpu_lib):
     trace = [serving.Request(i, 0.002 * i, t) for i, t in enumerate(tabs)]
     srv = serving.Server(engine=serving.GpuEngine(variant=1), max_slots=3, quantum=16)
     mixed = srv.serve(trace)
+    srv.engine.close()
     assert srv.peak_slots == 3
     for r, t in zip(mixed, tabs):
         with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP32) as g:
