@@ -267,17 +267,20 @@ def _timed_steps(g, k):
 def bench_target_512(device, peak):
     """The roofline target: 512^3 PML-bounded free-space mesh, point source."""
     from ggi_tlm_b200 import autotune, capi
-    from ggi_tlm_b200.problem import build_tables
+    from ggi_tlm_b200.problem import build_tables, probe_series
 
-    t = build_tables(__import__("ggi_tlm_b200.cases", fromlist=["x"]).pml_point_source(512, steps=400))
+    t = build_tables(__import__("ggi_tlm_b200.cases", fromlist=["x"]).pml_point_source(512, steps=2000))
     n = t["nx"] * t["ny"] * t["nz"]
     out = {"workload": "pml_point_source_512^3_pml8", "cells": n, "pml_cells": int(t["n_pml_cells"])}
+    probes = {}
     for prec, esz, key in ((capi.TLM_PRECISION_FP32, 4, "fp32"), (capi.TLM_PRECISION_FP64, 8, "fp64")):
         g = capi.GpuMesh(t, precision=prec, device=device)
         tv = autotune.tune(g, steps_per_variant=2, use_cache=False)
         g.run(3)
         K = 60
         total, bulk = _timed_steps(g, K)
+        g.run(t["n_timesteps"] - g.step)  # untimed: the rest of the solve, for the probe accuracy
+        probes[key] = probe_series(t, g.cell_output())
         g.close()
         ab = algorithmic_bytes(t, esz)
         step_gbs = ab["total"] / (total / K / 1e3) / 1e9
@@ -287,6 +290,11 @@ def bench_target_512(device, peak):
                     "bulk_kernel_gbs": ab["bulk"] / (bulk / K / 1e3) / 1e9,
                     "bulk_kernel_frac_of_measured_hbm": ab["bulk"] / (bulk / K / 1e3) / 1e9 / peak,
                     "variant": tv["variant"], "timed_steps": K}
+    a, b = probes["fp32"], probes["fp64"]
+    errs = [float(np.linalg.norm(a[i] - b[i]) / np.linalg.norm(b[i])) for i in range(len(b)) if np.linalg.norm(b[i]) > 0]
+    out["probe_rel_l2_fp32_vs_fp64_max"] = max(errs)
+    out["probe_rel_l2_fp32_vs_fp64_median"] = float(np.median(errs))
+    out["probe_steps"] = int(t["n_timesteps"])
     return out
 
 
