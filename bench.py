@@ -101,12 +101,12 @@ def cell_counts(t):
 
 def algorithmic_bytes(t, esz):
     """Bytes per step that the fused single-pass algorithm must move:
-    12 link reads + 12 link writes per cell, +24 PML state values read and
+    12 link reads + 12 link writes per cell, +18 PML state values read and
     written per PML cell, +3 filter taps (FP64) read and written per filter
     order per dispersive cell, +16 B per DFT accumulator."""
     n, npml, nmat, taps = cell_counts(t)
     links = n * 24 * esz
-    pml = npml * 48 * esz
+    pml = npml * 36 * esz
     filt = taps * 3 * 16
     dft = int(t["dft_face_ptr"][-1]) * 16 if int(t["n_dft"]) else 0
     return dict(total=links + pml + filt + dft, bulk=(n - npml - nmat) * 24 * esz,

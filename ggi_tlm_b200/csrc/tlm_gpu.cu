@@ -172,6 +172,51 @@ cudaError_t buf_alloc(DevBuf &b, size_t bytes) {
   return e;
 }
 
+// A second stream for the cell kernels that run beside the bulk kernel in a
+// step.  The bulk, PML, PML-material and special-cell kernels all read the
+// step-t links and write disjoint cells of step t+1, so the side kernels
+// take the SM slots the persistent bulk kernel leaves free and its SMs as
+// its CTAs retire, instead of waiting for its last wave.  The face kernel,
+// which reads what all of them wrote, runs after the join.
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  int init() {
+    if (s) return TLM_OK;
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    return TLM_OK;
+  }
+  int begin(cudaStream_t main) {
+    CK(cudaEventRecord(fork, main));
+    CK(cudaStreamWaitEvent(s, fork, 0));
+    return TLM_OK;
+  }
+  int end(cudaStream_t main) {
+    CK(cudaEventRecord(join, s));
+    CK(cudaStreamWaitEvent(main, join, 0));
+    return TLM_OK;
+  }
+  ~SideStream() {
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
+// Whether a mesh of n_cells runs its side kernels on the side stream.
+// Measured on B200: it pays where the bulk kernel has few tiles per CTA
+// (96^3 PML box -8 % per step, batches of serving meshes -1.4 %) and costs
+// on large meshes, where the side kernels slow the bulk kernel down
+// (256^3 +3 %, 512^3 +2 %).  TLM_SIDE_STREAM=0 / 1 forces it off / on.
+bool side_stream_enabled(long long n_cells, bool batch) {
+  const char *e = getenv("TLM_SIDE_STREAM");
+  if (e && e[0] == '0') return false;
+  if (e && e[0] == '1') return true;
+  return batch || n_cells <= 4LL * 1024 * 1024;
+}
+
 struct Mesh {
   tlm_gpu_mesh_desc desc{};
   int Px = 0, Py = 0, Pz = 0;
@@ -248,6 +293,8 @@ struct Mesh {
   int small_every = 0;       // set_small_to_zero: period in steps (0 = off)
   double small_value = 0.0;
   int pml_prefetch = 1200;  // blocks ahead for the PML state L2 prefetch (0 = off)
+  SideStream side;          // PML / PML-material / special kernels beside the bulk kernel
+  bool side_on = false;
 
   // graph of kGraphSteps steps
   static constexpr int kGraphSteps = 8;
@@ -524,8 +571,10 @@ int finalize(Mesh *m) {
           if (pidx != (int)pml_pos.size())
             return fail(TLM_E_BADARG, "PML cell numbers must follow (cz,cy,cx) traversal order (cell %lld)", cell + 1);
           const int par = m->pml_cell_param[pidx];
-          if (par < 1 || par > m->n_pml_params || par > 65535)
+          if (par < 1 || par > m->n_pml_params)
             return fail(TLM_E_BADARG, "PML cell %d: parameter %d out of range", pidx + 1, par);
+          if (par > tlm::kPmlOutputFlag - 1)  // bit 15 of the packed index is the output flag
+            return fail(TLM_E_UNSUPPORTED, "more than %d PML parameter rows", tlm::kPmlOutputFlag - 1);
           unsigned long long pk = (unsigned long long)x | ((unsigned long long)y << 21) | ((unsigned long long)z << 42);
           if (mat) {  // PML cell in a volume material: own list, own kernel
             pmm_pos.push_back(int4{x, y, z, m->sp_out[s] ? out_no++ : -1});
@@ -534,12 +583,14 @@ int finalize(Mesh *m) {
             pml_par.push_back(tlm::kPmlMaterialSlot);
             continue;
           }
+          int pw = par - 1;
           if (m->sp_out[s]) {
             pk |= 1ull << 63;
             pml_out.push_back(int2{pidx, out_no++});
+            pw |= tlm::kPmlOutputFlag;
           }
           pml_pos.push_back(pk);
-          pml_par.push_back((uint16_t)(par - 1));
+          pml_par.push_back((uint16_t)pw);
           continue;
         } else {
           if (mat) {
@@ -593,6 +644,7 @@ int finalize(Mesh *m) {
   {
     int rc2;
     pml_pos.resize(pml_pos.size() + 8, 0ull);  // 64 bytes of padding for the widened L2 prefetch
+    pml_par.resize(pml_par.size() + 128, 0);    // 256 bytes of padding for the index L2 prefetch
     if ((rc2 = upload(m, m->pml_pos, pml_pos)) || (rc2 = upload(m, m->pml_par16, pml_par)) ||
         (rc2 = upload(m, m->pml_outmap, pml_out)))
       return rc2;
@@ -836,6 +888,11 @@ int finalize(Mesh *m) {
   CK(cudaEventCreate(&m->ev0));
   CK(cudaEventCreate(&m->ev1));
   if (const char *pf = getenv("TLM_PML_PREFETCH_BLOCKS")) m->pml_prefetch = atoi(pf);
+  m->side_on = side_stream_enabled((long long)m->desc.nx * m->desc.ny * m->desc.nz, false);
+  if (m->side_on) {
+    int rc = m->side.init();
+    if (rc) return rc;
+  }
   m->finalized = true;
   return TLM_OK;
 }
@@ -992,26 +1049,32 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
       tlm::tlm_flush_small_kernel<T><<<4 * m->n_sms, 256, 0, m->stream>>>(md, k, m->small_every, m->small_value);
       m->last_launches++;
     }
+    // timed runs keep one stream, so the events around the bulk kernel time it alone
+    const bool side = m->side_on && !kev && (m->n_pml_list || m->n_pmm || m->n_sp_dev);
+    int rc;
+    if (side && (rc = m->side.begin(m->stream))) return rc;
     if (kev) cudaEventRecord(kev[2 * k], m->stream);
-    int rc = launch_bulk<T, VEC>(m, md, k);
+    rc = launch_bulk<T, VEC>(m, md, k);
     if (rc) return rc;
     if (kev) cudaEventRecord(kev[2 * k + 1], m->stream);
     m->last_launches++;
+    const cudaStream_t ss = side ? m->side.s : m->stream;
     if (m->n_pml_list) {
       tlm::PmlList pl{(const unsigned long long *)m->pml_pos.p, (const uint16_t *)m->pml_par16.p,
                       (const int2 *)m->pml_outmap.p, m->n_pml_list, m->n_pml_out, m->pml_shell};
-      tlm::tlm_pml_kernel<T><<<(m->n_pml_list + 127) / 128, 128, 0, m->stream>>>(md, pl, k, m->pml_prefetch);
+      tlm::tlm_pml_kernel<T><<<(m->n_pml_list + 127) / 128, 128, 0, ss>>>(md, pl, k, m->pml_prefetch);
       m->last_launches++;
     }
     if (m->n_pmm) {
-      tlm::tlm_pml_material_kernel<T><<<(m->n_pmm + 127) / 128, 128, 0, m->stream>>>(md, pmm_list(m), k);
+      tlm::tlm_pml_material_kernel<T><<<(m->n_pmm + 127) / 128, 128, 0, ss>>>(md, pmm_list(m), k);
       m->last_launches++;
     }
     if (m->n_sp_dev) {
-      launch_special<T>(special_order_bound(std::max(m->filt_eo, m->filt_mo)), (m->n_sp_dev + 127) / 128, m->stream,
-                        md, m->n_sp_dev, k);
+      launch_special<T>(special_order_bound(std::max(m->filt_eo, m->filt_mo)), (m->n_sp_dev + 127) / 128, ss, md,
+                        m->n_sp_dev, k);
       m->last_launches++;
     }
+    if (side && (rc = m->side.end(m->stream))) return rc;
     if (fd.n_faces) {
       tlm::tlm_face_kernel<T><<<(fd.n_faces + 127) / 128, 128, 0, m->stream>>>(md, fd, k);
       m->last_launches++;
@@ -1669,6 +1732,8 @@ struct Batch {
   int variant = 1;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  SideStream side;  // PML / PML-material / special kernels beside the bulk kernel
+  bool side_on = false;
   cudaGraphExec_t graph = nullptr;
   std::vector<int> active;  // indices into handles of the current segment
   DevBuf meshes_d, pml_d, faces_d, dfts_d, nsp_d, tiles_d, pmlb_d, spb_d, faceb_d, dftb_d, dbases_d, err_d;
@@ -1779,6 +1844,13 @@ int batch_step(Batch *b, bool dry) {
       }
     }
   }
+  bool pmm_any = false;
+  for (int i : b->active) {
+    Mesh *m = get(b->handles[i]);
+    if (m && m->n_pmm) pmm_any = true;
+  }
+  const bool side = !dry && b->side_on && (b->n_pmlb || b->n_spb || pmm_any);
+  if (side && (rc = b->side.begin(b->stream))) return rc;
   if constexpr (sizeof(T) == 4) {
     switch (b->variant) {
       case 1: rc = launch_batch_tma<T, VEC, 1024, 2>(b, dry); break;
@@ -1813,11 +1885,12 @@ int batch_step(Batch *b, bool dry) {
   bd.n_dft_blocks = b->n_dftb;
   bd.d_bases = (int *const *)b->dbases_d.p;
   bd.n_active = (int)b->active.size();
-  if (b->n_pmlb) { tlm::tlm_pml_batch_kernel<T><<<b->n_pmlb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
+  const cudaStream_t ss = side ? b->side.s : b->stream;
+  if (b->n_pmlb) { tlm::tlm_pml_batch_kernel<T><<<b->n_pmlb, 128, 0, ss>>>(bd, 0); b->last_launches++; }
   for (int i : b->active) {  // PML cells inside materials of the members that have them
     Mesh *m = get(b->handles[i]);
     if (m && m->n_pmm) {
-      tlm::tlm_pml_material_kernel<T><<<(m->n_pmm + 127) / 128, 128, 0, b->stream>>>(mesh_dev<T>(m), pmm_list(m), 0);
+      tlm::tlm_pml_material_kernel<T><<<(m->n_pmm + 127) / 128, 128, 0, ss>>>(mesh_dev<T>(m), pmm_list(m), 0);
       b->last_launches++;
     }
   }
@@ -1828,14 +1901,15 @@ int batch_step(Batch *b, bool dry) {
       if (m) maxo = std::max(maxo, std::max(m->filt_eo, m->filt_mo));
     }
     switch (special_order_bound(maxo)) {
-      case 1: tlm::tlm_special_batch_kernel<T, 1><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
-      case 2: tlm::tlm_special_batch_kernel<T, 2><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
-      case 3: tlm::tlm_special_batch_kernel<T, 3><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
-      case 4: tlm::tlm_special_batch_kernel<T, 4><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
-      default: tlm::tlm_special_batch_kernel<T, tlm::kMaxOrder><<<b->n_spb, 128, 0, b->stream>>>(bd, 0); break;
+      case 1: tlm::tlm_special_batch_kernel<T, 1><<<b->n_spb, 128, 0, ss>>>(bd, 0); break;
+      case 2: tlm::tlm_special_batch_kernel<T, 2><<<b->n_spb, 128, 0, ss>>>(bd, 0); break;
+      case 3: tlm::tlm_special_batch_kernel<T, 3><<<b->n_spb, 128, 0, ss>>>(bd, 0); break;
+      case 4: tlm::tlm_special_batch_kernel<T, 4><<<b->n_spb, 128, 0, ss>>>(bd, 0); break;
+      default: tlm::tlm_special_batch_kernel<T, tlm::kMaxOrder><<<b->n_spb, 128, 0, ss>>>(bd, 0); break;
     }
     b->last_launches++;
   }
+  if (side && (rc = b->side.end(b->stream))) return rc;
   if (b->n_faceb) { tlm::tlm_face_batch_kernel<T><<<b->n_faceb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
   for (int i : b->active) {  // outer-boundary Huygens surfaces of the members that have them
     Mesh *m = get(b->handles[i]);
@@ -1901,6 +1975,11 @@ int tlm_gpu_batch_create(const int64_t *handles, int32_t n, int64_t *batch) {
   CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
   CK(cudaEventCreate(&b->ev0));
   CK(cudaEventCreate(&b->ev1));
+  b->side_on = side_stream_enabled(0, true);
+  if (b->side_on) {
+    int rc = b->side.init();
+    if (rc) return rc;
+  }
   {
     std::vector<int> zero(1, 0);
     int rc = bupload(b.get(), b->err_d, zero);

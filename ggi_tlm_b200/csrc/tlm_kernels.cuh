@@ -48,13 +48,21 @@ enum PmlPort {
 enum SpecialFlags : int { SP_MAT = 2, SP_EXC = 4, SP_OUT = 8 };
 
 constexpr int kMaxOrder = 8;
-// PML state layout: tiles of 32 cells, each holding the 24 values as 24
-// runs of 32 words ([n/32][24][32]), so a warp's state is one contiguous
-// 3 KB (FP32) or 6 KB (FP64) block instead of 24 separate streams.
+// PML state: 18 values per cell.  scatter_PML.F90 keeps 24 (last I x3, the
+// 12 incident pulses, Vxt/Vyt/Vzt, six series voltages), but its STAGE 5
+// reads the 12 pulses only as six sums of opposite-port pairs, so the
+// pairs are stored instead: slots 0-2 last I, 3-8 the pair sums
+// (znx+zpx, ynx+ypx | xny+xpy, zny+zpy | ynz+ypz, xnz+xpz), 9-11 Vt, 12-17
+// the series voltages.  Layout: tiles of 32 cells, each holding the values
+// as runs of 32 words ([n/32][18][32]), so a warp's state is one contiguous
+// 2.25 KB (FP32) or 4.5 KB (FP64) block instead of 18 separate streams.
+constexpr int kPmlState = 18;
 __host__ __device__ __forceinline__ size_t pml_sidx(int k, long long s) {
-  return ((size_t)(s >> 5) * 24 + (size_t)k) * 32 + (size_t)(s & 31);
+  return ((size_t)(s >> 5) * kPmlState + (size_t)k) * 32 + (size_t)(s & 31);
 }
-__host__ __device__ __forceinline__ size_t pml_state_elems(long long n) { return (size_t)((n + 31) / 32) * 24 * 32; }
+__host__ __device__ __forceinline__ size_t pml_state_elems(long long n) {
+  return (size_t)((n + 31) / 32) * kPmlState * 32;
+}
 
 // FP32 path: free-space scatter arithmetic in FP64 on the FP32 links.  A
 // static field (the charge a Gaussian point source leaves) repeats the same
@@ -68,7 +76,8 @@ __host__ __device__ __forceinline__ size_t pml_state_elems(long long n) { return
 // PML-list parameter index of a PML cell inside a volume material (those
 // cells take tlm_pml_material_kernel)
 constexpr uint16_t kPmlMaterialSlot = 0xFFFF;
-constexpr int kPmlState = 24;  // Ix,Iy,Iz, Vi(12), Vxt,Vyt,Vzt, Vxyt,Vyxt,Vzxt,Vxzt,Vyzt,Vzyt
+// Bit 15 of a PML cell's parameter index marks an output cell (rows < 2^15).
+constexpr int kPmlOutputFlag = 0x8000;
 
 // One volume material after calculate_volume_material_filter_coefficients.
 struct MatDev {
@@ -106,7 +115,7 @@ struct MeshDev {
   const uint32_t *seg_base;
   const int4 *sp_rec;
   const int4 *sp_pos;       // (x, y, z) 0-based of each special cell
-  typename PmlTypes<T>::state *pml_state;  // [24][n_pml]
+  typename PmlTypes<T>::state *pml_state;  // [n_pml/32][18][32], pml_sidx
   int n_pml;
   const double *pml_par;    // [n_par][16], FP64 in both precisions
   typename PmlTypes<T>::state *pml_ixt;    // [n_out][3]
@@ -226,7 +235,7 @@ __device__ __forceinline__ void free_space_cell(const T *inc, T *out) {
 // ---------------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par, int out_no, const T *inc_in, T *out,
-                                      double *cell_out_row) {
+                                      double *cell_out_row, const typename PmlTypes<T>::state (&st)[kPmlState]) {
   using A = typename PmlTypes<T>::arith;
   using ST = typename PmlTypes<T>::state;
   // FP64: literal scatter_PML.F90 arithmetic.  FP32: currents (and the
@@ -239,16 +248,17 @@ __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par,
   const A Csx2 = A(P[9]), Csy2 = A(P[10]), Csz2 = A(P[11]);
   const A Csy_sz = A(P[12]), Csz_sx = A(P[13]), Csx_sy = A(P[14]);
   ST *S = m.pml_state;
-  const int n = m.n_pml;
-  const A last_Ix = __ldcs(S + pml_sidx(0, pidx)), last_Iy = __ldcs(S + pml_sidx(1, pidx)), last_Iz = __ldcs(S + pml_sidx(2, pidx));
-  A last_Vi[12];
+  // st: the cell's state as the caller loaded it (slot order of pml_sidx)
+  auto ld = [&](int k) -> A { return A(st[k]); };
+  const A last_Ix = ld(0), last_Iy = ld(1), last_Iz = ld(2);
+  // last incident pulses, as the opposite-port pair sums STAGE 5 uses
+  A last_P[6];
 #pragma unroll
-  for (int k = 0; k < 12; k++) last_Vi[k] = __ldcs(S + pml_sidx(3 + k, pidx));
-  const A last_Vxt = __ldcs(S + pml_sidx(15, pidx)), last_Vyt = __ldcs(S + pml_sidx(16, pidx));
-  const A last_Vzt = __ldcs(S + pml_sidx(17, pidx));
-  const A last_Vxyt = __ldcs(S + pml_sidx(18, pidx)), last_Vyxt = __ldcs(S + pml_sidx(19, pidx));
-  const A last_Vzxt = __ldcs(S + pml_sidx(20, pidx)), last_Vxzt = __ldcs(S + pml_sidx(21, pidx));
-  const A last_Vyzt = __ldcs(S + pml_sidx(22, pidx)), last_Vzyt = __ldcs(S + pml_sidx(23, pidx));
+  for (int k = 0; k < 6; k++) last_P[k] = ld(3 + k);
+  const A last_Vxt = ld(9), last_Vyt = ld(10), last_Vzt = ld(11);
+  const A last_Vxyt = ld(12), last_Vyxt = ld(13);
+  const A last_Vzxt = ld(14), last_Vxzt = ld(15);
+  const A last_Vyzt = ld(16), last_Vzyt = ld(17);
 
   // STAGE 3: half-cell loss on incident pulses
   A V[12];
@@ -268,15 +278,16 @@ __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par,
   const A Iy = (V[Vzpx] - V[Vxpz] - V[Vznx] + V[Vxnz]) * inv2Z0;
   const A Iz = (V[Vxpy] - V[Vypx] - V[Vxny] + V[Vynx]) * inv2Z0;
   // STAGE 5
-  const A Vx_sh = ax * (-(last_Vi[Vznx] + last_Vi[Vzpx] + last_Vi[Vynx] + last_Vi[Vypx]) / A(2) +
-                        Csy * ((V[Vznx] + V[Vzpx]) + (last_Vi[Vznx] + last_Vi[Vzpx])) +
-                        Csz * ((V[Vynx] + V[Vypx]) + (last_Vi[Vynx] + last_Vi[Vypx])) + Csy_sz * last_Vxt);
-  const A Vy_sh = ay * (-(last_Vi[Vxny] + last_Vi[Vxpy] + last_Vi[Vzny] + last_Vi[Vzpy]) / A(2) +
-                        Csz * ((V[Vxny] + V[Vxpy]) + (last_Vi[Vxny] + last_Vi[Vxpy])) +
-                        Csx * ((V[Vzny] + V[Vzpy]) + (last_Vi[Vzny] + last_Vi[Vzpy])) + Csz_sx * last_Vyt);
-  const A Vz_sh = az * (-(last_Vi[Vynz] + last_Vi[Vypz] + last_Vi[Vxnz] + last_Vi[Vxpz]) / A(2) +
-                        Csx * ((V[Vynz] + V[Vypz]) + (last_Vi[Vynz] + last_Vi[Vypz])) +
-                        Csy * ((V[Vxnz] + V[Vxpz]) + (last_Vi[Vxnz] + last_Vi[Vxpz])) + Csx_sy * last_Vzt);
+  A Pn[6];
+  Pn[0] = V[Vznx] + V[Vzpx]; Pn[1] = V[Vynx] + V[Vypx];
+  Pn[2] = V[Vxny] + V[Vxpy]; Pn[3] = V[Vzny] + V[Vzpy];
+  Pn[4] = V[Vynz] + V[Vypz]; Pn[5] = V[Vxnz] + V[Vxpz];
+  const A Vx_sh = ax * (-(last_P[0] + last_P[1]) / A(2) + Csy * (Pn[0] + last_P[0]) + Csz * (Pn[1] + last_P[1]) +
+                        Csy_sz * last_Vxt);
+  const A Vy_sh = ay * (-(last_P[2] + last_P[3]) / A(2) + Csz * (Pn[2] + last_P[2]) + Csx * (Pn[3] + last_P[3]) +
+                        Csz_sx * last_Vyt);
+  const A Vz_sh = az * (-(last_P[4] + last_P[5]) / A(2) + Csx * (Pn[4] + last_P[4]) + Csy * (Pn[5] + last_P[5]) +
+                        Csx_sy * last_Vzt);
   // STAGE 6
   const A Vxt = ax * Vx + Vx_sh, Vyt = ay * Vy + Vy_sh, Vzt = az * Vz + Vz_sh;
   // STAGE 7a (output cells only)
@@ -298,14 +309,14 @@ __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par,
   // STAGE 8 + 9: save state
   __stcs(S + pml_sidx(0, pidx), ST(Ix)); __stcs(S + pml_sidx(1, pidx), ST(Iy)); __stcs(S + pml_sidx(2, pidx), ST(Iz));
 #pragma unroll
-  for (int k = 0; k < 12; k++) __stcs(S + pml_sidx(3 + k, pidx), ST(V[k]));
-  __stcs(S + pml_sidx(15, pidx), ST(Vxt)); __stcs(S + pml_sidx(16, pidx), ST(Vyt)); __stcs(S + pml_sidx(17, pidx), ST(Vzt));
-  __stcs(S + pml_sidx(18, pidx), ST(az * Iz * Z0 + Vxy_se));
-  __stcs(S + pml_sidx(19, pidx), ST(az * Iz * Z0 + Vyx_se));
-  __stcs(S + pml_sidx(20, pidx), ST(ay * Iy * Z0 + Vzx_se));
-  __stcs(S + pml_sidx(21, pidx), ST(ay * Iy * Z0 + Vxz_se));
-  __stcs(S + pml_sidx(22, pidx), ST(ax * Ix * Z0 + Vyz_se));
-  __stcs(S + pml_sidx(23, pidx), ST(ax * Ix * Z0 + Vzy_se));
+  for (int k = 0; k < 6; k++) __stcs(S + pml_sidx(3 + k, pidx), ST(Pn[k]));
+  __stcs(S + pml_sidx(9, pidx), ST(Vxt)); __stcs(S + pml_sidx(10, pidx), ST(Vyt)); __stcs(S + pml_sidx(11, pidx), ST(Vzt));
+  __stcs(S + pml_sidx(12, pidx), ST(az * Iz * Z0 + Vxy_se));
+  __stcs(S + pml_sidx(13, pidx), ST(az * Iz * Z0 + Vyx_se));
+  __stcs(S + pml_sidx(14, pidx), ST(ay * Iy * Z0 + Vzx_se));
+  __stcs(S + pml_sidx(15, pidx), ST(ay * Iy * Z0 + Vxz_se));
+  __stcs(S + pml_sidx(16, pidx), ST(ax * Ix * Z0 + Vyz_se));
+  __stcs(S + pml_sidx(17, pidx), ST(ax * Ix * Z0 + Vzy_se));
   // STAGE 10
   const A Vynx_P = Vx_sh - Vyx_se, Vypx_P = Vx_sh + Vyx_se;
   const A Vznx_P = Vx_sh + Vzx_se, Vzpx_P = Vx_sh - Vzx_se;
@@ -999,6 +1010,12 @@ __device__ __forceinline__ void special_body(const MeshDev<T> &m, int s, int rel
 #ifndef TLM_PML_MIN_BLOCKS
 #define TLM_PML_MIN_BLOCKS 3
 #endif
+// The FP32 kernel (FP32 state, FP64 arithmetic) fits 4 blocks in 128
+// registers without spills; 0.7 % faster per step than 3 on the 256^3
+// PML-spheres mesh, 1.6 % on a 96^3 PML box.
+#ifndef TLM_PML_MIN_BLOCKS_FP32
+#define TLM_PML_MIN_BLOCKS_FP32 4
+#endif
 
 // The PML cells of the reference's meshes form a box shell: the cells within
 // xl/xh of the x ends, yl/yh of the y ends or zl/zh of the z ends
@@ -1073,7 +1090,7 @@ template <typename T>
 __device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl, int s, int rel_step);
 
 template <typename T>
-__global__ void __launch_bounds__(128, TLM_PML_MIN_BLOCKS) tlm_pml_kernel(const MeshDev<T> m, const PmlList pl, int rel_step,
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? TLM_PML_MIN_BLOCKS_FP32 : TLM_PML_MIN_BLOCKS) tlm_pml_kernel(const MeshDev<T> m, const PmlList pl, int rel_step,
                                                       int prefetch_blocks) {
   // one elected thread per block pulls the PML state of the block that runs
   // prefetch_blocks later into L2 (one contiguous range of whole 32-cell
@@ -1086,7 +1103,10 @@ __global__ void __launch_bounds__(128, TLM_PML_MIN_BLOCKS) tlm_pml_kernel(const 
       const int cnt = (int)min((long long)blockDim.x, (long long)pl.n - s0);
       const long long tiles = ((long long)cnt + 31) / 32;  // s0 is a multiple of 128
       const char *a = reinterpret_cast<const char *>(m.pml_state + pml_sidx(0, s0));
-      bulk_prefetch_l2(a, (uint32_t)(tiles * 24 * 32 * sizeof(typename PmlTypes<T>::state)));
+      bulk_prefetch_l2(a, (uint32_t)(tiles * kPmlState * 32 * sizeof(typename PmlTypes<T>::state)));
+      // parameter indices: 2 bytes a cell from a 256-byte-aligned start; the
+      // index buffer carries 256 bytes of padding
+      bulk_prefetch_l2(pl.par + s0, (uint32_t)((cnt * 2 + 15) & ~15));
       if (!pl.sh.on) {
         const char *pa = reinterpret_cast<const char *>(reinterpret_cast<uintptr_t>(pl.pos + s0) & ~(uintptr_t)15);
         bulk_prefetch_l2(pa, (uint32_t)((cnt * 8 + 15) & ~15) + 16);
@@ -1104,27 +1124,18 @@ __device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl,
   const T *__restrict__ in = (t & 1) ? m.links0 : m.links1;
   T *__restrict__ out = (t & 1) ? m.links1 : m.links0;
   const long long P = m.plane;
-  int x, y, z, out_no = -1;
+  int x, y, z;
   if (pl.sh.on) {
     pml_shell_pos(pl.sh, s, x, y, z);
-    if (pl.n_out_map) {  // binary search of the sorted output map
-      int lo = 0, hi = pl.n_out_map - 1;
-      while (lo <= hi) {
-        const int mid = (lo + hi) >> 1;
-        const int2 e = pl.out_map[mid];
-        if (e.x == s) { out_no = e.y; break; }
-        if (e.x < s) lo = mid + 1; else hi = mid - 1;
-      }
-    }
   } else {
     const unsigned long long pk = __ldcs(pl.pos + s);
     x = (int)(pk & 0x1fffffull); y = (int)((pk >> 21) & 0x1fffffull); z = (int)((pk >> 42) & 0x1fffffull);
-    if (pk >> 63)
-      for (int k = 0; k < pl.n_out_map; k++)
-        if (pl.out_map[k].x == s) out_no = pl.out_map[k].y;
   }
-  const int par = __ldcs(pl.par + s);
-  if (par == kPmlMaterialSlot) return;  // PML cell in a material: tlm_pml_material_kernel
+  // Every load of the cell is issued before anything waits on one: the
+  // parameter index (which also says whether the cell is an output cell or
+  // a PML cell in a material) is checked only after the link and state
+  // loads are in flight, so a warp waits for one memory round trip, not two.
+  const int pw = __ldcs(pl.par + s);
   const long long idx = (long long)(z + 1) * m.PxPy + (long long)(y + 1) * m.Px + x;
   const long long dy = m.Px, dz = m.PxPy;
   T ci[12], co[12];
@@ -1140,8 +1151,26 @@ __device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl,
   ci[Vy_zmin] = __ldcs(in + Vy_zmax * P + idx - dz);
   ci[Vx_zmax] = __ldcs(in + Vx_zmin * P + idx + dz);
   ci[Vy_zmax] = __ldcs(in + Vy_zmin * P + idx + dz);
+  // state value k of this cell: S[pml_sidx(k, s)] = S[pml_sidx(0, s) + 32 k]
+  using ST = typename PmlTypes<T>::state;
+  ST st[kPmlState];
+  const ST *Lg = m.pml_state + pml_sidx(0, s);
+#pragma unroll
+  for (int k = 0; k < kPmlState; k++) st[k] = __ldcs(Lg + 32 * k);
+  if (pw == kPmlMaterialSlot) return;  // PML cell in a material: tlm_pml_material_kernel
+  const int par = pw & (kPmlOutputFlag - 1);
+  int out_no = -1;
+  if (pw & kPmlOutputFlag) {  // binary search of the output map (sorted by PML cell)
+    int lo = 0, hi = pl.n_out_map - 1;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1;
+      const int2 e = pl.out_map[mid];
+      if (e.x == s) { out_no = e.y; break; }
+      if (e.x < s) lo = mid + 1; else hi = mid - 1;
+    }
+  }
   double *row = (out_no >= 0) ? m.cell_out + ((size_t)(t - 1) * m.n_out + out_no) * 6 : nullptr;
-  pml_cell<T>(m, s, par, out_no, ci, co, row);
+  pml_cell<T>(m, s, par, out_no, ci, co, row, st);
 #pragma unroll
   for (int p = 0; p < 12; p++) __stcs(out + p * P + idx, co[p]);
   if (x == 0) {

@@ -68,7 +68,7 @@ def footprint_bytes(t: dict, precision: int = capi.TLM_PRECISION_FP32) -> int:
     px = ((nx + 1 + 3) // 4) * 4
     plane = px * (ny + 2) * (nz + 2)
     links = 2 * 12 * plane * esz
-    pml = int(t["n_pml_cells"]) * (24 * esz + 10) + int(t.get("n_pml_material_cells", 0)) * (66 * 8 + 24)
+    pml = int(t["n_pml_cells"]) * (18 * esz + 10) + int(t.get("n_pml_material_cells", 0)) * (66 * 8 + 24)
     special = int(t["n_special"]) * 32 + (ny * px + 31) // 32 * nz * 8
     filt = int(t["n_special"]) * 0 + 6 * 8 * 8 * int((np.asarray(t["sp_material"]) > 0).sum())
     outs = int(t["n_out_cells"]) * 6 * 8 * n + int(t["n_exc_cells"]) * 9 * 8 * n
