@@ -485,6 +485,10 @@ tlm::PmlShell detect_pml_shell(const std::vector<unsigned long long> &pos, int n
   h.xl = xl; h.xh = xh; h.yl = yl; h.yh = yh; h.zl = zl; h.zh = zh;
   h.full = (int)full;
   h.partial = (yl + yh) * nx + (ny - yl - yh) * (xl + xh);
+  h.d_full = tlm::make_fast_div(h.full);
+  h.d_nx = tlm::make_fast_div(nx);
+  h.d_partial = tlm::make_fast_div(h.partial);
+  h.d_w = tlm::make_fast_div(xl + xh);
   const long long count = (long long)(zl + zh) * full + (long long)(nz - zl - zh) * h.partial;
   if (count != (long long)pos.size()) return tlm::PmlShell{};
   // the decoder the kernels run must reproduce every listed position

@@ -1011,10 +1011,16 @@ __device__ __forceinline__ void special_body(const MeshDev<T> &m, int s, int rel
 #define TLM_PML_MIN_BLOCKS 3
 #endif
 // The FP32 kernel (FP32 state, FP64 arithmetic) fits 4 blocks in 128
-// registers without spills; 0.7 % faster per step than 3 on the 256^3
-// PML-spheres mesh, 1.6 % on a 96^3 PML box.
+// registers without spills, 0.7-1.6 % faster per step than 3; 5 blocks (96
+// registers, a 16-byte spill) gains another 0-2 % (C3 and 160^3 most);
+// 6 blocks (80 registers, 136-byte spill) is 3-16 % slower.
 #ifndef TLM_PML_MIN_BLOCKS_FP32
-#define TLM_PML_MIN_BLOCKS_FP32 4
+#define TLM_PML_MIN_BLOCKS_FP32 5
+#endif
+// L2 prefetch of the link runs a contiguous PML block will gather (with its
+// state): 1-3 % per step on PML-bounded meshes.
+#ifndef TLM_PML_LINK_PREFETCH
+#define TLM_PML_LINK_PREFETCH 1
 #endif
 
 // The PML cells of the reference's meshes form a box shell: the cells within
@@ -1022,10 +1028,33 @@ __device__ __forceinline__ void special_body(const MeshDev<T> &m, int s, int rel
 // (calc_pml_dist).  Numbered in traversal order, a cell's position then
 // follows from its PML number, so the link addresses do not wait for a
 // position load.
+// Division by a constant divisor d >= 1 for dividends 0 <= n < 2^31:
+// floor(n / d) = (n * m) >> sh with l = ceil(log2 d), sh = 31 + l and
+// m = floor(2^sh / d) + 1 (Granlund and Montgomery, "Division by invariant
+// integers using multiplication", PLDI 1994, theorem 4.2: 2^sh < m d <=
+// 2^sh + 2^l).  n * m < 2^31 (2^32 + 1) fits 64 bits.
+struct FastDiv {
+  unsigned long long m;
+  int sh;
+};
+__host__ __device__ __forceinline__ int fast_div(int n, const FastDiv &f) {
+  return (int)(((unsigned long long)(unsigned)n * f.m) >> f.sh);
+}
+inline FastDiv make_fast_div(int d) {
+  if (d < 1) d = 1;  // a divisor the decoder never uses
+  int l = 0;
+  while ((1ll << l) < d) l++;
+  FastDiv f;
+  f.sh = 31 + l;
+  f.m = (1ull << f.sh) / (unsigned long long)d + 1ull;
+  return f;
+}
+
 struct PmlShell {
   int on;                 // 1: positions from the shell, 0: from `pos`
   int nx, ny, nz, xl, xh, yl, yh, zl, zh;
   int full, partial;      // PML cells of a whole z-plane / of a plane between the z slabs
+  FastDiv d_full, d_nx, d_partial, d_w;  // divisors full, nx, partial, xl + xh
 };
 
 struct PmlList {
@@ -1040,21 +1069,21 @@ struct PmlList {
 __host__ __device__ __forceinline__ void pml_shell_pos(const PmlShell &h, int s, int &x, int &y, int &z) {
   const int lo = h.zl * h.full;
   if (s < lo) {
-    z = s / h.full;
+    z = fast_div(s, h.d_full);
     const int r = s - z * h.full;
-    y = r / h.nx;
+    y = fast_div(r, h.d_nx);
     x = r - y * h.nx;
     return;
   }
   const int s2 = s - lo;
   const int mid = h.nz - h.zl - h.zh;
   if (s2 < mid * h.partial) {
-    const int zz = s2 / h.partial;
+    const int zz = fast_div(s2, h.d_partial);
     z = h.zl + zz;
     const int r = s2 - zz * h.partial;
     const int rows_lo = h.yl * h.nx;
     if (r < rows_lo) {
-      y = r / h.nx;
+      y = fast_div(r, h.d_nx);
       x = r - y * h.nx;
       return;
     }
@@ -1062,23 +1091,23 @@ __host__ __device__ __forceinline__ void pml_shell_pos(const PmlShell &h, int s,
     const int w = h.xl + h.xh;
     const int midrows = h.ny - h.yl - h.yh;
     if (r2 < midrows * w) {
-      const int yy = r2 / w;
+      const int yy = fast_div(r2, h.d_w);
       y = h.yl + yy;
       const int c = r2 - yy * w;
       x = c < h.xl ? c : h.nx - h.xh + (c - h.xl);
       return;
     }
     const int r3 = r2 - midrows * w;
-    const int yy = r3 / h.nx;
+    const int yy = fast_div(r3, h.d_nx);
     y = h.ny - h.yh + yy;
     x = r3 - yy * h.nx;
     return;
   }
   const int s3 = s2 - mid * h.partial;
-  const int zz = s3 / h.full;
+  const int zz = fast_div(s3, h.d_full);
   z = h.nz - h.zh + zz;
   const int r = s3 - zz * h.full;
-  y = r / h.nx;
+  y = fast_div(r, h.d_nx);
   x = r - y * h.nx;
 }
 
@@ -1110,6 +1139,34 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? TLM_PML_MIN_BLOCKS_FP32 
       if (!pl.sh.on) {
         const char *pa = reinterpret_cast<const char *>(reinterpret_cast<uintptr_t>(pl.pos + s0) & ~(uintptr_t)15);
         bulk_prefetch_l2(pa, (uint32_t)((cnt * 8 + 15) & ~15) + 16);
+      } else if (TLM_PML_LINK_PREFETCH) {
+        // the links the block will gather, when its cells fill one run of
+        // plane elements (z-slab planes, y-slab rows): that run of each
+        // source plane, shifted by the port's pull offset and widened to
+        // 16-byte boundaries.  idx - 1 >= 0 and idx + dz + 1 < plane for
+        // every cell, and planes are whole multiples of 16 bytes, so the
+        // widened runs stay inside the link buffer.
+        int x0, y0, z0, x1, y1, z1;
+        pml_shell_pos(pl.sh, (int)s0, x0, y0, z0);
+        pml_shell_pos(pl.sh, (int)(s0 + cnt - 1), x1, y1, z1);
+        const long long e0 = (long long)y0 * m.Px + x0, e1 = (long long)y1 * m.Px + x1;
+        if (z0 == z1 && e1 - e0 < 2LL * cnt) {
+          const int t = *m.d_base + rel_step;
+          const T *in = (t & 1) ? m.links0 : m.links1;
+          const long long i0 = (long long)(z0 + 1) * m.PxPy + (long long)m.Px + e0;
+          const long long len = e1 - e0 + 1;
+          const long long P = m.plane, dy = m.Px, dz = m.PxPy;
+          const int src[12] = {Vy_xmax, Vz_xmax, Vy_xmin, Vz_xmin, Vx_ymax, Vz_ymax,
+                               Vx_ymin, Vz_ymin, Vx_zmax, Vy_zmax, Vx_zmin, Vy_zmin};
+          const long long sft[12] = {-1, -1, 1, 1, -dy, -dy, dy, dy, -dz, -dz, dz, dz};
+#pragma unroll
+          for (int k = 0; k < 12; k++) {
+            const uintptr_t b = reinterpret_cast<uintptr_t>(in + src[k] * P + i0 + sft[k]);
+            const uintptr_t e = b + (uintptr_t)len * sizeof(T);
+            const uintptr_t b16 = b & ~(uintptr_t)15, e16 = (e + 15) & ~(uintptr_t)15;
+            bulk_prefetch_l2(reinterpret_cast<const void *>(b16), (uint32_t)(e16 - b16));
+          }
+        }
       }
     }
   }
