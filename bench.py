@@ -45,7 +45,7 @@ BULK_VARIANTS = [(0, 0, 0, 0), (1024, 2, 512, 2), (512, 3, 256, 3), (512, 4, 256
 # dram__bytes_write.sum) from one ncu --set full capture of the same workload.
 NCU_TRAFFIC = {
     "pml_spheres_256^3_pml8_32spheres_huygens_dft64x64x64": {
-        "bytes": 756.220672e6 + 610.022912e6,
+        "bytes": 755.997440e6 + 609.044480e6,
         "source": "profiles/tlm_bulk_tma_kernel_pml_spheres_256_fp32.md (tlm_bulk_tma_kernel<float,4,512,3>)"},
     "debye_slabs_384x384x192_pml10_6slabs_dft64x64x64": {
         "bytes": None,

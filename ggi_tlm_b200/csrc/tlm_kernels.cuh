@@ -1118,57 +1118,62 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void *p, uint32_t bytes) 
 template <typename T>
 __device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl, int s, int rel_step);
 
+// One elected thread pulls into L2 what the PML block of 128 cells starting
+// at s0 (a multiple of 128) will read: its state (one contiguous range of
+// whole 32-cell tiles), its parameter indices, and its positions or, for a
+// shell, the link runs it gathers.  The position range is widened to 16-byte
+// boundaries; the position buffer carries 64 bytes of padding so the
+// widened range stays inside its allocation.
+template <typename T>
+__device__ __forceinline__ void pml_prefetch_block(const MeshDev<T> &m, const PmlList &pl, long long s0, int rel_step) {
+  const int cnt = (int)min(128LL, (long long)pl.n - s0);
+  const long long tiles = ((long long)cnt + 31) / 32;  // s0 is a multiple of 128
+  const char *a = reinterpret_cast<const char *>(m.pml_state + pml_sidx(0, s0));
+  bulk_prefetch_l2(a, (uint32_t)(tiles * kPmlState * 32 * sizeof(typename PmlTypes<T>::state)));
+  // parameter indices: 2 bytes a cell from a 256-byte-aligned start; the
+  // index buffer carries 256 bytes of padding
+  bulk_prefetch_l2(pl.par + s0, (uint32_t)((cnt * 2 + 15) & ~15));
+  if (!pl.sh.on) {
+    const char *pa = reinterpret_cast<const char *>(reinterpret_cast<uintptr_t>(pl.pos + s0) & ~(uintptr_t)15);
+    bulk_prefetch_l2(pa, (uint32_t)((cnt * 8 + 15) & ~15) + 16);
+  } else if (TLM_PML_LINK_PREFETCH) {
+    // the links the block will gather, when its cells fill one run of
+    // plane elements (z-slab planes, y-slab rows): that run of each
+    // source plane, shifted by the port's pull offset and widened to
+    // 16-byte boundaries.  idx - 1 >= 0 and idx + dz + 1 < plane for
+    // every cell, and planes are whole multiples of 16 bytes, so the
+    // widened runs stay inside the link buffer.
+    int x0, y0, z0, x1, y1, z1;
+    pml_shell_pos(pl.sh, (int)s0, x0, y0, z0);
+    pml_shell_pos(pl.sh, (int)(s0 + cnt - 1), x1, y1, z1);
+    const long long e0 = (long long)y0 * m.Px + x0, e1 = (long long)y1 * m.Px + x1;
+    if (z0 == z1 && e1 - e0 < 2LL * cnt) {
+      const int t = *m.d_base + rel_step;
+      const T *in = (t & 1) ? m.links0 : m.links1;
+      const long long i0 = (long long)(z0 + 1) * m.PxPy + (long long)m.Px + e0;
+      const long long len = e1 - e0 + 1;
+      const long long P = m.plane, dy = m.Px, dz = m.PxPy;
+      const int src[12] = {Vy_xmax, Vz_xmax, Vy_xmin, Vz_xmin, Vx_ymax, Vz_ymax,
+                           Vx_ymin, Vz_ymin, Vx_zmax, Vy_zmax, Vx_zmin, Vy_zmin};
+      const long long sft[12] = {-1, -1, 1, 1, -dy, -dy, dy, dy, -dz, -dz, dz, dz};
+#pragma unroll
+      for (int k = 0; k < 12; k++) {
+        const uintptr_t b = reinterpret_cast<uintptr_t>(in + src[k] * P + i0 + sft[k]);
+        const uintptr_t e = b + (uintptr_t)len * sizeof(T);
+        const uintptr_t b16 = b & ~(uintptr_t)15, e16 = (e + 15) & ~(uintptr_t)15;
+        bulk_prefetch_l2(reinterpret_cast<const void *>(b16), (uint32_t)(e16 - b16));
+      }
+    }
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(128, sizeof(T) == 4 ? TLM_PML_MIN_BLOCKS_FP32 : TLM_PML_MIN_BLOCKS) tlm_pml_kernel(const MeshDev<T> m, const PmlList pl, int rel_step,
                                                       int prefetch_blocks) {
-  // one elected thread per block pulls the PML state of the block that runs
-  // prefetch_blocks later into L2 (one contiguous range of whole 32-cell
-  // tiles + metadata), so that block's state loads hit L2.  The position
-  // range is widened to 16-byte boundaries; the position buffer carries 64
-  // bytes of padding so the widened range stays inside its allocation.
+  // prefetch for the block that runs prefetch_blocks later, so its loads hit L2
   if (threadIdx.x == 0 && prefetch_blocks > 0) {
     const long long s0 = (long long)(blockIdx.x + prefetch_blocks) * blockDim.x;
-    if (s0 < pl.n) {
-      const int cnt = (int)min((long long)blockDim.x, (long long)pl.n - s0);
-      const long long tiles = ((long long)cnt + 31) / 32;  // s0 is a multiple of 128
-      const char *a = reinterpret_cast<const char *>(m.pml_state + pml_sidx(0, s0));
-      bulk_prefetch_l2(a, (uint32_t)(tiles * kPmlState * 32 * sizeof(typename PmlTypes<T>::state)));
-      // parameter indices: 2 bytes a cell from a 256-byte-aligned start; the
-      // index buffer carries 256 bytes of padding
-      bulk_prefetch_l2(pl.par + s0, (uint32_t)((cnt * 2 + 15) & ~15));
-      if (!pl.sh.on) {
-        const char *pa = reinterpret_cast<const char *>(reinterpret_cast<uintptr_t>(pl.pos + s0) & ~(uintptr_t)15);
-        bulk_prefetch_l2(pa, (uint32_t)((cnt * 8 + 15) & ~15) + 16);
-      } else if (TLM_PML_LINK_PREFETCH) {
-        // the links the block will gather, when its cells fill one run of
-        // plane elements (z-slab planes, y-slab rows): that run of each
-        // source plane, shifted by the port's pull offset and widened to
-        // 16-byte boundaries.  idx - 1 >= 0 and idx + dz + 1 < plane for
-        // every cell, and planes are whole multiples of 16 bytes, so the
-        // widened runs stay inside the link buffer.
-        int x0, y0, z0, x1, y1, z1;
-        pml_shell_pos(pl.sh, (int)s0, x0, y0, z0);
-        pml_shell_pos(pl.sh, (int)(s0 + cnt - 1), x1, y1, z1);
-        const long long e0 = (long long)y0 * m.Px + x0, e1 = (long long)y1 * m.Px + x1;
-        if (z0 == z1 && e1 - e0 < 2LL * cnt) {
-          const int t = *m.d_base + rel_step;
-          const T *in = (t & 1) ? m.links0 : m.links1;
-          const long long i0 = (long long)(z0 + 1) * m.PxPy + (long long)m.Px + e0;
-          const long long len = e1 - e0 + 1;
-          const long long P = m.plane, dy = m.Px, dz = m.PxPy;
-          const int src[12] = {Vy_xmax, Vz_xmax, Vy_xmin, Vz_xmin, Vx_ymax, Vz_ymax,
-                               Vx_ymin, Vz_ymin, Vx_zmax, Vy_zmax, Vx_zmin, Vy_zmin};
-          const long long sft[12] = {-1, -1, 1, 1, -dy, -dy, dy, dy, -dz, -dz, dz, dz};
-#pragma unroll
-          for (int k = 0; k < 12; k++) {
-            const uintptr_t b = reinterpret_cast<uintptr_t>(in + src[k] * P + i0 + sft[k]);
-            const uintptr_t e = b + (uintptr_t)len * sizeof(T);
-            const uintptr_t b16 = b & ~(uintptr_t)15, e16 = (e + 15) & ~(uintptr_t)15;
-            bulk_prefetch_l2(reinterpret_cast<const void *>(b16), (uint32_t)(e16 - b16));
-          }
-        }
-      }
-    }
+    if (s0 < pl.n) pml_prefetch_block<T>(m, pl, s0, rel_step);
   }
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= pl.n) return;
@@ -1812,8 +1817,22 @@ struct BatchDev {
   int n_active;
 };
 
+// Blocks ahead of the running one whose PML data the batched kernel prefetches.
+constexpr int kPmlBatchPrefetch = 1200;
+
+// The batched PML kernel (one more indirection per block) spills 68 bytes
+// at 5 blocks; at 4 (128 registers, no spill) C4 runs 0.7 % faster.
+#ifndef TLM_PML_BATCH_MIN_BLOCKS_FP32
+#define TLM_PML_BATCH_MIN_BLOCKS_FP32 4
+#endif
+
 template <typename T>
-__global__ void __launch_bounds__(128) tlm_pml_batch_kernel(const BatchDev<T> b, int rel_step) {
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? TLM_PML_BATCH_MIN_BLOCKS_FP32 : TLM_PML_MIN_BLOCKS)
+    tlm_pml_batch_kernel(const BatchDev<T> b, int rel_step) {
+  if (threadIdx.x == 0 && blockIdx.x + kPmlBatchPrefetch < b.n_pml_blocks) {
+    const int2 f = b.pml_blocks[blockIdx.x + kPmlBatchPrefetch];  // (mesh, first cell)
+    pml_prefetch_block<T>(b.meshes[f.x], b.pml[f.x], f.y, rel_step);
+  }
   const int2 w = b.pml_blocks[blockIdx.x];
   const int s = w.y + threadIdx.x;
   const PmlList &pl = b.pml[w.x];
