@@ -40,7 +40,7 @@ EXPORTS = [
     "tlm_gpu_set_small_to_zero", "tlm_gpu_set_pml_sigma", "tlm_gpu_set_face_excitation",
     "tlm_gpu_set_face_outputs", "tlm_gpu_fetch_face_output", "tlm_gpu_set_outer_huygens",
     "tlm_gpu_set_far_field", "tlm_gpu_fetch_far_field", "tlm_gpu_pool_release", "tlm_gpu_pool_cached_bytes",
-    "tlm_gpu_prepare",
+    "tlm_gpu_prepare", "tlm_gpu_set_output_series", "tlm_gpu_set_volume_dft", "tlm_gpu_fetch_volume_dft",
 ]
 
 
@@ -91,6 +91,9 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_faces": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, i32, i32],
         "tlm_gpu_set_huygens": [i64, i32, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double, C.c_double, i32],
         "tlm_gpu_set_outputs": [i64, i32],
+        "tlm_gpu_set_output_series": [i64, i32, _i32p],
+        "tlm_gpu_set_volume_dft": [i64, i32, _f64p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p],
+        "tlm_gpu_fetch_volume_dft": [i64, _f64p],
         "tlm_gpu_set_small_to_zero": [i64, i32, C.c_double],
         "tlm_gpu_set_dft": [i64, i32, _f64p, _i32p, _i32p, _i32p, _i32p],
         "tlm_gpu_run": [i64, i32, i32],
@@ -221,6 +224,14 @@ class GpuMesh:
             _check(lib.tlm_gpu_set_huygens(self.h, int(t["hs_n"]), _p(hf), _p(hn), _p(ho), _p(Ei), _p(Hi),
                                            float(t["hs_offset_min"]), float(t["hs_c"]), int(t["hs_fn"])))
         _check(lib.tlm_gpu_set_outputs(self.h, int(t["n_out_cells"])))
+        keep = t.get("out_keep")
+        if keep is not None and int(t["n_out_cells"]) and not np.all(np.asarray(keep) == 1):
+            kp = _i32(keep)
+            _check(lib.tlm_gpu_set_output_series(self.h, int(t["n_out_cells"]), _p(kp)))
+        if int(t.get("n_vdft", 0)):
+            vd = [_f64(t["vdft_freq"]), _i32(t["vdft_comp"]), _i32(t["vdft_first"]), _i32(t["vdft_last"]),
+                  _i32(t["vdft_interval"]), _i32(t["vdft_cell_ptr"]), _i32(t["vdft_cell_out"])]
+            _check(lib.tlm_gpu_set_volume_dft(self.h, int(t["n_vdft"]), *[_p(x) for x in vd]))
         if int(t["n_dft"]):
             df = [_f64(t["dft_freq"]), _i32(t["dft_comp"]), _i32(t["dft_face_ptr"]), _i32(t["dft_face_out"]),
                   _i32(t["dft_face_side"])]
@@ -277,10 +288,13 @@ class GpuMesh:
 
     # -- results -----------------------------------------------------------
     def cell_output(self, first: int = 1, n: Optional[int] = None) -> np.ndarray:
-        """cell_output_field snapshots [n, n_out_cells, 6] of steps first.."""
+        """cell_output_field snapshots [n, n_kept, 6] of steps first.., for
+        the output cells that keep a time series (all of them unless the
+        tables' ``out_keep`` says otherwise), in output-number order."""
         if n is None:
             n = self.step - first + 1
-        no = int(self.t["n_out_cells"])
+        keep = self.t.get("out_keep")
+        no = int(self.t["n_out_cells"]) if keep is None else int(np.sum(keep))
         out = np.zeros((n, max(no, 1), 6))
         _check(_lib.tlm_gpu_fetch_cell_output(self.h, first, n, out.ctypes.data_as(_f64p)))
         return out[:, :no, :]
@@ -301,6 +315,15 @@ class GpuMesh:
         _check(_lib.tlm_gpu_fetch_far_field(self.h, out.ctypes.data_as(_f64p)))
         v = out[: 12 * n].reshape(n, 6, 2)
         return v[..., 0] + 1j * v[..., 1]
+
+    def volume_dft(self) -> np.ndarray:
+        """Frequency output volume values [entries] complex, in the tables'
+        volume then cell order."""
+        n = int(self.t["vdft_cell_ptr"][-1]) if int(self.t.get("n_vdft", 0)) else 0
+        out = np.zeros(max(2 * n, 2))
+        _check(_lib.tlm_gpu_fetch_volume_dft(self.h, out.ctypes.data_as(_f64p)))
+        v = out[: 2 * n].reshape(-1, 2)
+        return v[:, 0] + 1j * v[:, 1]
 
     def dft(self) -> np.ndarray:
         n = int(self.t["dft_face_ptr"][-1]) if int(self.t["n_dft"]) else 0

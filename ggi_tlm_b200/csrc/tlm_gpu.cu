@@ -260,6 +260,12 @@ struct Mesh {
   bool hs_outer = false;             // the Huygens surface is the outer boundary
   std::vector<int32_t> hs_cell;      // outer: 4 per patch (cx, cy, cz 1-based, face code)
   int n_out_cells = 0;
+  std::vector<int32_t> out_keep;     // per output cell: 1 keeps a time series (empty: all do)
+  int n_hist = 0;                    // outputs that keep a time series
+  std::vector<double> vdft_freq;     // frequency output volumes, one per frequency
+  std::vector<int32_t> vdft_gate;    // 4 per volume: first, last, interval, component
+  std::vector<int32_t> vdft_ptr, vdft_out;
+  int vdft_entries = 0;
   int n_dft = 0;
   std::vector<double> dft_freq;
   std::vector<int32_t> dft_comp, dft_ptr, dft_fout, dft_fcode;
@@ -268,7 +274,8 @@ struct Mesh {
   DevBuf links, seg_mask, seg_base, sp_rec, sp_pos, pml_state, pml_par, pml_ixt, filt, mats_d, exc_field, exc_type,
       cell_out, faces, face_io, face_hs, value_face, face_field, dft_entry, dft_phasor, dft_acc, d_base,
       pmm_pos, pmm_parmat, pmm_state, pmm_sigma, face_src, fpt_field_d, fpt_type_d, fprobe, fprobe_rec,
-      ohs_face, ohs_offset, ff_entry, ff_phasor, ff_acc;
+      ohs_face, ohs_offset, ff_entry, ff_phasor, ff_acc, cell_cur, out_hist, vdft_entry, vdft_gate_d, vdft_phasor,
+      vdft_acc;
   int n_pt_rows = 0;
   int n_pmm = 0;  // PML cells inside a volume material
   int n_filt = 0, filt_eo = 0, filt_mo = 0;
@@ -299,6 +306,7 @@ struct Mesh {
   // graph of kGraphSteps steps
   static constexpr int kGraphSteps = 8;
   cudaGraphExec_t graph = nullptr;
+  long long graph_launches = 0;  // kernel launches in one replay of the graph
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> kev;
 
@@ -371,7 +379,10 @@ tlm::MeshDev<T> mesh_dev(Mesh *m) {
   d.exc_type = (const int8_t *)m->exc_type.p;
   d.n_exc = m->n_exc_cells;
   d.cell_out = (double *)m->cell_out.p;
+  d.cell_cur = (double *)m->cell_cur.p;
+  d.out_hist = (const int *)m->out_hist.p;
   d.n_out = m->n_out_cells;
+  d.n_hist = m->n_hist;
   d.dl = m->desc.dl;
   d.dt = m->desc.dt;
   d.d_base = (const int *)m->d_base.p;
@@ -433,6 +444,18 @@ tlm::FarFieldDev far_field_dev(Mesh *m) {
 
 tlm::FaceProbeDev face_probe_dev(Mesh *m) {
   return tlm::FaceProbeDev{(const int4 *)m->fprobe.p, (double *)m->fprobe_rec.p, (int)m->fpr_face.size()};
+}
+
+tlm::VolDftDev vol_dft_dev(Mesh *m) {
+  tlm::VolDftDev d{};
+  d.n_entries = m->vdft_entries;
+  d.n_vol = (int)m->vdft_freq.size();
+  d.entry = (const int2 *)m->vdft_entry.p;
+  d.gate = (const int4 *)m->vdft_gate_d.p;
+  d.phasor = (const double2 *)m->vdft_phasor.p;
+  d.cell_cur = (const double *)m->cell_cur.p;
+  d.acc = (double2 *)m->vdft_acc.p;
+  return d;
 }
 
 tlm::DftDev dft_dev(Mesh *m) {
@@ -709,9 +732,56 @@ int finalize(Mesh *m) {
     }
     if ((rc = upload(m, m->exc_field, field)) || (rc = upload(m, m->exc_type, type))) return rc;
   }
-  // ---- cell outputs
-  if ((rc = dalloc(m, m->cell_out, (size_t)std::max(m->n_out_cells, 1) * 6 * nsteps * sizeof(double)))) return rc;
-  CK(cudaMemset(m->cell_out.p, 0, m->cell_out.bytes));
+  // ---- cell outputs: the current-step rows of all of them, the time series
+  // of those that keep one
+  {
+    const int no = m->n_out_cells;
+    if (!m->out_keep.empty() && (int)m->out_keep.size() != no)
+      return fail(TLM_E_BADARG, "output series flags: %zu given for %d output cells", m->out_keep.size(), no);
+    std::vector<int32_t> slot(std::max(no, 1), -1);
+    int nh = 0;
+    for (int i = 0; i < no; i++)
+      if (m->out_keep.empty() || m->out_keep[i]) slot[i] = nh++;
+    m->n_hist = nh;
+    if ((rc = upload(m, m->out_hist, slot))) return rc;
+    if ((rc = dalloc(m, m->cell_cur, (size_t)std::max(no, 1) * 6 * sizeof(double)))) return rc;
+    CK(cudaMemset(m->cell_cur.p, 0, m->cell_cur.bytes));
+    if ((rc = dalloc(m, m->cell_out, (size_t)std::max(nh, 1) * 6 * nsteps * sizeof(double)))) return rc;
+    CK(cudaMemset(m->cell_out.p, 0, m->cell_out.bytes));
+  }
+  // ---- frequency output volumes
+  {
+    const int nv = (int)m->vdft_freq.size();
+    std::vector<int2> ent;
+    std::vector<int4> gate(std::max(nv, 1), int4{1, 0, 1, 1});
+    for (int v = 0; v < nv; v++) {
+      const int *g = &m->vdft_gate[(size_t)v * 4];
+      if (g[3] < 1 || g[3] > 6) return fail(TLM_E_BADARG, "output volume %d: component %d is not Ex..Hz", v + 1, g[3]);
+      if (g[2] < 1) return fail(TLM_E_BADARG, "output volume %d: timestep interval must be >= 1", v + 1);
+      gate[v] = int4{g[0], g[1], g[2], g[3]};
+      for (int k = m->vdft_ptr[v]; k < m->vdft_ptr[v + 1]; k++) {
+        const int o = m->vdft_out[k];
+        if (o < 1 || o > m->n_out_cells) return fail(TLM_E_BADARG, "output volume %d: output cell %d out of range", v + 1, o);
+        ent.push_back(int2{v, o - 1});
+      }
+    }
+    m->vdft_entries = (int)ent.size();
+    if (ent.empty()) ent.resize(1);
+    std::vector<double2> ph((size_t)std::max(nv, 1) * nsteps, double2{0, 0});
+    const double pi = 3.141592653589793;
+    for (int t = 0; t < nsteps; t++) {
+      const double time = (double)t * D.dt;  // (timestep-1)*dt: cell outputs come before the half step
+      for (int v = 0; v < nv; v++) {
+        const double arg = -2.0 * pi * m->vdft_freq[v] * time;
+        ph[(size_t)t * nv + v] = double2{cos(arg), sin(arg)};
+      }
+    }
+    if ((rc = upload(m, m->vdft_entry, ent)) || (rc = upload(m, m->vdft_gate_d, gate)) ||
+        (rc = upload(m, m->vdft_phasor, ph)))
+      return rc;
+    if ((rc = dalloc(m, m->vdft_acc, ent.size() * sizeof(double2)))) return rc;
+    CK(cudaMemset(m->vdft_acc.p, 0, m->vdft_acc.bytes));
+  }
   // ---- special faces
   {
     const int nf = (int)m->f_cx.size();
@@ -1079,6 +1149,11 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
       m->last_launches++;
     }
     if (side && (rc = m->side.end(m->stream))) return rc;
+    if (m->vdft_entries) {  // reads the cell outputs this step's cell kernels wrote
+      const tlm::VolDftDev vd = vol_dft_dev(m);
+      tlm::tlm_volume_dft_kernel<<<(vd.n_entries + 255) / 256, 256, 0, m->stream>>>(vd, md.d_base, k);
+      m->last_launches++;
+    }
     if (fd.n_faces) {
       tlm::tlm_face_kernel<T><<<(fd.n_faces + 127) / 128, 128, 0, m->stream>>>(md, fd, k);
       m->last_launches++;
@@ -1145,14 +1220,12 @@ int run_steps(Mesh *m, int n) {
       ce = cudaGraphInstantiate(&m->graph, g, 0);
       cudaGraphDestroy(g);
       if (ce != cudaSuccess) return fail(TLM_E_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+      m->graph_launches = m->last_launches - saved + 1;  // the kernels captured, + the counter advance
       m->last_launches = saved;
     }
-    const long long per_graph =
-        (long long)G * (1 + (m->n_pml_list ? 1 : 0) + (m->n_sp_dev ? 1 : 0) + (m->f_cx.empty() ? 0 : 1) +
-                          (m->dft_entries ? 1 : 0)) + 1;
     for (int i = 0; i < full; i++) {
       CK(cudaGraphLaunch(m->graph, m->stream));
-      m->last_launches += per_graph;
+      m->last_launches += m->graph_launches;
     }
     for (int i = 0; i < rem; i++) {
       if ((rc = enqueue(m, 1, nullptr))) return rc;
@@ -1402,6 +1475,52 @@ int tlm_gpu_set_outputs(int64_t h, int32_t n_out_cells) {
   return TLM_OK;
 }
 
+int tlm_gpu_set_output_series(int64_t h, int32_t n, const int32_t *keep) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && !keep)) return fail(TLM_E_BADARG, "bad output series flags");
+  for (int i = 0; i < n; i++)
+    if (keep[i] != 0 && keep[i] != 1) return fail(TLM_E_BADARG, "output series flag %d is not 0 or 1", i + 1);
+  m->out_keep.assign(keep, keep + n);
+  return TLM_OK;
+}
+
+int tlm_gpu_set_volume_dft(int64_t h, int32_t n, const double *freq, const int32_t *component,
+                           const int32_t *first_step, const int32_t *last_step, const int32_t *interval,
+                           const int32_t *ptr, const int32_t *out_cells) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && (!freq || !component || !first_step || !last_step || !interval || !ptr || !out_cells)))
+    return fail(TLM_E_BADARG, "bad output volume arguments");
+  for (int v = 0; v < n; v++)
+    if (ptr[v] < 0 || ptr[v + 1] < ptr[v]) return fail(TLM_E_BADARG, "output volume cell pointers must be non-decreasing");
+  m->vdft_freq.assign(freq, freq + n);
+  m->vdft_gate.resize((size_t)n * 4);
+  for (int v = 0; v < n; v++) {
+    m->vdft_gate[(size_t)v * 4 + 0] = first_step[v];
+    m->vdft_gate[(size_t)v * 4 + 1] = last_step[v];
+    m->vdft_gate[(size_t)v * 4 + 2] = interval[v];
+    m->vdft_gate[(size_t)v * 4 + 3] = component[v];
+  }
+  m->vdft_ptr.assign(ptr, ptr + (n ? n + 1 : 0));
+  const int ne = n ? ptr[n] : 0;
+  m->vdft_out.assign(out_cells, out_cells + ne);
+  return TLM_OK;
+}
+
+int tlm_gpu_fetch_volume_dft(int64_t h, double *out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
+  if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
+  if (!m->vdft_entries) return TLM_OK;
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(out, m->vdft_acc.p, (size_t)m->vdft_entries * 2 * sizeof(double), cudaMemcpyDeviceToHost));
+  return TLM_OK;
+}
+
 int tlm_gpu_set_small_to_zero(int64_t h, int32_t n_small, double small) {
   Mesh *m = get(h);
   if (!m) return fail(TLM_E_BADARG, "bad handle");
@@ -1542,9 +1661,9 @@ int tlm_gpu_fetch_cell_output(int64_t h, int32_t first, int32_t n, double *out) 
   if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
   if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
   if (first < 1 || n < 0 || first + n - 1 >= m->next_step) return fail(TLM_E_BADARG, "steps not yet computed");
-  if (m->n_out_cells == 0 || n == 0) return TLM_OK;
+  if (m->n_hist == 0 || n == 0) return TLM_OK;
   CK(cudaStreamSynchronize(m->stream));
-  const size_t row = (size_t)m->n_out_cells * 6;
+  const size_t row = (size_t)m->n_hist * 6;
   CK(cudaMemcpy(out, (double *)m->cell_out.p + (size_t)(first - 1) * row, (size_t)n * row * sizeof(double),
                 cudaMemcpyDeviceToHost));
   return TLM_OK;
@@ -1914,6 +2033,14 @@ int batch_step(Batch *b, bool dry) {
     b->last_launches++;
   }
   if (side && (rc = b->side.end(b->stream))) return rc;
+  for (int i : b->active) {  // frequency output volumes of the members that have them
+    Mesh *m = get(b->handles[i]);
+    if (m && m->vdft_entries) {
+      const tlm::VolDftDev vd = vol_dft_dev(m);
+      tlm::tlm_volume_dft_kernel<<<(vd.n_entries + 255) / 256, 256, 0, b->stream>>>(vd, (const int *)m->d_base.p, 0);
+      b->last_launches++;
+    }
+  }
   if (b->n_faceb) { tlm::tlm_face_batch_kernel<T><<<b->n_faceb, 128, 0, b->stream>>>(bd, 0); b->last_launches++; }
   for (int i : b->active) {  // outer-boundary Huygens surfaces of the members that have them
     Mesh *m = get(b->handles[i]);

@@ -125,11 +125,30 @@ struct MeshDev {
   const double *exc_field;  // [n_timesteps][n_exc][9]
   const int8_t *exc_type;   // [n_exc][6]
   int n_exc;
-  double *cell_out;         // [n_timesteps][n_out][6]
-  int n_out;
+  double *cell_out;         // [n_timesteps][n_hist][6]: outputs that keep a time series
+  double *cell_cur;         // [n_out][6]: every output cell's fields at the current step
+  const int *out_hist;      // [n_out]: slot in cell_out, or -1 (no time series)
+  int n_out, n_hist;
   double dl, dt;
   const int *d_base;        // device step counter (1-based step of relative step 0)
 };
+
+// cell_output_field(out_no, 1:6) of step t (output_points.F90:463-612):
+// every output cell writes its current-step row, which the volume outputs
+// read; an output that keeps a time series (a probe) also writes row t of
+// its series.
+template <typename T>
+__device__ __forceinline__ void store_cell_out(const MeshDev<T> &m, int t, int out_no, const double (&f)[6]) {
+  double *cur = m.cell_cur + (size_t)out_no * 6;
+#pragma unroll
+  for (int c = 0; c < 6; c++) cur[c] = f[c];
+  const int h = m.out_hist[out_no];
+  if (h >= 0) {
+    double *row = m.cell_out + ((size_t)(t - 1) * m.n_hist + h) * 6;
+#pragma unroll
+    for (int c = 0; c < 6; c++) row[c] = f[c];
+  }
+}
 
 template <typename T, int VEC> struct VecT;
 template <> struct VecT<float, 4> { using type = float4; };
@@ -235,7 +254,7 @@ __device__ __forceinline__ void free_space_cell(const T *inc, T *out) {
 // ---------------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par, int out_no, const T *inc_in, T *out,
-                                      double *cell_out_row, const typename PmlTypes<T>::state (&st)[kPmlState]) {
+                                      int t, const typename PmlTypes<T>::state (&st)[kPmlState]) {
   using A = typename PmlTypes<T>::arith;
   using ST = typename PmlTypes<T>::state;
   // FP64: literal scatter_PML.F90 arithmetic.  FP32: currents (and the
@@ -282,21 +301,26 @@ __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par,
   Pn[0] = V[Vznx] + V[Vzpx]; Pn[1] = V[Vynx] + V[Vypx];
   Pn[2] = V[Vxny] + V[Vxpy]; Pn[3] = V[Vzny] + V[Vzpy];
   Pn[4] = V[Vynz] + V[Vypz]; Pn[5] = V[Vxnz] + V[Vxpz];
-  const A Vx_sh = ax * (-(last_P[0] + last_P[1]) / A(2) + Csy * (Pn[0] + last_P[0]) + Csz * (Pn[1] + last_P[1]) +
-                        Csy_sz * last_Vxt);
-  const A Vy_sh = ay * (-(last_P[2] + last_P[3]) / A(2) + Csz * (Pn[2] + last_P[2]) + Csx * (Pn[3] + last_P[3]) +
-                        Csz_sx * last_Vyt);
-  const A Vz_sh = az * (-(last_P[4] + last_P[5]) / A(2) + Csx * (Pn[4] + last_P[4]) + Csy * (Pn[5] + last_P[5]) +
-                        Csx_sy * last_Vzt);
+  // The recursions that end in the reported fields (Vxt.., Ixt..) fuse
+  // their multiply-adds explicitly, in the reference's association order,
+  // so the rounding does not depend on the compiler's choices (and the
+  // FP32 kernel fits 96 registers without a spill).
+  static_assert(sizeof(A) == 8, "the PML recursion runs in FP64");
+  const A Vx_sh = __dmul_rn(ax, __fma_rn(Csy_sz, last_Vxt, __fma_rn(Csz, Pn[1] + last_P[1],
+                                         __fma_rn(Csy, Pn[0] + last_P[0], -(last_P[0] + last_P[1]) / A(2)))));
+  const A Vy_sh = __dmul_rn(ay, __fma_rn(Csz_sx, last_Vyt, __fma_rn(Csx, Pn[3] + last_P[3],
+                                         __fma_rn(Csz, Pn[2] + last_P[2], -(last_P[2] + last_P[3]) / A(2)))));
+  const A Vz_sh = __dmul_rn(az, __fma_rn(Csx_sy, last_Vzt, __fma_rn(Csy, Pn[5] + last_P[5],
+                                         __fma_rn(Csx, Pn[4] + last_P[4], -(last_P[4] + last_P[5]) / A(2)))));
   // STAGE 6
-  const A Vxt = ax * Vx + Vx_sh, Vyt = ay * Vy + Vy_sh, Vzt = az * Vz + Vz_sh;
+  const A Vxt = __fma_rn(ax, Vx, Vx_sh), Vyt = __fma_rn(ay, Vy, Vy_sh), Vzt = __fma_rn(az, Vz, Vz_sh);
   // STAGE 7a (output cells only)
   A Ixt = A(0), Iyt = A(0), Izt = A(0);
   if (out_no >= 0) {
     ST *X = m.pml_ixt + (size_t)out_no * 3;
-    Ixt = ax * (Ix - last_Ix + Csx2 * (Ix + last_Ix) + Csy_sz * X[0]);
-    Iyt = ay * (Iy - last_Iy + Csy2 * (Iy + last_Iy) + Csz_sx * X[1]);
-    Izt = az * (Iz - last_Iz + Csz2 * (Iz + last_Iz) + Csx_sy * X[2]);
+    Ixt = __dmul_rn(ax, __fma_rn(Csy_sz, A(X[0]), __fma_rn(Csx2, Ix + last_Ix, Ix - last_Ix)));
+    Iyt = __dmul_rn(ay, __fma_rn(Csz_sx, A(X[1]), __fma_rn(Csy2, Iy + last_Iy, Iy - last_Iy)));
+    Izt = __dmul_rn(az, __fma_rn(Csx_sy, A(X[2]), __fma_rn(Csz2, Iz + last_Iz, Iz - last_Iz)));
     X[0] = ST(Ixt); X[1] = ST(Iyt); X[2] = ST(Izt);
   }
   // STAGE 7
@@ -340,9 +364,10 @@ __device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par,
   // STAGE 12: output
   if (out_no >= 0) {
     const double dl = m.dl;
-    cell_out_row[0] = -double(Vxt) / dl; cell_out_row[1] = -double(Vyt) / dl; cell_out_row[2] = -double(Vzt) / dl;
     const double hs = sizeof(T) == 8 ? dl : dl * kZ0;  // FP32 carries Z0*I
-    cell_out_row[3] = double(Ixt) / hs; cell_out_row[4] = double(Iyt) / hs; cell_out_row[5] = double(Izt) / hs;
+    const double f[6] = {-double(Vxt) / dl, -double(Vyt) / dl, -double(Vzt) / dl,
+                         double(Ixt) / hs,  double(Iyt) / hs,  double(Izt) / hs};
+    store_cell_out(m, t, out_no, f);
   }
 }
 
@@ -470,9 +495,8 @@ __device__ __forceinline__ void special_cell(const MeshDev<T> &m, int s, int4 re
   if (flags & SP_OUT) {
     // scatter.F90:465-480
     const double dl = m.dl;
-    double *f = m.cell_out + ((size_t)(t - 1) * m.n_out + rec.w) * 6;
-    f[0] = -Vx / dl; f[1] = -Vy / dl; f[2] = -Vz / dl;
-    f[3] = Ix / dl; f[4] = Iy / dl; f[5] = Iz / dl;
+    const double f[6] = {-Vx / dl, -Vy / dl, -Vz / dl, Ix / dl, Iy / dl, Iz / dl};
+    store_cell_out(m, t, rec.w, f);
   }
   if (type == 3) {
     // filter update, scatter.F90:483-515; store taps w(0..order-1)
@@ -1231,8 +1255,7 @@ __device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl,
       if (e.x < s) lo = mid + 1; else hi = mid - 1;
     }
   }
-  double *row = (out_no >= 0) ? m.cell_out + ((size_t)(t - 1) * m.n_out + out_no) * 6 : nullptr;
-  pml_cell<T>(m, s, par, out_no, ci, co, row, st);
+  pml_cell<T>(m, s, par, out_no, ci, co, t, st);
 #pragma unroll
   for (int p = 0; p < 12; p++) __stcs(out + p * P + idx, co[p]);
   if (x == 0) {
@@ -1433,10 +1456,9 @@ __device__ __forceinline__ void pml_material_body(const MeshDev<T> &m, const Pmm
   }
   // STAGE 12: output
   if (ps.w >= 0) {
-    double *row = m.cell_out + ((size_t)(t - 1) * m.n_out + ps.w) * 6;
     const double dl = m.dl;
-    row[0] = -Vt[0] / dl; row[1] = -Vt[1] / dl; row[2] = -Vt[2] / dl;
-    row[3] = It[0] / dl; row[4] = It[1] / dl; row[5] = It[2] / dl;
+    const double f[6] = {-Vt[0] / dl, -Vt[1] / dl, -Vt[2] / dl, It[0] / dl, It[1] / dl, It[2] / dl};
+    store_cell_out(m, t, ps.w, f);
   }
   // STAGE 13: half-cell loss on the scattered pulses, then the pulses leave
   R[Vynx] = R[Vynx] * ex[1]; R[Vypx] = R[Vypx] * ex[1];
@@ -1713,6 +1735,36 @@ __device__ __forceinline__ void face_body(const MeshDev<T> &m, const FaceDev &fd
 // ---------------------------------------------------------------------------
 // FP64 DFT accumulation, frequency_output_surfaces.F90:343-410
 // ---------------------------------------------------------------------------
+// Frequency-domain output volumes, frequency_output_volumes.F90:309-390:
+// on the output steps of a volume (get_output_flag, output.F90:564-598:
+// first <= t <= last and (t - first) mod interval == 0),
+//   value(cell) += cell_output_field(cell, component) * exp(-j 2 pi f time),
+// time = (timestep-1) dt, the time of the cell outputs.  One thread per
+// (volume, cell) entry; it reads the current-step row of its output cell.
+struct VolDftDev {
+  int n_entries, n_vol;
+  const int2 *entry;       // (volume, output cell 0-based)
+  const int4 *gate;        // per volume: (first, last, interval, component 1..6)
+  const double2 *phasor;   // [n_timesteps][n_vol]: exp(-j 2 pi f (timestep-1) dt)
+  const double *cell_cur;  // [n_out][6]
+  double2 *acc;            // [n_entries]
+};
+
+__global__ void tlm_volume_dft_kernel(const VolDftDev d, const int *d_base, int rel_step) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.n_entries) return;
+  const int t = *d_base + rel_step;
+  const int2 e = d.entry[k];
+  const int4 g = d.gate[e.x];
+  if (t < g.x || t > g.y || (t - g.x) % g.z != 0) return;
+  const double v = d.cell_cur[(size_t)e.y * 6 + (g.w - 1)];
+  const double2 p = d.phasor[(size_t)(t - 1) * d.n_vol + e.x];
+  double2 a = d.acc[k];
+  a.x = a.x + v * p.x;
+  a.y = a.y + v * p.y;
+  d.acc[k] = a;
+}
+
 struct DftDev {
   int n_entries, n_dft;
   const int4 *entry;        // (surface, out face index, face code 1..6, component 1..9)
@@ -1820,14 +1872,14 @@ struct BatchDev {
 // Blocks ahead of the running one whose PML data the batched kernel prefetches.
 constexpr int kPmlBatchPrefetch = 1200;
 
-// The batched PML kernel (one more indirection per block) spills 68 bytes
-// at 5 blocks; at 4 (128 registers, no spill) C4 runs 0.7 % faster.
-#ifndef TLM_PML_BATCH_MIN_BLOCKS_FP32
-#define TLM_PML_BATCH_MIN_BLOCKS_FP32 4
-#endif
-
+// The batched PML kernel has the solo kernel's register budget: compiled
+// for a different budget, the compiler fused some FP64 multiply-adds of the
+// PML update differently, and in FP32 (where those values are rounded
+// before they reach the links but reported unrounded) a few reported PML
+// fields came out one rounding apart from the solo run.  With the same
+// budget the two agree bit for bit.
 template <typename T>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? TLM_PML_BATCH_MIN_BLOCKS_FP32 : TLM_PML_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? TLM_PML_MIN_BLOCKS_FP32 : TLM_PML_MIN_BLOCKS)
     tlm_pml_batch_kernel(const BatchDev<T> b, int rel_step) {
   if (threadIdx.x == 0 && blockIdx.x + kPmlBatchPrefetch < b.n_pml_blocks) {
     const int2 f = b.pml_blocks[blockIdx.x + kPmlBatchPrefetch];  // (mesh, first cell)

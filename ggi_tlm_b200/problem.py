@@ -482,6 +482,34 @@ class DFTSurface:
 
 
 @dataclass
+class FrequencyOutputVolume:
+    """Frequency-domain output volume (OUTPUT/frequency_output_volumes.F90):
+    the cells of a region (Block or Sphere), optionally only every
+    ``every``-th cell per axis counted from the region's lowest cell
+    (frequency_output_volume_output_every, :58-108), one field component
+    Ex..Hz, a list of frequencies, and the output steps first..last every
+    ``interval`` (output.F90:564-598; last None = the final step)."""
+
+    region: object
+    frequencies: Sequence[float]
+    component: str
+    first_step: int = 1
+    last_step: Optional[int] = None
+    interval: int = 1
+    every: int = 1
+
+    def mask(self, spec: "ProblemSpec") -> np.ndarray:
+        m = _region_mask(spec, self.region)
+        if self.every > 1 and m.any():
+            z, y, x = np.nonzero(m)
+            keep = (((x - x.min()) % self.every == 0) & ((y - y.min()) % self.every == 0) &
+                    ((z - z.min()) % self.every == 0))
+            m = np.zeros_like(m)
+            m[z[keep], y[keep], x[keep]] = True
+        return m
+
+
+@dataclass
 class ProblemSpec:
     nx: int
     ny: int
@@ -501,6 +529,7 @@ class ProblemSpec:
     outputs: List[OutputPoint] = field(default_factory=list)
     dft_surfaces: List[DFTSurface] = field(default_factory=list)
     far_field_surfaces: List["FarFieldSurface"] = field(default_factory=list)
+    frequency_output_volumes: List[FrequencyOutputVolume] = field(default_factory=list)
     reduced_c: float = 1.0
     # set_small_to_zero packet (read_small_to_zero.F90:55-59): (n_small_to_zero, small_to_zero_value)
     small_to_zero: Optional[Tuple[int, float]] = None
@@ -692,6 +721,16 @@ def build_tables(spec: ProblemSpec) -> dict:
     for op in centre_outs:
         i, j, k = op.cell
         cell_out[k - 1, j - 1, i - 1] = True
+    point_out = cell_out.copy()  # output points keep a time series; volume cells need only the current step
+    vol_masks = []
+    for fv in spec.frequency_output_volumes:
+        if COMPONENTS.get(fv.component, 0) not in range(1, 7):
+            raise ValueError("a frequency output volume records Ex..Hz")
+        if fv.interval < 1 or fv.every < 1:
+            raise ValueError("frequency output volume interval and cell spacing must be >= 1")
+        vm = fv.mask(spec)
+        vol_masks.append(vm)
+        cell_out |= vm
     if np.any(in_pml & cell_exc):
         raise UnsupportedFeature("Excitation intersects PML")  # set_update_codes.F90:347-354
     special = (cell_mat != 0) | in_pml | cell_exc | cell_out
@@ -968,6 +1007,23 @@ def build_tables(spec: ProblemSpec) -> dict:
         [out_number[(o.cell[2] - 1) * nx * ny + (o.cell[1] - 1) * nx + o.cell[0] - 1] for o in centre_outs],
         dtype=np.int32)
     tables["out_comp"] = np.array([COMPONENTS[o.component] for o in centre_outs], dtype=np.int32)
+    tables["out_keep"] = point_out.reshape(-1)[cell_out.reshape(-1)].astype(np.int32)
+    # frequency output volumes: one reference volume entry per frequency
+    vf, vc, v0, v1, vi, vptr, vout = [], [], [], [], [], [0], []
+    for fv, vm in zip(spec.frequency_output_volumes, vol_masks):
+        cells = out_number[vm.reshape(-1)]  # traversal order
+        for fr in fv.frequencies:
+            vf.append(fr)
+            vc.append(COMPONENTS[fv.component])
+            v0.append(fv.first_step)
+            v1.append(nsteps if fv.last_step is None else fv.last_step)
+            vi.append(fv.interval)
+            vout.extend(int(c) for c in cells)
+            vptr.append(len(vout))
+    tables.update(n_vdft=len(vf), vdft_freq=np.array(vf, dtype=np.float64), vdft_comp=np.array(vc, dtype=np.int32),
+                  vdft_first=np.array(v0, dtype=np.int32), vdft_last=np.array(v1, dtype=np.int32),
+                  vdft_interval=np.array(vi, dtype=np.int32), vdft_cell_ptr=np.array(vptr, dtype=np.int32),
+                  vdft_cell_out=np.array(vout, dtype=np.int32))
 
     # DFT surfaces: one reference surface entry per frequency
     freqs, comps, ptr, fo, fs = [], [], [0], [], []
@@ -1005,7 +1061,12 @@ def build_tables(spec: ProblemSpec) -> dict:
 
 def probe_series(tables: dict, cell_out: np.ndarray) -> np.ndarray:
     """Pick the output-point time series from cell_output_field snapshots
-    (output_points.F90:463-612): cell_out is [steps, n_out_cells, 6]."""
+    (output_points.F90:463-612): cell_out is [steps, n_out_cells, 6], or
+    [steps, n_kept, 6] with only the output cells that keep a series."""
     idx = tables["out_cell"] - 1
+    keep = tables.get("out_keep")
+    if keep is not None and cell_out.shape[1] != int(tables["n_out_cells"]):
+        slot = np.cumsum(np.asarray(keep)) - 1
+        idx = slot[idx]
     comp = tables["out_comp"] - 1
     return cell_out[:, idx, comp].T.copy()  # [n_points, steps]

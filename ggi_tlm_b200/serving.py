@@ -71,7 +71,10 @@ def footprint_bytes(t: dict, precision: int = capi.TLM_PRECISION_FP32) -> int:
     pml = int(t["n_pml_cells"]) * (18 * esz + 10) + int(t.get("n_pml_material_cells", 0)) * (66 * 8 + 24)
     special = int(t["n_special"]) * 32 + (ny * px + 31) // 32 * nz * 8
     filt = int(t["n_special"]) * 0 + 6 * 8 * 8 * int((np.asarray(t["sp_material"]) > 0).sum())
-    outs = int(t["n_out_cells"]) * 6 * 8 * n + int(t["n_exc_cells"]) * 9 * 8 * n
+    kept = int(np.sum(t["out_keep"])) if "out_keep" in t else int(t["n_out_cells"])
+    outs = kept * 6 * 8 * n + int(t["n_out_cells"]) * 6 * 8 + int(t["n_exc_cells"]) * 9 * 8 * n
+    if int(t.get("n_vdft", 0)):
+        outs += int(t["vdft_cell_ptr"][-1]) * (16 + 8) + int(t["n_vdft"]) * 16 * n
     dft = int(t["dft_face_ptr"][-1]) * 16 + int(t["n_dft"]) * 16 * n if int(t["n_dft"]) else 0
     return int(links + pml + special + filt + outs + dft + (1 << 20))
 

@@ -166,6 +166,29 @@ int tlm_gpu_set_face_outputs(int64_t handle, int32_t n_points, const int32_t *fa
    step (SRC/TLM_SOLVER/scatter.F90:465-480, scatter_PML.F90 STAGE 12). */
 int tlm_gpu_set_outputs(int64_t handle, int32_t n_out_cells);
 
+/* Which output cells keep a time series: keep[i] = 1 for output cell i+1
+   when its cell_output_field rows are read back step by step (the output
+   points, SRC/OUTPUT/output_points.F90:463-612), 0 when only volume outputs
+   read it.  Without this call every output cell keeps one.  No counterpart
+   in the reference, which writes output points to file every step and
+   keeps no history. */
+int tlm_gpu_set_output_series(int64_t handle, int32_t n_out_cells, const int32_t *keep);
+
+/* Frequency output volumes (SRC/OUTPUT/frequency_output_volumes.F90:35-390),
+   one entry per volume and frequency as frequency_output_volume(:):
+   frequency, field component 1..6 (Ex..Hz), first_timestep, last_timestep
+   and timestep_interval (SRC/OUTPUT/output.F90:564-598), and a CSR list
+   (cell_ptr[n_volumes+1]) of the 1-based output cell numbers of the
+   volume's cells (cell_output_field_number_list).  On each output step
+   value += cell_output_field(cell, component) exp(-j 2 pi f (timestep-1) dt). */
+int tlm_gpu_set_volume_dft(int64_t handle, int32_t n_volumes, const double *frequency, const int32_t *component,
+                           const int32_t *first_step, const int32_t *last_step, const int32_t *interval,
+                           const int32_t *cell_ptr, const int32_t *cell_out);
+
+/* Frequency output volume values per volume cell in set_volume_dft order,
+   (re, im) pairs: frequency_output_volume(:)%value(:). */
+int tlm_gpu_fetch_volume_dft(int64_t handle, double *out);
+
 /* Frequency-domain output surfaces (one entry per frequency, as
    frequency_output_surface(:) in SRC/OUTPUT/frequency_output_surfaces.F90:
    297-421): frequency, field component (1..6 E/H, 7..9 J=nxH), and a CSR
@@ -209,8 +232,9 @@ int tlm_gpu_run(int64_t handle, int32_t first_step, int32_t n_steps);
 /* Block until all work of the handle has finished. */
 int tlm_gpu_synchronize(int64_t handle);
 
-/* cell_output_field snapshots of steps first..first+n-1:
-   out[n][n_out_cells][6] doubles. */
+/* cell_output_field snapshots of steps first..first+n-1 of the output
+   cells that keep a time series (all of them unless set_output_series
+   says otherwise), in output-number order: out[n][n_kept][6] doubles. */
 int tlm_gpu_fetch_cell_output(int64_t handle, int32_t first_step, int32_t n_steps, double *out);
 
 /* Face output point values of steps first..first+n-1: out[n][n_points]

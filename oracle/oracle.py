@@ -194,3 +194,30 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+
+def volume_dft(t: dict, cell_out: np.ndarray) -> np.ndarray:
+    """Frequency output volumes, restating cell_output_frequency_output_volumes
+    (OUTPUT/frequency_output_volumes.F90:309-390) over the oracle's
+    cell_output_field history cell_out [steps, n_out_cells, 6] (from
+    ``Oracle.run``): on every step that get_output_flag (OUTPUT/output.F90:
+    564-598) accepts, value(cell) = value(cell) + field * exp(-j*2*pi*f*time)
+    with time = (timestep-1)*dt (TLM_SOLVER/run_TLM.F90:240-243, before the
+    half step).  Returns the values [entries] in volume then cell order."""
+    n = int(t.get("n_vdft", 0))
+    ptr = t["vdft_cell_ptr"]
+    out = []
+    for v in range(n):
+        cells = np.asarray(t["vdft_cell_out"][ptr[v]:ptr[v + 1]], dtype=np.int64) - 1
+        comp = int(t["vdft_comp"][v]) - 1
+        first, last, every = int(t["vdft_first"][v]), int(t["vdft_last"][v]), int(t["vdft_interval"][v])
+        f = float(t["vdft_freq"][v])
+        acc = np.zeros(len(cells), dtype=np.complex128)
+        for timestep in range(1, cell_out.shape[0] + 1):
+            if timestep < first or timestep > last or (timestep - first) % every != 0:
+                continue
+            time = (timestep - 1) * t["dt"]
+            ejwt = np.exp(-1j * 2.0 * np.pi * f * time)
+            acc = acc + cell_out[timestep - 1, cells, comp] * ejwt
+        out.append(acc)
+    return np.concatenate(out) if out else np.zeros(0, dtype=np.complex128)
