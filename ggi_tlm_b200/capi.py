@@ -41,7 +41,20 @@ EXPORTS = [
     "tlm_gpu_set_face_outputs", "tlm_gpu_fetch_face_output", "tlm_gpu_set_outer_huygens",
     "tlm_gpu_set_far_field", "tlm_gpu_fetch_far_field", "tlm_gpu_pool_release", "tlm_gpu_pool_cached_bytes",
     "tlm_gpu_prepare", "tlm_gpu_set_output_series", "tlm_gpu_set_volume_dft", "tlm_gpu_fetch_volume_dft",
+    "tlm_gpu_set_output_surfaces", "tlm_gpu_fetch_output_surfaces",
 ]
+
+
+def output_surface_shapes(t: dict) -> list:
+    """(n_output_steps, n_faces) of each time-domain output surface: the
+    steps first..min(last, n_timesteps) every interval."""
+    res = []
+    ptr = t.get("osurf_face_ptr", [0])
+    for k in range(int(t.get("n_osurf", 0))):
+        first, last, every = int(t["osurf_first"][k]), int(t["osurf_last"][k]), int(t["osurf_interval"][k])
+        hi = min(last, int(t["n_timesteps"]))
+        res.append(((hi - first) // every + 1 if hi >= first else 0, int(ptr[k + 1] - ptr[k])))
+    return res
 
 
 class TLMError(RuntimeError):
@@ -94,6 +107,8 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_output_series": [i64, i32, _i32p],
         "tlm_gpu_set_volume_dft": [i64, i32, _f64p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p],
         "tlm_gpu_fetch_volume_dft": [i64, _f64p],
+        "tlm_gpu_set_output_surfaces": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p],
+        "tlm_gpu_fetch_output_surfaces": [i64, _f64p],
         "tlm_gpu_set_small_to_zero": [i64, i32, C.c_double],
         "tlm_gpu_set_dft": [i64, i32, _f64p, _i32p, _i32p, _i32p, _i32p],
         "tlm_gpu_run": [i64, i32, i32],
@@ -232,6 +247,10 @@ class GpuMesh:
             vd = [_f64(t["vdft_freq"]), _i32(t["vdft_comp"]), _i32(t["vdft_first"]), _i32(t["vdft_last"]),
                   _i32(t["vdft_interval"]), _i32(t["vdft_cell_ptr"]), _i32(t["vdft_cell_out"])]
             _check(lib.tlm_gpu_set_volume_dft(self.h, int(t["n_vdft"]), *[_p(x) for x in vd]))
+        if int(t.get("n_osurf", 0)):
+            os_ = [_i32(t[k]) for k in ("osurf_comp", "osurf_first", "osurf_last", "osurf_interval", "osurf_both",
+                                        "osurf_face_ptr", "osurf_face_out", "osurf_face_code")]
+            _check(lib.tlm_gpu_set_output_surfaces(self.h, int(t["n_osurf"]), *[_p(x) for x in os_]))
         if int(t["n_dft"]):
             df = [_f64(t["dft_freq"]), _i32(t["dft_comp"]), _i32(t["dft_face_ptr"]), _i32(t["dft_face_out"]),
                   _i32(t["dft_face_side"])]
@@ -315,6 +334,20 @@ class GpuMesh:
         _check(_lib.tlm_gpu_fetch_far_field(self.h, out.ctypes.data_as(_f64p)))
         v = out[: 12 * n].reshape(n, 6, 2)
         return v[..., 0] + 1j * v[..., 1]
+
+    def output_surfaces(self) -> list:
+        """Time-domain output surface values: one array [n_output_steps,
+        n_faces] per surface (rows of steps not run yet are zero)."""
+        t = self.t
+        shapes = output_surface_shapes(t)
+        total = sum(a * b for a, b in shapes)
+        out = np.zeros(max(total, 1))
+        _check(_lib.tlm_gpu_fetch_output_surfaces(self.h, out.ctypes.data_as(_f64p)))
+        res, off = [], 0
+        for a, b in shapes:
+            res.append(out[off:off + a * b].reshape(a, b).copy())
+            off += a * b
+        return res
 
     def volume_dft(self) -> np.ndarray:
         """Frequency output volume values [entries] complex, in the tables'

@@ -266,6 +266,11 @@ struct Mesh {
   std::vector<int32_t> vdft_gate;    // 4 per volume: first, last, interval, component
   std::vector<int32_t> vdft_ptr, vdft_out;
   int vdft_entries = 0;
+  std::vector<int32_t> osurf_gate;   // time-domain output surfaces: 5 per surface (first, last, interval,
+                                     // component, both sides)
+  std::vector<int32_t> osurf_ptr, osurf_fout, osurf_fcode;
+  int osurf_entries = 0;
+  size_t osurf_hist_len = 0;
   int n_dft = 0;
   std::vector<double> dft_freq;
   std::vector<int32_t> dft_comp, dft_ptr, dft_fout, dft_fcode;
@@ -275,7 +280,7 @@ struct Mesh {
       cell_out, faces, face_io, face_hs, value_face, face_field, dft_entry, dft_phasor, dft_acc, d_base,
       pmm_pos, pmm_parmat, pmm_state, pmm_sigma, face_src, fpt_field_d, fpt_type_d, fprobe, fprobe_rec,
       ohs_face, ohs_offset, ff_entry, ff_phasor, ff_acc, cell_cur, out_hist, vdft_entry, vdft_gate_d, vdft_phasor,
-      vdft_acc;
+      vdft_acc, osurf_entry, osurf_pos, osurf_dev, osurf_hist;
   int n_pt_rows = 0;
   int n_pmm = 0;  // PML cells inside a volume material
   int n_filt = 0, filt_eo = 0, filt_mo = 0;
@@ -444,6 +449,23 @@ tlm::FarFieldDev far_field_dev(Mesh *m) {
 
 tlm::FaceProbeDev face_probe_dev(Mesh *m) {
   return tlm::FaceProbeDev{(const int4 *)m->fprobe.p, (double *)m->fprobe_rec.p, (int)m->fpr_face.size()};
+}
+
+tlm::OutSurfDev out_surf_dev(Mesh *m) {
+  tlm::OutSurfDev d{};
+  d.n_entries = m->osurf_entries;
+  d.entry = (const int2 *)m->osurf_entry.p;
+  d.pos = (const int2 *)m->osurf_pos.p;
+  d.surf = (const tlm::OSurfDev *)m->osurf_dev.p;
+  d.face_field = (const double *)m->face_field.p;
+  d.hist = (double *)m->osurf_hist.p;
+  return d;
+}
+
+// Output steps of a surface within 1..n_steps: first..last every interval.
+long long osurf_steps(int first, int last, int interval, int n_steps) {
+  const int hi = std::min(last, n_steps);
+  return hi >= first ? (long long)(hi - first) / interval + 1 : 0;
 }
 
 tlm::VolDftDev vol_dft_dev(Mesh *m) {
@@ -943,6 +965,38 @@ int finalize(Mesh *m) {
     if ((rc = dalloc(m, m->ff_acc, ent.size() * 6 * sizeof(double2)))) return rc;
     CK(cudaMemset(m->ff_acc.p, 0, m->ff_acc.bytes));
   }
+  // ---- time-domain output surfaces
+  {
+    const int ns = (int)m->osurf_gate.size() / 5;
+    std::vector<int2> ent, pos;
+    std::vector<tlm::OSurfDev> sd(std::max(ns, 1));
+    size_t off = 0;
+    for (int v = 0; v < ns; v++) {
+      const int *g = &m->osurf_gate[(size_t)v * 5];
+      const int comp = g[3];
+      if (!((comp >= 1 && comp <= 9) || (comp >= 13 && comp <= 15)))
+        return fail(TLM_E_BADARG, "output surface %d: component %d is not E, H, J or a magnitude", v + 1, comp);
+      if (g[0] < 1 || g[2] < 1) return fail(TLM_E_BADARG, "output surface %d: first step and interval must be >= 1", v + 1);
+      if (g[4] != 0 && g[4] != 1) return fail(TLM_E_BADARG, "output surface %d: both-sides flag must be 0 or 1", v + 1);
+      const int nf = m->osurf_ptr[v + 1] - m->osurf_ptr[v];
+      sd[v] = tlm::OSurfDev{int4{g[0], g[1], g[2], comp}, g[4], nf, (long long)off};
+      for (int k = m->osurf_ptr[v]; k < m->osurf_ptr[v + 1]; k++) {
+        const int fo = m->osurf_fout[k], code = m->osurf_fcode[k];
+        if (fo < 1 || fo > m->n_out_faces) return fail(TLM_E_BADARG, "output surface %d: face output number out of range", v + 1);
+        if (code < 1 || code > 6) return fail(TLM_E_BADARG, "output surface %d: face code out of range", v + 1);
+        ent.push_back(int2{v, fo - 1});
+        pos.push_back(int2{code, k - m->osurf_ptr[v]});
+      }
+      off += (size_t)osurf_steps(g[0], g[1], g[2], nsteps) * (size_t)nf;
+    }
+    m->osurf_entries = (int)ent.size();
+    m->osurf_hist_len = off;
+    if (ent.empty()) { ent.resize(1); pos.resize(1); }
+    if ((rc = upload(m, m->osurf_entry, ent)) || (rc = upload(m, m->osurf_pos, pos)) || (rc = upload(m, m->osurf_dev, sd)))
+      return rc;
+    if ((rc = dalloc(m, m->osurf_hist, std::max<size_t>(off, 1) * sizeof(double)))) return rc;
+    CK(cudaMemset(m->osurf_hist.p, 0, m->osurf_hist.bytes));
+  }
   if ((rc = dalloc(m, m->d_base, sizeof(int)))) return rc;
   if ((rc = dalloc(m, m->d_err, sizeof(int)))) return rc;
   CK(cudaMemset(m->d_err.p, 0, sizeof(int)));
@@ -1161,6 +1215,11 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
     if (!m->fpr_face.empty()) {
       const tlm::FaceProbeDev pd = face_probe_dev(m);
       tlm::tlm_face_probe_kernel<<<(pd.n + 127) / 128, 128, 0, m->stream>>>(pd, fd.face_field, md.d_base, k);
+      m->last_launches++;
+    }
+    if (m->osurf_entries) {  // reads the face fields the face kernel wrote
+      const tlm::OutSurfDev od = out_surf_dev(m);
+      tlm::tlm_output_surface_kernel<<<(od.n_entries + 255) / 256, 256, 0, m->stream>>>(od, md.d_base, k);
       m->last_launches++;
     }
     if (m->hs_outer && m->hs_n) {
@@ -1507,6 +1566,41 @@ int tlm_gpu_set_volume_dft(int64_t h, int32_t n, const double *freq, const int32
   m->vdft_ptr.assign(ptr, ptr + (n ? n + 1 : 0));
   const int ne = n ? ptr[n] : 0;
   m->vdft_out.assign(out_cells, out_cells + ne);
+  return TLM_OK;
+}
+
+int tlm_gpu_set_output_surfaces(int64_t h, int32_t n, const int32_t *component, const int32_t *first_step,
+                                const int32_t *last_step, const int32_t *interval, const int32_t *both_sides,
+                                const int32_t *face_ptr, const int32_t *face_out, const int32_t *face_code) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && (!component || !first_step || !last_step || !interval || !both_sides || !face_ptr ||
+                      !face_out || !face_code)))
+    return fail(TLM_E_BADARG, "bad output surface arguments");
+  for (int v = 0; v < n; v++)
+    if (face_ptr[v] < 0 || face_ptr[v + 1] < face_ptr[v])
+      return fail(TLM_E_BADARG, "output surface face pointers must be non-decreasing");
+  m->osurf_gate.resize((size_t)n * 5);
+  for (int v = 0; v < n; v++) {
+    int *g = &m->osurf_gate[(size_t)v * 5];
+    g[0] = first_step[v]; g[1] = last_step[v]; g[2] = interval[v]; g[3] = component[v]; g[4] = both_sides[v];
+  }
+  m->osurf_ptr.assign(face_ptr, face_ptr + (n ? n + 1 : 0));
+  const int ne = n ? face_ptr[n] : 0;
+  m->osurf_fout.assign(face_out, face_out + ne);
+  m->osurf_fcode.assign(face_code, face_code + ne);
+  return TLM_OK;
+}
+
+int tlm_gpu_fetch_output_surfaces(int64_t h, double *out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
+  if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
+  if (!m->osurf_hist_len) return TLM_OK;
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(out, m->osurf_hist.p, m->osurf_hist_len * sizeof(double), cudaMemcpyDeviceToHost));
   return TLM_OK;
 }
 
@@ -2063,6 +2157,15 @@ int batch_step(Batch *b, bool dry) {
       const tlm::FaceProbeDev pd = face_probe_dev(m);
       tlm::tlm_face_probe_kernel<<<(pd.n + 127) / 128, 128, 0, b->stream>>>(pd, (const double *)m->face_field.p,
                                                                              (const int *)m->d_base.p, 0);
+      b->last_launches++;
+    }
+  }
+  for (int i : b->active) {  // time-domain output surfaces of the members that have them
+    Mesh *m = get(b->handles[i]);
+    if (m && m->osurf_entries) {
+      const tlm::OutSurfDev od = out_surf_dev(m);
+      tlm::tlm_output_surface_kernel<<<(od.n_entries + 255) / 256, 256, 0, b->stream>>>(od, (const int *)m->d_base.p,
+                                                                                        0);
       b->last_launches++;
     }
   }

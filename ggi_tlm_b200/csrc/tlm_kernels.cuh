@@ -1735,6 +1735,66 @@ __device__ __forceinline__ void face_body(const MeshDev<T> &m, const FaceDev &fd
 // ---------------------------------------------------------------------------
 // FP64 DFT accumulation, frequency_output_surfaces.F90:343-410
 // ---------------------------------------------------------------------------
+// Time-domain output surfaces, face_output_surfaces (output_surfaces.F90:
+// 601-760): on the output steps of a surface (first..last every interval)
+// each face's value is written to row (t - first) / interval of the
+// surface's history.  The face code (after the side flip) gives the side of
+// face_output_field (1 on a min face, 2 on a max face) and the normal n
+// (+1 on a min face, -1 on a max face); with both_sides the two sides are
+// field and field2.  Components: 1..6 field(c); 7..9 J = n x H(field) -
+// n x H(field2); 13 |E|, 14 |H| of field; 15 |J|.
+struct OSurfDev {
+  int4 gate;      // first, last, interval, component
+  int both, n_faces;
+  long long off;  // first value of the surface in the history
+};
+struct OutSurfDev {
+  int n_entries;
+  const int2 *entry;         // (surface, face output 0-based)
+  const int2 *pos;           // (face code 1..6, index within the surface)
+  const OSurfDev *surf;
+  const double *face_field;  // [n_out_faces][2][6]
+  double *hist;
+};
+
+__global__ void tlm_output_surface_kernel(const OutSurfDev d, const int *d_base, int rel_step) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.n_entries) return;
+  const int t = *d_base + rel_step;
+  const int2 e = d.entry[k];
+  const OSurfDev sf = d.surf[e.x];
+  const int4 g = sf.gate;
+  if (t < g.x || t > g.y || (t - g.x) % g.z != 0) return;
+  const int2 q = d.pos[k];
+  const int code = q.x;
+  const int side = code <= 3 ? 0 : 1;
+  double normx = 0.0, normy = 0.0, normz = 0.0;
+  if (code == 1) normx = 1.0; else if (code == 4) normx = -1.0;
+  else if (code == 2) normy = 1.0; else if (code == 5) normy = -1.0;
+  else if (code == 3) normz = 1.0; else normz = -1.0;
+  const double *ff = d.face_field + (size_t)e.y * 12;
+  double f[6], f2[6];
+#pragma unroll
+  for (int c = 0; c < 6; c++) {
+    f[c] = sf.both ? ff[c] : ff[side * 6 + c];
+    f2[c] = sf.both ? ff[6 + c] : 0.0;
+  }
+  // field indices: Ex Ey Ez Hx Hy Hz = 0..5
+  const double Jsx = (normy * f[5] - normz * f[4]) - (normy * f2[5] - normz * f2[4]);
+  const double Jsy = (normz * f[3] - normx * f[5]) - (normz * f2[3] - normx * f2[5]);
+  const double Jsz = (normx * f[4] - normy * f[3]) - (normx * f2[4] - normy * f2[3]);
+  double v;
+  const int comp = g.w;
+  if (comp <= 6) v = f[comp - 1];
+  else if (comp == 7) v = Jsx;
+  else if (comp == 8) v = Jsy;
+  else if (comp == 9) v = Jsz;
+  else if (comp == 13) v = sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+  else if (comp == 14) v = sqrt(f[3] * f[3] + f[4] * f[4] + f[5] * f[5]);
+  else v = sqrt(Jsx * Jsx + Jsy * Jsy + Jsz * Jsz);
+  d.hist[sf.off + (long long)((t - g.x) / g.z) * sf.n_faces + q.y] = v;
+}
+
 // Frequency-domain output volumes, frequency_output_volumes.F90:309-390:
 // on the output steps of a volume (get_output_flag, output.F90:564-598:
 // first <= t <= last and (t - first) mod interval == 0),

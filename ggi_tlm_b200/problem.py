@@ -461,6 +461,38 @@ class FarFieldSurface:
         return _huygens_patches(g)
 
 
+# output surface components: E, H, J = n x H, and the magnitudes
+# |E|, |H|, |J| (TLM_MODULES/TLM_Modules.F90:178-180)
+SURFACE_COMPONENTS = {"Ex": 1, "Ey": 2, "Ez": 3, "Hx": 4, "Hy": 5, "Hz": 6, "Jx": 7, "Jy": 8, "Jz": 9,
+                      "Em": 13, "Hm": 14, "Jm": 15}
+
+
+@dataclass
+class OutputSurface:
+    """A time-domain output surface (Output_surface packet,
+    OUTPUT/output_surfaces.F90): on the output steps first..last every
+    ``interval`` (last None = the final step), the value of ``component``
+    (SURFACE_COMPONENTS) on every face of a closed box of cells ``box`` or a
+    planar patch ``plane``, faces as for FarFieldSurface (``side`` -1 samples
+    the other side of each face, output_on_outward_normal false).  With
+    ``both_sides`` (output_average_of_both_sides) J is n x H of side 1 minus
+    n x H of side 2; other components read side 1."""
+
+    component: str
+    box: Optional[Tuple[Tuple[int, int], Tuple[int, int], Tuple[int, int]]] = None
+    plane: Optional[Tuple[int, int, Tuple[int, int], Tuple[int, int]]] = None
+    side: int = 1
+    both_sides: bool = False
+    first_step: int = 1
+    last_step: Optional[int] = None
+    interval: int = 1
+
+    def faces(self) -> List[Tuple[Tuple[int, int, int], int]]:
+        if (self.box is None) == (self.plane is None):
+            raise ValueError("an output surface is either a box or a plane")
+        return FarFieldSurface([], self.box, self.plane, self.side).faces()
+
+
 @dataclass
 class OutputPoint:
     cell: Tuple[int, int, int]
@@ -530,6 +562,7 @@ class ProblemSpec:
     dft_surfaces: List[DFTSurface] = field(default_factory=list)
     far_field_surfaces: List["FarFieldSurface"] = field(default_factory=list)
     frequency_output_volumes: List[FrequencyOutputVolume] = field(default_factory=list)
+    output_surfaces: List[OutputSurface] = field(default_factory=list)
     reduced_c: float = 1.0
     # set_small_to_zero packet (read_small_to_zero.F90:55-59): (n_small_to_zero, small_to_zero_value)
     small_to_zero: Optional[Tuple[int, float]] = None
@@ -881,6 +914,10 @@ def build_tables(spec: ProblemSpec) -> dict:
     for fl in ff_faces:
         for c, code in fl:
             face_out[connect_key(c, code)] = True
+    os_faces = [os_.faces() for os_ in spec.output_surfaces]
+    for fl in os_faces:
+        for c, code in fl:
+            face_out[connect_key(c, code)] = True
     for ds in spec.dft_surfaces:
         for f in _plane_faces(ds.axis, ds.index, ds.r0, ds.r1):
             face_out[(f, ds.axis)] = True
@@ -1049,6 +1086,26 @@ def build_tables(spec: ProblemSpec) -> dict:
                 ffo.append(fout_num[connect_key(c, code)])
                 ffc.append(code)
             fptr.append(len(ffo))
+    # time-domain output surfaces
+    oc, o0, o1, oi, ob, optr, ofo, ofc = [], [], [], [], [], [0], [], []
+    for os_, fl in zip(spec.output_surfaces, os_faces):
+        if os_.component not in SURFACE_COMPONENTS:
+            raise ValueError(f"output surface component {os_.component!r}")
+        if os_.first_step < 1 or os_.interval < 1:
+            raise ValueError("output surface first step and interval must be >= 1")
+        oc.append(SURFACE_COMPONENTS[os_.component])
+        o0.append(os_.first_step)
+        o1.append(nsteps if os_.last_step is None else os_.last_step)
+        oi.append(os_.interval)
+        ob.append(1 if os_.both_sides else 0)
+        for c, code in fl:
+            ofo.append(fout_num[connect_key(c, code)])
+            ofc.append(code)
+        optr.append(len(ofo))
+    tables.update(n_osurf=len(oc), osurf_comp=np.array(oc, dtype=np.int32), osurf_first=np.array(o0, dtype=np.int32),
+                  osurf_last=np.array(o1, dtype=np.int32), osurf_interval=np.array(oi, dtype=np.int32),
+                  osurf_both=np.array(ob, dtype=np.int32), osurf_face_ptr=np.array(optr, dtype=np.int32),
+                  osurf_face_out=np.array(ofo, dtype=np.int32), osurf_face_code=np.array(ofc, dtype=np.int32))
     tables.update(n_ff=len(ffreq), ff_freq=np.array(ffreq, dtype=np.float64),
                   ff_face_ptr=np.array(fptr, dtype=np.int32), ff_face_out=np.array(ffo, dtype=np.int32),
                   ff_face_code=np.array(ffc, dtype=np.int32))

@@ -189,6 +189,23 @@ int tlm_gpu_set_volume_dft(int64_t handle, int32_t n_volumes, const double *freq
    (re, im) pairs: frequency_output_volume(:)%value(:). */
 int tlm_gpu_fetch_volume_dft(int64_t handle, double *out);
 
+/* Time-domain output surfaces (SRC/OUTPUT/output_surfaces.F90:42-760), as
+   output_surfaces(:): field component (1..6 Ex..Hz, 7..9 Jx..Jz = n x H,
+   13 |E|, 14 |H|, 15 |J|), first_timestep, last_timestep, timestep_interval,
+   output_average_of_both_sides (0/1), and a CSR list (face_ptr[n+1]) of the
+   surface's faces: output face number and face code 1..6 after the side
+   flip (output_on_outward_normal).  On each output step every face's
+   value (face_output_surfaces, :601-760) is recorded. */
+int tlm_gpu_set_output_surfaces(int64_t handle, int32_t n_surfaces, const int32_t *component,
+                                const int32_t *first_step, const int32_t *last_step, const int32_t *interval,
+                                const int32_t *both_sides, const int32_t *face_ptr, const int32_t *face_out,
+                                const int32_t *face_code);
+
+/* Output surface values, surface after surface, each [n_output_steps][n_faces]
+   doubles, n_output_steps = the steps first..min(last, n_timesteps) every
+   interval; rows of steps not run yet are zero. */
+int tlm_gpu_fetch_output_surfaces(int64_t handle, double *out);
+
 /* Frequency-domain output surfaces (one entry per frequency, as
    frequency_output_surface(:) in SRC/OUTPUT/frequency_output_surfaces.F90:
    297-421): frequency, field component (1..6 E/H, 7..9 J=nxH), and a CSR

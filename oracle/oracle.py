@@ -221,3 +221,65 @@ def volume_dft(t: dict, cell_out: np.ndarray) -> np.ndarray:
             acc = acc + cell_out[timestep - 1, cells, comp] * ejwt
         out.append(acc)
     return np.concatenate(out) if out else np.zeros(0, dtype=np.complex128)
+
+
+def output_surfaces(t: dict) -> list:
+    """Time-domain output surfaces, restating face_output_surfaces
+    (OUTPUT/output_surfaces.F90:601-760) on the oracle's face fields: the
+    oracle runs the whole solve with face output points added on both sides
+    (1, 2) and all six components of every surface face, and each output
+    step (get_output_flag, OUTPUT/output.F90:564-598) takes, per face,
+    field = side of the face code (or side 1 and field2 = side 2 with both
+    sides), the normal +1 on a min face and -1 on a max face, and the
+    component: E/H, J = n x H(field) - n x H(field2), |E|, |H| or |J|.
+    Returns one array [n_output_steps, n_faces] per surface."""
+    ns = int(t.get("n_osurf", 0))
+    if not ns:
+        return []
+    ptr = t["osurf_face_ptr"]
+    fo = np.asarray(t["osurf_face_out"], dtype=np.int32)
+    n0 = int(t.get("n_face_probes", 0))
+    add_face = np.repeat(fo, 12)
+    add_side = np.tile(np.repeat(np.array([1, 2], dtype=np.int32), 6), len(fo))
+    add_comp = np.tile(np.arange(1, 7, dtype=np.int32), 2 * len(fo))
+    t2 = dict(t)
+    t2["n_face_probes"] = n0 + len(add_face)
+    t2["fprobe_face"] = np.concatenate([np.asarray(t.get("fprobe_face", []), dtype=np.int32), add_face])
+    t2["fprobe_side"] = np.concatenate([np.asarray(t.get("fprobe_side", []), dtype=np.int32), add_side])
+    t2["fprobe_comp"] = np.concatenate([np.asarray(t.get("fprobe_comp", []), dtype=np.int32), add_comp])
+    o = Oracle(t2)
+    o.run(int(t["n_timesteps"]))
+    vals = o.face_probes()[n0:].reshape(len(fo), 2, 6, -1)  # [face, side, comp, step]
+    res = []
+    for k in range(ns):
+        faces = range(ptr[k], ptr[k + 1])
+        comp, both = int(t["osurf_comp"][k]), bool(t["osurf_both"][k])
+        first, last, every = int(t["osurf_first"][k]), int(t["osurf_last"][k]), int(t["osurf_interval"][k])
+        steps = [s for s in range(first, min(last, int(t["n_timesteps"])) + 1) if (s - first) % every == 0]
+        out = np.zeros((len(steps), len(faces)))
+        for j, f in enumerate(faces):
+            code = int(t["osurf_face_code"][f])
+            side = 0 if code <= 3 else 1
+            n = [0.0, 0.0, 0.0]
+            n[(code - 1) % 3] = 1.0 if code <= 3 else -1.0
+            normx, normy, normz = n
+            for r, s in enumerate(steps):
+                field = vals[f, 0 if both else side, :, s - 1]
+                field2 = vals[f, 1, :, s - 1] if both else np.zeros(6)
+                Ex, Ey, Ez, Hx, Hy, Hz = field
+                Jsx = (normy * Hz - normz * Hy) - (normy * field2[5] - normz * field2[4])
+                Jsy = (normz * Hx - normx * Hz) - (normz * field2[3] - normx * field2[5])
+                Jsz = (normx * Hy - normy * Hx) - (normx * field2[4] - normy * field2[3])
+                if comp <= 6:
+                    v = field[comp - 1]
+                elif comp in (7, 8, 9):
+                    v = (Jsx, Jsy, Jsz)[comp - 7]
+                elif comp == 13:
+                    v = np.sqrt(Ex ** 2 + Ey ** 2 + Ez ** 2)
+                elif comp == 14:
+                    v = np.sqrt(Hx ** 2 + Hy ** 2 + Hz ** 2)
+                else:
+                    v = np.sqrt(Jsx ** 2 + Jsy ** 2 + Jsz ** 2)
+                out[r, j] = v
+        res.append(out)
+    return res
