@@ -41,7 +41,7 @@ EXPORTS = [
     "tlm_gpu_set_face_outputs", "tlm_gpu_fetch_face_output", "tlm_gpu_set_outer_huygens",
     "tlm_gpu_set_far_field", "tlm_gpu_fetch_far_field", "tlm_gpu_pool_release", "tlm_gpu_pool_cached_bytes",
     "tlm_gpu_prepare", "tlm_gpu_set_output_series", "tlm_gpu_set_volume_dft", "tlm_gpu_fetch_volume_dft",
-    "tlm_gpu_set_output_surfaces", "tlm_gpu_fetch_output_surfaces",
+    "tlm_gpu_set_output_surfaces", "tlm_gpu_fetch_output_surfaces", "tlm_gpu_set_rcs", "tlm_gpu_fetch_rcs",
 ]
 
 
@@ -109,6 +109,8 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_fetch_volume_dft": [i64, _f64p],
         "tlm_gpu_set_output_surfaces": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p],
         "tlm_gpu_fetch_output_surfaces": [i64, _f64p],
+        "tlm_gpu_set_rcs": [i64, C.c_double, C.c_double, i32, i32, i32, i32, _i32p, _i32p, _f64p],
+        "tlm_gpu_fetch_rcs": [i64, _f64p],
         "tlm_gpu_set_small_to_zero": [i64, i32, C.c_double],
         "tlm_gpu_set_dft": [i64, i32, _f64p, _i32p, _i32p, _i32p, _i32p],
         "tlm_gpu_run": [i64, i32, i32],
@@ -247,6 +249,10 @@ class GpuMesh:
             vd = [_f64(t["vdft_freq"]), _i32(t["vdft_comp"]), _i32(t["vdft_first"]), _i32(t["vdft_last"]),
                   _i32(t["vdft_interval"]), _i32(t["vdft_cell_ptr"]), _i32(t["vdft_cell_out"])]
             _check(lib.tlm_gpu_set_volume_dft(self.h, int(t["n_vdft"]), *[_p(x) for x in vd]))
+        if int(t.get("rcs_on", 0)):
+            rf, rc_, rd = _i32(t["rcs_face_out"]), _i32(t["rcs_face_code"]), _f64(t["rcs_face_dist"])
+            _check(lib.tlm_gpu_set_rcs(self.h, float(t["rcs_theta"]), float(t["rcs_phi"]), int(t["rcs_npc"]),
+                                       int(t["rcs_points"]), int(t["rcs_offset"]), len(rf), _p(rf), _p(rc_), _p(rd)))
         if int(t.get("n_osurf", 0)):
             os_ = [_i32(t[k]) for k in ("osurf_comp", "osurf_first", "osurf_last", "osurf_interval", "osurf_both",
                                         "osurf_face_ptr", "osurf_face_out", "osurf_face_code")]
@@ -334,6 +340,13 @@ class GpuMesh:
         _check(_lib.tlm_gpu_fetch_far_field(self.h, out.ctypes.data_as(_f64p)))
         v = out[: 12 * n].reshape(n, 6, 2)
         return v[..., 0] + 1j * v[..., 1]
+
+    def rcs(self) -> np.ndarray:
+        """RCS far-field arrays [4, n_points]: Etheta, Ephi, Htheta, Hphi."""
+        n = int(self.t["rcs_points"]) if int(self.t.get("rcs_on", 0)) else 0
+        out = np.zeros(max(4 * n, 4))
+        _check(_lib.tlm_gpu_fetch_rcs(self.h, out.ctypes.data_as(_f64p)))
+        return out[: 4 * n].reshape(4, n)
 
     def output_surfaces(self) -> list:
         """Time-domain output surface values: one array [n_output_steps,

@@ -271,6 +271,11 @@ struct Mesh {
   std::vector<int32_t> osurf_ptr, osurf_fout, osurf_fcode;
   int osurf_entries = 0;
   size_t osurf_hist_len = 0;
+  bool rcs_on = false;               // the RCS surface (rcs_surface)
+  double rcs_theta = 0, rcs_phi = 0;
+  int rcs_npc = 2, rcs_points = 0, rcs_offset = 0;
+  std::vector<int32_t> rcs_fout, rcs_fcode;
+  std::vector<double> rcs_dist;
   int n_dft = 0;
   std::vector<double> dft_freq;
   std::vector<int32_t> dft_comp, dft_ptr, dft_fout, dft_fcode;
@@ -280,7 +285,7 @@ struct Mesh {
       cell_out, faces, face_io, face_hs, value_face, face_field, dft_entry, dft_phasor, dft_acc, d_base,
       pmm_pos, pmm_parmat, pmm_state, pmm_sigma, face_src, fpt_field_d, fpt_type_d, fprobe, fprobe_rec,
       ohs_face, ohs_offset, ff_entry, ff_phasor, ff_acc, cell_cur, out_hist, vdft_entry, vdft_gate_d, vdft_phasor,
-      vdft_acc, osurf_entry, osurf_pos, osurf_dev, osurf_hist;
+      vdft_acc, osurf_entry, osurf_pos, osurf_dev, osurf_hist, rcs_face, rcs_dist_d, rcs_tc0, rcs_acc;
   int n_pt_rows = 0;
   int n_pmm = 0;  // PML cells inside a volume material
   int n_filt = 0, filt_eo = 0, filt_mo = 0;
@@ -449,6 +454,25 @@ tlm::FarFieldDev far_field_dev(Mesh *m) {
 
 tlm::FaceProbeDev face_probe_dev(Mesh *m) {
   return tlm::FaceProbeDev{(const int4 *)m->fprobe.p, (double *)m->fprobe_rec.p, (int)m->fpr_face.size()};
+}
+
+tlm::RcsDev rcs_dev(Mesh *m) {
+  tlm::RcsDev d{};
+  d.n_faces = (int)m->rcs_fout.size();
+  d.n_points = m->rcs_points;
+  d.npc = m->rcs_npc;
+  d.offset = m->rcs_offset;
+  d.ct = cos(m->rcs_theta); d.st = sin(m->rcs_theta);
+  d.cp = cos(m->rcs_phi); d.sp = sin(m->rcs_phi);
+  d.dA = m->desc.dl * m->desc.dl;
+  d.four_pi = 4.0 * 3.141592653589793;
+  d.dl = m->desc.dl;
+  d.face = (const int2 *)m->rcs_face.p;
+  d.dist = (const double *)m->rcs_dist_d.p;
+  d.tc0 = (const double *)m->rcs_tc0.p;
+  d.face_field = (const double *)m->face_field.p;
+  d.acc = (double *)m->rcs_acc.p;
+  return d;
 }
 
 tlm::OutSurfDev out_surf_dev(Mesh *m) {
@@ -997,6 +1021,34 @@ int finalize(Mesh *m) {
     if ((rc = dalloc(m, m->osurf_hist, std::max<size_t>(off, 1) * sizeof(double)))) return rc;
     CK(cudaMemset(m->osurf_hist.p, 0, m->osurf_hist.bytes));
   }
+  // ---- RCS surface: faces sorted by K.x (then list order), time*c0 per step
+  if (m->rcs_on) {
+    const int nf = (int)m->rcs_fout.size();
+    std::vector<int> order(nf);
+    for (int i = 0; i < nf; i++) {
+      order[i] = i;
+      if (m->rcs_fout[i] < 1 || m->rcs_fout[i] > m->n_out_faces) return fail(TLM_E_BADARG, "RCS face output number out of range");
+      if (m->rcs_fcode[i] < 1 || m->rcs_fcode[i] > 6) return fail(TLM_E_BADARG, "RCS face code out of range");
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return m->rcs_dist[a] < m->rcs_dist[b]; });
+    std::vector<int2> fc(std::max(nf, 1));
+    std::vector<double> ds(std::max(nf, 1));
+    for (int k = 0; k < nf; k++) {
+      fc[k] = int2{m->rcs_fout[order[k]] - 1, m->rcs_fcode[order[k]]};
+      ds[k] = m->rcs_dist[order[k]];
+    }
+    std::vector<double> tc0(nsteps);
+    const double c0 = 2.99792458e8;  // CONSTANTS/constants.F90
+    for (int t = 0; t < nsteps; t++) {
+      double time = (double)t * D.dt;  // (timestep-1)*dt, then the half step of the face outputs
+      time = time + D.dt / 2.0;
+      tc0[t] = time * c0;
+    }
+    if ((rc = upload(m, m->rcs_face, fc)) || (rc = upload(m, m->rcs_dist_d, ds)) || (rc = upload(m, m->rcs_tc0, tc0)))
+      return rc;
+    if ((rc = dalloc(m, m->rcs_acc, (size_t)std::max(m->rcs_points, 1) * 4 * sizeof(double)))) return rc;
+    CK(cudaMemset(m->rcs_acc.p, 0, m->rcs_acc.bytes));
+  }
   if ((rc = dalloc(m, m->d_base, sizeof(int)))) return rc;
   if ((rc = dalloc(m, m->d_err, sizeof(int)))) return rc;
   CK(cudaMemset(m->d_err.p, 0, sizeof(int)));
@@ -1220,6 +1272,11 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
     if (m->osurf_entries) {  // reads the face fields the face kernel wrote
       const tlm::OutSurfDev od = out_surf_dev(m);
       tlm::tlm_output_surface_kernel<<<(od.n_entries + 255) / 256, 256, 0, m->stream>>>(od, md.d_base, k);
+      m->last_launches++;
+    }
+    if (m->rcs_on && !m->rcs_fout.empty()) {
+      const tlm::RcsDev rd = rcs_dev(m);
+      tlm::tlm_rcs_kernel<<<(rd.n_faces + 255) / 256, 256, 0, m->stream>>>(rd, md.d_base, k);
       m->last_launches++;
     }
     if (m->hs_outer && m->hs_n) {
@@ -1590,6 +1647,37 @@ int tlm_gpu_set_output_surfaces(int64_t h, int32_t n, const int32_t *component, 
   const int ne = n ? face_ptr[n] : 0;
   m->osurf_fout.assign(face_out, face_out + ne);
   m->osurf_fcode.assign(face_code, face_code + ne);
+  return TLM_OK;
+}
+
+int tlm_gpu_set_rcs(int64_t h, double theta, double phi, int32_t points_per_cell, int32_t n_points,
+                    int32_t point_offset, int32_t n_faces, const int32_t *face_out, const int32_t *face_code,
+                    const double *face_dist) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (points_per_cell < 1 || n_points < 1 || n_faces < 0 || (n_faces && (!face_out || !face_code || !face_dist)))
+    return fail(TLM_E_BADARG, "bad RCS surface arguments");
+  m->rcs_on = true;
+  m->rcs_theta = theta;
+  m->rcs_phi = phi;
+  m->rcs_npc = points_per_cell;
+  m->rcs_points = n_points;
+  m->rcs_offset = point_offset;
+  m->rcs_fout.assign(face_out, face_out + n_faces);
+  m->rcs_fcode.assign(face_code, face_code + n_faces);
+  m->rcs_dist.assign(face_dist, face_dist + n_faces);
+  return TLM_OK;
+}
+
+int tlm_gpu_fetch_rcs(int64_t h, double *out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
+  if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
+  if (!m->rcs_on) return TLM_OK;
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(out, m->rcs_acc.p, (size_t)m->rcs_points * 4 * sizeof(double), cudaMemcpyDeviceToHost));
   return TLM_OK;
 }
 
@@ -2157,6 +2245,14 @@ int batch_step(Batch *b, bool dry) {
       const tlm::FaceProbeDev pd = face_probe_dev(m);
       tlm::tlm_face_probe_kernel<<<(pd.n + 127) / 128, 128, 0, b->stream>>>(pd, (const double *)m->face_field.p,
                                                                              (const int *)m->d_base.p, 0);
+      b->last_launches++;
+    }
+  }
+  for (int i : b->active) {  // RCS surfaces of the members that have them
+    Mesh *m = get(b->handles[i]);
+    if (m && m->rcs_on && !m->rcs_fout.empty()) {
+      const tlm::RcsDev rd = rcs_dev(m);
+      tlm::tlm_rcs_kernel<<<(rd.n_faces + 255) / 256, 256, 0, b->stream>>>(rd, (const int *)m->d_base.p, 0);
       b->last_launches++;
     }
   }

@@ -1795,6 +1795,69 @@ __global__ void tlm_output_surface_kernel(const OutSurfDev d, const int *d_base,
   d.hist[sf.off + (long long)((t - g.x) / g.z) * sf.n_faces + q.y] = v;
 }
 
+// Time-domain far field for the RCS surface, face_output_rcs
+// (RCS_surfaces.F90:386-560).  Every step each face adds its contribution
+// to the far-field time bin
+//   point = INT(npc * (-(K.x) + time c0) / dl) - offset   (kept when 1..n_points),
+// time the face-output time (timestep-1) dt + dt/2, from its fields on its
+// side of face_output_field: Js = n x H, Ms = -(n x E), n = +1 on a min
+// face and -1 on a max face; N, L = (Js, Ms) projected on theta and phi
+// times dA / (4 pi); Etheta = -(Lphi + Z0 Ntheta), Ephi = Ltheta - Z0 Nphi,
+// Htheta = Nphi - Ltheta / Z0, Hphi = -(Ntheta + Lphi / Z0).
+// The host sorts the faces by K.x, so INT(...) does not increase along the
+// list and the faces of one bin form one run; the first face of each run
+// adds the run's contributions in list order.  The bin arithmetic is
+// rounded step by step (no contraction) so that it matches the oracle's.
+struct RcsDev {
+  int n_faces, n_points, npc, offset;
+  double ct, st, cp, sp, dA, four_pi, dl;
+  const int2 *face;          // (face output 0-based, face code 1..6), sorted by K.x
+  const double *dist;        // K.x of each face, ascending
+  const double *tc0;         // [n_timesteps]: time * c0 at the face outputs
+  const double *face_field;  // [n_out_faces][2][6]
+  double *acc;               // [4][n_points]: Etheta, Ephi, Htheta, Hphi
+};
+
+__device__ __forceinline__ int rcs_point(const RcsDev &d, int i, double tc0) {
+  const double a = __dadd_rn(-d.dist[i], tc0);
+  const double b = __ddiv_rn(__dmul_rn((double)d.npc, a), d.dl);
+  return (int)b - d.offset;  // INT truncates toward zero, as C does
+}
+
+__global__ void tlm_rcs_kernel(const RcsDev d, const int *d_base, int rel_step) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n_faces) return;
+  const int t = *d_base + rel_step;
+  const double tc0 = d.tc0[t - 1];
+  const int p = rcs_point(d, i, tc0);
+  if (i > 0 && rcs_point(d, i - 1, tc0) == p) return;  // not the first face of its run
+  if (p < 1 || p > d.n_points) return;
+  const size_t np = (size_t)d.n_points;
+  double et = d.acc[p - 1], ep = d.acc[np + p - 1], ht = d.acc[2 * np + p - 1], hp = d.acc[3 * np + p - 1];
+  for (int j = i; j < d.n_faces; j++) {
+    if (j > i && rcs_point(d, j, tc0) != p) break;
+    const int2 fc = d.face[j];
+    const int side = fc.y <= 3 ? 0 : 1;
+    double normx = 0.0, normy = 0.0, normz = 0.0;
+    if (fc.y == 1) normx = 1.0; else if (fc.y == 4) normx = -1.0;
+    else if (fc.y == 2) normy = 1.0; else if (fc.y == 5) normy = -1.0;
+    else if (fc.y == 3) normz = 1.0; else normz = -1.0;
+    const double *f = d.face_field + (size_t)fc.x * 12 + side * 6;
+    const double Jsx = normy * f[5] - normz * f[4], Jsy = normz * f[3] - normx * f[5], Jsz = normx * f[4] - normy * f[3];
+    const double Msx = -(normy * f[2] - normz * f[1]), Msy = -(normz * f[0] - normx * f[2]);
+    const double Msz = -(normx * f[1] - normy * f[0]);
+    const double Nt = (Jsx * d.ct * d.cp + Jsy * d.ct * d.sp - Jsz * d.st) * d.dA / d.four_pi;
+    const double Np = (-Jsx * d.sp + Jsy * d.cp) * d.dA / d.four_pi;
+    const double Lt = (Msx * d.ct * d.cp + Msy * d.ct * d.sp - Msz * d.st) * d.dA / d.four_pi;
+    const double Lp = (-Msx * d.sp + Msy * d.cp) * d.dA / d.four_pi;
+    et = et + (-(Lp + kZ0 * Nt));
+    ep = ep + (Lt - kZ0 * Np);
+    ht = ht + (Np - Lt / kZ0);
+    hp = hp + (-(Nt + Lp / kZ0));
+  }
+  d.acc[p - 1] = et; d.acc[np + p - 1] = ep; d.acc[2 * np + p - 1] = ht; d.acc[3 * np + p - 1] = hp;
+}
+
 // Frequency-domain output volumes, frequency_output_volumes.F90:309-390:
 // on the output steps of a volume (get_output_flag, output.F90:564-598:
 // first <= t <= last and (t - first) mod interval == 0),

@@ -494,6 +494,28 @@ class OutputSurface:
 
 
 @dataclass
+class RCSSurface:
+    """The RCS surface (RCS_surface packet, OUTPUT/RCS_surfaces.F90): the
+    faces of a closed box or planar patch as for FarFieldSurface, and the
+    far-field direction ``theta``, ``phi`` in degrees
+    (read_rcs_surface.F90:79-86 turns them into radians)."""
+
+    theta: float
+    phi: float
+    box: Optional[Tuple[Tuple[int, int], Tuple[int, int], Tuple[int, int]]] = None
+    plane: Optional[Tuple[int, int, Tuple[int, int], Tuple[int, int]]] = None
+    side: int = 1
+
+    def faces(self) -> List[Tuple[Tuple[int, int, int], int]]:
+        if (self.box is None) == (self.plane is None):
+            raise ValueError("an RCS surface is either a box or a plane")
+        return FarFieldSurface([], self.box, self.plane, self.side).faces()
+
+
+RCS_POINTS_PER_CELL = 2  # n_rcs_points_per_cell, TLM_MODULES/TLM_output_modules.F90:388
+
+
+@dataclass
 class OutputPoint:
     cell: Tuple[int, int, int]
     component: str
@@ -563,6 +585,7 @@ class ProblemSpec:
     far_field_surfaces: List["FarFieldSurface"] = field(default_factory=list)
     frequency_output_volumes: List[FrequencyOutputVolume] = field(default_factory=list)
     output_surfaces: List[OutputSurface] = field(default_factory=list)
+    rcs_surface: Optional[RCSSurface] = None
     reduced_c: float = 1.0
     # set_small_to_zero packet (read_small_to_zero.F90:55-59): (n_small_to_zero, small_to_zero_value)
     small_to_zero: Optional[Tuple[int, float]] = None
@@ -918,6 +941,9 @@ def build_tables(spec: ProblemSpec) -> dict:
     for fl in os_faces:
         for c, code in fl:
             face_out[connect_key(c, code)] = True
+    rcs_faces = spec.rcs_surface.faces() if spec.rcs_surface is not None else []
+    for c, code in rcs_faces:
+        face_out[connect_key(c, code)] = True
     for ds in spec.dft_surfaces:
         for f in _plane_faces(ds.axis, ds.index, ds.r0, ds.r1):
             face_out[(f, ds.axis)] = True
@@ -1106,6 +1132,32 @@ def build_tables(spec: ProblemSpec) -> dict:
                   osurf_last=np.array(o1, dtype=np.int32), osurf_interval=np.array(oi, dtype=np.int32),
                   osurf_both=np.array(ob, dtype=np.int32), osurf_face_ptr=np.array(optr, dtype=np.int32),
                   osurf_face_out=np.array(ofo, dtype=np.int32), osurf_face_code=np.array(ofc, dtype=np.int32))
+    # the RCS surface, initialise_rcs_surfaces (RCS_surfaces.F90:159-360)
+    if spec.rcs_surface is not None:
+        rs = spec.rcs_surface
+        theta, phi = (math.pi / 180.0) * rs.theta, (math.pi / 180.0) * rs.phi
+        K = (1.0 * math.sin(theta) * math.cos(phi), 1.0 * math.sin(theta) * math.sin(phi), 1.0 * math.cos(theta))
+        xmin0, ymin0, zmin0 = spec.origin
+        dist = []
+        for c, code in rcs_faces:
+            # get_cell_point_coordinate, general_mesh_subroutines.F90:84-140
+            off = [-0.5, -0.5, -0.5]
+            off[(code - 1) % 3] = -1.0 if code <= 3 else 0.0
+            x = xmin0 + c[0] * dl + dl * off[0]
+            y = ymin0 + c[1] * dl + dl * off[1]
+            z = zmin0 + c[2] * dl + dl * off[2]
+            dist.append(K[0] * x + K[1] * y + K[2] * z)
+        dmin, dmax = min(dist), max(dist)
+        period = (dmax - dmin) / C0 + nsteps * dt  # simulation_time = n_timesteps dt
+        distance = period * C0
+        tables.update(rcs_on=1, rcs_theta=theta, rcs_phi=phi, rcs_npc=RCS_POINTS_PER_CELL,
+                      rcs_points=int(RCS_POINTS_PER_CELL * distance / dl + 2),
+                      rcs_offset=int(RCS_POINTS_PER_CELL * dmin / dl - 1),
+                      rcs_face_out=np.array([fout_num[connect_key(c, code)] for c, code in rcs_faces], dtype=np.int32),
+                      rcs_face_code=np.array([code for _, code in rcs_faces], dtype=np.int32),
+                      rcs_face_dist=np.array(dist, dtype=np.float64))
+    else:
+        tables.update(rcs_on=0)
     tables.update(n_ff=len(ffreq), ff_freq=np.array(ffreq, dtype=np.float64),
                   ff_face_ptr=np.array(fptr, dtype=np.int32), ff_face_out=np.array(ffo, dtype=np.int32),
                   ff_face_code=np.array(ffc, dtype=np.int32))

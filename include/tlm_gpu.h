@@ -206,6 +206,22 @@ int tlm_gpu_set_output_surfaces(int64_t handle, int32_t n_surfaces, const int32_
    interval; rows of steps not run yet are zero. */
 int tlm_gpu_fetch_output_surfaces(int64_t handle, double *out);
 
+/* The RCS surface (SRC/OUTPUT/RCS_surfaces.F90:159-560, rcs_surface):
+   theta and phi in radians, n_rcs_points_per_cell, n_far_field_points and
+   far_field_point_offset as initialise_rcs_surfaces sets them, and the
+   surface's faces: output face number, face code 1..6 after the side flip
+   and K.x of the face point (get_cell_point_coordinate).  Every step each
+   face adds its far-field contribution to Etheta/Ephi/Htheta/Hphi at point
+   INT(n_rcs_points_per_cell ((time c0) - K.x) / dl) - far_field_point_offset,
+   time = (timestep-1) dt + dt/2; points outside 1..n_far_field_points are
+   dropped, as the reference drops them after its warning. */
+int tlm_gpu_set_rcs(int64_t handle, double theta, double phi, int32_t points_per_cell, int32_t n_points,
+                    int32_t point_offset, int32_t n_faces, const int32_t *face_out, const int32_t *face_code,
+                    const double *face_dist);
+
+/* RCS far-field arrays: Etheta, Ephi, Htheta, Hphi, each n_points doubles. */
+int tlm_gpu_fetch_rcs(int64_t handle, double *out);
+
 /* Frequency-domain output surfaces (one entry per frequency, as
    frequency_output_surface(:) in SRC/OUTPUT/frequency_output_surfaces.F90:
    297-421): frequency, field component (1..6 E/H, 7..9 J=nxH), and a CSR

@@ -8,6 +8,7 @@ GPU path consumes (ggi_tlm_b200.problem.build_tables).
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -283,3 +284,61 @@ def output_surfaces(t: dict) -> list:
                 out[r, j] = v
         res.append(out)
     return res
+
+
+def rcs(t: dict) -> np.ndarray:
+    """The RCS surface's time-domain far field, restating face_output_rcs
+    (OUTPUT/RCS_surfaces.F90:386-560) on the oracle's face fields: the oracle
+    runs the whole solve with face output points added on each RCS face's
+    side for all six components; every step, for every face in list order,
+    point = INT(n_rcs_points_per_cell * (-(K.x) + time*c0) / dl) - offset
+    with time = (timestep-1)*dt + dt/2, and when 1 <= point <= n_points the
+    face adds Etheta, Ephi, Htheta, Hphi there.  Returns [4, n_points]."""
+    if not int(t.get("rcs_on", 0)):
+        return np.zeros((4, 0))
+    fo = np.asarray(t["rcs_face_out"], dtype=np.int32)
+    codes = np.asarray(t["rcs_face_code"], dtype=np.int32)
+    sides = np.where(codes <= 3, 1, 2).astype(np.int32)
+    n0 = int(t.get("n_face_probes", 0))
+    t2 = dict(t)
+    t2["n_face_probes"] = n0 + 6 * len(fo)
+    t2["fprobe_face"] = np.concatenate([np.asarray(t.get("fprobe_face", []), dtype=np.int32), np.repeat(fo, 6)])
+    t2["fprobe_side"] = np.concatenate([np.asarray(t.get("fprobe_side", []), dtype=np.int32), np.repeat(sides, 6)])
+    t2["fprobe_comp"] = np.concatenate([np.asarray(t.get("fprobe_comp", []), dtype=np.int32),
+                                        np.tile(np.arange(1, 7, dtype=np.int32), len(fo))])
+    o = Oracle(t2)
+    o.run(int(t["n_timesteps"]))
+    vals = o.face_probes()[n0:].reshape(len(fo), 6, -1)  # [face, comp, step]
+    theta, phi = float(t["rcs_theta"]), float(t["rcs_phi"])
+    ct, st, cp, sp = math.cos(theta), math.sin(theta), math.cos(phi), math.sin(phi)
+    dl, dt = float(t["dl"]), float(t["dt"])
+    dA, four_pi = dl * dl, 4.0 * math.pi
+    npc, n_pts, offset = int(t["rcs_npc"]), int(t["rcs_points"]), int(t["rcs_offset"])
+    dist = np.asarray(t["rcs_face_dist"], dtype=np.float64)
+    acc = np.zeros((4, n_pts))
+    Z0 = 376.73031346177
+    for timestep in range(1, int(t["n_timesteps"]) + 1):
+        time = (timestep - 1) * dt
+        time = time + dt / 2.0
+        tc0 = time * 2.99792458e8
+        for f in range(len(fo)):
+            dm = -float(dist[f]) + tc0
+            point = int(float(npc) * dm / dl) - offset
+            if point < 1 or point > n_pts:
+                continue
+            code = int(codes[f])
+            n = [0.0, 0.0, 0.0]
+            n[(code - 1) % 3] = 1.0 if code <= 3 else -1.0
+            normx, normy, normz = n
+            Ex, Ey, Ez, Hx, Hy, Hz = (float(v) for v in vals[f, :, timestep - 1])
+            Jsx, Jsy, Jsz = normy * Hz - normz * Hy, normz * Hx - normx * Hz, normx * Hy - normy * Hx
+            Msx, Msy, Msz = -(normy * Ez - normz * Ey), -(normz * Ex - normx * Ez), -(normx * Ey - normy * Ex)
+            Nt = (Jsx * ct * cp + Jsy * ct * sp - Jsz * st) * dA / four_pi
+            Np = (-Jsx * sp + Jsy * cp) * dA / four_pi
+            Lt = (Msx * ct * cp + Msy * ct * sp - Msz * st) * dA / four_pi
+            Lp = (-Msx * sp + Msy * cp) * dA / four_pi
+            acc[0, point - 1] += -(Lp + Z0 * Nt)
+            acc[1, point - 1] += Lt - Z0 * Np
+            acc[2, point - 1] += Np - Lt / Z0
+            acc[3, point - 1] += -(Nt + Lp / Z0)
+    return acc
