@@ -42,6 +42,7 @@ EXPORTS = [
     "tlm_gpu_set_far_field", "tlm_gpu_fetch_far_field", "tlm_gpu_pool_release", "tlm_gpu_pool_cached_bytes",
     "tlm_gpu_prepare", "tlm_gpu_set_output_series", "tlm_gpu_set_volume_dft", "tlm_gpu_fetch_volume_dft",
     "tlm_gpu_set_output_surfaces", "tlm_gpu_fetch_output_surfaces", "tlm_gpu_set_rcs", "tlm_gpu_fetch_rcs",
+    "tlm_gpu_set_output_volumes", "tlm_gpu_fetch_output_volumes",
 ]
 
 
@@ -111,6 +112,8 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_fetch_output_surfaces": [i64, _f64p],
         "tlm_gpu_set_rcs": [i64, C.c_double, C.c_double, i32, i32, i32, i32, _i32p, _i32p, _f64p],
         "tlm_gpu_fetch_rcs": [i64, _f64p],
+        "tlm_gpu_set_output_volumes": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p],
+        "tlm_gpu_fetch_output_volumes": [i64, _f64p],
         "tlm_gpu_set_small_to_zero": [i64, i32, C.c_double],
         "tlm_gpu_set_dft": [i64, i32, _f64p, _i32p, _i32p, _i32p, _i32p],
         "tlm_gpu_run": [i64, i32, i32],
@@ -249,6 +252,10 @@ class GpuMesh:
             vd = [_f64(t["vdft_freq"]), _i32(t["vdft_comp"]), _i32(t["vdft_first"]), _i32(t["vdft_last"]),
                   _i32(t["vdft_interval"]), _i32(t["vdft_cell_ptr"]), _i32(t["vdft_cell_out"])]
             _check(lib.tlm_gpu_set_volume_dft(self.h, int(t["n_vdft"]), *[_p(x) for x in vd]))
+        if int(t.get("n_ovol", 0)):
+            ov = [_i32(t[k]) for k in ("ovol_kind", "ovol_comp", "ovol_first", "ovol_last", "ovol_interval",
+                                       "ovol_cell_ptr", "ovol_cell_out")]
+            _check(lib.tlm_gpu_set_output_volumes(self.h, int(t["n_ovol"]), *[_p(x) for x in ov]))
         if int(t.get("rcs_on", 0)):
             rf, rc_, rd = _i32(t["rcs_face_out"]), _i32(t["rcs_face_code"]), _f64(t["rcs_face_dist"])
             _check(lib.tlm_gpu_set_rcs(self.h, float(t["rcs_theta"]), float(t["rcs_phi"]), int(t["rcs_npc"]),
@@ -340,6 +347,27 @@ class GpuMesh:
         _check(_lib.tlm_gpu_fetch_far_field(self.h, out.ctypes.data_as(_f64p)))
         v = out[: 12 * n].reshape(n, 6, 2)
         return v[..., 0] + 1j * v[..., 1]
+
+    def output_volumes(self) -> list:
+        """Time-domain output volume values, one array per volume: [n_output_steps,
+        n_cells] for a "field" volume, [n_output_steps] for an average or a peak."""
+        t = self.t
+        shapes = []
+        ptr = t.get("ovol_cell_ptr", [0])
+        for k in range(int(t.get("n_ovol", 0))):
+            first, last, every = int(t["ovol_first"][k]), int(t["ovol_last"][k]), int(t["ovol_interval"][k])
+            hi = min(last, int(t["n_timesteps"]))
+            ns = (hi - first) // every + 1 if hi >= first else 0
+            shapes.append((ns, int(ptr[k + 1] - ptr[k])) if int(t["ovol_kind"][k]) == 0 else (ns,))
+        total = sum(int(np.prod(s)) for s in shapes)
+        out = np.zeros(max(total, 1))
+        _check(_lib.tlm_gpu_fetch_output_volumes(self.h, out.ctypes.data_as(_f64p)))
+        res, off = [], 0
+        for s in shapes:
+            n = int(np.prod(s))
+            res.append(out[off:off + n].reshape(s).copy())
+            off += n
+        return res
 
     def rcs(self) -> np.ndarray:
         """RCS far-field arrays [4, n_points]: Etheta, Ephi, Htheta, Hphi."""

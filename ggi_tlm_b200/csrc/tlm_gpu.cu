@@ -271,6 +271,10 @@ struct Mesh {
   std::vector<int32_t> osurf_ptr, osurf_fout, osurf_fcode;
   int osurf_entries = 0;
   size_t osurf_hist_len = 0;
+  std::vector<int32_t> ovol_gate;     // time-domain output volumes: 5 per volume (first, last, interval,
+                                     // component, kind)
+  std::vector<int32_t> ovol_ptr, ovol_out;
+  size_t ovol_hist_len = 0;
   bool rcs_on = false;               // the RCS surface (rcs_surface)
   double rcs_theta = 0, rcs_phi = 0;
   int rcs_npc = 2, rcs_points = 0, rcs_offset = 0;
@@ -285,7 +289,8 @@ struct Mesh {
       cell_out, faces, face_io, face_hs, value_face, face_field, dft_entry, dft_phasor, dft_acc, d_base,
       pmm_pos, pmm_parmat, pmm_state, pmm_sigma, face_src, fpt_field_d, fpt_type_d, fprobe, fprobe_rec,
       ohs_face, ohs_offset, ff_entry, ff_phasor, ff_acc, cell_cur, out_hist, vdft_entry, vdft_gate_d, vdft_phasor,
-      vdft_acc, osurf_entry, osurf_pos, osurf_dev, osurf_hist, rcs_face, rcs_dist_d, rcs_tc0, rcs_acc;
+      vdft_acc, osurf_entry, osurf_pos, osurf_dev, osurf_hist, rcs_face, rcs_dist_d, rcs_tc0, rcs_acc, ovol_dev,
+      ovol_cells, ovol_hist;
   int n_pt_rows = 0;
   int n_pmm = 0;  // PML cells inside a volume material
   int n_filt = 0, filt_eo = 0, filt_mo = 0;
@@ -454,6 +459,16 @@ tlm::FarFieldDev far_field_dev(Mesh *m) {
 
 tlm::FaceProbeDev face_probe_dev(Mesh *m) {
   return tlm::FaceProbeDev{(const int4 *)m->fprobe.p, (double *)m->fprobe_rec.p, (int)m->fpr_face.size()};
+}
+
+tlm::OutVolDev out_vol_dev(Mesh *m) {
+  tlm::OutVolDev d{};
+  d.n_vol = (int)m->ovol_gate.size() / 5;
+  d.vol = (const tlm::OVolDev *)m->ovol_dev.p;
+  d.cells = (const int *)m->ovol_cells.p;
+  d.cell_cur = (const double *)m->cell_cur.p;
+  d.hist = (double *)m->ovol_hist.p;
+  return d;
 }
 
 tlm::RcsDev rcs_dev(Mesh *m) {
@@ -1021,6 +1036,32 @@ int finalize(Mesh *m) {
     if ((rc = dalloc(m, m->osurf_hist, std::max<size_t>(off, 1) * sizeof(double)))) return rc;
     CK(cudaMemset(m->osurf_hist.p, 0, m->osurf_hist.bytes));
   }
+  // ---- time-domain output volumes
+  {
+    const int nv = (int)m->ovol_gate.size() / 5;
+    std::vector<tlm::OVolDev> vd(std::max(nv, 1));
+    std::vector<int> cells;
+    size_t off = 0;
+    for (int v = 0; v < nv; v++) {
+      const int *g = &m->ovol_gate[(size_t)v * 5];
+      if (g[3] < 1 || g[3] > 6) return fail(TLM_E_BADARG, "output volume %d: component %d is not Ex..Hz", v + 1, g[3]);
+      if (g[0] < 1 || g[2] < 1) return fail(TLM_E_BADARG, "output volume %d: first step and interval must be >= 1", v + 1);
+      if (g[4] < 0 || g[4] > 2) return fail(TLM_E_BADARG, "output volume %d: kind %d is not 0, 1 or 2", v + 1, g[4]);
+      const int nc = m->ovol_ptr[v + 1] - m->ovol_ptr[v];
+      vd[v] = tlm::OVolDev{int4{g[0], g[1], g[2], g[3]}, g[4], nc, (int)cells.size(), (long long)off};
+      for (int k = m->ovol_ptr[v]; k < m->ovol_ptr[v + 1]; k++) {
+        const int o = m->ovol_out[k];
+        if (o < 1 || o > m->n_out_cells) return fail(TLM_E_BADARG, "output volume %d: output cell %d out of range", v + 1, o);
+        cells.push_back(o - 1);
+      }
+      off += (size_t)osurf_steps(g[0], g[1], g[2], nsteps) * (size_t)(g[4] == 0 ? nc : 1);
+    }
+    m->ovol_hist_len = off;
+    if (cells.empty()) cells.resize(1);
+    if ((rc = upload(m, m->ovol_dev, vd)) || (rc = upload(m, m->ovol_cells, cells))) return rc;
+    if ((rc = dalloc(m, m->ovol_hist, std::max<size_t>(off, 1) * sizeof(double)))) return rc;
+    CK(cudaMemset(m->ovol_hist.p, 0, m->ovol_hist.bytes));
+  }
   // ---- RCS surface: faces sorted by K.x (then list order), time*c0 per step
   if (m->rcs_on) {
     const int nf = (int)m->rcs_fout.size();
@@ -1258,6 +1299,11 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
     if (m->vdft_entries) {  // reads the cell outputs this step's cell kernels wrote
       const tlm::VolDftDev vd = vol_dft_dev(m);
       tlm::tlm_volume_dft_kernel<<<(vd.n_entries + 255) / 256, 256, 0, m->stream>>>(vd, md.d_base, k);
+      m->last_launches++;
+    }
+    if (!m->ovol_gate.empty()) {  // likewise
+      const tlm::OutVolDev ov = out_vol_dev(m);
+      tlm::tlm_output_volume_kernel<<<ov.n_vol, tlm::kOutVolThreads, 0, m->stream>>>(ov, md.d_base, k);
       m->last_launches++;
     }
     if (fd.n_faces) {
@@ -1667,6 +1713,39 @@ int tlm_gpu_set_rcs(int64_t h, double theta, double phi, int32_t points_per_cell
   m->rcs_fout.assign(face_out, face_out + n_faces);
   m->rcs_fcode.assign(face_code, face_code + n_faces);
   m->rcs_dist.assign(face_dist, face_dist + n_faces);
+  return TLM_OK;
+}
+
+int tlm_gpu_set_output_volumes(int64_t h, int32_t n, const int32_t *kind, const int32_t *component,
+                               const int32_t *first_step, const int32_t *last_step, const int32_t *interval,
+                               const int32_t *cell_ptr, const int32_t *cell_out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && (!kind || !component || !first_step || !last_step || !interval || !cell_ptr || !cell_out)))
+    return fail(TLM_E_BADARG, "bad output volume arguments");
+  for (int v = 0; v < n; v++)
+    if (cell_ptr[v] < 0 || cell_ptr[v + 1] < cell_ptr[v])
+      return fail(TLM_E_BADARG, "output volume cell pointers must be non-decreasing");
+  m->ovol_gate.resize((size_t)n * 5);
+  for (int v = 0; v < n; v++) {
+    int *g = &m->ovol_gate[(size_t)v * 5];
+    g[0] = first_step[v]; g[1] = last_step[v]; g[2] = interval[v]; g[3] = component[v]; g[4] = kind[v];
+  }
+  m->ovol_ptr.assign(cell_ptr, cell_ptr + (n ? n + 1 : 0));
+  const int ne = n ? cell_ptr[n] : 0;
+  m->ovol_out.assign(cell_out, cell_out + ne);
+  return TLM_OK;
+}
+
+int tlm_gpu_fetch_output_volumes(int64_t h, double *out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
+  if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
+  if (!m->ovol_hist_len) return TLM_OK;
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(out, m->ovol_hist.p, m->ovol_hist_len * sizeof(double), cudaMemcpyDeviceToHost));
   return TLM_OK;
 }
 
@@ -2215,6 +2294,14 @@ int batch_step(Batch *b, bool dry) {
     b->last_launches++;
   }
   if (side && (rc = b->side.end(b->stream))) return rc;
+  for (int i : b->active) {  // time-domain output volumes of the members that have them
+    Mesh *m = get(b->handles[i]);
+    if (m && !m->ovol_gate.empty()) {
+      const tlm::OutVolDev ov = out_vol_dev(m);
+      tlm::tlm_output_volume_kernel<<<ov.n_vol, tlm::kOutVolThreads, 0, b->stream>>>(ov, (const int *)m->d_base.p, 0);
+      b->last_launches++;
+    }
+  }
   for (int i : b->active) {  // frequency output volumes of the members that have them
     Mesh *m = get(b->handles[i]);
     if (m && m->vdft_entries) {

@@ -1858,6 +1858,65 @@ __global__ void tlm_rcs_kernel(const RcsDev d, const int *d_base, int rel_step) 
   d.acc[p - 1] = et; d.acc[np + p - 1] = ep; d.acc[2 * np + p - 1] = ht; d.acc[3 * np + p - 1] = hp;
 }
 
+// Time-domain output volumes on their output steps (first..last every
+// interval), from the current-step cell output rows:
+//   kind 0, cell_output_volumes (output_volumes.F90:20-140): each cell's
+//     field(component) into row (t - first) / interval of the volume's history;
+//   kind 1, cell_output_volume_averages (output_volume_averages.F90): the
+//     sum over the cells divided by their number;
+//   kind 2, cell_output_volume_peak (output_volume_peak.F90): the largest
+//     |field(component)|, from 0;
+// kinds 1 and 2 write 0 when |value| < 1e-30.  One block per volume; the
+// sum is taken in a fixed order (strided partial sums, then a fixed tree),
+// so it is the same on every run and in a batch.
+struct OVolDev {
+  int4 gate;      // first, last, interval, component 1..6
+  int kind, n_cells, cell0;
+  long long off;  // first value of the volume in the history
+};
+struct OutVolDev {
+  int n_vol;
+  const OVolDev *vol;
+  const int *cells;          // output cell 0-based, volume after volume
+  const double *cell_cur;    // [n_out][6]
+  double *hist;
+};
+constexpr int kOutVolThreads = 256;
+
+__global__ void __launch_bounds__(kOutVolThreads) tlm_output_volume_kernel(const OutVolDev d, const int *d_base,
+                                                                             int rel_step) {
+  __shared__ double red[kOutVolThreads];
+  const OVolDev v = d.vol[blockIdx.x];
+  const int t = *d_base + rel_step;
+  const int4 g = v.gate;
+  if (t < g.x || t > g.y || (t - g.x) % g.z != 0) return;  // uniform over the block
+  const long long row = (t - g.x) / g.z;
+  const int tid = threadIdx.x;
+  const int *cells = d.cells + v.cell0;
+  if (v.kind == 0) {
+    for (int k = tid; k < v.n_cells; k += kOutVolThreads)
+      d.hist[v.off + row * v.n_cells + k] = d.cell_cur[(size_t)cells[k] * 6 + (g.w - 1)];
+    return;
+  }
+  double a = 0.0;
+  for (int k = tid; k < v.n_cells; k += kOutVolThreads) {
+    const double x = d.cell_cur[(size_t)cells[k] * 6 + (g.w - 1)];
+    a = v.kind == 1 ? a + x : fmax(a, fabs(x));
+  }
+  red[tid] = a;
+  __syncthreads();
+  for (int w = kOutVolThreads / 2; w > 0; w >>= 1) {
+    if (tid < w) red[tid] = v.kind == 1 ? red[tid] + red[tid + w] : fmax(red[tid], red[tid + w]);
+    __syncthreads();
+  }
+  if (tid == 0) {
+    double r = red[0];
+    if (v.kind == 1) r = v.n_cells ? r / (double)v.n_cells : 0.0;
+    if (fabs(r) < 1e-30) r = 0.0;
+    d.hist[v.off + row] = r;
+  }
+}
+
 // Frequency-domain output volumes, frequency_output_volumes.F90:309-390:
 // on the output steps of a volume (get_output_flag, output.F90:564-598:
 // first <= t <= last and (t - first) mod interval == 0),

@@ -563,6 +563,29 @@ class FrequencyOutputVolume:
         return m
 
 
+OUTPUT_VOLUME_KINDS = {"field": 0, "average": 1, "peak": 2}
+
+
+@dataclass
+class OutputVolume:
+    """A time-domain output volume on the output steps first..last every
+    ``interval``: ``kind`` "field" records each cell's ``component``
+    (OUTPUT/output_volumes.F90), "average" their mean
+    (output_volume_averages.F90), "peak" the largest magnitude
+    (output_volume_peak.F90).  Cells as for FrequencyOutputVolume."""
+
+    region: object
+    component: str
+    kind: str = "field"
+    first_step: int = 1
+    last_step: Optional[int] = None
+    interval: int = 1
+    every: int = 1
+
+    def mask(self, spec: "ProblemSpec") -> np.ndarray:
+        return FrequencyOutputVolume(self.region, [], self.component, every=self.every).mask(spec)
+
+
 @dataclass
 class ProblemSpec:
     nx: int
@@ -586,6 +609,7 @@ class ProblemSpec:
     frequency_output_volumes: List[FrequencyOutputVolume] = field(default_factory=list)
     output_surfaces: List[OutputSurface] = field(default_factory=list)
     rcs_surface: Optional[RCSSurface] = None
+    output_volumes: List[OutputVolume] = field(default_factory=list)
     reduced_c: float = 1.0
     # set_small_to_zero packet (read_small_to_zero.F90:55-59): (n_small_to_zero, small_to_zero_value)
     small_to_zero: Optional[Tuple[int, float]] = None
@@ -786,6 +810,15 @@ def build_tables(spec: ProblemSpec) -> dict:
             raise ValueError("frequency output volume interval and cell spacing must be >= 1")
         vm = fv.mask(spec)
         vol_masks.append(vm)
+        cell_out |= vm
+    ovol_masks = []
+    for ov in spec.output_volumes:
+        if COMPONENTS.get(ov.component, 0) not in range(1, 7):
+            raise ValueError("an output volume records Ex..Hz")
+        if ov.kind not in OUTPUT_VOLUME_KINDS or ov.first_step < 1 or ov.interval < 1 or ov.every < 1:
+            raise ValueError("output volume kind, first step, interval or cell spacing")
+        vm = ov.mask(spec)
+        ovol_masks.append(vm)
         cell_out |= vm
     if np.any(in_pml & cell_exc):
         raise UnsupportedFeature("Excitation intersects PML")  # set_update_codes.F90:347-354
@@ -1083,6 +1116,19 @@ def build_tables(spec: ProblemSpec) -> dict:
             vi.append(fv.interval)
             vout.extend(int(c) for c in cells)
             vptr.append(len(vout))
+    ok, oc, o0, o1, oi, optr, oout = [], [], [], [], [], [0], []
+    for ov, vm in zip(spec.output_volumes, ovol_masks):
+        ok.append(OUTPUT_VOLUME_KINDS[ov.kind])
+        oc.append(COMPONENTS[ov.component])
+        o0.append(ov.first_step)
+        o1.append(nsteps if ov.last_step is None else ov.last_step)
+        oi.append(ov.interval)
+        oout.extend(int(c) for c in out_number[vm.reshape(-1)])
+        optr.append(len(oout))
+    tables.update(n_ovol=len(ok), ovol_kind=np.array(ok, dtype=np.int32), ovol_comp=np.array(oc, dtype=np.int32),
+                  ovol_first=np.array(o0, dtype=np.int32), ovol_last=np.array(o1, dtype=np.int32),
+                  ovol_interval=np.array(oi, dtype=np.int32), ovol_cell_ptr=np.array(optr, dtype=np.int32),
+                  ovol_cell_out=np.array(oout, dtype=np.int32))
     tables.update(n_vdft=len(vf), vdft_freq=np.array(vf, dtype=np.float64), vdft_comp=np.array(vc, dtype=np.int32),
                   vdft_first=np.array(v0, dtype=np.int32), vdft_last=np.array(v1, dtype=np.int32),
                   vdft_interval=np.array(vi, dtype=np.int32), vdft_cell_ptr=np.array(vptr, dtype=np.int32),

@@ -189,6 +189,24 @@ int tlm_gpu_set_volume_dft(int64_t handle, int32_t n_volumes, const double *freq
    (re, im) pairs: frequency_output_volume(:)%value(:). */
 int tlm_gpu_fetch_volume_dft(int64_t handle, double *out);
 
+/* Time-domain output volumes: kind 0 = output_volumes(:) (each cell's
+   field, SRC/OUTPUT/output_volumes.F90), 1 = output_volume_averages(:)
+   (the mean over the cells, output_volume_averages.F90), 2 =
+   output_volume_peak(:) (the largest |field|, output_volume_peak.F90);
+   field component 1..6, first_timestep, last_timestep, timestep_interval
+   and a CSR list (cell_ptr[n+1]) of the 1-based output cell numbers
+   (cell_output_field_number_list).  Averages and peaks below 1e-30 in
+   magnitude are recorded as 0, as the reference writes them. */
+int tlm_gpu_set_output_volumes(int64_t handle, int32_t n_volumes, const int32_t *kind, const int32_t *component,
+                               const int32_t *first_step, const int32_t *last_step, const int32_t *interval,
+                               const int32_t *cell_ptr, const int32_t *cell_out);
+
+/* Output volume values, volume after volume: kind 0 [n_output_steps][n_cells],
+   kinds 1 and 2 [n_output_steps], n_output_steps = the steps
+   first..min(last, n_timesteps) every interval; rows of steps not run yet
+   are zero. */
+int tlm_gpu_fetch_output_volumes(int64_t handle, double *out);
+
 /* Time-domain output surfaces (SRC/OUTPUT/output_surfaces.F90:42-760), as
    output_surfaces(:): field component (1..6 Ex..Hz, 7..9 Jx..Jz = n x H,
    13 |E|, 14 |H|, 15 |J|), first_timestep, last_timestep, timestep_interval,

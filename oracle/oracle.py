@@ -342,3 +342,35 @@ def rcs(t: dict) -> np.ndarray:
             acc[2, point - 1] += Np - Lt / Z0
             acc[3, point - 1] += -(Nt + Lp / Z0)
     return acc
+
+
+def output_volumes(t: dict, cell_out: np.ndarray) -> list:
+    """Time-domain output volumes over the oracle's cell_output_field history
+    cell_out [steps, n_out_cells, 6], on every step get_output_flag accepts:
+    kind 0 each cell's field (OUTPUT/output_volumes.F90 cell_output_volumes),
+    kind 1 the sum in list order over the number of cells
+    (output_volume_averages.F90), kind 2 the largest |field| starting from 0
+    (output_volume_peak.F90); kinds 1 and 2 give 0 below 1e-30.  Returns one
+    array per volume ([n_output_steps, n_cells] or [n_output_steps])."""
+    res = []
+    ptr = t.get("ovol_cell_ptr", [0])
+    for k in range(int(t.get("n_ovol", 0))):
+        cells = np.asarray(t["ovol_cell_out"][ptr[k]:ptr[k + 1]], dtype=np.int64) - 1
+        comp, kind = int(t["ovol_comp"][k]) - 1, int(t["ovol_kind"][k])
+        first, last, every = int(t["ovol_first"][k]), int(t["ovol_last"][k]), int(t["ovol_interval"][k])
+        rows = []
+        for timestep in range(first, min(last, cell_out.shape[0]) + 1):
+            if (timestep - first) % every:
+                continue
+            f = cell_out[timestep - 1, cells, comp]
+            if kind == 0:
+                rows.append(f.copy())
+                continue
+            v = 0.0
+            for x in f:
+                v = v + float(x) if kind == 1 else max(v, abs(float(x)))
+            if kind == 1:
+                v = v / float(len(cells)) if len(cells) else 0.0
+            rows.append(0.0 if abs(v) < 1e-30 else v)
+        res.append(np.array(rows))
+    return res
