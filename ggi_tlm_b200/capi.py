@@ -42,7 +42,8 @@ EXPORTS = [
     "tlm_gpu_set_far_field", "tlm_gpu_fetch_far_field", "tlm_gpu_pool_release", "tlm_gpu_pool_cached_bytes",
     "tlm_gpu_prepare", "tlm_gpu_set_output_series", "tlm_gpu_set_volume_dft", "tlm_gpu_fetch_volume_dft",
     "tlm_gpu_set_output_surfaces", "tlm_gpu_fetch_output_surfaces", "tlm_gpu_set_rcs", "tlm_gpu_fetch_rcs",
-    "tlm_gpu_set_output_volumes", "tlm_gpu_fetch_output_volumes",
+    "tlm_gpu_set_output_volumes", "tlm_gpu_fetch_output_volumes", "tlm_gpu_set_sar_volumes",
+    "tlm_gpu_fetch_sar_volumes",
 ]
 
 
@@ -114,6 +115,8 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_fetch_rcs": [i64, _f64p],
         "tlm_gpu_set_output_volumes": [i64, i32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p],
         "tlm_gpu_fetch_output_volumes": [i64, _f64p],
+        "tlm_gpu_set_sar_volumes": [i64, i32, _f64p, _i32p, _i32p],
+        "tlm_gpu_fetch_sar_volumes": [i64, _f64p],
         "tlm_gpu_set_small_to_zero": [i64, i32, C.c_double],
         "tlm_gpu_set_dft": [i64, i32, _f64p, _i32p, _i32p, _i32p, _i32p],
         "tlm_gpu_run": [i64, i32, i32],
@@ -252,6 +255,9 @@ class GpuMesh:
             vd = [_f64(t["vdft_freq"]), _i32(t["vdft_comp"]), _i32(t["vdft_first"]), _i32(t["vdft_last"]),
                   _i32(t["vdft_interval"]), _i32(t["vdft_cell_ptr"]), _i32(t["vdft_cell_out"])]
             _check(lib.tlm_gpu_set_volume_dft(self.h, int(t["n_vdft"]), *[_p(x) for x in vd]))
+        if int(t.get("n_sar", 0)):
+            sv = [_f64(t["sar_freq"]), _i32(t["sar_cell_ptr"]), _i32(t["sar_cell_out"])]
+            _check(lib.tlm_gpu_set_sar_volumes(self.h, int(t["n_sar"]), *[_p(x) for x in sv]))
         if int(t.get("n_ovol", 0)):
             ov = [_i32(t[k]) for k in ("ovol_kind", "ovol_comp", "ovol_first", "ovol_last", "ovol_interval",
                                        "ovol_cell_ptr", "ovol_cell_out")]
@@ -346,6 +352,14 @@ class GpuMesh:
         out = np.zeros(max(12 * n, 12))
         _check(_lib.tlm_gpu_fetch_far_field(self.h, out.ctypes.data_as(_f64p)))
         v = out[: 12 * n].reshape(n, 6, 2)
+        return v[..., 0] + 1j * v[..., 1]
+
+    def sar_volumes(self) -> np.ndarray:
+        """SAR volume accumulators [entries, 3] complex: Ex, Ey, Ez per cell."""
+        n = int(self.t["sar_cell_ptr"][-1]) if int(self.t.get("n_sar", 0)) else 0
+        out = np.zeros(max(6 * n, 6))
+        _check(_lib.tlm_gpu_fetch_sar_volumes(self.h, out.ctypes.data_as(_f64p)))
+        v = out[: 6 * n].reshape(n, 3, 2)
         return v[..., 0] + 1j * v[..., 1]
 
     def output_volumes(self) -> list:

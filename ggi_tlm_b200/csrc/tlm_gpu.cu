@@ -275,6 +275,9 @@ struct Mesh {
                                      // component, kind)
   std::vector<int32_t> ovol_ptr, ovol_out;
   size_t ovol_hist_len = 0;
+  std::vector<double> sar_freq;      // SAR volumes, one per frequency
+  std::vector<int32_t> sar_ptr, sar_out;
+  int sar_entries = 0;
   bool rcs_on = false;               // the RCS surface (rcs_surface)
   double rcs_theta = 0, rcs_phi = 0;
   int rcs_npc = 2, rcs_points = 0, rcs_offset = 0;
@@ -290,7 +293,7 @@ struct Mesh {
       pmm_pos, pmm_parmat, pmm_state, pmm_sigma, face_src, fpt_field_d, fpt_type_d, fprobe, fprobe_rec,
       ohs_face, ohs_offset, ff_entry, ff_phasor, ff_acc, cell_cur, out_hist, vdft_entry, vdft_gate_d, vdft_phasor,
       vdft_acc, osurf_entry, osurf_pos, osurf_dev, osurf_hist, rcs_face, rcs_dist_d, rcs_tc0, rcs_acc, ovol_dev,
-      ovol_cells, ovol_hist;
+      ovol_cells, ovol_hist, sar_entry, sar_phasor, sar_acc;
   int n_pt_rows = 0;
   int n_pmm = 0;  // PML cells inside a volume material
   int n_filt = 0, filt_eo = 0, filt_mo = 0;
@@ -459,6 +462,18 @@ tlm::FarFieldDev far_field_dev(Mesh *m) {
 
 tlm::FaceProbeDev face_probe_dev(Mesh *m) {
   return tlm::FaceProbeDev{(const int4 *)m->fprobe.p, (double *)m->fprobe_rec.p, (int)m->fpr_face.size()};
+}
+
+tlm::SarDev sar_dev(Mesh *m) {
+  tlm::SarDev d{};
+  d.n_entries = m->sar_entries;
+  d.n_vol = (int)m->sar_freq.size();
+  d.dt = m->desc.dt;
+  d.entry = (const int2 *)m->sar_entry.p;
+  d.phasor = (const double2 *)m->sar_phasor.p;
+  d.cell_cur = (const double *)m->cell_cur.p;
+  d.acc = (double2 *)m->sar_acc.p;
+  return d;
 }
 
 tlm::OutVolDev out_vol_dev(Mesh *m) {
@@ -1036,6 +1051,31 @@ int finalize(Mesh *m) {
     if ((rc = dalloc(m, m->osurf_hist, std::max<size_t>(off, 1) * sizeof(double)))) return rc;
     CK(cudaMemset(m->osurf_hist.p, 0, m->osurf_hist.bytes));
   }
+  // ---- SAR volumes
+  {
+    const int nv = (int)m->sar_freq.size();
+    std::vector<int2> ent;
+    for (int v = 0; v < nv; v++)
+      for (int k = m->sar_ptr[v]; k < m->sar_ptr[v + 1]; k++) {
+        const int o = m->sar_out[k];
+        if (o < 1 || o > m->n_out_cells) return fail(TLM_E_BADARG, "SAR volume %d: output cell %d out of range", v + 1, o);
+        ent.push_back(int2{v, o - 1});
+      }
+    m->sar_entries = (int)ent.size();
+    if (ent.empty()) ent.resize(1);
+    std::vector<double2> ph((size_t)std::max(nv, 1) * nsteps, double2{0, 0});
+    const double pi = 3.141592653589793;
+    for (int t = 0; t < nsteps; t++) {
+      const double time = (double)t * D.dt;  // (timestep-1)*dt, the time of the cell outputs
+      for (int v = 0; v < nv; v++) {
+        const double arg = -2.0 * pi * m->sar_freq[v] * time;
+        ph[(size_t)t * nv + v] = double2{cos(arg), sin(arg)};
+      }
+    }
+    if ((rc = upload(m, m->sar_entry, ent)) || (rc = upload(m, m->sar_phasor, ph))) return rc;
+    if ((rc = dalloc(m, m->sar_acc, ent.size() * 3 * sizeof(double2)))) return rc;
+    CK(cudaMemset(m->sar_acc.p, 0, m->sar_acc.bytes));
+  }
   // ---- time-domain output volumes
   {
     const int nv = (int)m->ovol_gate.size() / 5;
@@ -1299,6 +1339,11 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
     if (m->vdft_entries) {  // reads the cell outputs this step's cell kernels wrote
       const tlm::VolDftDev vd = vol_dft_dev(m);
       tlm::tlm_volume_dft_kernel<<<(vd.n_entries + 255) / 256, 256, 0, m->stream>>>(vd, md.d_base, k);
+      m->last_launches++;
+    }
+    if (m->sar_entries) {  // likewise
+      const tlm::SarDev sd = sar_dev(m);
+      tlm::tlm_sar_kernel<<<(sd.n_entries + 255) / 256, 256, 0, m->stream>>>(sd, md.d_base, k);
       m->last_launches++;
     }
     if (!m->ovol_gate.empty()) {  // likewise
@@ -1746,6 +1791,33 @@ int tlm_gpu_fetch_output_volumes(int64_t h, double *out) {
   if (!m->ovol_hist_len) return TLM_OK;
   CK(cudaStreamSynchronize(m->stream));
   CK(cudaMemcpy(out, m->ovol_hist.p, m->ovol_hist_len * sizeof(double), cudaMemcpyDeviceToHost));
+  return TLM_OK;
+}
+
+int tlm_gpu_set_sar_volumes(int64_t h, int32_t n, const double *freq, const int32_t *cell_ptr,
+                            const int32_t *cell_out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && (!freq || !cell_ptr || !cell_out))) return fail(TLM_E_BADARG, "bad SAR volume arguments");
+  for (int v = 0; v < n; v++)
+    if (cell_ptr[v] < 0 || cell_ptr[v + 1] < cell_ptr[v])
+      return fail(TLM_E_BADARG, "SAR volume cell pointers must be non-decreasing");
+  m->sar_freq.assign(freq, freq + n);
+  m->sar_ptr.assign(cell_ptr, cell_ptr + (n ? n + 1 : 0));
+  const int ne = n ? cell_ptr[n] : 0;
+  m->sar_out.assign(cell_out, cell_out + ne);
+  return TLM_OK;
+}
+
+int tlm_gpu_fetch_sar_volumes(int64_t h, double *out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
+  if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
+  if (!m->sar_entries) return TLM_OK;
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(out, m->sar_acc.p, (size_t)m->sar_entries * 6 * sizeof(double), cudaMemcpyDeviceToHost));
   return TLM_OK;
 }
 
@@ -2294,6 +2366,14 @@ int batch_step(Batch *b, bool dry) {
     b->last_launches++;
   }
   if (side && (rc = b->side.end(b->stream))) return rc;
+  for (int i : b->active) {  // SAR volumes of the members that have them
+    Mesh *m = get(b->handles[i]);
+    if (m && m->sar_entries) {
+      const tlm::SarDev sd = sar_dev(m);
+      tlm::tlm_sar_kernel<<<(sd.n_entries + 255) / 256, 256, 0, b->stream>>>(sd, (const int *)m->d_base.p, 0);
+      b->last_launches++;
+    }
+  }
   for (int i : b->active) {  // time-domain output volumes of the members that have them
     Mesh *m = get(b->handles[i]);
     if (m && !m->ovol_gate.empty()) {

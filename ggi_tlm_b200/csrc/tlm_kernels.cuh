@@ -1917,6 +1917,35 @@ __global__ void __launch_bounds__(kOutVolThreads) tlm_output_volume_kernel(const
   }
 }
 
+// SAR volumes, cell_output_SAR_volumes (SAR_volumes.F90:257-330): every
+// step each cell accumulates E_c += exp(-j 2 pi f time) * E_c(t) * dt,
+// c = x, y, z, at the cell-output time (timestep-1) dt, for write_SAR_volumes
+// to turn into SAR afterwards.  One thread per (volume, cell) entry.
+struct SarDev {
+  int n_entries, n_vol;
+  double dt;
+  const int2 *entry;       // (volume, output cell 0-based)
+  const double2 *phasor;   // [n_timesteps][n_vol]: exp(-j 2 pi f (timestep-1) dt)
+  const double *cell_cur;  // [n_out][6]
+  double2 *acc;            // [n_entries][3]
+};
+
+__global__ void tlm_sar_kernel(const SarDev d, const int *d_base, int rel_step) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.n_entries) return;
+  const int t = *d_base + rel_step;
+  const int2 e = d.entry[k];
+  const double2 p = d.phasor[(size_t)(t - 1) * d.n_vol + e.x];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const double v = d.cell_cur[(size_t)e.y * 6 + c];
+    double2 a = d.acc[(size_t)k * 3 + c];
+    a.x = a.x + p.x * v * d.dt;
+    a.y = a.y + p.y * v * d.dt;
+    d.acc[(size_t)k * 3 + c] = a;
+  }
+}
+
 // Frequency-domain output volumes, frequency_output_volumes.F90:309-390:
 // on the output steps of a volume (get_output_flag, output.F90:564-598:
 // first <= t <= last and (t - first) mod interval == 0),

@@ -567,6 +567,21 @@ OUTPUT_VOLUME_KINDS = {"field": 0, "average": 1, "peak": 2}
 
 
 @dataclass
+class SARVolume:
+    """A SAR volume (SAR_volume packet, OUTPUT/SAR_volumes.F90): the cells of
+    a region, optionally every ``every``-th per axis, and a list of
+    frequencies; every step each cell accumulates the DFT of Ex, Ey, Ez
+    times dt, from which write_SAR_volumes computes SAR on the host."""
+
+    region: object
+    frequencies: Sequence[float]
+    every: int = 1
+
+    def mask(self, spec: "ProblemSpec") -> np.ndarray:
+        return FrequencyOutputVolume(self.region, [], "Ex", every=self.every).mask(spec)
+
+
+@dataclass
 class OutputVolume:
     """A time-domain output volume on the output steps first..last every
     ``interval``: ``kind`` "field" records each cell's ``component``
@@ -610,6 +625,7 @@ class ProblemSpec:
     output_surfaces: List[OutputSurface] = field(default_factory=list)
     rcs_surface: Optional[RCSSurface] = None
     output_volumes: List[OutputVolume] = field(default_factory=list)
+    sar_volumes: List[SARVolume] = field(default_factory=list)
     reduced_c: float = 1.0
     # set_small_to_zero packet (read_small_to_zero.F90:55-59): (n_small_to_zero, small_to_zero_value)
     small_to_zero: Optional[Tuple[int, float]] = None
@@ -810,6 +826,13 @@ def build_tables(spec: ProblemSpec) -> dict:
             raise ValueError("frequency output volume interval and cell spacing must be >= 1")
         vm = fv.mask(spec)
         vol_masks.append(vm)
+        cell_out |= vm
+    sar_masks = []
+    for sv in spec.sar_volumes:
+        if sv.every < 1:
+            raise ValueError("SAR volume cell spacing must be >= 1")
+        vm = sv.mask(spec)
+        sar_masks.append(vm)
         cell_out |= vm
     ovol_masks = []
     for ov in spec.output_volumes:
@@ -1116,6 +1139,15 @@ def build_tables(spec: ProblemSpec) -> dict:
             vi.append(fv.interval)
             vout.extend(int(c) for c in cells)
             vptr.append(len(vout))
+    sf, sptr, sout = [], [0], []
+    for sv, vm in zip(spec.sar_volumes, sar_masks):
+        cells = out_number[vm.reshape(-1)]
+        for fr in sv.frequencies:
+            sf.append(fr)
+            sout.extend(int(c) for c in cells)
+            sptr.append(len(sout))
+    tables.update(n_sar=len(sf), sar_freq=np.array(sf, dtype=np.float64), sar_cell_ptr=np.array(sptr, dtype=np.int32),
+                  sar_cell_out=np.array(sout, dtype=np.int32))
     ok, oc, o0, o1, oi, optr, oout = [], [], [], [], [], [0], []
     for ov, vm in zip(spec.output_volumes, ovol_masks):
         ok.append(OUTPUT_VOLUME_KINDS[ov.kind])

@@ -207,6 +207,19 @@ int tlm_gpu_set_output_volumes(int64_t handle, int32_t n_volumes, const int32_t 
    are zero. */
 int tlm_gpu_fetch_output_volumes(int64_t handle, double *out);
 
+/* SAR volumes (SRC/OUTPUT/SAR_volumes.F90:36-330), one entry per volume
+   and frequency as SAR_volume_list(:): frequency and a CSR list
+   (cell_ptr[n+1]) of the 1-based output cell numbers of the volume's
+   cells.  Every step each cell accumulates Ex, Ey, Ez +=
+   exp(-j 2 pi f (timestep-1) dt) * field * dt; write_SAR_volumes turns
+   them into SAR on the host. */
+int tlm_gpu_set_sar_volumes(int64_t handle, int32_t n_volumes, const double *frequency, const int32_t *cell_ptr,
+                            const int32_t *cell_out);
+
+/* SAR volume accumulators per cell in set_sar_volumes order: Ex, Ey, Ez as
+   (re, im) pairs, 6 doubles per cell (SAR_volume_list(:)%Ex(:), %Ey, %Ez). */
+int tlm_gpu_fetch_sar_volumes(int64_t handle, double *out);
+
 /* Time-domain output surfaces (SRC/OUTPUT/output_surfaces.F90:42-760), as
    output_surfaces(:): field component (1..6 Ex..Hz, 7..9 Jx..Jz = n x H,
    13 |E|, 14 |H|, 15 |J|), first_timestep, last_timestep, timestep_interval,

@@ -374,3 +374,24 @@ def output_volumes(t: dict, cell_out: np.ndarray) -> list:
             rows.append(0.0 if abs(v) < 1e-30 else v)
         res.append(np.array(rows))
     return res
+
+
+def sar_volumes(t: dict, cell_out: np.ndarray) -> np.ndarray:
+    """SAR volume accumulators, restating cell_output_SAR_volumes
+    (OUTPUT/SAR_volumes.F90:257-330) over the oracle's cell_output_field
+    history: every step, E_c = E_c + ejwt * field_c * dt for c = x, y, z,
+    ejwt = exp(-j*2*pi*f*time), time = (timestep-1)*dt.  Returns [entries, 3]."""
+    n = int(t.get("n_sar", 0))
+    ptr = t["sar_cell_ptr"] if n else [0]
+    dt = float(t["dt"])
+    out = []
+    for v in range(n):
+        cells = np.asarray(t["sar_cell_out"][ptr[v]:ptr[v + 1]], dtype=np.int64) - 1
+        f = float(t["sar_freq"][v])
+        acc = np.zeros((len(cells), 3), dtype=np.complex128)
+        for timestep in range(1, cell_out.shape[0] + 1):
+            time = (timestep - 1) * dt
+            ejwt = np.exp(-1j * 2.0 * np.pi * f * time)
+            acc = acc + ejwt * cell_out[timestep - 1][cells][:, 0:3] * dt
+        out.append(acc)
+    return np.concatenate(out) if out else np.zeros((0, 3), dtype=np.complex128)
