@@ -43,7 +43,8 @@ EXPORTS = [
     "tlm_gpu_prepare", "tlm_gpu_set_output_series", "tlm_gpu_set_volume_dft", "tlm_gpu_fetch_volume_dft",
     "tlm_gpu_set_output_surfaces", "tlm_gpu_fetch_output_surfaces", "tlm_gpu_set_rcs", "tlm_gpu_fetch_rcs",
     "tlm_gpu_set_output_volumes", "tlm_gpu_fetch_output_volumes", "tlm_gpu_set_sar_volumes",
-    "tlm_gpu_fetch_sar_volumes",
+    "tlm_gpu_fetch_sar_volumes", "tlm_gpu_set_power_surfaces", "tlm_gpu_fetch_power_surfaces",
+    "tlm_gpu_set_mode_outputs", "tlm_gpu_fetch_mode_outputs",
 ]
 
 
@@ -117,6 +118,10 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_fetch_output_volumes": [i64, _f64p],
         "tlm_gpu_set_sar_volumes": [i64, i32, _f64p, _i32p, _i32p],
         "tlm_gpu_fetch_sar_volumes": [i64, _f64p],
+        "tlm_gpu_set_power_surfaces": [i64, i32, _f64p, _i32p, _i32p, _i32p],
+        "tlm_gpu_fetch_power_surfaces": [i64, _f64p],
+        "tlm_gpu_set_mode_outputs": [i64, i32, _i32p, _i32p, _i32p, _i32p, _f64p],
+        "tlm_gpu_fetch_mode_outputs": [i64, i32, i32, _f64p],
         "tlm_gpu_set_small_to_zero": [i64, i32, C.c_double],
         "tlm_gpu_set_dft": [i64, i32, _f64p, _i32p, _i32p, _i32p, _i32p],
         "tlm_gpu_run": [i64, i32, i32],
@@ -255,6 +260,13 @@ class GpuMesh:
             vd = [_f64(t["vdft_freq"]), _i32(t["vdft_comp"]), _i32(t["vdft_first"]), _i32(t["vdft_last"]),
                   _i32(t["vdft_interval"]), _i32(t["vdft_cell_ptr"]), _i32(t["vdft_cell_out"])]
             _check(lib.tlm_gpu_set_volume_dft(self.h, int(t["n_vdft"]), *[_p(x) for x in vd]))
+        if int(t.get("n_ps", 0)):
+            pv = [_f64(t["ps_freq"]), _i32(t["ps_face_ptr"]), _i32(t["ps_face_out"]), _i32(t["ps_face_code"])]
+            _check(lib.tlm_gpu_set_power_surfaces(self.h, int(t["n_ps"]), *[_p(x) for x in pv]))
+        if int(t.get("n_modes", 0)):
+            mv = [_i32(t["mode_comp"]), _i32(t["mode_face_ptr"]), _i32(t["mode_face_out"]), _i32(t["mode_face_code"]),
+                  _f64(t["mode_field"])]
+            _check(lib.tlm_gpu_set_mode_outputs(self.h, int(t["n_modes"]), *[_p(x) for x in mv]))
         if int(t.get("n_sar", 0)):
             sv = [_f64(t["sar_freq"]), _i32(t["sar_cell_ptr"]), _i32(t["sar_cell_out"])]
             _check(lib.tlm_gpu_set_sar_volumes(self.h, int(t["n_sar"]), *[_p(x) for x in sv]))
@@ -353,6 +365,23 @@ class GpuMesh:
         _check(_lib.tlm_gpu_fetch_far_field(self.h, out.ctypes.data_as(_f64p)))
         v = out[: 12 * n].reshape(n, 6, 2)
         return v[..., 0] + 1j * v[..., 1]
+
+    def power_surfaces(self) -> np.ndarray:
+        """Power surface accumulators [entries, 4] complex: E1, E2, H1, H2 per face."""
+        n = int(self.t["ps_face_ptr"][-1]) if int(self.t.get("n_ps", 0)) else 0
+        out = np.zeros(max(8 * n, 8))
+        _check(_lib.tlm_gpu_fetch_power_surfaces(self.h, out.ctypes.data_as(_f64p)))
+        v = out[: 8 * n].reshape(n, 4, 2)
+        return v[..., 0] + 1j * v[..., 1]
+
+    def mode_outputs(self, first: int = 1, n: Optional[int] = None) -> np.ndarray:
+        """Mode output values [n_modes, n] of steps first.."""
+        if n is None:
+            n = self.step - first + 1
+        nm = int(self.t.get("n_modes", 0))
+        out = np.zeros((max(n, 1), max(nm, 1)))
+        _check(_lib.tlm_gpu_fetch_mode_outputs(self.h, first, n, out.ctypes.data_as(_f64p)))
+        return out[:n, :nm].T.copy()
 
     def sar_volumes(self) -> np.ndarray:
         """SAR volume accumulators [entries, 3] complex: Ex, Ey, Ez per cell."""

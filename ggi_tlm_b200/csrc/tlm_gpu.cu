@@ -275,6 +275,11 @@ struct Mesh {
                                      // component, kind)
   std::vector<int32_t> ovol_ptr, ovol_out;
   size_t ovol_hist_len = 0;
+  std::vector<double> ps_freq;       // frequency-domain power surfaces, one per surface and frequency
+  std::vector<int32_t> ps_ptr, ps_fout, ps_fcode;
+  int ps_entries = 0;
+  std::vector<int32_t> mode_comp, mode_ptr, mode_fout, mode_fcode;  // mode outputs
+  std::vector<double> mode_w;
   std::vector<double> sar_freq;      // SAR volumes, one per frequency
   std::vector<int32_t> sar_ptr, sar_out;
   int sar_entries = 0;
@@ -293,7 +298,8 @@ struct Mesh {
       pmm_pos, pmm_parmat, pmm_state, pmm_sigma, face_src, fpt_field_d, fpt_type_d, fprobe, fprobe_rec,
       ohs_face, ohs_offset, ff_entry, ff_phasor, ff_acc, cell_cur, out_hist, vdft_entry, vdft_gate_d, vdft_phasor,
       vdft_acc, osurf_entry, osurf_pos, osurf_dev, osurf_hist, rcs_face, rcs_dist_d, rcs_tc0, rcs_acc, ovol_dev,
-      ovol_cells, ovol_hist, sar_entry, sar_phasor, sar_acc;
+      ovol_cells, ovol_hist, sar_entry, sar_phasor, sar_acc, ps_entry, ps_phasor, ps_acc, mode_d, mode_face, mode_wd,
+      mode_hist;
   int n_pt_rows = 0;
   int n_pmm = 0;  // PML cells inside a volume material
   int n_filt = 0, filt_eo = 0, filt_mo = 0;
@@ -462,6 +468,28 @@ tlm::FarFieldDev far_field_dev(Mesh *m) {
 
 tlm::FaceProbeDev face_probe_dev(Mesh *m) {
   return tlm::FaceProbeDev{(const int4 *)m->fprobe.p, (double *)m->fprobe_rec.p, (int)m->fpr_face.size()};
+}
+
+tlm::PowerSurfDev power_surf_dev(Mesh *m) {
+  tlm::PowerSurfDev d{};
+  d.n_entries = m->ps_entries;
+  d.n_ps = (int)m->ps_freq.size();
+  d.entry = (const int4 *)m->ps_entry.p;
+  d.phasor = (const double2 *)m->ps_phasor.p;
+  d.face_field = (const double *)m->face_field.p;
+  d.acc = (double2 *)m->ps_acc.p;
+  return d;
+}
+
+tlm::ModeDev mode_dev(Mesh *m) {
+  tlm::ModeDev d{};
+  d.n_modes = (int)m->mode_comp.size();
+  d.mode = (const int4 *)m->mode_d.p;
+  d.face = (const int2 *)m->mode_face.p;
+  d.weight = (const double *)m->mode_wd.p;
+  d.face_field = (const double *)m->face_field.p;
+  d.hist = (double *)m->mode_hist.p;
+  return d;
 }
 
 tlm::SarDev sar_dev(Mesh *m) {
@@ -1051,6 +1079,54 @@ int finalize(Mesh *m) {
     if ((rc = dalloc(m, m->osurf_hist, std::max<size_t>(off, 1) * sizeof(double)))) return rc;
     CK(cudaMemset(m->osurf_hist.p, 0, m->osurf_hist.bytes));
   }
+  // ---- frequency-domain power surfaces
+  {
+    const int np_ = (int)m->ps_freq.size();
+    std::vector<int4> ent;
+    for (int v = 0; v < np_; v++)
+      for (int k = m->ps_ptr[v]; k < m->ps_ptr[v + 1]; k++) {
+        const int fo = m->ps_fout[k], code = m->ps_fcode[k];
+        if (fo < 1 || fo > m->n_out_faces) return fail(TLM_E_BADARG, "power surface %d: face output number out of range", v + 1);
+        if (code < 1 || code > 6) return fail(TLM_E_BADARG, "power surface %d: face code out of range", v + 1);
+        ent.push_back(int4{v, fo - 1, code, 0});
+      }
+    m->ps_entries = (int)ent.size();
+    if (ent.empty()) ent.resize(1);
+    std::vector<double2> ph((size_t)std::max(np_, 1) * nsteps, double2{0, 0});
+    const double pi = 3.141592653589793;
+    for (int t = 0; t < nsteps; t++) {
+      double time = (double)t * D.dt;  // (timestep-1)*dt, then the half step of the face outputs
+      time = time + D.dt / 2.0;
+      for (int v = 0; v < np_; v++) {
+        const double arg = -2.0 * pi * m->ps_freq[v] * time;
+        ph[(size_t)t * np_ + v] = double2{cos(arg), sin(arg)};
+      }
+    }
+    if ((rc = upload(m, m->ps_entry, ent)) || (rc = upload(m, m->ps_phasor, ph))) return rc;
+    if ((rc = dalloc(m, m->ps_acc, ent.size() * 4 * sizeof(double2)))) return rc;
+    CK(cudaMemset(m->ps_acc.p, 0, m->ps_acc.bytes));
+  }
+  // ---- mode outputs
+  {
+    const int nm = (int)m->mode_comp.size();
+    std::vector<int4> md(std::max(nm, 1));
+    std::vector<int2> fc;
+    for (int v = 0; v < nm; v++) {
+      if (m->mode_comp[v] < 1 || m->mode_comp[v] > 6) return fail(TLM_E_BADARG, "mode output %d: component is not Ex..Hz", v + 1);
+      md[v] = int4{m->mode_ptr[v], m->mode_ptr[v + 1] - m->mode_ptr[v], m->mode_comp[v], 0};
+      for (int k = m->mode_ptr[v]; k < m->mode_ptr[v + 1]; k++) {
+        const int fo = m->mode_fout[k], code = m->mode_fcode[k];
+        if (fo < 1 || fo > m->n_out_faces) return fail(TLM_E_BADARG, "mode output %d: face output number out of range", v + 1);
+        if (code < 1 || code > 6) return fail(TLM_E_BADARG, "mode output %d: face code out of range", v + 1);
+        fc.push_back(int2{fo - 1, code});
+      }
+    }
+    std::vector<double> w = m->mode_w;
+    if (fc.empty()) { fc.resize(1); w.assign(1, 0.0); }
+    if ((rc = upload(m, m->mode_d, md)) || (rc = upload(m, m->mode_face, fc)) || (rc = upload(m, m->mode_wd, w))) return rc;
+    if ((rc = dalloc(m, m->mode_hist, (size_t)std::max(nm, 1) * nsteps * sizeof(double)))) return rc;
+    CK(cudaMemset(m->mode_hist.p, 0, m->mode_hist.bytes));
+  }
   // ---- SAR volumes
   {
     const int nv = (int)m->sar_freq.size();
@@ -1368,6 +1444,16 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
     if (m->rcs_on && !m->rcs_fout.empty()) {
       const tlm::RcsDev rd = rcs_dev(m);
       tlm::tlm_rcs_kernel<<<(rd.n_faces + 255) / 256, 256, 0, m->stream>>>(rd, md.d_base, k);
+      m->last_launches++;
+    }
+    if (m->ps_entries) {
+      const tlm::PowerSurfDev pd2 = power_surf_dev(m);
+      tlm::tlm_power_surface_kernel<<<(pd2.n_entries + 255) / 256, 256, 0, m->stream>>>(pd2, md.d_base, k);
+      m->last_launches++;
+    }
+    if (!m->mode_comp.empty()) {
+      const tlm::ModeDev mdv = mode_dev(m);
+      tlm::tlm_mode_kernel<<<mdv.n_modes, tlm::kOutVolThreads, 0, m->stream>>>(mdv, md.d_base, k);
       m->last_launches++;
     }
     if (m->hs_outer && m->hs_n) {
@@ -1791,6 +1877,67 @@ int tlm_gpu_fetch_output_volumes(int64_t h, double *out) {
   if (!m->ovol_hist_len) return TLM_OK;
   CK(cudaStreamSynchronize(m->stream));
   CK(cudaMemcpy(out, m->ovol_hist.p, m->ovol_hist_len * sizeof(double), cudaMemcpyDeviceToHost));
+  return TLM_OK;
+}
+
+int tlm_gpu_set_power_surfaces(int64_t h, int32_t n, const double *freq, const int32_t *face_ptr,
+                               const int32_t *face_out, const int32_t *face_code) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && (!freq || !face_ptr || !face_out || !face_code))) return fail(TLM_E_BADARG, "bad power surface arguments");
+  for (int v = 0; v < n; v++)
+    if (face_ptr[v] < 0 || face_ptr[v + 1] < face_ptr[v])
+      return fail(TLM_E_BADARG, "power surface face pointers must be non-decreasing");
+  m->ps_freq.assign(freq, freq + n);
+  m->ps_ptr.assign(face_ptr, face_ptr + (n ? n + 1 : 0));
+  const int ne = n ? face_ptr[n] : 0;
+  m->ps_fout.assign(face_out, face_out + ne);
+  m->ps_fcode.assign(face_code, face_code + ne);
+  return TLM_OK;
+}
+
+int tlm_gpu_fetch_power_surfaces(int64_t h, double *out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
+  if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
+  if (!m->ps_entries) return TLM_OK;
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(out, m->ps_acc.p, (size_t)m->ps_entries * 8 * sizeof(double), cudaMemcpyDeviceToHost));
+  return TLM_OK;
+}
+
+int tlm_gpu_set_mode_outputs(int64_t h, int32_t n, const int32_t *component, const int32_t *face_ptr,
+                             const int32_t *face_out, const int32_t *face_code, const double *mode_field) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && (!component || !face_ptr || !face_out || !face_code || !mode_field)))
+    return fail(TLM_E_BADARG, "bad mode output arguments");
+  for (int v = 0; v < n; v++)
+    if (face_ptr[v] < 0 || face_ptr[v + 1] < face_ptr[v])
+      return fail(TLM_E_BADARG, "mode output face pointers must be non-decreasing");
+  m->mode_comp.assign(component, component + n);
+  m->mode_ptr.assign(face_ptr, face_ptr + (n ? n + 1 : 0));
+  const int ne = n ? face_ptr[n] : 0;
+  m->mode_fout.assign(face_out, face_out + ne);
+  m->mode_fcode.assign(face_code, face_code + ne);
+  m->mode_w.assign(mode_field, mode_field + ne);
+  return TLM_OK;
+}
+
+int tlm_gpu_fetch_mode_outputs(int64_t h, int32_t first, int32_t n, double *out) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
+  if (!m->finalized) return fail(TLM_E_STATE, "no run yet");
+  if (first < 1 || n < 0 || first + n - 1 >= m->next_step) return fail(TLM_E_BADARG, "steps not yet computed");
+  const size_t nm = m->mode_comp.size();
+  if (!nm || !n) return TLM_OK;
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(out, (double *)m->mode_hist.p + (size_t)(first - 1) * nm, (size_t)n * nm * sizeof(double),
+                cudaMemcpyDeviceToHost));
   return TLM_OK;
 }
 
@@ -2412,6 +2559,20 @@ int batch_step(Batch *b, bool dry) {
       const tlm::FaceProbeDev pd = face_probe_dev(m);
       tlm::tlm_face_probe_kernel<<<(pd.n + 127) / 128, 128, 0, b->stream>>>(pd, (const double *)m->face_field.p,
                                                                              (const int *)m->d_base.p, 0);
+      b->last_launches++;
+    }
+  }
+  for (int i : b->active) {  // power surfaces and mode outputs of the members that have them
+    Mesh *m = get(b->handles[i]);
+    if (m && m->ps_entries) {
+      const tlm::PowerSurfDev pd2 = power_surf_dev(m);
+      tlm::tlm_power_surface_kernel<<<(pd2.n_entries + 255) / 256, 256, 0, b->stream>>>(pd2, (const int *)m->d_base.p,
+                                                                                       0);
+      b->last_launches++;
+    }
+    if (m && !m->mode_comp.empty()) {
+      const tlm::ModeDev mdv = mode_dev(m);
+      tlm::tlm_mode_kernel<<<mdv.n_modes, tlm::kOutVolThreads, 0, b->stream>>>(mdv, (const int *)m->d_base.p, 0);
       b->last_launches++;
     }
   }

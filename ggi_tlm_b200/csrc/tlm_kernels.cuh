@@ -1946,6 +1946,77 @@ __global__ void tlm_sar_kernel(const SarDev d, const int *d_base, int rel_step) 
   }
 }
 
+// Frequency-domain power surfaces, face_output_frequency_domain_power_surfaces
+// (frequency_domain_power_surfaces.F90:287-420): every step each face adds
+// E1, E2, H1, H2 times exp(-j 2 pi f time), at the face-output time, where
+// (E1, E2, H1, H2) are the tangential fields on the face's side: (Ey, Ez,
+// Hy, Hz) on x faces, (Ez, Ex, Hz, Hx) on y faces, (Ex, Ey, Hx, Hy) on z
+// faces.  One thread per (surface and frequency, face) entry.
+struct PowerSurfDev {
+  int n_entries, n_ps;
+  const int4 *entry;         // (surface-frequency, face output 0-based, face code 1..6, 0)
+  const double2 *phasor;     // [n_timesteps][n_ps]
+  const double *face_field;  // [n_out_faces][2][6]
+  double2 *acc;              // [n_entries][4]
+};
+
+__global__ void tlm_power_surface_kernel(const PowerSurfDev d, const int *d_base, int rel_step) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.n_entries) return;
+  const int t = *d_base + rel_step;
+  const int4 e = d.entry[k];
+  const int axis = (e.z - 1) % 3, side = e.z <= 3 ? 0 : 1;
+  const double *f = d.face_field + (size_t)e.y * 12 + side * 6;
+  const int c1 = axis == 0 ? 1 : (axis == 1 ? 2 : 0), c2 = axis == 0 ? 2 : (axis == 1 ? 0 : 1);
+  const double v[4] = {f[c1], f[c2], f[3 + c1], f[3 + c2]};
+  const double2 p = d.phasor[(size_t)(t - 1) * d.n_ps + e.x];
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    double2 a = d.acc[(size_t)k * 4 + c];
+    a.x = a.x + v[c] * p.x;
+    a.y = a.y + v[c] * p.y;
+    d.acc[(size_t)k * 4 + c] = a;
+  }
+}
+
+// Mode outputs, Mode_output (output_modes.F90:546-620): every step each
+// mode's value is the sum over its faces of face_output_field(side, component)
+// times the mode field at the face, 0 when below 1e-30 in magnitude.  One
+// block per mode, the sum in a fixed order (strided partial sums, then a
+// fixed tree).
+struct ModeDev {
+  int n_modes;
+  const int4 *mode;          // (first face entry, n_faces, component 1..6, 0)
+  const int2 *face;          // (face output 0-based, face code 1..6)
+  const double *weight;      // mode field per face entry
+  const double *face_field;  // [n_out_faces][2][6]
+  double *hist;              // [n_timesteps][n_modes]
+};
+
+__global__ void __launch_bounds__(kOutVolThreads) tlm_mode_kernel(const ModeDev d, const int *d_base, int rel_step) {
+  __shared__ double red[kOutVolThreads];
+  const int4 md = d.mode[blockIdx.x];
+  const int t = *d_base + rel_step;
+  const int tid = threadIdx.x;
+  double a = 0.0;
+  for (int k = tid; k < md.y; k += kOutVolThreads) {
+    const int2 fc = d.face[md.x + k];
+    const int side = fc.y <= 3 ? 0 : 1;
+    a = a + d.face_field[(size_t)fc.x * 12 + side * 6 + (md.z - 1)] * d.weight[md.x + k];
+  }
+  red[tid] = a;
+  __syncthreads();
+  for (int w = kOutVolThreads / 2; w > 0; w >>= 1) {
+    if (tid < w) red[tid] = red[tid] + red[tid + w];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    double r = red[0];
+    if (fabs(r) < 1e-30) r = 0.0;
+    d.hist[(size_t)(t - 1) * d.n_modes + blockIdx.x] = r;
+  }
+}
+
 // Frequency-domain output volumes, frequency_output_volumes.F90:309-390:
 // on the output steps of a volume (get_output_flag, output.F90:564-598:
 // first <= t <= last and (t - first) mod interval == 0),

@@ -516,6 +516,39 @@ RCS_POINTS_PER_CELL = 2  # n_rcs_points_per_cell, TLM_MODULES/TLM_output_modules
 
 
 @dataclass
+class PowerSurface:
+    """A frequency-domain power surface (OUTPUT/frequency_domain_power_surfaces.F90):
+    faces of a box or plane as for FarFieldSurface and a list of
+    frequencies; every step each face accumulates the DFT of the two
+    tangential E and H components on its side."""
+
+    frequencies: Sequence[float]
+    box: Optional[Tuple[Tuple[int, int], Tuple[int, int], Tuple[int, int]]] = None
+    plane: Optional[Tuple[int, int, Tuple[int, int], Tuple[int, int]]] = None
+    side: int = 1
+
+    def faces(self) -> List[Tuple[Tuple[int, int, int], int]]:
+        if (self.box is None) == (self.plane is None):
+            raise ValueError("a power surface is either a box or a plane")
+        return FarFieldSurface([], self.box, self.plane, self.side).faces()
+
+
+@dataclass
+class ModeOutput:
+    """A mode output (OUTPUT/output_modes.F90): every step the sum over the
+    faces of a plane patch of one field component on each face's side
+    times the mode field ``profile(i, j, k)`` of the face's cell."""
+
+    component: str
+    plane: Tuple[int, int, Tuple[int, int], Tuple[int, int]]
+    profile: object
+    side: int = 1
+
+    def faces(self) -> List[Tuple[Tuple[int, int, int], int]]:
+        return FarFieldSurface([], None, self.plane, self.side).faces()
+
+
+@dataclass
 class OutputPoint:
     cell: Tuple[int, int, int]
     component: str
@@ -624,6 +657,8 @@ class ProblemSpec:
     frequency_output_volumes: List[FrequencyOutputVolume] = field(default_factory=list)
     output_surfaces: List[OutputSurface] = field(default_factory=list)
     rcs_surface: Optional[RCSSurface] = None
+    power_surfaces: List[PowerSurface] = field(default_factory=list)
+    mode_outputs: List[ModeOutput] = field(default_factory=list)
     output_volumes: List[OutputVolume] = field(default_factory=list)
     sar_volumes: List[SARVolume] = field(default_factory=list)
     reduced_c: float = 1.0
@@ -997,6 +1032,11 @@ def build_tables(spec: ProblemSpec) -> dict:
     for fl in os_faces:
         for c, code in fl:
             face_out[connect_key(c, code)] = True
+    ps_faces = [ps.faces() for ps in spec.power_surfaces]
+    mode_faces = [mo.faces() for mo in spec.mode_outputs]
+    for fl in ps_faces + mode_faces:
+        for c, code in fl:
+            face_out[connect_key(c, code)] = True
     rcs_faces = spec.rcs_surface.faces() if spec.rcs_surface is not None else []
     for c, code in rcs_faces:
         face_out[connect_key(c, code)] = True
@@ -1210,6 +1250,31 @@ def build_tables(spec: ProblemSpec) -> dict:
                   osurf_last=np.array(o1, dtype=np.int32), osurf_interval=np.array(oi, dtype=np.int32),
                   osurf_both=np.array(ob, dtype=np.int32), osurf_face_ptr=np.array(optr, dtype=np.int32),
                   osurf_face_out=np.array(ofo, dtype=np.int32), osurf_face_code=np.array(ofc, dtype=np.int32))
+    # frequency-domain power surfaces: one entry per frequency
+    pf, pptr, pfo, pfc = [], [0], [], []
+    for ps, fl in zip(spec.power_surfaces, ps_faces):
+        for fr in ps.frequencies:
+            pf.append(fr)
+            for c, code in fl:
+                pfo.append(fout_num[connect_key(c, code)])
+                pfc.append(code)
+            pptr.append(len(pfo))
+    tables.update(n_ps=len(pf), ps_freq=np.array(pf, dtype=np.float64), ps_face_ptr=np.array(pptr, dtype=np.int32),
+                  ps_face_out=np.array(pfo, dtype=np.int32), ps_face_code=np.array(pfc, dtype=np.int32))
+    # mode outputs
+    mc, mptr, mfo, mfc, mw = [], [0], [], [], []
+    for mo, fl in zip(spec.mode_outputs, mode_faces):
+        if COMPONENTS.get(mo.component, 0) not in range(1, 7):
+            raise ValueError("a mode output samples Ex..Hz")
+        mc.append(COMPONENTS[mo.component])
+        for c, code in fl:
+            mfo.append(fout_num[connect_key(c, code)])
+            mfc.append(code)
+            mw.append(float(mo.profile(*c)))
+        mptr.append(len(mfo))
+    tables.update(n_modes=len(mc), mode_comp=np.array(mc, dtype=np.int32), mode_face_ptr=np.array(mptr, dtype=np.int32),
+                  mode_face_out=np.array(mfo, dtype=np.int32), mode_face_code=np.array(mfc, dtype=np.int32),
+                  mode_field=np.array(mw, dtype=np.float64))
     # the RCS surface, initialise_rcs_surfaces (RCS_surfaces.F90:159-360)
     if spec.rcs_surface is not None:
         rs = spec.rcs_surface

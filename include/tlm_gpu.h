@@ -253,6 +253,30 @@ int tlm_gpu_set_rcs(int64_t handle, double theta, double phi, int32_t points_per
 /* RCS far-field arrays: Etheta, Ephi, Htheta, Hphi, each n_points doubles. */
 int tlm_gpu_fetch_rcs(int64_t handle, double *out);
 
+/* Frequency-domain power surfaces
+   (SRC/OUTPUT/frequency_domain_power_surfaces.F90:35-420), one entry per
+   surface and frequency (fmin + (k-1) fstep): frequency and a CSR list
+   (face_ptr[n+1]) of output face numbers and face codes 1..6.  Every step
+   each face accumulates E1, E2, H1, H2 (the tangential fields on its side)
+   times exp(-j 2 pi f t) at the face-output time. */
+int tlm_gpu_set_power_surfaces(int64_t handle, int32_t n, const double *frequency, const int32_t *face_ptr,
+                               const int32_t *face_out, const int32_t *face_code);
+
+/* Power surface accumulators per face in set order: E1, E2, H1, H2 as
+   (re, im) pairs, 8 doubles per face. */
+int tlm_gpu_fetch_power_surfaces(int64_t handle, double *out);
+
+/* Mode outputs (SRC/OUTPUT/output_modes.F90:35-620), as output_mode_list(:):
+   field component 1..6 and a CSR list (face_ptr[n+1]) of the mode samples:
+   output face number, face code 1..6 and mode_field.  Every step each
+   mode's value is the sum of face_output_field(side, component) *
+   mode_field over its faces, 0 below 1e-30 in magnitude. */
+int tlm_gpu_set_mode_outputs(int64_t handle, int32_t n_modes, const int32_t *component, const int32_t *face_ptr,
+                             const int32_t *face_out, const int32_t *face_code, const double *mode_field);
+
+/* Mode output values of steps first..first+n-1: out[n][n_modes]. */
+int tlm_gpu_fetch_mode_outputs(int64_t handle, int32_t first_step, int32_t n_steps, double *out);
+
 /* Frequency-domain output surfaces (one entry per frequency, as
    frequency_output_surface(:) in SRC/OUTPUT/frequency_output_surfaces.F90:
    297-421): frequency, field component (1..6 E/H, 7..9 J=nxH), and a CSR

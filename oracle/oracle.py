@@ -395,3 +395,68 @@ def sar_volumes(t: dict, cell_out: np.ndarray) -> np.ndarray:
             acc = acc + ejwt * cell_out[timestep - 1][cells][:, 0:3] * dt
         out.append(acc)
     return np.concatenate(out) if out else np.zeros((0, 3), dtype=np.complex128)
+
+
+def _face_field_probes(t: dict, fo, codes) -> np.ndarray:
+    """Run the oracle over the whole solve with face output points on each
+    listed face's side (face code 1..3 -> side 1, 4..6 -> side 2) for all six
+    components; returns the values [face, component, step]."""
+    fo = np.asarray(fo, dtype=np.int32)
+    sides = np.where(np.asarray(codes) <= 3, 1, 2).astype(np.int32)
+    n0 = int(t.get("n_face_probes", 0))
+    t2 = dict(t)
+    t2["n_face_probes"] = n0 + 6 * len(fo)
+    t2["fprobe_face"] = np.concatenate([np.asarray(t.get("fprobe_face", []), dtype=np.int32), np.repeat(fo, 6)])
+    t2["fprobe_side"] = np.concatenate([np.asarray(t.get("fprobe_side", []), dtype=np.int32), np.repeat(sides, 6)])
+    t2["fprobe_comp"] = np.concatenate([np.asarray(t.get("fprobe_comp", []), dtype=np.int32),
+                                        np.tile(np.arange(1, 7, dtype=np.int32), len(fo))])
+    o = Oracle(t2)
+    o.run(int(t["n_timesteps"]))
+    return o.face_probes()[n0:].reshape(len(fo), 6, -1)
+
+
+def power_surfaces(t: dict) -> np.ndarray:
+    """Frequency-domain power surfaces, restating
+    face_output_frequency_domain_power_surfaces
+    (OUTPUT/frequency_domain_power_surfaces.F90:287-420): every step each face
+    adds E1, E2, H1, H2 (tangential fields on its side) * exp(-j*2*pi*f*time),
+    time = (timestep-1)*dt + dt/2.  Returns [entries, 4]."""
+    n = int(t.get("n_ps", 0))
+    if not n:
+        return np.zeros((0, 4), dtype=np.complex128)
+    vals = _face_field_probes(t, t["ps_face_out"], t["ps_face_code"])
+    ptr, codes = t["ps_face_ptr"], np.asarray(t["ps_face_code"])
+    pick = {0: (1, 2, 4, 5), 1: (2, 0, 5, 3), 2: (0, 1, 3, 4)}  # (E1, E2, H1, H2) by face axis
+    acc = np.zeros((len(codes), 4), dtype=np.complex128)
+    dt = float(t["dt"])
+    for v in range(n):
+        f = float(t["ps_freq"][v])
+        for timestep in range(1, int(t["n_timesteps"]) + 1):
+            time = (timestep - 1) * dt
+            time = time + dt / 2.0
+            ejwt = np.exp(-1j * 2.0 * np.pi * f * time)
+            for k in range(ptr[v], ptr[v + 1]):
+                comps = pick[(int(codes[k]) - 1) % 3]
+                for c in range(4):
+                    acc[k, c] = acc[k, c] + vals[k, comps[c], timestep - 1] * ejwt
+    return acc
+
+
+def mode_outputs(t: dict) -> np.ndarray:
+    """Mode outputs, restating Mode_output (OUTPUT/output_modes.F90:546-620):
+    every step the sum in list order of face_output_field(side, component) *
+    mode_field over the mode's faces, 0 below 1e-30.  Returns [n_modes, steps]."""
+    n = int(t.get("n_modes", 0))
+    if not n:
+        return np.zeros((0, int(t["n_timesteps"])))
+    vals = _face_field_probes(t, t["mode_face_out"], t["mode_face_code"])
+    ptr, w = t["mode_face_ptr"], np.asarray(t["mode_field"])
+    out = np.zeros((n, int(t["n_timesteps"])))
+    for v in range(n):
+        comp = int(t["mode_comp"][v]) - 1
+        for s in range(int(t["n_timesteps"])):
+            acc = 0.0
+            for k in range(ptr[v], ptr[v + 1]):
+                acc = acc + float(vals[k, comp, s]) * float(w[k])
+            out[v, s] = 0.0 if abs(acc) < 1e-30 else acc
+    return out
