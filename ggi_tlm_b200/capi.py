@@ -44,7 +44,7 @@ EXPORTS = [
     "tlm_gpu_set_output_surfaces", "tlm_gpu_fetch_output_surfaces", "tlm_gpu_set_rcs", "tlm_gpu_fetch_rcs",
     "tlm_gpu_set_output_volumes", "tlm_gpu_fetch_output_volumes", "tlm_gpu_set_sar_volumes",
     "tlm_gpu_fetch_sar_volumes", "tlm_gpu_set_power_surfaces", "tlm_gpu_fetch_power_surfaces",
-    "tlm_gpu_set_mode_outputs", "tlm_gpu_fetch_mode_outputs",
+    "tlm_gpu_set_mode_outputs", "tlm_gpu_fetch_mode_outputs", "tlm_gpu_set_face_materials",
 ]
 
 
@@ -121,6 +121,7 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_power_surfaces": [i64, i32, _f64p, _i32p, _i32p, _i32p],
         "tlm_gpu_fetch_power_surfaces": [i64, _f64p],
         "tlm_gpu_set_mode_outputs": [i64, i32, _i32p, _i32p, _i32p, _i32p, _f64p],
+        "tlm_gpu_set_face_materials": [i64, i32, _i32p],
         "tlm_gpu_fetch_mode_outputs": [i64, i32, i32, _f64p],
         "tlm_gpu_set_small_to_zero": [i64, i32, C.c_double],
         "tlm_gpu_set_dft": [i64, i32, _f64p, _i32p, _i32p, _i32p, _i32p],
@@ -242,6 +243,10 @@ class GpuMesh:
         fa = [_i32(t[k]) for k in ("face_cx", "face_cy", "face_cz", "face_dir", "face_exc", "face_out")]
         _check(lib.tlm_gpu_set_faces(self.h, int(t["n_faces"]), *[_p(x) for x in fa], int(t["n_exc_faces"]),
                                      int(t["n_out_faces"])))
+        fm = t.get("face_mat")
+        if fm is not None and np.any(np.asarray(fm) != 0):
+            fmv = _i32(fm)
+            _check(lib.tlm_gpu_set_face_materials(self.h, int(t["n_faces"]), _p(fmv)))
         if int(t["hs_n"]) and int(t.get("hs_outer", 0)):
             hc, ho, Ei, Hi = _i32(t["hs_cell"]), _f64(t["hs_offset"]), _f64(t["hs_Ei"]), _f64(t["hs_Hi"])
             _check(lib.tlm_gpu_set_outer_huygens(self.h, int(t["hs_n"]), _p(hc), _p(ho), _p(Ei), _p(Hi),

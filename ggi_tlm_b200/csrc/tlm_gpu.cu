@@ -247,6 +247,7 @@ struct Mesh {
   std::vector<int32_t> pt_cell, pt_comp, pt_fn, pt_type;
   int n_exc_cells = 0;
   std::vector<int32_t> f_cx, f_cy, f_cz, f_dir, f_exc, f_out;
+  std::vector<int32_t> f_mat;  // surface material per special face (empty: none)
   // point sources on faces (excitation face number, component 1..12, function, type)
   std::vector<int32_t> fpt_face, fpt_comp, fpt_fn, fpt_type;
   // output points on faces (output face number, side 1/2, component 1..6)
@@ -298,7 +299,7 @@ struct Mesh {
       pmm_pos, pmm_parmat, pmm_state, pmm_sigma, face_src, fpt_field_d, fpt_type_d, fprobe, fprobe_rec,
       ohs_face, ohs_offset, ff_entry, ff_phasor, ff_acc, cell_cur, out_hist, vdft_entry, vdft_gate_d, vdft_phasor,
       vdft_acc, osurf_entry, osurf_pos, osurf_dev, osurf_hist, rcs_face, rcs_dist_d, rcs_tc0, rcs_acc, ovol_dev,
-      ovol_cells, ovol_hist, sar_entry, sar_phasor, sar_acc, ps_entry, ps_phasor, ps_acc, mode_d, mode_face, mode_wd,
+      face_mat_d, ovol_cells, ovol_hist, sar_entry, sar_phasor, sar_acc, ps_entry, ps_phasor, ps_acc, mode_d, mode_face, mode_wd,
       mode_hist;
   int n_pt_rows = 0;
   int n_pmm = 0;  // PML cells inside a volume material
@@ -434,6 +435,7 @@ tlm::FaceDev face_dev(Mesh *m) {
   f.pt_field = (const double *)m->fpt_field_d.p;
   f.pt_type = (const int8_t *)m->fpt_type_d.p;
   f.n_pt_rows = m->n_pt_rows;
+  f.mat = (const int8_t *)m->face_mat_d.p;
   return f;
 }
 
@@ -907,6 +909,16 @@ int finalize(Mesh *m) {
       }
       if (m->f_out[f] > m->n_out_faces) return fail(TLM_E_BADARG, "face output number out of range");
     }
+    if (!m->f_mat.empty() && (int)m->f_mat.size() != nf)
+      return fail(TLM_E_BADARG, "face materials: %zu given for %d special faces", m->f_mat.size(), nf);
+    std::vector<int8_t> fmat(std::max(nf, 1), 0);
+    for (int f = 0; f < (int)m->f_mat.size(); f++) {
+      const int t = m->f_mat[f];
+      if (t != 0 && t != 1 && t != 2 && t != 4)
+        return fail(TLM_E_UNSUPPORTED, "special face %d: surface material type %d (only PEC 1, PMC 2, free space 4)", f + 1, t);
+      fmat[f] = (int8_t)t;
+    }
+    if ((rc = upload(m, m->face_mat_d, fmat))) return rc;
     std::vector<int> covered(m->n_exc_faces + 1, 0);
     std::vector<int2> src(std::max(nf, 1), int2{0, -1});
     for (int h = 0; h < (m->hs_outer ? 0 : m->hs_n); h++) {
@@ -1688,6 +1700,15 @@ int tlm_gpu_set_faces(int64_t h, int32_t n, const int32_t *cx, const int32_t *cy
   m->f_out.assign(out, out + n);
   m->n_exc_faces = n_exc_faces;
   m->n_out_faces = n_out_faces;
+  return TLM_OK;
+}
+
+int tlm_gpu_set_face_materials(int64_t h, int32_t n, const int32_t *type) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && !type)) return fail(TLM_E_BADARG, "bad face material arguments");
+  m->f_mat.assign(type, type + n);
   return TLM_OK;
 }
 

@@ -1523,6 +1523,7 @@ struct FaceDev {
   const double *pt_field;  // [n_timesteps][n_pt_rows][12] summed face point sources (E, H, J, M)
   const int8_t *pt_type;   // [n_pt_rows][6] hard (0) / soft (1) source factor of E, H
   int n_pt_rows;
+  const int8_t *mat;       // per special face: surface material 0 none, 1 PEC, 2 PMC, 4 free space
 };
 
 template <typename T>
@@ -1640,6 +1641,12 @@ __device__ __forceinline__ void face_body(const MeshDev<T> &m, const FaceDev &fd
   const double a2 = double(R[pmin2 * P + ip]), b2 = double(R[pmax2 * P + im]);
   double A_min = a1 + b1, A_max = A_min;
   double B_min = a2 + b2, B_max = B_min;
+  const int mat = fd.mat[f];
+  if (mat == 1) {  // PEC sheet, connect_normal_to_x.F90:36-40: each side reflects with -1
+    A_min = 0.0; A_max = 0.0; B_min = 0.0; B_max = 0.0;
+  } else if (mat == 2) {  // PMC sheet, connect_normal_to_x.F90:41-45: each side reflects with +1
+    A_min = 2.0 * a1; A_max = 2.0 * b1; B_min = 2.0 * a2; B_max = 2.0 * b2;
+  }  // 0 and 4 (a free-space surface material): the plain sum
   if (io.x >= 0) {
     // face_excitation_field / face_excitation_type of this face: point
     // sources first (excitation_points.F90:286-323, the same value on both

@@ -514,6 +514,25 @@ class RCSSurface:
 
 RCS_POINTS_PER_CELL = 2  # n_rcs_points_per_cell, TLM_MODULES/TLM_output_modules.F90:388
 
+# surface_material_type_*, TLM_MODULES/TLM_material_modules.F90:153-159
+SURFACE_SHEET_TYPES = {"PEC": 1, "PMC": 2, "free": 4}
+
+
+@dataclass
+class SurfaceSheet:
+    """A PEC, PMC or free-space surface material on a planar patch of
+    internal cell faces (the same (axis, index, r0, r1) convention as
+    DFTSurface): the connect across those faces reflects each side with -1
+    (PEC) or +1 (PMC), or is the plain connect (free space)
+    (connect_normal_to_x.F90:36-52).  Thin-layer and other surface
+    materials stay unsupported."""
+
+    kind: str
+    axis: int
+    index: int
+    r0: Tuple[int, int]
+    r1: Tuple[int, int]
+
 
 @dataclass
 class PowerSurface:
@@ -656,6 +675,7 @@ class ProblemSpec:
     far_field_surfaces: List["FarFieldSurface"] = field(default_factory=list)
     frequency_output_volumes: List[FrequencyOutputVolume] = field(default_factory=list)
     output_surfaces: List[OutputSurface] = field(default_factory=list)
+    surface_sheets: List[SurfaceSheet] = field(default_factory=list)
     rcs_surface: Optional[RCSSurface] = None
     power_surfaces: List[PowerSurface] = field(default_factory=list)
     mode_outputs: List[ModeOutput] = field(default_factory=list)
@@ -1043,7 +1063,13 @@ def build_tables(spec: ProblemSpec) -> dict:
     for ds in spec.dft_surfaces:
         for f in _plane_faces(ds.axis, ds.index, ds.r0, ds.r1):
             face_out[(f, ds.axis)] = True
-    keys = set(face_exc) | set(face_out)
+    face_mat = {}
+    for sh in spec.surface_sheets:
+        if sh.kind not in SURFACE_SHEET_TYPES:
+            raise UnsupportedFeature(f"surface material {sh.kind!r}: only PEC, PMC and free-space sheets")
+        for f in _plane_faces(sh.axis, sh.index, sh.r0, sh.r1):
+            face_mat[(f, sh.axis)] = SURFACE_SHEET_TYPES[sh.kind]
+    keys = set(face_exc) | set(face_out) | set(face_mat)
     for (c, axis) in keys:
         if c[axis - 1] <= 1 or c[axis - 1] > (nx, ny, nz)[axis - 1]:
             raise UnsupportedFeature("special face on the outer boundary")
@@ -1078,6 +1104,7 @@ def build_tables(spec: ProblemSpec) -> dict:
     for q, _, _ in face_probes:
         if COMPONENTS[q.component] > 6:
             raise ValueError("a face output point records E or H (components 1..6)")
+    tables["face_mat"] = np.array([face_mat.get(k, 0) for k in ordered], dtype=np.int32)
     tables.update(n_faces=len(ordered), face_cx=np.array(face_cx, dtype=np.int32),
                   face_cy=np.array(face_cy, dtype=np.int32), face_cz=np.array(face_cz, dtype=np.int32),
                   face_dir=np.array(face_dir, dtype=np.int32), face_exc=np.array(face_e, dtype=np.int32),

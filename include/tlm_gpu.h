@@ -125,6 +125,15 @@ int tlm_gpu_set_faces(int64_t handle, int32_t n_faces, const int32_t *cx, const 
                       const int32_t *dir, const int32_t *exc, const int32_t *out, int32_t n_exc_faces,
                       int32_t n_out_faces);
 
+/* Surface materials on the special faces, in set_faces order
+   (face_update_code_to_material_data, connect_normal_to_x.F90:20-52 and the
+   y, z analogues): 0 none, 1 PEC (surface_material_type_PEC: each side
+   reflects its own pulse with -1), 2 PMC (+1), 4 free space (the plain
+   connect).  Other surface material types (thin layers, dispersive, switches,
+   diodes, spice ports) are rejected with TLM_E_UNSUPPORTED at the first run.
+   Without this call no special face carries a material. */
+int tlm_gpu_set_face_materials(int64_t handle, int32_t n_faces, const int32_t *type);
+
 /* Huygens surface (SRC/EXCITATION/huygens_surface.F90:247-848): per patch
    the face excitation number, normal (3 ints) and offset; the incident
    field vectors Ei, Hi; offset_min, the wave speed c0/reduced_c and the

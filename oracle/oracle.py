@@ -51,7 +51,7 @@ class _Problem(C.Structure):
         ("n_face_probes", C.c_int32), ("fprobe_face", _i32p), ("fprobe_side", _i32p), ("fprobe_comp", _i32p),
         ("hs_outer", C.c_int32), ("hs_cell", _i32p),
         ("n_ff", C.c_int32), ("ff_freq", _f64p), ("ff_face_ptr", _i32p), ("ff_face_out", _i32p),
-        ("ff_face_code", _i32p),
+        ("ff_face_code", _i32p), ("face_mat", _i32p),
     ]
 
 
@@ -134,6 +134,8 @@ class Oracle:
         p.ff_freq = arr("ff_freq", np.float64) if "ff_freq" in t else arr_empty_f()
         for k in ("ff_face_ptr", "ff_face_out", "ff_face_code"):
             setattr(p, k, arr(k, np.int32) if k in t else arr_empty())
+        if "face_mat" in t and np.any(np.asarray(t["face_mat"]) != 0):
+            p.face_mat = arr("face_mat", np.int32)  # else NULL: no surface materials
         for k in ("fpt_face", "fpt_comp", "fpt_fn", "fpt_type", "fprobe_face", "fprobe_side", "fprobe_comp",
                   "hs_cell"):
             setattr(p, k, arr(k, np.int32) if k in t else arr_empty())

@@ -750,6 +750,13 @@ static void connect_special_face(tlm_oracle_state *s, int f, int cx, int cy, int
   double p2a = V_(pmax1, mx, my, mz), p2b = V_(pmax2, mx, my, mz);
   double A_min = V_(pmin1, cx, cy, cz) + V_(pmax1, mx, my, mz), A_max = A_min;
   double B_min = V_(pmin2, cx, cy, cz) + V_(pmax2, mx, my, mz), B_max = B_min;
+  const int mat = p->face_mat ? p->face_mat[f] : 0;
+  if (mat == 1) { /* PEC sheet: connect_normal_to_x.F90:36-40 */
+    A_min = 0.0; A_max = 0.0; B_min = 0.0; B_max = 0.0;
+  } else if (mat == 2) { /* PMC sheet: connect_normal_to_x.F90:41-45 */
+    A_min = 2.0 * V_(pmin1, cx, cy, cz); A_max = 2.0 * V_(pmax1, mx, my, mz);
+    B_min = 2.0 * V_(pmin2, cx, cy, cz); B_max = 2.0 * V_(pmax2, mx, my, mz);
+  } /* 0 and 4 (free-space surface material): the plain sum */
   if (exc != 0) {
     const double *fmin = s->face_exc + (size_t)(*excitation_face_number) * 24;
     const double *fmax = fmin + 12;

@@ -130,6 +130,12 @@ typedef struct {
   int32_t n_ff;
   const double *ff_freq;
   const int32_t *ff_face_ptr, *ff_face_out, *ff_face_code;
+
+  /* surface materials on the special faces, connect_normal_to_x.F90:36-52
+     (and the y, z analogues): per face 0 none, 1 PEC, 2 PMC, 4 free space
+     (surface_material_type_*, TLM_MODULES/TLM_material_modules.F90:153-159);
+     NULL: no surface materials */
+  const int32_t *face_mat;
 } tlm_oracle_problem;
 
 typedef struct tlm_oracle_state tlm_oracle_state;
