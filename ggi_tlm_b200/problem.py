@@ -1194,6 +1194,10 @@ def build_tables(spec: ProblemSpec) -> dict:
         dtype=np.int32)
     tables["out_comp"] = np.array([COMPONENTS[o.component] for o in centre_outs], dtype=np.int32)
     tables["out_keep"] = point_out.reshape(-1)[cell_out.reshape(-1)].astype(np.int32)
+    # 1-based output point numbers (output_points(:) order) of the centre and face points, for .tout files
+    tables["out_point_no"] = np.array([i + 1 for i, q in enumerate(spec.outputs) if q.face == "centre"], dtype=np.int32)
+    tables["fprobe_point_no"] = np.array([i + 1 for i, q in enumerate(spec.outputs) if q.face != "centre"],
+                                         dtype=np.int32)
     # frequency output volumes: one reference volume entry per frequency
     vf, vc, v0, v1, vi, vptr, vout = [], [], [], [], [], [0], []
     for fv, vm in zip(spec.frequency_output_volumes, vol_masks):

@@ -24,6 +24,11 @@ CASES = {
 }
 
 
+# raw text of the reference's .tout files (header and every data line), kept
+# to check that the library's .tout writer reproduces them byte for byte
+TEXT_CASES = ["tem_pml_Ey", "material_test2_Ex", "huygens_box_Hz"]
+
+
 def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     here = os.path.dirname(os.path.abspath(__file__))
@@ -33,6 +38,12 @@ def main():
         np.savez_compressed(os.path.join(here, name + ".npz"), time=d[:, 0], point=d[:, 1].astype(np.int32),
                             value=d[:, 2], source=rel)
         print(name, d.shape)
+    lines = {}
+    for name in TEXT_CASES:
+        with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", CASES[name])) as f:
+            lines[name] = np.array(f.read().splitlines())
+    np.savez_compressed(os.path.join(here, "tout_text.npz"), **lines)
+    print("tout_text", {k: len(v) for k, v in lines.items()})
 
 
 if __name__ == "__main__":
