@@ -76,7 +76,38 @@ def footprint_bytes(t: dict, precision: int = capi.TLM_PRECISION_FP32) -> int:
     if int(t.get("n_vdft", 0)):
         outs += int(t["vdft_cell_ptr"][-1]) * (16 + 8) + int(t["n_vdft"]) * 16 * n
     dft = int(t["dft_face_ptr"][-1]) * 16 + int(t["n_dft"]) * 16 * n if int(t["n_dft"]) else 0
+    outs += _output_bytes(t)
     return int(links + pml + special + filt + outs + dft + (1 << 20))
+
+
+def _output_bytes(t: dict) -> int:
+    """Device bytes of the optional outputs: far-field, power-surface, SAR
+    accumulators and their phasor tables, output-surface and output-volume
+    histories, mode series and the RCS far field."""
+    n = int(t["n_timesteps"])
+    b = 0
+    if int(t.get("n_ff", 0)):
+        b += int(t["ff_face_ptr"][-1]) * (16 + 6 * 16) + int(t["n_ff"]) * 16 * n
+    if int(t.get("n_ps", 0)):
+        b += int(t["ps_face_ptr"][-1]) * (16 + 4 * 16) + int(t["n_ps"]) * 16 * n
+    if int(t.get("n_sar", 0)):
+        b += int(t["sar_cell_ptr"][-1]) * (8 + 3 * 16) + int(t["n_sar"]) * 16 * n
+    if int(t.get("n_osurf", 0)):
+        from . import capi as _capi
+        b += sum(a * f for a, f in _capi.output_surface_shapes(t)) * 8 + int(t["osurf_face_ptr"][-1]) * 16
+    if int(t.get("n_ovol", 0)):
+        ptr = t["ovol_cell_ptr"]
+        for k in range(int(t["n_ovol"])):
+            first, last, every = int(t["ovol_first"][k]), int(t["ovol_last"][k]), int(t["ovol_interval"][k])
+            hi = min(last, n)
+            ns = (hi - first) // every + 1 if hi >= first else 0
+            b += ns * (int(ptr[k + 1] - ptr[k]) if int(t["ovol_kind"][k]) == 0 else 1) * 8
+        b += int(ptr[-1]) * 4
+    if int(t.get("n_modes", 0)):
+        b += int(t["n_modes"]) * 8 * n + int(t["mode_face_ptr"][-1]) * 16
+    if int(t.get("rcs_on", 0)):
+        b += int(t["rcs_points"]) * 32 + len(t["rcs_face_out"]) * 16 + 8 * n
+    return b
 
 
 class GpuEngine:

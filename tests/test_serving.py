@@ -107,3 +107,16 @@ def test_results_same_alone_and_in_the_mix(gpu_lib):
             alone_dft = g.dft()
         assert np.array_equal(r.probes, alone)
         assert np.array_equal(r.dft, alone_dft)
+
+
+def test_footprint_counts_optional_outputs():
+    from ggi_tlm_b200.problem import Block, OutputSurface, OutputVolume
+
+    base = cases.pml_point_source(20, steps=100, pml=3, n_probes=1)
+    t0 = build_tables(base)
+    base.output_surfaces = [OutputSurface("Ex", plane=(3, 10, (4, 16), (4, 16)))]
+    base.output_volumes = [OutputVolume(Block(5, 14, 5, 14, 5, 14), "Ey", "field")]
+    t1 = build_tables(base)
+    extra = serving.footprint_bytes(t1) - serving.footprint_bytes(t0)
+    # the two histories alone: 13*13 faces and 10^3 cells, 100 steps each, 8 bytes a value
+    assert extra >= (13 * 13 + 1000) * 100 * 8
