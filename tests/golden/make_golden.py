@@ -27,6 +27,7 @@ CASES = {
 # raw text of the reference's .tout files (header and every data line), kept
 # to check that the library's .tout writer reproduces them byte for byte
 TEXT_CASES = ["tem_pml_Ey", "material_test2_Ex", "huygens_box_Hz"]
+VMAT_CASES = ["debye_1", "debye_2", "FR4_at_7GHz"]
 
 
 def main():
@@ -44,6 +45,13 @@ def main():
             lines[name] = np.array(f.read().splitlines())
     np.savez_compressed(os.path.join(here, "tout_text.npz"), **lines)
     print("tout_text", {k: len(v) for k, v in lines.items()})
+    # the reference's volume material files that its known-answer cases use, as text
+    vm = {}
+    for name in VMAT_CASES:
+        with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", "MATERIAL_DATA", name + ".vmat")) as f:
+            vm[name] = np.array(f.read().splitlines())
+    np.savez_compressed(os.path.join(here, "vmat_text.npz"), **vm)
+    print("vmat_text", sorted(vm))
 
 
 if __name__ == "__main__":
