@@ -1,0 +1,550 @@
+"""Reader for the reference's problem input files (``.inp``).
+
+A GGI_TLM input is a sequence of packets: a keyword line (the names read by
+PROCESS_INPUT_FILE/read_input_file_geometry.F90 and read_input_file_solver.F90)
+followed by its data, read with Fortran list-directed input (values taken
+from as many lines as needed, the rest of the last line ignored, reals such
+as ``3.0-3`` allowed).  ``read_inp`` turns the packets the time loop needs
+into a ProblemSpec, restating the reference's set-up for axis-aligned
+geometry without rotations:
+
+- the mesh (set_mesh_parameters.F90:55-100): ``Mesh_cell_dimension`` gives
+  nx = NINT(extent / dl); ``Mesh_dimensions_in_cells`` gives dl as the mean
+  of the three spacings (evaluated as the reference's build does, see
+  cases.cubic_mesh_dl);
+- points, volumes and surfaces with a transformation of zero Euler angles
+  (GEOMETRY/transformations.F90: the point plus the translation);
+  ``rectangular_block`` volumes take the cells whose centres lie inside,
+  ``rectangle`` / ``xplane`` / ``yplane`` / ``zplane`` surfaces on a cell
+  boundary become face patches, ``rectangular_block`` surfaces closed boxes;
+- PML thicknesses in metres, NINT(t / dl) cells (TLM_PML_volume_materials.F90:465);
+- volume materials from ``.vmat`` files (ggi_tlm_b200.vmat), excitation
+  functions, point excitations, the Huygens surface, output points,
+  ``Simulation_time`` (n_timesteps = NINT(T / dt)) and ``set_small_to_zero``.
+
+Packets that only post-processing or other programs use are listed in
+``InpProblem.skipped``; geometry or packets that the GPU path does not
+support raise UnsupportedFeature.
+"""
+from __future__ import annotations
+
+import os
+import re
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional, Sequence, Tuple
+
+from .problem import (C0, MAT_PEC, MAT_PMC, SOURCE_HARD, SOURCE_SOFT, SURFACE_COMPONENTS, Block,
+                      ExcitationFunction, HuygensBox, HuygensOuter, HuygensPlane, OutputPoint, OutputSurface,
+                      OutputVolume, PointExcitation, ProblemSpec, UnsupportedFeature, VolumeMaterial, Z0, nint)
+
+GEOMETRY_PACKETS = ["periodic_boundary", "mesh_outer_boundary_dimension", "mesh_dimensions_in_cells",
+                    "mesh_cell_dimension", "volume_list", "surface_list", "line_list", "point_list", "pml",
+                    "new_mesh_generation", "no_geometry_vtk_files"]
+SOLVER_PACKETS = ["simulation_time", "volume_material_list", "surface_material_list",
+                  "outer_boundary_reflection_coefficient", "excitation_function_list", "excitation_point_list",
+                  "excitation_surface_list", "excitation_volume_list", "huygens_surface", "output_point_list",
+                  "ngspice_node_output_list", "output_surface_list", "output_volume_list",
+                  "output_volume_average_list", "output_volume_peak_list", "sar_volume_list",
+                  "far_field_surface_list", "periodic_boundary_far_field_surface", "frequency_output_surface_list",
+                  "frequency_output_volume_list_xyz", "frequency_output_volume_list",
+                  "frequency_domain_power_surface_list", "rcs_surface", "excitation_mode_list", "output_mode_list",
+                  "mode_stir_surface_list", "bicubic_warp_flag", "frequency_scale_flag", "compress_output_files",
+                  "reduced_c_factor", "wrapping_boundary_conditions", "random_number_seed",
+                  "ngspice_timestep_factor", "ngspice_lpf_alpha", "set_small_to_zero"]
+PACKETS = set(GEOMETRY_PACKETS + SOLVER_PACKETS)
+# packets that change nothing the time loop computes here
+NEUTRAL = {"new_mesh_generation", "no_geometry_vtk_files", "compress_output_files", "line_list",
+           "random_number_seed", "frequency_scale_flag"}
+# packets of other parts of the reference the GPU path does not run
+UNSUPPORTED = {"periodic_boundary", "surface_material_list", "excitation_surface_list", "excitation_volume_list",
+               "ngspice_node_output_list", "periodic_boundary_far_field_surface", "excitation_mode_list",
+               "mode_stir_surface_list", "wrapping_boundary_conditions", "ngspice_timestep_factor",
+               "ngspice_lpf_alpha"}
+
+# field component names (TLM_MODULES/TLM_Modules.F90:149-161): read_field_component
+# takes Ex..Hz, read_field_or_currrent_component also Jx..Jz, both comparing
+# the whole line; read_field_component_surface_output compares the first two
+# columns only ('(A2)') and adds the magnitudes em, hm, jm
+_FIELD = {"ex": "Ex", "ey": "Ey", "ez": "Ez", "hx": "Hx", "hy": "Hy", "hz": "Hz"}
+_FIELD_OR_CURRENT = {**_FIELD, "jx": "Jx", "jy": "Jy", "jz": "Jz"}
+_SURFACE_FIELD = {**_FIELD_OR_CURRENT, "em": "Em", "hm": "Hm", "jm": "Jm"}
+_FACES = {"centre", "xmin", "xmax", "ymin", "ymax", "zmin", "zmax"}  # read_centre_or_face
+# parameters per geometry type (read_volume_list.F90:107-159, read_surface_list.F90:108-220);
+# the types marked with a file name read that line before the parameters
+_VOLUME_PARAMS = {"rectangular_block2": 6, "rectangular_block": 3, "cylinder": 2, "sphere": 1, "tet": 12, "hex": 24,
+                  "pyramid_ram": 3, "pyramid": 2, "tet_volume_mesh": 1, "fill_surface": 1}
+_SURFACE_PARAMS = {"rectangular_block2": 6, "rectangular_block": 3, "cylinder": 2, "sphere": 1, "hemisphere": 1,
+                   "rectangle": 2, "circle": 1, "quad": 12, "xplane": 6, "yplane": 6, "zplane": 6, "triangle": 9,
+                   "annulus": 2, "split_ring": 3, "helix": 6, "triangulated_surface": 2,
+                   "vtk_triangulated_surface": 2, "stl_triangulated_surface": 2}
+_WITH_FILE = {"tet_volume_mesh", "triangulated_surface", "vtk_triangulated_surface", "stl_triangulated_surface"}
+# parameters per excitation function type, read_excitation_function_list.F90:108-160
+_N_PARAMS = {"impulse": 1, "gaussian_step": 3, "step": 2, "gaussian": 3, "sinusoid": 3, "gaussian_sinusoid": 5,
+             "differential_gaussian": 3}
+
+_REAL = re.compile(r"^([+-]?(?:\d+\.?\d*|\.\d+))(?:[eEdD]([+-]?\d+)|([+-]\d+))?$")
+
+
+def fortran_real(tok: str) -> float:
+    """A real as Fortran list-directed input reads it, exponent letter optional
+    (``1.0e-3``, ``1.0d-3``, ``1.0-3``)."""
+    m = _REAL.match(tok)
+    if not m:
+        raise ValueError(tok)
+    exp = m.group(2) or m.group(3)
+    return float(m.group(1) + ("e" + exp if exp else ""))
+
+
+class Records:
+    """The data lines of one packet, read as Fortran sequential records."""
+
+    def __init__(self, name: str, lines: Sequence[str]):
+        self.name = name
+        self.lines = list(lines)
+        self.pos = 0
+
+    def line(self) -> str:
+        if self.pos >= len(self.lines):
+            raise ValueError(f"{self.name} packet ends too early")
+        self.pos += 1
+        return self.lines[self.pos - 1]
+
+    def text(self) -> str:
+        """The next line read with '(A)' and converted to lower case; the
+        reference compares it whole with a keyword (trailing blanks ignored)."""
+        return self.line().rstrip().lower()
+
+    def peek_text(self, width: int = 256) -> str:
+        """The next line's first ``width`` columns in lower case, without
+        consuming it (a read followed by BACKSPACE)."""
+        if self.pos >= len(self.lines):
+            return ""
+        return self.lines[self.pos][:width].rstrip().lower()
+
+    def values(self, n: int) -> List[float]:
+        out: List[float] = []
+        while len(out) < n:
+            for tok in re.split(r"[\s,]+", self.line().strip()):
+                if not tok:
+                    continue
+                try:
+                    out.append(fortran_real(tok))
+                except ValueError:
+                    break  # a remark ends the values of this line
+                if len(out) == n:
+                    break
+        return out
+
+    def ints(self, n: int) -> List[int]:
+        return [int(v) for v in self.values(n)]
+
+
+def split_packets(lines: Sequence[str]) -> List[Tuple[str, List[str]]]:
+    """(keyword, data lines) of each packet in file order; blank lines and
+    lines before the first keyword (the title) are dropped."""
+    out: List[Tuple[str, List[str]]] = []
+    for raw in lines:
+        line = raw.rstrip("\n")
+        if not line.strip():
+            continue
+        tok = line.split()
+        if tok[0].lower() in PACKETS and (len(tok) == 1 or tok[1][0] in "!#"):
+            out.append((tok[0].lower(), []))
+        elif out:
+            out[-1][1].append(line)
+    return out
+
+
+@dataclass
+class Mesh:
+    xmin: float
+    ymin: float
+    zmin: float
+    dl: float
+    n: Tuple[int, int, int]
+
+    def lo(self, axis: int) -> float:
+        return (self.xmin, self.ymin, self.zmin)[axis]
+
+    def cell_of(self, p: Sequence[float]) -> Tuple[int, int, int]:
+        """get_cell_number: int((p - min) * (1/dl)) + 1 per axis, the
+        multiplication by 1/dl as the reference's build evaluates it."""
+        return tuple(int((p[a] - self.lo(a)) * (1.0 / self.dl)) + 1 for a in range(3))
+
+    def centres_in(self, axis: int, lo: float, hi: float) -> Tuple[int, int]:
+        """1-based range of cells along ``axis`` whose centres lie in [lo, hi];
+        a centre on the boundary is ambiguous under rounding and is refused."""
+        cells = []
+        for c in range(1, self.n[axis] + 1):
+            x = self.lo(axis) + (c - 0.5) * self.dl
+            if min(abs(x - lo), abs(x - hi)) < 1e-9 * self.dl:
+                raise UnsupportedFeature("a cell centre lies on a volume or surface boundary")
+            if lo < x < hi:
+                cells.append(c)
+        if not cells:
+            raise UnsupportedFeature("a volume or surface contains no cell")
+        return cells[0], cells[-1]
+
+    def boundary(self, axis: int, x: float) -> int:
+        """The cell boundary index k (between cells k and k+1) at coordinate x."""
+        k = (x - self.lo(axis)) / self.dl
+        if abs(k - round(k)) > 1e-6:
+            raise UnsupportedFeature("a surface does not lie on cell boundaries")
+        return int(round(k))
+
+
+def _transform(r: Records, what: str) -> Tuple[float, float, float]:
+    """A transformation (3 Euler angles in degrees, 3 translations); only zero angles are supported."""
+    t = r.values(6)
+    if any(v != 0.0 for v in t[:3]):
+        raise UnsupportedFeature(f"rotated {what}: only zero Euler angles are supported")
+    return t[3], t[4], t[5]
+
+
+@dataclass
+class InpProblem:
+    spec: ProblemSpec
+    skipped: List[str] = field(default_factory=list)
+    # per output point: (first, last, interval) timesteps, or None for every step
+    output_timing: List[Optional[Tuple[int, int, int]]] = field(default_factory=list)
+
+
+
+
+@dataclass
+class Shape:
+    """A volume or surface of the geometry lists after its transformation:
+    ``kind`` is the reference's type name, ``par`` its parameters and ``tr``
+    the translation (None for types this reader does not voxelise), and
+    ``rough`` marks a surface with a surface_roughness line."""
+
+    kind: str
+    par: Optional[List[float]]
+    tr: Optional[Tuple[float, float, float]]
+    rough: bool = False
+
+
+def _geometry_list(r: Records, what: str, counts: Dict[str, int], supported: set) -> Dict[int, Shape]:
+    """read_volume_list / read_surface_list: number, type line, [file name],
+    parameters, [surface_roughness + values], transformation."""
+    out: Dict[int, Shape] = {}
+    n = r.ints(1)[0]
+    for k in range(1, n + 1):
+        if r.ints(1)[0] != k:
+            raise ValueError(f"{r.name} packet: {what}s must be numbered in order")
+        kind = r.text()
+        if kind not in counts:
+            raise ValueError(f"{r.name} packet: unknown {what} type {kind!r}")
+        if kind in _WITH_FILE:
+            r.line()
+        par = r.values(counts[kind])
+        rough = False
+        if what == "surface" and r.peek_text(17) == "surface_roughness":
+            r.line()
+            r.values(1 if kind == "sphere" else 2)
+            rough = True
+        if kind in supported:
+            out[k] = Shape(kind, par, _transform(r, f"{what} {k}"), rough)
+        else:
+            r.values(6)  # its transformation
+            out[k] = Shape(kind, None, None, rough)
+    return out
+
+
+def _block_cells(mesh: Mesh, par, tr) -> Block:
+    """The cells whose centres lie inside an axis-aligned block of sides
+    ``par`` centred on the translation ``tr`` (build_volume_rectangular_block.F90)."""
+    rng = [mesh.centres_in(a, tr[a] - par[a] / 2.0, tr[a] + par[a] / 2.0) for a in range(3)]
+    return Block(rng[0][0], rng[0][1], rng[1][0], rng[1][1], rng[2][0], rng[2][1])
+
+
+def _surface_cells(mesh: Mesh, s: Shape, what: str):
+    """("box", ((i0, i1), (j0, j1), (k0, k1))) for a rectangular_block surface,
+    or ("plane", (axis, index, r0, r1), orient) for a planar one.  ``orient``
+    is +1 when the triangles' normal (v3-v1)x(v2-v1) points along -axis, the
+    orientation of build_surface_rectangle.F90 that HuygensPlane side 1
+    describes, and -1 when it points along +axis: build_surface_xplane.F90
+    (and y/z) order the corners so that the normal is +x for y2>y1, z2>z1,
+    -y for x2>x1, z2>z1 and +z for x2>x1, y2>y1."""
+    if s.par is None:
+        raise UnsupportedFeature(f"{what} on a surface of type {s.kind!r}")
+    if s.rough:
+        raise UnsupportedFeature(f"{what} on a surface with random roughness")
+    par, tr = s.par, s.tr
+    if s.kind == "rectangular_block":
+        b = _block_cells(mesh, par, tr)
+        return "box", ((b.i0, b.i1), (b.j0, b.j1), (b.k0, b.k1)), 1
+    if s.kind == "rectangle":  # lx by ly in the local xy-plane, centred on the translation
+        axis, orient = 2, 1
+        lo = [tr[0] - par[0] / 2.0, tr[1] - par[1] / 2.0, tr[2]]
+        hi = [tr[0] + par[0] / 2.0, tr[1] + par[1] / 2.0, tr[2]]
+    else:
+        axis = {"xplane": 0, "yplane": 1, "zplane": 2}[s.kind]
+        p1 = [par[a] + tr[a] for a in range(3)]
+        p2 = [par[3 + a] + tr[a] for a in range(3)]
+        if p1[axis] != p2[axis]:
+            raise ValueError(f"{s.kind} surface: the two corners differ in the normal coordinate")
+        d = [p2[a] - p1[a] for a in range(3)]
+        normal = (d[1] * d[2], -(d[0] * d[2]), d[0] * d[1])[axis]
+        if normal == 0.0:
+            raise UnsupportedFeature(f"{s.kind} surface of zero area")
+        orient = -1 if normal > 0.0 else 1
+        lo, hi = [min(a, b) for a, b in zip(p1, p2)], [max(a, b) for a, b in zip(p1, p2)]
+    t = [a for a in range(3) if a != axis]
+    return "plane", (axis + 1, mesh.boundary(axis, lo[axis]), mesh.centres_in(t[0], lo[t[0]], hi[t[0]]),
+                     mesh.centres_in(t[1], lo[t[1]], hi[t[1]])), orient
+
+
+def _timing(r: Records, dt: float) -> Optional[Tuple[int, int, int]]:
+    """read_output_time_information.F90 followed by set_output_time_information
+    (OUTPUT/output.F90:487-545): an optional output_timestep_information
+    (three integers) or output_time_information (three times, NINT(t/dt))
+    block, each value raised to at least 1; None when the block is absent
+    (every step)."""
+    w = r.peek_text()
+    if w == "output_timestep_information":
+        r.line()
+        first, last, step = (r.ints(1)[0] for _ in range(3))
+    elif w == "output_time_information":
+        r.line()
+        first, last, step = (nint(r.values(1)[0] / dt) for _ in range(3))
+    else:
+        return None
+    return max(first, 1), max(last, 1), max(step, 1)
+
+
+def _steps(t: Optional[Tuple[int, int, int]]) -> dict:
+    if t is None:
+        return dict(first_step=1, last_step=None, interval=1)
+    return dict(first_step=t[0], last_step=t[1], interval=t[2])
+
+
+def _component(r: Records, names: Dict[str, str], width: int = 256) -> str:
+    key = r.line()[:width].rstrip().lower()
+    if key not in names:
+        raise ValueError(f"{r.name} packet: unknown field component {key!r}")
+    return names[key]
+
+
+def _face(r: Records) -> str:
+    f = r.text()
+    if f not in _FACES:
+        raise ValueError(f"{r.name} packet: expected centre or a face name, got {f!r}")
+    return f
+
+
+def _logical(tok: str) -> bool:
+    """A list-directed LOGICAL value: optional '.', then T or F."""
+    t = tok.strip().lower().lstrip(".")
+    if not t or t[0] not in "tf":
+        raise ValueError(f"not a logical value: {tok!r}")
+    return t[0] == "t"
+
+
+def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial]) -> InpProblem:
+    """The ProblemSpec of a .inp file's lines; ``material(name)`` returns the
+    volume material of a dispersive Volume_material_list entry, ``name``
+    being the file name line as written (the reference opens name + '.vmat')."""
+    packets = split_packets(lines)
+    rec: Dict[str, Records] = {}
+    for name, data in packets:
+        if name in UNSUPPORTED:
+            raise UnsupportedFeature(f"{name} packet: not supported by the GPU path")
+        rec[name] = Records(name, data)
+    handled = {"mesh_outer_boundary_dimension", "mesh_cell_dimension", "mesh_dimensions_in_cells", "pml",
+               "volume_list", "surface_list", "point_list", "simulation_time", "volume_material_list",
+               "outer_boundary_reflection_coefficient", "excitation_function_list", "excitation_point_list",
+               "huygens_surface", "output_point_list", "output_surface_list", "output_volume_list",
+               "set_small_to_zero", "reduced_c_factor", "bicubic_warp_flag"}
+    skipped = [n for n, _ in packets if n not in handled]
+    # the mesh, MESH/set_mesh_parameters.F90:40-100: a cell size wins over a cell count
+    xmin, xmax, ymin, ymax, zmin, zmax = rec["mesh_outer_boundary_dimension"].values(6)
+    ext = (xmax - xmin, ymax - ymin, zmax - zmin)
+    if "mesh_cell_dimension" in rec:
+        dl = rec["mesh_cell_dimension"].values(1)[0]
+        n = tuple(max(1, nint(e / dl)) for e in ext)
+    elif "mesh_dimensions_in_cells" in rec:
+        nc = rec["mesh_dimensions_in_cells"].ints(3)
+        # the division by 3 as a multiplication by 1/3, as the reference's build compiles it
+        dl = (ext[0] / float(nc[0]) + ext[1] / float(nc[1]) + ext[2] / float(nc[2])) * (1.0 / 3.0)
+        n = tuple(nint(e / dl) for e in ext)
+    else:
+        raise ValueError("neither Mesh_cell_dimension nor Mesh_dimensions_in_cells is given")
+    mesh = Mesh(xmin, ymin, zmin, dl, n)
+    reduced_c = rec["reduced_c_factor"].values(1)[0] if "reduced_c_factor" in rec else 1.0
+    if "bicubic_warp_flag" in rec and _logical(rec["bicubic_warp_flag"].line().split()[0]):
+        raise UnsupportedFeature("bicubic frequency warping of the material filters")
+    dt = dl / (2.0 * C0 / reduced_c)  # TLM_SOLVER/set_TLM_solver_parameters.F90:93-95
+    steps = nint(rec["simulation_time"].values(1)[0] / dt)
+    R = tuple(rec["outer_boundary_reflection_coefficient"].values(6)) \
+        if "outer_boundary_reflection_coefficient" in rec else (0.0,) * 6
+    spec = ProblemSpec(nx=n[0], ny=n[1], nz=n[2], dl=dl, n_timesteps=steps, R=R, origin=(xmin, ymin, zmin),
+                       reduced_c=reduced_c)
+    # PML, read_pml.F90:70-150: a line of six thicknesses (metres) or one for
+    # all sides, the same for the reflection coefficients, then the order
+    if "pml" in rec:
+        r = rec["pml"]
+
+        def six(line: str) -> List[float]:
+            vals = []
+            for tok in re.split(r"[\s,]+", line.strip()):
+                try:
+                    vals.append(fortran_real(tok))
+                except ValueError:
+                    break
+            if not vals:
+                raise ValueError(f"PML packet: no value on {line!r}")
+            return vals[:6] if len(vals) >= 6 else vals[:1] * 6
+
+        t, rr = six(r.line()), six(r.line())
+        spec.pml_cells = tuple(nint(v / dl) for v in t)  # TLM_PML_volume_materials.F90:465
+        spec.pml_r = tuple(rr)
+        spec.pml_order = r.ints(1)[0]
+    # geometry, GEOMETRY/build_*.F90 with a translation only
+    points: Dict[int, Tuple[float, float, float]] = {}
+    if "point_list" in rec:
+        r = rec["point_list"]
+        for k in range(1, r.ints(1)[0] + 1):
+            if r.ints(1)[0] != k:
+                raise ValueError("Point_list packet: points must be numbered in order")
+            p = r.values(3)
+            tr = _transform(r, f"point {k}")
+            points[k] = (p[0] + tr[0], p[1] + tr[1], p[2] + tr[2])
+    volumes = _geometry_list(rec["volume_list"], "volume", _VOLUME_PARAMS, {"rectangular_block"}) \
+        if "volume_list" in rec else {}
+    surfaces = _geometry_list(rec["surface_list"], "surface", _SURFACE_PARAMS,
+                              {"rectangular_block", "rectangle", "xplane", "yplane", "zplane"}) \
+        if "surface_list" in rec else {}
+
+    def volume_block(v: int, what: str) -> Block:
+        s = volumes[v]
+        if s.par is None:
+            raise UnsupportedFeature(f"{what} on a volume of type {s.kind!r}")
+        return _block_cells(mesh, s.par, s.tr)
+
+    # volume materials, read_volume_material_list.F90:90-180
+    if "volume_material_list" in rec:
+        r = rec["volume_material_list"]
+        for k in range(1, r.ints(1)[0] + 1):
+            if r.ints(1)[0] != k:
+                raise ValueError("Volume_material_list packet: materials must be numbered in order")
+            kind = r.text()
+            if kind == "dispersive":
+                mat = material(r.line().strip())
+            elif kind in ("pec", "pmc"):
+                mat = VolumeMaterial(type=MAT_PEC if kind == "pec" else MAT_PMC)
+            else:
+                raise ValueError(f"Volume_material_list packet: unknown material type {kind!r}")
+            spec.materials.append(mat)
+            nv = r.ints(1)[0]
+            for v in r.ints(nv):
+                spec.material_regions.append((k, volume_block(v, "a volume material")))
+    # excitation functions, read_excitation_function_list.F90:92-250
+    if "excitation_function_list" in rec:
+        r = rec["excitation_function_list"]
+        for k in range(1, r.ints(1)[0] + 1):
+            if r.ints(1)[0] != k:
+                raise ValueError("Excitation_function_list packet: functions must be numbered in order")
+            kind = r.text()
+            if kind not in _N_PARAMS:
+                raise UnsupportedFeature(f"excitation function {kind!r}")
+            spec.functions.append(ExcitationFunction(kind, tuple(r.values(_N_PARAMS[kind]))))
+    # point excitations, read_excitation_point_list.F90:75-110
+    if "excitation_point_list" in rec:
+        r = rec["excitation_point_list"]
+        for k in range(1, r.ints(1)[0] + 1):
+            if r.ints(1)[0] != k:
+                raise ValueError("Excitation_point_list packet: points must be numbered in order")
+            fn, pt = r.ints(1)[0], r.ints(1)[0]
+            comp = _component(r, _FIELD_OR_CURRENT)
+            face = _face(r)
+            kind = r.text()
+            if kind not in ("soft", "hard"):
+                raise ValueError(f"Excitation_point_list packet: source type {kind!r}")
+            spec.point_excitations.append(PointExcitation(mesh.cell_of(points[pt]), comp, fn,
+                                                          SOURCE_SOFT if kind == "soft" else SOURCE_HARD, face=face))
+    # the Huygens surface, read_huygens_surface.F90:89-200
+    if "huygens_surface" in rec:
+        r = rec["huygens_surface"]
+        surf, side = r.ints(1)[0], r.ints(1)[0]
+        if side not in (1, -1):
+            raise ValueError("Huygens_surface packet: the side must be 1 or -1")
+        z0 = Z0
+        if r.peek_text() == "wave_impedance":
+            r.line()
+            z0 = r.values(1)[0]
+        fn = r.ints(1)[0]
+        angles = []
+        for _ in range(2):  # '(A1)': a line starting with r or R asks for a random choice
+            if r.pos < len(r.lines) and r.lines[r.pos][:1] in ("r", "R"):
+                raise UnsupportedFeature("random Huygens wave direction or polarisation")
+            angles += r.values(2)
+        kt, kp, et, ep = angles
+        if surf == 0:
+            spec.huygens = HuygensOuter(fn, kt, kp, et, ep, wave_impedance=z0)
+        else:
+            kind, g, orient = _surface_cells(mesh, surfaces[surf], "a Huygens surface")
+            if kind == "box":
+                spec.huygens = HuygensBox(g[0], g[1], g[2], fn, kt, kp, et, ep, side=side, wave_impedance=z0)
+            else:
+                spec.huygens = HuygensPlane(g[0], g[1], g[2], g[3], fn, kt, kp, et, ep, side=side * orient,
+                                            wave_impedance=z0)
+    # output points, read_output_point_list.F90:85-125
+    timing: List[Optional[Tuple[int, int, int]]] = []
+    if "output_point_list" in rec:
+        r = rec["output_point_list"]
+        for k in range(1, r.ints(1)[0] + 1):
+            if r.ints(1)[0] != k:
+                raise ValueError("Output_point_list packet: points must be numbered in order")
+            pt = r.ints(1)[0]
+            comp = _component(r, _FIELD)
+            spec.outputs.append(OutputPoint(mesh.cell_of(points[pt]), comp, _face(r)))
+            timing.append(_timing(r, dt))
+    # output surfaces, read_output_surface_list.F90:88-135: side 1, -1, or 0
+    # (J from both sides, on the faces of side -1)
+    if "output_surface_list" in rec:
+        r = rec["output_surface_list"]
+        for k in range(1, r.ints(1)[0] + 1):
+            if r.ints(1)[0] != k:
+                raise ValueError("Output_surface_list packet: surfaces must be numbered in order")
+            surf, side = r.ints(1)[0], r.ints(1)[0]
+            if side not in (1, -1, 0):
+                raise ValueError("Output_surface_list packet: the side must be 1, -1 or 0")
+            comp = _component(r, _SURFACE_FIELD, width=2)
+            if side == 0 and comp not in ("Jx", "Jy", "Jz", "Jm"):
+                raise ValueError("Output_surface_list packet: output on both sides is for Jx, Jy, Jz, Jmagnitude")
+            kind, g, orient = _surface_cells(mesh, surfaces[surf], "an output surface")
+            eff = (-1 if side == 0 else side) * orient
+            geo = dict(box=g) if kind == "box" else dict(plane=g)
+            spec.output_surfaces.append(OutputSurface(comp, side=eff, both_sides=side == 0,
+                                                      **geo, **_steps(_timing(r, dt))))
+    # output volumes, read_output_volume_list.F90:85-105
+    if "output_volume_list" in rec:
+        r = rec["output_volume_list"]
+        for k in range(1, r.ints(1)[0] + 1):
+            if r.ints(1)[0] != k:
+                raise ValueError("Output_volume_list packet: volumes must be numbered in order")
+            v = r.ints(1)[0]
+            comp = _component(r, _FIELD)
+            spec.output_volumes.append(OutputVolume(volume_block(v, "an output volume"), comp, "field",
+                                                    **_steps(_timing(r, dt))))
+    if "set_small_to_zero" in rec:  # read_small_to_zero.F90:55-59
+        r = rec["set_small_to_zero"]
+        spec.small_to_zero = (r.ints(1)[0], r.values(1)[0])
+    return InpProblem(spec, skipped, timing)
+
+
+def vmat_in(directory: str) -> Callable[[str], VolumeMaterial]:
+    """A material resolver reading ``<directory>/<name>.vmat``."""
+    from .vmat import read_vmat
+
+    return lambda name: read_vmat(os.path.join(directory, name + ".vmat"))
+
+
+def read_inp_file(path: str, material: Optional[Callable[[str], VolumeMaterial]] = None) -> InpProblem:
+    """read_inp of a file; material file names resolve against the file's
+    directory unless ``material`` is given.  The text is read as Latin-1: the
+    reference's inputs hold stray non-ASCII bytes in remarks."""
+    with open(path, encoding="latin-1") as f:
+        lines = f.read().splitlines()
+    return read_inp(lines, material or vmat_in(os.path.dirname(os.path.abspath(path))))

@@ -391,6 +391,7 @@ class HuygensPlane:
     etheta: float
     ephi: float
     side: int = 1
+    wave_impedance: float = Z0  # the optional wave_impedance line (read_huygens_surface.F90:107-116)
 
 
 @dataclass
@@ -417,6 +418,7 @@ class HuygensBox:
     etheta: float
     ephi: float
     side: int = 1
+    wave_impedance: float = Z0  # the optional wave_impedance line (read_huygens_surface.F90:107-116)
 
 
 @dataclass
@@ -432,6 +434,7 @@ class HuygensOuter:
     kphi: float
     etheta: float
     ephi: float
+    wave_impedance: float = Z0
 
 
 @dataclass
@@ -1112,7 +1115,7 @@ def build_tables(spec: ProblemSpec) -> dict:
 
     # Huygens surface data, huygens_surface.F90:247-715
     if outer:
-        K, Ei, Hi = huygens_vectors(hs.ktheta, hs.kphi, hs.etheta, hs.ephi)
+        K, Ei, Hi = huygens_vectors(hs.ktheta, hs.kphi, hs.etheta, hs.ephi, hs.wave_impedance)
         cells = []  # huygens_surface.F90:517-612 order
         for cz in range(1, nz + 1):
             for cy in range(1, ny + 1):
@@ -1148,7 +1151,7 @@ def build_tables(spec: ProblemSpec) -> dict:
                       hs_c=C0 / spec.reduced_c, hs_fn=hs.function, hs_outer=1,
                       hs_cell=np.array(cells, dtype=np.int32).reshape(-1))
     elif hs is not None:
-        K, Ei, Hi = huygens_vectors(hs.ktheta, hs.kphi, hs.etheta, hs.ephi)
+        K, Ei, Hi = huygens_vectors(hs.ktheta, hs.kphi, hs.etheta, hs.ephi, hs.wave_impedance)
         norms, offsets, fexc = [], [], []
         xmin0, ymin0, zmin0 = spec.origin
         cents = []

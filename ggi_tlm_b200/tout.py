@@ -12,7 +12,7 @@ reference's post-processing reads are unchanged.
 """
 from __future__ import annotations
 
-from typing import Iterable, List, Sequence, Tuple
+from typing import Iterable, List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -55,27 +55,46 @@ def write_tout(path: str, rows: Iterable[Tuple[float, int, float]], n_points: in
             f.write(data_line(t, p, v) + "\n")
 
 
-def field_rows(tables: dict, centre: np.ndarray, face: np.ndarray, first_step: int = 1) -> List[Tuple[float, int, float]]:
+def output_flag(timestep: int, timing: Optional[Tuple[int, int, int]]) -> bool:
+    """get_output_flag (OUTPUT/output.F90:570-600): output on the steps
+    first..last that are a multiple of interval after first; None (no
+    timing block) is every step."""
+    if timing is None:
+        return True
+    first, last, interval = timing
+    return first <= timestep <= last and (timestep - first) % interval == 0
+
+
+def field_rows(tables: dict, centre: np.ndarray, face: np.ndarray, first_step: int = 1,
+               timing: Optional[Sequence[Optional[Tuple[int, int, int]]]] = None) -> List[Tuple[float, int, float]]:
     """Rows of a .field.tout for output points sampled every step, in the
     reference's order: each step the cell-centre points at the cell-output
     time (timestep-1)*dt (cell_output_point, output_points.F90:586-600),
     then the face points half a step later (face_output_points, :428-441).
     ``centre`` is [n_centre_points, steps] (probe_series), ``face`` is
     [n_face_points, steps] (GpuMesh.face_output); the point numbers are the
-    tables' ``out_point_no`` / ``fprobe_point_no``."""
+    tables' ``out_point_no`` / ``fprobe_point_no``.  ``timing``, indexed by
+    output point number - 1, gives each point's (first, last, interval)
+    output steps or None for every step (the .inp reader's output_timing)."""
     dt = float(tables["dt"])
     cno = np.asarray(tables.get("out_point_no", np.arange(1, centre.shape[0] + 1)))
     fno = np.asarray(tables.get("fprobe_point_no", np.arange(1, face.shape[0] + 1)))
     n_steps = centre.shape[1] if centre.size else (face.shape[1] if face.size else 0)
+
+    def on(point: int, timestep: int) -> bool:
+        return timing is None or output_flag(timestep, timing[point - 1])
+
     rows = []
     for s in range(n_steps):
         timestep = first_step + s
         time = (timestep - 1) * dt
         for k in range(centre.shape[0]):
-            rows.append((time, int(cno[k]), float(centre[k, s])))
+            if on(int(cno[k]), timestep):
+                rows.append((time, int(cno[k]), float(centre[k, s])))
         time = time + dt / 2.0
         for k in range(face.shape[0]):
-            rows.append((time, int(fno[k]), float(face[k, s])))
+            if on(int(fno[k]), timestep):
+                rows.append((time, int(fno[k]), float(face[k, s])))
     return rows
 
 

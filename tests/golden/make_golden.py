@@ -27,7 +27,16 @@ CASES = {
 # raw text of the reference's .tout files (header and every data line), kept
 # to check that the library's .tout writer reproduces them byte for byte
 TEXT_CASES = ["tem_pml_Ey", "material_test2_Ex", "huygens_box_Hz"]
-VMAT_CASES = ["debye_1", "debye_2", "FR4_at_7GHz"]
+VMAT_CASES = ["debye_1", "debye_2", "FR4_at_7GHz", "mur_lorentz"]
+# the known-answer cases' problem input files, as text, for the .inp reader;
+# read as Latin-1 since their remarks hold stray non-ASCII bytes
+INP_CASES = {
+    "tem_pml": "TEM_PML_TEST/PROBLEM_SPECIFICATION_FILES/TEM_cell.inp",
+    "tem_material": "TEM_MATERIAL_TEST/PROBLEM_SPECIFICATION_FILES/TEM_cell.inp",
+    "material_stability": "MATERIAL_STABILITY_TEST/PROBLEM_SPECIFICATION_FILES/cavity.inp",
+    "material_test2": "MATERIAL_TEST2/PROBLEM_SPECIFICATION_FILES/mat_test.inp",
+    "huygens_box": "HUYGENS_SURFACE/PROBLEM_SPECIFICATION_FILES/huygens_test.inp",
+}
 
 
 def main():
@@ -52,6 +61,12 @@ def main():
             vm[name] = np.array(f.read().splitlines())
     np.savez_compressed(os.path.join(here, "vmat_text.npz"), **vm)
     print("vmat_text", sorted(vm))
+    inp = {}
+    for name, rel in INP_CASES.items():
+        with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", rel), encoding="latin-1") as f:
+            inp[name] = np.array(f.read().splitlines())
+    np.savez_compressed(os.path.join(here, "inp_text.npz"), **inp)
+    print("inp_text", {k: len(v) for k, v in inp.items()})
 
 
 if __name__ == "__main__":

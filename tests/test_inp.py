@@ -1,0 +1,383 @@
+"""The .inp reader (ggi_tlm_b200/inp.py) on the reference's own problem
+input files (kept as text in tests/golden/inp_text.npz by
+tests/golden/make_golden.py) and on small inputs written here.
+
+The five known-answer inputs must give tables equal, array for array, to
+the hand-built known-answer specs, whose probe series the oracle pins
+against the reference's golden output; the HUYGENS_SURFACE input, read
+whole (30 output points, 3 output surfaces, 3 output volumes), must
+reproduce all six golden centre series through the oracle.  The small
+inputs check the reader's rules one at a time: Fortran reals, packet
+keywords, plane orientation, output timing, refusals.  GPU: the whole
+HUYGENS_SURFACE input against the oracle."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from ggi_tlm_b200 import capi, cases, inp
+from ggi_tlm_b200.problem import (Z0, HuygensOuter, HuygensPlane, UnsupportedFeature, build_tables,
+                                  material_coefficients, probe_series)
+from ggi_tlm_b200.tout import field_rows, output_flag
+from ggi_tlm_b200.vmat import parse_vmat
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(os.path.dirname(HERE), "oracle"))
+import oracle  # noqa: E402
+
+KAT = {"tem_pml": "tem_pml_Ey", "tem_material": "tem_material_Ey", "material_stability": "material_stability_Ey",
+       "material_test2": "material_test2_Ex", "huygens_box": "huygens_box_Ex"}
+TOL = 5e-7  # the golden series' E16.7 print precision
+
+
+def inputs():
+    d = np.load(os.path.join(HERE, "golden", "inp_text.npz"))
+    return {k: [str(x) for x in d[k]] for k in d.files}
+
+
+def materials(name):
+    """The material resolver: MATERIAL_DIRECTORY/<name> -> the fixture's .vmat text."""
+    d = np.load(os.path.join(HERE, "golden", "vmat_text.npz"))
+    return parse_vmat([str(x) for x in d[name.split("/")[-1]]])[0]
+
+
+def read(name):
+    return inp.read_inp(inputs()[name], materials)
+
+
+def same_tables(a, b):
+    keys = set(a) | set(b)
+    return [k for k in keys if k not in a or k not in b or
+            np.asarray(a[k]).shape != np.asarray(b[k]).shape or not np.array_equal(np.asarray(a[k]), np.asarray(b[k]))]
+
+
+@pytest.mark.parametrize("name", sorted(KAT))
+def test_known_answer_inputs_give_the_known_answer_tables(name):
+    p = read(name)
+    spec = p.spec
+    if name == "huygens_box":  # the known-answer spec keeps output point 1 only
+        assert len(spec.outputs) == 30 and len(spec.output_surfaces) == 3 and len(spec.output_volumes) == 3
+        spec.outputs, spec.output_surfaces, spec.output_volumes = spec.outputs[:1], [], []
+    assert p.skipped == []
+    assert same_tables(build_tables(spec), build_tables(cases.KAT_CASES[KAT[name]]())) == []
+
+
+def test_lorentz_material_file_is_the_known_answer_material():
+    a = material_coefficients(materials("MATERIAL_DIRECTORY/mur_lorentz"), 1e-4, 1e-4 / (2 * 299792458.0))
+    want = cases.kat_material_test2().materials[0]
+    b = material_coefficients(want, 1e-4, 1e-4 / (2 * 299792458.0))
+    assert a.keys() == b.keys() and all(np.array_equal(a[k], b[k]) for k in a)
+
+
+def test_huygens_input_reproduces_all_golden_centre_series():
+    """Output points 1, 6, 11, 16, 21, 26 of huygens_test.inp are Ex..Hz at
+    the centre; the face points and the output surfaces and volumes ride
+    along in the same run."""
+    p = read("huygens_box")
+    t = build_tables(p.spec)
+    assert list(t["out_point_no"]) == [1, 6, 11, 16, 21, 26]
+    assert int(t["n_face_probes"]) == 24
+    series = probe_series(t, oracle.Oracle(t).run(t["n_timesteps"]))
+    for k, comp in enumerate(("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")):
+        g = np.load(os.path.join(HERE, "golden", f"huygens_box_{comp}.npz"))
+        v = np.where(np.abs(series[k]) < 1e-30, 0.0, series[k])
+        assert np.linalg.norm(v - g["value"]) / np.linalg.norm(g["value"]) < TOL, comp
+
+
+def test_huygens_input_output_surfaces_and_volumes():
+    """The xplane/yplane/zplane output surfaces with side -1 over the whole
+    mesh, Emagnitude on steps 1, 5, ..., 117 (first step 0 raised to 1), and
+    the 2 x 2 x 0.1 m output volume: one layer of 20 x 20 cells at z = 0.05."""
+    p = read("huygens_box")
+    s1, s2, s3 = p.spec.output_surfaces
+    # xplane and zplane corners ascending: normal +axis, so side -1 samples the faces of HuygensPlane side 1;
+    # yplane corners ascending: normal -y, so side -1 samples side -1
+    assert (s1.plane, s1.side) == ((1, 20, (1, 40), (1, 40)), 1)
+    assert (s2.plane, s2.side) == ((2, 20, (1, 40), (1, 40)), -1)
+    assert (s3.plane, s3.side) == ((3, 20, (1, 40), (1, 40)), 1)
+    assert all((s.component, s.first_step, s.last_step, s.interval, s.both_sides) == ("Em", 1, 120, 4, False)
+               for s in (s1, s2, s3))
+    v = p.spec.output_volumes
+    assert [o.component for o in v] == ["Hx", "Hy", "Hz"]
+    b = v[0].region
+    assert (b.i0, b.i1, b.j0, b.j1, b.k0, b.k1) == (11, 30, 11, 30, 21, 21)
+    t = build_tables(p.spec)
+    shapes = capi.output_surface_shapes(t)
+    assert shapes == [(30, 1600)] * 3
+
+
+# ---------------------------------------------------------------------------
+# the reader's rules on small inputs
+# ---------------------------------------------------------------------------
+BASE = """# a small test problem
+Mesh_outer_boundary_dimension
+0.0 1.0  0.0 1.0  0.0 1.0
+Mesh_cell_dimension
+0.1
+Point_list
+1
+1
+0.55 0.55 0.55
+0 0 0
+0 0 0
+Excitation_function_list
+1
+1
+gaussian
+1.0 1e-9 3e-9
+Simulation_time
+1e-8
+"""
+
+
+def small(extra="", base=BASE):
+    return inp.read_inp((base + extra).splitlines(), materials)
+
+
+def test_fortran_reals():
+    assert inp.fortran_real("3.0-3") == 3.0e-3
+    assert inp.fortran_real("1.5d+2") == 150.0
+    assert inp.fortran_real("2E1") == 20.0
+    assert inp.fortran_real(".5") == 0.5 and inp.fortran_real("5.") == 5.0 and inp.fortran_real("-7") == -7.0
+    for bad in ("x", "1.0e", "--1", "1,0"):
+        with pytest.raises(ValueError):
+            inp.fortran_real(bad)
+    # list-directed: values spill over lines, a remark ends a line's values
+    r = inp.Records("t", ["1 2 ! remark 3", "4,5 6 7"])
+    assert r.values(4) == [1.0, 2.0, 4.0, 5.0]
+
+
+def test_packet_keywords():
+    pk = inp.split_packets(["title line", "MESH_CELL_DIMENSION   ! remark", "0.1", "", "simulation_time",
+                            "pml 3 cells", "1e-8"])
+    assert pk == [("mesh_cell_dimension", ["0.1"]), ("simulation_time", ["pml 3 cells", "1e-8"])]
+
+
+def test_small_problem_mesh_time_and_points():
+    p = small("""Excitation_point_list
+1
+1
+1
+1
+Jz
+xmax
+hard
+Output_point_list
+2
+1
+1
+Ey
+centre
+output_time_information
+2e-9
+5e-9
+0.5e-9
+2
+1
+Hx
+zmin
+output_timestep_information
+0
+7
+3
+""")
+    s = p.spec
+    assert (s.nx, s.ny, s.nz, s.dl) == (10, 10, 10, 0.1)
+    dt = 0.1 / (2 * 299792458.0)
+    assert s.n_timesteps == round(1e-8 / dt)
+    e = s.point_excitations[0]
+    assert (e.cell, e.component, e.face, e.source_type) == ((6, 6, 6), "Jz", "xmax", 0)
+    assert [(o.cell, o.component, o.face) for o in s.outputs] == [((6, 6, 6), "Ey", "centre"), ((6, 6, 6), "Hx", "zmin")]
+    assert p.output_timing == [(round(2e-9 / dt), round(5e-9 / dt), round(0.5e-9 / dt)), (1, 7, 3)]
+    assert [ts for ts in range(1, 12) if output_flag(ts, p.output_timing[1])] == [1, 4, 7]
+
+
+def test_cell_count_mesh_and_pml():
+    base = BASE.replace("Mesh_cell_dimension\n0.1\n", "Mesh_dimensions_in_cells\n20 20 20\n")
+    p = small("""PML
+0.2   ! the same thickness on every side
+1e-3 1e-3 1e-3 1e-3 1e-3 1e-2
+3
+""", base)
+    s = p.spec
+    assert (s.nx, s.dl) == (20, 0.05)
+    assert s.pml_cells == (4,) * 6 and s.pml_r == (1e-3,) * 5 + (1e-2,) and s.pml_order == 3
+    # a cell size wins over a cell count
+    both = BASE + "Mesh_dimensions_in_cells\n20 20 20\n"
+    assert small("", both).spec.nx == 10
+
+
+def test_plane_orientation_and_huygens_variants():
+    surf = """Surface_list
+3
+1
+zplane
+0.0 0.0 0.5   1.0 1.0 0.5
+0 0 0
+0 0 0
+2
+zplane
+1.0 0.0 0.5   0.0 1.0 0.5
+0 0 0
+0 0 0
+3
+rectangle
+1.0 1.0
+0 0 0
+0.5 0.5 0.5
+"""
+    hs = "Huygens_surface\n{n}\n1\n{z}1\n0.0 0.0\n1.0 0.0\n"
+    got = {}
+    for n in (1, 2, 3):
+        got[n] = small(surf + hs.format(n=n, z="")).spec.huygens
+        assert isinstance(got[n], HuygensPlane) and (got[n].axis, got[n].index) == (3, 5)
+    # ascending zplane corners: normal +z, the other side of the rectangle's -z; swapping x flips it back
+    assert (got[1].side, got[2].side, got[3].side) == (-1, 1, 1)
+    # a wave impedance other than Z0 scales H only
+    t0 = build_tables(small(surf + hs.format(n=3, z="")).spec)
+    t1 = build_tables(small(surf + hs.format(n=3, z="wave_impedance\n100.0\n")).spec)
+    assert np.array_equal(t0["hs_Ei"], t1["hs_Ei"])
+    assert np.allclose(t1["hs_Hi"], t0["hs_Hi"] * (Z0 / 100.0), rtol=1e-15, atol=0)
+    assert isinstance(small(hs.format(n=0, z="")).spec.huygens, HuygensOuter)
+    with pytest.raises(UnsupportedFeature):
+        small(surf + "Huygens_surface\n3\n1\n1\nrandom\n1.0 0.0\n")
+    with pytest.raises(ValueError):
+        small(surf + "Huygens_surface\n3\n2\n1\n0.0 0.0\n1.0 0.0\n")
+
+
+def test_output_surface_both_sides_and_volumes():
+    geo = """Volume_list
+1
+1
+rectangular_block
+0.4 0.4 0.4
+0 0 0
+0.5 0.5 0.5
+Surface_list
+1
+1
+rectangular_block
+0.4 0.4 0.4
+0 0 0
+0.5 0.5 0.5
+"""
+    p = small(geo + """Output_surface_list
+2
+1
+1
+0
+Jmagnitude
+2
+1
+1
+Hy
+output_timestep_information
+2
+10
+2
+Output_volume_list
+1
+1
+1
+Ez
+""")
+    a, b = p.spec.output_surfaces
+    assert (a.component, a.side, a.both_sides, a.box) == ("Jm", -1, True, ((4, 7), (4, 7), (4, 7)))
+    assert (b.component, b.side, b.first_step, b.last_step, b.interval) == ("Hy", 1, 2, 10, 2)
+    v = p.spec.output_volumes[0]
+    assert (v.component, v.kind, v.first_step, v.last_step, v.region.i0, v.region.i1) == ("Ez", "field", 1, None, 4, 7)
+    with pytest.raises(ValueError):  # both sides is for J only
+        small(geo + "Output_surface_list\n1\n1\n1\n0\nEx\n")
+
+
+@pytest.mark.parametrize("extra, match", [
+    ("Volume_list\n1\n1\nrectangular_block\n0.4 0.4 0.4\n0 0 45\n0.5 0.5 0.5\n", "rotated volume"),
+    ("Volume_list\n1\n1\nsphere\n0.2\n0 0 0\n0.5 0.5 0.5\nVolume_material_list\n1\n1\nPEC\n1\n1\n",
+     "type 'sphere'"),                                                                      # not voxelised here
+    ("Volume_list\n1\n1\nrectangular_block\n0.5 0.5 0.5\n0 0 0\n0.5 0.5 0.5\nVolume_material_list\n1\n1\nPEC\n1\n1\n",
+     "centre lies on"),                                                                      # a face through centres
+    ("Surface_material_list\n0\n", "surface_material_list packet"),
+    ("Bicubic_warp_flag\n.true.\n", "bicubic"),
+    ("Excitation_function_list\n1\n1\nnoise\n1.0\n", "function 'noise'"),
+    ("Output_point_list\n1\n2\n1\nEx\ncentre\n", "numbered in order"),                                  # numbering
+    ("Output_point_list\n1\n1\n1\nJx\ncentre\n", "component 'jx'"),                                  # not a field
+    ("Surface_list\n1\n1\nrectangle\n1.0 1.0\nsurface_roughness\n0.01 0.1\n0 0 0\n0.5 0.5 0.5\n"
+     "Huygens_surface\n1\n1\n1\n0 0\n1 0\n", "roughness"),                               # random roughness
+])
+def test_refusals(extra, match):
+    """Inputs the GPU path cannot run exactly raise UnsupportedFeature; a
+    malformed input raises ValueError, as the reference stops with an error."""
+    base = BASE.replace("Excitation_function_list\n1\n1\ngaussian\n1.0 1e-9 3e-9\n", "") \
+        if "Excitation_function_list" in extra else BASE
+    err = ValueError if match in ("numbered in order", "component 'jx'") else UnsupportedFeature
+    with pytest.raises(err, match=match) as e:
+        small(extra, base)
+    assert (e.type is UnsupportedFeature) == (err is UnsupportedFeature)
+
+
+def test_neutral_packets_are_listed_and_pec_materials():
+    p = small("""New_mesh_generation
+No_geometry_vtk_files
+Far_field_surface_list
+0
+Volume_list
+1
+1
+rectangular_block
+0.4 0.4 0.4
+0 0 0
+0.5 0.5 0.5
+Volume_material_list
+1
+1
+PMC
+1
+1
+Bicubic_warp_flag
+F
+""")
+    assert p.skipped == ["new_mesh_generation", "no_geometry_vtk_files", "far_field_surface_list"]
+    assert p.spec.materials[0].type == 2 and p.spec.material_regions[0][1].i0 == 4
+
+
+def test_field_rows_follow_output_timing():
+    p = small("""Output_point_list
+2
+1
+1
+Ex
+centre
+output_timestep_information
+2
+6
+2
+2
+1
+Ey
+centre
+""")
+    p.spec.n_timesteps = 8
+    t = build_tables(p.spec)
+    centre = np.arange(16, dtype=float).reshape(2, 8) + 1.0
+    rows = field_rows(t, centre, np.zeros((0, 8)), timing=p.output_timing)
+    assert [(r[1], round(r[0] / t["dt"]) + 1) for r in rows if r[1] == 1] == [(1, 2), (1, 4), (1, 6)]
+    assert sum(1 for r in rows if r[1] == 2) == 8
+
+
+@pytest.mark.gpu
+def test_gpu_huygens_input_matches_oracle(gpu_lib):
+    p = read("huygens_box")
+    t = build_tables(p.spec)
+    o = oracle.Oracle(t)
+    want = o.run(t["n_timesteps"])
+    want_faces = o.face_probes()
+    want_surf = oracle.output_surfaces(t)
+    with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64) as g:
+        g.run(t["n_timesteps"])
+        got, faces, surf = g.cell_output(), g.face_output(), g.output_surfaces()
+    for a, b in zip(probe_series(t, got), probe_series(t, want)):
+        assert np.linalg.norm(a - b) <= 1e-10 * np.linalg.norm(b)
+    assert np.linalg.norm(faces - want_faces) <= 1e-10 * np.linalg.norm(want_faces)
+    for a, b in zip(surf, want_surf):
+        assert a.shape == b.shape and np.linalg.norm(a - b) <= 1e-10 * np.linalg.norm(b)
