@@ -33,9 +33,10 @@ import re
 from dataclasses import dataclass, field
 from typing import Callable, Dict, List, Optional, Sequence, Tuple
 
-from .problem import (C0, MAT_PEC, MAT_PMC, SOURCE_HARD, SOURCE_SOFT, SURFACE_COMPONENTS, Block,
-                      ExcitationFunction, HuygensBox, HuygensOuter, HuygensPlane, OutputPoint, OutputSurface,
-                      OutputVolume, PointExcitation, ProblemSpec, UnsupportedFeature, VolumeMaterial, Z0, nint)
+from .problem import (C0, MAT_PEC, MAT_PMC, SOURCE_HARD, SOURCE_SOFT, Block, DFTSurface, ExcitationFunction,
+                      FarFieldSurface, FrequencyOutputVolume, HuygensBox, HuygensOuter, HuygensPlane, OutputPoint,
+                      OutputSurface, OutputVolume, PointExcitation, PowerSurface, ProblemSpec, RCSSurface, SARVolume,
+                      SurfaceSheet, UnsupportedFeature, VolumeMaterial, Z0, nint)
 
 GEOMETRY_PACKETS = ["periodic_boundary", "mesh_outer_boundary_dimension", "mesh_dimensions_in_cells",
                     "mesh_cell_dimension", "volume_list", "surface_list", "line_list", "point_list", "pml",
@@ -51,15 +52,36 @@ SOLVER_PACKETS = ["simulation_time", "volume_material_list", "surface_material_l
                   "mode_stir_surface_list", "bicubic_warp_flag", "frequency_scale_flag", "compress_output_files",
                   "reduced_c_factor", "wrapping_boundary_conditions", "random_number_seed",
                   "ngspice_timestep_factor", "ngspice_lpf_alpha", "set_small_to_zero"]
-PACKETS = set(GEOMETRY_PACKETS + SOLVER_PACKETS)
-# packets that change nothing the time loop computes here
+# read_input_file_cables.F90: the cable model's packets, in the same file
+CABLE_PACKETS = ["cable_geometry_list", "cable_list", "cable_junction_list", "cable_output_list",
+                 "tlm_cell_equivalent_radius_factor", "capacitance_equivalent_radius_factor",
+                 "inductance_equivalent_radius_factor", "lc_correction_type_geometry_scale",
+                 "lc_correction_type_subtract_cell_inductance", "max_cable_bundle_diameter_factor"]
+PACKETS = set(GEOMETRY_PACKETS + SOLVER_PACKETS + CABLE_PACKETS)
+# packets that change nothing the time loop computes here: mesh and output
+# file options, lines (used by cables only), the random seed (used by the
+# random options, which are refused) and the cable model's factors
 NEUTRAL = {"new_mesh_generation", "no_geometry_vtk_files", "compress_output_files", "line_list",
-           "random_number_seed", "frequency_scale_flag"}
+           "random_number_seed", "tlm_cell_equivalent_radius_factor", "capacitance_equivalent_radius_factor",
+           "inductance_equivalent_radius_factor", "lc_correction_type_geometry_scale",
+           "lc_correction_type_subtract_cell_inductance", "max_cable_bundle_diameter_factor"}
 # packets of other parts of the reference the GPU path does not run
-UNSUPPORTED = {"periodic_boundary", "surface_material_list", "excitation_surface_list", "excitation_volume_list",
+UNSUPPORTED = {"periodic_boundary", "excitation_surface_list", "excitation_volume_list",
                "ngspice_node_output_list", "periodic_boundary_far_field_surface", "excitation_mode_list",
                "mode_stir_surface_list", "wrapping_boundary_conditions", "ngspice_timestep_factor",
-               "ngspice_lpf_alpha"}
+               "ngspice_lpf_alpha", "cable_geometry_list", "cable_list", "cable_junction_list", "cable_output_list"}
+# run by the GPU path but not read here: a mode output's profile comes from a
+# separate mode field file (ModeOutput takes the profile directly)
+NOT_READ = {"output_mode_list"}
+# packets read_inp turns into the spec
+HANDLED = {"mesh_outer_boundary_dimension", "mesh_cell_dimension", "mesh_dimensions_in_cells", "pml",
+           "volume_list", "surface_list", "point_list", "simulation_time", "volume_material_list",
+           "surface_material_list", "outer_boundary_reflection_coefficient", "excitation_function_list",
+           "excitation_point_list", "huygens_surface", "output_point_list", "output_surface_list",
+           "output_volume_list", "output_volume_average_list", "output_volume_peak_list",
+           "frequency_output_volume_list", "frequency_output_volume_list_xyz", "frequency_output_surface_list",
+           "far_field_surface_list", "rcs_surface", "frequency_domain_power_surface_list", "sar_volume_list",
+           "set_small_to_zero", "reduced_c_factor", "bicubic_warp_flag", "frequency_scale_flag"}
 
 # field component names (TLM_MODULES/TLM_Modules.F90:149-161): read_field_component
 # takes Ex..Hz, read_field_or_currrent_component also Jx..Jz, both comparing
@@ -122,18 +144,25 @@ class Records:
         return self.lines[self.pos][:width].rstrip().lower()
 
     def values(self, n: int) -> List[float]:
+        """``n`` values of a list-directed read: as many lines as needed, the
+        rest of the last line ignored (the remarks after the numbers), a
+        value written ``r*c`` repeated r times; any other text where a value
+        is still needed is a read error, as in the reference."""
         out: List[float] = []
         while len(out) < n:
-            for tok in re.split(r"[\s,]+", self.line().strip()):
+            line = self.line()
+            for tok in re.split(r"[\s,]+", line.strip()):
                 if not tok:
                     continue
+                rep = re.match(r"^(\d+)\*(.+)$", tok)
                 try:
-                    out.append(fortran_real(tok))
+                    vals = [fortran_real(rep.group(2))] * int(rep.group(1)) if rep else [fortran_real(tok)]
                 except ValueError:
-                    break  # a remark ends the values of this line
-                if len(out) == n:
+                    raise ValueError(f"{self.name} packet: expected a number, read {line.strip()!r}") from None
+                out.extend(vals)
+                if len(out) >= n:
                     break
-        return out
+        return out[:n]
 
     def ints(self, n: int) -> List[int]:
         return [int(v) for v in self.values(n)]
@@ -203,10 +232,17 @@ def _transform(r: Records, what: str) -> Tuple[float, float, float]:
 
 @dataclass
 class InpProblem:
+    """The spec, the packets read but without effect on the time loop
+    (``skipped``), each output point's output steps, and the parameters only
+    the host-side post-processing uses (``post``: "far_field" -> one dict of
+    angle ranges per far-field surface, "rcs" -> the frequency range,
+    "sar_density" -> one density per SAR volume)."""
+
     spec: ProblemSpec
     skipped: List[str] = field(default_factory=list)
     # per output point: (first, last, interval) timesteps, or None for every step
     output_timing: List[Optional[Tuple[int, int, int]]] = field(default_factory=list)
+    post: Dict[str, object] = field(default_factory=dict)
 
 
 
@@ -350,13 +386,12 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial]) ->
     for name, data in packets:
         if name in UNSUPPORTED:
             raise UnsupportedFeature(f"{name} packet: not supported by the GPU path")
+        if name in NOT_READ:
+            raise UnsupportedFeature(f"{name} packet: not read from .inp files; give the spec a ModeOutput")
+        if name in rec:
+            raise ValueError(f"{name} packet given twice")
         rec[name] = Records(name, data)
-    handled = {"mesh_outer_boundary_dimension", "mesh_cell_dimension", "mesh_dimensions_in_cells", "pml",
-               "volume_list", "surface_list", "point_list", "simulation_time", "volume_material_list",
-               "outer_boundary_reflection_coefficient", "excitation_function_list", "excitation_point_list",
-               "huygens_surface", "output_point_list", "output_surface_list", "output_volume_list",
-               "set_small_to_zero", "reduced_c_factor", "bicubic_warp_flag"}
-    skipped = [n for n, _ in packets if n not in handled]
+    skipped = [n for n, _ in packets if n in NEUTRAL]
     # the mesh, MESH/set_mesh_parameters.F90:40-100: a cell size wins over a cell count
     xmin, xmax, ymin, ymax, zmin, zmax = rec["mesh_outer_boundary_dimension"].values(6)
     ext = (xmax - xmin, ymax - ymin, zmax - zmin)
@@ -374,6 +409,11 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial]) ->
     reduced_c = rec["reduced_c_factor"].values(1)[0] if "reduced_c_factor" in rec else 1.0
     if "bicubic_warp_flag" in rec and _logical(rec["bicubic_warp_flag"].line().split()[0]):
         raise UnsupportedFeature("bicubic frequency warping of the material filters")
+    if "frequency_scale_flag" in rec:  # read_frequency_scale_flag.F90:53-54: a flag, then the scale
+        r = rec["frequency_scale_flag"]
+        r.line()
+        if r.values(1)[0] != 1.0:  # s_to_z_warp (FILTER/filter_functions.F90:343-385) divides dt by it
+            raise UnsupportedFeature("a frequency scale other than 1 for the material filters")
     dt = dl / (2.0 * C0 / reduced_c)  # TLM_SOLVER/set_TLM_solver_parameters.F90:93-95
     steps = nint(rec["simulation_time"].values(1)[0] / dt)
     R = tuple(rec["outer_boundary_reflection_coefficient"].values(6)) \
@@ -528,10 +568,169 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial]) ->
             comp = _component(r, _FIELD)
             spec.output_volumes.append(OutputVolume(volume_block(v, "an output volume"), comp, "field",
                                                     **_steps(_timing(r, dt))))
+    _read_outputs(rec, mesh, dt, spec, volumes, surfaces, volume_block, post := {})
+    if "surface_material_list" in rec:
+        _read_surface_materials(rec["surface_material_list"], mesh, spec, surfaces)
     if "set_small_to_zero" in rec:  # read_small_to_zero.F90:55-59
         r = rec["set_small_to_zero"]
         spec.small_to_zero = (r.ints(1)[0], r.values(1)[0])
-    return InpProblem(spec, skipped, timing)
+    return InpProblem(spec, skipped, timing, post)
+
+
+def _side(r: Records, allowed=(1, -1)) -> int:
+    side = r.ints(1)[0]
+    if side not in allowed:
+        raise ValueError(f"{r.name} packet: the side must be one of {allowed}")
+    return side
+
+
+def _surface_geo(mesh: Mesh, s: Shape, what: str, side: int) -> Tuple[dict, int]:
+    """The box= or plane= argument of a spec surface and the side in the
+    spec's convention (the packet's side times the plane's orientation)."""
+    kind, g, orient = _surface_cells(mesh, s, what)
+    return (dict(box=g) if kind == "box" else dict(plane=g)), side * orient
+
+
+def _numbered(r: Records, what: str):
+    n = r.ints(1)[0]
+    for k in range(1, n + 1):
+        if r.ints(1)[0] != k:
+            raise ValueError(f"{r.name} packet: {what} must be numbered in order")
+        yield k
+
+
+def _read_outputs(rec: Dict[str, Records], mesh: Mesh, dt: float, spec: ProblemSpec, volumes: Dict[int, Shape],
+                  surfaces: Dict[int, Shape], volume_block: Callable[[int, str], Block], post: dict) -> None:
+    """The volume and surface output packets other than Output_volume_list
+    and Output_surface_list, each entry becoming one spec entry (one
+    frequency per entry, as the reference stores them)."""
+    for name, kind in (("output_volume_average_list", "average"), ("output_volume_peak_list", "peak")):
+        if name in rec:  # read_output_volume_average_list.F90:78-100 / read_output_volume_peak_list.F90:78-100
+            r = rec[name]
+            for _ in _numbered(r, "volumes"):
+                v = r.ints(1)[0]
+                comp = _component(r, _FIELD)
+                spec.output_volumes.append(OutputVolume(volume_block(v, f"an output volume {kind}"), comp, kind,
+                                                        **_steps(_timing(r, dt))))
+    if "frequency_output_volume_list" in rec and "frequency_output_volume_list_xyz" in rec:
+        raise ValueError("frequency_output_volume_list and frequency_output_volume_list_xyz both given")
+    for name in ("frequency_output_volume_list", "frequency_output_volume_list_xyz"):
+        if name in rec:  # read_frequency_output_volume.F90:77-160
+            r = rec[name]
+            n = r.ints(1)[0]
+            every = 1
+            if name.endswith("_xyz") and r.peek_text(80)[:12] == "output_every":
+                every = int(fortran_real(r.line()[12:].split()[0]))
+            for k in range(1, n + 1):
+                if r.ints(1)[0] != k:
+                    raise ValueError(f"{name} packet: volumes must be numbered in order")
+                v = r.ints(1)[0]
+                freq = r.values(1)[0]
+                comp = _component(r, _FIELD)
+                spec.frequency_output_volumes.append(FrequencyOutputVolume(
+                    volume_block(v, "a frequency output volume"), [freq], comp, every=every,
+                    **_steps(_timing(r, dt))))
+    if "frequency_output_surface_list" in rec:  # read_frequency_output_surface.F90:63-125
+        r = rec["frequency_output_surface_list"]
+        for _ in _numbered(r, "surfaces"):
+            surf, side = r.ints(1)[0], _side(r)
+            freq = r.values(1)[0]
+            comp = _component(r, _FIELD_OR_CURRENT, width=2)
+            geo, eff = _surface_geo(mesh, surfaces[surf], "a frequency output surface", side)
+            t = _timing(r, dt)
+            if "plane" not in geo or eff != 1:
+                raise UnsupportedFeature("frequency output surface: only planar patches sampled on side 1 "
+                                         "of the rectangle orientation")
+            if t is not None and (t[0] > 1 or t[1] < spec.n_timesteps or t[2] != 1):
+                raise UnsupportedFeature("frequency output surface with output timing: every step only")
+            ax, ix, r0, r1 = geo["plane"]
+            spec.dft_surfaces.append(DFTSurface(ax, ix, r0, r1, [freq], comp))
+    if "far_field_surface_list" in rec:  # read_far_field_surface.F90:79-165
+        r = rec["far_field_surface_list"]
+        post["far_field"] = []
+        for _ in _numbered(r, "surfaces"):
+            surf, side = r.ints(1)[0], _side(r)
+            freq = r.values(1)[0]
+            theta, phi = tuple(r.values(3)), tuple(r.values(3))
+            dim = 3
+            if r.peek_text(2) == "2d":  # the optional 2D transform, about z only
+                r.line()
+                if r.text() != "z":
+                    raise ValueError("far_field_surface_list packet: a 2D transform about z only")
+                dim, theta = 2, (90.0, 90.0, 180.0 / 3.141592653589793)  # theta pi/2 with a 1 rad step
+            geo, eff = _surface_geo(mesh, surfaces[surf], "a far-field surface", side)
+            spec.far_field_surfaces.append(FarFieldSurface([freq], side=eff, **geo))
+            post["far_field"].append(dict(frequency=freq, theta=theta, phi=phi, dim=dim))
+    if "rcs_surface" in rec:  # read_rcs_surface.F90:63-85
+        r = rec["rcs_surface"]
+        surf, side = r.ints(1)[0], _side(r)
+        post["rcs"] = tuple(r.values(3))  # fmin, fmax, fstep
+        theta, phi = r.values(1)[0], r.values(1)[0]
+        geo, eff = _surface_geo(mesh, surfaces[surf], "an RCS surface", side)
+        spec.rcs_surface = RCSSurface(theta, phi, side=eff, **geo)
+    if "frequency_domain_power_surface_list" in rec:  # read_frequency_domain_power_surface.F90:63-105
+        r = rec["frequency_domain_power_surface_list"]
+        n_first = None
+        for _ in _numbered(r, "surfaces"):
+            surf, side = r.ints(1)[0], _side(r)
+            fmin, fmax, nf = r.values(3)
+            nf = int(nf)
+            if n_first is not None and nf != n_first:
+                raise ValueError("frequency_domain_power_surface_list packet: the surfaces must have the same "
+                                 "number of frequencies")
+            n_first = nf
+            fstep = (fmax - fmin) / float(nf - 1) if nf != 1 else 0.0
+            freqs = [fmin + (k - 1) * fstep for k in range(1, nf + 1)]  # frequency_domain_power_surfaces.F90:328
+            geo, eff = _surface_geo(mesh, surfaces[surf], "a power surface", side)
+            spec.power_surfaces.append(PowerSurface(freqs, side=eff, **geo))
+    if "sar_volume_list" in rec:  # read_SAR_volume_list.F90:69-90: material number, frequency, density
+        r = rec["sar_volume_list"]
+        post["sar_density"] = []
+        for _ in _numbered(r, "volumes"):
+            m = r.ints(1)[0]
+            freq, rho = r.values(1)[0], r.values(1)[0]
+            spec.sar_volumes.append(SARVolume(_material_block(spec, m), [freq]))
+            post["sar_density"].append(rho)
+
+
+def _material_block(spec: ProblemSpec, m: int) -> Block:
+    """The cells of volume material ``m`` (SAR_volumes.F90:62-95 takes every
+    cell whose material is m) when they form one block that no other
+    material overlaps."""
+    own = [b for k, b in spec.material_regions if k == m]
+    if len(own) != 1:
+        raise UnsupportedFeature("a SAR volume on a material of several volumes")
+    b = own[0]
+    for k, o in spec.material_regions:
+        if k != m and not (o.i1 < b.i0 or o.i0 > b.i1 or o.j1 < b.j0 or o.j0 > b.j1 or o.k1 < b.k0 or o.k0 > b.k1):
+            raise UnsupportedFeature("a SAR volume on a material that another material overlaps")
+    return b
+
+
+def _read_surface_materials(r: Records, mesh: Mesh, spec: ProblemSpec, surfaces: Dict[int, Shape]) -> None:
+    """read_surface_material_list.F90:111-470 for PEC, PMC and free-space
+    surfaces: number, type, the number of surfaces, their numbers and their
+    orientations (which a symmetric sheet does not use).  A box surface
+    becomes its six boundary planes."""
+    names = {"pec": "PEC", "pmc": "PMC", "free_space": "free"}
+    for _ in _numbered(r, "surface materials"):
+        kind = r.text()
+        if kind not in names:
+            raise UnsupportedFeature(f"surface material {kind!r}: only PEC, PMC and free-space surfaces")
+        n = r.ints(1)[0]
+        nums = r.ints(n)
+        r.ints(n)  # orientations
+        for num in nums:
+            geo, _ = _surface_geo(mesh, surfaces[num], "a surface material", 1)
+            if "plane" in geo:
+                ax, ix, r0, r1 = geo["plane"]
+                spec.surface_sheets.append(SurfaceSheet(names[kind], ax, ix, r0, r1))
+            else:
+                (i0, i1), (j0, j1), (k0, k1) = geo["box"]
+                for ax, ix, r0, r1 in ((1, i0 - 1, (j0, j1), (k0, k1)), (1, i1, (j0, j1), (k0, k1)),
+                                       (2, j0 - 1, (i0, i1), (k0, k1)), (2, j1, (i0, i1), (k0, k1)),
+                                       (3, k0 - 1, (i0, i1), (j0, j1)), (3, k1, (i0, i1), (j0, j1))):
+                    spec.surface_sheets.append(SurfaceSheet(names[kind], ax, ix, r0, r1))
 
 
 def vmat_in(directory: str) -> Callable[[str], VolumeMaterial]:

@@ -135,6 +135,12 @@ def small(extra="", base=BASE):
     return inp.read_inp((base + extra).splitlines(), materials)
 
 
+def test_every_keyword_has_one_treatment():
+    groups = [inp.HANDLED, inp.NEUTRAL, inp.UNSUPPORTED, inp.NOT_READ]
+    assert set().union(*groups) == inp.PACKETS
+    assert sum(len(g) for g in groups) == len(inp.PACKETS)
+
+
 def test_fortran_reals():
     assert inp.fortran_real("3.0-3") == 3.0e-3
     assert inp.fortran_real("1.5d+2") == 150.0
@@ -143,9 +149,11 @@ def test_fortran_reals():
     for bad in ("x", "1.0e", "--1", "1,0"):
         with pytest.raises(ValueError):
             inp.fortran_real(bad)
-    # list-directed: values spill over lines, a remark ends a line's values
-    r = inp.Records("t", ["1 2 ! remark 3", "4,5 6 7"])
-    assert r.values(4) == [1.0, 2.0, 4.0, 5.0]
+    # list-directed: values spill over lines, the rest of the last line is ignored, r*c repeats c
+    r = inp.Records("t", ["1 2", "4,5 6 ! remark", "2*0.5 remark"])
+    assert r.values(4) == [1.0, 2.0, 4.0, 5.0] and r.values(2) == [0.5, 0.5]
+    with pytest.raises(ValueError, match="expected a number"):
+        inp.Records("t", ["1 2 ! remark 3"]).values(3)
 
 
 def test_packet_keywords():
@@ -297,7 +305,11 @@ Ez
      "type 'sphere'"),                                                                      # not voxelised here
     ("Volume_list\n1\n1\nrectangular_block\n0.5 0.5 0.5\n0 0 0\n0.5 0.5 0.5\nVolume_material_list\n1\n1\nPEC\n1\n1\n",
      "centre lies on"),                                                                      # a face through centres
-    ("Surface_material_list\n0\n", "surface_material_list packet"),
+    ("Surface_list\n1\n1\nrectangle\n1.0 1.0\n0 0 0\n0.5 0.5 0.5\nSurface_material_list\n1\n1\nDISPERSIVE\n"
+     "MATERIAL_DIRECTORY/sheet\n1\n1\n1\n", "surface material 'dispersive'"),
+    ("Cable_list\n0\n", "cable_list packet"),
+    ("Output_mode_list\n0\n", "ModeOutput"),
+    ("Frequency_scale_flag\nT\n2.0\n", "frequency scale"),
     ("Bicubic_warp_flag\n.true.\n", "bicubic"),
     ("Excitation_function_list\n1\n1\nnoise\n1.0\n", "function 'noise'"),
     ("Output_point_list\n1\n2\n1\nEx\ncentre\n", "numbered in order"),                                  # numbering
@@ -337,7 +349,8 @@ PMC
 Bicubic_warp_flag
 F
 """)
-    assert p.skipped == ["new_mesh_generation", "no_geometry_vtk_files", "far_field_surface_list"]
+    assert p.skipped == ["new_mesh_generation", "no_geometry_vtk_files"]
+    assert p.spec.far_field_surfaces == [] and p.post["far_field"] == []
     assert p.spec.materials[0].type == 2 and p.spec.material_regions[0][1].i0 == 4
 
 
@@ -381,3 +394,170 @@ def test_gpu_huygens_input_matches_oracle(gpu_lib):
     assert np.linalg.norm(faces - want_faces) <= 1e-10 * np.linalg.norm(want_faces)
     for a, b in zip(surf, want_surf):
         assert a.shape == b.shape and np.linalg.norm(a - b) <= 1e-10 * np.linalg.norm(b)
+
+
+ALL_OUTPUTS = BASE.replace("0.55 0.55 0.55", "0.15 0.15 0.15") + """Volume_list
+1
+1
+rectangular_block
+0.4 0.4 0.4
+0 0 0
+0.5 0.5 0.5
+Surface_list
+3
+1
+rectangular_block
+0.6 0.6 0.6
+0 0 0
+0.5 0.5 0.5
+2
+zplane
+0.2 0.2 0.3   0.8 0.8 0.3
+0 0 0
+0 0 0
+3
+rectangle
+0.6 0.6
+0 0 0
+0.5 0.5 0.7
+Volume_material_list
+1
+1
+dispersive
+MATERIAL_DIRECTORY/debye_2
+1
+1
+Surface_material_list
+2
+1
+free_space
+1
+1
+1
+2
+PEC
+1
+2
+-1
+Excitation_point_list
+1
+1
+1
+1
+Ez
+centre
+soft
+Output_point_list
+1
+1
+1
+Ez
+centre
+Output_volume_average_list
+1
+1
+1
+Ex
+output_timestep_information
+2
+20
+3
+Output_volume_peak_list
+1
+1
+1
+Hz
+Frequency_output_volume_list_xyz
+1
+output_every 2
+1
+1
+1e8
+Ey
+Frequency_output_surface_list
+1
+1
+3
+1
+2e8
+Jx
+Far_field_surface_list
+1
+1
+1
+1
+3e8
+0 180 5
+0 90 10
+2D
+z
+RCS_surface
+1
+-1
+1e8 5e8 1e8
+90.0
+0.0
+Frequency_domain_power_surface_list
+1
+1
+2
+1
+1e8 3e8 3
+SAR_volume_list
+1
+1
+1
+1e8
+1000.0
+"""
+
+
+def test_all_output_packets():
+    p = small(base=ALL_OUTPUTS)
+    s = p.spec
+    blk = (4, 7, 4, 7, 4, 7)
+    cells = lambda b: (b.i0, b.i1, b.j0, b.j1, b.k0, b.k1)  # noqa: E731
+    assert [(v.kind, v.component, v.first_step, v.last_step, v.interval, cells(v.region)) for v in s.output_volumes] \
+        == [("average", "Ex", 2, 20, 3, blk), ("peak", "Hz", 1, None, 1, blk)]
+    fv = s.frequency_output_volumes[0]
+    assert (list(fv.frequencies), fv.component, fv.every, cells(fv.region)) == ([1e8], "Ey", 2, blk)
+    ds = s.dft_surfaces[0]
+    assert (ds.axis, ds.index, ds.r0, ds.r1, list(ds.frequencies), ds.component) == (3, 7, (3, 8), (3, 8), [2e8], "Jx")
+    ff = s.far_field_surfaces[0]
+    assert (ff.frequencies, ff.box, ff.side) == ([3e8], ((3, 8), (3, 8), (3, 8)), 1)
+    assert p.post["far_field"][0]["dim"] == 2 and p.post["far_field"][0]["phi"] == (0.0, 90.0, 10.0)
+    rc = s.rcs_surface
+    assert (rc.theta, rc.phi, rc.box, rc.side, p.post["rcs"]) == (90.0, 0.0, ((3, 8), (3, 8), (3, 8)), -1,
+                                                                  (1e8, 5e8, 1e8))
+    ps = s.power_surfaces[0]
+    # ascending zplane corners: normal +z, so side 1 of the packet is side -1 of the spec
+    assert (ps.frequencies, ps.plane, ps.side) == ([1e8, 2e8, 3e8], (3, 3, (3, 8), (3, 8)), -1)
+    assert (list(s.sar_volumes[0].frequencies), cells(s.sar_volumes[0].region), p.post["sar_density"]) == \
+        ([1e8], blk, [1000.0])
+    kinds = [(sh.kind, sh.axis, sh.index) for sh in s.surface_sheets]
+    assert kinds == [("free", 1, 2), ("free", 1, 8), ("free", 2, 2), ("free", 2, 8), ("free", 3, 2), ("free", 3, 8),
+                     ("PEC", 3, 3)]
+    t = build_tables(s)
+    assert (t["n_ovol"], t["n_vdft"], t["n_dft"], t["n_sar"], t["n_ff"], t["n_ps"]) == (2, 1, 1, 1, 1, 3)
+    assert int(np.count_nonzero(t["face_mat"])) == 6 * 36 + 36  # free-space box faces and the PEC sheet
+
+
+@pytest.mark.gpu
+def test_gpu_all_output_packets_match_oracle(gpu_lib):
+    t = build_tables(small(base=ALL_OUTPUTS).spec)
+    o = oracle.Oracle(t)
+    want = o.run(t["n_timesteps"])
+    with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64) as g:
+        g.run(t["n_timesteps"])
+        got, got_dft, got_ps, got_ov = g.cell_output(), g.dft(), g.power_surfaces(), g.output_volumes()
+
+    def rel(a, b):
+        return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+    assert rel(got, want) < 1e-10
+    assert rel(got_dft, o.dft()) < 1e-10
+    want_ps, ptr = oracle.power_surfaces(t), t["ps_face_ptr"]
+    for k in range(t["n_ps"]):
+        assert rel(got_ps[ptr[k]:ptr[k + 1]], want_ps[ptr[k]:ptr[k + 1]]) < 1e-10, k
+    for a, b in zip(got_ov, oracle.output_volumes(t, want)):
+        assert a.shape == b.shape and rel(a, b) < 1e-10
