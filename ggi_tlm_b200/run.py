@@ -1,0 +1,123 @@
+"""Run a GGI_TLM problem file on the GPU and write its time-domain results.
+
+    python -m ggi_tlm_b200.run <problem_name> [--fp32] [--device N] [--chunk STEPS]
+
+As the reference's GGI_TLM program does (SRC/GGI_TLM.F90), this reads
+``<problem_name>.inp`` from the working directory (material files resolve
+against it too), runs the time loop, and writes, in the reference's format
+and file names (TLM_MODULES/File_information.F90:143-158):
+
+- ``<problem_name>.field.tout``: the output points, each on its own output
+  steps (output_points.F90);
+- ``<problem_name>.volume_average_field.tout`` and
+  ``.volume_peak_field.tout``: one value per output volume average or peak
+  and output step (output_volume_averages.F90:330-350,
+  output_volume_peak.F90:320-340), numbered within their own packet.
+
+The run goes through the library's C ABI in chunks of ``--chunk`` steps,
+reading the output points back after each chunk.  The other outputs
+(surfaces, volumes, DFTs, far field, SAR, power) are returned by the
+GpuMesh accessors.  Without the CUDA library or a GPU it stops with the
+library's message and exit code 1.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import capi
+from .inp import InpProblem, read_inp_file
+from .problem import build_tables, probe_series
+from .tout import data_line, field_rows, header, output_flag
+
+
+def _volume_rows(t: dict, spec, values: List[np.ndarray], kind: str):
+    """(time, number, value) rows of the output volumes of one kind, at the
+    cell-output time (timestep-1)*dt of each step get_output_flag accepts."""
+    dt = float(t["dt"])
+    n = int(t["n_timesteps"])
+    vols = [(k, v) for k, v in enumerate(spec.output_volumes) if v.kind == kind]
+    row_of = []  # per volume: output step -> row of its result array
+    for _, v in vols:
+        last = n if v.last_step is None else v.last_step
+        st = [ts for ts in range(1, n + 1) if output_flag(ts, (v.first_step, last, v.interval))]
+        row_of.append({ts: i for i, ts in enumerate(st)})
+    rows = []
+    for ts in range(1, n + 1):
+        for num, ((k, _), rmap) in enumerate(zip(vols, row_of), start=1):
+            if ts in rmap:
+                rows.append(((ts - 1) * dt, num, float(values[k][rmap[ts]])))
+    return rows, len(vols)
+
+
+def write_results(name: str, p: InpProblem, t: dict, cell_out: np.ndarray, face_out: np.ndarray,
+                  volumes: Optional[List[np.ndarray]] = None, directory: str = ".") -> List[str]:
+    """Write the .tout files of a finished run; returns the paths written.
+    ``cell_out`` is [steps, n_kept, 6], ``face_out`` [n_face_points, steps]."""
+    written = []
+    n = int(t["n_timesteps"])
+    if p.spec.outputs:
+        centre = probe_series(t, cell_out) if int(t["n_out_cells"]) else np.zeros((0, n))
+        rows = field_rows(t, centre, face_out, timing=p.output_timing)
+        path = os.path.join(directory, name + ".field.tout")
+        _write(path, header(len(p.spec.outputs), n), rows)
+        written.append(path)
+    for kind, extn in (("average", ".volume_average_field.tout"), ("peak", ".volume_peak_field.tout")):
+        if any(v.kind == kind for v in p.spec.output_volumes):
+            rows, count = _volume_rows(t, p.spec, volumes, kind)
+            path = os.path.join(directory, name + extn)
+            _write(path, header(count, n), rows)
+            written.append(path)
+    return written
+
+
+def _write(path: str, head: Sequence[str], rows) -> None:
+    with open(path, "w") as f:
+        for line in head:
+            f.write(line + "\n")
+        for time, num, value in rows:
+            f.write(data_line(time, num, value) + "\n")
+
+
+def run(name: str, precision: int = capi.TLM_PRECISION_FP64, device: int = 0, chunk: int = 1000,
+        directory: str = ".") -> List[str]:
+    """Read ``<directory>/<name>.inp``, run it and write its .tout files."""
+    p = read_inp_file(os.path.join(directory, name + ".inp"))
+    t = build_tables(p.spec)
+    n = int(t["n_timesteps"])
+    with capi.GpuMesh(t, precision=precision, device=device) as g:
+        cells, faces = [], []
+        for first in range(1, n + 1, chunk):
+            k = min(chunk, n - first + 1)
+            g.run(k)
+            cells.append(g.cell_output(first, k))
+            faces.append(g.face_output(first, k))
+        cell_out = np.concatenate(cells) if cells else np.zeros((0, 0, 6))
+        face_out = np.concatenate(faces, axis=1) if faces else np.zeros((0, 0))
+        volumes = g.output_volumes() if p.spec.output_volumes else None
+    return write_results(name, p, t, cell_out, face_out, volumes, directory)
+
+
+def main(argv: Optional[Sequence[str]] = None) -> int:
+    ap = argparse.ArgumentParser(prog="python -m ggi_tlm_b200.run", description=__doc__.split("\n")[0])
+    ap.add_argument("problem_name")
+    ap.add_argument("--fp32", action="store_true", help="FP32 link state (default FP64)")
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--chunk", type=int, default=1000, help="steps per run call between read-backs")
+    a = ap.parse_args(argv)
+    try:
+        for path in run(a.problem_name, capi.TLM_PRECISION_FP32 if a.fp32 else capi.TLM_PRECISION_FP64, a.device,
+                        a.chunk):
+            print("wrote", path)
+    except (RuntimeError, OSError) as e:  # TLMError is a RuntimeError, as is a library not built
+        print(f"ERROR in run_TLM_gpu: {e}", file=sys.stderr)
+        return 1
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

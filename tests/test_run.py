@@ -1,0 +1,123 @@
+"""The problem-file runner (python -m ggi_tlm_b200.run): .inp in, .tout out.
+
+CPU: the files it writes, from the oracle's results of the reference's
+HUYGENS_SURFACE input, carry the reference's header and the golden centre
+series; volume average and peak files follow their output steps and
+numbering; without a GPU the runner stops with the library's message and
+exit code 1.  GPU: the runner's own files against the oracle's."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from ggi_tlm_b200 import run as runner
+from ggi_tlm_b200.inp import read_inp
+from ggi_tlm_b200.problem import build_tables
+from ggi_tlm_b200.tout import read_tout
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+import oracle  # noqa: E402
+import test_inp  # noqa: E402
+
+TOL = 5e-7  # E16.7
+
+
+def problem_dir(tmp, name, text):
+    """A run directory holding <name>.inp and the material files it names."""
+    with open(os.path.join(tmp, name + ".inp"), "w", encoding="latin-1") as f:
+        f.write("\n".join(text) + "\n")
+    os.makedirs(os.path.join(tmp, "MATERIAL_DIRECTORY"), exist_ok=True)
+    d = np.load(os.path.join(HERE, "golden", "vmat_text.npz"))
+    for k in d.files:
+        with open(os.path.join(tmp, "MATERIAL_DIRECTORY", k + ".vmat"), "w") as f:
+            f.write("\n".join(str(x) for x in d[k]) + "\n")
+    return tmp
+
+
+def oracle_files(tmp, name, lines):
+    p = read_inp(lines, test_inp.materials)
+    t = build_tables(p.spec)
+    o = oracle.Oracle(t)
+    cell = o.run(t["n_timesteps"])
+    face = o.face_probes() if int(t["n_face_probes"]) else np.zeros((0, t["n_timesteps"]))
+    vols = oracle.output_volumes(t, cell) if p.spec.output_volumes else None
+    return runner.write_results(name, p, t, cell, face, vols, tmp), p, t
+
+
+def test_field_tout_from_the_huygens_input(tmp_path):
+    lines = test_inp.inputs()["huygens_box"]
+    (path,), p, t = oracle_files(str(tmp_path), "huygens_test", lines)
+    assert os.path.basename(path) == "huygens_test.field.tout"
+    with open(path) as f:
+        head = [next(f).rstrip("\n") for _ in range(3)]
+    assert head == ["# Time Domain Data", "# Number of data points:         30",
+                    "# Number of Timesteps  :        120"]
+    d = read_tout(path)
+    assert d.shape == (30 * 120, 3)
+    # each step: the 6 centre points at (ts-1)*dt, then the 24 face points half a step later
+    assert list(d[:6, 1]) == [1, 6, 11, 16, 21, 26] and d[6, 1] == 2 and d[6, 0] > d[0, 0]
+    for k, comp in zip((1, 6, 11, 16, 21, 26), ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")):
+        got = d[d[:, 1] == k, 2]
+        g = np.load(os.path.join(HERE, "golden", f"huygens_box_{comp}.npz"))
+        assert np.linalg.norm(got - g["value"]) / np.linalg.norm(g["value"]) < TOL, comp
+
+
+def test_volume_average_and_peak_files(tmp_path):
+    lines = test_inp.ALL_OUTPUTS.splitlines()
+    paths, p, t = oracle_files(str(tmp_path), "all", lines)
+    names = sorted(os.path.basename(x) for x in paths)
+    assert names == ["all.field.tout", "all.volume_average_field.tout", "all.volume_peak_field.tout"]
+    avg = read_tout(os.path.join(str(tmp_path), "all.volume_average_field.tout"))
+    peak = read_tout(os.path.join(str(tmp_path), "all.volume_peak_field.tout"))
+    dt = float(t["dt"])
+    # the average runs on steps 2, 5, ..., 20 (output_timestep_information 2 20 3), the peak every step
+    assert np.allclose(avg[:, 0] / dt + 1, np.arange(2, 21, 3)) and set(avg[:, 1]) == {1.0}
+    assert len(peak) == int(t["n_timesteps"]) and set(peak[:, 1]) == {1.0}
+    want = oracle.output_volumes(t, oracle.Oracle(t).run(t["n_timesteps"]))
+    np.testing.assert_allclose(avg[:, 2], want[0], rtol=TOL, atol=1e-30)
+    np.testing.assert_allclose(peak[:, 2], want[1], rtol=TOL, atol=1e-30)
+
+
+def test_runner_stops_cleanly_without_a_gpu(tmp_path):
+    import torch
+
+    from ggi_tlm_b200 import build
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present: the GPU test runs the problem")
+    build.build()
+    d = problem_dir(str(tmp_path), "huygens_test", test_inp.inputs()["huygens_box"])
+    env = dict(os.environ, PYTHONPATH=REPO + os.pathsep + os.environ.get("PYTHONPATH", ""))
+    res = subprocess.run([sys.executable, "-m", "ggi_tlm_b200.run", "huygens_test"], cwd=d, env=env,
+                         capture_output=True, text=True, timeout=600)
+    assert res.returncode == 1
+    assert "ERROR in run_TLM_gpu:" in res.stderr
+    assert not os.path.exists(os.path.join(d, "huygens_test.field.tout"))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name, text", [("huygens_test", None), ("all", "all")])
+def test_gpu_runner_files_match_oracle_files(gpu_lib, tmp_path, name, text):
+    lines = test_inp.inputs()["huygens_box"] if text is None else test_inp.ALL_OUTPUTS.splitlines()
+    run_dir, ref_dir = str(tmp_path / "run"), str(tmp_path / "oracle")
+    os.makedirs(run_dir)
+    os.makedirs(ref_dir)
+    problem_dir(run_dir, name, lines)
+    got = runner.run(name, chunk=37, directory=run_dir)
+    want, _, _ = oracle_files(ref_dir, name, lines)
+    assert sorted(os.path.basename(x) for x in got) == sorted(os.path.basename(x) for x in want)
+    for a in want:
+        b = os.path.join(run_dir, os.path.basename(a))
+        with open(a) as fa, open(b) as fb:
+            la, lb = fa.read().splitlines(), fb.read().splitlines()
+        assert la[:3] == lb[:3] and len(la) == len(lb)
+        da, db = read_tout(a), read_tout(b)
+        assert np.array_equal(da[:, 1], db[:, 1])
+        np.testing.assert_allclose(db[:, 0], da[:, 0], rtol=1e-7)
+        # printed to 7 digits: one unit in the last digit is up to 1e-6 relative; round-off-level values
+        # (components zero by symmetry) are held to an absolute floor below the file's largest value
+        np.testing.assert_allclose(db[:, 2], da[:, 2], rtol=1.01e-6, atol=1e-9 * np.abs(da[:, 2]).max())
