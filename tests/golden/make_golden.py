@@ -27,7 +27,7 @@ CASES = {
 # raw text of the reference's .tout files (header and every data line), kept
 # to check that the library's .tout writer reproduces them byte for byte
 TEXT_CASES = ["tem_pml_Ey", "material_test2_Ex", "huygens_box_Hz"]
-VMAT_CASES = ["debye_1", "debye_2", "FR4_at_7GHz", "mur_lorentz"]
+VMAT_CASES = ["debye_1", "debye_2", "FR4_at_7GHz", "mur_lorentz", "epsr=2", "mur=2"]
 # the known-answer cases' problem input files, as text, for the .inp reader;
 # read as Latin-1 since their remarks hold stray non-ASCII bytes
 INP_CASES = {
@@ -36,6 +36,19 @@ INP_CASES = {
     "material_stability": "MATERIAL_STABILITY_TEST/PROBLEM_SPECIFICATION_FILES/cavity.inp",
     "material_test2": "MATERIAL_TEST2/PROBLEM_SPECIFICATION_FILES/mat_test.inp",
     "huygens_box": "HUYGENS_SURFACE/PROBLEM_SPECIFICATION_FILES/huygens_test.inp",
+    "cavity_free_space": "CAVITY_FREE_SPACE/PROBLEM_SPECIFICATION_FILES/cavity_1_2_3.inp",
+    "cavity_epsr2": "CAVITY_EPSR=2/PROBLEM_SPECIFICATION_FILES/cavity_1_2_3.inp",
+    "cavity_mur2": "CAVITY_MUR=2/PROBLEM_SPECIFICATION_FILES/cavity_1_2_3.inp",
+    "parallel_test": "PARALLEL_TEST/PROBLEM_SPECIFICATION_FILES/cavity.inp",
+}
+# the post-processor's Fourier transforms of those four cases' output point
+# (GGI_TLM_post_process_in.txt beside each: option 3, point 1, lin 1 MHz to
+# 300 MHz, 1000 frequencies; 100 for PARALLEL_TEST), as text
+FOUT_CASES = {
+    "cavity_free_space": "CAVITY_FREE_SPACE/PROBLEM_SPECIFICATION_FILES/cavity_1_2_3.fout_ref",
+    "cavity_epsr2": "CAVITY_EPSR=2/PROBLEM_SPECIFICATION_FILES/cavity_1_2_3.fout_ref",
+    "cavity_mur2": "CAVITY_MUR=2/PROBLEM_SPECIFICATION_FILES/cavity_1_2_3.fout_ref",
+    "parallel_test": "PARALLEL_TEST/PROBLEM_SPECIFICATION_FILES/cavity.fout_ref",
 }
 
 
@@ -67,6 +80,12 @@ def main():
             inp[name] = np.array(f.read().splitlines())
     np.savez_compressed(os.path.join(here, "inp_text.npz"), **inp)
     print("inp_text", {k: len(v) for k, v in inp.items()})
+    fo = {}
+    for name, rel in FOUT_CASES.items():
+        with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", rel)) as f:
+            fo[name] = np.array(f.read().splitlines())
+    np.savez_compressed(os.path.join(here, "fout_text.npz"), **fo)
+    print("fout_text", {k: len(v) for k, v in fo.items()})
 
 
 if __name__ == "__main__":
