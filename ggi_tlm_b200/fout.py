@@ -81,6 +81,18 @@ def read_fout(path_or_lines) -> np.ndarray:
     return np.loadtxt([x for x in path_or_lines if not x.startswith("#")], ndmin=2)
 
 
+def spectrum(rows: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    """(frequencies, complex values) of .fout rows [n, 7] (read_fout), as
+    read_frequency_domain_data takes them: from the printed Re and Im columns."""
+    return rows[:, 0], rows[:, 2] + 1j * rows[:, 3]
+
+
+def combine(f1: np.ndarray, f2: np.ndarray, a: float = 1.0, b: float = 1.0, c: float = 0.0) -> np.ndarray:
+    """Post-processor option 6 (POST_PROCESSOR/combine_frequency_domain_data.F90):
+    (A f1) / (B f2) + C at each frequency; the two grids must be equal."""
+    return (a * np.asarray(f1)) / (b * np.asarray(f2)) + c
+
+
 def tout_series(rows: np.ndarray, point: int) -> Tuple[np.ndarray, np.ndarray]:
     """(time, value) of one output point from .tout rows [n, 3] (read_tout)."""
     sel = rows[:, 1] == point

@@ -7,6 +7,8 @@ As the reference's GGI_TLM program does (SRC/GGI_TLM.F90), this reads
 against it too), runs the time loop, and writes, in the reference's format
 and file names (TLM_MODULES/File_information.F90:143-158):
 
+- ``<problem_name>.excitation.tout``: every excitation function at every
+  timestep (excitation.F90:186-553);
 - ``<problem_name>.field.tout``: the output points, each on its own output
   steps (output_points.F90);
 - ``<problem_name>.volume_average_field.tout`` and
@@ -32,7 +34,7 @@ import numpy as np
 from . import capi
 from .inp import InpProblem, read_inp_file
 from .problem import build_tables, probe_series
-from .tout import data_line, field_rows, header, output_flag
+from .tout import data_line, excitation_rows, field_rows, header, output_flag
 
 
 def _volume_rows(t: dict, spec, values: List[np.ndarray], kind: str):
@@ -60,6 +62,10 @@ def write_results(name: str, p: InpProblem, t: dict, cell_out: np.ndarray, face_
     ``cell_out`` is [steps, n_kept, 6], ``face_out`` [n_face_points, steps]."""
     written = []
     n = int(t["n_timesteps"])
+    if int(t["n_functions"]):
+        path = os.path.join(directory, name + ".excitation.tout")
+        _write(path, header(int(t["n_functions"]), n), excitation_rows(t), flush_small=False)
+        written.append(path)
     if p.spec.outputs:
         centre = probe_series(t, cell_out) if int(t["n_out_cells"]) else np.zeros((0, n))
         rows = field_rows(t, centre, face_out, timing=p.output_timing)
@@ -75,12 +81,12 @@ def write_results(name: str, p: InpProblem, t: dict, cell_out: np.ndarray, face_
     return written
 
 
-def _write(path: str, head: Sequence[str], rows) -> None:
+def _write(path: str, head: Sequence[str], rows, flush_small: bool = True) -> None:
     with open(path, "w") as f:
         for line in head:
             f.write(line + "\n")
         for time, num, value in rows:
-            f.write(data_line(time, num, value) + "\n")
+            f.write(data_line(time, num, value, flush_small) + "\n")
 
 
 def run(name: str, precision: int = capi.TLM_PRECISION_FP64, device: int = 0, chunk: int = 1000,

@@ -40,9 +40,10 @@ def header(n_points: int, n_timesteps: int) -> List[str]:
     return [HEADER, "# Number of data points: " + f"{n_points:10d}", "# Number of Timesteps  : " + f"{n_timesteps:10d}"]
 
 
-def data_line(time: float, point: int, value: float) -> str:
-    """One ``(E16.7,I5,E16.7)`` line; |value| < 1e-30 is written as 0."""
-    v = 0.0 if abs(value) < 1e-30 else float(value)
+def data_line(time: float, point: int, value: float, flush_small: bool = True) -> str:
+    """One ``(E16.7,I5,E16.7)`` line; with ``flush_small`` (the output files)
+    |value| < 1e-30 is written as 0, without it (the excitation file) as is."""
+    v = 0.0 if flush_small and abs(value) < 1e-30 else float(value)
     return fortran_e(time) + f"{int(point):5d}" + fortran_e(v)
 
 
@@ -96,6 +97,16 @@ def field_rows(tables: dict, centre: np.ndarray, face: np.ndarray, first_step: i
             if on(int(fno[k]), timestep):
                 rows.append((time, int(fno[k]), float(face[k, s])))
     return rows
+
+
+def excitation_rows(tables: dict) -> List[Tuple[float, int, float]]:
+    """Rows of the .excitation.tout file initialise_excitation_functions writes
+    (EXCITATION/excitation.F90:186-553): for each function in turn, its value
+    at every timestep at time (timestep-1)*dt, without the small-value flush."""
+    dt = float(tables["dt"])
+    val = np.asarray(tables["fn_value"]).reshape(int(tables["n_functions"]), -1)
+    return [((ts - 1) * dt, e + 1, float(val[e, ts - 1])) for e in range(val.shape[0])
+            for ts in range(1, val.shape[1] + 1)]
 
 
 def read_tout(path: str) -> np.ndarray:

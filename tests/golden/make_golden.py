@@ -40,6 +40,7 @@ INP_CASES = {
     "cavity_epsr2": "CAVITY_EPSR=2/PROBLEM_SPECIFICATION_FILES/cavity_1_2_3.inp",
     "cavity_mur2": "CAVITY_MUR=2/PROBLEM_SPECIFICATION_FILES/cavity_1_2_3.inp",
     "parallel_test": "PARALLEL_TEST/PROBLEM_SPECIFICATION_FILES/cavity.inp",
+    "box_slot": "SHIELDING_EFFECTIVENESS_BOX_SLOT/PROBLEM_SPECIFICATION_FILES/box_slot.inp",
 }
 # the post-processor's Fourier transforms of those four cases' output point
 # (GGI_TLM_post_process_in.txt beside each: option 3, point 1, lin 1 MHz to
@@ -49,6 +50,8 @@ FOUT_CASES = {
     "cavity_epsr2": "CAVITY_EPSR=2/PROBLEM_SPECIFICATION_FILES/cavity_1_2_3.fout_ref",
     "cavity_mur2": "CAVITY_MUR=2/PROBLEM_SPECIFICATION_FILES/cavity_1_2_3.fout_ref",
     "parallel_test": "PARALLEL_TEST/PROBLEM_SPECIFICATION_FILES/cavity.fout_ref",
+    # option 3 on the excitation and on the probe, then option 6: excitation / probe
+    "box_slot": "SHIELDING_EFFECTIVENESS_BOX_SLOT/PROBLEM_SPECIFICATION_FILES/Shielding_effectiveness.fout_ref",
 }
 
 

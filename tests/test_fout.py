@@ -129,3 +129,40 @@ def test_command_line_transform(tmp_path):
     assert lines == fout.format_fout(freqs, v)
     check("parallel_test", freqs, v)
     assert fout.main([src, "7", "lin", "1e6", "3e8", "100", out]) == 1  # no such point
+
+
+def shielding_effectiveness(p, t, cell_out, face_out):
+    """SHIELDING_EFFECTIVENESS_BOX_SLOT's recipe: option 3 on box_slot.excitation.tout
+    and on box_slot.field.tout (point 1, lin 1 MHz to 300 MHz, 1000
+    frequencies), each written as .fout and read back, then option 6 with
+    A = B = 1, C = 0: excitation / Ey."""
+    freqs = fout.frequencies(1e6, 3e8, 1000)
+    spectra = []
+    files = [(tout.excitation_rows(t), False),  # the excitation file is written without the 1e-30 flush
+             (tout.field_rows(t, probe_series(t, cell_out), face_out, timing=p.output_timing), True)]
+    for rows, flush in files:
+        printed = [tout.data_line(*r, flush_small=flush) for r in rows]
+        series = np.array([[float(x[:16]), int(x[16:21]), float(x[21:])] for x in printed])
+        v = fout.fourier_transform(*fout.tout_series(series, 1), freqs)
+        spectra.append(fout.spectrum(fout.read_fout(fout.format_fout(freqs, v)))[1])
+    return freqs, fout.combine(spectra[0], spectra[1], 1.0, 1.0, 0.0)
+
+
+def test_oracle_shielding_effectiveness_matches_reference_golden():
+    """A PEC box with a free-space slot in its top face (the slot's surface
+    material overrides the box's), lit by a plane wave from the outer
+    Huygens surface, 29979 steps."""
+    p, t = problem("box_slot")
+    assert [sh.kind for sh in p.spec.surface_sheets] == ["PEC"] * 6 + ["free"]
+    o = oracle.Oracle(t)
+    cell = o.run(t["n_timesteps"])
+    check("box_slot", *shielding_effectiveness(p, t, cell, np.zeros((0, t["n_timesteps"]))))
+
+
+@pytest.mark.gpu
+def test_gpu_shielding_effectiveness_matches_reference_golden(gpu_lib):
+    p, t = problem("box_slot")
+    with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64) as g:
+        g.run(t["n_timesteps"])
+        cell = g.cell_output()
+    check("box_slot", *shielding_effectiveness(p, t, cell, np.zeros((0, t["n_timesteps"]))))

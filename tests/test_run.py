@@ -50,8 +50,12 @@ def oracle_files(tmp, name, lines):
 
 def test_field_tout_from_the_huygens_input(tmp_path):
     lines = test_inp.inputs()["huygens_box"]
-    (path,), p, t = oracle_files(str(tmp_path), "huygens_test", lines)
-    assert os.path.basename(path) == "huygens_test.field.tout"
+    (exc, path), p, t = oracle_files(str(tmp_path), "huygens_test", lines)
+    assert [os.path.basename(exc), os.path.basename(path)] == ["huygens_test.excitation.tout", "huygens_test.field.tout"]
+    e = read_tout(exc)  # the Gaussian at every step, (ts-1)*dt, not flushed below 1e-30
+    assert e.shape == (120, 3) and set(e[:, 1]) == {1.0}
+    np.testing.assert_allclose(e[:, 2], np.asarray(t["fn_value"]).reshape(-1), rtol=5.01e-7, atol=0)
+    np.testing.assert_allclose(e[:, 0], np.arange(120) * t["dt"], rtol=5.01e-7)
     with open(path) as f:
         head = [next(f).rstrip("\n") for _ in range(3)]
     assert head == ["# Time Domain Data", "# Number of data points:         30",
@@ -70,7 +74,8 @@ def test_volume_average_and_peak_files(tmp_path):
     lines = test_inp.ALL_OUTPUTS.splitlines()
     paths, p, t = oracle_files(str(tmp_path), "all", lines)
     names = sorted(os.path.basename(x) for x in paths)
-    assert names == ["all.field.tout", "all.volume_average_field.tout", "all.volume_peak_field.tout"]
+    assert names == ["all.excitation.tout", "all.field.tout", "all.volume_average_field.tout",
+                     "all.volume_peak_field.tout"]
     avg = read_tout(os.path.join(str(tmp_path), "all.volume_average_field.tout"))
     peak = read_tout(os.path.join(str(tmp_path), "all.volume_peak_field.tout"))
     dt = float(t["dt"])
