@@ -103,6 +103,8 @@ _WITH_FILE = {"tet_volume_mesh", "triangulated_surface", "vtk_triangulated_surfa
 # parameters per excitation function type, read_excitation_function_list.F90:108-160
 _N_PARAMS = {"impulse": 1, "gaussian_step": 3, "step": 2, "gaussian": 3, "sinusoid": 3, "gaussian_sinusoid": 5,
              "differential_gaussian": 3}
+# the reference's other function types, which the GPU path's tables do not restate
+_OTHER_FUNCTIONS = {"gaussian_step_sinusoid", "double_exponential", "noise", "sinusoidal_pulse", "ring_wave"}
 
 _REAL = re.compile(r"^([+-]?(?:\d+\.?\d*|\.\d+))(?:[eEdD]([+-]?\d+)|([+-]\d+))?$")
 
@@ -377,10 +379,34 @@ def _logical(tok: str) -> bool:
     return t[0] == "t"
 
 
-def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial]) -> InpProblem:
+def _samples(lines: Sequence[str], n_ignore: int, n_time: int, n_value: int) -> Tuple[List[float], List[float]]:
+    """read_excitation_function_list.F90:182-215: skip n_ignore lines, then
+    list-directed records of max(n_time, n_value) values to the end of the
+    file, keeping the n_time-th as the time and the n_value-th as the value."""
+    r = Records("excitation function file", list(lines)[n_ignore:])
+    n = max(n_time, n_value)
+    times: List[float] = []
+    values: List[float] = []
+    while any(x.strip() for x in r.lines[r.pos:]):
+        try:
+            rec = r.values(n)
+        except ValueError as e:
+            if "ends too early" in str(e):
+                break  # the end of the file inside a record ends the samples
+            raise
+        times.append(rec[n_time - 1])
+        values.append(rec[n_value - 1])
+    if not times:
+        raise ValueError("an excitation function file without samples")
+    return times, values
+
+
+def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
+             open_file: Optional[Callable[[str], Sequence[str]]] = None) -> InpProblem:
     """The ProblemSpec of a .inp file's lines; ``material(name)`` returns the
     volume material of a dispersive Volume_material_list entry, ``name``
-    being the file name line as written (the reference opens name + '.vmat')."""
+    being the file name line as written (the reference opens name + '.vmat');
+    ``open_file(name)`` returns the lines of an excitation function's data file."""
     packets = split_packets(lines)
     rec: Dict[str, Records] = {}
     for name, data in packets:
@@ -479,16 +505,25 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial]) ->
             nv = r.ints(1)[0]
             for v in r.ints(nv):
                 spec.material_regions.append((k, volume_block(v, "a volume material")))
-    # excitation functions, read_excitation_function_list.F90:92-250
+    # excitation functions, read_excitation_function_list.F90:92-250; a
+    # name that is no function type is a data file of samples
     if "excitation_function_list" in rec:
         r = rec["excitation_function_list"]
         for k in range(1, r.ints(1)[0] + 1):
             if r.ints(1)[0] != k:
                 raise ValueError("Excitation_function_list packet: functions must be numbered in order")
-            kind = r.text()
-            if kind not in _N_PARAMS:
+            raw = r.line()
+            kind = raw.rstrip().lower()
+            if kind in _N_PARAMS:
+                spec.functions.append(ExcitationFunction(kind, tuple(r.values(_N_PARAMS[kind]))))
+            elif kind in _OTHER_FUNCTIONS:
                 raise UnsupportedFeature(f"excitation function {kind!r}")
-            spec.functions.append(ExcitationFunction(kind, tuple(r.values(_N_PARAMS[kind]))))
+            else:
+                if open_file is None:
+                    raise UnsupportedFeature(f"excitation function from the file {raw.strip()!r}: no file opener")
+                n_ignore, n_time, n_value = r.ints(1)[0], r.ints(1)[0], r.ints(1)[0]
+                samples = _samples(open_file(raw.strip()), n_ignore, n_time, n_value)
+                spec.functions.append(ExcitationFunction("file", tuple(r.values(2)), samples))
     # point excitations, read_excitation_point_list.F90:75-110
     if "excitation_point_list" in rec:
         r = rec["excitation_point_list"]
@@ -744,6 +779,12 @@ def read_inp_file(path: str, material: Optional[Callable[[str], VolumeMaterial]]
     """read_inp of a file; material file names resolve against the file's
     directory unless ``material`` is given.  The text is read as Latin-1: the
     reference's inputs hold stray non-ASCII bytes in remarks."""
+    directory = os.path.dirname(os.path.abspath(path))
     with open(path, encoding="latin-1") as f:
         lines = f.read().splitlines()
-    return read_inp(lines, material or vmat_in(os.path.dirname(os.path.abspath(path))))
+
+    def open_file(name: str) -> List[str]:
+        with open(os.path.join(directory, name), encoding="latin-1") as g:
+            return g.read().splitlines()
+
+    return read_inp(lines, material or vmat_in(directory), open_file)

@@ -280,8 +280,30 @@ def material_coefficients(mat: VolumeMaterial, dl: float, dt: float, reduced_c: 
 # ---------------------------------------------------------------------------
 @dataclass
 class ExcitationFunction:
-    type: str  # impulse | gaussian | gaussian_step | step | sinusoid | gaussian_sinusoid | differential_gaussian
+    """``type`` impulse | gaussian | gaussian_step | step | sinusoid |
+    gaussian_sinusoid | differential_gaussian, or "file": a table of
+    ``samples`` (times, values) read from a data file, evaluated as
+    parameters[0] * interpolate_function(t - parameters[1])
+    (EXCITATION/excitation.F90:522-540)."""
+
+    type: str
     parameters: Tuple[float, ...]
+    samples: Optional[Tuple[Sequence[float], Sequence[float]]] = None
+
+
+def interpolate_function(time: float, times: Sequence[float], values: Sequence[float]) -> float:
+    """EXCITATION/excitation.F90:710-768: the end values outside the table,
+    else linear interpolation in the first interval [t_i, t_i+1] holding time."""
+    if time <= times[0]:
+        return float(values[0])
+    if time >= times[-1]:
+        return float(values[-1])
+    for i in range(len(times) - 1):
+        t1, t2 = times[i], times[i + 1]
+        if t1 <= time <= t2:
+            v1, v2 = values[i], values[i + 1]
+            return float(v1 + (time - t1) * (v2 - v1) / (t2 - t1))
+    raise ValueError(f"interpolate_function: no interval holds time {time!r}")
 
 
 def excitation_tables(fns: Sequence[ExcitationFunction], n_timesteps: int, dt: float):
@@ -317,6 +339,10 @@ def excitation_tables(fns: Sequence[ExcitationFunction], n_timesteps: int, dt: f
                     phase = p[4] * PI / 180.0
                     g = math.exp(-(((t - delay) / width) ** 2)) if abs(t - delay) < width * 5.0 else 0.0
                     v = amp * g * math.sin(2.0 * PI * freq * (t - delay) - phase)
+                elif fn.type == "file":
+                    if fn.samples is None or len(fn.samples[0]) < 1:
+                        raise ValueError("a file excitation function without samples")
+                    v = p[0] * interpolate_function(t - p[1], fn.samples[0], fn.samples[1])
                 elif fn.type == "differential_gaussian":
                     amp, width, delay = p[0], p[1], p[2]
                     if abs(t - delay) < width * 5.0:

@@ -21,6 +21,9 @@ CASES = {
     "material_test2_Ex": "MATERIAL_TEST2/PROBLEM_SPECIFICATION_FILES/mat_test.field.tout_ref",
     **{f"huygens_box_{f}": f"HUYGENS_SURFACE/PROBLEM_SPECIFICATION_FILES/{f}_centre.tout_ref"
        for f in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")},
+    # the case's create_reference_result copies only this file; its excitation.tout_ref is
+    # from another delay (its pulse peaks 4.8 ns later than the input's) and is not used
+    "excitation_test_Ex": "EXCITATION_FUNCTION_TEST/PROBLEM_SPECIFICATION_FILES/excitation_test.field.tout_ref",
 }
 
 
@@ -41,6 +44,11 @@ INP_CASES = {
     "cavity_mur2": "CAVITY_MUR=2/PROBLEM_SPECIFICATION_FILES/cavity_1_2_3.inp",
     "parallel_test": "PARALLEL_TEST/PROBLEM_SPECIFICATION_FILES/cavity.inp",
     "box_slot": "SHIELDING_EFFECTIVENESS_BOX_SLOT/PROBLEM_SPECIFICATION_FILES/box_slot.inp",
+    "excitation_test": "EXCITATION_FUNCTION_TEST/PROBLEM_SPECIFICATION_FILES/excitation_test.inp",
+}
+# data files the inputs name (excitation function samples), as text
+DATA_CASES = {
+    "gaussian_from_file.dat": "EXCITATION_FUNCTION_TEST/PROBLEM_SPECIFICATION_FILES/gaussian_from_file.dat",
 }
 # the post-processor's Fourier transforms of those four cases' output point
 # (GGI_TLM_post_process_in.txt beside each: option 3, point 1, lin 1 MHz to
@@ -83,6 +91,12 @@ def main():
             inp[name] = np.array(f.read().splitlines())
     np.savez_compressed(os.path.join(here, "inp_text.npz"), **inp)
     print("inp_text", {k: len(v) for k, v in inp.items()})
+    data = {}
+    for name, rel in DATA_CASES.items():
+        with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", rel), encoding="latin-1") as f:
+            data[name] = np.array(f.read().splitlines())
+    np.savez_compressed(os.path.join(here, "data_text.npz"), **data)
+    print("data_text", {k: len(v) for k, v in data.items()})
     fo = {}
     for name, rel in FOUT_CASES.items():
         with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", rel)) as f:

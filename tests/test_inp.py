@@ -561,3 +561,61 @@ def test_gpu_all_output_packets_match_oracle(gpu_lib):
         assert rel(got_ps[ptr[k]:ptr[k + 1]], want_ps[ptr[k]:ptr[k + 1]]) < 1e-10, k
     for a, b in zip(got_ov, oracle.output_volumes(t, want)):
         assert a.shape == b.shape and rel(a, b) < 1e-10
+
+
+def data_file(name):
+    d = np.load(os.path.join(HERE, "golden", "data_text.npz"))
+    return [str(x) for x in d[name]]
+
+
+def test_interpolate_function():
+    from ggi_tlm_b200.problem import interpolate_function
+
+    ts, vs = [0.0, 1.0, 3.0], [2.0, 4.0, 0.0]
+    assert interpolate_function(-1.0, ts, vs) == 2.0 and interpolate_function(5.0, ts, vs) == 0.0
+    assert interpolate_function(1.0, ts, vs) == 4.0  # a sample time: the first interval holding it
+    assert interpolate_function(0.5, ts, vs) == 3.0 and interpolate_function(2.0, ts, vs) == 2.0
+
+
+def test_excitation_function_from_a_file_reproduces_the_golden_field():
+    """EXCITATION_FUNCTION_TEST: a Gaussian read from gaussian_from_file.dat
+    (240 samples, amplitude 5, delay 1 ns) launched by a closed Huygens box;
+    the centre Ex series against excitation_test.field.tout_ref."""
+    p = inp.read_inp(inputs()["excitation_test"], materials, data_file)
+    f = p.spec.functions[0]
+    assert (f.type, f.parameters, len(f.samples[0])) == ("file", (5.0, 1e-9), 240)
+    t = build_tables(p.spec)
+    assert t["n_timesteps"] == 300
+    # the tabulated values are the interpolated samples, scaled and delayed, at (ts-1)*dt
+    from ggi_tlm_b200.problem import interpolate_function
+
+    val = np.asarray(t["fn_value"]).reshape(-1)
+    for ts in (1, 40, 100, 300):
+        assert val[ts - 1] == 5.0 * interpolate_function((ts - 1) * t["dt"] - 1e-9, *f.samples)
+    series = probe_series(t, oracle.Oracle(t).run(t["n_timesteps"]))[0]
+    g = np.load(os.path.join(HERE, "golden", "excitation_test_Ex.npz"))
+    v = np.where(np.abs(series) < 1e-30, 0.0, series)
+    assert np.linalg.norm(v - g["value"]) / np.linalg.norm(g["value"]) < TOL
+
+
+def test_file_function_needs_an_opener_and_samples():
+    lines = inputs()["excitation_test"]
+    with pytest.raises(UnsupportedFeature, match="no file opener"):
+        inp.read_inp(lines, materials)
+    with pytest.raises(ValueError, match="without samples"):
+        inp.read_inp(lines, materials, lambda name: ["# nothing here"][1:])
+    with pytest.raises(UnsupportedFeature, match="'noise'"):
+        small("Excitation_function_list\n1\n1\nnoise\n1.0\n", BASE.replace(
+            "Excitation_function_list\n1\n1\ngaussian\n1.0 1e-9 3e-9\n", ""))
+
+
+@pytest.mark.gpu
+def test_gpu_excitation_function_from_a_file(gpu_lib):
+    p = inp.read_inp(inputs()["excitation_test"], materials, data_file)
+    t = build_tables(p.spec)
+    with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64) as g:
+        g.run(t["n_timesteps"])
+        series = probe_series(t, g.cell_output())[0]
+    gold = np.load(os.path.join(HERE, "golden", "excitation_test_Ex.npz"))["value"]
+    v = np.where(np.abs(series) < 1e-30, 0.0, series)
+    assert np.linalg.norm(v - gold) / np.linalg.norm(gold) < TOL
