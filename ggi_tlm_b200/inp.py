@@ -102,9 +102,10 @@ _SURFACE_PARAMS = {"rectangular_block2": 6, "rectangular_block": 3, "cylinder": 
 _WITH_FILE = {"tet_volume_mesh", "triangulated_surface", "vtk_triangulated_surface", "stl_triangulated_surface"}
 # parameters per excitation function type, read_excitation_function_list.F90:108-160
 _N_PARAMS = {"impulse": 1, "gaussian_step": 3, "step": 2, "gaussian": 3, "sinusoid": 3, "gaussian_sinusoid": 5,
-             "differential_gaussian": 3}
-# the reference's other function types, which the GPU path's tables do not restate
-_OTHER_FUNCTIONS = {"gaussian_step_sinusoid", "double_exponential", "noise", "sinusoidal_pulse", "ring_wave"}
+             "gaussian_step_sinusoid": 5, "double_exponential": 3, "differential_gaussian": 3,
+             "sinusoidal_pulse": 7, "ring_wave": 4}
+# noise draws from the Fortran run-time's random number generator, which the tables cannot reproduce
+_OTHER_FUNCTIONS = {"noise"}
 
 _REAL = re.compile(r"^([+-]?(?:\d+\.?\d*|\.\d+))(?:[eEdD]([+-]?\d+)|([+-]\d+))?$")
 

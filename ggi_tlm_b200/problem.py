@@ -281,7 +281,8 @@ def material_coefficients(mat: VolumeMaterial, dl: float, dt: float, reduced_c: 
 @dataclass
 class ExcitationFunction:
     """``type`` impulse | gaussian | gaussian_step | step | sinusoid |
-    gaussian_sinusoid | differential_gaussian, or "file": a table of
+    gaussian_sinusoid | differential_gaussian | gaussian_step_sinusoid |
+    double_exponential | sinusoidal_pulse | ring_wave, or "file": a table of
     ``samples`` (times, values) read from a data file, evaluated as
     parameters[0] * interpolate_function(t - parameters[1])
     (EXCITATION/excitation.F90:522-540)."""
@@ -343,12 +344,45 @@ def excitation_tables(fns: Sequence[ExcitationFunction], n_timesteps: int, dt: f
                     if fn.samples is None or len(fn.samples[0]) < 1:
                         raise ValueError("a file excitation function without samples")
                     v = p[0] * interpolate_function(t - p[1], fn.samples[0], fn.samples[1])
-                elif fn.type == "differential_gaussian":
+                elif fn.type == "differential_gaussian":  # normalised to a peak of amplitude, :395-415
                     amp, width, delay = p[0], p[1], p[2]
+                    tpeak = -width / math.sqrt(2.0)
+                    fpeak = -2.0 * (tpeak / (width ** 2)) * math.exp(-((tpeak / width) ** 2))
                     if abs(t - delay) < width * 5.0:
-                        v = -amp * 2.0 * ((t - delay) / width) * math.exp(-(((t - delay) / width) ** 2))
+                        v = -2.0 * ((t - delay) / width ** 2) * amp * math.exp(-(((t - delay) / width) ** 2)) / fpeak
                     else:
                         v = 0.0
+                elif fn.type == "gaussian_step_sinusoid":  # :335-373
+                    amp, width, delay, freq = p[0], p[1], p[2], p[3]
+                    phase = p[4] * PI / 180.0
+                    if t < delay:
+                        g = math.exp(-(((t - delay) / width) ** 2)) if abs(t - delay) < width * 5 else 0.0
+                    else:
+                        g = 1.0
+                    v = amp * g * math.sin(2.0 * PI * freq * t - phase)
+                elif fn.type in ("double_exponential", "ring_wave"):  # :375-393, :485-513
+                    # the face value takes 1/parameters(1) as its amplitude, as the reference does
+                    amp = p[0] if k == 0 else 1.0 / p[0]
+                    if t >= 0.0:
+                        alpha, beta = 1.0 / p[1], 1.0 / p[2]
+                        tpeak = (math.log(beta) - math.log(alpha)) / (beta - alpha)
+                        fpeak = math.exp(-alpha * tpeak) - math.exp(-beta * tpeak)
+                        v = (amp / fpeak) * (math.exp(-alpha * t) - math.exp(-beta * t))
+                        if fn.type == "ring_wave":
+                            v = v * math.sin(2.0 * PI * p[3] * t)
+                    else:
+                        v = 0.0
+                elif fn.type == "sinusoidal_pulse":  # :448-483: trapezoidal envelope t1..t4
+                    amp, freq, t1, t2, t3, t4 = p[0], p[1], p[3], p[4], p[5], p[6]
+                    phase = p[2] * PI / 180.0
+                    env = 0.0
+                    if t1 <= t < t2:
+                        env = (t - t1) / (t2 - t1)
+                    elif t2 <= t <= t3:
+                        env = 1.0
+                    elif t3 <= t <= t4:
+                        env = (t4 - t) / (t4 - t3)
+                    v = amp * env * math.sin(2.0 * PI * freq * t - phase)
                 else:
                     raise UnsupportedFeature(f"excitation function type {fn.type}")
                 if k == 0:
