@@ -99,6 +99,42 @@ def tout_series(rows: np.ndarray, point: int) -> Tuple[np.ndarray, np.ndarray]:
     return rows[sel, 0], rows[sel, 2]
 
 
+def power_surfaces(tables: dict, acc: np.ndarray) -> np.ndarray:
+    """write_frequency_domain_power_surfaces (OUTPUT/frequency_domain_power_surfaces.F90:
+    420-574): per power surface entry (surface, frequency) the sum over its
+    faces of sign (E1 H2* - E2 H1*) dl^2 / 2, sign +1 on a min face and -1 on
+    a max face; ``acc`` is the [faces, 4] (E1, E2, H1, H2) accumulator array
+    the library (GpuMesh.power_surfaces) or the oracle returns."""
+    ptr = np.asarray(tables["ps_face_ptr"])
+    codes = np.asarray(tables["ps_face_code"])
+    dl = float(tables["dl"])
+    out = np.zeros(len(ptr) - 1, dtype=np.complex128)
+    for e in range(len(ptr) - 1):
+        pwr = 0j
+        for k in range(ptr[e], ptr[e + 1]):
+            sign = 1.0 if codes[k] <= 3 else -1.0
+            e1, e2, h1, h2 = acc[k]
+            pwr = pwr + sign * (e1 * np.conj(h2) - e2 * np.conj(h1)) * dl * dl / 2.0
+        out[e] = pwr
+    return out
+
+
+def power_surface_lines(freqs: Sequence[float], surface: Sequence[int], power: Sequence[complex]) -> List[str]:
+    """The .frequency_domain_power_surface.fout file: its own header
+    (``(A,I10)`` counts: the surfaces and the frequencies of the first one),
+    then f, surface number, Re P, Im P, |Re P|, atan2(Im P, Re P), 10 log10 |Re P|."""
+    n_surf = len(set(surface))
+    n_freq = sum(1 for x in surface if x == surface[0]) if len(surface) else 0
+    lines = [HEADER, "# Number of data points:" + f"{n_surf:10d}", "# Number of frequencies:" + f"{n_freq:10d}"]
+    for f, num, p in zip(freqs, surface, power):
+        p = complex(p)
+        re = abs(p.real)
+        db = 10.0 * math.log10(re) if re > 0.0 else -math.inf
+        lines.append(fortran_e(f) + f"{int(num):5d}" +
+                     "".join(fortran_e(x) for x in (p.real, p.imag, re, math.atan2(p.imag, p.real), db)))
+    return lines
+
+
 def main(argv=None) -> int:
     """python -m ggi_tlm_b200.fout <file.tout> <point> <lin|log> <fmin> <fmax> <n_frequencies> <out.fout>:
     the post-processor's option 3 without its prompts."""

@@ -261,6 +261,7 @@ class Shape:
     par: Optional[List[float]]
     tr: Optional[Tuple[float, float, float]]
     rough: bool = False
+    rotated: bool = False
 
 
 def _geometry_list(r: Records, what: str, counts: Dict[str, int], supported: set) -> Dict[int, Shape]:
@@ -282,11 +283,11 @@ def _geometry_list(r: Records, what: str, counts: Dict[str, int], supported: set
             r.line()
             r.values(1 if kind == "sphere" else 2)
             rough = True
-        if kind in supported:
-            out[k] = Shape(kind, par, _transform(r, f"{what} {k}"), rough)
-        else:
-            r.values(6)  # its transformation
-            out[k] = Shape(kind, None, None, rough)
+        t = r.values(6)  # the transformation: three Euler angles, three translations
+        if kind in supported and not any(v != 0.0 for v in t[:3]):
+            out[k] = Shape(kind, par, (t[3], t[4], t[5]), rough)
+        else:  # refused when something uses it
+            out[k] = Shape(kind, None, None, rough, rotated=kind in supported)
     return out
 
 
@@ -305,6 +306,8 @@ def _surface_cells(mesh: Mesh, s: Shape, what: str):
     describes, and -1 when it points along +axis: build_surface_xplane.F90
     (and y/z) order the corners so that the normal is +x for y2>y1, z2>z1,
     -y for x2>x1, z2>z1 and +z for x2>x1, y2>y1."""
+    if s.rotated:
+        raise UnsupportedFeature(f"{what} on a rotated {s.kind}: only zero Euler angles are supported")
     if s.par is None:
         raise UnsupportedFeature(f"{what} on a surface of type {s.kind!r}")
     if s.rough:
@@ -485,6 +488,8 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
 
     def volume_block(v: int, what: str) -> Block:
         s = volumes[v]
+        if s.rotated:
+            raise UnsupportedFeature(f"{what} on a rotated {s.kind}: only zero Euler angles are supported")
         if s.par is None:
             raise UnsupportedFeature(f"{what} on a volume of type {s.kind!r}")
         return _block_cells(mesh, s.par, s.tr)
@@ -769,6 +774,42 @@ def _read_surface_materials(r: Records, mesh: Mesh, spec: ProblemSpec, surfaces:
                     spec.surface_sheets.append(SurfaceSheet(names[kind], ax, ix, r0, r1))
 
 
+# the packets that only ask for results; read_inp_lenient may leave them out
+OUTPUT_PACKETS = {"output_point_list", "output_surface_list", "output_volume_list", "output_volume_average_list",
+                  "output_volume_peak_list", "frequency_output_volume_list", "frequency_output_volume_list_xyz",
+                  "frequency_output_surface_list", "far_field_surface_list", "rcs_surface",
+                  "frequency_domain_power_surface_list", "sar_volume_list", "output_mode_list"}
+
+
+def read_inp_lenient(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
+                     open_file: Optional[Callable[[str], Sequence[str]]] = None) -> InpProblem:
+    """read_inp, leaving out each output packet that read_inp refuses (a
+    result the GPU path cannot produce exactly, such as an output surface on
+    rotated geometry) and listing it in ``skipped`` as "<packet>: <reason>".
+    Everything else is read as strictly as read_inp reads it."""
+    packets = split_packets(lines)
+
+    def text(keep):
+        out = []
+        for name, data in packets:
+            if name in keep:
+                out.append(name)
+                out.extend(data)
+        return out
+
+    core = {n for n, _ in packets if n not in OUTPUT_PACKETS}
+    dropped = []
+    for name in [n for n, _ in packets if n in OUTPUT_PACKETS]:
+        try:
+            read_inp(text(core | {name}), material, open_file)
+        except UnsupportedFeature as e:
+            dropped.append(f"{name}: {e}")
+    keep = core | {n for n, _ in packets if n in OUTPUT_PACKETS and not any(d.startswith(n + ":") for d in dropped)}
+    p = read_inp(text(keep), material, open_file)
+    p.skipped.extend(dropped)
+    return p
+
+
 def vmat_in(directory: str) -> Callable[[str], VolumeMaterial]:
     """A material resolver reading ``<directory>/<name>.vmat``."""
     from .vmat import read_vmat
@@ -776,10 +817,12 @@ def vmat_in(directory: str) -> Callable[[str], VolumeMaterial]:
     return lambda name: read_vmat(os.path.join(directory, name + ".vmat"))
 
 
-def read_inp_file(path: str, material: Optional[Callable[[str], VolumeMaterial]] = None) -> InpProblem:
-    """read_inp of a file; material file names resolve against the file's
-    directory unless ``material`` is given.  The text is read as Latin-1: the
-    reference's inputs hold stray non-ASCII bytes in remarks."""
+def read_inp_file(path: str, material: Optional[Callable[[str], VolumeMaterial]] = None,
+                  lenient: bool = False) -> InpProblem:
+    """read_inp (read_inp_lenient with ``lenient``) of a file; material and
+    data file names resolve against the file's directory unless ``material``
+    is given.  The text is read as Latin-1: the reference's inputs hold stray
+    non-ASCII bytes in remarks."""
     directory = os.path.dirname(os.path.abspath(path))
     with open(path, encoding="latin-1") as f:
         lines = f.read().splitlines()
@@ -788,4 +831,4 @@ def read_inp_file(path: str, material: Optional[Callable[[str], VolumeMaterial]]
         with open(os.path.join(directory, name), encoding="latin-1") as g:
             return g.read().splitlines()
 
-    return read_inp(lines, material or vmat_in(directory), open_file)
+    return (read_inp_lenient if lenient else read_inp)(lines, material or vmat_in(directory), open_file)

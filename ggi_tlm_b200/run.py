@@ -11,6 +11,9 @@ and file names (TLM_MODULES/File_information.F90:143-158):
   timestep (excitation.F90:186-553);
 - ``<problem_name>.field.tout``: the output points, each on its own output
   steps (output_points.F90);
+- ``<problem_name>.frequency_domain_power_surface.fout``: the power through
+  each power surface at each of its frequencies
+  (frequency_domain_power_surfaces.F90:420-574);
 - ``<problem_name>.volume_average_field.tout`` and
   ``.volume_peak_field.tout``: one value per output volume average or peak
   and output step (output_volume_averages.F90:330-350,
@@ -31,7 +34,7 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
-from . import capi
+from . import capi, fout
 from .inp import InpProblem, read_inp_file
 from .problem import build_tables, probe_series
 from .tout import data_line, excitation_rows, field_rows, header, output_flag
@@ -57,9 +60,12 @@ def _volume_rows(t: dict, spec, values: List[np.ndarray], kind: str):
 
 
 def write_results(name: str, p: InpProblem, t: dict, cell_out: np.ndarray, face_out: np.ndarray,
-                  volumes: Optional[List[np.ndarray]] = None, directory: str = ".") -> List[str]:
-    """Write the .tout files of a finished run; returns the paths written.
-    ``cell_out`` is [steps, n_kept, 6], ``face_out`` [n_face_points, steps]."""
+                  volumes: Optional[List[np.ndarray]] = None, directory: str = ".",
+                  power: Optional[np.ndarray] = None) -> List[str]:
+    """Write the result files of a finished run; returns the paths written.
+    ``cell_out`` is [steps, n_kept, 6], ``face_out`` [n_face_points, steps],
+    ``volumes`` the output volume results, ``power`` the power surface
+    accumulators [faces, 4]."""
     written = []
     n = int(t["n_timesteps"])
     if int(t["n_functions"]):
@@ -71,6 +77,13 @@ def write_results(name: str, p: InpProblem, t: dict, cell_out: np.ndarray, face_
         rows = field_rows(t, centre, face_out, timing=p.output_timing)
         path = os.path.join(directory, name + ".field.tout")
         _write(path, header(len(p.spec.outputs), n), rows)
+        written.append(path)
+    if p.spec.power_surfaces and power is not None:
+        surf = [k + 1 for k, ps in enumerate(p.spec.power_surfaces) for _ in ps.frequencies]
+        path = os.path.join(directory, name + ".frequency_domain_power_surface.fout")
+        with open(path, "w") as f:
+            for line in fout.power_surface_lines(t["ps_freq"], surf, fout.power_surfaces(t, power)):
+                f.write(line + "\n")
         written.append(path)
     for kind, extn in (("average", ".volume_average_field.tout"), ("peak", ".volume_peak_field.tout")):
         if any(v.kind == kind for v in p.spec.output_volumes):
@@ -90,9 +103,13 @@ def _write(path: str, head: Sequence[str], rows, flush_small: bool = True) -> No
 
 
 def run(name: str, precision: int = capi.TLM_PRECISION_FP64, device: int = 0, chunk: int = 1000,
-        directory: str = ".") -> List[str]:
-    """Read ``<directory>/<name>.inp``, run it and write its .tout files."""
-    p = read_inp_file(os.path.join(directory, name + ".inp"))
+        directory: str = ".", lenient: bool = False) -> List[str]:
+    """Read ``<directory>/<name>.inp``, run it and write its result files;
+    ``lenient`` leaves out the output packets the GPU path refuses."""
+    p = read_inp_file(os.path.join(directory, name + ".inp"), lenient=lenient)
+    for item in p.skipped:
+        if ":" in item:
+            print("left out", item)
     t = build_tables(p.spec)
     n = int(t["n_timesteps"])
     with capi.GpuMesh(t, precision=precision, device=device) as g:
@@ -105,7 +122,8 @@ def run(name: str, precision: int = capi.TLM_PRECISION_FP64, device: int = 0, ch
         cell_out = np.concatenate(cells) if cells else np.zeros((0, 0, 6))
         face_out = np.concatenate(faces, axis=1) if faces else np.zeros((0, 0))
         volumes = g.output_volumes() if p.spec.output_volumes else None
-    return write_results(name, p, t, cell_out, face_out, volumes, directory)
+        power = g.power_surfaces() if p.spec.power_surfaces else None
+    return write_results(name, p, t, cell_out, face_out, volumes, directory, power)
 
 
 def main(argv: Optional[Sequence[str]] = None) -> int:
@@ -114,10 +132,11 @@ def main(argv: Optional[Sequence[str]] = None) -> int:
     ap.add_argument("--fp32", action="store_true", help="FP32 link state (default FP64)")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--chunk", type=int, default=1000, help="steps per run call between read-backs")
+    ap.add_argument("--lenient", action="store_true", help="leave out output packets the GPU path refuses")
     a = ap.parse_args(argv)
     try:
         for path in run(a.problem_name, capi.TLM_PRECISION_FP32 if a.fp32 else capi.TLM_PRECISION_FP64, a.device,
-                        a.chunk):
+                        a.chunk, lenient=a.lenient):
             print("wrote", path)
     except (RuntimeError, OSError) as e:  # TLMError is a RuntimeError, as is a library not built
         print(f"ERROR in run_TLM_gpu: {e}", file=sys.stderr)

@@ -24,6 +24,7 @@ CASES = {
     # the case's create_reference_result copies only this file; its excitation.tout_ref is
     # from another delay (its pulse peaks 4.8 ns later than the input's) and is not used
     "excitation_test_Ex": "EXCITATION_FUNCTION_TEST/PROBLEM_SPECIFICATION_FILES/excitation_test.field.tout_ref",
+    "power_calc_Ex": "POWER_CALCS/PROBLEM_SPECIFICATION_FILES/power_calc.field.tout_ref",
 }
 
 
@@ -45,6 +46,7 @@ INP_CASES = {
     "parallel_test": "PARALLEL_TEST/PROBLEM_SPECIFICATION_FILES/cavity.inp",
     "box_slot": "SHIELDING_EFFECTIVENESS_BOX_SLOT/PROBLEM_SPECIFICATION_FILES/box_slot.inp",
     "excitation_test": "EXCITATION_FUNCTION_TEST/PROBLEM_SPECIFICATION_FILES/excitation_test.inp",
+    "power_calc": "POWER_CALCS/PROBLEM_SPECIFICATION_FILES/power_calc.inp",
 }
 # data files the inputs name (excitation function samples), as text
 DATA_CASES = {
@@ -60,6 +62,8 @@ FOUT_CASES = {
     "parallel_test": "PARALLEL_TEST/PROBLEM_SPECIFICATION_FILES/cavity.fout_ref",
     # option 3 on the excitation and on the probe, then option 6: excitation / probe
     "box_slot": "SHIELDING_EFFECTIVENESS_BOX_SLOT/PROBLEM_SPECIFICATION_FILES/Shielding_effectiveness.fout_ref",
+    # written by the solver itself (write_frequency_domain_power_surfaces)
+    "power_calc": "POWER_CALCS/PROBLEM_SPECIFICATION_FILES/power_calc.frequency_domain_power_surface.fout_ref",
 }
 
 

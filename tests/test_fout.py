@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 from ggi_tlm_b200 import capi, fout, tout
-from ggi_tlm_b200.inp import read_inp
+from ggi_tlm_b200.inp import read_inp, read_inp_lenient
 from ggi_tlm_b200.problem import build_tables, probe_series
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -166,3 +166,48 @@ def test_gpu_shielding_effectiveness_matches_reference_golden(gpu_lib):
         g.run(t["n_timesteps"])
         cell = g.cell_output()
     check("box_slot", *shielding_effectiveness(p, t, cell, np.zeros((0, t["n_timesteps"]))))
+
+
+def power_calc():
+    p = read_inp_lenient(test_inp.inputs()["power_calc"], test_inp.materials)
+    return p, build_tables(p.spec)
+
+
+def check_power_calc(t, face, acc):
+    """POWER_CALCS: an impulse plane wave from the outer Huygens surface.  The
+    zmax-face probe against power_calc.field.tout_ref, and the power through
+    a 1 m^2 patch against power_calc.frequency_domain_power_surface.fout_ref.
+    That file predates the removal of the dt factor from the power
+    accumulators (frequency_domain_power_surfaces.F90:331, "remove dt
+    normalisation here"), which this library follows, so it is compared
+    with P dt^2."""
+    g = np.load(os.path.join(HERE, "golden", "power_calc_Ex.npz"))["value"]
+    v = np.where(np.abs(face[0]) < 1e-30, 0.0, face[0])
+    assert np.linalg.norm(v - g) / np.linalg.norm(g) < TOL
+    power = fout.power_surfaces(t, acc)
+    lines = fout.power_surface_lines(t["ps_freq"], [1] * len(power), power)
+    gl = golden("power_calc")
+    assert lines[:3] == gl[:3] and len(lines) == len(gl)
+    gf = fout.read_fout(gl)
+    np.testing.assert_allclose(np.asarray(t["ps_freq"]), gf[:, 0], rtol=5.01e-7)
+    scaled = power * float(t["dt"]) ** 2
+    assert np.linalg.norm(scaled.real - gf[:, 2]) / np.linalg.norm(gf[:, 2]) < TOL
+    assert np.abs(scaled.imag - gf[:, 3]).max() < 1e-9 * np.abs(gf[:, 2]).max()
+
+
+def test_oracle_power_calcs_matches_reference_golden():
+    p, t = power_calc()
+    assert p.skipped == ["output_surface_list: an output surface on a rotated rectangle: only zero Euler angles "
+                         "are supported"]
+    o = oracle.Oracle(t)
+    o.run(t["n_timesteps"])
+    check_power_calc(t, o.face_probes(), oracle.power_surfaces(t))
+
+
+@pytest.mark.gpu
+def test_gpu_power_calcs_matches_reference_golden(gpu_lib):
+    p, t = power_calc()
+    with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64) as g:
+        g.run(t["n_timesteps"])
+        face, acc = g.face_output(), g.power_surfaces()
+    check_power_calc(t, face, acc)

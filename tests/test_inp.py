@@ -619,3 +619,16 @@ def test_gpu_excitation_function_from_a_file(gpu_lib):
     gold = np.load(os.path.join(HERE, "golden", "excitation_test_Ex.npz"))["value"]
     v = np.where(np.abs(series) < 1e-30, 0.0, series)
     assert np.linalg.norm(v - gold) / np.linalg.norm(gold) < TOL
+
+
+def test_lenient_reading_leaves_out_only_refused_output_packets():
+    lines = inputs()["power_calc"]
+    with pytest.raises(UnsupportedFeature, match="rotated rectangle"):
+        inp.read_inp(lines, materials)  # strict: the output surface on the rotated rectangle
+    p = inp.read_inp_lenient(lines, materials)
+    assert p.skipped == ["output_surface_list: an output surface on a rotated rectangle: only zero Euler angles "
+                         "are supported"]
+    assert p.spec.output_surfaces == [] and len(p.spec.outputs) == 1 and len(p.spec.power_surfaces) == 1
+    # geometry and sources are never left out
+    with pytest.raises(UnsupportedFeature):
+        inp.read_inp_lenient(BASE.splitlines() + ["Cable_list", "0"], materials)
