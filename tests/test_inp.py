@@ -300,7 +300,9 @@ Ez
 
 
 @pytest.mark.parametrize("extra, match", [
-    ("Volume_list\n1\n1\nrectangular_block\n0.4 0.4 0.4\n0 0 45\n0.5 0.5 0.5\n", "rotated volume"),
+    ("Volume_list\n1\n1\nrectangular_block\n0.4 0.4 0.4\n0 0 45\n0.5 0.5 0.5\nVolume_material_list\n1\n1\nPEC\n1\n1\n",
+     "rotated rectangular_block"),                                                             # rotated, used
+    ("Volume_list\n1\n1\nrectangular_block\n0.4 0.4 0.4\n0 0 45\n0.5 0.5 0.5\n", None),    # rotated, unused
     ("Volume_list\n1\n1\nsphere\n0.2\n0 0 0\n0.5 0.5 0.5\nVolume_material_list\n1\n1\nPEC\n1\n1\n",
      "type 'sphere'"),                                                                      # not voxelised here
     ("Volume_list\n1\n1\nrectangular_block\n0.5 0.5 0.5\n0 0 0\n0.5 0.5 0.5\nVolume_material_list\n1\n1\nPEC\n1\n1\n",
@@ -322,6 +324,9 @@ def test_refusals(extra, match):
     malformed input raises ValueError, as the reference stops with an error."""
     base = BASE.replace("Excitation_function_list\n1\n1\ngaussian\n1.0 1e-9 3e-9\n", "") \
         if "Excitation_function_list" in extra else BASE
+    if match is None:  # refused only where it is used
+        small(extra, base)
+        return
     err = ValueError if match in ("numbered in order", "component 'jx'") else UnsupportedFeature
     with pytest.raises(err, match=match) as e:
         small(extra, base)
