@@ -422,6 +422,9 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
             raise ValueError(f"{name} packet given twice")
         rec[name] = Records(name, data)
     skipped = [n for n, _ in packets if n in NEUTRAL]
+    for need in ("mesh_outer_boundary_dimension", "simulation_time"):
+        if need not in rec:
+            raise ValueError(f"not a GGI_TLM problem file: no {need} packet")
     # the mesh, MESH/set_mesh_parameters.F90:40-100: a cell size wins over a cell count
     xmin, xmax, ymin, ymax, zmin, zmax = rec["mesh_outer_boundary_dimension"].values(6)
     ext = (xmax - xmin, ymax - ymin, zmax - zmin)

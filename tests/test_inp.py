@@ -135,6 +135,13 @@ def small(extra="", base=BASE):
     return inp.read_inp((base + extra).splitlines(), materials)
 
 
+def test_required_packets():
+    with pytest.raises(ValueError, match="no simulation_time packet"):
+        small(base=BASE.replace("Simulation_time\n1e-8\n", ""))
+    with pytest.raises(ValueError, match="no mesh_outer_boundary_dimension packet"):
+        inp.read_inp(["# the input of another program", "Filter_order", "2"], materials)
+
+
 def test_every_keyword_has_one_treatment():
     groups = [inp.HANDLED, inp.NEUTRAL, inp.UNSUPPORTED, inp.NOT_READ]
     assert set().union(*groups) == inp.PACKETS
