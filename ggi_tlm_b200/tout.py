@@ -24,6 +24,10 @@ def fortran_e(value: float, width: int = 16, digits: int = 7) -> str:
     the exponent as ``E+xx`` (or ``+xxx`` without the E when it needs three
     digits), right-justified in ``width`` columns."""
     v = float(value)
+    if v != v:
+        return "NaN".rjust(width)
+    if v in (float("inf"), float("-inf")):  # gfortran writes the word, signed only when negative
+        return ("-Infinity" if v < 0 else "Infinity").rjust(width)
     if v == 0.0:
         body = "0." + "0" * digits + "E+00"
         return body.rjust(width)

@@ -45,7 +45,8 @@ def oracle_files(tmp, name, lines):
     cell = o.run(t["n_timesteps"])
     face = o.face_probes() if int(t["n_face_probes"]) else np.zeros((0, t["n_timesteps"]))
     vols = oracle.output_volumes(t, cell) if p.spec.output_volumes else None
-    return runner.write_results(name, p, t, cell, face, vols, tmp), p, t
+    power = oracle.power_surfaces(t) if p.spec.power_surfaces else None
+    return runner.write_results(name, p, t, cell, face, vols, tmp, power), p, t
 
 
 def test_field_tout_from_the_huygens_input(tmp_path):
@@ -74,8 +75,11 @@ def test_volume_average_and_peak_files(tmp_path):
     lines = test_inp.ALL_OUTPUTS.splitlines()
     paths, p, t = oracle_files(str(tmp_path), "all", lines)
     names = sorted(os.path.basename(x) for x in paths)
-    assert names == ["all.excitation.tout", "all.field.tout", "all.volume_average_field.tout",
-                     "all.volume_peak_field.tout"]
+    assert names == ["all.excitation.tout", "all.field.tout", "all.frequency_domain_power_surface.fout",
+                     "all.volume_average_field.tout", "all.volume_peak_field.tout"]
+    pw = [x for x in open(os.path.join(str(tmp_path), "all.frequency_domain_power_surface.fout")).read().splitlines()]
+    assert pw[:3] == ["# Frequency Domain Data", "# Number of data points:         1",
+                      "# Number of frequencies:         3"] and len(pw) == 6
     avg = read_tout(os.path.join(str(tmp_path), "all.volume_average_field.tout"))
     peak = read_tout(os.path.join(str(tmp_path), "all.volume_peak_field.tout"))
     dt = float(t["dt"])
@@ -120,6 +124,10 @@ def test_gpu_runner_files_match_oracle_files(gpu_lib, tmp_path, name, text):
         with open(a) as fa, open(b) as fb:
             la, lb = fa.read().splitlines(), fb.read().splitlines()
         assert la[:3] == lb[:3] and len(la) == len(lb)
+        if a.endswith(".fout"):
+            da, db = np.loadtxt(la, comments="#", ndmin=2), np.loadtxt(lb, comments="#", ndmin=2)
+            np.testing.assert_allclose(db[:, 2:4], da[:, 2:4], rtol=1.01e-6, atol=1e-9 * np.abs(da[:, 2:4]).max())
+            continue
         da, db = read_tout(a), read_tout(b)
         assert np.array_equal(da[:, 1], db[:, 1])
         np.testing.assert_allclose(db[:, 0], da[:, 0], rtol=1e-7)

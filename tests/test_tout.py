@@ -59,3 +59,11 @@ def test_field_file_from_oracle_series(tmp_path):
     assert np.allclose(back[:, 2], want, rtol=5.01e-7, atol=0)  # 0.ddddddd: half a unit of the 7th digit
     with open(path) as f:
         assert f.readline().rstrip("\n") == tout.HEADER
+
+
+def test_non_finite_values():
+    from ggi_tlm_b200.tout import fortran_e
+
+    assert fortran_e(float("-inf")) == "       -Infinity"
+    assert fortran_e(float("inf")) == "        Infinity"
+    assert fortran_e(float("nan")) == "             NaN"
