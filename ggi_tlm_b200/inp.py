@@ -291,10 +291,18 @@ def _geometry_list(r: Records, what: str, counts: Dict[str, int], supported: set
     return out
 
 
-def _block_cells(mesh: Mesh, par, tr) -> Block:
-    """The cells whose centres lie inside an axis-aligned block of sides
-    ``par`` centred on the translation ``tr`` (build_volume_rectangular_block.F90)."""
-    rng = [mesh.centres_in(a, tr[a] - par[a] / 2.0, tr[a] + par[a] / 2.0) for a in range(3)]
+def _block_cells(mesh: Mesh, par, tr, kind: str = "rectangular_block") -> Block:
+    """The cells whose centres lie inside an axis-aligned block: of sides
+    ``par`` centred on the translation ``tr`` (build_volume_rectangular_block.F90),
+    or for rectangular_block2 between the corners par[0:3] and par[3:6], each
+    pair sorted, moved by ``tr`` (build_volume_rectangular_block2.F90)."""
+    if kind == "rectangular_block2":
+        lo = [min(par[a], par[3 + a]) + tr[a] for a in range(3)]
+        hi = [max(par[a], par[3 + a]) + tr[a] for a in range(3)]
+    else:
+        lo = [tr[a] - par[a] / 2.0 for a in range(3)]
+        hi = [tr[a] + par[a] / 2.0 for a in range(3)]
+    rng = [mesh.centres_in(a, lo[a], hi[a]) for a in range(3)]
     return Block(rng[0][0], rng[0][1], rng[1][0], rng[1][1], rng[2][0], rng[2][1])
 
 
@@ -313,8 +321,9 @@ def _surface_cells(mesh: Mesh, s: Shape, what: str):
     if s.rough:
         raise UnsupportedFeature(f"{what} on a surface with random roughness")
     par, tr = s.par, s.tr
-    if s.kind == "rectangular_block":
-        b = _block_cells(mesh, par, tr)
+    if s.kind in ("rectangular_block", "rectangular_block2"):
+        # both builders give every triangle an inward normal (the HuygensBox convention)
+        b = _block_cells(mesh, par, tr, s.kind)
         return "box", ((b.i0, b.i1), (b.j0, b.j1), (b.k0, b.k1)), 1
     if s.kind == "rectangle":  # lx by ly in the local xy-plane, centred on the translation
         axis, orient = 2, 1
@@ -483,11 +492,11 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
             p = r.values(3)
             tr = _transform(r, f"point {k}")
             points[k] = (p[0] + tr[0], p[1] + tr[1], p[2] + tr[2])
-    volumes = _geometry_list(rec["volume_list"], "volume", _VOLUME_PARAMS, {"rectangular_block"}) \
-        if "volume_list" in rec else {}
+    volumes = _geometry_list(rec["volume_list"], "volume", _VOLUME_PARAMS,
+                             {"rectangular_block", "rectangular_block2"}) if "volume_list" in rec else {}
     surfaces = _geometry_list(rec["surface_list"], "surface", _SURFACE_PARAMS,
-                              {"rectangular_block", "rectangle", "xplane", "yplane", "zplane"}) \
-        if "surface_list" in rec else {}
+                              {"rectangular_block", "rectangular_block2", "rectangle", "xplane", "yplane",
+                               "zplane"}) if "surface_list" in rec else {}
 
     def volume_block(v: int, what: str) -> Block:
         s = volumes[v]
@@ -495,7 +504,7 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
             raise UnsupportedFeature(f"{what} on a rotated {s.kind}: only zero Euler angles are supported")
         if s.par is None:
             raise UnsupportedFeature(f"{what} on a volume of type {s.kind!r}")
-        return _block_cells(mesh, s.par, s.tr)
+        return _block_cells(mesh, s.par, s.tr, s.kind)
 
     # volume materials, read_volume_material_list.F90:90-180
     if "volume_material_list" in rec:

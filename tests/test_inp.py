@@ -644,3 +644,50 @@ def test_lenient_reading_leaves_out_only_refused_output_packets():
     # geometry and sources are never left out
     with pytest.raises(UnsupportedFeature):
         inp.read_inp_lenient(BASE.splitlines() + ["Cable_list", "0"], materials)
+
+
+def test_two_corner_blocks_equal_centred_blocks():
+    """rectangular_block2 (corners, either order, plus the translation) gives
+    the cells and, as a surface, the Huygens box of the centred block with
+    the same extent; both builders give the box's triangles inward normals."""
+    geo = """Volume_list
+2
+1
+rectangular_block
+0.4 0.4 0.6
+0 0 0
+0.5 0.5 0.5
+2
+rectangular_block2
+0.2 0.2 -0.1   -0.2 -0.2 0.5
+0 0 0
+0.5 0.5 0.3
+Surface_list
+2
+1
+rectangular_block
+0.4 0.4 0.6
+0 0 0
+0.5 0.5 0.5
+2
+rectangular_block2
+-0.2 -0.2 -0.3   0.2 0.2 0.3
+0 0 0
+0.5 0.5 0.5
+Volume_material_list
+2
+1
+PEC
+1
+1
+2
+PMC
+1
+2
+"""
+    hs = "Huygens_surface\n{n}\n-1\n1\n30.0 20.0\n1.0 0.0\n"
+    a = small(geo + hs.format(n=1))
+    b = small(geo + hs.format(n=2))
+    (_, b1), (_, b2) = a.spec.material_regions
+    assert b1 == b2 and (b1.i0, b1.i1, b1.k0, b1.k1) == (4, 7, 3, 8)
+    assert a.spec.huygens == b.spec.huygens
