@@ -78,13 +78,15 @@ def _load():
         _lib.tlm_oracle_get_links.argtypes = [C.c_void_p, _f64p]
         _lib.tlm_oracle_get_face_probes.argtypes = [C.c_void_p, _f64p]
         _lib.tlm_oracle_get_far_field.argtypes = [C.c_void_p, _f64p]
+        _lib.tlm_oracle_set_threads.argtypes = [C.c_void_p, C.c_int32]
+        _lib.tlm_oracle_set_threads.restype = C.c_int32
     return _lib
 
 
 class Oracle:
     """One oracle instance over one problem's tables."""
 
-    def __init__(self, t: dict):
+    def __init__(self, t: dict, threads: int = 1):
         lib = _load()
         self.t = t
         keep = []
@@ -148,6 +150,7 @@ class Oracle:
         self._h = lib.tlm_oracle_create(C.byref(p))
         if not self._h:
             raise MemoryError("oracle allocation failed")
+        self.threads = lib.tlm_oracle_set_threads(self._h, int(threads))
         self.step = 0
 
     def run(self, n_steps: int) -> np.ndarray:

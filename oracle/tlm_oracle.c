@@ -9,6 +9,7 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <pthread.h>
 
 /* SRC/CONSTANTS/constants.F90:27-39 */
 static const double Z0 = 376.73031346177;
@@ -74,6 +75,12 @@ struct tlm_oracle_state {
   int32_t *face_code;  /* [nz][ny][nx][3] -> 1-based special face index */
   double *dft;         /* per surface face: re, im */
   int32_t *dft_off;
+  /* host threads for scatter and connect (tlm_oracle_set_threads), and the
+     running output / excitation counters at the start of every z-plane, so
+     the planes can be taken by different threads with the numbering of the
+     sequential traversal */
+  int threads;
+  int32_t *plane_out0, *plane_exc0, *plane_fexc0, *plane_fout0;
 };
 
 #define VIDX(s, port, cx, cy, cz) \
@@ -171,6 +178,37 @@ tlm_oracle_state *tlm_oracle_create(const tlm_oracle_problem *p) {
     size_t cell = ((size_t)(p->face_cz[f] - 1) * p->ny + (p->face_cy[f] - 1)) * p->nx + (p->face_cx[f] - 1);
     s->face_code[cell * 3 + (p->face_dir[f] - 1)] = f + 1;
   }
+  s->threads = 1;
+  s->plane_out0 = (int32_t *)calloc((size_t)p->nz + 1, sizeof(int32_t));
+  s->plane_exc0 = (int32_t *)calloc((size_t)p->nz + 1, sizeof(int32_t));
+  s->plane_fexc0 = (int32_t *)calloc((size_t)p->nz + 1, sizeof(int32_t));
+  s->plane_fout0 = (int32_t *)calloc((size_t)p->nz + 1, sizeof(int32_t));
+  {
+    /* the counters scatter() and connect() advance, at the start of each plane */
+    int out = 0, exc = 0, fexc = 0, fout = 0;
+    size_t cell = 0;
+    for (int cz = 0; cz < p->nz; cz++) {
+      s->plane_out0[cz] = out; s->plane_exc0[cz] = exc;
+      s->plane_fexc0[cz] = fexc; s->plane_fout0[cz] = fout;
+      for (size_t c = 0; c < (size_t)p->nx * p->ny; c++, cell++) {
+        int code = p->cell_code[cell];
+        if (code) {
+          int sc = code - 1;
+          if (p->sp_output[sc]) out++;
+          if (!p->sp_pml[sc] && p->sp_excitation[sc]) exc++;
+        }
+        /* connect() skips the faces on the mesh's min boundary planes */
+        const int on_min[3] = {(int)(c % (size_t)p->nx) == 0, (int)(c / (size_t)p->nx) == 0, cz == 0};
+        for (int d = 0; d < 3; d++) {
+          int f = on_min[d] ? 0 : s->face_code[cell * 3 + d];
+          if (f) {
+            if (p->face_exc[f - 1]) fexc++;
+            if (p->face_out[f - 1]) fout++;
+          }
+        }
+      }
+    }
+  }
   int ndftf = p->n_dft ? p->dft_face_ptr[p->n_dft] : 0;
   s->dft = (double *)calloc((size_t)ndftf * 2 + 1, sizeof(double));
   s->timestep = 0;
@@ -182,6 +220,7 @@ void tlm_oracle_destroy(tlm_oracle_state *s) {
   free(s->V); free(s->sp_filter); free(s->eps_f); free(s->mu_f); free(s->pml); free(s->pml_mat); free(s->pml_mat_pos); free(s->face_probe_rec); free(s->ff_acc);
   free(s->cell_exc); free(s->cell_exc_type); free(s->cell_out); free(s->face_exc);
   free(s->face_exc_type); free(s->face_out); free(s->face_code); free(s->dft);
+  free(s->plane_out0); free(s->plane_exc0); free(s->plane_fexc0); free(s->plane_fout0);
   free(s);
 }
 
@@ -599,13 +638,14 @@ static void scatter_pulses(tlm_oracle_state *s, int cx, int cy, int cz, double V
   V_(Vz_ymax, cx, cy, cz) = Vz - Z0 * Ix - V_min;
 }
 
-/* scatter(), TLM_SOLVER/scatter.F90:49-591 */
-static int scatter(tlm_oracle_state *s) {
+/* scatter(), TLM_SOLVER/scatter.F90:49-591, for the cells of plane cz; the
+   output and excitation cell counters run on from *out_no / *exc_no */
+static int scatter_plane(tlm_oracle_state *s, int cz, int *out_no, int *exc_no) {
   const tlm_oracle_problem *p = &s->p;
   const double dl = p->dl;
   const double Z04 = Z0 * 4.0, Y04 = Y0 * 4.0;
-  int cell_number = 0, output_cell_number = 0, excitation_cell_number = 0;
-  for (int cz = 1; cz <= s->nz; cz++)
+  int cell_number = (cz - 1) * s->ny * s->nx, output_cell_number = *out_no, excitation_cell_number = *exc_no;
+  {
     for (int cy = 1; cy <= s->ny; cy++)
       for (int cx = 1; cx <= s->nx; cx++) {
         int code = p->cell_code[cell_number];
@@ -729,7 +769,72 @@ static int scatter(tlm_oracle_state *s) {
         }
         scatter_pulses(s, cx, cy, cz, Vx, Vy, Vz, Ix, Iy, Iz);
       }
+  }
+  *out_no = output_cell_number;
+  *exc_no = excitation_cell_number;
   return 0;
+}
+
+static void connect_plane(tlm_oracle_state *s, int cz, int excitation_face_number, int output_face_number);
+
+/* z-planes shared among s->threads POSIX threads in contiguous slabs, each
+   plane starting from the counters of the sequential traversal */
+typedef struct {
+  tlm_oracle_state *s;
+  int pass, z0, z1, rc;
+} plane_job;
+
+static void *plane_worker(void *arg) {
+  plane_job *j = (plane_job *)arg;
+  tlm_oracle_state *s = j->s;
+  for (int cz = j->z0; cz <= j->z1; cz++) {
+    if (j->pass == 0) {
+      int out_no = s->plane_out0[cz - 1], exc_no = s->plane_exc0[cz - 1];
+      int rc = scatter_plane(s, cz, &out_no, &exc_no);
+      if (rc && !j->rc) j->rc = rc;
+    } else {
+      connect_plane(s, cz, s->plane_fexc0[cz - 1], s->plane_fout0[cz - 1]);
+    }
+  }
+  return NULL;
+}
+
+static int run_planes(tlm_oracle_state *s, int pass) {
+  int T = s->threads < s->nz ? s->threads : s->nz;
+  if (T > 256) T = 256;
+  plane_job jobs[256];
+  pthread_t th[256];
+  int started[256];
+  for (int t = 0; t < T; t++) {
+    jobs[t].s = s;
+    jobs[t].pass = pass;
+    jobs[t].z0 = 1 + (int)((long long)s->nz * t / T);
+    jobs[t].z1 = (int)((long long)s->nz * (t + 1) / T);
+    jobs[t].rc = 0;
+    started[t] = t > 0 && pthread_create(&th[t], NULL, plane_worker, &jobs[t]) == 0;
+    if (t > 0 && !started[t]) plane_worker(&jobs[t]); /* no thread: do the slab here */
+  }
+  plane_worker(&jobs[0]);
+  int rc = 0;
+  for (int t = 0; t < T; t++) {
+    if (t > 0 && started[t]) pthread_join(th[t], NULL);
+    if (jobs[t].rc && !rc) rc = jobs[t].rc;
+  }
+  return rc;
+}
+
+/* scatter() over all planes: in traversal order on one thread, or planes
+   shared among threads with the counters each plane starts from */
+static int scatter(tlm_oracle_state *s) {
+  if (s->threads <= 1) {
+    int out_no = 0, exc_no = 0;
+    for (int cz = 1; cz <= s->nz; cz++) {
+      int rc = scatter_plane(s, cz, &out_no, &exc_no);
+      if (rc) return rc;
+    }
+    return 0;
+  }
+  return run_planes(s, 0);
 }
 
 /* one special face of connect(): connect_normal_to_{x,y,z}.F90 for faces
@@ -810,10 +915,9 @@ static void connect_special_face(tlm_oracle_state *s, int f, int cx, int cy, int
 
 /* connect(), TLM_SOLVER/connect.F90:180-214 with the free-space branches of
    connect_normal_to_{x,y,z}.F90:1-10 */
-static void connect(tlm_oracle_state *s) {
-  int excitation_face_number = 0, output_face_number = 0;
-  size_t cell = 0;
-  for (int cz = 1; cz <= s->nz; cz++)
+static void connect_plane(tlm_oracle_state *s, int cz, int excitation_face_number, int output_face_number) {
+  size_t cell = (size_t)(cz - 1) * s->ny * s->nx;
+  {
     for (int cy = 1; cy <= s->ny; cy++)
       for (int cx = 1; cx <= s->nx; cx++, cell++) {
         if (cx != 1) {
@@ -856,6 +960,18 @@ static void connect(tlm_oracle_state *s) {
           }
         }
       }
+  }
+}
+
+/* Every port takes part in exactly one face, so the faces of different
+   planes touch disjoint ports and the planes can be connected in any order
+   or at once, with the same result. */
+static void connect(tlm_oracle_state *s) {
+  if (s->threads <= 1) {
+    for (int cz = 1; cz <= s->nz; cz++) connect_plane(s, cz, s->plane_fexc0[cz - 1], s->plane_fout0[cz - 1]);
+    return;
+  }
+  run_planes(s, 1);
 }
 
 /* outer_boundary(), TLM_SOLVER/outer_boundary.F90:71-131 */
@@ -1049,4 +1165,9 @@ int tlm_oracle_get_links(tlm_oracle_state *s, double *out) {
       for (int cx = 1; cx <= s->nx; cx++)
         for (int port = 0; port < 12; port++) out[i++] = V_(port, cx, cy, cz);
   return 0;
+}
+
+int tlm_oracle_set_threads(tlm_oracle_state *s, int32_t threads) {
+  s->threads = threads < 1 ? 1 : (threads > 256 ? 256 : threads);
+  return s->threads;
 }

@@ -153,6 +153,11 @@ int tlm_oracle_get_far_field(tlm_oracle_state *s, double *out);
 int tlm_oracle_get_face_probes(tlm_oracle_state *s, double *out);
 /* link array dump in the reference layout V(12, nx, ny, nz) interior only */
 int tlm_oracle_get_links(tlm_oracle_state *s, double *out);
+/* host threads for the scatter and connect passes (z-planes shared among
+   them, as the reference's MPI build shares z-slabs among ranks); the
+   arithmetic of every cell and face is unchanged, so the results are the
+   same for any count (at most 256).  Returns the count in use. */
+int tlm_oracle_set_threads(tlm_oracle_state *s, int32_t threads);
 
 #ifdef __cplusplus
 }

@@ -3,11 +3,11 @@ known-answer cases into compact fixtures (tests/golden/*.npz).
 
 Reads GGI_TLM's TEST_DATA/*/PROBLEM_SPECIFICATION_FILES/*.tout_ref (text,
 format (E16.7,I5,E16.7), SRC/TLM_MODULES/File_information.F90:235) from the
-reference checkout given on the command line (default /root/reference) and
-stores (time, value) arrays.  Run once where the reference is present; the
+reference checkout named on the command line (or by the GGI_TLM_REFERENCE
+environment variable) and stores (time, value) arrays.  Run once where the reference is present; the
 fixtures travel with the repository.
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
 """
 import os
 import sys
@@ -68,7 +68,9 @@ FOUT_CASES = {
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GGI_TLM_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py <reference checkout> (or set GGI_TLM_REFERENCE)")
     here = os.path.dirname(os.path.abspath(__file__))
     for name, rel in CASES.items():
         path = os.path.join(ref, "GGI_TLM", "TEST_DATA", rel)

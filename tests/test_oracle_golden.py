@@ -82,3 +82,33 @@ def test_mesh_dl_uses_reciprocal_of_three():
     assert (dlx + dlx + dlx) / 3.0 != 0.1
     assert cases.cubic_mesh_dl(-2.0, 2.0, 40) == 0.1
     assert cases.kat_huygens_box().outputs[0].cell == (21, 21, 21)
+
+
+def _run_all(t, threads):
+    o = O.Oracle(t, threads=threads)
+    co = o.run(t["n_timesteps"])
+    res = (co, o.links(), o.dft(), o.far_field(), o.face_probes())
+    o.close()
+    return res
+
+
+@pytest.mark.parametrize("threads", [2, 3, 7])
+def test_threaded_oracle_is_bit_identical(threads):
+    """The oracle's plane-parallel scatter and connect (the CPU baseline's
+    multi-core run) give the sequential results bit for bit: output cells,
+    excitation cells, special faces with sources and outputs, PML, materials
+    and far-field faces spread over planes that different threads take."""
+    sys_path = os.path.join(os.path.dirname(__file__))
+    import sys
+
+    sys.path.insert(0, sys_path)
+    import test_inp as T
+
+    tabs = [build_tables(cases.pml_spheres(n=20, pml=4, n_spheres=3, steps=40, n_probes=4, n_freq=2, dft_size=6,
+                                           rmin=2.0, rmax=3.0)),
+            build_tables(cases.debye_slabs(nx=18, ny=16, nz=22, pml=4, n_slabs=2, thickness=2, steps=40)),
+            build_tables(T.small(base=T.ALL_OUTPUTS).spec)]
+    for t in tabs:
+        a, b = _run_all(t, 1), _run_all(t, threads)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
