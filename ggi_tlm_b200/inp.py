@@ -33,10 +33,13 @@ import re
 from dataclasses import dataclass, field
 from typing import Callable, Dict, List, Optional, Sequence, Tuple
 
-from .problem import (C0, MAT_PEC, MAT_PMC, SOURCE_HARD, SOURCE_SOFT, Block, DFTSurface, ExcitationFunction,
+import numpy as np
+
+from .meshfile import MeshFile, check_cells, connect_faces, pml_cells_from_mesh, read_mesh
+from .problem import (C0, MAT_PEC, MAT_PMC, SOURCE_HARD, SOURCE_SOFT, Block, CellList, DFTSurface, ExcitationFunction,
                       FarFieldSurface, FrequencyOutputVolume, HuygensBox, HuygensOuter, HuygensPlane, OutputPoint,
                       OutputSurface, OutputVolume, PointExcitation, PowerSurface, ProblemSpec, RCSSurface, SARVolume,
-                      SurfaceSheet, UnsupportedFeature, VolumeMaterial, Z0, nint)
+                      SurfaceSheet, UnsupportedFeature, VolumeMaterial, Z0, _region_mask, nint)
 
 GEOMETRY_PACKETS = ["periodic_boundary", "mesh_outer_boundary_dimension", "mesh_dimensions_in_cells",
                     "mesh_cell_dimension", "volume_list", "surface_list", "line_list", "point_list", "pml",
@@ -415,11 +418,20 @@ def _samples(lines: Sequence[str], n_ignore: int, n_time: int, n_value: int) -> 
 
 
 def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
-             open_file: Optional[Callable[[str], Sequence[str]]] = None) -> InpProblem:
+             open_file: Optional[Callable[[str], Sequence[str]]] = None,
+             mesh_file: Optional[MeshFile] = None) -> InpProblem:
     """The ProblemSpec of a .inp file's lines; ``material(name)`` returns the
     volume material of a dispersive Volume_material_list entry, ``name``
     being the file name line as written (the reference opens name + '.vmat');
-    ``open_file(name)`` returns the lines of an excitation function's data file."""
+    ``open_file(name)`` returns the lines of an excitation function's data file.
+
+    ``mesh_file`` is the problem's NAME.mesh as the reference's mesher wrote
+    it (``meshfile.read_mesh``).  With it the geometry is the mesher's, as
+    the reference's solver takes it (MESH/read_mesh.F90): every volume is
+    its cell list (any shape or rotation), the surface materials sit on
+    their surfaces' face lists, the points on the mesh file's cells, and the
+    PML volumes are checked against the PML packet.  Without it the reader
+    voxelises the axis-aligned geometry itself."""
     packets = split_packets(lines)
     rec: Dict[str, Records] = {}
     for name, data in packets:
@@ -447,6 +459,11 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
         n = tuple(nint(e / dl) for e in ext)
     else:
         raise ValueError("neither Mesh_cell_dimension nor Mesh_dimensions_in_cells is given")
+    if mesh_file is not None:  # the solver takes the mesh file's cell size and counts
+        if tuple(mesh_file.n) != tuple(n) or abs(mesh_file.dl - dl) > 1e-9 * dl:
+            raise ValueError(f"the mesh file's {mesh_file.n} cells of {mesh_file.dl} m do not match the problem "
+                             f"file's {n} cells of {dl} m")
+        dl = mesh_file.dl
     mesh = Mesh(xmin, ymin, zmin, dl, n)
     reduced_c = rec["reduced_c_factor"].values(1)[0] if "reduced_c_factor" in rec else 1.0
     if "bicubic_warp_flag" in rec and _logical(rec["bicubic_warp_flag"].line().split()[0]):
@@ -482,6 +499,9 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
         spec.pml_cells = tuple(nint(v / dl) for v in t)  # TLM_PML_volume_materials.F90:465
         spec.pml_r = tuple(rr)
         spec.pml_order = r.ints(1)[0]
+    if mesh_file is not None and mesh_file.has_pml_section:
+        if pml_cells_from_mesh(mesh_file) != tuple(spec.pml_cells):
+            raise ValueError("the mesh file's PML volumes do not match the PML packet")
     # geometry, GEOMETRY/build_*.F90 with a translation only
     points: Dict[int, Tuple[float, float, float]] = {}
     if "point_list" in rec:
@@ -492,19 +512,46 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
             p = r.values(3)
             tr = _transform(r, f"point {k}")
             points[k] = (p[0] + tr[0], p[1] + tr[1], p[2] + tr[2])
+    def point_cell(pt: int) -> Tuple[int, int, int]:
+        """The cell of a point: the mesh file's (problem_points(n)%cell), else get_cell_number."""
+        if mesh_file is not None:
+            if not 1 <= pt <= len(mesh_file.points):
+                raise ValueError(f"point {pt} is not in the mesh file")
+            return tuple(mesh_file.points[pt - 1].cell)
+        return mesh.cell_of(points[pt])
+
     volumes = _geometry_list(rec["volume_list"], "volume", _VOLUME_PARAMS,
                              {"rectangular_block", "rectangular_block2"}) if "volume_list" in rec else {}
     surfaces = _geometry_list(rec["surface_list"], "surface", _SURFACE_PARAMS,
                               {"rectangular_block", "rectangular_block2", "rectangle", "xplane", "yplane",
                                "zplane"}) if "surface_list" in rec else {}
 
-    def volume_block(v: int, what: str) -> Block:
+    def volume_block(v: int, what: str):
+        if mesh_file is not None:  # the mesher's cells, whatever the volume's shape
+            if not 1 <= v <= len(mesh_file.volumes):
+                raise ValueError(f"{what}: volume {v} is not in the mesh file")
+            cells = mesh_file.volumes[v - 1]
+            check_cells(mesh_file, cells, f"volume {v}")
+            return CellList(cells[:, :3])
         s = volumes[v]
         if s.rotated:
             raise UnsupportedFeature(f"{what} on a rotated {s.kind}: only zero Euler angles are supported")
         if s.par is None:
             raise UnsupportedFeature(f"{what} on a volume of type {s.kind!r}")
         return _block_cells(mesh, s.par, s.tr, s.kind)
+
+    def surface_geo(surf: int, what: str, side: int) -> Tuple[dict, int]:
+        """box=, plane= or (with a mesh file) records= of a surface, and the
+        side in the spec's convention: the packet's side times the plane's
+        orientation, or the packet's side for the mesh file's own faces."""
+        if mesh_file is not None:
+            if not 1 <= surf <= len(mesh_file.surfaces):
+                raise ValueError(f"{what}: surface {surf} is not in the mesh file")
+            f = mesh_file.surfaces[surf - 1].faces
+            if f.size and (f[:, 3].min() < 1 or f[:, 3].max() > 6):
+                raise ValueError(f"{what}: surface {surf} lists a face code outside 1..6")
+            return dict(records=[((int(i), int(j), int(k)), int(c)) for i, j, k, c in f.tolist()]), side
+        return _surface_geo(mesh, surfaces[surf], what, side)
 
     # volume materials, read_volume_material_list.F90:90-180
     if "volume_material_list" in rec:
@@ -554,7 +601,7 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
             kind = r.text()
             if kind not in ("soft", "hard"):
                 raise ValueError(f"Excitation_point_list packet: source type {kind!r}")
-            spec.point_excitations.append(PointExcitation(mesh.cell_of(points[pt]), comp, fn,
+            spec.point_excitations.append(PointExcitation(point_cell(pt), comp, fn,
                                                           SOURCE_SOFT if kind == "soft" else SOURCE_HARD, face=face))
     # the Huygens surface, read_huygens_surface.F90:89-200
     if "huygens_surface" in rec:
@@ -591,7 +638,7 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
                 raise ValueError("Output_point_list packet: points must be numbered in order")
             pt = r.ints(1)[0]
             comp = _component(r, _FIELD)
-            spec.outputs.append(OutputPoint(mesh.cell_of(points[pt]), comp, _face(r)))
+            spec.outputs.append(OutputPoint(point_cell(pt), comp, _face(r)))
             timing.append(_timing(r, dt))
     # output surfaces, read_output_surface_list.F90:88-135: side 1, -1, or 0
     # (J from both sides, on the faces of side -1)
@@ -606,9 +653,7 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
             comp = _component(r, _SURFACE_FIELD, width=2)
             if side == 0 and comp not in ("Jx", "Jy", "Jz", "Jm"):
                 raise ValueError("Output_surface_list packet: output on both sides is for Jx, Jy, Jz, Jmagnitude")
-            kind, g, orient = _surface_cells(mesh, surfaces[surf], "an output surface")
-            eff = (-1 if side == 0 else side) * orient
-            geo = dict(box=g) if kind == "box" else dict(plane=g)
+            geo, eff = surface_geo(surf, "an output surface", -1 if side == 0 else side)
             spec.output_surfaces.append(OutputSurface(comp, side=eff, both_sides=side == 0,
                                                       **geo, **_steps(_timing(r, dt))))
     # output volumes, read_output_volume_list.F90:85-105
@@ -621,9 +666,9 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
             comp = _component(r, _FIELD)
             spec.output_volumes.append(OutputVolume(volume_block(v, "an output volume"), comp, "field",
                                                     **_steps(_timing(r, dt))))
-    _read_outputs(rec, mesh, dt, spec, volumes, surfaces, volume_block, post := {})
+    _read_outputs(rec, mesh, dt, spec, surface_geo, volume_block, post := {})
     if "surface_material_list" in rec:
-        _read_surface_materials(rec["surface_material_list"], mesh, spec, surfaces)
+        _read_surface_materials(rec["surface_material_list"], mesh, spec, surfaces, mesh_file)
     if "set_small_to_zero" in rec:  # read_small_to_zero.F90:55-59
         r = rec["set_small_to_zero"]
         spec.small_to_zero = (r.ints(1)[0], r.values(1)[0])
@@ -652,8 +697,9 @@ def _numbered(r: Records, what: str):
         yield k
 
 
-def _read_outputs(rec: Dict[str, Records], mesh: Mesh, dt: float, spec: ProblemSpec, volumes: Dict[int, Shape],
-                  surfaces: Dict[int, Shape], volume_block: Callable[[int, str], Block], post: dict) -> None:
+def _read_outputs(rec: Dict[str, Records], mesh: Mesh, dt: float, spec: ProblemSpec,
+                  surface_geo: Callable[[int, str, int], Tuple[dict, int]], volume_block: Callable[[int, str], object],
+                  post: dict) -> None:
     """The volume and surface output packets other than Output_volume_list
     and Output_surface_list, each entry becoming one spec entry (one
     frequency per entry, as the reference stores them)."""
@@ -689,15 +735,19 @@ def _read_outputs(rec: Dict[str, Records], mesh: Mesh, dt: float, spec: ProblemS
             surf, side = r.ints(1)[0], _side(r)
             freq = r.values(1)[0]
             comp = _component(r, _FIELD_OR_CURRENT, width=2)
-            geo, eff = _surface_geo(mesh, surfaces[surf], "a frequency output surface", side)
+            geo, eff = surface_geo(surf, "a frequency output surface", side)
             t = _timing(r, dt)
-            if "plane" not in geo or eff != 1:
-                raise UnsupportedFeature("frequency output surface: only planar patches sampled on side 1 "
-                                         "of the rectangle orientation")
+            if "box" in geo:
+                raise UnsupportedFeature("frequency output surface on a closed box: planar patches or a mesh "
+                                         "file's faces only")
             if t is not None and (t[0] > 1 or t[1] < spec.n_timesteps or t[2] != 1):
                 raise UnsupportedFeature("frequency output surface with output timing: every step only")
-            ax, ix, r0, r1 = geo["plane"]
-            spec.dft_surfaces.append(DFTSurface(ax, ix, r0, r1, [freq], comp))
+            if "plane" in geo:
+                ax, ix, r0, r1 = geo["plane"]
+                spec.dft_surfaces.append(DFTSurface(ax, ix, r0, r1, [freq], comp, side=eff))
+            else:
+                spec.dft_surfaces.append(DFTSurface(0, 0, (0, 0), (0, 0), [freq], comp, side=eff,
+                                                    records=geo["records"]))
     if "far_field_surface_list" in rec:  # read_far_field_surface.F90:79-165
         r = rec["far_field_surface_list"]
         post["far_field"] = []
@@ -711,7 +761,7 @@ def _read_outputs(rec: Dict[str, Records], mesh: Mesh, dt: float, spec: ProblemS
                 if r.text() != "z":
                     raise ValueError("far_field_surface_list packet: a 2D transform about z only")
                 dim, theta = 2, (90.0, 90.0, 180.0 / 3.141592653589793)  # theta pi/2 with a 1 rad step
-            geo, eff = _surface_geo(mesh, surfaces[surf], "a far-field surface", side)
+            geo, eff = surface_geo(surf, "a far-field surface", side)
             spec.far_field_surfaces.append(FarFieldSurface([freq], side=eff, **geo))
             post["far_field"].append(dict(frequency=freq, theta=theta, phi=phi, dim=dim))
     if "rcs_surface" in rec:  # read_rcs_surface.F90:63-85
@@ -719,7 +769,7 @@ def _read_outputs(rec: Dict[str, Records], mesh: Mesh, dt: float, spec: ProblemS
         surf, side = r.ints(1)[0], _side(r)
         post["rcs"] = tuple(r.values(3))  # fmin, fmax, fstep
         theta, phi = r.values(1)[0], r.values(1)[0]
-        geo, eff = _surface_geo(mesh, surfaces[surf], "an RCS surface", side)
+        geo, eff = surface_geo(surf, "an RCS surface", side)
         spec.rcs_surface = RCSSurface(theta, phi, side=eff, **geo)
     if "frequency_domain_power_surface_list" in rec:  # read_frequency_domain_power_surface.F90:63-105
         r = rec["frequency_domain_power_surface_list"]
@@ -734,7 +784,7 @@ def _read_outputs(rec: Dict[str, Records], mesh: Mesh, dt: float, spec: ProblemS
             n_first = nf
             fstep = (fmax - fmin) / float(nf - 1) if nf != 1 else 0.0
             freqs = [fmin + (k - 1) * fstep for k in range(1, nf + 1)]  # frequency_domain_power_surfaces.F90:328
-            geo, eff = _surface_geo(mesh, surfaces[surf], "a power surface", side)
+            geo, eff = surface_geo(surf, "a power surface", side)
             spec.power_surfaces.append(PowerSurface(freqs, side=eff, **geo))
     if "sar_volume_list" in rec:  # read_SAR_volume_list.F90:69-90: material number, frequency, density
         r = rec["sar_volume_list"]
@@ -746,25 +796,28 @@ def _read_outputs(rec: Dict[str, Records], mesh: Mesh, dt: float, spec: ProblemS
             post["sar_density"].append(rho)
 
 
-def _material_block(spec: ProblemSpec, m: int) -> Block:
+def _material_block(spec: ProblemSpec, m: int):
     """The cells of volume material ``m`` (SAR_volumes.F90:62-95 takes every
-    cell whose material is m) when they form one block that no other
-    material overlaps."""
+    cell whose material is m) when they form one region (a block, or a mesh
+    file's cell list) that no other material overlaps."""
     own = [b for k, b in spec.material_regions if k == m]
     if len(own) != 1:
         raise UnsupportedFeature("a SAR volume on a material of several volumes")
     b = own[0]
+    mine = _region_mask(spec, b)
     for k, o in spec.material_regions:
-        if k != m and not (o.i1 < b.i0 or o.i0 > b.i1 or o.j1 < b.j0 or o.j0 > b.j1 or o.k1 < b.k0 or o.k0 > b.k1):
+        if k != m and np.any(mine & _region_mask(spec, o)):
             raise UnsupportedFeature("a SAR volume on a material that another material overlaps")
     return b
 
 
-def _read_surface_materials(r: Records, mesh: Mesh, spec: ProblemSpec, surfaces: Dict[int, Shape]) -> None:
+def _read_surface_materials(r: Records, mesh: Mesh, spec: ProblemSpec, surfaces: Dict[int, Shape],
+                            mesh_file: Optional[MeshFile] = None) -> None:
     """read_surface_material_list.F90:111-470 for PEC, PMC and free-space
     surfaces: number, type, the number of surfaces, their numbers and their
     orientations (which a symmetric sheet does not use).  A box surface
-    becomes its six boundary planes."""
+    becomes its six boundary planes; with a mesh file every surface is its
+    face list, whatever its shape."""
     names = {"pec": "PEC", "pmc": "PMC", "free_space": "free"}
     for _ in _numbered(r, "surface materials"):
         kind = r.text()
@@ -774,6 +827,12 @@ def _read_surface_materials(r: Records, mesh: Mesh, spec: ProblemSpec, surfaces:
         nums = r.ints(n)
         r.ints(n)  # orientations
         for num in nums:
+            if mesh_file is not None:
+                if not 1 <= num <= len(mesh_file.surfaces):
+                    raise ValueError(f"surface {num} is not in the mesh file")
+                faces = connect_faces(mesh_file, mesh_file.surfaces[num - 1].faces, f"surface {num}")
+                spec.surface_sheets.append(SurfaceSheet(names[kind], 0, 0, (0, 0), (0, 0), faces=faces))
+                continue
             geo, _ = _surface_geo(mesh, surfaces[num], "a surface material", 1)
             if "plane" in geo:
                 ax, ix, r0, r1 = geo["plane"]
@@ -794,7 +853,8 @@ OUTPUT_PACKETS = {"output_point_list", "output_surface_list", "output_volume_lis
 
 
 def read_inp_lenient(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
-                     open_file: Optional[Callable[[str], Sequence[str]]] = None) -> InpProblem:
+                     open_file: Optional[Callable[[str], Sequence[str]]] = None,
+                     mesh_file: Optional[MeshFile] = None) -> InpProblem:
     """read_inp, leaving out each output packet that read_inp refuses (a
     result the GPU path cannot produce exactly, such as an output surface on
     rotated geometry) and listing it in ``skipped`` as "<packet>: <reason>".
@@ -813,11 +873,11 @@ def read_inp_lenient(lines: Sequence[str], material: Callable[[str], VolumeMater
     dropped = []
     for name in [n for n, _ in packets if n in OUTPUT_PACKETS]:
         try:
-            read_inp(text(core | {name}), material, open_file)
+            read_inp(text(core | {name}), material, open_file, mesh_file)
         except UnsupportedFeature as e:
             dropped.append(f"{name}: {e}")
     keep = core | {n for n, _ in packets if n in OUTPUT_PACKETS and not any(d.startswith(n + ":") for d in dropped)}
-    p = read_inp(text(keep), material, open_file)
+    p = read_inp(text(keep), material, open_file, mesh_file)
     p.skipped.extend(dropped)
     return p
 
@@ -830,17 +890,25 @@ def vmat_in(directory: str) -> Callable[[str], VolumeMaterial]:
 
 
 def read_inp_file(path: str, material: Optional[Callable[[str], VolumeMaterial]] = None,
-                  lenient: bool = False) -> InpProblem:
+                  lenient: bool = False, mesh: Optional[bool] = None) -> InpProblem:
     """read_inp (read_inp_lenient with ``lenient``) of a file; material and
     data file names resolve against the file's directory unless ``material``
     is given.  The text is read as Latin-1: the reference's inputs hold stray
-    non-ASCII bytes in remarks."""
+    non-ASCII bytes in remarks.  The mesh file NAME.mesh beside NAME.inp,
+    when there is one (or when ``mesh`` is True), gives the geometry, as it
+    does to the reference's solver; ``mesh=False`` voxelises the .inp
+    geometry instead."""
     directory = os.path.dirname(os.path.abspath(path))
     with open(path, encoding="latin-1") as f:
         lines = f.read().splitlines()
+    mesh_path = os.path.splitext(path)[0] + ".mesh"
+    mesh_file = None
+    if mesh or (mesh is None and os.path.exists(mesh_path)):
+        with open(mesh_path, encoding="latin-1") as f:
+            mesh_file = read_mesh(f.read().splitlines())
 
     def open_file(name: str) -> List[str]:
         with open(os.path.join(directory, name), encoding="latin-1") as g:
             return g.read().splitlines()
 
-    return (read_inp_lenient if lenient else read_inp)(lines, material or vmat_in(directory), open_file)
+    return (read_inp_lenient if lenient else read_inp)(lines, material or vmat_in(directory), open_file, mesh_file)

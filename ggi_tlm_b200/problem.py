@@ -408,6 +408,18 @@ class Block:
 
 
 @dataclass
+class CellList:
+    """An explicit set of cells (1-based i, j, k rows): a volume as the
+    reference's mesher voxelised it, read from a mesh file's cell list
+    (MESH/read_mesh.F90:112-160)."""
+
+    cells: np.ndarray
+
+    def __post_init__(self):
+        self.cells = np.asarray(self.cells, dtype=np.int64).reshape(-1, 3)
+
+
+@dataclass
 class Sphere:
     """Cells whose centres lie inside a sphere (centre and radius in cells,
     cell centres at integer+0.5 in 0-based cell coordinates)."""
@@ -512,10 +524,15 @@ class FarFieldSurface:
     box: Optional[Tuple[Tuple[int, int], Tuple[int, int], Tuple[int, int]]] = None
     plane: Optional[Tuple[int, int, Tuple[int, int], Tuple[int, int]]] = None
     side: int = 1
+    # or the surface's faces as a mesh file lists them: (cell, face code) per
+    # face before the side flip (MESH/read_mesh.F90:186-225)
+    records: Optional[List[Tuple[Tuple[int, int, int], int]]] = None
 
     def faces(self) -> List[Tuple[Tuple[int, int, int], int]]:
-        if (self.box is None) == (self.plane is None):
-            raise ValueError("a far-field surface is either a box or a plane")
+        if sum(g is not None for g in (self.box, self.plane, self.records)) != 1:
+            raise ValueError("a far-field surface is a box, a plane or a list of mesh faces")
+        if self.records is not None:
+            return _side_flip(self.records, self.side)
         if self.box is not None:
             g = HuygensBox(self.box[0], self.box[1], self.box[2], 0, 0.0, 0.0, 1.0, 0.0, side=self.side)
         else:
@@ -549,11 +566,10 @@ class OutputSurface:
     first_step: int = 1
     last_step: Optional[int] = None
     interval: int = 1
+    records: Optional[List[Tuple[Tuple[int, int, int], int]]] = None  # mesh faces, as for FarFieldSurface
 
     def faces(self) -> List[Tuple[Tuple[int, int, int], int]]:
-        if (self.box is None) == (self.plane is None):
-            raise ValueError("an output surface is either a box or a plane")
-        return FarFieldSurface([], self.box, self.plane, self.side).faces()
+        return FarFieldSurface([], self.box, self.plane, self.side, self.records).faces()
 
 
 @dataclass
@@ -568,11 +584,10 @@ class RCSSurface:
     box: Optional[Tuple[Tuple[int, int], Tuple[int, int], Tuple[int, int]]] = None
     plane: Optional[Tuple[int, int, Tuple[int, int], Tuple[int, int]]] = None
     side: int = 1
+    records: Optional[List[Tuple[Tuple[int, int, int], int]]] = None  # mesh faces, as for FarFieldSurface
 
     def faces(self) -> List[Tuple[Tuple[int, int, int], int]]:
-        if (self.box is None) == (self.plane is None):
-            raise ValueError("an RCS surface is either a box or a plane")
-        return FarFieldSurface([], self.box, self.plane, self.side).faces()
+        return FarFieldSurface([], self.box, self.plane, self.side, self.records).faces()
 
 
 RCS_POINTS_PER_CELL = 2  # n_rcs_points_per_cell, TLM_MODULES/TLM_output_modules.F90:388
@@ -595,6 +610,15 @@ class SurfaceSheet:
     index: int
     r0: Tuple[int, int]
     r1: Tuple[int, int]
+    # explicit faces instead of the patch: ((cx, cy, cz) of the cell on the
+    # + side, axis) per face, e.g. a triangulated surface as the reference's
+    # mesher put it on cell faces (read from a mesh file)
+    faces: Optional[List[Tuple[Tuple[int, int, int], int]]] = None
+
+    def face_keys(self):
+        if self.faces is not None:
+            return list(self.faces)
+        return [(f, self.axis) for f in _plane_faces(self.axis, self.index, self.r0, self.r1)]
 
 
 @dataclass
@@ -608,11 +632,10 @@ class PowerSurface:
     box: Optional[Tuple[Tuple[int, int], Tuple[int, int], Tuple[int, int]]] = None
     plane: Optional[Tuple[int, int, Tuple[int, int], Tuple[int, int]]] = None
     side: int = 1
+    records: Optional[List[Tuple[Tuple[int, int, int], int]]] = None  # mesh faces, as for FarFieldSurface
 
     def faces(self) -> List[Tuple[Tuple[int, int, int], int]]:
-        if (self.box is None) == (self.plane is None):
-            raise ValueError("a power surface is either a box or a plane")
-        return FarFieldSurface([], self.box, self.plane, self.side).faces()
+        return FarFieldSurface([], self.box, self.plane, self.side, self.records).faces()
 
 
 @dataclass
@@ -640,7 +663,9 @@ class OutputPoint:
 @dataclass
 class DFTSurface:
     """Frequency-domain output surface: a planar face patch (same convention
-    as HuygensPlane) and a list of frequencies for one field component."""
+    as HuygensPlane) and a list of frequencies for one field component.
+    ``records`` (a mesh file's faces, as for FarFieldSurface) replace the
+    patch; ``side`` -1 samples the other side of each face."""
 
     axis: int
     index: int
@@ -648,6 +673,14 @@ class DFTSurface:
     r1: Tuple[int, int]
     frequencies: Sequence[float]
     component: str
+    side: int = 1
+    records: Optional[List[Tuple[Tuple[int, int, int], int]]] = None
+
+    def faces(self) -> List[Tuple[Tuple[int, int, int], int]]:
+        if self.records is not None:
+            return _side_flip(self.records, self.side)
+        return _side_flip([(c, self.axis) for c in _plane_faces(self.axis, self.index, self.r0, self.r1)],
+                          self.side)
 
 
 @dataclass
@@ -766,6 +799,12 @@ def _region_mask(spec: ProblemSpec, region) -> np.ndarray:
                               np.arange(lo[2], hi[2]) + 0.5, indexing="ij")
         m[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = (
             (x - region.cx) ** 2 + (y - region.cy) ** 2 + (z - region.cz) ** 2 <= region.r ** 2)
+    elif isinstance(region, CellList):
+        c = region.cells
+        if c.size:
+            if (c.min(axis=0) < 1).any() or (c.max(axis=0) > (spec.nx, spec.ny, spec.nz)).any():
+                raise ValueError("a cell list reaches outside the mesh")
+            m[c[:, 2] - 1, c[:, 1] - 1, c[:, 0] - 1] = True
     else:
         raise TypeError(region)
     return m
@@ -881,15 +920,23 @@ def _huygens_patches(hs) -> List[Tuple[Tuple[int, int, int], int]]:
                 for cy in rng[1]:
                     for cx in rng[0]:
                         rec.append(((cx, cy, cz), code))
+    return _side_flip(rec, hs.side)
+
+
+def _side_flip(rec, side: int) -> List[Tuple[Tuple[int, int, int], int]]:
+    """(cell, face code) records as they are, for side 1, or each moved to
+    the same face seen from the neighbouring cell, for side -1
+    (huygens_surface.F90:412-450 and the output surfaces' side flag)."""
     out = []
     for c, code in rec:
-        if hs.side != 1:  # excitation on the other side of the face
+        c = tuple(int(v) for v in c)
+        if side != 1:
             axis = (code - 1) % 3
             c = list(c)
             c[axis] += -1 if code <= 3 else 1
             code = code + 3 if code <= 3 else code - 3
             c = tuple(c)
-        out.append((c, code))
+        out.append((c, int(code)))
     return out
 
 
@@ -1123,15 +1170,16 @@ def build_tables(spec: ProblemSpec) -> dict:
     rcs_faces = spec.rcs_surface.faces() if spec.rcs_surface is not None else []
     for c, code in rcs_faces:
         face_out[connect_key(c, code)] = True
-    for ds in spec.dft_surfaces:
-        for f in _plane_faces(ds.axis, ds.index, ds.r0, ds.r1):
-            face_out[(f, ds.axis)] = True
+    dft_faces = [ds.faces() for ds in spec.dft_surfaces]
+    for fl in dft_faces:
+        for c, code in fl:
+            face_out[connect_key(c, code)] = True
     face_mat = {}
     for sh in spec.surface_sheets:
         if sh.kind not in SURFACE_SHEET_TYPES:
             raise UnsupportedFeature(f"surface material {sh.kind!r}: only PEC, PMC and free-space sheets")
-        for f in _plane_faces(sh.axis, sh.index, sh.r0, sh.r1):
-            face_mat[(f, sh.axis)] = SURFACE_SHEET_TYPES[sh.kind]
+        for key in sh.face_keys():
+            face_mat[key] = SURFACE_SHEET_TYPES[sh.kind]
     keys = set(face_exc) | set(face_out) | set(face_mat)
     for (c, axis) in keys:
         if c[axis - 1] <= 1 or c[axis - 1] > (nx, ny, nz)[axis - 1]:
@@ -1302,15 +1350,13 @@ def build_tables(spec: ProblemSpec) -> dict:
 
     # DFT surfaces: one reference surface entry per frequency
     freqs, comps, ptr, fo, fs = [], [], [0], [], []
-    for ds in spec.dft_surfaces:
-        faces = _plane_faces(ds.axis, ds.index, ds.r0, ds.r1)
-        side_code = ds.axis  # min face of the + cell: face_xmin/ymin/zmin = 1/2/3
+    for ds, faces in zip(spec.dft_surfaces, dft_faces):
         for fr in ds.frequencies:
             freqs.append(fr)
             comps.append(COMPONENTS[ds.component])
-            for f in faces:
-                fo.append(fout_num[(f, ds.axis)])
-                fs.append(side_code)
+            for c, code in faces:  # the face code says which side's field the entry reads
+                fo.append(fout_num[connect_key(c, code)])
+                fs.append(code)
             ptr.append(len(fo))
     tables.update(n_dft=len(freqs), dft_freq=np.array(freqs, dtype=np.float64),
                   dft_comp=np.array(comps, dtype=np.int32), dft_face_ptr=np.array(ptr, dtype=np.int32),

@@ -31,7 +31,7 @@ CASES = {
 # raw text of the reference's .tout files (header and every data line), kept
 # to check that the library's .tout writer reproduces them byte for byte
 TEXT_CASES = ["tem_pml_Ey", "material_test2_Ex", "huygens_box_Hz"]
-VMAT_CASES = ["debye_1", "debye_2", "FR4_at_7GHz", "mur_lorentz", "epsr=2", "mur=2"]
+VMAT_CASES = ["debye_1", "debye_2", "FR4_at_7GHz", "mur_lorentz", "epsr=2", "mur=2", "epsr=1.5"]
 # the known-answer cases' problem input files, as text, for the .inp reader;
 # read as Latin-1 since their remarks hold stray non-ASCII bytes
 INP_CASES = {
@@ -47,6 +47,11 @@ INP_CASES = {
     "box_slot": "SHIELDING_EFFECTIVENESS_BOX_SLOT/PROBLEM_SPECIFICATION_FILES/box_slot.inp",
     "excitation_test": "EXCITATION_FUNCTION_TEST/PROBLEM_SPECIFICATION_FILES/excitation_test.inp",
     "power_calc": "POWER_CALCS/PROBLEM_SPECIFICATION_FILES/power_calc.inp",
+    "helix": "HELIX_ANTENNA/helix.inp",
+}
+# mesh files written by the reference's mesher (MESH/write_mesh.F90), as text
+MESH_CASES = {
+    "helix": "HELIX_ANTENNA/helix.mesh",
 }
 # data files the inputs name (excitation function samples), as text
 DATA_CASES = {
@@ -109,6 +114,12 @@ def main():
             fo[name] = np.array(f.read().splitlines())
     np.savez_compressed(os.path.join(here, "fout_text.npz"), **fo)
     print("fout_text", {k: len(v) for k, v in fo.items()})
+    me = {}
+    for name, rel in MESH_CASES.items():
+        with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", rel)) as f:
+            me[name] = np.array(f.read().splitlines())
+    np.savez_compressed(os.path.join(here, "mesh_text.npz"), **me)
+    print("mesh_text", {k: len(v) for k, v in me.items()})
 
 
 if __name__ == "__main__":
