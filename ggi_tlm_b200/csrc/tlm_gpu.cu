@@ -2270,7 +2270,11 @@ int tlm_gpu_fetch_links_noalloc(int64_t h, double *out) {
   if (!m) return fail(TLM_E_BADARG, "bad handle");
   if (!out) return fail(TLM_E_BADARG, "null output");
   if (!m->finalized)
-    return fail(TLM_E_STATE, "the mesh has no device state yet: call tlm_gpu_run at least once first");
+    return fail(TLM_E_STATE,
+                "the mesh has no device state yet: call tlm_gpu_prepare, tlm_gpu_run or tlm_gpu_batch_create first");
+  // a mesh inside a batch is advanced on the batch's stream: wait for it, as
+  // every other read-back does, so the gather sees the finished steps
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
   const long long n = (long long)m->desc.nx * m->desc.ny * m->desc.nz;
   if ((size_t)n * 12 > kNoAllocScratchDoubles)
     return fail(TLM_E_BADARG, "mesh of %lld cells exceeds the allocation-free read-back limit of %zu cells", n,

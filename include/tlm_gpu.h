@@ -355,7 +355,9 @@ int tlm_gpu_fetch_links(int64_t handle, double *out);
    device that loads the library, kept until the process exits), so the mesh
    may have at most 87381 cells (nx*ny*nz*12 <= 2^20 doubles); larger meshes
    are rejected with TLM_E_BADARG.  The mesh must already have device state
-   (at least one tlm_gpu_run).  The first call on a device looks up the
+   (built by tlm_gpu_prepare, tlm_gpu_run or tlm_gpu_batch_create; before
+   any run it returns the initial, all-zero links).  A mesh that belongs to
+   a batch is read after the batch's queued steps finish.  The first call on a device looks up the
    scratch address (cudaGetSymbolAddress) and should come before any stream
    capture.  All calls share the one scratch array, which keeps the last
    call's contents: calls that overlap on the GPU (other host threads, other

@@ -48,6 +48,32 @@ def test_noalloc_fetch_matches_allocating_fetch(gpu_lib, precision):
         assert np.max(np.abs(got - ref)) <= TOL * max(scale, np.max(np.abs(ref)))
 
 
+def test_noalloc_fetch_of_a_batched_mesh_waits_for_the_batch(gpu_lib):
+    """A mesh inside a batch is advanced on the batch's stream, and
+    tlm_gpu_batch_run returns before its steps finish: the read-back must
+    still see the finished steps, twice in a row, as the allocating
+    read-back does."""
+    specs = cases.batch_boxes(n_boxes=2, edge=(18, 26), steps=(60, 80), pml=3, max_spheres=2, seed=5)
+    tabs = [build_tables(s) for s in specs]
+    meshes = [capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64) for t in tabs]
+    try:
+        with capi.GpuBatch(meshes) as b:
+            b.run(23, sync=False)  # no batch_synchronize before the read-back
+            got = [fetch(capi._lib, g.h, "tlm_gpu_fetch_links_noalloc", (t["nz"], t["ny"], t["nx"], 12))
+                   for g, t in zip(meshes, tabs)]
+            again = fetch(capi._lib, meshes[0].h, "tlm_gpu_fetch_links_noalloc",
+                          (tabs[0]["nz"], tabs[0]["ny"], tabs[0]["nx"], 12))
+            b.synchronize()
+            ref = [g.links() for g in meshes]
+        for a, r in zip(got + [again], ref + [ref[0]]):
+            scale = np.max(np.abs(r))
+            assert scale > 0
+            assert np.max(np.abs(a - r)) <= TOL * scale
+    finally:
+        for g in meshes:
+            g.close()
+
+
 def test_noalloc_fetch_rejects_oversized_mesh(gpu_lib):
     t = build_tables(cases.pec_box(n=45, steps=3))  # 91125 cells > 87381
     with capi.GpuMesh(t) as g:
