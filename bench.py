@@ -1,18 +1,28 @@
 #!/usr/bin/env python
 """Benchmark of the B200 SCN-TLM time-stepping core.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2|t512|c3|c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload t512|c2|c3|c1]
 
 One "step" is one TLM time step (excitation, scatter, connect, outer boundary,
-face outputs, DFT) over the whole mesh.  Default workload: the 256^3
-PML-bounded box with 32 dielectric spheres, a Huygens plane wave, 16 probes
-and a 64-frequency 64x64-face FP64 DFT (seeded synthetic input), FP32 links.
-The metric is cell-updates per second (whole job, all GPUs), with the fused
-cell kernel's achieved HBM bandwidth against the measured copy peak.
+probes) over the whole mesh.  Default workload: the 512^3 free-space box with
+an 8-cell PML on all six faces, a Gaussian point source and 4 probes (seeded
+synthetic input, 2000 steps).  The headline ``value`` is the plain FP64 path,
+the reference's own precision; the FP32 fast path (FP32 links, FP64 filter,
+PML recursion and DFT) and its probe error over the complete solve are in
+the ``fp32`` key.  The metric is cell-updates per second (whole job, all
+GPUs), with the bulk cell kernel's achieved HBM bandwidth against the
+measured copy peak.  Sections at N=1: the 256^3 PML-spheres mesh (c2), the
+384x384x192 Debye-slab mesh (c3), 96 uneven boxes batched (c4) and the
+serving trace (c5).
 
 Multi-GPU (torchrun, one process per GPU): the path does not shard here
 (replicas only); every rank advances its own copy of the mesh, the timed
 region is bracketed by barriers and the time is the max over ranks.
+
+``--impl reference`` times the reference's CPU path on the host cores: the
+oracle's C restatement of the reference's sequential loop (the Fortran
+builds cannot be compiled on this box), z-planes shared among all host
+threads, on the same tables.
 """
 from __future__ import annotations
 
@@ -41,16 +51,14 @@ FALLBACK_HBM_GBS = 6650.0
 BULK_VARIANTS = [(0, 0, 0, 0), (1024, 2, 512, 2), (512, 3, 256, 3), (512, 4, 256, 4), (1024, 3, 512, 3),
                  (256, 6, 128, 6)]
 
-# DRAM bytes per launch of the bulk kernel (dram__bytes_read.sum +
-# dram__bytes_write.sum) from one ncu --set full capture of the same workload.
+# DRAM traffic of the bulk kernel (dram__bytes_read.sum + dram__bytes_write.sum)
+# per free-space cell it updates, from one ncu capture of the FP64 kernel; the
+# traffic of a launch grows with the cells it updates, so a full launch is
+# this figure times its cells.
 NCU_TRAFFIC = {
-    "pml_spheres_256^3_pml8_32spheres_huygens_dft64x64x64": {
-        "bytes": 755.997440e6 + 609.044480e6,
-        "source": "profiles/tlm_bulk_tma_kernel_pml_spheres_256_fp32.md (tlm_bulk_tma_kernel<float,4,512,3>)"},
-    "debye_slabs_384x384x192_pml10_6slabs_dft64x64x64": {
-        "bytes": None,
-        "source": "no ncu capture of the bulk kernel on this workload; "
-                  "profiles/tlm_special_kernel_debye_slabs_384x384x192_fp32.md covers its largest special kernel"},
+    "pml_point_source_512^3_pml8": {
+        "bytes_per_cell": None,
+        "source": "no ncu capture of the FP64 bulk kernel yet"},
 }
 
 
@@ -213,13 +221,22 @@ def replica_rate(cells: int, steps: int, world: int, local_ms: float) -> tuple:
     return cells * steps * world / (ms / 1e3) / 1e9, ms
 
 
-def cpu_oracle_rate(t, budget_s: float, max_steps: int):
-    """Time the CPU oracle (the C restatement of the reference's loop) on the
-    same tables for a bounded number of steps; returns (Gcell/s, steps, s)."""
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_oracle_rate(t, budget_s: float, max_steps: int, threads: int = 1):
+    """Time the CPU oracle (the C restatement of the reference's loop, its
+    z-planes shared among ``threads`` host threads as the reference's MPI
+    build shares z-slabs among ranks) on the same tables for a bounded number
+    of steps; returns (Gcell/s, steps, s, threads used)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
-    o = oracle.Oracle(t)
+    o = oracle.Oracle(t, threads=threads)
     n = t["nx"] * t["ny"] * t["nz"]
     o.run(1)  # warm-up step (page-in)
     steps, t0 = 0, time.perf_counter()
@@ -229,11 +246,23 @@ def cpu_oracle_rate(t, budget_s: float, max_steps: int):
         if time.perf_counter() - t0 > budget_s:
             break
     el = time.perf_counter() - t0
+    used = o.threads
     o.close()
-    return n * steps / el / 1e9, steps, el
+    return n * steps / el / 1e9, steps, el, used
+
+
+def workload_config(t, wname, world):
+    n, npml, nmat, _ = cell_counts(t)
+    return {"workload": wname, "cells": n, "pml_cells": npml, "material_cells": nmat,
+            "n_timesteps": int(t["n_timesteps"]), "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (126 MB): no flush"}
 
 
 def run_reference_arm(args, world, rank):
+    """The reference's CPU implementation of the path on this box's host
+    cores.  The reference is Fortran and no Fortran compiler exists here, so
+    the oracle (the plain-C restatement of its sequential loop, pinned by the
+    reference's golden vectors) stands in for it, with all host threads."""
     if rank != 0:
         return
     from ggi_tlm_b200.problem import build_tables
@@ -241,61 +270,93 @@ def run_reference_arm(args, world, rank):
     spec, wname = workload_spec(args.workload)
     t = build_tables(spec)
     budget = float(os.environ.get("TLM_REFERENCE_BUDGET_S", "60"))
-    rate, steps, el = cpu_oracle_rate(t, budget, max(args.steps, 1))
-    sample = f"{steps} time steps of the full {t['nx']}x{t['ny']}x{t['nz']} mesh ({el:.1f} s)"
+    W = max(args.warmup, 3)
+    rate, steps, el, used = cpu_oracle_rate(t, budget, max(args.steps, 1), host_threads())
+    sample = (f"{steps} FP64 time steps of the full {t['nx']}x{t['ny']}x{t['nz']} mesh ({el:.1f} s) after 1 "
+              f"untimed step")
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world, "steps": steps,
-        "warmup": 1, "ms_per_step": el / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "warmup": W, "ms_per_step": el / steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": wname, "cells": t["nx"] * t["ny"] * t["nz"]},
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample,
-                         "note": "reference Fortran build unavailable on this box (no Fortran compiler); "
-                                 "single-threaded C restatement of its sequential loop"},
+        "config": workload_config(t, wname, world),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": used, "kind": "port", "sample": sample,
+                         "note": "reference Fortran builds (SEQ, MPI) unavailable on this box (no Fortran "
+                                 "compiler); the oracle's C restatement of the sequential loop, z-planes shared "
+                                 "among host threads (the MPI build's z-slab split)"},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def _timed_steps(g, k):
-    g.set_timing(True)
-    g.run(k)
-    total, bulk = g.last_run_time()
-    g.set_timing(False)
-    return total, bulk
-
-
-def bench_target_512(device, peak):
-    """The roofline target: 512^3 PML-bounded free-space mesh, point source."""
+def timed_solo(t, precision, device, K, W, world, finish=True, sample_clocks=False):
+    """Advance one mesh: autotune on real steps, W warm-up steps, K timed
+    steps (CUDA events on the launch stream, barriers around), then the rest
+    of the solve untimed for the probe accuracy."""
     from ggi_tlm_b200 import autotune, capi
-    from ggi_tlm_b200.problem import build_tables, probe_series
+    from ggi_tlm_b200.problem import probe_series
 
-    t = build_tables(__import__("ggi_tlm_b200.cases", fromlist=["x"]).pml_point_source(512, steps=2000))
+    g = capi.GpuMesh(t, precision=precision, device=device)
+    tv = autotune.tune(g, steps_per_variant=2, use_cache=False)
+    g.run(W)
+    g.set_timing(True)
+    barrier(world)
+    g.synchronize()
+    sampler = ClockSampler(device) if sample_clocks else None
+    if sampler:
+        sampler.start()
+    g.run(K)
+    g.synchronize()
+    clocks = sampler.stop() if sampler else None
+    barrier(world)
+    total, bulk = g.last_run_time()
+    launches = g.last_run_launches()
+    g.set_timing(False)
+    probes = None
+    if finish:
+        g.run(t["n_timesteps"] - g.step)
+        probes = probe_series(t, g.cell_output())
+    mem = g.memory_bytes()
+    g.close()
+    return {"total_ms": total, "bulk_ms": bulk, "launches": launches, "clocks": clocks, "probes": probes,
+            "variant": tv["variant"], "device_bytes": mem}
+
+
+def probe_error(a, b):
+    errs = [float(np.linalg.norm(a[i] - b[i]) / np.linalg.norm(b[i])) for i in range(len(b))
+            if np.linalg.norm(b[i]) > 0]
+    return max(errs) if errs else None
+
+
+def bench_pair(t, device, peak, K=60, W=3):
+    """FP32 and FP64 step rates of one mesh with the FP32 probe error over
+    the complete solve (compact record for the section keys)."""
     n = t["nx"] * t["ny"] * t["nz"]
-    out = {"workload": "pml_point_source_512^3_pml8", "cells": n, "pml_cells": int(t["n_pml_cells"])}
-    probes = {}
-    for prec, esz, key in ((capi.TLM_PRECISION_FP32, 4, "fp32"), (capi.TLM_PRECISION_FP64, 8, "fp64")):
-        g = capi.GpuMesh(t, precision=prec, device=device)
-        tv = autotune.tune(g, steps_per_variant=2, use_cache=False)
-        g.run(3)
-        K = 60
-        total, bulk = _timed_steps(g, K)
-        g.run(t["n_timesteps"] - g.step)  # untimed: the rest of the solve, for the probe accuracy
-        probes[key] = probe_series(t, g.cell_output())
-        g.close()
+    r32 = timed_solo(t, 0, device, K, W, 1)
+    r64 = timed_solo(t, 1, device, K, W, 1)
+    out = {}
+    for key, r, esz in (("fp32", r32, 4), ("fp64", r64, 8)):
         ab = algorithmic_bytes(t, esz)
-        step_gbs = ab["total"] / (total / K / 1e3) / 1e9
-        out[key] = {"gcell_per_s": n * K / (total / 1e3) / 1e9, "ms_per_step": total / K,
-                    "step_achieved_gbs": step_gbs, "step_frac_of_measured_hbm": step_gbs / peak,
-                    "step_frac_of_8tbs": step_gbs / 8000.0,
-                    "bulk_kernel_gbs": ab["bulk"] / (bulk / K / 1e3) / 1e9,
-                    "bulk_kernel_frac_of_measured_hbm": ab["bulk"] / (bulk / K / 1e3) / 1e9 / peak,
-                    "variant": tv["variant"], "timed_steps": K}
-    a, b = probes["fp32"], probes["fp64"]
-    errs = [float(np.linalg.norm(a[i] - b[i]) / np.linalg.norm(b[i])) for i in range(len(b)) if np.linalg.norm(b[i]) > 0]
-    out["probe_rel_l2_fp32_vs_fp64_max"] = max(errs)
-    out["probe_rel_l2_fp32_vs_fp64_median"] = float(np.median(errs))
-    out["probe_steps"] = int(t["n_timesteps"])
+        out[key] = {"gcell_s": round(n * K / (r["total_ms"] / 1e3) / 1e9, 3),
+                    "step_frac": round(ab["total"] / (r["total_ms"] / K / 1e3) / 1e9 / peak, 4),
+                    "bulk_frac": round(ab["bulk"] / (r["bulk_ms"] / K / 1e3) / 1e9 / peak, 4)}
+    out["fp32_probe_err"] = probe_error(r32["probes"], r64["probes"])
+    out["steps"] = int(t["n_timesteps"])
     return out
+
+
+def build_many(specs):
+    """Tables of many problems, built in a pool of host processes (spawned,
+    so no process inherits a CUDA context); table building is host work
+    outside every timed region."""
+    import multiprocessing as mp
+
+    from ggi_tlm_b200.problem import build_tables
+
+    n = max(1, min(len(specs), host_threads(), 32))
+    if n == 1:
+        return [build_tables(s) for s in specs]
+    with mp.get_context("spawn").Pool(n) as pool:
+        return pool.map(build_tables, specs, chunksize=1)
 
 
 def bench_batch(device):
@@ -303,10 +364,8 @@ def bench_batch(device):
     sources, 1500-5000 steps) advanced together, FP32, against the same boxes
     solved one after another."""
     from ggi_tlm_b200 import capi, cases
-    from ggi_tlm_b200.problem import build_tables
 
-    specs = cases.batch_boxes()
-    tabs = [build_tables(s) for s in specs]
+    tabs = build_many(cases.batch_boxes())
     meshes = [capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP32, device=device) for t in tabs]
     b = capi.GpuBatch(meshes)
     # tune the batch kernel configuration on the first real steps
@@ -332,24 +391,24 @@ def bench_batch(device):
             total, _ = g.last_run_time()
             solo_ms += total
             solo_cu += t["nx"] * t["ny"] * t["nz"] * t["n_timesteps"]
-    return {"workload": "96 PML boxes, edges U[24,160], 0-8 spheres, 1500-5000 steps, FP32",
-            "boxes": len(tabs), "cell_updates": cu, "gcell_per_s": cu / (ms / 1e3) / 1e9, "device_ms": ms,
-            "variant": best, "variant_ms_per_step": tune, "kernel_launches": launches,
-            "solo_sequential_gcell_per_s": solo_cu / (solo_ms / 1e3) / 1e9,
-            "speedup_vs_solo_sequential": (cu / ms) / (solo_cu / solo_ms) if solo_ms else None,
-            "note": "first 24 steps of every box ran during variant tuning (same numerics)"}
+    steps = max(t["n_timesteps"] for t in tabs)
+    return {"gcell_s": round(cu / (ms / 1e3) / 1e9, 3), "solo_gcell_s": round(solo_cu / (solo_ms / 1e3) / 1e9, 3),
+            "speedup_vs_solo": round((cu / ms) / (solo_cu / solo_ms), 3) if solo_ms else None,
+            "launches": launches, "launches_per_step": round(launches / max(steps - 24, 1), 2),
+            "boxes": len(tabs), "variant": best,
+            "note": "96 PML boxes, edges U[24,160], 0-8 spheres, 1500-5000 steps, FP32; the first 24 steps of "
+                    "every box ran during variant tuning (same numerics)"}
 
 
-def bench_serving(device, n_requests=32):
+def bench_serving(device, n_requests=256):
     """Config 5: Poisson arrivals (40/s, seeded) of solves with edges
     log-U[32,256], 0-3 Debye slabs, 6-10 cell PML, 1000-8000 steps; FP32
     continuous batching under a 150 GB budget against sequential plain-FP64
     solves of the same trace."""
     from ggi_tlm_b200 import cases, serving
-    from ggi_tlm_b200.problem import build_tables
 
-    specs = cases.serving_requests(n_requests)
-    trace = serving.poisson_trace(specs, rate_per_s=40.0, seed=7, build=build_tables)
+    tabs = build_many(cases.serving_requests(n_requests))
+    trace = serving.poisson_trace(list(range(len(tabs))), rate_per_s=40.0, seed=7, build=lambda i: tabs[i])
     srv = serving.Server(engine=serving.GpuEngine(device=device, variant=1), budget_bytes=150e9, max_slots=64,
                          quantum=64)
     res = srv.serve(trace)
@@ -359,29 +418,32 @@ def bench_serving(device, n_requests=32):
     base = serving.summarize(base_res)
     errs = []
     for a, b_ in zip(res, base_res):
-        for i in range(a.probes.shape[0]):
-            nb = np.linalg.norm(b_.probes[i])
-            if nb > 0:
-                errs.append(float(np.linalg.norm(a.probes[i] - b_.probes[i]) / nb))
-    return {"workload": f"{n_requests}-request Poisson trace, 40 req/s, edges log-U[32,256], 0-3 Debye slabs",
-            "fp32_batched": ours, "fp64_sequential": base,
-            "solves_per_s_ratio": ours["solves_per_s"] / base["solves_per_s"],
-            "probe_rel_l2_vs_fp64_median": float(np.median(errs)) if errs else None,
-            "probe_rel_l2_vs_fp64_max": float(np.max(errs)) if errs else None,
-            "peak_slots": srv.peak_slots, "peak_bytes": srv.peak_bytes}
+        e = probe_error(a.probes, b_.probes)
+        if e is not None:
+            errs.append(e)
+    return {"ratio": round(ours["solves_per_s"] / base["solves_per_s"], 3),
+            "solves_s": round(ours["solves_per_s"], 3), "fp64_seq_solves_s": round(base["solves_per_s"], 3),
+            "p50_s": round(ours["latency_p50_s"], 3), "p95_s": round(ours["latency_p95_s"], 3),
+            "p99_s": round(ours["latency_p99_s"], 3),
+            "fp64_seq_p50_s": round(base["latency_p50_s"], 3), "fp64_seq_p99_s": round(base["latency_p99_s"], 3),
+            "probe_err_max": max(errs) if errs else None,
+            "probe_err_median": float(np.median(errs)) if errs else None,
+            "solves": len(res), "peak_slots": srv.peak_slots, "peak_gb": round(srv.peak_bytes / 1e9, 2),
+            "detail": {"fp32_batched": ours, "fp64_sequential": base,
+                       "request_errors": [round(e, 9) for e in errs]}}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "t512", "c3", "c1"])
-    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--workload", default="t512", choices=["t512", "c2", "c3", "c1"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--quick", action="store_true", help="main workload only (no 512^3, batch, serving sections)")
+    ap.add_argument("--quick", action="store_true", help="main workload only (no C2, C3, batch, serving sections)")
+    ap.add_argument("--serving-requests", type=int, default=256)
     args = ap.parse_args()
     if args.impl == "reference":  # rank 0 alone; no process group, no collective
         world, rank, _ = dist_env()
@@ -389,8 +451,8 @@ def main():
         return
     world, rank, local = dist_setup()
 
-    from ggi_tlm_b200 import autotune, build, capi
-    from ggi_tlm_b200.problem import build_tables, probe_series
+    from ggi_tlm_b200 import build, capi
+    from ggi_tlm_b200.problem import build_tables
 
     build.build()
     spec, wname = workload_spec(args.workload)
@@ -398,66 +460,34 @@ def main():
     K, W = args.steps, max(args.warmup, 3)
     if K + W + 40 > t["n_timesteps"]:
         K = t["n_timesteps"] - W - 40
-    n, npml, nmat, taps = cell_counts(t)
+    n = t["nx"] * t["ny"] * t["nz"]
     peak, peak_kind = measured_peak()
 
-    tuned = {}
+    # headline: the plain FP64 path (the reference's precision); then the FP32 fast path
+    r64 = timed_solo(t, capi.TLM_PRECISION_FP64, local, K, W, world, sample_clocks=True)
+    value, ms_max = replica_rate(n, K, world, r64["total_ms"])
+    r32 = timed_solo(t, capi.TLM_PRECISION_FP32, local, K, W, world)
+    v32, ms32 = replica_rate(n, K, world, r32["total_ms"])
+    ab64, ab32 = algorithmic_bytes(t, 8), algorithmic_bytes(t, 4)
+    bulk_gbs = ab64["bulk"] / (r64["bulk_ms"] / K / 1e3) / 1e9
+    step64 = ab64["total"] / (r64["total_ms"] / K / 1e3) / 1e9
+    step32 = ab32["total"] / (r32["total_ms"] / K / 1e3) / 1e9
+    bulk32 = ab32["bulk"] / (r32["bulk_ms"] / K / 1e3) / 1e9
+    err32 = probe_error(r32["probes"], r64["probes"])
 
-    def timed_run(precision, finish):
-        g = capi.GpuMesh(t, precision=precision, device=local)
-        tuned[precision] = autotune.tune(g, steps_per_variant=3, use_cache=False)  # real steps of the solve
-        g.run(W)
-        g.set_timing(True)
+    # end to end through the C-ABI with host buffers, FP64: create + table
+    # upload, every step tlm_gpu_run(t, 1) + read-back of that step's probe
+    # samples, DFT read-back at the end
+    e2e = None
+    if not args.no_e2e:
         barrier(world)
-        g.synchronize()
-        sampler = ClockSampler(local)
-        sampler.start()
-        g.run(K)
-        g.synchronize()
-        clocks = sampler.stop()
-        barrier(world)
-        total_ms, bulk_ms = g.last_run_time()
-        launches = g.last_run_launches()
-        probes = None
-        if finish:  # untimed: complete the solve for the probe-accuracy comparison
-            g.set_timing(False)
-            g.run(t["n_timesteps"] - g.step)
-            probes = probe_series(t, g.cell_output())
-        mem = g.memory_bytes()
-        g.close()
-        return total_ms, bulk_ms, launches, clocks, probes, mem
-
-    total32, bulk32, launches, clocks, p32, mem32 = timed_run(capi.TLM_PRECISION_FP32, not args.no_fp64)
-    value, ms_max = replica_rate(n, K, world, total32)
-    ab32 = algorithmic_bytes(t, 4)
-    bulk_gbs = ab32["bulk"] / (bulk32 / K / 1e3) / 1e9
-    step_gbs = ab32["total"] / (total32 / K / 1e3) / 1e9
-
-    fp64 = None
-    if not args.no_fp64:
-        total64, bulk64, _, _, p64, mem64 = timed_run(capi.TLM_PRECISION_FP64, True)
-        ab64 = algorithmic_bytes(t, 8)
-        norms = [np.linalg.norm(p64[i]) for i in range(len(p64))]
-        rel = max(np.linalg.norm(p32[i] - p64[i]) / norms[i] for i in range(len(p64)) if norms[i] > 0)
-        fp64 = {"value": replica_rate(n, K, world, total64)[0], "unit": UNIT,
-                "ms_per_step": total64 / K,
-                "step_achieved_gbs": ab64["total"] / (total64 / K / 1e3) / 1e9,
-                "step_frac_of_measured_hbm": ab64["total"] / (total64 / K / 1e3) / 1e9 / peak,
-                "bulk_kernel_achieved_gbs": ab64["bulk"] / (bulk64 / K / 1e3) / 1e9,
-                "probe_rel_l2_fp32_vs_fp64_max": rel, "probe_steps": int(t["n_timesteps"]),
-                "device_bytes": mem64}
-
-    # end to end through the C-ABI with host buffers: create + table upload,
-    # every step tlm_gpu_run(t,1) + read back that step's probe samples, DFT read at the end
-    barrier(world)
-    t0 = time.perf_counter()
-    NE = t["n_timesteps"] if not args.no_e2e else 0
-    if NE:
-        g = capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP32, device=local)
+        t0 = time.perf_counter()
+        NE = int(t["n_timesteps"])
+        g = capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64, device=local)
         row = np.zeros((1, max(int(t["n_out_cells"]), 1), 6))
-        for s in range(NE):
+        for s_ in range(NE):
             g.run(1, sync=False)
-            capi._check(capi._lib.tlm_gpu_fetch_cell_output(g.h, s + 1, 1, row.ctypes.data_as(capi._f64p)))
+            capi._check(capi._lib.tlm_gpu_fetch_cell_output(g.h, s_ + 1, 1, row.ctypes.data_as(capi._f64p)))
         dft = g.dft()
         g.close()
         e2e_s = max_over_ranks(time.perf_counter() - t0, world)
@@ -465,44 +495,55 @@ def main():
         e2e = {"value": n * NE * world / e2e_s / 1e9, "unit": UNIT, "steps": NE,
                "h2d_bytes_per_step": int(table_bytes / NE),
                "d2h_bytes_per_step": int(int(t["n_out_cells"]) * 6 * 8 + dft.nbytes / NE),
-               "includes": "a whole solve through the C-ABI from host buffers: handle create, table upload, "
+               "dtype": "f64",
+               "includes": "a whole FP64 solve through the C-ABI from host buffers: handle create, table upload, "
                            "every step tlm_gpu_run + read-back of that step's probe samples, DFT read-back"}
-    else:
-        e2e = None
 
     sections = not args.quick and world == 1  # per-GPU sections, reported at N=1
-    t512 = bench_target_512(local, peak) if sections else None
-    c4 = bench_batch(local) if sections else None
-    c5 = bench_serving(local) if sections else None
+    c2 = c3 = c4 = c5 = None
+    if sections:
+        c2 = bench_pair(build_tables(workload_spec("c2")[0]), local, peak)
+        c3 = bench_pair(build_tables(workload_spec("c3")[0]), local, peak)
+        c4 = bench_batch(local)
+        c5 = bench_serving(local, args.serving_requests)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, steps, el = cpu_oracle_rate(t, float(os.environ.get("TLM_CPU_BUDGET_S", "20")), 1000)
-        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"{steps} time steps of the same {t['nx']}x{t['ny']}x{t['nz']} mesh ({el:.1f} s)"}
+        rate, steps, el, used = cpu_oracle_rate(t, float(os.environ.get("TLM_CPU_BUDGET_S", "20")), 1000,
+                                                host_threads())
+        cpu = {"value": rate, "unit": UNIT, "cores": used, "kind": "port",
+               "sample": f"{steps} FP64 time steps of the same {t['nx']}x{t['ny']}x{t['nz']} mesh ({el:.1f} s), "
+                         f"oracle z-planes shared among {used} host threads"}
 
     if rank == 0:
+        nm = NCU_TRAFFIC.get(wname, {})
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wname, "cells": n, "pml_cells": npml, "material_cells": nmat,
-                       "parallelism": f"replicas{world}", "precision": "fp32 links+scatter, fp64 filters+DFT",
-                       "bulk_variant_fp32": tuned[capi.TLM_PRECISION_FP32]["variant"],
-                       "bulk_variant_fp64": tuned.get(capi.TLM_PRECISION_FP64, {}).get("variant"),
-                       "l2": "state (%.2f GB) larger than L2 (126 MB)" % (ab32["total"] / 1e9)},
-            "roofline": {"bound": "hbm", "kernel": bulk_kernel_name(tuned[capi.TLM_PRECISION_FP32]["variant"], 4),
-                         "achieved": bulk_gbs, "peak": peak,
-                         "unit": "GB/s", "frac": bulk_gbs / peak, "peak_kind": peak_kind,
-                         "traffic": NCU_TRAFFIC.get(wname, {}).get("bytes"),
-                         "traffic_source": NCU_TRAFFIC.get(wname, {}).get("source"),
-                         "algorithmic_bytes_per_launch": ab32["bulk"],
-                         "avg_launch_ms": bulk32 / K},
-            "step_roofline": {"achieved": step_gbs, "frac": step_gbs / peak,
-                              "algorithmic_bytes_per_step": ab32["total"]},
-            "fp64": fp64, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
-            "target_512": t512, "batch_c4": c4, "serving_c5": c5,
-            "device_bytes": mem32,
+            "dtype": "f64", "data": "synthetic",
+            "fp32": {"value": v32, "ms_per_step": ms32 / K, "step_frac": step32 / peak, "bulk_frac": bulk32 / peak,
+                     "step_frac_of_8tbs": step32 / 8000.0, "probe_rel_l2_vs_fp64_max": err32,
+                     "probe_steps": int(t["n_timesteps"]), "variant": r32["variant"]},
+            "fp64_step_frac": step64 / peak,
+            "c2": c2, "c3": c3,
+            "c4": {k: v for k, v in c4.items() if k != "note"} if c4 else None,
+            "c5": {k: v for k, v in c5.items() if k != "detail"} if c5 else None,
+            "config": dict(workload_config(t, wname, world),
+                           precision="fp64 everywhere (headline); fp32 links with fp64 filters, PML recursion and "
+                                     "DFT (fp32 key)",
+                           bulk_variant_fp64=r64["variant"], bulk_variant_fp32=r32["variant"]),
+            "roofline": {"bound": "hbm", "kernel": bulk_kernel_name(r64["variant"], 2),
+                         "achieved": bulk_gbs, "peak": peak, "unit": "GB/s", "frac": bulk_gbs / peak,
+                         "peak_kind": peak_kind,
+                         "traffic": (nm["bytes_per_cell"] * ab64["bulk"] / 192) if nm.get("bytes_per_cell") else None,
+                         "traffic_source": nm.get("source"),
+                         "algorithmic_bytes_per_launch": ab64["bulk"], "avg_launch_ms": r64["bulk_ms"] / K},
+            "step_roofline": {"achieved": step64, "frac": step64 / peak,
+                              "algorithmic_bytes_per_step": ab64["total"], "frac_of_8tbs": step64 / 8000.0},
+            "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": r64["launches"], "clocks": r64["clocks"],
+            "device_bytes": r64["device_bytes"],
+            "c4_note": c4.get("note") if c4 else None,
+            "c5_detail": c5.get("detail") if c5 else None,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
