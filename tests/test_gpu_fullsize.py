@@ -55,8 +55,10 @@ def _compare(t, steps):
     assert np.any(wl != 0.0)
     assert _links_rel(links, wl) <= TOL
     del links
+    assert got.shape == want.shape
     assert _rel(got, want) <= TOL or np.array_equal(got, want)
     wd = o.dft()
+    assert dft.shape == wd.shape
     assert _rel(dft, wd) <= TOL or np.array_equal(dft, wd)
     o.close()
 
