@@ -1,0 +1,239 @@
+"""Result files computed on the host from the device accumulators.
+
+The time loop leaves frequency-domain accumulators on the device (far-field
+J and M per face, SAR field DFTs per cell); after the run the reference
+turns them into its result files.  These are the same computations, in the
+reference's formulas and file formats, on the arrays the library returns:
+
+- far-field patterns, ``write_far_field_surfaces``
+  (OUTPUT/far_field_surfaces.F90:370-712): per far-field surface and
+  (theta, phi), the radiation integrals N, L over the surface faces
+  (Balanis' 3D form; the 2D form about z) and |E_theta|, |E_phi| at 1 m, in
+  ``NAME.far_field.fout.<surface>``;
+- SAR, ``write_SAR_volumes`` (OUTPUT/SAR_volumes.F90:334-622): per SAR
+  volume the sum over its cells of |E|^2 / 2 times the conductivity and the
+  cell volume, divided by the volume's mass, in ``NAME.SAR.fout``.
+"""
+from __future__ import annotations
+
+import math
+import os
+from typing import List, Sequence, Tuple
+
+import numpy as np
+
+from .problem import C0, PI, Z0
+from .tout import fortran_e
+
+
+def face_point(origin: Sequence[float], dl: float, cell: Sequence[int], code: int) -> Tuple[float, float, float]:
+    """get_cell_point_coordinate (MESH/general_mesh_subroutines.F90:84-135):
+    the centre of face ``code`` (1..6: xmin, ymin, zmin, xmax, ymax, zmax) of
+    the 1-based ``cell``, or the cell centre for code 7."""
+    off = [-0.5, -0.5, -0.5]
+    if 1 <= code <= 6:
+        off[(code - 1) % 3] = -1.0 if code <= 3 else 0.0
+    return tuple(origin[a] + cell[a] * dl + dl * off[a] for a in range(3))
+
+
+def _angles(lo: float, hi: float, step: float) -> np.ndarray:
+    """The reference's angle loop after read_far_field_surface converts the
+    degrees to radians: int((max - min) / step) + 1 values min + (n - 1) step."""
+    a0, a1, da = (PI / 180.0) * lo, (PI / 180.0) * hi, (PI / 180.0) * step
+    n = int((a1 - a0) / da) + 1
+    return np.array([a0 + k * da for k in range(n)])
+
+
+def far_field_pattern(acc: np.ndarray, points: np.ndarray, frequency: float, dl: float, theta, phi,
+                      dim: int = 3):
+    """|E_theta| and |E_phi| at r0 = 1 m from one far-field surface's
+    accumulators ``acc`` [faces, 6] (complex J_x, J_y, J_z, M_x, M_y, M_z)
+    and face centres ``points`` [faces, 3]; ``theta`` and ``phi`` are
+    (min, max, step) in degrees.  Returns (theta, phi) in radians [n] and
+    |E_theta|, |E_phi| [n], theta outer and phi inner as the reference
+    loops."""
+    beta = 2.0 * PI * frequency / C0
+    jbeta = 1j * beta
+    r0 = 1.0
+    J, M = acc[:, 0:3], acc[:, 3:6]
+    if dim == 2:
+        dA = dl
+        prop2 = np.sqrt(jbeta / (8.0 * PI * r0)) * np.exp(jbeta * r0)
+        th = np.array([PI / 2.0])
+    else:
+        dA = dl * dl
+        prop2 = jbeta * np.exp(jbeta * r0) / (4.0 * PI * r0)
+        th = _angles(*theta)
+    ph = _angles(*phi)
+    out_t, out_p, et, ep = [], [], [], []
+    for t in th:
+        ct, st = math.cos(t), math.sin(t)
+        for p in ph:
+            cp, sp = math.cos(p), math.sin(p)
+            r = np.array([r0 * st * cp, r0 * st * sp, r0 * ct])  # rthetaphi_to_xyz_point
+            if dim == 2:
+                rp_cos = points[:, 0] * r[0] + points[:, 1] * r[1]
+            else:
+                rp_cos = points @ r
+            prop = np.exp(jbeta * rp_cos) * dA
+            if dim == 2:
+                Nz = np.sum(J[:, 2] * prop)
+                Nphi = np.sum((-J[:, 0] * sp + J[:, 1] * cp) * prop)
+                Lz = np.sum(M[:, 2] * prop)
+                Lphi = np.sum((-M[:, 0] * sp + M[:, 1] * cp) * prop)
+                e_t = -prop2 * (Lphi - Z0 * Nz)  # minus the Ez component
+                e_p = prop2 * (Lz + Z0 * Nphi)
+            else:
+                Nt = np.sum((J[:, 0] * ct * cp + J[:, 1] * ct * sp - J[:, 2] * st) * prop)
+                Nphi = np.sum((-J[:, 0] * sp + J[:, 1] * cp) * prop)
+                Lt = np.sum((M[:, 0] * ct * cp + M[:, 1] * ct * sp - M[:, 2] * st) * prop)
+                Lphi = np.sum((-M[:, 0] * sp + M[:, 1] * cp) * prop)
+                e_t = -prop2 * (Lphi + Z0 * Nt)
+                e_p = prop2 * (Lt - Z0 * Nphi)
+            out_t.append(t)
+            out_p.append(p)
+            et.append(abs(e_t))
+            ep.append(abs(e_p))
+    return np.array(out_t), np.array(out_p), np.array(et), np.array(ep)
+
+
+def far_field_lines(theta: np.ndarray, phi: np.ndarray, et: np.ndarray, ep: np.ndarray, n_theta: int, n_phi: int,
+                    dt: float, dim: int = 3) -> List[str]:
+    """The far-field file: for the 3D transform a ``(A2,2I6,ES16.6)`` header
+    ('# ', the theta and phi counts, 1/dt), then one ``4E14.6`` line per
+    angle pair (degrees, |E_theta|, |E_phi|).  The 2D transform writes the
+    lines only (the reference opens no file for it and writes to its far
+    field unit as it stands; here it goes to the same numbered file)."""
+    lines = []
+    if dim != 2:
+        lines.append("# " + f"{n_theta:6d}{n_phi:6d}" + _es(1.0 / dt, 16, 6))
+    for t, p, a, b in zip(theta, phi, et, ep):
+        lines.append(fortran_e(t * 180.0 / PI, 14, 6) + fortran_e(p * 180.0 / PI, 14, 6) + fortran_e(a, 14, 6) +
+                     fortran_e(b, 14, 6))
+    return lines
+
+
+def _es(v: float, width: int, digits: int) -> str:
+    """Fortran ``ESw.d``: d.ddddddE+xx, right-justified."""
+    if v == 0.0:
+        body = "0." + "0" * digits + "E+00"
+    else:
+        m, e = f"{abs(v):.{digits}e}".split("e")
+        e = int(e)
+        body = ("-" if v < 0 else "") + m + (f"E{'+' if e >= 0 else '-'}{abs(e):02d}" if abs(e) < 100 else
+                                              f"{'+' if e >= 0 else '-'}{abs(e):03d}")
+    return body.rjust(width)
+
+
+def far_field_face_points(spec, t: dict) -> List[np.ndarray]:
+    """Per far-field table entry (one surface and frequency), the face
+    centres [faces, 3] in the order of the entry's accumulators."""
+    pts = []
+    for ff in spec.far_field_surfaces:
+        faces = ff.faces()
+        p = np.array([face_point(spec.origin, spec.dl, c, code) for c, code in faces]).reshape(-1, 3)
+        for _ in ff.frequencies:
+            pts.append(p)
+    return pts
+
+
+def write_far_field_surfaces(name: str, spec, t: dict, acc: np.ndarray, post: Sequence[dict],
+                             directory: str = ".") -> List[str]:
+    """Write ``<name>.far_field.fout.<k>`` for every far-field surface entry
+    k (1-based, one frequency each as the .inp reader makes them); ``acc`` is
+    the library's far-field accumulator array [faces of all entries, 6]
+    complex and ``post`` the reader's far-field angle records."""
+    written = []
+    ptr = np.asarray(t["ff_face_ptr"])
+    pts = far_field_face_points(spec, t)
+    for k, (pinfo, p) in enumerate(zip(post, pts), start=1):
+        a = acc[ptr[k - 1]:ptr[k]]
+        th, ph, et, ep = far_field_pattern(a, p, pinfo["frequency"], spec.dl, pinfo["theta"], pinfo["phi"],
+                                           pinfo.get("dim", 3))
+        n_phi = len(_angles(*pinfo["phi"]))
+        n_theta = len(th) // max(n_phi, 1)
+        path = os.path.join(directory, f"{name}.far_field.fout.{k}")
+        with open(path, "w") as f:
+            for line in far_field_lines(th, ph, et, ep, n_theta, n_phi, float(t["dt"]), pinfo.get("dim", 3)):
+                f.write(line + "\n")
+        written.append(path)
+    return written
+
+
+def sar_values(spec, t: dict, acc: np.ndarray, densities: Sequence[float]) -> List[Tuple[float, int, float]]:
+    """(frequency, SAR volume number, SAR) per SAR entry from the library's
+    SAR accumulators ``acc`` [cells of all entries, 3] complex (E_x, E_y,
+    E_z DFTs times dt): SAR = sigma V_cell sum_cells |E|^2 / 2 / mass with
+    mass = V_cell rho n_cells (SAR_volumes.F90:195-205, 576-605).  The
+    conductivity is the SAR material's sigma_e; the reference allows only
+    a material with a constant permittivity and no magnetic conductivity
+    (SAR_volumes.F90:150-195)."""
+    ptr = np.asarray(t["sar_cell_ptr"])
+    freqs = np.asarray(t["sar_freq"])
+    vol = spec.dl ** 3
+    rows = []
+    k = 0
+    for n, sv in enumerate(spec.sar_volumes, start=1):
+        mat = _sar_material(spec, sv)
+        for _ in sv.frequencies:
+            e = acc[ptr[k]:ptr[k + 1]]
+            s = 0.0
+            for c in range(e.shape[0]):  # the reference's cell order, summed left to right
+                s = s + 0.5 * (abs(e[c, 0]) ** 2 + abs(e[c, 1]) ** 2 + abs(e[c, 2]) ** 2)
+            mass = vol * densities[n - 1] * e.shape[0]
+            rows.append((float(freqs[k]), n, s * mat.sigma_e * vol / mass))
+            k += 1
+    return rows
+
+
+def _sar_material(spec, sv):
+    """The volume material whose cells the SAR volume covers."""
+    from .problem import _region_mask
+
+    from .problem import MAT_DISPERSIVE
+
+    want = sv.mask(spec)
+    for num, region in spec.material_regions:
+        if np.array_equal(_region_mask(spec, region), want):
+            m = spec.materials[num - 1]
+            if m.type != MAT_DISPERSIVE:
+                raise ValueError("SAR in a PEC or PMC material")
+            if len(m.eps.a) != 1 or len(m.eps.b) != 1:  # filter orders above 0
+                raise ValueError("SAR in a dispersive dielectric material")
+            if len(m.mu.a) != 1 or len(m.mu.b) != 1:
+                raise ValueError("SAR in a dispersive magnetic material")
+            if m.sigma_m != 0.0:
+                raise ValueError("SAR in a material with a magnetic conductivity")
+            return m
+    raise ValueError("a SAR volume that is not one material's cells")
+
+
+def sar_line(freq: float, number: int, sar: float) -> str:
+    """``write(unit,*) frequency, volume, SAR`` as gfortran's list-directed
+    output writes a REAL*8, a default INTEGER (I12) and a REAL*8."""
+    return (_ld_real(freq) + f"{number:12d}" + _ld_real(sar)).rstrip()
+
+
+def _ld_real(v: float) -> str:
+    """gfortran list-directed REAL*8, the edit descriptor 1PG26.17E3: for
+    0.1 <= |v| < 1e17 F editing with 17 significant digits right-justified
+    in 21 columns and 5 blanks after, else d.dddddddddddddddd with a
+    three-digit exponent, right-justified in 26 columns."""
+    a = abs(v)
+    if v == 0.0:
+        return "0.0000000000000000".rjust(21) + " " * 5
+    m, e = f"{v:.16e}".split("e")
+    e = int(e)
+    if -1 <= e < 17:  # |v|, rounded to 17 significant digits, in [0.1, 1e17)
+        k = e + 1 if a >= 1.0 else 0
+        return f"{v:.{17 - k}f}".rjust(21) + " " * 5
+    return (m + f"E{'+' if e >= 0 else '-'}{abs(e):03d}").rjust(26)
+
+
+def write_sar_volumes(name: str, spec, t: dict, acc: np.ndarray, densities: Sequence[float],
+                      directory: str = ".") -> List[str]:
+    path = os.path.join(directory, name + ".SAR.fout")
+    with open(path, "w") as f:
+        for row in sar_values(spec, t, acc, densities):
+            f.write(sar_line(*row) + "\n")
+    return [path]

@@ -17,7 +17,11 @@ and file names (TLM_MODULES/File_information.F90:143-158):
 - ``<problem_name>.volume_average_field.tout`` and
   ``.volume_peak_field.tout``: one value per output volume average or peak
   and output step (output_volume_averages.F90:330-350,
-  output_volume_peak.F90:320-340), numbered within their own packet.
+  output_volume_peak.F90:320-340), numbered within their own packet;
+- ``<problem_name>.far_field.fout.<k>``: the far-field pattern of each
+  far-field surface (far_field_surfaces.F90:370-712, ``postprocess``);
+- ``<problem_name>.SAR.fout``: the SAR of each SAR volume
+  (SAR_volumes.F90:334-622, ``postprocess``).
 
 The run goes through the library's C ABI in chunks of ``--chunk`` steps,
 reading the output points back after each chunk.  The other outputs
@@ -34,7 +38,7 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
-from . import capi, fout
+from . import capi, fout, postprocess
 from .inp import InpProblem, read_inp_file
 from .problem import build_tables, probe_series
 from .tout import data_line, excitation_rows, field_rows, header, output_flag
@@ -61,11 +65,13 @@ def _volume_rows(t: dict, spec, values: List[np.ndarray], kind: str):
 
 def write_results(name: str, p: InpProblem, t: dict, cell_out: np.ndarray, face_out: np.ndarray,
                   volumes: Optional[List[np.ndarray]] = None, directory: str = ".",
-                  power: Optional[np.ndarray] = None) -> List[str]:
+                  power: Optional[np.ndarray] = None, far_field: Optional[np.ndarray] = None,
+                  sar: Optional[np.ndarray] = None) -> List[str]:
     """Write the result files of a finished run; returns the paths written.
     ``cell_out`` is [steps, n_kept, 6], ``face_out`` [n_face_points, steps],
     ``volumes`` the output volume results, ``power`` the power surface
-    accumulators [faces, 4]."""
+    accumulators [faces, 4], ``far_field`` the far-field accumulators
+    [faces, 6] and ``sar`` the SAR accumulators [cells, 3]."""
     written = []
     n = int(t["n_timesteps"])
     if int(t["n_functions"]):
@@ -85,6 +91,10 @@ def write_results(name: str, p: InpProblem, t: dict, cell_out: np.ndarray, face_
             for line in fout.power_surface_lines(t["ps_freq"], surf, fout.power_surfaces(t, power)):
                 f.write(line + "\n")
         written.append(path)
+    if p.spec.far_field_surfaces and far_field is not None:
+        written += postprocess.write_far_field_surfaces(name, p.spec, t, far_field, p.post["far_field"], directory)
+    if p.spec.sar_volumes and sar is not None:
+        written += postprocess.write_sar_volumes(name, p.spec, t, sar, p.post["sar_density"], directory)
     for kind, extn in (("average", ".volume_average_field.tout"), ("peak", ".volume_peak_field.tout")):
         if any(v.kind == kind for v in p.spec.output_volumes):
             rows, count = _volume_rows(t, p.spec, volumes, kind)
@@ -123,7 +133,9 @@ def run(name: str, precision: int = capi.TLM_PRECISION_FP64, device: int = 0, ch
         face_out = np.concatenate(faces, axis=1) if faces else np.zeros((0, 0))
         volumes = g.output_volumes() if p.spec.output_volumes else None
         power = g.power_surfaces() if p.spec.power_surfaces else None
-    return write_results(name, p, t, cell_out, face_out, volumes, directory, power)
+        far_field = g.far_field() if p.spec.far_field_surfaces else None
+        sar = g.sar_volumes() if p.spec.sar_volumes else None
+    return write_results(name, p, t, cell_out, face_out, volumes, directory, power, far_field, sar)
 
 
 def main(argv: Optional[Sequence[str]] = None) -> int:

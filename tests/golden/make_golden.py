@@ -49,6 +49,10 @@ INP_CASES = {
     "power_calc": "POWER_CALCS/PROBLEM_SPECIFICATION_FILES/power_calc.inp",
     "helix": "HELIX_ANTENNA/helix.inp",
 }
+# result files the solver writes after the run (write_SAR_volumes), as text
+RESULT_CASES = {
+    "sar_test": "SAR_TEST/PROBLEM_SPECIFICATION_FILES/SAR_test.SAR.fout_ref",
+}
 # mesh files written by the reference's mesher (MESH/write_mesh.F90), as text
 MESH_CASES = {
     "helix": "HELIX_ANTENNA/helix.mesh",
@@ -114,6 +118,12 @@ def main():
             fo[name] = np.array(f.read().splitlines())
     np.savez_compressed(os.path.join(here, "fout_text.npz"), **fo)
     print("fout_text", {k: len(v) for k, v in fo.items()})
+    rs = {}
+    for name, rel in RESULT_CASES.items():
+        with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", rel)) as f:
+            rs[name] = np.array(f.read().splitlines())
+    np.savez_compressed(os.path.join(here, "result_text.npz"), **rs)
+    print("result_text", {k: len(v) for k, v in rs.items()})
     me = {}
     for name, rel in MESH_CASES.items():
         with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", rel)) as f:

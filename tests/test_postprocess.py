@@ -1,0 +1,130 @@
+"""Host-side result files from the device accumulators
+(ggi_tlm_b200/postprocess.py): the far-field pattern
+(far_field_surfaces.F90:370-712) and SAR (SAR_volumes.F90:334-622).
+
+The SAR file's list-directed lines are checked against the reference's
+SAR_TEST golden file (tests/golden/result_text.npz); the far-field transform
+against the radiation pattern of a small dipole (|E_theta| ~ sin theta,
+E_phi ~ 0) computed from the oracle's far-field accumulators; SAR against
+its definition on the oracle's accumulators.  GPU: the library's
+accumulators give the oracle's files."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from ggi_tlm_b200 import postprocess as pp
+from ggi_tlm_b200.problem import (Block, FarFieldSurface, PointExcitation, SARVolume, VolumeMaterial, build_tables)
+from ggi_tlm_b200 import cases
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(os.path.dirname(HERE), "oracle"))
+import oracle  # noqa: E402
+
+
+def test_sar_lines_match_the_reference_file():
+    lines = [str(x) for x in np.load(os.path.join(HERE, "golden", "result_text.npz"))["sar_test"]]
+    assert len(lines) == 2
+    for k, line in enumerate(lines, start=1):
+        f, n, v = line.split()
+        assert int(n) == k
+        assert pp.sar_line(float(f), k, float(v)) == line
+
+
+def test_list_directed_reals():
+    assert pp._ld_real(0.5) == "0.50000000000000000".rjust(21) + " " * 5
+    assert pp._ld_real(-12.25) == "-12.250000000000000".rjust(21) + " " * 5
+    assert pp._ld_real(1e17) == "1.0000000000000000E+017".rjust(26)
+    assert pp._ld_real(0.05) == "5.0000000000000003E-002".rjust(26)
+    assert pp._ld_real(0.0) == "0.0000000000000000".rjust(21) + " " * 5
+
+
+def test_face_points():
+    o, dl = (-1.0, 0.0, 2.0), 0.5
+    assert pp.face_point(o, dl, (1, 1, 1), 7) == (-0.75, 0.25, 2.25)
+    assert pp.face_point(o, dl, (1, 1, 1), 1) == (-1.0, 0.25, 2.25)
+    assert pp.face_point(o, dl, (1, 1, 1), 6) == (-0.75, 0.25, 2.5)
+
+
+def dipole_spec(n=32, steps=400):
+    """A PML box with a soft Ez point source at its centre and a closed
+    far-field box around it, 300 MHz (wavelength 100 cells)."""
+    s = cases.pml_point_source(n, pml=6, steps=steps, dl=0.01, n_probes=0)
+    c = (n + 1) // 2
+    s.point_excitations = [PointExcitation((c, c, c), "Ez", 1)]
+    s.far_field_surfaces = [FarFieldSurface([3e8], box=((10, n - 9), (10, n - 9), (10, n - 9)))]
+    return s
+
+
+POST = dict(frequency=3e8, theta=(0.0, 180.0, 10.0), phi=(0.0, 90.0, 45.0), dim=3)
+
+
+def test_small_dipole_far_field_pattern():
+    s = dipole_spec()
+    t = build_tables(s)
+    o = oracle.Oracle(t)
+    o.run(t["n_timesteps"])
+    acc = o.far_field()
+    o.close()
+    th, ph, et, ep = pp.far_field_pattern(acc, pp.far_field_face_points(s, t)[0], dl=s.dl, **POST)
+    assert len(th) == 19 * 3
+    peak = et.max()
+    assert peak > 0
+    ok = (th > np.radians(15)) & (th < np.radians(165))
+    np.testing.assert_allclose(et[ok] / peak, np.sin(th[ok]), atol=0.02)
+    assert ep.max() < 1e-2 * peak
+    lines = pp.far_field_lines(th, ph, et, ep, 19, 3, t["dt"])
+    assert lines[0] == "#     19     3" + pp._es(1.0 / t["dt"], 16, 6) and len(lines) == 1 + 57
+    assert lines[1].split()[:2] == ["0.000000E+00", "0.000000E+00"]
+
+
+def sar_spec():
+    s = cases.pml_point_source(24, pml=5, steps=300, dl=0.01, n_probes=0)
+    s.materials = [VolumeMaterial.dielectric(4.0, 0.5)]
+    s.material_regions = [(1, Block(10, 15, 10, 15, 14, 17))]
+    s.sar_volumes = [SARVolume(Block(10, 15, 10, 15, 14, 17), [3e8])]
+    return s
+
+
+def test_sar_value_is_its_definition():
+    s = sar_spec()
+    t = build_tables(s)
+    o = oracle.Oracle(t)
+    co = o.run(t["n_timesteps"])
+    o.close()
+    acc = oracle.sar_volumes(t, co)
+    (f, n, v), = pp.sar_values(s, t, acc, [1000.0])
+    e2 = 0.5 * np.sum(np.abs(acc) ** 2)
+    assert (f, n) == (3e8, 1) and v > 0
+    assert v == pytest.approx(e2 * 0.5 * s.dl ** 3 / (s.dl ** 3 * 1000.0 * acc.shape[0]), rel=1e-12)
+    bad = sar_spec()
+    bad.materials = [VolumeMaterial.debye(2.0, [4.0], [1e-10])]
+    with pytest.raises(ValueError, match="dispersive dielectric"):
+        pp.sar_values(bad, t, acc, [1000.0])
+
+
+@pytest.mark.gpu
+def test_gpu_far_field_and_sar_files_match_the_oracle(gpu_lib, tmp_path):
+    from ggi_tlm_b200 import capi
+
+    s = dipole_spec(steps=300)
+    s.materials = [VolumeMaterial.dielectric(4.0, 0.5)]
+    s.material_regions = [(1, Block(12, 14, 12, 14, 18, 20))]
+    s.sar_volumes = [SARVolume(Block(12, 14, 12, 14, 18, 20), [3e8])]
+    t = build_tables(s)
+    o = oracle.Oracle(t)
+    co = o.run(t["n_timesteps"])
+    ff_o, sar_o = o.far_field(), oracle.sar_volumes(t, co)
+    o.close()
+    with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64) as g:
+        g.run(t["n_timesteps"])
+        ff_g, sar_g = g.far_field(), g.sar_volumes()
+    pts = pp.far_field_face_points(s, t)[0]
+    a = pp.far_field_pattern(ff_g, pts, dl=s.dl, **POST)
+    b = pp.far_field_pattern(ff_o, pts, dl=s.dl, **POST)
+    for x, y in zip(a, b):
+        assert np.linalg.norm(x - y) <= 1e-10 * np.linalg.norm(y)
+    (_, _, vg), = pp.sar_values(s, t, sar_g, [1000.0])
+    (_, _, vo), = pp.sar_values(s, t, sar_o, [1000.0])
+    assert vg == pytest.approx(vo, rel=1e-10)
