@@ -474,11 +474,12 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
         if r.values(1)[0] != 1.0:  # s_to_z_warp (FILTER/filter_functions.F90:343-385) divides dt by it
             raise UnsupportedFeature("a frequency scale other than 1 for the material filters")
     dt = dl / (2.0 * C0 / reduced_c)  # TLM_SOLVER/set_TLM_solver_parameters.F90:93-95
-    steps = nint(rec["simulation_time"].values(1)[0] / dt)
+    sim_time = rec["simulation_time"].values(1)[0]
+    steps = nint(sim_time / dt)
     R = tuple(rec["outer_boundary_reflection_coefficient"].values(6)) \
         if "outer_boundary_reflection_coefficient" in rec else (0.0,) * 6
     spec = ProblemSpec(nx=n[0], ny=n[1], nz=n[2], dl=dl, n_timesteps=steps, R=R, origin=(xmin, ymin, zmin),
-                       reduced_c=reduced_c)
+                       reduced_c=reduced_c, simulation_time=sim_time)
     # PML, read_pml.F90:70-150: a line of six thicknesses (metres) or one for
     # all sides, the same for the reflection coefficients, then the order
     if "pml" in rec:

@@ -12,7 +12,10 @@ reference's formulas and file formats, on the arrays the library returns:
   ``NAME.far_field.fout.<surface>``;
 - SAR, ``write_SAR_volumes`` (OUTPUT/SAR_volumes.F90:334-622): per SAR
   volume the sum over its cells of |E|^2 / 2 times the conductivity and the
-  cell volume, divided by the volume's mass, in ``NAME.SAR.fout``.
+  cell volume, divided by the volume's mass, in ``NAME.SAR.fout``;
+- the RCS, ``write_rcs_surfaces`` (OUTPUT/RCS_surfaces.F90:575-762): the
+  monostatic far field in time (``NAME.rcs.tout``) and its spectrum
+  against the incident field's (``NAME.rcs.fout``).
 """
 from __future__ import annotations
 
@@ -237,3 +240,64 @@ def write_sar_volumes(name: str, spec, t: dict, acc: np.ndarray, densities: Sequ
         for row in sar_values(spec, t, acc, densities):
             f.write(sar_line(*row) + "\n")
     return [path]
+
+
+def rcs_lines(t: dict, far: np.ndarray, fmin: float, fmax: float, fstep: float, function: int) -> Tuple[List[str],
+                                                                                                       List[str]]:
+    """The RCS files of write_rcs_surfaces (RCS_surfaces.F90:575-762) from
+    the library's time-domain far field ``far`` [4, n_points] (E_theta,
+    E_phi, H_theta, H_phi per far-field time bin):
+
+    - ``.rcs.tout``: per bin d its time d dl / (n_points_per_cell c0) and
+      the four values, |v| < 1e-30 written as 0, format (I10,5E14.6);
+    - ``.rcs.fout``: per frequency fmin + (k-1) fstep, k up to
+      int((fmax-fmin)/fstep)+1, the DFT of the four series times
+      j 2 pi f / c0, the incident field's DFT (the Huygens surface's
+      excitation function over the run's steps) and
+      RCS = 10 log10(4 pi Re(E_theta H_phi* - E_phi H_theta*) / (|Einc|^2 / Z0))
+      (-1000 when not positive), format 5E14.6."""
+    dl, dt = float(t["dl"]), float(t["dt"])
+    npc = int(t["rcs_npc"])
+    n = far.shape[1]
+    tout = []
+    for d in range(1, n + 1):
+        tl = d * dl / (npc * C0)
+        v = [0.0 if abs(x) < 1e-30 else float(x) for x in far[:, d - 1]]
+        tout.append(f"{d:10d}" + fortran_e(tl, 14, 6) + "".join(fortran_e(x, 14, 6) for x in v))
+    fn = np.asarray(t["fn_value"]).reshape(int(t["n_functions"]), -1)[function - 1]
+    nsteps = int(t["n_timesteps"])
+    dt_local = dl / (npc * C0)
+    nf = int((fmax - fmin) / fstep) + 1
+    fout_lines = []
+    for k in range(1, nf + 1):
+        f = fmin + (k - 1) * fstep
+        einc = 0j
+        for ts in range(1, nsteps + 1):
+            einc = einc + fn[ts - 1] * (dt * np.exp(-1j * 2.0 * PI * f * ((ts - 1) * dt)))
+        acc = [0j, 0j, 0j, 0j]
+        for d in range(1, n + 1):
+            fc = dt_local * np.exp(-1j * 2.0 * PI * f * (d * dl / (npc * C0)))
+            for c in range(4):
+                acc[c] = acc[c] + far[c, d - 1] * fc
+        et, ep, ht, hp = (a * 1j * 2.0 * PI * f / C0 for a in acc)
+        rpower = (et * np.conj(hp) - ep * np.conj(ht)).real
+        ipower = abs(einc) ** 2 / Z0
+        rcs = 10.0 * math.log10(4.0 * PI * rpower / ipower) if (rpower > 0.0 and ipower != 0.0) else -1000.0
+        fout_lines.append("".join(fortran_e(x, 14, 6) for x in (f, abs(et), abs(ep), abs(einc), rcs)))
+    return tout, fout_lines
+
+
+def write_rcs(name: str, t: dict, far: np.ndarray, rcs_range: Sequence[float], function: int,
+              directory: str = ".") -> List[str]:
+    """Write ``<name>.rcs.tout`` and ``<name>.rcs.fout``; ``rcs_range`` is
+    the packet's (fmin, fmax, fstep) and ``function`` the Huygens surface's
+    excitation function number."""
+    tout, fo = rcs_lines(t, far, *rcs_range, function)
+    out = []
+    for extn, lines in ((".rcs.tout", tout), (".rcs.fout", fo)):
+        path = os.path.join(directory, name + extn)
+        with open(path, "w") as f:
+            for line in lines:
+                f.write(line + "\n")
+        out.append(path)
+    return out

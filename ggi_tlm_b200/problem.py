@@ -778,6 +778,9 @@ class ProblemSpec:
     output_volumes: List[OutputVolume] = field(default_factory=list)
     sar_volumes: List[SARVolume] = field(default_factory=list)
     reduced_c: float = 1.0
+    # the Simulation_time packet's value (read_simulation_time), where the
+    # problem came from a problem file; n_timesteps = NINT(simulation_time/dt)
+    simulation_time: Optional[float] = None
     # set_small_to_zero packet (read_small_to_zero.F90:55-59): (n_small_to_zero, small_to_zero_value)
     small_to_zero: Optional[Tuple[int, float]] = None
     # features rejected up front by the GPU path
@@ -1431,7 +1434,9 @@ def build_tables(spec: ProblemSpec) -> dict:
             z = zmin0 + c[2] * dl + dl * off[2]
             dist.append(K[0] * x + K[1] * y + K[2] * z)
         dmin, dmax = min(dist), max(dist)
-        period = (dmax - dmin) / C0 + nsteps * dt  # simulation_time = n_timesteps dt
+        # the problem file's simulation_time, or n_timesteps dt for a spec without one
+        sim = spec.simulation_time if spec.simulation_time is not None else nsteps * dt
+        period = (dmax - dmin) / C0 + sim
         distance = period * C0
         tables.update(rcs_on=1, rcs_theta=theta, rcs_phi=phi, rcs_npc=RCS_POINTS_PER_CELL,
                       rcs_points=int(RCS_POINTS_PER_CELL * distance / dl + 2),

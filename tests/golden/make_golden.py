@@ -48,10 +48,13 @@ INP_CASES = {
     "excitation_test": "EXCITATION_FUNCTION_TEST/PROBLEM_SPECIFICATION_FILES/excitation_test.inp",
     "power_calc": "POWER_CALCS/PROBLEM_SPECIFICATION_FILES/power_calc.inp",
     "helix": "HELIX_ANTENNA/helix.inp",
+    "rcs_plate": "RCS_PEC_PLATE_ROUGH_SURFACE/PROBLEM_SPECIFICATION_FILES/plate.inp",
 }
 # result files the solver writes after the run (write_SAR_volumes), as text
 RESULT_CASES = {
     "sar_test": "SAR_TEST/PROBLEM_SPECIFICATION_FILES/SAR_test.SAR.fout_ref",
+    "rcs_plate_fout": "RCS_PEC_PLATE_ROUGH_SURFACE/PROBLEM_SPECIFICATION_FILES/plate.rcs.fout_ref",
+    "rcs_plate_tout": "RCS_PEC_PLATE_ROUGH_SURFACE/PROBLEM_SPECIFICATION_FILES/plate.rcs.tout_ref",
 }
 # mesh files written by the reference's mesher (MESH/write_mesh.F90), as text
 MESH_CASES = {
