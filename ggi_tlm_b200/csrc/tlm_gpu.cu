@@ -248,6 +248,8 @@ struct Mesh {
   int n_exc_cells = 0;
   std::vector<int32_t> f_cx, f_cy, f_cz, f_dir, f_exc, f_out;
   std::vector<int32_t> f_mat;  // surface material per special face (empty: none)
+  std::vector<int32_t> f_smat;  // signed thin-layer material per special face (empty: none)
+  std::vector<tlm::ThinLayerDev> thin;  // thin-layer materials
   // point sources on faces (excitation face number, component 1..12, function, type)
   std::vector<int32_t> fpt_face, fpt_comp, fpt_fn, fpt_type;
   // output points on faces (output face number, side 1/2, component 1..6)
@@ -299,7 +301,7 @@ struct Mesh {
       pmm_pos, pmm_parmat, pmm_state, pmm_sigma, face_src, fpt_field_d, fpt_type_d, fprobe, fprobe_rec,
       ohs_face, ohs_offset, ff_entry, ff_phasor, ff_acc, cell_cur, out_hist, vdft_entry, vdft_gate_d, vdft_phasor,
       vdft_acc, osurf_entry, osurf_pos, osurf_dev, osurf_hist, rcs_face, rcs_dist_d, rcs_tc0, rcs_acc, ovol_dev,
-      face_mat_d, ovol_cells, ovol_hist, sar_entry, sar_phasor, sar_acc, ps_entry, ps_phasor, ps_acc, mode_d, mode_face, mode_wd,
+      face_mat_d, face_smat_d, thin_d, thin_taps, ovol_cells, ovol_hist, sar_entry, sar_phasor, sar_acc, ps_entry, ps_phasor, ps_acc, mode_d, mode_face, mode_wd,
       mode_hist;
   int n_pt_rows = 0;
   int n_pmm = 0;  // PML cells inside a volume material
@@ -436,6 +438,9 @@ tlm::FaceDev face_dev(Mesh *m) {
   f.pt_type = (const int8_t *)m->fpt_type_d.p;
   f.n_pt_rows = m->n_pt_rows;
   f.mat = (const int8_t *)m->face_mat_d.p;
+  f.smat = (const int *)m->face_smat_d.p;
+  f.tl = (const tlm::ThinLayerDev *)m->thin_d.p;
+  f.tl_taps = (double *)m->thin_taps.p;
   return f;
 }
 
@@ -912,13 +917,34 @@ int finalize(Mesh *m) {
     if (!m->f_mat.empty() && (int)m->f_mat.size() != nf)
       return fail(TLM_E_BADARG, "face materials: %zu given for %d special faces", m->f_mat.size(), nf);
     std::vector<int8_t> fmat(std::max(nf, 1), 0);
+    if (!m->f_smat.empty() && (int)m->f_smat.size() != nf)
+      return fail(TLM_E_BADARG, "face thin layers: %zu given for %d special faces", m->f_smat.size(), nf);
+    std::vector<int> fsmat(std::max(nf, 1), 0);
     for (int f = 0; f < (int)m->f_mat.size(); f++) {
       const int t = m->f_mat[f];
-      if (t != 0 && t != 1 && t != 2 && t != 4)
-        return fail(TLM_E_UNSUPPORTED, "special face %d: surface material type %d (only PEC 1, PMC 2, free space 4)", f + 1, t);
+      if (t != 0 && t != 1 && t != 2 && t != 3 && t != 4)
+        return fail(TLM_E_UNSUPPORTED,
+                    "special face %d: surface material type %d (only PEC 1, PMC 2, thin layer 3, free space 4)", f + 1, t);
       fmat[f] = (int8_t)t;
+      const int sm = m->f_smat.empty() ? 0 : m->f_smat[f];
+      if ((t == 3) != (sm != 0))
+        return fail(TLM_E_BADARG, "special face %d: a thin layer needs material type 3 and a thin-layer material", f + 1);
+      if (sm && std::abs(sm) > (int)m->thin.size())
+        return fail(TLM_E_BADARG, "special face %d: thin-layer material %d is not defined", f + 1, std::abs(sm));
+      fsmat[f] = sm;
     }
-    if ((rc = upload(m, m->face_mat_d, fmat))) return rc;
+    if (m->f_mat.empty())
+      for (int f = 0; f < (int)m->f_smat.size(); f++)
+        if (m->f_smat[f]) return fail(TLM_E_BADARG, "special face %d: a thin layer needs material type 3", f + 1);
+    {
+      std::vector<tlm::ThinLayerDev> tl = m->thin;
+      if (tl.empty()) tl.resize(1);
+      if ((rc = upload(m, m->face_mat_d, fmat)) || (rc = upload(m, m->face_smat_d, fsmat)) ||
+          (rc = upload(m, m->thin_d, tl)) ||
+          (rc = dalloc(m, m->thin_taps, (size_t)std::max(nf, 1) * 8 * tlm::kMaxOrder * sizeof(double))))
+        return rc;
+      CK(cudaMemset(m->thin_taps.p, 0, m->thin_taps.bytes));  // allocate_Zfilter_response: w = 0
+    }
     std::vector<int> covered(m->n_exc_faces + 1, 0);
     std::vector<int2> src(std::max(nf, 1), int2{0, -1});
     for (int h = 0; h < (m->hs_outer ? 0 : m->hs_n); h++) {
@@ -1709,6 +1735,50 @@ int tlm_gpu_set_face_materials(int64_t h, int32_t n, const int32_t *type) {
   if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
   if (n < 0 || (n && !type)) return fail(TLM_E_BADARG, "bad face material arguments");
   m->f_mat.assign(type, type + n);
+  return TLM_OK;
+}
+
+int tlm_gpu_set_thin_layers(int64_t h, int32_t n, const double *f, const double *a, const double *b,
+                            const int32_t *order, int32_t stride) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && (!f || !a || !b || !order)) || stride < 1)
+    return fail(TLM_E_BADARG, "bad thin-layer arguments");
+  m->thin.assign(n, tlm::ThinLayerDev{});
+  for (int i = 0; i < n; i++)
+    for (int p = 0; p < 3; p++)
+      for (int k = 0; k < 4; k++) {
+        const size_t e = ((size_t)i * 3 + p) * 4 + k;
+        const int o = order[e];
+        if (o < 0 || o > tlm::kMaxOrder || o + 1 > stride)
+          return fail(TLM_E_UNSUPPORTED, "thin layer %d: filter order %d (at most %d)", i + 1, o, tlm::kMaxOrder);
+        tlm::ThinLayerDev &d = m->thin[i];
+        d.order[p][k] = o;
+        d.f[p][k] = f[e];
+        for (int c = 0; c <= tlm::kMaxOrder; c++) {
+          d.a[p][k][c] = c <= o ? a[e * stride + c] : 0.0;
+          d.b[p][k][c] = c <= o ? b[e * stride + c] : 0.0;
+        }
+        if (d.b[p][k][0] == 0.0) return fail(TLM_E_BADARG, "thin layer %d: filter b(0) is zero", i + 1);
+      }
+  for (int i = 0; i < n; i++)  // surface_material_update stops on a singular impedance matrix
+    for (int p = 0; p < 3; p++)
+      for (int rev = 0; rev < 2; rev++) {
+        const tlm::ThinLayerDev &d = m->thin[i];
+        const double U11 = tlm::kZ0 + d.f[p][0], U22 = tlm::kZ0 + d.f[p][3];
+        if (U11 * U22 - d.f[p][2] * d.f[p][1] == 0.0)
+          return fail(TLM_E_BADARG, "thin layer %d: singular impedance matrix", i + 1);
+      }
+  return TLM_OK;
+}
+
+int tlm_gpu_set_face_thin_layers(int64_t h, int32_t n, const int32_t *material) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && !material)) return fail(TLM_E_BADARG, "bad face thin-layer arguments");
+  m->f_smat.assign(material, material + n);
   return TLM_OK;
 }
 

@@ -1509,6 +1509,15 @@ __global__ void __launch_bounds__(128) tlm_pml_material_kernel(const MeshDev<T> 
 // ---------------------------------------------------------------------------
 // Special faces: Huygens excitation + face outputs, connect_normal_to_*.F90
 // ---------------------------------------------------------------------------
+// A dispersive thin layer after calculate_surface_material_filter_coefficients
+// (MATERIALS/TLM_surface_materials.F90:225-280): per polarisation (x, y, z)
+// and filter (Z11, Z12, Z21, Z22) the fast part f and the slow Z filter.
+struct ThinLayerDev {
+  double f[3][4];
+  double a[3][4][kMaxOrder + 1], b[3][4][kMaxOrder + 1];
+  int order[3][4];
+};
+
 struct FaceDev {
   const int4 *face;        // (x, y, z) 0-based of the + cell, dir 1..3
   const int2 *face_io;     // (exc index or -1, out index or -1)
@@ -1523,8 +1532,59 @@ struct FaceDev {
   const double *pt_field;  // [n_timesteps][n_pt_rows][12] summed face point sources (E, H, J, M)
   const int8_t *pt_type;   // [n_pt_rows][6] hard (0) / soft (1) source factor of E, H
   int n_pt_rows;
-  const int8_t *mat;       // per special face: surface material 0 none, 1 PEC, 2 PMC, 4 free space
+  const int8_t *mat;       // per special face: surface material 0 none, 1 PEC, 2 PMC, 3 thin layer, 4 free space
+  const int *smat;         // per special face: signed thin-layer material (positive: reversed), 0 none
+  const ThinLayerDev *tl;  // thin-layer materials
+  double *tl_taps;         // per special face: [2 polarisations][4 filters][kMaxOrder] filter taps w(1..order)
 };
+
+// surface_material_update (MATERIALS/TLM_surface_materials.F90:535-697) for
+// one polarisation of one face: the layer's two-port impedance matrix,
+// fast parts plus the slow filters' responses, between the incident pulses
+// Vli (from the cell below the face) and Vri (from the cell above), each
+// side on the line impedance Z0; returns the total voltages Vl, Vr on the
+// two sides and updates and time-shifts the four filters (taps w(1..order)
+// at w + k * kMaxOrder).  The arithmetic is the reference's, in its order.
+__device__ __forceinline__ void thin_layer_update(const ThinLayerDev &L, int pol, bool reverse, double *w,
+                                                  double Vli, double Vri, double &Vl, double &Vr) {
+  double slow[4];
+  for (int k = 0; k < 4; k++) {  // evaluate_Zfilter with G = 0
+    const int o = L.order[pol][k];
+    const double *a = L.a[pol][k], *b = L.b[pol][k];
+    const double *wk = w + k * kMaxOrder;
+    double W0 = 0.0;
+    for (int i = 1; i <= o; i++) W0 = W0 - b[i] * wk[i - 1];
+    W0 = W0 / b[0];
+    double F0 = 0.0;
+    F0 = F0 + a[0] * W0;
+    for (int i = 1; i <= o; i++) F0 = F0 + a[i] * wk[i - 1];
+    slow[k] = F0;
+  }
+  const double Zl = kZ0, Zr = kZ0;
+  const double Z1 = reverse ? Zr : Zl, Z2 = reverse ? Zl : Zr;
+  const double U11 = Z1 + L.f[pol][0], U12 = L.f[pol][1], U21 = L.f[pol][2], U22 = Z2 + L.f[pol][3];
+  const double det = U11 * U22 - U21 * U12;  // the host refuses layers for which it is zero
+  const double V1i = reverse ? Vri : Vli, V2i = reverse ? Vli : Vri;
+  const double rhs1 = 2.0 * V1i - slow[0] - slow[1];
+  const double rhs2 = 2.0 * V2i - slow[2] - slow[3];
+  const double i1 = (U22 * rhs1 - U12 * rhs2) / det;
+  const double i2 = (-U21 * rhs1 + U11 * rhs2) / det;
+  const double V1 = 2.0 * V1i - i1 * Z1;
+  const double V2 = 2.0 * V2i - i2 * Z2;
+  const double G[4] = {i1, i2, i1, i2};
+  for (int k = 0; k < 4; k++) {  // evaluate_Zfilter with the port current, then timeshift_Zfilter
+    const int o = L.order[pol][k];
+    const double *b = L.b[pol][k];
+    double *wk = w + k * kMaxOrder;
+    double W0 = G[k];
+    for (int i = 1; i <= o; i++) W0 = W0 - b[i] * wk[i - 1];
+    W0 = W0 / b[0];
+    for (int i = o - 1; i >= 1; i--) wk[i] = wk[i - 1];
+    if (o > 0) wk[0] = W0;
+  }
+  Vl = reverse ? V2 : V1;
+  Vr = reverse ? V1 : V2;
+}
 
 template <typename T>
 __device__ __forceinline__ void face_body(const MeshDev<T> &m, const FaceDev &fd, int f, int rel_step);
@@ -1646,6 +1706,13 @@ __device__ __forceinline__ void face_body(const MeshDev<T> &m, const FaceDev &fd
     A_min = 0.0; A_max = 0.0; B_min = 0.0; B_max = 0.0;
   } else if (mat == 2) {  // PMC sheet, connect_normal_to_x.F90:41-45: each side reflects with +1
     A_min = 2.0 * a1; A_max = 2.0 * b1; B_min = 2.0 * a2; B_max = 2.0 * b2;
+  } else if (mat == 3) {  // thin layer, connect_normal_to_x.F90:268-282 (y, z analogues)
+    const int sm = fd.smat[f];
+    const ThinLayerDev &L = fd.tl[(sm > 0 ? sm : -sm) - 1];
+    const int pol1 = dir == 1 ? 1 : 0, pol2 = dir == 3 ? 1 : 2;  // x faces: y, z; y faces: x, z; z faces: x, y
+    double *w = fd.tl_taps + (size_t)f * 8 * kMaxOrder;
+    thin_layer_update(L, pol1, sm > 0, w, b1, a1, A_max, A_min);
+    thin_layer_update(L, pol2, sm > 0, w + 4 * kMaxOrder, b2, a2, B_max, B_min);
   }  // 0 and 4 (a free-space surface material): the plain sum
   if (io.x >= 0) {
     // face_excitation_field / face_excitation_type of this face: point

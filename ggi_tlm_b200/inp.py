@@ -39,7 +39,7 @@ from .meshfile import MeshFile, check_cells, connect_faces, pml_cells_from_mesh,
 from .problem import (C0, MAT_PEC, MAT_PMC, SOURCE_HARD, SOURCE_SOFT, Block, CellList, DFTSurface, ExcitationFunction,
                       FarFieldSurface, FrequencyOutputVolume, HuygensBox, HuygensOuter, HuygensPlane, OutputPoint,
                       OutputSurface, OutputVolume, PointExcitation, PowerSurface, ProblemSpec, RCSSurface, SARVolume,
-                      SurfaceSheet, UnsupportedFeature, VolumeMaterial, Z0, _region_mask, nint)
+                      SurfaceMaterial, SurfaceSheet, UnsupportedFeature, VolumeMaterial, Z0, _region_mask, nint)
 
 GEOMETRY_PACKETS = ["periodic_boundary", "mesh_outer_boundary_dimension", "mesh_dimensions_in_cells",
                     "mesh_cell_dimension", "volume_list", "surface_list", "line_list", "point_list", "pml",
@@ -419,11 +419,14 @@ def _samples(lines: Sequence[str], n_ignore: int, n_time: int, n_value: int) -> 
 
 def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
              open_file: Optional[Callable[[str], Sequence[str]]] = None,
-             mesh_file: Optional[MeshFile] = None) -> InpProblem:
+             mesh_file: Optional[MeshFile] = None,
+             thin_layer: Optional[Callable[[str, bool], SurfaceMaterial]] = None) -> InpProblem:
     """The ProblemSpec of a .inp file's lines; ``material(name)`` returns the
     volume material of a dispersive Volume_material_list entry, ``name``
     being the file name line as written (the reference opens name + '.vmat');
-    ``open_file(name)`` returns the lines of an excitation function's data file.
+    ``open_file(name)`` returns the lines of an excitation function's data file;
+    ``thin_layer(name, anisotropic)`` the thin layer of a dispersive surface
+    material entry (the reference opens name + '.smat').
 
     ``mesh_file`` is the problem's NAME.mesh as the reference's mesher wrote
     it (``meshfile.read_mesh``).  With it the geometry is the mesher's, as
@@ -669,7 +672,7 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
                                                     **_steps(_timing(r, dt))))
     _read_outputs(rec, mesh, dt, spec, surface_geo, volume_block, post := {})
     if "surface_material_list" in rec:
-        _read_surface_materials(rec["surface_material_list"], mesh, spec, surfaces, mesh_file)
+        _read_surface_materials(rec["surface_material_list"], mesh, spec, surfaces, mesh_file, thin_layer)
     if "set_small_to_zero" in rec:  # read_small_to_zero.F90:55-59
         r = rec["set_small_to_zero"]
         spec.small_to_zero = (r.ints(1)[0], r.values(1)[0])
@@ -813,37 +816,63 @@ def _material_block(spec: ProblemSpec, m: int):
 
 
 def _read_surface_materials(r: Records, mesh: Mesh, spec: ProblemSpec, surfaces: Dict[int, Shape],
-                            mesh_file: Optional[MeshFile] = None) -> None:
-    """read_surface_material_list.F90:111-470 for PEC, PMC and free-space
-    surfaces: number, type, the number of surfaces, their numbers and their
-    orientations (which a symmetric sheet does not use).  A box surface
-    becomes its six boundary planes; with a mesh file every surface is its
-    face list, whatever its shape."""
-    names = {"pec": "PEC", "pmc": "PMC", "free_space": "free"}
+                            mesh_file: Optional[MeshFile] = None,
+                            thin_layer: Optional[Callable[[str, bool], SurfaceMaterial]] = None) -> None:
+    """read_surface_material_list.F90:111-470 for PEC, PMC, free-space and
+    dispersive (isotropic or anisotropic thin-layer) surfaces: number, type,
+    for a thin layer the name of its .smat file, the number of surfaces,
+    their numbers and their orientations (+1 or -1).  A box surface becomes
+    its six boundary planes; with a mesh file every surface is its face
+    list, whatever its shape.  ``thin_layer(name, anisotropic)`` returns the
+    layer a .smat file describes.
+
+    A thin layer's orientation matters: set_surface_material_mesh
+    (TLM_surface_materials.F90:150-175) gives each face the orientation's
+    sign when the surface records the face as the min face of a cell and the
+    opposite sign when it records it as the max face of the cell below."""
+    names = {"pec": "PEC", "pmc": "PMC", "free_space": "free", "dispersive": "dispersive",
+             "anisotropic_dispersive": "dispersive"}
     for _ in _numbered(r, "surface materials"):
         kind = r.text()
         if kind not in names:
-            raise UnsupportedFeature(f"surface material {kind!r}: only PEC, PMC and free-space surfaces")
+            raise UnsupportedFeature(f"surface material {kind!r}: only PEC, PMC, free-space and dispersive "
+                                     "surfaces")
+        material = 0
+        if names[kind] == "dispersive":
+            name = r.line().strip()
+            if thin_layer is None:
+                raise UnsupportedFeature(f"thin-layer material {name!r}: no surface material file resolver")
+            spec.thin_layers.append(thin_layer(name, kind == "anisotropic_dispersive"))
+            material = len(spec.thin_layers)
         n = r.ints(1)[0]
         nums = r.ints(n)
-        r.ints(n)  # orientations
-        for num in nums:
+        signs = r.ints(n)
+        if any(v not in (1, -1) for v in signs):
+            raise ValueError("surface_material_list packet: orientations must be +1 or -1")
+        for num, sg in zip(nums, signs):
             if mesh_file is not None:
                 if not 1 <= num <= len(mesh_file.surfaces):
                     raise ValueError(f"surface {num} is not in the mesh file")
-                faces = connect_faces(mesh_file, mesh_file.surfaces[num - 1].faces, f"surface {num}")
-                spec.surface_sheets.append(SurfaceSheet(names[kind], 0, 0, (0, 0), (0, 0), faces=faces))
+                rec = mesh_file.surfaces[num - 1].faces
+                faces = connect_faces(mesh_file, rec, f"surface {num}")
+                fs = [sg if code <= 3 else -sg for code in rec[:, 3].tolist()]
+                spec.surface_sheets.append(SurfaceSheet(names[kind], 0, 0, (0, 0), (0, 0), faces=faces,
+                                                        material=material, sign=fs))
                 continue
-            geo, _ = _surface_geo(mesh, surfaces[num], "a surface material", 1)
+            geo, orient = _surface_geo(mesh, surfaces[num], "a surface material", 1)
             if "plane" in geo:
                 ax, ix, r0, r1 = geo["plane"]
-                spec.surface_sheets.append(SurfaceSheet(names[kind], ax, ix, r0, r1))
+                spec.surface_sheets.append(SurfaceSheet(names[kind], ax, ix, r0, r1, material=material,
+                                                        sign=sg * orient))
             else:
                 (i0, i1), (j0, j1), (k0, k1) = geo["box"]
-                for ax, ix, r0, r1 in ((1, i0 - 1, (j0, j1), (k0, k1)), (1, i1, (j0, j1), (k0, k1)),
-                                       (2, j0 - 1, (i0, i1), (k0, k1)), (2, j1, (i0, i1), (k0, k1)),
-                                       (3, k0 - 1, (i0, i1), (j0, j1)), (3, k1, (i0, i1), (j0, j1))):
-                    spec.surface_sheets.append(SurfaceSheet(names[kind], ax, ix, r0, r1))
+                # the block's faces sit on the outside cells: max faces of the cells before its min
+                # planes, min faces of the cells past its max planes
+                for ax, ix, r0, r1, rs in ((1, i0 - 1, (j0, j1), (k0, k1), -1), (1, i1, (j0, j1), (k0, k1), 1),
+                                           (2, j0 - 1, (i0, i1), (k0, k1), -1), (2, j1, (i0, i1), (k0, k1), 1),
+                                           (3, k0 - 1, (i0, i1), (j0, j1), -1), (3, k1, (i0, i1), (j0, j1), 1)):
+                    spec.surface_sheets.append(SurfaceSheet(names[kind], ax, ix, r0, r1, material=material,
+                                                            sign=sg * rs))
 
 
 # the packets that only ask for results; read_inp_lenient may leave them out
@@ -855,7 +884,8 @@ OUTPUT_PACKETS = {"output_point_list", "output_surface_list", "output_volume_lis
 
 def read_inp_lenient(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
                      open_file: Optional[Callable[[str], Sequence[str]]] = None,
-                     mesh_file: Optional[MeshFile] = None) -> InpProblem:
+                     mesh_file: Optional[MeshFile] = None,
+                     thin_layer: Optional[Callable[[str, bool], SurfaceMaterial]] = None) -> InpProblem:
     """read_inp, leaving out each output packet that read_inp refuses (a
     result the GPU path cannot produce exactly, such as an output surface on
     rotated geometry) and listing it in ``skipped`` as "<packet>: <reason>".
@@ -874,11 +904,11 @@ def read_inp_lenient(lines: Sequence[str], material: Callable[[str], VolumeMater
     dropped = []
     for name in [n for n, _ in packets if n in OUTPUT_PACKETS]:
         try:
-            read_inp(text(core | {name}), material, open_file, mesh_file)
+            read_inp(text(core | {name}), material, open_file, mesh_file, thin_layer)
         except UnsupportedFeature as e:
             dropped.append(f"{name}: {e}")
     keep = core | {n for n, _ in packets if n in OUTPUT_PACKETS and not any(d.startswith(n + ":") for d in dropped)}
-    p = read_inp(text(keep), material, open_file, mesh_file)
+    p = read_inp(text(keep), material, open_file, mesh_file, thin_layer)
     p.skipped.extend(dropped)
     return p
 
@@ -888,6 +918,13 @@ def vmat_in(directory: str) -> Callable[[str], VolumeMaterial]:
     from .vmat import read_vmat
 
     return lambda name: read_vmat(os.path.join(directory, name + ".vmat"))
+
+
+def smat_in(directory: str) -> Callable[[str, bool], SurfaceMaterial]:
+    """A thin-layer resolver reading ``<directory>/<name>.smat``."""
+    from .smat import read_smat
+
+    return lambda name, anisotropic: read_smat(os.path.join(directory, name + ".smat"), anisotropic)
 
 
 def read_inp_file(path: str, material: Optional[Callable[[str], VolumeMaterial]] = None,
@@ -912,4 +949,5 @@ def read_inp_file(path: str, material: Optional[Callable[[str], VolumeMaterial]]
         with open(os.path.join(directory, name), encoding="latin-1") as g:
             return g.read().splitlines()
 
-    return (read_inp_lenient if lenient else read_inp)(lines, material or vmat_in(directory), open_file, mesh_file)
+    return (read_inp_lenient if lenient else read_inp)(lines, material or vmat_in(directory), open_file, mesh_file,
+                                                      smat_in(directory))

@@ -245,6 +245,41 @@ class VolumeMaterial:
         return VolumeMaterial(MAT_DISPERSIVE, Sfilter(wnorm, num, den), sigma, Sfilter(wnorm, [1.0], [1.0]), 0.0)
 
 
+@dataclass
+class SurfaceMaterial:
+    """A dispersive thin layer (surface_material_type_DISPERSIVE or
+    ANISOTROPIC_DISPERSIVE, TLM_MODULES/TLM_material_modules.F90): the
+    S-domain two-port impedance filters ``z[pol][k]`` for the x, y and z
+    polarisations (pol 0..2), k = 0..3 for Z11, Z12, Z21, Z22."""
+
+    z: List[List[Sfilter]]
+
+
+def surface_material_coefficients(sm: SurfaceMaterial, dt: float) -> dict:
+    """calculate_surface_material_filter_coefficients
+    (MATERIALS/TLM_surface_materials.F90:225-280): every filter through the
+    bilinear transform and the fast/slow decomposition.  Returns f [3][4]
+    (the fast parts), a, b [3][4][MAX_ORDER+1] (the slow Z filters, b(0)
+    kept) and order [3][4]."""
+    MO = MAX_ORDER + 1
+    f = np.zeros((3, 4))
+    a = np.zeros((3, 4, MO))
+    b = np.zeros((3, 4, MO))
+    order = np.zeros((3, 4), dtype=np.int32)
+    for p in range(3):
+        for k in range(4):
+            za, zb = bilinear_s_to_z(sm.z[p][k], dt)
+            ff, sa, sb = z_fast_slow_decomposition(za, zb)
+            o = len(sb) - 1
+            if o > MAX_ORDER:
+                raise UnsupportedFeature(f"thin-layer filter of order {o} (at most {MAX_ORDER})")
+            f[p, k] = ff
+            a[p, k, :o + 1] = sa
+            b[p, k, :o + 1] = sb
+            order[p, k] = o
+    return dict(f=f, a=a, b=b, order=order)
+
+
 def material_coefficients(mat: VolumeMaterial, dl: float, dt: float, reduced_c: float = 1.0):
     """calculate_volume_material_filter_coefficients,
     MATERIALS/TLM_volume_materials.F90:190-385 (bilinear warp, frequency_scale=1)."""
@@ -592,8 +627,9 @@ class RCSSurface:
 
 RCS_POINTS_PER_CELL = 2  # n_rcs_points_per_cell, TLM_MODULES/TLM_output_modules.F90:388
 
-# surface_material_type_*, TLM_MODULES/TLM_material_modules.F90:153-159
-SURFACE_SHEET_TYPES = {"PEC": 1, "PMC": 2, "free": 4}
+# surface_material_type_*, TLM_MODULES/TLM_material_modules.F90:153-161; a
+# dispersive and an anisotropic dispersive layer take the same update
+SURFACE_SHEET_TYPES = {"PEC": 1, "PMC": 2, "dispersive": 3, "free": 4}
 
 
 @dataclass
@@ -614,11 +650,24 @@ class SurfaceSheet:
     # + side, axis) per face, e.g. a triangulated surface as the reference's
     # mesher put it on cell faces (read from a mesh file)
     faces: Optional[List[Tuple[Tuple[int, int, int], int]]] = None
+    # a "dispersive" sheet: its thin-layer material (1-based into
+    # ProblemSpec.thin_layers) and, per face (or one value for all), the
+    # sign set_surface_material_mesh (TLM_surface_materials.F90:150-175)
+    # gives the face's min-face entry: the orientation list's sign, negated
+    # where the surface records the max face of the cell below.  The
+    # connect treats the layer as reversed where the sign is positive
+    # (connect_normal_to_x.F90:14-19).
+    material: int = 0
+    sign: object = 1
 
     def face_keys(self):
         if self.faces is not None:
             return list(self.faces)
         return [(f, self.axis) for f in _plane_faces(self.axis, self.index, self.r0, self.r1)]
+
+    def face_signs(self) -> List[int]:
+        n = len(self.face_keys())
+        return [int(v) for v in self.sign] if isinstance(self.sign, (list, tuple)) else [int(self.sign)] * n
 
 
 @dataclass
@@ -772,6 +821,7 @@ class ProblemSpec:
     frequency_output_volumes: List[FrequencyOutputVolume] = field(default_factory=list)
     output_surfaces: List[OutputSurface] = field(default_factory=list)
     surface_sheets: List[SurfaceSheet] = field(default_factory=list)
+    thin_layers: List[SurfaceMaterial] = field(default_factory=list)  # materials of the "dispersive" sheets
     rcs_surface: Optional[RCSSurface] = None
     power_surfaces: List[PowerSurface] = field(default_factory=list)
     mode_outputs: List[ModeOutput] = field(default_factory=list)
@@ -1177,12 +1227,16 @@ def build_tables(spec: ProblemSpec) -> dict:
     for fl in dft_faces:
         for c, code in fl:
             face_out[connect_key(c, code)] = True
-    face_mat = {}
+    face_mat, face_smat = {}, {}
     for sh in spec.surface_sheets:
         if sh.kind not in SURFACE_SHEET_TYPES:
-            raise UnsupportedFeature(f"surface material {sh.kind!r}: only PEC, PMC and free-space sheets")
-        for key in sh.face_keys():
+            raise UnsupportedFeature(f"surface material {sh.kind!r}: only PEC, PMC, free-space and dispersive "
+                                     "sheets")
+        if sh.kind == "dispersive" and not 1 <= sh.material <= len(spec.thin_layers):
+            raise ValueError(f"dispersive sheet: thin-layer material {sh.material} is not defined")
+        for key, sg in zip(sh.face_keys(), sh.face_signs()):  # the last sheet on a face wins
             face_mat[key] = SURFACE_SHEET_TYPES[sh.kind]
+            face_smat[key] = sg * sh.material if sh.kind == "dispersive" else 0
     keys = set(face_exc) | set(face_out) | set(face_mat)
     for (c, axis) in keys:
         if c[axis - 1] <= 1 or c[axis - 1] > (nx, ny, nz)[axis - 1]:
@@ -1219,6 +1273,16 @@ def build_tables(spec: ProblemSpec) -> dict:
         if COMPONENTS[q.component] > 6:
             raise ValueError("a face output point records E or H (components 1..6)")
     tables["face_mat"] = np.array([face_mat.get(k, 0) for k in ordered], dtype=np.int32)
+    # thin layers: the signed material per special face (positive: reversed)
+    # and the filters of every thin-layer material
+    tables["face_smat"] = np.array([face_smat.get(k, 0) for k in ordered], dtype=np.int32)
+    MOs = MAX_ORDER + 1
+    smc = [surface_material_coefficients(sm, dt) for sm in spec.thin_layers]
+    tables.update(n_smat=len(smc),
+                  smat_f=np.array([c["f"] for c in smc], dtype=np.float64).reshape(-1, 3, 4),
+                  smat_a=np.array([c["a"] for c in smc], dtype=np.float64).reshape(-1, 3, 4, MOs),
+                  smat_b=np.array([c["b"] for c in smc], dtype=np.float64).reshape(-1, 3, 4, MOs),
+                  smat_order=np.array([c["order"] for c in smc], dtype=np.int32).reshape(-1, 3, 4))
     tables.update(n_faces=len(ordered), face_cx=np.array(face_cx, dtype=np.int32),
                   face_cy=np.array(face_cy, dtype=np.int32), face_cz=np.array(face_cz, dtype=np.int32),
                   face_dir=np.array(face_dir, dtype=np.int32), face_exc=np.array(face_e, dtype=np.int32),

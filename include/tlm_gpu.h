@@ -128,11 +128,31 @@ int tlm_gpu_set_faces(int64_t handle, int32_t n_faces, const int32_t *cx, const 
 /* Surface materials on the special faces, in set_faces order
    (face_update_code_to_material_data, connect_normal_to_x.F90:20-52 and the
    y, z analogues): 0 none, 1 PEC (surface_material_type_PEC: each side
-   reflects its own pulse with -1), 2 PMC (+1), 4 free space (the plain
-   connect).  Other surface material types (thin layers, dispersive, switches,
-   diodes, spice ports) are rejected with TLM_E_UNSUPPORTED at the first run.
+   reflects its own pulse with -1), 2 PMC (+1), 3 a dispersive thin layer
+   (tlm_gpu_set_thin_layers, tlm_gpu_set_face_thin_layers), 4 free space
+   (the plain connect).  Other surface material types (switches, diodes,
+   spice ports) are rejected with TLM_E_UNSUPPORTED at the first run.
    Without this call no special face carries a material. */
 int tlm_gpu_set_face_materials(int64_t handle, int32_t n_faces, const int32_t *type);
+
+/* Dispersive thin layers (surface material types DISPERSIVE and
+   ANISOTROPIC_DISPERSIVE; replaces calculate_surface_material_filter_
+   coefficients, MATERIALS/TLM_surface_materials.F90:225-280, whose results
+   the Fortran driver passes here).  n materials; for material i,
+   polarisation p (x, y, z) and filter k (Z11, Z12, Z21, Z22), entry
+   e = (i*3 + p)*4 + k: the fast part f[e], the slow Z filter's
+   coefficients a[e*stride .. e*stride+order[e]] and b[...] (b(0) != 0).
+   Orders above 8 and impedance matrices that surface_material_update
+   could not solve are rejected. */
+int tlm_gpu_set_thin_layers(int64_t handle, int32_t n, const double *f, const double *a, const double *b,
+                            const int32_t *order, int32_t stride);
+
+/* Per special face (tlm_gpu_set_faces order) the signed thin-layer
+   material, face_update_code_to_material_data(:,1) of a thin-layer face:
+   0 none, +m material m with the layer reversed, -m not reversed
+   (connect_normal_to_x.F90:14-19).  A face with a thin layer has surface
+   material type 3 in tlm_gpu_set_face_materials. */
+int tlm_gpu_set_face_thin_layers(int64_t handle, int32_t n, const int32_t *material);
 
 /* Huygens surface (SRC/EXCITATION/huygens_surface.F90:247-848): per patch
    the face excitation number, normal (3 ints) and offset; the incident

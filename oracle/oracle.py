@@ -52,6 +52,8 @@ class _Problem(C.Structure):
         ("hs_outer", C.c_int32), ("hs_cell", _i32p),
         ("n_ff", C.c_int32), ("ff_freq", _f64p), ("ff_face_ptr", _i32p), ("ff_face_out", _i32p),
         ("ff_face_code", _i32p), ("face_mat", _i32p),
+        ("face_smat", _i32p), ("n_smat", C.c_int32), ("smat_f", _f64p), ("smat_a", _f64p), ("smat_b", _f64p),
+        ("smat_order", _i32p),
     ]
 
 
@@ -138,6 +140,12 @@ class Oracle:
             setattr(p, k, arr(k, np.int32) if k in t else arr_empty())
         if "face_mat" in t and np.any(np.asarray(t["face_mat"]) != 0):
             p.face_mat = arr("face_mat", np.int32)  # else NULL: no surface materials
+        if int(t.get("n_smat", 0)):
+            p.face_smat = arr("face_smat", np.int32)
+            p.n_smat = int(t["n_smat"])
+            for k in ("smat_f", "smat_a", "smat_b"):
+                setattr(p, k, arr(k, np.float64))
+            p.smat_order = arr("smat_order", np.int32)
         for k in ("fpt_face", "fpt_comp", "fpt_fn", "fpt_type", "fprobe_face", "fprobe_side", "fprobe_comp",
                   "hs_cell"):
             setattr(p, k, arr(k, np.int32) if k in t else arr_empty())

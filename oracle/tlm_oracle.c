@@ -81,6 +81,10 @@ struct tlm_oracle_state {
      sequential traversal */
   int threads;
   int32_t *plane_out0, *plane_exc0, *plane_fexc0, *plane_fout0;
+  /* thin-layer filter responses: per special face two polarisations of
+     four filters (Z11, Z12, Z21, Z22), allocate_surface_material_filter_data */
+  zresp_t *sm_f;
+  int err;
 };
 
 #define VIDX(s, port, cx, cy, cz) \
@@ -178,6 +182,15 @@ tlm_oracle_state *tlm_oracle_create(const tlm_oracle_problem *p) {
     size_t cell = ((size_t)(p->face_cz[f] - 1) * p->ny + (p->face_cy[f] - 1)) * p->nx + (p->face_cx[f] - 1);
     s->face_code[cell * 3 + (p->face_dir[f] - 1)] = f + 1;
   }
+  s->sm_f = (zresp_t *)calloc((size_t)p->n_faces * 8 + 1, sizeof(zresp_t));
+  for (int f = 0; f < p->n_faces; f++) {
+    int sm = p->face_smat ? p->face_smat[f] : 0;
+    if (!sm || !p->face_mat || p->face_mat[f] != 3) continue;
+    int m = abs(sm) - 1, d = p->face_dir[f];
+    int pols[2] = {d == 1 ? 1 : 0, d == 3 ? 1 : 2}; /* x faces: y, z; y faces: x, z; z faces: x, y */
+    for (int q = 0; q < 2; q++)
+      for (int k = 0; k < 4; k++) s->sm_f[((size_t)f * 2 + q) * 4 + k].order = p->smat_order[(m * 3 + pols[q]) * 4 + k];
+  }
   s->threads = 1;
   s->plane_out0 = (int32_t *)calloc((size_t)p->nz + 1, sizeof(int32_t));
   s->plane_exc0 = (int32_t *)calloc((size_t)p->nz + 1, sizeof(int32_t));
@@ -221,6 +234,7 @@ void tlm_oracle_destroy(tlm_oracle_state *s) {
   free(s->cell_exc); free(s->cell_exc_type); free(s->cell_out); free(s->face_exc);
   free(s->face_exc_type); free(s->face_out); free(s->face_code); free(s->dft);
   free(s->plane_out0); free(s->plane_exc0); free(s->plane_fexc0); free(s->plane_fout0);
+  free(s->sm_f);
   free(s);
 }
 
@@ -837,6 +851,42 @@ static int scatter(tlm_oracle_state *s) {
   return run_planes(s, 0);
 }
 
+/* surface_material_update (MATERIALS/TLM_surface_materials.F90:535-697):
+   a thin layer as a two-port impedance matrix between the incident pulses
+   from the left (the cell below the face) and the right; both sides see
+   the line impedance Z0.  flt: the four filter responses Z11, Z12, Z21, Z22
+   of this face and polarisation.  Returns -3 when the matrix is singular
+   (the reference stops there). */
+static int thin_layer_update(const tlm_oracle_problem *p, int m, int pol, int reverse, zresp_t *flt, double Vli,
+                             double Vri, double *Vl, double *Vr) {
+  const int MO = ORACLE_MAX_ORDER + 1, base = (m * 3 + pol) * 4;
+  const double *f = p->smat_f + base;
+  double slow[4];
+  for (int k = 0; k < 4; k++) {
+    evaluate_Zfilter(p->smat_a + (size_t)(base + k) * MO, p->smat_b + (size_t)(base + k) * MO, &flt[k], 0.0);
+    slow[k] = flt[k].f;
+  }
+  double Zl = Z0, Zr = Z0;
+  double Z1 = reverse ? Zr : Zl, Z2 = reverse ? Zl : Zr;
+  double U11 = Z1 + f[0], U12 = f[1], U21 = f[2], U22 = Z2 + f[3];
+  double det = U11 * U22 - U21 * U12;
+  if (det == 0.0) return -3;
+  double V1i = reverse ? Vri : Vli, V2i = reverse ? Vli : Vri;
+  double rhs1 = 2.0 * V1i - slow[0] - slow[1];
+  double rhs2 = 2.0 * V2i - slow[2] - slow[3];
+  double i1 = (U22 * rhs1 - U12 * rhs2) / det;
+  double i2 = (-U21 * rhs1 + U11 * rhs2) / det;
+  double V1 = 2.0 * V1i - i1 * Z1;
+  double V2 = 2.0 * V2i - i2 * Z2;
+  const double G[4] = {i1, i2, i1, i2};
+  for (int k = 0; k < 4; k++)
+    evaluate_Zfilter(p->smat_a + (size_t)(base + k) * MO, p->smat_b + (size_t)(base + k) * MO, &flt[k], G[k]);
+  *Vl = reverse ? V2 : V1;
+  *Vr = reverse ? V1 : V2;
+  for (int k = 0; k < 4; k++) timeshift_Zfilter(&flt[k]);
+  return 0;
+}
+
 /* one special face of connect(): connect_normal_to_{x,y,z}.F90 for faces
    with no surface material (material_type 0), face excitation and face output.
    pa/pb are the two port pairs (min port on cell c, max port on cell c-1). */
@@ -861,6 +911,14 @@ static void connect_special_face(tlm_oracle_state *s, int f, int cx, int cy, int
   } else if (mat == 2) { /* PMC sheet: connect_normal_to_x.F90:41-45 */
     A_min = 2.0 * V_(pmin1, cx, cy, cz); A_max = 2.0 * V_(pmax1, mx, my, mz);
     B_min = 2.0 * V_(pmin2, cx, cy, cz); B_max = 2.0 * V_(pmax2, mx, my, mz);
+  } else if (mat == 3) { /* thin layer: connect_normal_to_x.F90:268-282 (y, z analogues) */
+    int sm = p->face_smat[f], m = abs(sm) - 1;
+    int pol1 = dir == 1 ? 1 : 0, pol2 = dir == 3 ? 1 : 2;
+    zresp_t *flt = s->sm_f + (size_t)f * 8;
+    int rc = thin_layer_update(p, m, pol1, sm > 0, flt, V_(pmax1, mx, my, mz), V_(pmin1, cx, cy, cz), &A_max, &A_min);
+    if (!rc) rc = thin_layer_update(p, m, pol2, sm > 0, flt + 4, V_(pmax2, mx, my, mz), V_(pmin2, cx, cy, cz),
+                                    &B_max, &B_min);
+    if (rc) s->err = rc;
   } /* 0 and 4 (free-space surface material): the plain sum */
   if (exc != 0) {
     const double *fmin = s->face_exc + (size_t)(*excitation_face_number) * 24;
@@ -1130,6 +1188,7 @@ int tlm_oracle_run(tlm_oracle_state *s, int32_t first_step, int32_t n_steps, dou
       memcpy(cell_out + (size_t)k * p->n_out_cells * 6, s->cell_out, sizeof(double) * p->n_out_cells * 6);
     time = time + p->dt / 2.0;
     connect(s);
+    if (s->err) return s->err;
     /* face_output_points (output_points.F90:255-444): side 1/2 of the output face */
     for (int q = 0; q < p->n_face_probes; q++)
       s->face_probe_rec[(size_t)(timestep - 1) * p->n_face_probes + q] =

@@ -136,6 +136,18 @@ typedef struct {
      (surface_material_type_*, TLM_MODULES/TLM_material_modules.F90:153-159);
      NULL: no surface materials */
   const int32_t *face_mat;
+
+  /* thin layers on the special faces whose face_mat is 3 (surface material
+     types DISPERSIVE and ANISOTROPIC_DISPERSIVE): per special face the
+     signed thin-layer material number (1-based; positive: the layer is
+     reversed, connect_normal_to_x.F90:14-19), and per material the fast
+     parts f[3][4], the slow Z filters a, b [3][4][ORACLE_MAX_ORDER+1] and
+     their orders [3][4] for the x, y, z polarisations and Z11, Z12, Z21,
+     Z22 (TLM_surface_materials.F90:225-280) */
+  const int32_t *face_smat;
+  int32_t n_smat;
+  const double *smat_f, *smat_a, *smat_b;
+  const int32_t *smat_order;
 } tlm_oracle_problem;
 
 typedef struct tlm_oracle_state tlm_oracle_state;

@@ -25,6 +25,11 @@ CASES = {
     # from another delay (its pulse peaks 4.8 ns later than the input's) and is not used
     "excitation_test_Ex": "EXCITATION_FUNCTION_TEST/PROBLEM_SPECIFICATION_FILES/excitation_test.field.tout_ref",
     "power_calc_Ex": "POWER_CALCS/PROBLEM_SPECIFICATION_FILES/power_calc.field.tout_ref",
+    # thin layers (dispersive and anisotropic dispersive surface materials)
+    "tem_thin_layer": "TEM_THIN_LAYER_TEST/PROBLEM_SPECIFICATION_FILES/Ey.tout_ref",
+    **{f"tem_{a.lower()}_aniso_{p.lower()}": f"TEM_{a}_ANISOTROPIC_THIN_LAYER_{p}_POL_TEST/PROBLEM_SPECIFICATION_FILES/Ey.tout_ref"
+       for a, p in (("X", "Y"), ("X", "Z"), ("Y", "X"), ("Y", "Z"), ("Z", "X"), ("Z", "Y"))},
+    "thin_layer_stability": "THIN_LAYER_STABILITY_TEST/PROBLEM_SPECIFICATION_FILES/cavity.field.tout_ref",
 }
 
 
@@ -49,7 +54,13 @@ INP_CASES = {
     "power_calc": "POWER_CALCS/PROBLEM_SPECIFICATION_FILES/power_calc.inp",
     "helix": "HELIX_ANTENNA/helix.inp",
     "rcs_plate": "RCS_PEC_PLATE_ROUGH_SURFACE/PROBLEM_SPECIFICATION_FILES/plate.inp",
+    "tem_thin_layer": "TEM_THIN_LAYER_TEST/PROBLEM_SPECIFICATION_FILES/TEM_cell.inp",
+    **{f"tem_{a.lower()}_aniso_{p.lower()}": f"TEM_{a}_ANISOTROPIC_THIN_LAYER_{p}_POL_TEST/PROBLEM_SPECIFICATION_FILES/TEM_cell.inp"
+       for a, p in (("X", "Y"), ("X", "Z"), ("Y", "X"), ("Y", "Z"), ("Z", "X"), ("Z", "Y"))},
+    "thin_layer_stability": "THIN_LAYER_STABILITY_TEST/PROBLEM_SPECIFICATION_FILES/cavity.inp",
 }
+# the surface material files the thin-layer cases use, as text
+SMAT_CASES = ["Dispersive_sheet", "Anisotropic_sheet"]
 # result files the solver writes after the run (write_SAR_volumes), as text
 RESULT_CASES = {
     "sar_test": "SAR_TEST/PROBLEM_SPECIFICATION_FILES/SAR_test.SAR.fout_ref",
@@ -103,6 +114,12 @@ def main():
             vm[name] = np.array(f.read().splitlines())
     np.savez_compressed(os.path.join(here, "vmat_text.npz"), **vm)
     print("vmat_text", sorted(vm))
+    sm = {}
+    for name in SMAT_CASES:
+        with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", "MATERIAL_DATA", name + ".smat")) as f:
+            sm[name] = np.array(f.read().splitlines())
+    np.savez_compressed(os.path.join(here, "smat_text.npz"), **sm)
+    print("smat_text", sorted(sm))
     inp = {}
     for name, rel in INP_CASES.items():
         with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", rel), encoding="latin-1") as f:

@@ -314,8 +314,10 @@ Ez
      "type 'sphere'"),                                                                      # not voxelised here
     ("Volume_list\n1\n1\nrectangular_block\n0.5 0.5 0.5\n0 0 0\n0.5 0.5 0.5\nVolume_material_list\n1\n1\nPEC\n1\n1\n",
      "centre lies on"),                                                                      # a face through centres
+    ("Surface_list\n1\n1\nrectangle\n1.0 1.0\n0 0 0\n0.5 0.5 0.5\nSurface_material_list\n1\n1\nDIODE\n"
+     "1e-14 0.025 1.0 1e-12 +x\n1\n1\n1\n", "surface material 'diode'"),
     ("Surface_list\n1\n1\nrectangle\n1.0 1.0\n0 0 0\n0.5 0.5 0.5\nSurface_material_list\n1\n1\nDISPERSIVE\n"
-     "MATERIAL_DIRECTORY/sheet\n1\n1\n1\n", "surface material 'dispersive'"),
+     "MATERIAL_DIRECTORY/sheet\n1\n1\n1\n", "no surface material file resolver"),
     ("Cable_list\n0\n", "cable_list packet"),
     ("Output_mode_list\n0\n", "ModeOutput"),
     ("Frequency_scale_flag\nT\n2.0\n", "frequency scale"),
