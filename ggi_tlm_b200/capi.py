@@ -45,7 +45,7 @@ EXPORTS = [
     "tlm_gpu_set_output_volumes", "tlm_gpu_fetch_output_volumes", "tlm_gpu_set_sar_volumes",
     "tlm_gpu_fetch_sar_volumes", "tlm_gpu_set_power_surfaces", "tlm_gpu_fetch_power_surfaces",
     "tlm_gpu_set_mode_outputs", "tlm_gpu_fetch_mode_outputs", "tlm_gpu_set_face_materials",
-    "tlm_gpu_set_thin_layers", "tlm_gpu_set_face_thin_layers",
+    "tlm_gpu_set_thin_layers", "tlm_gpu_set_face_thin_layers", "tlm_gpu_set_wrap",
 ]
 
 
@@ -125,6 +125,7 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_face_materials": [i64, i32, _i32p],
         "tlm_gpu_set_thin_layers": [i64, i32, _f64p, _f64p, _f64p, _i32p, i32],
         "tlm_gpu_set_face_thin_layers": [i64, i32, _i32p],
+        "tlm_gpu_set_wrap": [i64, i32, i32, i32],
         "tlm_gpu_fetch_mode_outputs": [i64, i32, i32, _f64p],
         "tlm_gpu_set_small_to_zero": [i64, i32, C.c_double],
         "tlm_gpu_set_dft": [i64, i32, _f64p, _i32p, _i32p, _i32p, _i32p],
@@ -250,6 +251,9 @@ class GpuMesh:
         if fm is not None and np.any(np.asarray(fm) != 0):
             fmv = _i32(fm)
             _check(lib.tlm_gpu_set_face_materials(self.h, int(t["n_faces"]), _p(fmv)))
+        if np.any(np.asarray(t.get("wrap", (0, 0, 0))) != 0):
+            w = [int(v) for v in t["wrap"]]
+            _check(lib.tlm_gpu_set_wrap(self.h, w[0], w[1], w[2]))
         if int(t.get("n_smat", 0)):
             sf, sa, sb, so = _f64(t["smat_f"]), _f64(t["smat_a"]), _f64(t["smat_b"]), _i32(t["smat_order"])
             _check(lib.tlm_gpu_set_thin_layers(self.h, int(t["n_smat"]), _p(sf), _p(sa), _p(sb), _p(so),

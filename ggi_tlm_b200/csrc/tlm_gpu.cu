@@ -249,6 +249,7 @@ struct Mesh {
   std::vector<int32_t> f_cx, f_cy, f_cz, f_dir, f_exc, f_out;
   std::vector<int32_t> f_mat;  // surface material per special face (empty: none)
   std::vector<int32_t> f_smat;  // signed thin-layer material per special face (empty: none)
+  int wrap = 0;                 // wrapping boundaries: bit 0 x, bit 1 y, bit 2 z
   std::vector<tlm::ThinLayerDev> thin;  // thin-layer materials
   // point sources on faces (excitation face number, component 1..12, function, type)
   std::vector<int32_t> fpt_face, fpt_comp, fpt_fn, fpt_type;
@@ -413,6 +414,7 @@ tlm::MeshDev<T> mesh_dev(Mesh *m) {
   d.dl = m->desc.dl;
   d.dt = m->desc.dt;
   d.d_base = (const int *)m->d_base.p;
+  d.wrap = m->wrap;
   return d;
 }
 
@@ -1011,6 +1013,8 @@ int finalize(Mesh *m) {
     }
     if ((rc = upload(m, m->value_face, vf))) return rc;
     // outer-boundary Huygens patches
+    if (m->hs_outer && m->wrap)  // its terms would go to the slots before the wrap moves them
+      return fail(TLM_E_UNSUPPORTED, "an outer-boundary Huygens surface with wrapping boundaries");
     if (m->hs_outer) {
       std::vector<int4> of(std::max(m->hs_n, 1));
       for (int h = 0; h < m->hs_n; h++) {
@@ -1770,6 +1774,16 @@ int tlm_gpu_set_thin_layers(int64_t h, int32_t n, const double *f, const double 
         if (U11 * U22 - d.f[p][2] * d.f[p][1] == 0.0)
           return fail(TLM_E_BADARG, "thin layer %d: singular impedance matrix", i + 1);
       }
+  return TLM_OK;
+}
+
+int tlm_gpu_set_wrap(int64_t h, int32_t wrap_x, int32_t wrap_y, int32_t wrap_z) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  for (int v : {wrap_x, wrap_y, wrap_z})
+    if (v != 0 && v != 1) return fail(TLM_E_BADARG, "wrapping flags must be 0 or 1");
+  m->wrap = wrap_x | (wrap_y << 1) | (wrap_z << 2);
   return TLM_OK;
 }
 

@@ -131,7 +131,57 @@ struct MeshDev {
   int n_out, n_hist;
   double dl, dt;
   const int *d_base;        // device step counter (1-based step of relative step 0)
+  int wrap;                 // wrapping boundaries: bit 0 x, bit 1 y, bit 2 z (wrap_outer_boundary.F90)
 };
+
+// The ghost slot a boundary cell writes: R times its reflected pulse on a
+// boundary port, where the neighbour across that boundary pulls it next
+// step.  Without wrapping that is the cell itself (outer_boundary.F90:
+// 71-131: the port keeps R times its pulse); with wrapping on that axis it is
+// the cell at the opposite end of the same row (wrap_outer_boundary.F90:
+// 101-273 swaps the two ends' ports after outer_boundary).  port: the
+// reflected port on the boundary; opp: the port on the same axis at the
+// other end; back: the element shift from the cell to its own ghost slot
+// (-1, +1, -dy, +dy, -dz, +dz); span: the shift to the ghost slot past the
+// other end (n elements along the axis, with back's sign flipped).
+template <typename T>
+__device__ __forceinline__ void ghost(T *out, long long P, long long idx, bool wrap, int port, int opp,
+                                      long long back, long long span, T v) {
+  if (wrap) out[port * P + idx + span] = v;
+  else out[opp * P + idx + back] = v;
+}
+
+// All ghost writes of one boundary cell at (x, y, z) with reflected pulses co.
+template <typename T>
+__device__ __forceinline__ void write_ghosts(const MeshDev<T> &m, T *out, long long idx, int x, int y, int z,
+                                             const T (&co)[12]) {
+  const long long P = m.plane, dy = m.Px, dz = m.PxPy;
+  const bool wx = m.wrap & 1, wy = m.wrap & 2, wz = m.wrap & 4;
+  if (x == 0) {
+    ghost(out, P, idx, wx, Vy_xmin, Vy_xmax, -1, (long long)m.nx, m.R[0] * co[Vy_xmin]);
+    ghost(out, P, idx, wx, Vz_xmin, Vz_xmax, -1, (long long)m.nx, m.R[0] * co[Vz_xmin]);
+  }
+  if (x == m.nx - 1) {
+    ghost(out, P, idx, wx, Vy_xmax, Vy_xmin, 1, -(long long)m.nx, m.R[1] * co[Vy_xmax]);
+    ghost(out, P, idx, wx, Vz_xmax, Vz_xmin, 1, -(long long)m.nx, m.R[1] * co[Vz_xmax]);
+  }
+  if (y == 0) {
+    ghost(out, P, idx, wy, Vx_ymin, Vx_ymax, -dy, m.ny * dy, m.R[2] * co[Vx_ymin]);
+    ghost(out, P, idx, wy, Vz_ymin, Vz_ymax, -dy, m.ny * dy, m.R[2] * co[Vz_ymin]);
+  }
+  if (y == m.ny - 1) {
+    ghost(out, P, idx, wy, Vx_ymax, Vx_ymin, dy, -m.ny * dy, m.R[3] * co[Vx_ymax]);
+    ghost(out, P, idx, wy, Vz_ymax, Vz_ymin, dy, -m.ny * dy, m.R[3] * co[Vz_ymax]);
+  }
+  if (z == 0) {
+    ghost(out, P, idx, wz, Vx_zmin, Vx_zmax, -dz, m.nz * dz, m.R[4] * co[Vx_zmin]);
+    ghost(out, P, idx, wz, Vy_zmin, Vy_zmax, -dz, m.nz * dz, m.R[4] * co[Vy_zmin]);
+  }
+  if (z == m.nz - 1) {
+    ghost(out, P, idx, wz, Vx_zmax, Vx_zmin, dz, -m.nz * dz, m.R[5] * co[Vx_zmax]);
+    ghost(out, P, idx, wz, Vy_zmax, Vy_zmin, dz, -m.nz * dz, m.R[5] * co[Vy_zmax]);
+  }
+}
 
 // cell_output_field(out_no, 1:6) of step t (output_points.F90:463-612):
 // every output cell writes its current-step row, which the volume outputs
@@ -641,8 +691,8 @@ __global__ void __launch_bounds__(256) tlm_cell_kernel(const MeshDev<T> m, int r
   }
   // ghost slots: R * own reflected pulse (outer_boundary.F90:71-131)
   if (x0 == 0 && (need & 1u)) {
-    out[Vy_xmax * P + idx - 1] = m.R[0] * res[Vy_xmin][0];
-    out[Vz_xmax * P + idx - 1] = m.R[0] * res[Vz_xmin][0];
+    ghost(out, P, idx, m.wrap & 1, Vy_xmin, Vy_xmax, -1, (long long)m.nx, m.R[0] * res[Vy_xmin][0]);
+    ghost(out, P, idx, m.wrap & 1, Vz_xmin, Vz_xmax, -1, (long long)m.nx, m.R[0] * res[Vz_xmin][0]);
   }
   if (x0 + nvalid == m.nx) {
     const int j = nvalid - 1;  // last cell of the row (selected without dynamic register indexing)
@@ -651,40 +701,40 @@ __global__ void __launch_bounds__(256) tlm_cell_kernel(const MeshDev<T> m, int r
     for (int k = 1; k < VEC; k++)
       if (j == k) { vy = res[Vy_xmax][k]; vz = res[Vz_xmax][k]; }
     if (need & (1u << j)) {
-      out[Vy_xmin * P + idx + j + 1] = m.R[1] * vy;
-      out[Vz_xmin * P + idx + j + 1] = m.R[1] * vz;
+      ghost(out, P, idx + j, m.wrap & 1, Vy_xmax, Vy_xmin, 1, -(long long)m.nx, m.R[1] * vy);
+      ghost(out, P, idx + j, m.wrap & 1, Vz_xmax, Vz_xmin, 1, -(long long)m.nx, m.R[1] * vz);
     }
   }
   if (y == 0) {
 #pragma unroll
     for (int j = 0; j < VEC; j++)
       if (need & (1u << j)) {
-        out[Vx_ymax * P + idx - dy + j] = m.R[2] * res[Vx_ymin][j];
-        out[Vz_ymax * P + idx - dy + j] = m.R[2] * res[Vz_ymin][j];
+        ghost(out, P, idx + j, m.wrap & 2, Vx_ymin, Vx_ymax, -dy, m.ny * dy, m.R[2] * res[Vx_ymin][j]);
+        ghost(out, P, idx + j, m.wrap & 2, Vz_ymin, Vz_ymax, -dy, m.ny * dy, m.R[2] * res[Vz_ymin][j]);
       }
   }
   if (y == m.ny - 1) {
 #pragma unroll
     for (int j = 0; j < VEC; j++)
       if (need & (1u << j)) {
-        out[Vx_ymin * P + idx + dy + j] = m.R[3] * res[Vx_ymax][j];
-        out[Vz_ymin * P + idx + dy + j] = m.R[3] * res[Vz_ymax][j];
+        ghost(out, P, idx + j, m.wrap & 2, Vx_ymax, Vx_ymin, dy, -m.ny * dy, m.R[3] * res[Vx_ymax][j]);
+        ghost(out, P, idx + j, m.wrap & 2, Vz_ymax, Vz_ymin, dy, -m.ny * dy, m.R[3] * res[Vz_ymax][j]);
       }
   }
   if (z == 0) {
 #pragma unroll
     for (int j = 0; j < VEC; j++)
       if (need & (1u << j)) {
-        out[Vx_zmax * P + idx - dz + j] = m.R[4] * res[Vx_zmin][j];
-        out[Vy_zmax * P + idx - dz + j] = m.R[4] * res[Vy_zmin][j];
+        ghost(out, P, idx + j, m.wrap & 4, Vx_zmin, Vx_zmax, -dz, m.nz * dz, m.R[4] * res[Vx_zmin][j]);
+        ghost(out, P, idx + j, m.wrap & 4, Vy_zmin, Vy_zmax, -dz, m.nz * dz, m.R[4] * res[Vy_zmin][j]);
       }
   }
   if (z == m.nz - 1) {
 #pragma unroll
     for (int j = 0; j < VEC; j++)
       if (need & (1u << j)) {
-        out[Vx_zmin * P + idx + dz + j] = m.R[5] * res[Vx_zmax][j];
-        out[Vy_zmin * P + idx + dz + j] = m.R[5] * res[Vy_zmax][j];
+        ghost(out, P, idx + j, m.wrap & 4, Vx_zmax, Vx_zmin, dz, -m.nz * dz, m.R[5] * res[Vx_zmax][j]);
+        ghost(out, P, idx + j, m.wrap & 4, Vy_zmax, Vy_zmin, dz, -m.nz * dz, m.R[5] * res[Vy_zmax][j]);
       }
   }
 }
@@ -893,8 +943,8 @@ __global__ void __launch_bounds__(TILE / VEC) tlm_bulk_tma_kernel(const MeshDev<
             }
         }
         if (x0 == 0 && (need & 1u)) {
-          out[Vy_xmax * P + idx - 1] = m.R[0] * inc[Vy_xmin][0];
-          out[Vz_xmax * P + idx - 1] = m.R[0] * inc[Vz_xmin][0];
+          ghost(out, P, idx, m.wrap & 1, Vy_xmin, Vy_xmax, -1, (long long)m.nx, m.R[0] * inc[Vy_xmin][0]);
+          ghost(out, P, idx, m.wrap & 1, Vz_xmin, Vz_xmax, -1, (long long)m.nx, m.R[0] * inc[Vz_xmin][0]);
         }
         if (x0 + nvalid == m.nx) {
           const int j = nvalid - 1;
@@ -903,40 +953,40 @@ __global__ void __launch_bounds__(TILE / VEC) tlm_bulk_tma_kernel(const MeshDev<
           for (int k = 1; k < VEC; k++)
             if (j == k) { vy = inc[Vy_xmax][k]; vz = inc[Vz_xmax][k]; }
           if (need & (1u << j)) {
-            out[Vy_xmin * P + idx + j + 1] = m.R[1] * vy;
-            out[Vz_xmin * P + idx + j + 1] = m.R[1] * vz;
+            ghost(out, P, idx + j, m.wrap & 1, Vy_xmax, Vy_xmin, 1, -(long long)m.nx, m.R[1] * vy);
+            ghost(out, P, idx + j, m.wrap & 1, Vz_xmax, Vz_xmin, 1, -(long long)m.nx, m.R[1] * vz);
           }
         }
         if (y == 0) {
 #pragma unroll
           for (int j = 0; j < VEC; j++)
             if (need & (1u << j)) {
-              out[Vx_ymax * P + idx - dy + j] = m.R[2] * inc[Vx_ymin][j];
-              out[Vz_ymax * P + idx - dy + j] = m.R[2] * inc[Vz_ymin][j];
+              ghost(out, P, idx + j, m.wrap & 2, Vx_ymin, Vx_ymax, -dy, m.ny * dy, m.R[2] * inc[Vx_ymin][j]);
+              ghost(out, P, idx + j, m.wrap & 2, Vz_ymin, Vz_ymax, -dy, m.ny * dy, m.R[2] * inc[Vz_ymin][j]);
             }
         }
         if (y == m.ny - 1) {
 #pragma unroll
           for (int j = 0; j < VEC; j++)
             if (need & (1u << j)) {
-              out[Vx_ymin * P + idx + dy + j] = m.R[3] * inc[Vx_ymax][j];
-              out[Vz_ymin * P + idx + dy + j] = m.R[3] * inc[Vz_ymax][j];
+              ghost(out, P, idx + j, m.wrap & 2, Vx_ymax, Vx_ymin, dy, -m.ny * dy, m.R[3] * inc[Vx_ymax][j]);
+              ghost(out, P, idx + j, m.wrap & 2, Vz_ymax, Vz_ymin, dy, -m.ny * dy, m.R[3] * inc[Vz_ymax][j]);
             }
         }
         if (z == 0) {
 #pragma unroll
           for (int j = 0; j < VEC; j++)
             if (need & (1u << j)) {
-              out[Vx_zmax * P + idx - dz + j] = m.R[4] * inc[Vx_zmin][j];
-              out[Vy_zmax * P + idx - dz + j] = m.R[4] * inc[Vy_zmin][j];
+              ghost(out, P, idx + j, m.wrap & 4, Vx_zmin, Vx_zmax, -dz, m.nz * dz, m.R[4] * inc[Vx_zmin][j]);
+              ghost(out, P, idx + j, m.wrap & 4, Vy_zmin, Vy_zmax, -dz, m.nz * dz, m.R[4] * inc[Vy_zmin][j]);
             }
         }
         if (z == m.nz - 1) {
 #pragma unroll
           for (int j = 0; j < VEC; j++)
             if (need & (1u << j)) {
-              out[Vx_zmin * P + idx + dz + j] = m.R[5] * inc[Vx_zmax][j];
-              out[Vy_zmin * P + idx + dz + j] = m.R[5] * inc[Vy_zmax][j];
+              ghost(out, P, idx + j, m.wrap & 4, Vx_zmax, Vx_zmin, dz, -m.nz * dz, m.R[5] * inc[Vx_zmax][j]);
+              ghost(out, P, idx + j, m.wrap & 4, Vy_zmax, Vy_zmin, dz, -m.nz * dz, m.R[5] * inc[Vy_zmax][j]);
             }
         }
       }
@@ -994,30 +1044,7 @@ __device__ __forceinline__ void special_body(const MeshDev<T> &m, int s, int rel
   special_cell<T, MAXO>(m, s, rec, t, ci, co);
 #pragma unroll
   for (int p = 0; p < 12; p++) out[p * P + idx] = co[p];
-  if (pos.x == 0) {
-    out[Vy_xmax * P + idx - 1] = m.R[0] * co[Vy_xmin];
-    out[Vz_xmax * P + idx - 1] = m.R[0] * co[Vz_xmin];
-  }
-  if (pos.x == m.nx - 1) {
-    out[Vy_xmin * P + idx + 1] = m.R[1] * co[Vy_xmax];
-    out[Vz_xmin * P + idx + 1] = m.R[1] * co[Vz_xmax];
-  }
-  if (pos.y == 0) {
-    out[Vx_ymax * P + idx - dy] = m.R[2] * co[Vx_ymin];
-    out[Vz_ymax * P + idx - dy] = m.R[2] * co[Vz_ymin];
-  }
-  if (pos.y == m.ny - 1) {
-    out[Vx_ymin * P + idx + dy] = m.R[3] * co[Vx_ymax];
-    out[Vz_ymin * P + idx + dy] = m.R[3] * co[Vz_ymax];
-  }
-  if (pos.z == 0) {
-    out[Vx_zmax * P + idx - dz] = m.R[4] * co[Vx_zmin];
-    out[Vy_zmax * P + idx - dz] = m.R[4] * co[Vy_zmin];
-  }
-  if (pos.z == m.nz - 1) {
-    out[Vx_zmin * P + idx + dz] = m.R[5] * co[Vx_zmax];
-    out[Vy_zmin * P + idx + dz] = m.R[5] * co[Vy_zmax];
-  }
+  write_ghosts<T>(m, out, idx, pos.x, pos.y, pos.z, co);
 }
 
 // ---------------------------------------------------------------------------
@@ -1258,30 +1285,7 @@ __device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl,
   pml_cell<T>(m, s, par, out_no, ci, co, t, st);
 #pragma unroll
   for (int p = 0; p < 12; p++) __stcs(out + p * P + idx, co[p]);
-  if (x == 0) {
-    out[Vy_xmax * P + idx - 1] = m.R[0] * co[Vy_xmin];
-    out[Vz_xmax * P + idx - 1] = m.R[0] * co[Vz_xmin];
-  }
-  if (x == m.nx - 1) {
-    out[Vy_xmin * P + idx + 1] = m.R[1] * co[Vy_xmax];
-    out[Vz_xmin * P + idx + 1] = m.R[1] * co[Vz_xmax];
-  }
-  if (y == 0) {
-    out[Vx_ymax * P + idx - dy] = m.R[2] * co[Vx_ymin];
-    out[Vz_ymax * P + idx - dy] = m.R[2] * co[Vz_ymin];
-  }
-  if (y == m.ny - 1) {
-    out[Vx_ymin * P + idx + dy] = m.R[3] * co[Vx_ymax];
-    out[Vz_ymin * P + idx + dy] = m.R[3] * co[Vz_ymax];
-  }
-  if (z == 0) {
-    out[Vx_zmax * P + idx - dz] = m.R[4] * co[Vx_zmin];
-    out[Vy_zmax * P + idx - dz] = m.R[4] * co[Vy_zmin];
-  }
-  if (z == m.nz - 1) {
-    out[Vx_zmin * P + idx + dz] = m.R[5] * co[Vx_zmax];
-    out[Vy_zmin * P + idx + dz] = m.R[5] * co[Vy_zmax];
-  }
+  write_ghosts<T>(m, out, idx, x, y, z, co);
 }
 
 // ---------------------------------------------------------------------------
@@ -1473,30 +1477,7 @@ __device__ __forceinline__ void pml_material_body(const MeshDev<T> &m, const Pmm
     co[p] = T(R[p]);
     out[p * P + idx] = co[p];
   }
-  if (x == 0) {
-    out[Vy_xmax * P + idx - 1] = m.R[0] * co[Vy_xmin];
-    out[Vz_xmax * P + idx - 1] = m.R[0] * co[Vz_xmin];
-  }
-  if (x == m.nx - 1) {
-    out[Vy_xmin * P + idx + 1] = m.R[1] * co[Vy_xmax];
-    out[Vz_xmin * P + idx + 1] = m.R[1] * co[Vz_xmax];
-  }
-  if (y == 0) {
-    out[Vx_ymax * P + idx - dy] = m.R[2] * co[Vx_ymin];
-    out[Vz_ymax * P + idx - dy] = m.R[2] * co[Vz_ymin];
-  }
-  if (y == m.ny - 1) {
-    out[Vx_ymin * P + idx + dy] = m.R[3] * co[Vx_ymax];
-    out[Vz_ymin * P + idx + dy] = m.R[3] * co[Vz_ymax];
-  }
-  if (z == 0) {
-    out[Vx_zmax * P + idx - dz] = m.R[4] * co[Vx_zmin];
-    out[Vy_zmax * P + idx - dz] = m.R[4] * co[Vy_zmin];
-  }
-  if (z == m.nz - 1) {
-    out[Vx_zmin * P + idx + dz] = m.R[5] * co[Vx_zmax];
-    out[Vy_zmin * P + idx + dz] = m.R[5] * co[Vy_zmax];
-  }
+  write_ghosts<T>(m, out, idx, x, y, z, co);
 }
 
 template <typename T>

@@ -71,13 +71,13 @@ NEUTRAL = {"new_mesh_generation", "no_geometry_vtk_files", "compress_output_file
 # packets of other parts of the reference the GPU path does not run
 UNSUPPORTED = {"periodic_boundary", "excitation_surface_list", "excitation_volume_list",
                "ngspice_node_output_list", "periodic_boundary_far_field_surface", "excitation_mode_list",
-               "mode_stir_surface_list", "wrapping_boundary_conditions", "ngspice_timestep_factor",
+               "mode_stir_surface_list", "ngspice_timestep_factor",
                "ngspice_lpf_alpha", "cable_geometry_list", "cable_list", "cable_junction_list", "cable_output_list"}
 # run by the GPU path but not read here: a mode output's profile comes from a
 # separate mode field file (ModeOutput takes the profile directly)
 NOT_READ = {"output_mode_list"}
 # packets read_inp turns into the spec
-HANDLED = {"mesh_outer_boundary_dimension", "mesh_cell_dimension", "mesh_dimensions_in_cells", "pml",
+HANDLED = {"wrapping_boundary_conditions", "mesh_outer_boundary_dimension", "mesh_cell_dimension", "mesh_dimensions_in_cells", "pml",
            "volume_list", "surface_list", "point_list", "simulation_time", "volume_material_list",
            "surface_material_list", "outer_boundary_reflection_coefficient", "excitation_function_list",
            "excitation_point_list", "huygens_surface", "output_point_list", "output_surface_list",
@@ -483,6 +483,11 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
         if "outer_boundary_reflection_coefficient" in rec else (0.0,) * 6
     spec = ProblemSpec(nx=n[0], ny=n[1], nz=n[2], dl=dl, n_timesteps=steps, R=R, origin=(xmin, ymin, zmin),
                        reduced_c=reduced_c, simulation_time=sim_time)
+    if "wrapping_boundary_conditions" in rec:  # read_wrapping_boundary_conditions.F90:55-66
+        w = rec["wrapping_boundary_conditions"].ints(3)
+        if any(v not in (0, 1) for v in w):
+            raise ValueError("wrapping_boundary_conditions packet: each flag is 1 or 0")
+        spec.wrap = tuple(w)
     # PML, read_pml.F90:70-150: a line of six thicknesses (metres) or one for
     # all sides, the same for the reflection coefficients, then the order
     if "pml" in rec:

@@ -806,6 +806,9 @@ class ProblemSpec:
     dl: float
     n_timesteps: int
     R: Tuple[float, float, float, float, float, float] = (0.0,) * 6
+    # Wrapping_boundary_conditions (read_wrapping_boundary_conditions.F90):
+    # 1 joins the two outer faces of that axis (wrap_outer_boundary.F90)
+    wrap: Tuple[int, int, int] = (0, 0, 0)
     origin: Tuple[float, float, float] = (0.0, 0.0, 0.0)
     pml_cells: Tuple[int, int, int, int, int, int] = (0,) * 6
     pml_r: Tuple[float, ...] = (1e-4,) * 6
@@ -1273,6 +1276,9 @@ def build_tables(spec: ProblemSpec) -> dict:
         if COMPONENTS[q.component] > 6:
             raise ValueError("a face output point records E or H (components 1..6)")
     tables["face_mat"] = np.array([face_mat.get(k, 0) for k in ordered], dtype=np.int32)
+    tables["wrap"] = np.array([int(bool(v)) for v in spec.wrap], dtype=np.int32)
+    if any(spec.wrap) and isinstance(spec.huygens, HuygensOuter):
+        raise UnsupportedFeature("an outer-boundary Huygens surface with wrapping boundaries")
     # thin layers: the signed material per special face (positive: reversed)
     # and the filters of every thin-layer material
     tables["face_smat"] = np.array([face_smat.get(k, 0) for k in ordered], dtype=np.int32)

@@ -154,6 +154,14 @@ int tlm_gpu_set_thin_layers(int64_t handle, int32_t n, const double *f, const do
    material type 3 in tlm_gpu_set_face_materials. */
 int tlm_gpu_set_face_thin_layers(int64_t handle, int32_t n, const int32_t *material);
 
+/* Wrapping boundaries (Wrapping_boundary_conditions packet, wrap_x/y/z;
+   TLM_SOLVER/wrap_outer_boundary.F90:101-273): on a wrapped axis the two
+   outer faces are joined, each boundary port receiving R times the
+   reflected pulse of the cell at the other end (the reference swaps the
+   two ends' ports after outer_boundary).  Flags 0 or 1.  Not with an
+   outer-boundary Huygens surface (TLM_E_UNSUPPORTED at the first run). */
+int tlm_gpu_set_wrap(int64_t handle, int32_t wrap_x, int32_t wrap_y, int32_t wrap_z);
+
 /* Huygens surface (SRC/EXCITATION/huygens_surface.F90:247-848): per patch
    the face excitation number, normal (3 ints) and offset; the incident
    field vectors Ei, Hi; offset_min, the wave speed c0/reduced_c and the

@@ -53,7 +53,7 @@ class _Problem(C.Structure):
         ("n_ff", C.c_int32), ("ff_freq", _f64p), ("ff_face_ptr", _i32p), ("ff_face_out", _i32p),
         ("ff_face_code", _i32p), ("face_mat", _i32p),
         ("face_smat", _i32p), ("n_smat", C.c_int32), ("smat_f", _f64p), ("smat_a", _f64p), ("smat_b", _f64p),
-        ("smat_order", _i32p),
+        ("smat_order", _i32p), ("wrap", C.c_int32 * 3),
     ]
 
 
@@ -140,6 +140,7 @@ class Oracle:
             setattr(p, k, arr(k, np.int32) if k in t else arr_empty())
         if "face_mat" in t and np.any(np.asarray(t["face_mat"]) != 0):
             p.face_mat = arr("face_mat", np.int32)  # else NULL: no surface materials
+        p.wrap[:] = [int(v) for v in t.get("wrap", (0, 0, 0))]
         if int(t.get("n_smat", 0)):
             p.face_smat = arr("face_smat", np.int32)
             p.n_smat = int(t["n_smat"])

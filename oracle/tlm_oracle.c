@@ -1099,6 +1099,43 @@ static void outer_boundary(tlm_oracle_state *s, int timestep) {
   }
 }
 
+/* wrap_outer_boundary, TLM_SOLVER/wrap_outer_boundary.F90:101-273 (one
+   process): the ports of the two outer faces of a wrapped axis swap */
+static void wrap_outer_boundary(tlm_oracle_state *s) {
+  const tlm_oracle_problem *p = &s->p;
+  int nx = s->nx, ny = s->ny, nz = s->nz;
+  if (p->wrap[0])
+    for (int cz = 1; cz <= nz; cz++)
+      for (int cy = 1; cy <= ny; cy++) {
+        double Vy = V_(Vy_xmin, 1, cy, cz);
+        V_(Vy_xmin, 1, cy, cz) = V_(Vy_xmax, nx, cy, cz);
+        V_(Vy_xmax, nx, cy, cz) = Vy;
+        double Vz = V_(Vz_xmin, 1, cy, cz);
+        V_(Vz_xmin, 1, cy, cz) = V_(Vz_xmax, nx, cy, cz);
+        V_(Vz_xmax, nx, cy, cz) = Vz;
+      }
+  if (p->wrap[1])
+    for (int cz = 1; cz <= nz; cz++)
+      for (int cx = 1; cx <= nx; cx++) {
+        double Vx = V_(Vx_ymin, cx, 1, cz);
+        V_(Vx_ymin, cx, 1, cz) = V_(Vx_ymax, cx, ny, cz);
+        V_(Vx_ymax, cx, ny, cz) = Vx;
+        double Vz = V_(Vz_ymin, cx, 1, cz);
+        V_(Vz_ymin, cx, 1, cz) = V_(Vz_ymax, cx, ny, cz);
+        V_(Vz_ymax, cx, ny, cz) = Vz;
+      }
+  if (p->wrap[2])
+    for (int cy = 1; cy <= ny; cy++)
+      for (int cx = 1; cx <= nx; cx++) {
+        double Vx = V_(Vx_zmin, cx, cy, 1);
+        V_(Vx_zmin, cx, cy, 1) = V_(Vx_zmax, cx, cy, nz);
+        V_(Vx_zmax, cx, cy, nz) = Vx;
+        double Vy = V_(Vy_zmin, cx, cy, 1);
+        V_(Vy_zmin, cx, cy, 1) = V_(Vy_zmax, cx, cy, nz);
+        V_(Vy_zmax, cx, cy, nz) = Vy;
+      }
+}
+
 /* face_output_frequency_output_surfaces, frequency_output_surfaces.F90:297-421 */
 static void dft_surfaces(tlm_oracle_state *s, double time) {
   const tlm_oracle_problem *p = &s->p;
@@ -1196,6 +1233,7 @@ int tlm_oracle_run(tlm_oracle_state *s, int32_t first_step, int32_t n_steps, dou
     dft_surfaces(s, time);
     far_field_surfaces(s, time);
     outer_boundary(s, timestep);
+    wrap_outer_boundary(s);
     s->timestep = timestep;
   }
   return 0;

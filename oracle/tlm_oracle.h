@@ -148,6 +148,10 @@ typedef struct {
   int32_t n_smat;
   const double *smat_f, *smat_a, *smat_b;
   const int32_t *smat_order;
+
+  /* wrapping boundaries on x, y, z (0 or 1): wrap_outer_boundary after
+     outer_boundary (TLM_SOLVER/wrap_outer_boundary.F90:101-273) */
+  int32_t wrap[3];
 } tlm_oracle_problem;
 
 typedef struct tlm_oracle_state tlm_oracle_state;

@@ -30,6 +30,7 @@ CASES = {
     **{f"tem_{a.lower()}_aniso_{p.lower()}": f"TEM_{a}_ANISOTROPIC_THIN_LAYER_{p}_POL_TEST/PROBLEM_SPECIFICATION_FILES/Ey.tout_ref"
        for a, p in (("X", "Y"), ("X", "Z"), ("Y", "X"), ("Y", "Z"), ("Z", "X"), ("Z", "Y"))},
     "thin_layer_stability": "THIN_LAYER_STABILITY_TEST/PROBLEM_SPECIFICATION_FILES/cavity.field.tout_ref",
+    "wrapping_Ex": "WRAPPING_BOUNDARY/PROBLEM_SPECIFICATION_FILES/Ex_centre.tout_ref",
 }
 
 
@@ -58,6 +59,7 @@ INP_CASES = {
     **{f"tem_{a.lower()}_aniso_{p.lower()}": f"TEM_{a}_ANISOTROPIC_THIN_LAYER_{p}_POL_TEST/PROBLEM_SPECIFICATION_FILES/TEM_cell.inp"
        for a, p in (("X", "Y"), ("X", "Z"), ("Y", "X"), ("Y", "Z"), ("Z", "X"), ("Z", "Y"))},
     "thin_layer_stability": "THIN_LAYER_STABILITY_TEST/PROBLEM_SPECIFICATION_FILES/cavity.inp",
+    "wrapping": "WRAPPING_BOUNDARY/PROBLEM_SPECIFICATION_FILES/wrapping_test.inp",
 }
 # the surface material files the thin-layer cases use, as text
 SMAT_CASES = ["Dispersive_sheet", "Anisotropic_sheet"]
