@@ -330,9 +330,11 @@ def probe_error(a, b):
 def bench_pair(t, device, peak, K=60, W=3):
     """FP32 and FP64 step rates of one mesh with the FP32 probe error over
     the complete solve (compact record for the section keys)."""
+    from ggi_tlm_b200 import capi
+
     n = t["nx"] * t["ny"] * t["nz"]
-    r32 = timed_solo(t, 0, device, K, W, 1)
-    r64 = timed_solo(t, 1, device, K, W, 1)
+    r32 = timed_solo(t, capi.TLM_PRECISION_FP32, device, K, W, 1)
+    r64 = timed_solo(t, capi.TLM_PRECISION_FP64, device, K, W, 1)
     out = {}
     for key, r, esz in (("fp32", r32, 4), ("fp64", r64, 8)):
         ab = algorithmic_bytes(t, esz)
