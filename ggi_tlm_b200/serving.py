@@ -111,59 +111,71 @@ def _output_bytes(t: dict) -> int:
 
 
 class GpuEngine:
-    """Default engine: solves are GpuMesh objects advanced in a GpuBatch.
+    """Default engine: solves are GpuMesh objects advanced in GpuBatch
+    objects, one batch per precision (a request's precision is
+    ``choose(tables)``, the engine's ``precision`` without a chooser).  The
+    FP32 and FP64 batches run on their own streams, so their work overlaps
+    on the device.
 
     A quantum runs asynchronously: ``advance`` starts it and returns, and
     ``wait`` blocks until it has finished.  Requests admitted meanwhile get
     their device state built at once (``GpuMesh.prepare``), overlapping the
-    running quantum; the batch is rebuilt with them, and without retired
+    running quantum; a batch is rebuilt with them, and without retired
     solves, when the next quantum starts."""
 
-    def __init__(self, precision: int = capi.TLM_PRECISION_FP32, device: int = 0, variant: Optional[int] = None):
+    def __init__(self, precision: int = capi.TLM_PRECISION_FP32, device: int = 0, variant: Optional[int] = None,
+                 choose: Optional[Callable[[dict], int]] = None):
         self.precision = precision
+        self.choose = choose
         self.device = device
         self.variant = variant
         self.meshes: Dict[int, capi.GpuMesh] = {}
-        self.batch: Optional[capi.GpuBatch] = None
+        self.batches: Dict[int, capi.GpuBatch] = {}
         self.retired: List[capi.GpuMesh] = []
-        self.dirty = False
+        self.dirty = set()
         self.running = False
 
+    def precision_of(self, tables: dict) -> int:
+        return self.choose(tables) if self.choose is not None else self.precision
+
     def add(self, rid: int, tables: dict):
-        g = capi.GpuMesh(tables, precision=self.precision, device=self.device)
+        prec = self.precision_of(tables)
+        g = capi.GpuMesh(tables, precision=prec, device=self.device)
         g.prepare()
         self.meshes[rid] = g
-        self.dirty = True
+        self.dirty.add(prec)
 
     def remove(self, rid: int):
-        self.retired.append(self.meshes.pop(rid))  # closed once the batch that holds it is gone
-        self.dirty = True
-
-    def _drop_batch(self):
-        if self.batch is not None:
-            self.batch.close()
-            self.batch = None
+        g = self.meshes.pop(rid)
+        self.retired.append(g)  # closed once the batch that holds it is gone
+        self.dirty.add(g.precision)
 
     def wait(self):
         if self.running:
-            self.batch.synchronize()
+            for b in self.batches.values():
+                b.synchronize()
             self.running = False
 
     def advance(self, n_steps: int):
         self.wait()
+        for prec in list(self.dirty):
+            b = self.batches.pop(prec, None)
+            if b is not None:
+                b.close()
         if self.dirty:
-            self._drop_batch()
             for g in self.retired:
                 g.close()
             self.retired.clear()
-            self.dirty = False
+        self.dirty.clear()
         if not self.meshes:
             return
-        if self.batch is None:
-            self.batch = capi.GpuBatch(list(self.meshes.values()))
-            if self.variant is not None:
-                self.batch.set_variant(self.variant)
-        self.batch.run(n_steps, sync=False)
+        for prec in {g.precision for g in self.meshes.values()}:
+            if prec not in self.batches:
+                self.batches[prec] = capi.GpuBatch([g for g in self.meshes.values() if g.precision == prec])
+                if self.variant is not None:
+                    self.batches[prec].set_variant(self.variant)
+        for b in self.batches.values():
+            b.run(n_steps, sync=False)
         self.running = True
 
     def progress(self, rid: int) -> int:
@@ -175,7 +187,9 @@ class GpuEngine:
 
     def close(self):
         self.wait()
-        self._drop_batch()
+        for b in self.batches.values():
+            b.close()
+        self.batches.clear()
         for g in list(self.meshes.values()) + self.retired:
             g.close()
         self.meshes.clear()
@@ -201,8 +215,9 @@ class Server:
 
     def serve(self, trace: List[Request]) -> List[Result]:
         pending = collections.deque(sorted(trace, key=lambda r: (r.arrival, r.rid)))
+        prec = getattr(self.engine, "precision_of", lambda t: self.precision)
         for r in pending:
-            if footprint_bytes(r.tables, self.precision) > self.budget:
+            if footprint_bytes(r.tables, prec(r.tables)) > self.budget:
                 raise ValueError(f"request {r.rid} needs more than the whole HBM budget")
         waiting: collections.deque = collections.deque()
         active: Dict[int, tuple] = {}  # rid -> (request, admitted time, bytes)
@@ -215,7 +230,7 @@ class Server:
                 waiting.append(pending.popleft())
             # admission: arrival order, while a slot and the budget allow
             while waiting and len(active) < self.max_slots:
-                need = footprint_bytes(waiting[0].tables, self.precision)
+                need = footprint_bytes(waiting[0].tables, prec(waiting[0].tables))
                 if used + need > self.budget:
                     break
                 r = waiting.popleft()
