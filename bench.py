@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the B200 SCN-TLM time-stepping core.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload t512|t256|c2|c3|c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload t512|t192|c2|c3|c1]
 
 One "step" is one TLM time step (excitation, scatter, connect, outer boundary,
 probes) over the whole mesh.  Default workload: the 512^3 free-space box with
@@ -87,8 +87,8 @@ def workload_spec(name: str):
         return cases.pml_spheres(), "pml_spheres_256^3_pml8_32spheres_huygens_dft64x64x64"
     if name == "t512":
         return cases.pml_point_source(512, steps=2000), "pml_point_source_512^3_pml8"
-    if name == "t256":  # the same mesh at 256^3: small enough for an ncu capture
-        return cases.pml_point_source(256, steps=300), "pml_point_source_256^3_pml8"
+    if name == "t192":  # the same mesh at 192^3: small enough for an ncu capture
+        return cases.pml_point_source(192, steps=300), "pml_point_source_192^3_pml8"
     if name == "c3":
         return cases.debye_slabs(), "debye_slabs_384x384x192_pml10_6slabs_dft64x64x64"
     if name == "c1":
@@ -443,7 +443,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="t512", choices=["t512", "t256", "c2", "c3", "c1"])
+    ap.add_argument("--workload", default="t512", choices=["t512", "t192", "c2", "c3", "c1"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--quick", action="store_true", help="main workload only (no C2, C3, batch, serving sections)")

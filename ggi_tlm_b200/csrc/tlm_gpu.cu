@@ -302,7 +302,7 @@ struct Mesh {
       pmm_pos, pmm_parmat, pmm_state, pmm_sigma, face_src, fpt_field_d, fpt_type_d, fprobe, fprobe_rec,
       ohs_face, ohs_offset, ff_entry, ff_phasor, ff_acc, cell_cur, out_hist, vdft_entry, vdft_gate_d, vdft_phasor,
       vdft_acc, osurf_entry, osurf_pos, osurf_dev, osurf_hist, rcs_face, rcs_dist_d, rcs_tc0, rcs_acc, ovol_dev,
-      face_mat_d, face_smat_d, thin_d, thin_taps, ovol_cells, ovol_hist, sar_entry, sar_phasor, sar_acc, ps_entry, ps_phasor, ps_acc, mode_d, mode_face, mode_wd,
+      face_mat_d, face_smat_d, pml_cls_par, thin_d, thin_taps, ovol_cells, ovol_hist, sar_entry, sar_phasor, sar_acc, ps_entry, ps_phasor, ps_acc, mode_d, mode_face, mode_wd,
       mode_hist;
   int n_pt_rows = 0;
   int n_pmm = 0;  // PML cells inside a volume material
@@ -328,6 +328,7 @@ struct Mesh {
   int small_every = 0;       // set_small_to_zero: period in steps (0 = off)
   double small_value = 0.0;
   int pml_prefetch = 1200;  // blocks ahead for the PML state L2 prefetch (0 = off)
+  bool pml_by_class = false;  // PML parameters loaded by distance class (pml_cls_par)
   SideStream side;          // PML / PML-material / special kernels beside the bulk kernel
   bool side_on = false;
 
@@ -812,6 +813,34 @@ int finalize(Mesh *m) {
     for (int i = 0; i < m->n_pml_params; i++)
       for (int k = 0; k < 15; k++) par[(size_t)i * 16 + k] = m->pml_params[(size_t)i * 15 + k];
     if ((rc = upload(m, m->pml_par, par))) return rc;
+    // the parameter rows by distance class, where every cell's row is its
+    // class's (TLM_PML_CLASS=0 turns the class path off)
+    m->pml_by_class = false;
+    const char *ce = getenv("TLM_PML_CLASS");
+    if (m->pml_shell.on && m->n_pml_list && !(ce && ce[0] == '0')) {
+      const tlm::PmlShell &h = m->pml_shell;
+      const size_t ncls = (size_t)(h.xl + h.xh + 1) * (h.yl + h.yh + 1) * (h.zl + h.zh + 1);
+      std::vector<int> row_of(ncls, -1);
+      bool ok = true;
+      for (int s2 = 0; s2 < m->n_pml_list && ok; s2++) {
+        if (pml_par[s2] == tlm::kPmlMaterialSlot) continue;
+        const int row = pml_par[s2] & (tlm::kPmlOutputFlag - 1);
+        int x, y, z;
+        tlm::pml_shell_pos(h, s2, x, y, z);
+        const int c = tlm::pml_class(h, x, y, z);
+        if (c < 0 || (size_t)c >= ncls) ok = false;
+        else if (row_of[c] < 0) row_of[c] = row;
+        else if (row_of[c] != row) ok = false;
+      }
+      if (ok) {
+        std::vector<double> cp(ncls * 16, 0.0);
+        for (size_t c = 0; c < ncls; c++)
+          if (row_of[c] >= 0)
+            for (int k = 0; k < 16; k++) cp[c * 16 + k] = par[(size_t)row_of[c] * 16 + k];
+        if ((rc = upload(m, m->pml_cls_par, cp))) return rc;
+        m->pml_by_class = true;
+      }
+    }
   }
   if ((rc = dalloc(m, m->pml_ixt, (size_t)std::max(m->n_out_cells, 1) * 3 * pesz))) return rc;
   CK(cudaMemset(m->pml_ixt.p, 0, m->pml_ixt.bytes));
@@ -1440,7 +1469,8 @@ int enqueue_steps(Mesh *m, int n, cudaEvent_t *kev) {
     const cudaStream_t ss = side ? m->side.s : m->stream;
     if (m->n_pml_list) {
       tlm::PmlList pl{(const unsigned long long *)m->pml_pos.p, (const uint16_t *)m->pml_par16.p,
-                      (const int2 *)m->pml_outmap.p, m->n_pml_list, m->n_pml_out, m->pml_shell};
+                      (const int2 *)m->pml_outmap.p, m->n_pml_list, m->n_pml_out, m->pml_shell,
+                      m->pml_by_class ? (const double *)m->pml_cls_par.p : nullptr};
       tlm::tlm_pml_kernel<T><<<(m->n_pml_list + 127) / 128, 128, 0, ss>>>(md, pl, k, m->pml_prefetch);
       m->last_launches++;
     }
@@ -2500,7 +2530,8 @@ int build_batch_lists(Batch *b) {
     if (rc) return rc;
     md.push_back(mesh_dev<T>(m));
     pl.push_back(tlm::PmlList{(const unsigned long long *)m->pml_pos.p, (const uint16_t *)m->pml_par16.p,
-                              (const int2 *)m->pml_outmap.p, m->n_pml_list, m->n_pml_out, m->pml_shell});
+                              (const int2 *)m->pml_outmap.p, m->n_pml_list, m->n_pml_out, m->pml_shell,
+                              m->pml_by_class ? (const double *)m->pml_cls_par.p : nullptr});
     fd.push_back(face_dev(m));
     dd.push_back(dft_dev(m));
     nsp.push_back(m->n_sp_dev);

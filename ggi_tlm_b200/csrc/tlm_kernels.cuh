@@ -303,14 +303,15 @@ __device__ __forceinline__ void free_space_cell(const T *inc, T *out) {
 // PML free-space cell, scatter_PML.F90:22-313
 // ---------------------------------------------------------------------------
 template <typename T>
-__device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, int par, int out_no, const T *inc_in, T *out,
-                                      int t, const typename PmlTypes<T>::state (&st)[kPmlState]) {
+__device__ __forceinline__ void pml_cell(const MeshDev<T> &m, int pidx, const double (&P)[15], int out_no,
+                                      const T *inc_in, T *out, int t,
+                                      const typename PmlTypes<T>::state (&st)[kPmlState]) {
   using A = typename PmlTypes<T>::arith;
   using ST = typename PmlTypes<T>::state;
   // FP64: literal scatter_PML.F90 arithmetic.  FP32: currents (and the
   // series-term state) carried scaled by Z0, i.e. Z0 = 1 below.
   const A Z0 = sizeof(T) == 8 ? A(kZ0) : A(1);
-  const double *P = m.pml_par + (size_t)par * 16;
+  // P: the cell's PML_parameters row (TLM_PML_volume_materials.F90:325-351)
   const A ax = A(P[0]), ay = A(P[1]), az = A(P[2]);
   const A exp_x = A(P[3]), exp_y = A(P[4]), exp_z = A(P[5]);
   const A Csx = A(P[6]), Csy = A(P[7]), Csz = A(P[8]);
@@ -1114,7 +1115,23 @@ struct PmlList {
   const int2 *out_map;  // (pml index, output number) of PML output cells, sorted by pml index
   int n, n_out_map;
   PmlShell sh;
+  // For a shell whose parameter rows follow the cells' PML distance classes
+  // (calc_pml_dist, TLM_PML_volume_materials.F90:446-481; the host checks
+  // every cell), the rows indexed by class, [(2 zl+..)][16]: a cell's
+  // parameters are then loaded from its position, beside its links and
+  // state, instead of after its parameter index arrives.  nullptr: off.
+  const double *cls_par;
 };
+
+// The PML distance-class index of shell position (x, y, z): per axis the
+// signed distance into the PML (-lo..-1 on the low side, 1..hi on the high
+// side, 0 outside), offset to 0..lo+hi and combined x fastest.
+__host__ __device__ __forceinline__ int pml_class(const PmlShell &h, int x, int y, int z) {
+  const int cx = x < h.xl ? x - h.xl : (x >= h.nx - h.xh ? x - (h.nx - h.xh) + 1 : 0);
+  const int cy = y < h.yl ? y - h.yl : (y >= h.ny - h.yh ? y - (h.ny - h.yh) + 1 : 0);
+  const int cz = z < h.zl ? z - h.zl : (z >= h.nz - h.zh ? z - (h.nz - h.zh) + 1 : 0);
+  return ((cz + h.zl) * (h.yl + h.yh + 1) + (cy + h.yl)) * (h.xl + h.xh + 1) + (cx + h.xl);
+}
 
 // Position of PML cell s of a shell (traversal order z, y, x).
 __host__ __device__ __forceinline__ void pml_shell_pos(const PmlShell &h, int s, int &x, int &y, int &z) {
@@ -1270,8 +1287,20 @@ __device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl,
   const ST *Lg = m.pml_state + pml_sidx(0, s);
 #pragma unroll
   for (int k = 0; k < kPmlState; k++) st[k] = __ldcs(Lg + 32 * k);
+  double prm[15];
+  const bool by_class = pl.cls_par != nullptr;
+  if (by_class) {  // the parameters from the position: no wait on the index
+    const double *row = pl.cls_par + (size_t)pml_class(pl.sh, x, y, z) * 16;
+#pragma unroll
+    for (int k = 0; k < 15; k++) prm[k] = __ldg(row + k);
+  }
   if (pw == kPmlMaterialSlot) return;  // PML cell in a material: tlm_pml_material_kernel
   const int par = pw & (kPmlOutputFlag - 1);
+  if (!by_class) {
+    const double *row = m.pml_par + (size_t)par * 16;
+#pragma unroll
+    for (int k = 0; k < 15; k++) prm[k] = row[k];
+  }
   int out_no = -1;
   if (pw & kPmlOutputFlag) {  // binary search of the output map (sorted by PML cell)
     int lo = 0, hi = pl.n_out_map - 1;
@@ -1282,7 +1311,7 @@ __device__ __forceinline__ void pml_body(const MeshDev<T> &m, const PmlList &pl,
       if (e.x < s) lo = mid + 1; else hi = mid - 1;
     }
   }
-  pml_cell<T>(m, s, par, out_no, ci, co, t, st);
+  pml_cell<T>(m, s, prm, out_no, ci, co, t, st);
 #pragma unroll
   for (int p = 0; p < 12; p++) __stcs(out + p * P + idx, co[p]);
   write_ghosts<T>(m, out, idx, x, y, z, co);
