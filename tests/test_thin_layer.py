@@ -83,13 +83,24 @@ def test_the_layer_changes_the_field():
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["tem_thin_layer", "tem_y_aniso_z", "tem_z_aniso_x", "thin_layer_stability"])
 def test_gpu_thin_layer_matches_the_oracle(gpu_lib, case):
+    """The links are compared a quarter of the way in, while the pulse is in
+    the mesh, and at the end against that scale: by the last step the pulse
+    has left the TEM column and the links that remain are ~1e-15 of it, so
+    rounding noise is all a comparison relative to them would see."""
     t = tables(case)
     o = oracle.Oracle(t)
-    want = o.run(t["n_timesteps"])
+    n1 = int(t["n_timesteps"]) // 4
+    want = o.run(n1)
     with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64) as g:
-        g.run(t["n_timesteps"])
+        g.run(n1)
+        mid = o.links()
+        scale = np.linalg.norm(mid)
+        assert scale > 0
+        assert np.linalg.norm(g.links() - mid) <= 1e-10 * scale
+        want = np.concatenate([want, o.run(int(t["n_timesteps"]) - n1)])
+        g.run(int(t["n_timesteps"]) - n1)
         got, links = g.cell_output(), g.links()
     assert got.shape == want.shape
     assert np.linalg.norm(got - want) <= 1e-10 * np.linalg.norm(want)
-    assert np.linalg.norm(links - o.links()) <= 1e-10 * np.linalg.norm(o.links())
+    assert np.linalg.norm(links - o.links()) <= 1e-10 * scale
     o.close()
