@@ -46,6 +46,7 @@ EXPORTS = [
     "tlm_gpu_fetch_sar_volumes", "tlm_gpu_set_power_surfaces", "tlm_gpu_fetch_power_surfaces",
     "tlm_gpu_set_mode_outputs", "tlm_gpu_fetch_mode_outputs", "tlm_gpu_set_face_materials",
     "tlm_gpu_set_thin_layers", "tlm_gpu_set_face_thin_layers", "tlm_gpu_set_wrap",
+    "tlm_gpu_halo_bytes", "tlm_gpu_halo_get", "tlm_gpu_halo_put",
 ]
 
 
@@ -126,6 +127,9 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_thin_layers": [i64, i32, _f64p, _f64p, _f64p, _i32p, i32],
         "tlm_gpu_set_face_thin_layers": [i64, i32, _i32p],
         "tlm_gpu_set_wrap": [i64, i32, i32, i32],
+        "tlm_gpu_halo_bytes": [i64, C.POINTER(i64)],
+        "tlm_gpu_halo_get": [i64, i32, C.c_void_p],
+        "tlm_gpu_halo_put": [i64, i32, C.c_void_p],
         "tlm_gpu_fetch_mode_outputs": [i64, i32, i32, _f64p],
         "tlm_gpu_set_small_to_zero": [i64, i32, C.c_double],
         "tlm_gpu_set_dft": [i64, i32, _f64p, _i32p, _i32p, _i32p, _i32p],
@@ -471,6 +475,22 @@ class GpuMesh:
         out = np.zeros(t["nx"] * t["ny"] * t["nz"] * 12)
         _check(_lib.tlm_gpu_fetch_links(self.h, out.ctypes.data_as(_f64p)))
         return out.reshape(t["nz"], t["ny"], t["nx"], 12)
+
+    def halo_bytes(self) -> int:
+        """Bytes of one side of the z-slab halo (two ports of a padded z-plane)."""
+        v = C.c_int64(0)
+        _check(_lib.tlm_gpu_halo_bytes(self.h, C.byref(v)))
+        return int(v.value)
+
+    def halo_get(self, side: int, dev_ptr: int):
+        """Copy this slab's first (side 0) or last (side 1) plane's outgoing
+        z pulses into device memory at ``dev_ptr``."""
+        _check(_lib.tlm_gpu_halo_get(self.h, side, C.c_void_p(dev_ptr)))
+
+    def halo_put(self, side: int, dev_ptr: int):
+        """Fill the ghost plane below (side 0) or above (side 1) from device
+        memory at ``dev_ptr`` (a neighbour slab's ``halo_get``)."""
+        _check(_lib.tlm_gpu_halo_put(self.h, side, C.c_void_p(dev_ptr)))
 
     def close(self):
         if getattr(self, "h", 0):

@@ -2423,6 +2423,72 @@ int tlm_gpu_fetch_links_noalloc(int64_t h, double *out) {
   return TLM_OK;
 }
 
+namespace {
+// One side of the z-slab halo: the two ports and the storage plane (0 =
+// ghost below, 1 = first cell plane, nz = last, nz + 1 = ghost above) of
+// the pulses that the last completed step reflected.
+int halo_span(Mesh *m, int side, bool put, char **p0, char **p1, size_t *bytes) {
+  const size_t esz = m->fp64 ? 8 : 4;
+  const int nz = m->desc.nz;
+  int z, a, b;
+  if (!put) {
+    z = side ? nz : 1;
+    a = side ? tlm::Vx_zmax : tlm::Vx_zmin;
+    b = side ? tlm::Vy_zmax : tlm::Vy_zmin;
+  } else {
+    z = side ? nz + 1 : 0;
+    a = side ? tlm::Vx_zmin : tlm::Vx_zmax;
+    b = side ? tlm::Vy_zmin : tlm::Vy_zmax;
+  }
+  const long long pxpy = (long long)m->Px * m->Py;
+  const int t_done = m->next_step - 1;
+  char *buf = (char *)m->links.p + ((t_done & 1) ? (size_t)12 * m->plane * esz : 0);
+  *p0 = buf + ((size_t)a * m->plane + (size_t)z * pxpy) * esz;
+  *p1 = buf + ((size_t)b * m->plane + (size_t)z * pxpy) * esz;
+  *bytes = (size_t)pxpy * esz;
+  return TLM_OK;
+}
+
+int halo_copy(int64_t h, int32_t side, void *dev, bool put) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (!dev) return fail(TLM_E_BADARG, "null halo buffer");
+  if (side != 0 && side != 1) return fail(TLM_E_BADARG, "halo side must be 0 (below) or 1 (above)");
+  if (m->batch_stream) CK(cudaStreamSynchronize(m->batch_stream));
+  CK(cudaSetDevice(m->desc.device));
+  int rc = finalize(m);
+  if (rc) return rc;
+  char *p0, *p1;
+  size_t bytes;
+  halo_span(m, side, put, &p0, &p1, &bytes);
+  char *d = (char *)dev;
+  if (put) {
+    CK(cudaMemcpyAsync(p0, d, bytes, cudaMemcpyDefault, m->stream));
+    CK(cudaMemcpyAsync(p1, d + bytes, bytes, cudaMemcpyDefault, m->stream));
+  } else {
+    CK(cudaMemcpyAsync(d, p0, bytes, cudaMemcpyDefault, m->stream));
+    CK(cudaMemcpyAsync(d + bytes, p1, bytes, cudaMemcpyDefault, m->stream));
+  }
+  CK(cudaStreamSynchronize(m->stream));
+  return TLM_OK;
+}
+}  // namespace
+
+int tlm_gpu_halo_bytes(int64_t h, int64_t *bytes) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (!bytes) return fail(TLM_E_BADARG, "null output");
+  const size_t esz = m->fp64 ? 8 : 4;
+  int rc = finalize(m);  // the padded plane (Px x Py elements) is laid out there
+  if (rc) return rc;
+  *bytes = (int64_t)(2 * (size_t)m->Px * m->Py * esz);
+  return TLM_OK;
+}
+
+int tlm_gpu_halo_get(int64_t h, int32_t side, void *dev) { return halo_copy(h, side, dev, false); }
+
+int tlm_gpu_halo_put(int64_t h, int32_t side, const void *dev) { return halo_copy(h, side, (void *)dev, true); }
+
 int tlm_gpu_destroy(int64_t h) {
   std::unique_ptr<Mesh> m;
   {

@@ -392,6 +392,28 @@ int tlm_gpu_fetch_links(int64_t handle, double *out);
    handles) race on it. */
 int tlm_gpu_fetch_links_noalloc(int64_t handle, double *out);
 
+/* z-slab halo exchange of a mesh that is one slab of a partitioned mesh
+   (replaces TLM_SOLVER/TLM_parallel_pass_data.F90:38-279, the MPI passes
+   between z-slab ranks; slabs as MESH/general_mesh_subroutines.F90:868-972
+   assigns them).  Between two timesteps, the slab below needs this slab's
+   first-plane Vx_zmin, Vy_zmin pulses in its ghost plane above, and the slab
+   above needs its last-plane Vx_zmax, Vy_zmax pulses in its ghost plane
+   below.  One side is two ports of one padded z-plane, *bytes bytes
+   (tlm_gpu_halo_bytes; slabs of one mesh have equal sizes).
+     tlm_gpu_halo_get side 0: this slab's first plane (Vx_zmin, Vy_zmin),
+                      side 1: its last plane (Vx_zmax, Vy_zmax);
+     tlm_gpu_halo_put side 0: the ghost plane below (Vx_zmax, Vy_zmax),
+                      side 1: the ghost plane above (Vx_zmin, Vy_zmin).
+   Both act on the pulses the last completed step reflected (the ones the
+   next step reads), with device-to-device copies on the mesh's stream
+   between `dev` (device memory of this mesh's device, or peer memory the
+   device can reach) and the link planes, and return once the copies are
+   done.  The mesh's outer boundary on a slab side is overwritten by the
+   put, so its R there does not matter. */
+int tlm_gpu_halo_bytes(int64_t handle, int64_t *bytes);
+int tlm_gpu_halo_get(int64_t handle, int32_t side, void *dev);
+int tlm_gpu_halo_put(int64_t handle, int32_t side, const void *dev);
+
 /* Use a caller CUDA stream (cudaStream_t passed as void*; NULL = own). */
 int tlm_gpu_set_stream(int64_t handle, void *stream);
 

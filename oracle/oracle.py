@@ -53,7 +53,7 @@ class _Problem(C.Structure):
         ("n_ff", C.c_int32), ("ff_freq", _f64p), ("ff_face_ptr", _i32p), ("ff_face_out", _i32p),
         ("ff_face_code", _i32p), ("face_mat", _i32p),
         ("face_smat", _i32p), ("n_smat", C.c_int32), ("smat_f", _f64p), ("smat_a", _f64p), ("smat_b", _f64p),
-        ("smat_order", _i32p), ("wrap", C.c_int32 * 3),
+        ("smat_order", _i32p), ("wrap", C.c_int32 * 3), ("slab", C.c_int32 * 2),
     ]
 
 
@@ -82,6 +82,9 @@ def _load():
         _lib.tlm_oracle_get_far_field.argtypes = [C.c_void_p, _f64p]
         _lib.tlm_oracle_set_threads.argtypes = [C.c_void_p, C.c_int32]
         _lib.tlm_oracle_set_threads.restype = C.c_int32
+        _lib.tlm_oracle_half_step.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _f64p]
+        _lib.tlm_oracle_get_zplane.argtypes = [C.c_void_p, C.c_int32, _f64p]
+        _lib.tlm_oracle_set_zplane.argtypes = [C.c_void_p, C.c_int32, _f64p]
     return _lib
 
 
@@ -141,6 +144,7 @@ class Oracle:
         if "face_mat" in t and np.any(np.asarray(t["face_mat"]) != 0):
             p.face_mat = arr("face_mat", np.int32)  # else NULL: no surface materials
         p.wrap[:] = [int(v) for v in t.get("wrap", (0, 0, 0))]
+        p.slab[:] = [int(v) for v in t.get("slab", (0, 0))]
         if int(t.get("n_smat", 0)):
             p.face_smat = arr("face_smat", np.int32)
             p.n_smat = int(t["n_smat"])
@@ -171,6 +175,31 @@ class Oracle:
             raise RuntimeError(f"oracle run failed rc={rc}")
         self.step += n_steps
         return out[:, : int(self.t["n_out_cells"]), :]
+
+    def half_step(self, half: int) -> np.ndarray:
+        """Half 1 (excitation, scatter, cell output: returns that step's
+        cell_output_field [n_out_cells, 6]) or half 2 (connect to the outer
+        boundary) of the next timestep, for a partitioned run that exchanges
+        z-planes between the halves (TLM_parallel_pass_data_1/2)."""
+        ts = self.step + 1
+        out = np.zeros((max(int(self.t["n_out_cells"]), 1), 6))
+        rc = _load().tlm_oracle_half_step(self._h, ts, half, out.ctypes.data_as(_f64p))
+        if rc != 0:
+            raise RuntimeError(f"oracle half step failed rc={rc}")
+        if half == 2:
+            self.step = ts
+        return out[: int(self.t["n_out_cells"])]
+
+    def zplane(self, plane: int) -> np.ndarray:
+        """Vx_zmax, Vy_zmax of the ghost plane below the slab (0) or of its
+        top plane (1), as [2, ny, nx]."""
+        out = np.zeros((2, int(self.t["ny"]), int(self.t["nx"])))
+        _load().tlm_oracle_get_zplane(self._h, plane, out.ctypes.data_as(_f64p))
+        return out
+
+    def set_zplane(self, plane: int, v: np.ndarray):
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(2, int(self.t["ny"]), int(self.t["nx"]))
+        _load().tlm_oracle_set_zplane(self._h, plane, v.ctypes.data_as(_f64p))
 
     def dft(self) -> np.ndarray:
         n = int(self.t["dft_face_ptr"][-1]) if self.t["n_dft"] else 0

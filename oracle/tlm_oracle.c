@@ -1004,8 +1004,8 @@ static void connect_plane(tlm_oracle_state *s, int cz, int excitation_face_numbe
             connect_special_face(s, f - 1, cx, cy, cz, 2, &excitation_face_number, &output_face_number);
           }
         }
-        if (cz != 1) {
-          int f = s->face_code[cell * 3 + 2];
+        if (cz != 1 || s->p.slab[0]) {  /* the z-face below a slab's first plane: connected here */
+          int f = cz != 1 ? s->face_code[cell * 3 + 2] : 0;
           if (f == 0) {
             double Vx = V_(Vx_zmin, cx, cy, cz) + V_(Vx_zmax, cx, cy, cz - 1);
             V_(Vx_zmin, cx, cy, cz) = Vx - V_(Vx_zmin, cx, cy, cz);
@@ -1051,16 +1051,18 @@ static void outer_boundary(tlm_oracle_state *s, int timestep) {
       V_(Vx_ymax, cx, ny, cz) = V_(Vx_ymax, cx, ny, cz) * R[3];
       V_(Vz_ymax, cx, ny, cz) = V_(Vz_ymax, cx, ny, cz) * R[3];
     }
-  for (int cy = 1; cy <= ny; cy++)
-    for (int cx = 1; cx <= nx; cx++) {
-      V_(Vx_zmin, cx, cy, 1) = V_(Vx_zmin, cx, cy, 1) * R[4];
-      V_(Vy_zmin, cx, cy, 1) = V_(Vy_zmin, cx, cy, 1) * R[4];
-    }
-  for (int cy = 1; cy <= ny; cy++)
-    for (int cx = 1; cx <= nx; cx++) {
-      V_(Vx_zmax, cx, cy, nz) = V_(Vx_zmax, cx, cy, nz) * R[5];
-      V_(Vy_zmax, cx, cy, nz) = V_(Vy_zmax, cx, cy, nz) * R[5];
-    }
+  if (!p->slab[0])
+    for (int cy = 1; cy <= ny; cy++)
+      for (int cx = 1; cx <= nx; cx++) {
+        V_(Vx_zmin, cx, cy, 1) = V_(Vx_zmin, cx, cy, 1) * R[4];
+        V_(Vy_zmin, cx, cy, 1) = V_(Vy_zmin, cx, cy, 1) * R[4];
+      }
+  if (!p->slab[1])
+    for (int cy = 1; cy <= ny; cy++)
+      for (int cx = 1; cx <= nx; cx++) {
+        V_(Vx_zmax, cx, cy, nz) = V_(Vx_zmax, cx, cy, nz) * R[5];
+        V_(Vy_zmax, cx, cy, nz) = V_(Vy_zmax, cx, cy, nz) * R[5];
+      }
   if (!p->hs_outer) return;
   /* outer-boundary Huygens surface (outer_boundary.F90:133-318): per
      boundary face, the two tangential ports get
@@ -1210,32 +1212,63 @@ static void set_small_to_zero(tlm_oracle_state *s) {
           if (fabs(V_(port, cx, cy, cz)) < small) V_(port, cx, cy, cz) = 0.0;
 }
 
+int tlm_oracle_half_step(tlm_oracle_state *s, int32_t timestep, int32_t half, double *cell_out) {
+  const tlm_oracle_problem *p = &s->p;
+  if (timestep != s->timestep + 1) return -10;
+  if (half == 1) {
+    /* run_TLM.F90:236-238, before the excitation of the step */
+    if (p->n_small_to_zero > 0 && timestep % p->n_small_to_zero == 0) set_small_to_zero(s);
+    excitation(s, timestep);
+    int rc = scatter(s);
+    if (rc) return rc;
+    if (cell_out && p->n_out_cells) memcpy(cell_out, s->cell_out, sizeof(double) * p->n_out_cells * 6);
+    return 0;
+  }
+  if (half != 2) return -11;
+  double time = (timestep - 1) * p->dt + p->dt / 2.0;
+  connect(s);
+  if (s->err) return s->err;
+  /* face_output_points (output_points.F90:255-444): side 1/2 of the output face */
+  for (int q = 0; q < p->n_face_probes; q++)
+    s->face_probe_rec[(size_t)(timestep - 1) * p->n_face_probes + q] =
+        s->face_out[(size_t)(p->fprobe_face[q] - 1) * 12 + (p->fprobe_side[q] - 1) * 6 + (p->fprobe_comp[q] - 1)];
+  dft_surfaces(s, time);
+  far_field_surfaces(s, time);
+  outer_boundary(s, timestep);
+  wrap_outer_boundary(s);
+  s->timestep = timestep;
+  return 0;
+}
+
 int tlm_oracle_run(tlm_oracle_state *s, int32_t first_step, int32_t n_steps, double *cell_out) {
   const tlm_oracle_problem *p = &s->p;
   if (first_step != s->timestep + 1) return -10;
   for (int k = 0; k < n_steps; k++) {
-    int timestep = first_step + k;
-    /* run_TLM.F90:236-238, before the excitation of the step */
-    if (p->n_small_to_zero > 0 && timestep % p->n_small_to_zero == 0) set_small_to_zero(s);
-    double time = (timestep - 1) * p->dt;
-    excitation(s, timestep);
-    int rc = scatter(s);
+    int rc = tlm_oracle_half_step(s, first_step + k, 1, cell_out ? cell_out + (size_t)k * p->n_out_cells * 6 : NULL);
     if (rc) return rc;
-    if (cell_out && p->n_out_cells)
-      memcpy(cell_out + (size_t)k * p->n_out_cells * 6, s->cell_out, sizeof(double) * p->n_out_cells * 6);
-    time = time + p->dt / 2.0;
-    connect(s);
-    if (s->err) return s->err;
-    /* face_output_points (output_points.F90:255-444): side 1/2 of the output face */
-    for (int q = 0; q < p->n_face_probes; q++)
-      s->face_probe_rec[(size_t)(timestep - 1) * p->n_face_probes + q] =
-          s->face_out[(size_t)(p->fprobe_face[q] - 1) * 12 + (p->fprobe_side[q] - 1) * 6 + (p->fprobe_comp[q] - 1)];
-    dft_surfaces(s, time);
-    far_field_surfaces(s, time);
-    outer_boundary(s, timestep);
-    wrap_outer_boundary(s);
-    s->timestep = timestep;
+    rc = tlm_oracle_half_step(s, first_step + k, 2, NULL);
+    if (rc) return rc;
   }
+  return 0;
+}
+
+int tlm_oracle_get_zplane(tlm_oracle_state *s, int32_t plane, double *out) {
+  if (plane != 0 && plane != 1) return -11;
+  const int cz = plane ? s->nz : 0;
+  size_t k = 0;
+  for (int port = 0; port < 2; port++)
+    for (int cy = 1; cy <= s->ny; cy++)
+      for (int cx = 1; cx <= s->nx; cx++) out[k++] = V_(port ? Vy_zmax : Vx_zmax, cx, cy, cz);
+  return 0;
+}
+
+int tlm_oracle_set_zplane(tlm_oracle_state *s, int32_t plane, const double *in) {
+  if (plane != 0 && plane != 1) return -11;
+  const int cz = plane ? s->nz : 0;
+  size_t k = 0;
+  for (int port = 0; port < 2; port++)
+    for (int cy = 1; cy <= s->ny; cy++)
+      for (int cx = 1; cx <= s->nx; cx++) V_(port ? Vy_zmax : Vx_zmax, cx, cy, cz) = in[k++];
   return 0;
 }
 

@@ -152,6 +152,14 @@ typedef struct {
   /* wrapping boundaries on x, y, z (0 or 1): wrap_outer_boundary after
      outer_boundary (TLM_SOLVER/wrap_outer_boundary.F90:101-273) */
   int32_t wrap[3];
+
+  /* z-slab of a partitioned mesh (the reference's MPI build,
+     general_mesh_subroutines.F90:868-972): slab[0] = 1 when a slab lies
+     below (its top plane's Vx_zmax, Vy_zmax arrive in the ghost plane
+     below this slab's first plane, and the z-faces between them are
+     connected here), slab[1] = 1 when one lies above.  The outer boundary
+     is not applied on such a side. */
+  int32_t slab[2];
 } tlm_oracle_problem;
 
 typedef struct tlm_oracle_state tlm_oracle_state;
@@ -174,6 +182,16 @@ int tlm_oracle_get_links(tlm_oracle_state *s, double *out);
    arithmetic of every cell and face is unchanged, so the results are the
    same for any count (at most 256).  Returns the count in use. */
 int tlm_oracle_set_threads(tlm_oracle_state *s, int32_t threads);
+/* one timestep in the two halves a partitioned run exchanges data between
+   (run_TLM.F90:242-291): half 1 = excitation, scatter, cell_output (then
+   TLM_parallel_pass_data_1); half 2 = connect, face outputs, outer boundary,
+   wrapping (then TLM_parallel_pass_data_2).  tlm_oracle_run does both. */
+int tlm_oracle_half_step(tlm_oracle_state *s, int32_t timestep, int32_t half, double *cell_out);
+/* the two ports of a z-plane the passes carry, as [2][ny][nx] (Vx_zmax,
+   Vy_zmax), TLM_parallel_pass_data.F90:38-279: plane 0 = the ghost plane
+   below the slab, plane 1 = the slab's top plane */
+int tlm_oracle_get_zplane(tlm_oracle_state *s, int32_t plane, double *out);
+int tlm_oracle_set_zplane(tlm_oracle_state *s, int32_t plane, const double *in);
 
 #ifdef __cplusplus
 }
