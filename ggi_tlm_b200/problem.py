@@ -1377,6 +1377,11 @@ def build_tables(spec: ProblemSpec) -> dict:
         [out_number[(o.cell[2] - 1) * nx * ny + (o.cell[1] - 1) * nx + o.cell[0] - 1] for o in centre_outs],
         dtype=np.int32)
     tables["out_comp"] = np.array([COMPONENTS[o.component] for o in centre_outs], dtype=np.int32)
+    # geometry of the solve for host-side policies (not uploaded): 1-based
+    # cells of the centre output points and point sources, PML depth per face
+    tables["out_xyz"] = np.array([o.cell for o in centre_outs], dtype=np.int32).reshape(-1, 3)
+    tables["pt_xyz"] = np.array([q.cell for q in centre_pts], dtype=np.int32).reshape(-1, 3)
+    tables["pml_depth"] = np.array(spec.pml_cells, dtype=np.int32)
     tables["out_keep"] = point_out.reshape(-1)[cell_out.reshape(-1)].astype(np.int32)
     # 1-based output point numbers (output_points(:) order) of the centre and face points, for .tout files
     tables["out_point_no"] = np.array([i + 1 for i, q in enumerate(spec.outputs) if q.face == "centre"], dtype=np.int32)
