@@ -46,7 +46,7 @@ EXPORTS = [
     "tlm_gpu_fetch_sar_volumes", "tlm_gpu_set_power_surfaces", "tlm_gpu_fetch_power_surfaces",
     "tlm_gpu_set_mode_outputs", "tlm_gpu_fetch_mode_outputs", "tlm_gpu_set_face_materials",
     "tlm_gpu_set_thin_layers", "tlm_gpu_set_face_thin_layers", "tlm_gpu_set_wrap",
-    "tlm_gpu_halo_bytes", "tlm_gpu_halo_get", "tlm_gpu_halo_put",
+    "tlm_gpu_halo_bytes", "tlm_gpu_halo_get", "tlm_gpu_halo_put", "tlm_gpu_set_test_wait_pad",
 ]
 
 
@@ -128,6 +128,7 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_face_thin_layers": [i64, i32, _i32p],
         "tlm_gpu_set_wrap": [i64, i32, i32, i32],
         "tlm_gpu_halo_bytes": [i64, C.POINTER(i64)],
+        "tlm_gpu_set_test_wait_pad": [i64, i32],
         "tlm_gpu_halo_get": [i64, i32, C.c_void_p],
         "tlm_gpu_halo_put": [i64, i32, C.c_void_p],
         "tlm_gpu_fetch_mode_outputs": [i64, i32, i32, _f64p],

@@ -329,6 +329,7 @@ struct Mesh {
   double small_value = 0.0;
   int pml_prefetch = 1200;  // blocks ahead for the PML state L2 prefetch (0 = off)
   bool pml_by_class = false;  // PML parameters loaded by distance class (pml_cls_par)
+  uint32_t tx_pad = 0;        // tlm_gpu_set_test_wait_pad
   SideStream side;          // PML / PML-material / special kernels beside the bulk kernel
   bool side_on = false;
 
@@ -416,6 +417,7 @@ tlm::MeshDev<T> mesh_dev(Mesh *m) {
   d.dt = m->desc.dt;
   d.d_base = (const int *)m->d_base.p;
   d.wrap = m->wrap;
+  d.tx_pad = m->tx_pad;
   return d;
 }
 
@@ -2473,6 +2475,19 @@ int halo_copy(int64_t h, int32_t side, void *dev, bool put) {
   return TLM_OK;
 }
 }  // namespace
+
+int tlm_gpu_set_test_wait_pad(int64_t h, int32_t bytes) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (bytes < 0 || bytes > 4096 || bytes % 16)
+    return fail(TLM_E_BADARG, "wait pad must be a multiple of 16 bytes in [0, 4096]");
+  if (m->graph) {  // the captured launches hold the old value
+    cudaGraphExecDestroy(m->graph);
+    m->graph = nullptr;
+  }
+  m->tx_pad = (uint32_t)bytes;
+  return TLM_OK;
+}
 
 int tlm_gpu_halo_bytes(int64_t h, int64_t *bytes) {
   Mesh *m = get(h);

@@ -132,6 +132,9 @@ struct MeshDev {
   double dl, dt;
   const int *d_base;        // device step counter (1-based step of relative step 0)
   int wrap;                 // wrapping boundaries: bit 0 x, bit 1 y, bit 2 z (wrap_outer_boundary.F90)
+  // bytes added to what every bulk-copy wait of the TMA cell kernel expects:
+  // 0, except under tlm_gpu_set_test_wait_pad (the waits then run out)
+  uint32_t tx_pad;
 };
 
 // The ghost slot a boundary cell writes: R times its reflected pulse on a
@@ -819,7 +822,7 @@ __device__ __forceinline__ void tma_issue(const MeshDev<T> &m, const T *in, cons
   const int len = tile.z;
   const uint32_t xb = (uint32_t)((len + 2 * C::H) * sizeof(T));
   const uint32_t yb = (uint32_t)(len * sizeof(T));
-  mbar_expect_tx(bar, 4 * xb + 8 * yb);
+  mbar_expect_tx(bar, 4 * xb + 8 * yb + m.tx_pad);
   // buffer b holds the source plane of incident port b (plane of the opposite port)
   const long long dy = m.Px, dz = m.PxPy;
   // x-planes, with a 16-byte halo on both sides

@@ -23,10 +23,11 @@
  *    (set_update_codes.F90:316, scatter.F90:561-567).
  *  - One host thread per handle.  The library launches on its own CUDA
  *    stream unless tlm_gpu_set_stream() gives it one.
- *  - Features outside the GPU path (cables, Ngspice, surface/thin-layer
- *    materials, diodes/switches, periodic or wrapping boundaries, mode
- *    stirring, MPI np>1, PML cells inside dispersive materials) are rejected
- *    with TLM_E_UNSUPPORTED at set-time.
+ *  - Features outside the GPU path (cables, Ngspice, diode/switch/SPICE-port
+ *    surface materials, periodic boundaries, mode stirring, PML cells inside
+ *    dispersive materials) are rejected with TLM_E_UNSUPPORTED at set-time.
+ *    The MPI build's z-slabs map to one mesh per slab with the halo calls
+ *    (tlm_gpu_halo_get / tlm_gpu_halo_put).
  */
 #ifndef TLM_GPU_H
 #define TLM_GPU_H
@@ -413,6 +414,15 @@ int tlm_gpu_fetch_links_noalloc(int64_t handle, double *out);
 int tlm_gpu_halo_bytes(int64_t handle, int64_t *bytes);
 int tlm_gpu_halo_get(int64_t handle, int32_t side, void *dev);
 int tlm_gpu_halo_put(int64_t handle, int32_t side, const void *dev);
+
+/* Test hook for the bounded waits (no counterpart in the reference): adds
+   `bytes` (a multiple of 16, at most 4096; 0 = normal operation) to the byte
+   count that every bulk-copy wait of the mesh's TMA cell kernel expects.
+   The copies all complete, but the waits cannot, so each runs out after its
+   2 s limit, the kernel records TLM_E_TIMEOUT and returns, and the next
+   tlm_gpu_synchronize (or tlm_gpu_batch_synchronize) reports it.  The mesh's
+   results are then invalid; the device context stays usable. */
+int tlm_gpu_set_test_wait_pad(int64_t handle, int32_t bytes);
 
 /* Use a caller CUDA stream (cudaStream_t passed as void*; NULL = own). */
 int tlm_gpu_set_stream(int64_t handle, void *stream);
