@@ -47,6 +47,7 @@ EXPORTS = [
     "tlm_gpu_set_mode_outputs", "tlm_gpu_fetch_mode_outputs", "tlm_gpu_set_face_materials",
     "tlm_gpu_set_thin_layers", "tlm_gpu_set_face_thin_layers", "tlm_gpu_set_wrap",
     "tlm_gpu_halo_bytes", "tlm_gpu_halo_get", "tlm_gpu_halo_put", "tlm_gpu_set_test_wait_pad",
+    "tlm_gpu_set_dft_gate",
 ]
 
 
@@ -129,6 +130,7 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_wrap": [i64, i32, i32, i32],
         "tlm_gpu_halo_bytes": [i64, C.POINTER(i64)],
         "tlm_gpu_set_test_wait_pad": [i64, i32],
+        "tlm_gpu_set_dft_gate": [i64, i32, _i32p, _i32p, _i32p],
         "tlm_gpu_halo_get": [i64, i32, C.c_void_p],
         "tlm_gpu_halo_put": [i64, i32, C.c_void_p],
         "tlm_gpu_fetch_mode_outputs": [i64, i32, i32, _f64p],
@@ -309,6 +311,9 @@ class GpuMesh:
             df = [_f64(t["dft_freq"]), _i32(t["dft_comp"]), _i32(t["dft_face_ptr"]), _i32(t["dft_face_out"]),
                   _i32(t["dft_face_side"])]
             _check(lib.tlm_gpu_set_dft(self.h, int(t["n_dft"]), *[_p(x) for x in df]))
+            if "dft_first" in t:
+                dg = [_i32(t["dft_first"]), _i32(t["dft_last"]), _i32(t["dft_interval"])]
+                _check(lib.tlm_gpu_set_dft_gate(self.h, int(t["n_dft"]), *[_p(x) for x in dg]))
         if int(t.get("n_ff", 0)):
             ff = [_f64(t["ff_freq"]), _i32(t["ff_face_ptr"]), _i32(t["ff_face_out"]), _i32(t["ff_face_code"])]
             _check(lib.tlm_gpu_set_far_field(self.h, int(t["n_ff"]), *[_p(x) for x in ff]))

@@ -295,6 +295,7 @@ struct Mesh {
   int n_dft = 0;
   std::vector<double> dft_freq;
   std::vector<int32_t> dft_comp, dft_ptr, dft_fout, dft_fcode;
+  std::vector<int32_t> dft_gate;  // [n_dft][3] first, last, interval (empty: every step)
 
   // device buffers
   DevBuf links, seg_mask, seg_base, sp_rec, sp_pos, pml_state, pml_par, pml_ixt, filt, mats_d, exc_field, exc_type,
@@ -1084,6 +1085,12 @@ int finalize(Mesh *m) {
       double time = (double)t * D.dt;  // (timestep-1)*dt
       time = time + D.dt / 2.0;
       for (int d = 0; d < m->n_dft; d++) {
+        // get_output_flag (output.F90:564-598): a step outside the
+        // surface's output steps adds value * 0
+        if (!m->dft_gate.empty()) {
+          const int ts = t + 1, f = m->dft_gate[3 * d], l = m->dft_gate[3 * d + 1], iv = m->dft_gate[3 * d + 2];
+          if (ts < f || ts > l || (ts - f) % iv != 0) continue;
+        }
         const double arg = -2.0 * pi * m->dft_freq[d] * time;
         ph[(size_t)t * m->n_dft + d] = double2{cos(arg), sin(arg)};
       }
@@ -2163,6 +2170,23 @@ int tlm_gpu_set_dft(int64_t h, int32_t n, const double *freq, const int32_t *com
   m->dft_fcode.assign(fcode, fcode + ne);
   for (int k = 0; k < ne; k++)
     if (fcode[k] < 1 || fcode[k] > 6) return fail(TLM_E_BADARG, "DFT face code out of range");
+  return TLM_OK;
+}
+
+int tlm_gpu_set_dft_gate(int64_t h, int32_t n, const int32_t *first, const int32_t *last,
+                         const int32_t *interval) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n != m->n_dft) return fail(TLM_E_BADARG, "gate count %d differs from the %d surfaces of tlm_gpu_set_dft", n, m->n_dft);
+  if (n && (!first || !last || !interval)) return fail(TLM_E_BADARG, "null gate array");
+  m->dft_gate.clear();
+  for (int d = 0; d < n; d++) {
+    if (first[d] < 1 || interval[d] < 1) return fail(TLM_E_BADARG, "DFT gate of surface %d: first and interval >= 1", d);
+    m->dft_gate.push_back(first[d]);
+    m->dft_gate.push_back(last[d]);
+    m->dft_gate.push_back(interval[d]);
+  }
   return TLM_OK;
 }
 

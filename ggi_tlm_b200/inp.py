@@ -749,14 +749,13 @@ def _read_outputs(rec: Dict[str, Records], mesh: Mesh, dt: float, spec: ProblemS
             if "box" in geo:
                 raise UnsupportedFeature("frequency output surface on a closed box: planar patches or a mesh "
                                          "file's faces only")
-            if t is not None and (t[0] > 1 or t[1] < spec.n_timesteps or t[2] != 1):
-                raise UnsupportedFeature("frequency output surface with output timing: every step only")
+            gate = _steps(t)  # the surface's output steps (get_output_flag)
             if "plane" in geo:
                 ax, ix, r0, r1 = geo["plane"]
-                spec.dft_surfaces.append(DFTSurface(ax, ix, r0, r1, [freq], comp, side=eff))
+                spec.dft_surfaces.append(DFTSurface(ax, ix, r0, r1, [freq], comp, side=eff, **gate))
             else:
                 spec.dft_surfaces.append(DFTSurface(0, 0, (0, 0), (0, 0), [freq], comp, side=eff,
-                                                    records=geo["records"]))
+                                                    records=geo["records"], **gate))
     if "far_field_surface_list" in rec:  # read_far_field_surface.F90:79-165
         r = rec["far_field_surface_list"]
         post["far_field"] = []

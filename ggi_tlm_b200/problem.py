@@ -724,6 +724,9 @@ class DFTSurface:
     component: str
     side: int = 1
     records: Optional[List[Tuple[Tuple[int, int, int], int]]] = None
+    first_step: int = 1            # output steps first..last every interval
+    last_step: Optional[int] = None  # (get_output_flag, output.F90:564-598); None = the final step
+    interval: int = 1
 
     def faces(self) -> List[Tuple[Tuple[int, int, int], int]]:
         if self.records is not None:
@@ -1427,18 +1430,24 @@ def build_tables(spec: ProblemSpec) -> dict:
                   vdft_cell_out=np.array(vout, dtype=np.int32))
 
     # DFT surfaces: one reference surface entry per frequency
-    freqs, comps, ptr, fo, fs = [], [], [0], [], []
+    freqs, comps, ptr, fo, fs, gate = [], [], [0], [], [], []
     for ds, faces in zip(spec.dft_surfaces, dft_faces):
+        if ds.first_step < 1 or ds.interval < 1:
+            raise ValueError("frequency output surface first step and interval must be at least 1")
         for fr in ds.frequencies:
             freqs.append(fr)
             comps.append(COMPONENTS[ds.component])
+            gate.append((ds.first_step, nsteps if ds.last_step is None else ds.last_step, ds.interval))
             for c, code in faces:  # the face code says which side's field the entry reads
                 fo.append(fout_num[connect_key(c, code)])
                 fs.append(code)
             ptr.append(len(fo))
     tables.update(n_dft=len(freqs), dft_freq=np.array(freqs, dtype=np.float64),
                   dft_comp=np.array(comps, dtype=np.int32), dft_face_ptr=np.array(ptr, dtype=np.int32),
-                  dft_face_out=np.array(fo, dtype=np.int32), dft_face_side=np.array(fs, dtype=np.int32))
+                  dft_face_out=np.array(fo, dtype=np.int32), dft_face_side=np.array(fs, dtype=np.int32),
+                  dft_first=np.array([g[0] for g in gate], dtype=np.int32),
+                  dft_last=np.array([g[1] for g in gate], dtype=np.int32),
+                  dft_interval=np.array([g[2] for g in gate], dtype=np.int32))
     # far-field surfaces: one reference surface entry per frequency
     ffreq, fptr, ffo, ffc = [], [0], [], []
     for ff, fl in zip(spec.far_field_surfaces, ff_faces):

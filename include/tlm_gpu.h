@@ -323,6 +323,15 @@ int tlm_gpu_fetch_mode_outputs(int64_t handle, int32_t first_step, int32_t n_ste
 int tlm_gpu_set_dft(int64_t handle, int32_t n_surfaces, const double *frequency, const int32_t *component,
                     const int32_t *face_ptr, const int32_t *face_out, const int32_t *face_code);
 
+/* Output steps of each frequency-domain output surface entry (call after
+   tlm_gpu_set_dft, same count): timesteps first..last every interval
+   contribute (get_output_flag, SRC/OUTPUT/output.F90:564-598, as
+   face_output_frequency_output_surfaces applies it,
+   frequency_output_surfaces.F90:336-342).  Without this call every step
+   contributes. */
+int tlm_gpu_set_dft_gate(int64_t handle, int32_t n_surfaces, const int32_t *first_timestep,
+                         const int32_t *last_timestep, const int32_t *timestep_interval);
+
 /* set_small_to_zero packet (SRC/PROCESS_INPUT_FILE/read_small_to_zero.F90:
    55-59): before the excitation of every timestep that is a multiple of
    n_small_to_zero, incident link pulses with |V| < small_to_zero_value

@@ -54,6 +54,7 @@ class _Problem(C.Structure):
         ("ff_face_code", _i32p), ("face_mat", _i32p),
         ("face_smat", _i32p), ("n_smat", C.c_int32), ("smat_f", _f64p), ("smat_a", _f64p), ("smat_b", _f64p),
         ("smat_order", _i32p), ("wrap", C.c_int32 * 3), ("slab", C.c_int32 * 2),
+        ("dft_gate", _i32p),
     ]
 
 
@@ -145,6 +146,11 @@ class Oracle:
             p.face_mat = arr("face_mat", np.int32)  # else NULL: no surface materials
         p.wrap[:] = [int(v) for v in t.get("wrap", (0, 0, 0))]
         p.slab[:] = [int(v) for v in t.get("slab", (0, 0))]
+        if int(t.get("n_dft", 0)) and "dft_first" in t:
+            g = np.ascontiguousarray(np.stack([t["dft_first"], t["dft_last"], t["dft_interval"]], axis=1),
+                                     dtype=np.int32)
+            keep.append(g)
+            p.dft_gate = g.ctypes.data_as(_i32p)
         if int(t.get("n_smat", 0)):
             p.face_smat = arr("face_smat", np.int32)
             p.n_smat = int(t["n_smat"])

@@ -1139,10 +1139,18 @@ static void wrap_outer_boundary(tlm_oracle_state *s) {
 }
 
 /* face_output_frequency_output_surfaces, frequency_output_surfaces.F90:297-421 */
-static void dft_surfaces(tlm_oracle_state *s, double time) {
+/* get_output_flag, OUTPUT/output.F90:564-598 */
+static int output_flag(int timestep, int first, int last, int interval) {
+  if (timestep < first || timestep > last) return 0;
+  return (timestep - first) % interval == 0;
+}
+
+static void dft_surfaces(tlm_oracle_state *s, double time, int timestep) {
   const tlm_oracle_problem *p = &s->p;
   const double pi = 3.141592653589793;
   for (int d = 0; d < p->n_dft; d++) {
+    if (p->dft_gate && !output_flag(timestep, p->dft_gate[3 * d], p->dft_gate[3 * d + 1], p->dft_gate[3 * d + 2]))
+      continue;
     double arg = -2.0 * pi * p->dft_freq[d] * time;
     double er = cos(arg), ei = sin(arg); /* exp(-j*2*pi*f*t) */
     int comp = p->dft_comp[d];
@@ -1232,7 +1240,7 @@ int tlm_oracle_half_step(tlm_oracle_state *s, int32_t timestep, int32_t half, do
   for (int q = 0; q < p->n_face_probes; q++)
     s->face_probe_rec[(size_t)(timestep - 1) * p->n_face_probes + q] =
         s->face_out[(size_t)(p->fprobe_face[q] - 1) * 12 + (p->fprobe_side[q] - 1) * 6 + (p->fprobe_comp[q] - 1)];
-  dft_surfaces(s, time);
+  dft_surfaces(s, time, timestep);
   far_field_surfaces(s, time);
   outer_boundary(s, timestep);
   wrap_outer_boundary(s);

@@ -160,6 +160,11 @@ typedef struct {
      connected here), slab[1] = 1 when one lies above.  The outer boundary
      is not applied on such a side. */
   int32_t slab[2];
+
+  /* output steps of each frequency output surface entry, [n_dft][3] =
+     first, last, interval (get_output_flag, OUTPUT/output.F90:564-598);
+     NULL: every step */
+  const int32_t *dft_gate;
 } tlm_oracle_problem;
 
 typedef struct tlm_oracle_state tlm_oracle_state;
