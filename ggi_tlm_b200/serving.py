@@ -80,6 +80,73 @@ def footprint_bytes(t: dict, precision: int = capi.TLM_PRECISION_FP32) -> int:
     return int(links + pml + special + filt + outs + dft + (1 << 20))
 
 
+def fp32_error_features(t: dict) -> np.ndarray:
+    """Per centre output point, the quantities the FP32 path's probe error
+    grows with: [log10 steps, log10 distance to the nearest point source
+    (cells), log10 (cells between the point and the PML + 1)].
+
+    The FP32 path rounds every stored pulse once a step; the rounding error
+    accumulates over the solve (a Gaussian source leaves a static field
+    that the same rounding meets every step), is largest against a weak
+    signal (far from the source), and grows near and inside the PML, whose
+    18-value state is stored in FP32 too."""
+    n = float(t["n_timesteps"])
+    dims = (int(t["nx"]), int(t["ny"]), int(t["nz"]))
+    depth = np.asarray(t.get("pml_depth", np.zeros(6)), dtype=np.int64)
+    src = np.asarray(t.get("pt_xyz", np.zeros((0, 3))), dtype=np.float64).reshape(-1, 3)
+    rows = []
+    for p in np.asarray(t.get("out_xyz", np.zeros((0, 3))), dtype=np.int64).reshape(-1, 3):
+        d = float(np.min(np.linalg.norm(src - p, axis=1))) if len(src) else 1.0
+        gap = min(min(int(p[a]) - 1 - int(depth[2 * a]), dims[a] - int(depth[2 * a + 1]) - int(p[a]))
+                  for a in range(3))
+        rows.append([np.log10(n), np.log10(max(d, 1.0)), np.log10(max(gap, 0) + 1.0)])
+    return np.array(rows, dtype=np.float64).reshape(-1, 3)
+
+
+def fit_fp32_error_model(records: List[dict]) -> dict:
+    """Least-squares fit of log10(probe error) on ``fp32_error_features``
+    over measured solves (records: {"features": [[...]...], "errors": [...]}
+    per solve, FP32 against FP64 over the complete solve), with the largest
+    residual as the margin: ``coef`` (intercept first) and ``margin``
+    (decades)."""
+    X, y = [], []
+    for r in records:
+        for f, e in zip(r["features"], r["errors"]):
+            if e > 0:
+                X.append([1.0] + list(f))
+                y.append(np.log10(e))
+    X, y = np.asarray(X), np.asarray(y)
+    coef = np.linalg.lstsq(X, y, rcond=None)[0]
+    return {"coef": [float(c) for c in coef], "margin": float(np.max(y - X @ coef)), "n_points": int(len(y))}
+
+
+def fp32_error_bound(t: dict, model: dict) -> float:
+    """Predicted upper bound of the FP32 path's worst probe error (relative
+    L2 over the solve) for a solve: the fitted model plus its margin, max
+    over the centre output points (0 for a solve without any)."""
+    f = fp32_error_features(t)
+    if not len(f):
+        return 0.0
+    c = np.asarray(model["coef"])
+    return float(10.0 ** (np.max(c[0] + f @ c[1:]) + model["margin"]))
+
+
+# fit_fp32_error_model over the FP32-vs-FP64 probe errors of the 256 solves
+# of cases.serving_requests(256, seed=8) measured on a B200
+# (tests/golden/fp32_error_records_seed8.json); the margin is the fit's
+# largest residual, so the bound is conservative for every point it saw.
+FP32_ERROR_MODEL = {"coef": [-6.745025873005773, 0.567966542539742, 0.6486369769777525, -0.676307771673149],
+                    "margin": 1.2867681759536773, "n_points": 512}
+
+
+def precision_by_error(model: dict, tol: float = 1e-4) -> Callable[[dict], int]:
+    """A per-request precision rule for ``GpuEngine(choose=...)``: FP32 when
+    the predicted error bound is within ``tol``, FP64 otherwise."""
+    def choose(t: dict) -> int:
+        return capi.TLM_PRECISION_FP32 if fp32_error_bound(t, model) <= tol else capi.TLM_PRECISION_FP64
+    return choose
+
+
 def _output_bytes(t: dict) -> int:
     """Device bytes of the optional outputs: far-field, power-surface, SAR
     accumulators and their phasor tables, output-surface and output-volume

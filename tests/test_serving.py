@@ -120,3 +120,60 @@ def test_footprint_counts_optional_outputs():
     extra = serving.footprint_bytes(t1) - serving.footprint_bytes(t0)
     # the two histories alone: 13*13 faces and 10^3 cells, 100 steps each, 8 bytes a value
     assert extra >= (13 * 13 + 1000) * 100 * 8
+
+
+def test_fp32_error_features_geometry():
+    """Features of a solve: steps, source distance, cells to the PML."""
+    s = cases.pml_point_source(40, 30, 24, pml=4, steps=1000, n_probes=0)
+    from ggi_tlm_b200.problem import OutputPoint
+    s.outputs = [OutputPoint((20, 15, 12), "Ex"), OutputPoint((5, 15, 12), "Ex"), OutputPoint((3, 3, 3), "Ey")]
+    t = build_tables(s)
+    src = np.asarray(s.point_excitations[0].cell, dtype=float)
+    f = serving.fp32_error_features(t)
+    assert f.shape == (3, 3)
+    np.testing.assert_allclose(f[:, 0], 3.0)
+    np.testing.assert_allclose(10 ** f[0, 1], max(1.0, np.linalg.norm(src - (20, 15, 12))))
+    # cells 1..4 are PML: cell 5 touches it (gap 0), cell 20 is 7 cells in along z (24 - 4 - 12 = 8, 12 - 5 = 7)
+    np.testing.assert_allclose(10 ** f[:, 2] - 1, [7, 0, 0])
+
+
+def test_fp32_error_fit_and_bound():
+    """The fit recovers a planted power law; the bound adds the largest
+    residual; the chooser routes by the bound."""
+    rng = np.random.default_rng(1)
+    coef = np.array([-7.0, 0.6, 0.8, -0.5])
+    recs = []
+    for _ in range(40):
+        f = np.column_stack([rng.uniform(3, 3.9, 2), rng.uniform(0, 2, 2), rng.uniform(0, 1.5, 2)])
+        e = 10 ** (coef[0] + f @ coef[1:] + rng.normal(0, 0.05, 2))
+        recs.append({"features": f.tolist(), "errors": e.tolist()})
+    m = serving.fit_fp32_error_model(recs)
+    np.testing.assert_allclose(m["coef"], coef, atol=0.1)
+    assert 0 < m["margin"] < 0.25 and m["n_points"] == 80
+    t = small_tables(16, 1000)
+    b = serving.fp32_error_bound(t, m)
+    f = serving.fp32_error_features(t)
+    assert b == pytest.approx(10 ** (np.max(m["coef"][0] + f @ np.asarray(m["coef"][1:])) + m["margin"]))
+    assert serving.precision_by_error(m, tol=b * 1.01)(t) == capi.TLM_PRECISION_FP32
+    assert serving.precision_by_error(m, tol=b * 0.99)(t) == capi.TLM_PRECISION_FP64
+    longer = small_tables(16, 4000)
+    assert serving.fp32_error_bound(longer, m) > b
+
+
+def test_fp32_error_model_is_the_fit_of_the_measured_records():
+    """The routing model is the fit of the FP32-vs-FP64 errors measured on a
+    B200 over the 256 solves of a trace with another seed than the serving
+    benchmark's (tests/golden/make_fp32_error_records.py)."""
+    import json
+    import os
+
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fp32_error_records_seed8.json")
+    d = json.load(open(path))
+    assert d["seed"] == 8 and len(d["records"]) == 256
+    m = serving.fit_fp32_error_model(d["records"])
+    np.testing.assert_allclose(m["coef"], serving.FP32_ERROR_MODEL["coef"], rtol=1e-9)
+    assert m["margin"] == pytest.approx(serving.FP32_ERROR_MODEL["margin"], rel=1e-9)
+    # the features the records hold are the library's own, recomputed from the trace
+    spec = cases.serving_requests(256, seed=8)[d["records"][3]["request"]]
+    np.testing.assert_allclose(serving.fp32_error_features(build_tables(spec)), d["records"][3]["features"],
+                               atol=1e-6)
