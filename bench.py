@@ -450,13 +450,39 @@ def bench_serving(device, n_requests=256):
                        "request_errors_fp32_all": [round(e, 9) for e in errs32]}}
 
 
+def run_batch_workload(args):
+    """``--workload c4``: the batched workload's step rate alone (the 96
+    boxes advanced together for W + K steps, FP32 and FP64), one JSON line;
+    small enough to run under a profiler's launch list."""
+    from ggi_tlm_b200 import build, capi, cases
+
+    build.build()
+    tabs = build_many(cases.batch_boxes())
+    cells = sum(t["nx"] * t["ny"] * t["nz"] for t in tabs)
+    out = {"workload": "batch_boxes_96", "cells": int(cells), "steps": args.steps, "warmup": max(args.warmup, 3)}
+    for key, prec in (("fp32", capi.TLM_PRECISION_FP32), ("fp64", capi.TLM_PRECISION_FP64)):
+        meshes = [capi.GpuMesh(t, precision=prec) for t in tabs]
+        b = capi.GpuBatch(meshes)
+        b.set_variant(int(os.environ.get("TLM_VARIANT", "1")))
+        b.run(max(args.warmup, 3))
+        b.run(args.steps)
+        ms, cu, launches = b.last_run()
+        out[key] = {"gcell_s": round(cu / (ms / 1e3) / 1e9, 3), "ms_per_step": round(ms / args.steps, 4),
+                    "launches_per_step": launches / args.steps}
+        b.close()
+        for g in meshes:
+            g.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="t512", choices=["t512", "t192", "c2", "c3", "c1"])
+    ap.add_argument("--workload", default="t512", choices=["t512", "t192", "c2", "c3", "c1", "c4"],
+                    help="c4: the batched workload's step rate alone (one JSON line of its own)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--quick", action="store_true", help="main workload only (no C2, C3, batch, serving sections)")
@@ -465,6 +491,9 @@ def main():
     if args.impl == "reference":  # rank 0 alone; no process group, no collective
         world, rank, _ = dist_env()
         run_reference_arm(args, world, rank)
+        return
+    if args.workload == "c4":
+        run_batch_workload(args)
         return
     world, rank, local = dist_setup()
 
