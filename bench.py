@@ -57,8 +57,11 @@ BULK_VARIANTS = [(0, 0, 0, 0), (1024, 2, 512, 2), (512, 3, 256, 3), (512, 4, 256
 # this figure times its cells.
 NCU_TRAFFIC = {
     "pml_point_source_512^3_pml8": {
-        "bytes_per_cell": None,
-        "source": "no ncu capture of the FP64 bulk kernel yet"},
+        "bytes_per_cell": 194.95,
+        "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one tlm_bulk_tma_kernel<double,2,512,2> "
+                  "launch on the same mesh at 192^3 (1062.8 MB for 5 451 771 free-space cells, "
+                  "profiles/tlm_bulk_tma_kernel_pml_point_source_192_fp64.md), scaled to 512^3 by the free-space "
+                  "cell count"},
 }
 
 
