@@ -94,6 +94,9 @@ def workload_spec(name: str):
         return cases.pml_point_source(192, steps=300), "pml_point_source_192^3_pml8"
     if name == "c3":
         return cases.debye_slabs(), "debye_slabs_384x384x192_pml10_6slabs_dft64x64x64"
+    if name == "c3h":  # the same configuration at half the edge lengths: small enough for an ncu capture
+        return (cases.debye_slabs(192, 192, 96, steps=300),
+                "debye_slabs_192x192x96_pml10_6slabs_dft64x64x64")
     if name == "c1":
         return cases.pec_box(), "pec_box_40^3"
     raise ValueError(name)
@@ -484,7 +487,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="t512", choices=["t512", "t192", "c2", "c3", "c1", "c4"],
+    ap.add_argument("--workload", default="t512", choices=["t512", "t192", "c2", "c3", "c3h", "c1", "c4"],
                     help="c4: the batched workload's step rate alone (one JSON line of its own)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
