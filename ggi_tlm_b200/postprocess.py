@@ -21,7 +21,7 @@ from __future__ import annotations
 
 import math
 import os
-from typing import List, Sequence, Tuple
+from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -301,3 +301,141 @@ def write_rcs(name: str, t: dict, far: np.ndarray, rcs_range: Sequence[float], f
                 f.write(line + "\n")
         out.append(path)
     return out
+
+
+# The four corners of a cell face (face codes 1..6: xmin, ymin, zmin, xmax,
+# ymax, zmax) as offsets from the cell's high corner in cells, in the order
+# get_cell_face_corner_coordinates lists them (MESH/general_mesh_subroutines.F90:154-269).
+_FACE_CORNERS = {
+    1: ((-1, -1, -1), (-1, -1, 0), (-1, 0, 0), (-1, 0, -1)),
+    2: ((-1, -1, -1), (0, -1, -1), (0, -1, 0), (-1, -1, 0)),
+    3: ((-1, -1, -1), (-1, 0, -1), (0, 0, -1), (0, -1, -1)),
+    4: ((0, -1, -1), (0, 0, -1), (0, 0, 0), (0, -1, 0)),
+    5: ((-1, 0, -1), (-1, 0, 0), (0, 0, 0), (0, 0, -1)),
+    6: ((-1, -1, 0), (0, -1, 0), (0, 0, 0), (-1, 0, 0)),
+}
+# the eight corners of a cell (get_cell_corner_coordinates, :285-330) and
+# the order output_volumes.F90:416-450 writes them: six faces of four points
+_CELL_CORNERS = ((-1, -1, -1), (-1, -1, 0), (-1, 0, 0), (-1, 0, -1), (0, -1, -1), (0, -1, 0), (0, 0, 0), (0, 0, -1))
+_CELL_FACE_POINTS = (1, 2, 3, 4, 5, 8, 7, 6, 1, 5, 6, 2, 4, 3, 7, 8, 1, 4, 8, 5, 2, 6, 7, 3)
+
+
+def _corner(origin: Sequence[float], dl: float, cell: Sequence[int], off: Sequence[int]) -> Tuple[float, ...]:
+    """mesh_min + cell*dl, less dl where the offset is -1 (the reference's
+    order of operations)."""
+    return tuple((origin[a] + cell[a] * dl) - dl if off[a] else origin[a] + cell[a] * dl for a in range(3))
+
+
+def _xyz_line(p: Sequence[float]) -> str:
+    return "".join(fortran_e(v, 14, 5) for v in p)  # format(3E14.5)
+
+
+def _list_int(v: int) -> str:
+    return f"{int(v):12d}"  # gfortran list-directed INTEGER
+
+
+def surface_field_template(number: int, spec, faces, n_frames: int) -> List[str]:
+    """The template block of one output surface in ``.surface_field.tout``
+    (output_surfaces.F90:532-569): point count, face count, frame count, the
+    four corners of every face, then each face as four point numbers."""
+    out = [f"# START SURFACE FIELD FILE TEMPLATE, OUTPUT SURFACE NUMBER:{number:5d}",
+           "# Number of points:", f"{4 * len(faces):10d}", "# Number of faces:", f"{len(faces):10d}",
+           "# Number of frames:", f"{n_frames:10d}"]
+    for cell, code in faces:
+        out += [_xyz_line(_corner(spec.origin, spec.dl, cell, off)) for off in _FACE_CORNERS[code]]
+    out += [f"{4:3d}" + "".join(f"{4 * k + j:12d}" for j in range(4)) for k in range(len(faces))]
+    out.append(f"# END SURFACE FIELD FILE TEMPLATE, OUTPUT SURFACE NUMBER:{number:5d}")
+    return out
+
+
+def _output_steps(first: int, last: Optional[int], interval: int, n: int) -> List[int]:
+    """get_output_flag (OUTPUT/output.F90:564-598) over timesteps 1..n."""
+    hi = n if last is None else min(last, n)
+    return [ts for ts in range(max(first, 1), hi + 1) if (ts - first) % interval == 0]
+
+
+def surface_field_lines(spec, t: dict, values: Sequence[np.ndarray]) -> List[str]:
+    """``NAME.surface_field.tout`` (output_surfaces.F90:326-327, 532-569,
+    906-927): the number of output surfaces, each surface's template, then
+    per output timestep, per surface that outputs on it, a frame of its face
+    values (E14.5).  ``values`` holds the library's [frames, faces] array of
+    each surface (``GpuMesh.output_surfaces``)."""
+    n = int(t["n_timesteps"])
+    surfs = spec.output_surfaces
+    steps = [_output_steps(s.first_step, s.last_step, s.interval, n) for s in surfs]
+    out = ["# NUMBER OF OUTPUT SURFACES", _list_int(len(surfs))]
+    for k, s in enumerate(surfs, start=1):
+        out += surface_field_template(k, spec, s.faces(), len(steps[k - 1]))
+    frame = [0] * len(surfs)
+    row_of = [{ts: i for i, ts in enumerate(st)} for st in steps]
+    for ts in range(1, n + 1):
+        for k in range(len(surfs)):
+            if ts not in row_of[k]:
+                continue
+            frame[k] += 1
+            vals = np.asarray(values[k])[row_of[k][ts]]
+            out += ["# START OF SURFACE FIELD OUTPUT DATA", "# OUTPUT SURFACE NUMBER", _list_int(k + 1),
+                    "# FRAME NUMBER", _list_int(frame[k]), "# NUMBER OF FACES", _list_int(len(vals)),
+                    "# SURFACE FIELD DATA"]
+            out += [fortran_e(v, 14, 5) for v in vals]
+            out.append(f"# END OF SURFACE FIELD OUTPUT DATA, OUTPUT SURFACE NUMBER:{k + 1:5d}")
+    return out
+
+
+def volume_field_lines(spec, t: dict, values: Sequence[np.ndarray]) -> List[str]:
+    """``NAME.volume_field.tout`` (output_volumes.F90:227-228, 403-465,
+    718-745) for the output volumes of kind "field", numbered in order: each
+    volume's template (24 corner points and six 4-point faces a cell, cells
+    in traversal order as the mesher lists them), then per output timestep a
+    frame with each cell's value written once per face.  ``values`` is
+    ``GpuMesh.output_volumes()`` (all kinds, in the spec's order)."""
+    n = int(t["n_timesteps"])
+    vols = [(k, v) for k, v in enumerate(spec.output_volumes) if v.kind == "field"]
+    out = ["# NUMBER OF OUTPUT VOLUMES", _list_int(len(vols))]
+    steps, cells = [], []
+    for num, (k, v) in enumerate(vols, start=1):
+        st = _output_steps(v.first_step, v.last_step, v.interval, n)
+        zz, yy, xx = np.nonzero(v.mask(spec))
+        cl = [(int(x) + 1, int(y) + 1, int(z) + 1) for z, y, x in zip(zz, yy, xx)]
+        steps.append(st)
+        cells.append(cl)
+        out += [f"# START volume FIELD FILE TEMPLATE, OUTPUT volume NUMBER:{num:5d}", "# Number of points:",
+                f"{24 * len(cl):10d}", "# Number of faces:", f"{6 * len(cl):10d}", "# Number of frames:",
+                f"{len(st):10d}"]
+        for c in cl:
+            out += [_xyz_line(_corner(spec.origin, spec.dl, c, _CELL_CORNERS[q - 1])) for q in _CELL_FACE_POINTS]
+        out += [f"{4:3d}" + "".join(f"{4 * f + j:12d}" for j in range(4)) for f in range(6 * len(cl))]
+        out.append(f"# END VOLUME FIELD FILE TEMPLATE, OUTPUT VOLUME NUMBER:{num:5d}")
+    frame = [0] * len(vols)
+    row_of = [{ts: i for i, ts in enumerate(st)} for st in steps]
+    for ts in range(1, n + 1):
+        for j, (k, _) in enumerate(vols):
+            if ts not in row_of[j]:
+                continue
+            frame[j] += 1
+            vals = np.asarray(values[k])[row_of[j][ts]]
+            out += ["# START OF VOLUME FIELD OUTPUT DATA", "# OUTPUT VOLUME NUMBER", _list_int(j + 1),
+                    "# FRAME NUMBER", _list_int(frame[j]), "# NUMBER OF cellS", _list_int(6 * len(vals)),
+                    "# volume FIELD DATA"]
+            for v in vals:
+                out += [fortran_e(v, 14, 5)] * 6
+            out.append(f"# END OF VOLUME FIELD OUTPUT DATA, OUTPUT volume NUMBER:{j + 1:5d}")
+    return out
+
+
+def write_field_files(name: str, spec, t: dict, surfaces: Optional[Sequence[np.ndarray]],
+                      volumes: Optional[Sequence[np.ndarray]], directory: str = ".") -> List[str]:
+    """Write ``NAME.surface_field.tout`` and ``NAME.volume_field.tout`` when
+    the problem has output surfaces / field output volumes."""
+    written = []
+    if spec.output_surfaces and surfaces is not None:
+        path = os.path.join(directory, name + ".surface_field.tout")
+        with open(path, "w") as f:
+            f.write("\n".join(surface_field_lines(spec, t, surfaces)) + "\n")
+        written.append(path)
+    if any(v.kind == "field" for v in spec.output_volumes) and volumes is not None:
+        path = os.path.join(directory, name + ".volume_field.tout")
+        with open(path, "w") as f:
+            f.write("\n".join(volume_field_lines(spec, t, volumes)) + "\n")
+        written.append(path)
+    return written

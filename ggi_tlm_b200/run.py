@@ -24,7 +24,11 @@ and file names (TLM_MODULES/File_information.F90:143-158):
   (SAR_volumes.F90:334-622, ``postprocess``);
 - ``<problem_name>.rcs.tout`` and ``.rcs.fout``: the RCS surface's far
   field in time and its RCS spectrum (RCS_surfaces.F90:575-762,
-  ``postprocess``).
+  ``postprocess``);
+- ``<problem_name>.surface_field.tout`` and ``.volume_field.tout``: the
+  frames of the output surfaces and field output volumes with their
+  geometry templates (output_surfaces.F90:326-927,
+  output_volumes.F90:227-745, ``postprocess``).
 
 The run goes through the library's C ABI in chunks of ``--chunk`` steps,
 reading the output points back after each chunk.  The other outputs
@@ -69,13 +73,14 @@ def _volume_rows(t: dict, spec, values: List[np.ndarray], kind: str):
 def write_results(name: str, p: InpProblem, t: dict, cell_out: np.ndarray, face_out: np.ndarray,
                   volumes: Optional[List[np.ndarray]] = None, directory: str = ".",
                   power: Optional[np.ndarray] = None, far_field: Optional[np.ndarray] = None,
-                  sar: Optional[np.ndarray] = None, rcs: Optional[np.ndarray] = None) -> List[str]:
+                  sar: Optional[np.ndarray] = None, rcs: Optional[np.ndarray] = None,
+                  surfaces: Optional[List[np.ndarray]] = None) -> List[str]:
     """Write the result files of a finished run; returns the paths written.
     ``cell_out`` is [steps, n_kept, 6], ``face_out`` [n_face_points, steps],
     ``volumes`` the output volume results, ``power`` the power surface
     accumulators [faces, 4], ``far_field`` the far-field accumulators
-    [faces, 6], ``sar`` the SAR accumulators [cells, 3] and ``rcs`` the RCS
-    far field [4, points]."""
+    [faces, 6], ``sar`` the SAR accumulators [cells, 3], ``rcs`` the RCS
+    far field [4, points] and ``surfaces`` the output surface frames."""
     written = []
     n = int(t["n_timesteps"])
     if int(t["n_functions"]):
@@ -101,6 +106,7 @@ def write_results(name: str, p: InpProblem, t: dict, cell_out: np.ndarray, face_
         written += postprocess.write_sar_volumes(name, p.spec, t, sar, p.post["sar_density"], directory)
     if p.spec.rcs_surface is not None and rcs is not None:
         written += postprocess.write_rcs(name, t, rcs, p.post["rcs"], int(t["hs_fn"]), directory)
+    written += postprocess.write_field_files(name, p.spec, t, surfaces, volumes, directory)
     for kind, extn in (("average", ".volume_average_field.tout"), ("peak", ".volume_peak_field.tout")):
         if any(v.kind == kind for v in p.spec.output_volumes):
             rows, count = _volume_rows(t, p.spec, volumes, kind)
@@ -142,7 +148,8 @@ def run(name: str, precision: int = capi.TLM_PRECISION_FP64, device: int = 0, ch
         far_field = g.far_field() if p.spec.far_field_surfaces else None
         sar = g.sar_volumes() if p.spec.sar_volumes else None
         rcs = g.rcs() if p.spec.rcs_surface is not None else None
-    return write_results(name, p, t, cell_out, face_out, volumes, directory, power, far_field, sar, rcs)
+        surfaces = g.output_surfaces() if p.spec.output_surfaces else None
+    return write_results(name, p, t, cell_out, face_out, volumes, directory, power, far_field, sar, rcs, surfaces)
 
 
 def main(argv: Optional[Sequence[str]] = None) -> int:

@@ -14,6 +14,8 @@ from __future__ import annotations
 
 from typing import Iterable, List, Optional, Sequence, Tuple
 
+import math
+
 import numpy as np
 
 HEADER = "# Time Domain Data"  # time_domain_output_file_header, File_information.F90:263
@@ -28,9 +30,9 @@ def fortran_e(value: float, width: int = 16, digits: int = 7) -> str:
         return "NaN".rjust(width)
     if v in (float("inf"), float("-inf")):  # gfortran writes the word, signed only when negative
         return ("-Infinity" if v < 0 else "Infinity").rjust(width)
-    if v == 0.0:
+    if v == 0.0:  # a negative zero keeps its sign, as gfortran writes it
         body = "0." + "0" * digits + "E+00"
-        return body.rjust(width)
+        return (("-" if math.copysign(1.0, v) < 0 else "") + body).rjust(width)
     s = f"{abs(v):.{digits - 1}e}"  # d.dddddde+xx, correctly rounded to `digits` significant digits
     mant, exp = s.split("e")
     e = int(exp) + 1

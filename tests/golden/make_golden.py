@@ -69,6 +69,12 @@ RESULT_CASES = {
     "rcs_plate_fout": "RCS_PEC_PLATE_ROUGH_SURFACE/PROBLEM_SPECIFICATION_FILES/plate.rcs.fout_ref",
     "rcs_plate_tout": "RCS_PEC_PLATE_ROUGH_SURFACE/PROBLEM_SPECIFICATION_FILES/plate.rcs.tout_ref",
 }
+# the head of long result files: (file, number of leading lines kept)
+RESULT_HEADS = {
+    # HELIX_ANTENNA's surface field file: the template of its one output
+    # surface and the first data frame (output_surfaces.F90:326-927)
+    "helix_surface_field": ("HELIX_ANTENNA/helix.surface_field.tout", 10603),
+}
 # mesh files written by the reference's mesher (MESH/write_mesh.F90), as text
 MESH_CASES = {
     "helix": "HELIX_ANTENNA/helix.mesh",
@@ -144,6 +150,9 @@ def main():
     for name, rel in RESULT_CASES.items():
         with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", rel)) as f:
             rs[name] = np.array(f.read().splitlines())
+    for name, (rel, n_lines) in RESULT_HEADS.items():
+        with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", rel)) as f:
+            rs[name] = np.array(f.read().splitlines()[:n_lines])
     np.savez_compressed(os.path.join(here, "result_text.npz"), **rs)
     print("result_text", {k: len(v) for k, v in rs.items()})
     me = {}

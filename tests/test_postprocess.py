@@ -187,3 +187,60 @@ def test_gpu_pec_plate_rcs_follows_physical_optics(gpu_lib):
         if 1.5e9 <= f <= 3e9:
             po = 10.0 * np.log10(4.0 * np.pi * area ** 2 / (299792458.0 / f) ** 2)
             assert abs(rcs - po) < 1.5, (f, rcs, po)
+
+
+def helix_spec():
+    """HELIX_ANTENNA read with its mesh file, cables left out."""
+    sys.path.insert(0, HERE)
+    import test_inp as T
+    import test_meshfile as M
+    from ggi_tlm_b200 import inp, meshfile
+
+    m = meshfile.read_mesh(M.helix_mesh_lines())
+    return inp.read_inp_lenient(M.without_cables(M.helix_inp_lines()), T.materials, mesh_file=m).spec
+
+
+def test_surface_field_file_matches_the_reference_template():
+    """HELIX_ANTENNA's .surface_field.tout: the header and the template of
+    its output surface (1764 faces of the mesh file's surface, 10 frames)
+    line for line; the first data frame's framing lines (its values need
+    the cable model, which is out of scope)."""
+    gold = [str(x) for x in np.load(os.path.join(HERE, "golden", "result_text.npz"))["helix_surface_field"]]
+    s = helix_spec()
+    t = build_tables(s)
+    (surf,) = s.output_surfaces
+    n_frames = len(pp._output_steps(surf.first_step, surf.last_step, surf.interval, int(t["n_timesteps"])))
+    vals = [np.zeros((n_frames, len(surf.faces())))]
+    lines = pp.surface_field_lines(s, t, vals)
+    end = gold.index("# END SURFACE FIELD FILE TEMPLATE, OUTPUT SURFACE NUMBER:    1")
+    assert lines[:end + 1] == gold[:end + 1]
+    frame = gold[end + 1:]
+    mine = lines[end + 1:end + 1 + len(frame)]
+    assert [a for a in mine if a.startswith("#") or not a.strip().startswith(("0.", "-0."))] == \
+        [a for a in frame if a.startswith("#") or not a.strip().startswith(("0.", "-0."))]
+    assert len(mine) == len(frame)
+
+
+def test_volume_field_file_layout():
+    """A field output volume's .volume_field.tout: 24 corner points and six
+    faces a cell in output_volumes.F90's order, one frame per output step,
+    each cell's value written six times."""
+    s = cases.pml_point_source(12, pml=2, steps=7, dl=0.5, n_probes=0)
+    from ggi_tlm_b200.problem import OutputVolume
+    s.origin = (1.0, -2.0, 0.5)
+    s.output_volumes = [OutputVolume(Block(3, 4, 5, 5, 6, 6), "Ez", kind="field", first_step=2, interval=3)]
+    t = build_tables(s)
+    vals = [np.arange(2 * 2, dtype=float).reshape(2, 2) + 0.5]  # steps 2 and 5, two cells
+    lines = pp.volume_field_lines(s, t, vals)
+    assert lines[:2] == ["# NUMBER OF OUTPUT VOLUMES", "           1"]
+    assert lines[3:9] == ["# Number of points:", "        48", "# Number of faces:", "        12",
+                          "# Number of frames:", "         2"]
+    # first cell (3, 5, 6): corner 1 = origin + (cell - 1) dl, corner 7 = origin + cell dl
+    assert lines[9] == pp.fortran_e(2.0, 14, 5) + pp.fortran_e(0.0, 14, 5) + pp.fortran_e(3.0, 14, 5)
+    assert lines[9 + 6] == pp.fortran_e(2.5, 14, 5) + pp.fortran_e(0.5, 14, 5) + pp.fortran_e(3.5, 14, 5)
+    assert lines[9 + 48] == "  4           0           1           2           3"
+    start = lines.index("# START OF VOLUME FIELD OUTPUT DATA")
+    assert lines[start + 1:start + 8] == ["# OUTPUT VOLUME NUMBER", "           1", "# FRAME NUMBER", "           1",
+                                          "# NUMBER OF cellS", "          12", "# volume FIELD DATA"]
+    assert lines[start + 8:start + 20] == [pp.fortran_e(0.5, 14, 5)] * 6 + [pp.fortran_e(1.5, 14, 5)] * 6
+    assert lines.count("# START OF VOLUME FIELD OUTPUT DATA") == 2

@@ -46,13 +46,57 @@ def oracle_files(tmp, name, lines):
     face = o.face_probes() if int(t["n_face_probes"]) else np.zeros((0, t["n_timesteps"]))
     vols = oracle.output_volumes(t, cell) if p.spec.output_volumes else None
     power = oracle.power_surfaces(t) if p.spec.power_surfaces else None
-    return runner.write_results(name, p, t, cell, face, vols, tmp, power), p, t
+    surfs = oracle.output_surfaces(t) if p.spec.output_surfaces else None
+    return runner.write_results(name, p, t, cell, face, vols, tmp, power, surfaces=surfs), p, t
+
+
+# ALL_OUTPUTS with an output surface (the rectangle at z = 0.7, Ez on output
+# steps 1, 5, .., 29) and a field output volume (the Debye block, Ey)
+FIELDS = test_inp.ALL_OUTPUTS + """Output_surface_list
+1
+1
+3
+1
+Ez
+output_timestep_information
+1
+30
+4
+Output_volume_list
+1
+1
+1
+Ey
+"""
+
+
+def test_surface_and_volume_field_files(tmp_path):
+    paths, p, t = oracle_files(str(tmp_path), "fields", FIELDS.splitlines())
+    names = sorted(os.path.basename(x) for x in paths)
+    assert "fields.surface_field.tout" in names and "fields.volume_field.tout" in names
+    sf = open(os.path.join(str(tmp_path), "fields.surface_field.tout")).read().splitlines()
+    n_faces = len(p.spec.output_surfaces[0].faces())
+    assert sf[:2] == ["# NUMBER OF OUTPUT SURFACES", "           1"]
+    assert sf[4] == f"{4 * n_faces:10d}" and sf[8] == f"{8:10d}"  # 8 frames: steps 1, 5, .., 29
+    assert sf.count("# START OF SURFACE FIELD OUTPUT DATA") == 8
+    want = oracle.output_surfaces(t)[0]
+    start = sf.index("# START OF SURFACE FIELD OUTPUT DATA")
+    got = np.array([float(x) for x in sf[start + 8:start + 8 + n_faces]])
+    np.testing.assert_allclose(got, want[0], rtol=1.01e-5, atol=1e-30)
+    vf = open(os.path.join(str(tmp_path), "fields.volume_field.tout")).read().splitlines()
+    n_cells = int((p.spec.output_volumes[-1].mask(p.spec)).sum())
+    assert vf[4] == f"{24 * n_cells:10d}" and vf[8] == f"{int(t['n_timesteps']):10d}"
+    assert vf.count("# START OF VOLUME FIELD OUTPUT DATA") == int(t["n_timesteps"])
 
 
 def test_field_tout_from_the_huygens_input(tmp_path):
     lines = test_inp.inputs()["huygens_box"]
-    (exc, path), p, t = oracle_files(str(tmp_path), "huygens_test", lines)
-    assert [os.path.basename(exc), os.path.basename(path)] == ["huygens_test.excitation.tout", "huygens_test.field.tout"]
+    paths, p, t = oracle_files(str(tmp_path), "huygens_test", lines)
+    # the input also has three output surfaces and three field output volumes
+    assert [os.path.basename(x) for x in paths] == ["huygens_test.excitation.tout", "huygens_test.field.tout",
+                                                    "huygens_test.surface_field.tout",
+                                                    "huygens_test.volume_field.tout"]
+    exc, path = paths[:2]
     e = read_tout(exc)  # the Gaussian at every step, (ts-1)*dt, not flushed below 1e-30
     assert e.shape == (120, 3) and set(e[:, 1]) == {1.0}
     np.testing.assert_allclose(e[:, 2], np.asarray(t["fn_value"]).reshape(-1), rtol=5.01e-7, atol=0)
@@ -109,9 +153,10 @@ def test_runner_stops_cleanly_without_a_gpu(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name, text", [("huygens_test", None), ("all", "all")])
+@pytest.mark.parametrize("name, text", [("huygens_test", None), ("all", "all"), ("fields", "fields")])
 def test_gpu_runner_files_match_oracle_files(gpu_lib, tmp_path, name, text):
-    lines = test_inp.inputs()["huygens_box"] if text is None else test_inp.ALL_OUTPUTS.splitlines()
+    lines = (test_inp.inputs()["huygens_box"] if text is None else
+             (FIELDS if text == "fields" else test_inp.ALL_OUTPUTS).splitlines())
     run_dir, ref_dir = str(tmp_path / "run"), str(tmp_path / "oracle")
     os.makedirs(run_dir)
     os.makedirs(ref_dir)
@@ -124,6 +169,14 @@ def test_gpu_runner_files_match_oracle_files(gpu_lib, tmp_path, name, text):
         with open(a) as fa, open(b) as fb:
             la, lb = fa.read().splitlines(), fb.read().splitlines()
         assert la[:3] == lb[:3] and len(la) == len(lb)
+        if a.endswith("_field.tout") and (".surface_" in a or ".volume_field" in a):
+            # templates and framing line for line; values to the file's 5 digits
+            num = [k for k, x in enumerate(la) if not x.startswith("#") and len(x.split()) == 1 and "." in x]
+            assert [x for k, x in enumerate(la) if k not in set(num)] == \
+                [x for k, x in enumerate(lb) if k not in set(num)]
+            va, vb = np.array([float(la[k]) for k in num]), np.array([float(lb[k]) for k in num])
+            np.testing.assert_allclose(vb, va, rtol=1.01e-5, atol=1e-9 * max(np.abs(va).max(), 1e-300))
+            continue
         if a.endswith(".fout"):
             da, db = np.loadtxt(la, comments="#", ndmin=2), np.loadtxt(lb, comments="#", ndmin=2)
             np.testing.assert_allclose(db[:, 2:4], da[:, 2:4], rtol=1.01e-6, atol=1e-9 * np.abs(da[:, 2:4]).max())
