@@ -10,10 +10,12 @@ logarithmic grid the sum  V(f) = sum_k v_k exp(-j 2 pi f t_k) dt  in step
 order.  write_frequency_domain_data (read_write_frequency_domain_data.F90:
 38-83) writes a three-line header and one ``(E16.7,I5,5E16.7)`` line per
 frequency: f, the point number 1, Re V, Im V, |V|, atan2(Im, Re) and
-20 log10 |V|.
+20 log10 |V|.  Option 10 (two-port analysis, ``twoport_lines``) turns the
+spectra of two planes on each side of a scatterer into S-parameters.
 """
 from __future__ import annotations
 
+import cmath
 import math
 from typing import List, Sequence, Tuple
 
@@ -133,6 +135,63 @@ def power_surface_lines(freqs: Sequence[float], surface: Sequence[int], power: S
         lines.append(fortran_e(f) + f"{int(num):5d}" +
                      "".join(fortran_e(x) for x in (p.real, p.imag, re, math.atan2(p.imag, p.real), db)))
     return lines
+
+
+def oneport_calc(e1: complex, e2: complex, h1: complex, h2: complex, d: float) -> Tuple[complex, complex, complex]:
+    """oneport_calc (POST_PROCESSOR/oneport.F90:206-249): from E and H at
+    two output planes 2d apart in a uniform section, the propagation
+    constant beta (real part made non-negative) and the right- and
+    left-going waves Er, El at the first plane: the root P = exp(j beta d)
+    of a P^2 + b P + c = 0 with a = c = E2 H1 + E1 H2, b = -2 (E1 H1 + E2 H2)."""
+    a = e2 * h1 + e1 * h2
+    b = -2.0 * (e1 * h1 + e2 * h2)
+    c = e2 * h1 + e1 * h2
+    s = cmath.sqrt(b * b - 4.0 * a * c)
+    p1 = (-b + s) / (2.0 * a)
+    beta = cmath.log(p1) / (2.0 * 1j * d)
+    if beta.real < 0.0:
+        beta = -beta
+    p = cmath.exp(1j * beta * d)
+    eit = (e2 * p - e1 * p * p * p) / (1.0 - p * p * p * p)
+    ert = -eit * p * p + e1 * p
+    return beta, eit, ert
+
+
+def twoport_lines(freqs: Sequence[float], ft: Sequence[Sequence[complex]], d_port1: float, l1: float,
+                  d_port2: float, l2: float, excitation_port: int = 1) -> List[str]:
+    """Post-processor option 10, two-port analysis (POST_PROCESSOR/twoport.F90):
+    ``ft`` holds the spectra E11, E12, H11, H12 (the two planes of port 1)
+    and E21, E22, H21, H22 (port 2) on one frequency grid; each port's
+    planes are ``d_port`` apart with their midpoint ``l`` from the interface.
+    Returns the output file's lines: the list-directed title and per
+    frequency (12E14.5) f, Re, Im, |.|, dB of S11 and S21 (S12 and S22 when
+    port 2 is excited), then the reflected, transmitted and absorbed power."""
+    E11, E12, H11, H12, E21, E22, H21, H22 = (np.asarray(x, dtype=np.complex128) for x in ft)
+    if excitation_port == 1:
+        title = " # f,dble(S11),dimag(S11),abs(S11),20.0*log10(abs(S11)),dble(S21),dimag(S21),abs(S21)," \
+                "20.0*log10(abs(S21)), Pr, Pt, Pa"
+    elif excitation_port == 2:
+        title = " # f,dble(S12),dimag(S12),abs(S12),20.0*log10(abs(S12)),dble(S22),dimag(S22),abs(S22)," \
+                "20.0*log10(abs(S22)), Pr, Pt, Pa"
+    else:
+        raise ValueError("excitation port must be 1 or 2")
+    d1, d2 = d_port1 / 2.0, d_port2 / 2.0
+    out = [title]
+    for k, f in enumerate(freqs):
+        beta1, er1, el1 = oneport_calc(E11[k], E12[k], H11[k], H12[k], d1)
+        beta2, er2, el2 = oneport_calc(E22[k], E21[k], H22[k], H21[k], d2)
+        if excitation_port == 1:
+            sa = el1 * cmath.exp(1j * beta1 * l1) / (er1 * cmath.exp(-1j * beta1 * l1))  # S11
+            sb = er2 * cmath.exp(1j * beta2 * l2) / (er1 * cmath.exp(-1j * beta1 * l1))  # S21
+            pr, pt = abs(sa) ** 2, abs(sb) ** 2
+        else:
+            sa = el1 * cmath.exp(1j * beta1 * l1) / (el2 * cmath.exp(-1j * beta2 * l2))  # S12
+            sb = er2 * cmath.exp(1j * beta2 * l2) / (el2 * cmath.exp(-1j * beta2 * l2))  # S22
+            pr, pt = abs(sb) ** 2, abs(sa) ** 2
+        vals = (f, sa.real, sa.imag, abs(sa), 20.0 * math.log10(abs(sa)), sb.real, sb.imag, abs(sb),
+                20.0 * math.log10(abs(sb)), pr, pt, 1.0 - pr - pt)
+        out.append("".join(fortran_e(v, 14, 5) for v in vals))
+    return out
 
 
 def main(argv=None) -> int:

@@ -60,6 +60,9 @@ INP_CASES = {
        for a, p in (("X", "Y"), ("X", "Z"), ("Y", "X"), ("Y", "Z"), ("Z", "X"), ("Z", "Y"))},
     "thin_layer_stability": "THIN_LAYER_STABILITY_TEST/PROBLEM_SPECIFICATION_FILES/cavity.inp",
     "wrapping": "WRAPPING_BOUNDARY/PROBLEM_SPECIFICATION_FILES/wrapping_test.inp",
+    # a frequency selective surface: two square PEC loops in a cell wrapped in x and y, a normally
+    # incident plane wave (the case's parameter set 4, which its S21.fout_4_ref is from)
+    "fss_single_cell": "PARAMETERISED_FSS/PROBLEM_SPECIFICATION_FILES/single_cell.inp",
 }
 # the surface material files the thin-layer cases use, as text
 SMAT_CASES = ["Dispersive_sheet", "Anisotropic_sheet"]
@@ -95,6 +98,8 @@ FOUT_CASES = {
     "box_slot": "SHIELDING_EFFECTIVENESS_BOX_SLOT/PROBLEM_SPECIFICATION_FILES/Shielding_effectiveness.fout_ref",
     # written by the solver itself (write_frequency_domain_power_surfaces)
     "power_calc": "POWER_CALCS/PROBLEM_SPECIFICATION_FILES/power_calc.frequency_domain_power_surface.fout_ref",
+    # eight volume averages Fourier transformed (option 3), then the two-port analysis (option 10)
+    "fss_s21": "PARAMETERISED_FSS/PROBLEM_SPECIFICATION_FILES/S21.fout_4_ref",
 }
 
 

@@ -1,0 +1,99 @@
+"""PARAMETERISED_FSS: a frequency selective surface (two square PEC loops
+on a zplane, the cell wrapped in x and y, a normally incident plane wave
+from a Huygens plane, matched z ends), read from the reference's own input
+and carried through the reference's post-processing chain to its golden
+S21.fout_4_ref:
+
+* eight volume averages (Ey, Hx on two planes each side of the surface) as
+  the run writes them (.volume_average_field.tout, E16.7);
+* post-processor option 3 on each (fourier_transform.F90, 1000 frequencies
+  1 MHz .. 3 GHz, written and read back as .fout, E16.7);
+* option 10, the two-port analysis (twoport.F90, oneport.F90:206-249).
+
+The S-parameters come from a nearly degenerate quadratic in each port's
+two planes (0.5 mm apart against wavelengths down to 10 cm), so the 7-digit
+files round their inputs hard: the oracle's S21 matches the golden file to
+1e-4 relative and a third of its lines byte for byte.  GPU: the library's
+volume averages against the oracle's."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from ggi_tlm_b200 import fout, inp, tout
+from ggi_tlm_b200 import run as runner
+from ggi_tlm_b200.problem import build_tables
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import test_inp as T  # noqa: E402
+import oracle  # noqa: E402
+
+
+def problem():
+    p = inp.read_inp(T.inputs()["fss_single_cell"], T.materials)
+    return p, build_tables(p.spec)
+
+
+def oracle_averages(t, chunk=100):
+    """The eight volume averages [8, steps] of the oracle's run, in chunks
+    (the output cells' full history would not fit)."""
+    o = oracle.Oracle(t, threads=os.cpu_count() or 1)
+    out = []
+    n = int(t["n_timesteps"])
+    for first in range(0, n, chunk):
+        out.append(np.array(oracle.output_volumes(t, o.run(min(chunk, n - first)))))
+    o.close()
+    return np.concatenate(out, axis=1)
+
+
+def s21_lines(p, t, averages):
+    rows, count = runner._volume_rows(t, p.spec, list(averages), "average")
+    text = tout.header(count, int(t["n_timesteps"])) + [tout.data_line(a, b, c) for a, b, c in rows]
+    series = np.loadtxt([x for x in text if not x.startswith("#")], ndmin=2)
+    freqs = fout.frequencies(1e6, 3e9, 1000, "lin")
+    spec = {}
+    for k in range(1, 9):
+        tm, v = fout.tout_series(series, k)
+        fr, spec[k] = fout.spectrum(fout.read_fout(fout.format_fout(freqs, fout.fourier_transform(tm, v, freqs))))
+    # the post-processing input's order: Ex1 Ex2 Hy1 Hy2 (port 1), Ex4 Ex3 Hy4 Hy3 (port 2), where ExN and
+    # HyN are averages 2N-1 and 2N
+    ft = [spec[1], spec[3], spec[2], spec[4], spec[7], spec[5], spec[8], spec[6]]
+    return fout.twoport_lines(fr, ft, 0.5e-3, 5e-3, 0.5e-3, 5e-3, 1)
+
+
+def test_reader_takes_the_fss_input():
+    p, t = problem()
+    s = p.spec
+    assert (s.nx, s.ny, s.nz, s.n_timesteps, s.wrap) == (64, 64, 80, 2398, (1, 1, 0))
+    assert [(sh.kind, sh.axis, sh.index) for sh in s.surface_sheets] == [("PEC", 3, 40), ("free", 3, 40)] * 2
+    assert [v.kind for v in s.output_volumes] == ["average"] * 8
+    assert int(t["hs_n"]) == 64 * 64
+
+
+def test_oracle_s21_matches_the_reference_file():
+    p, t = problem()
+    got = s21_lines(p, t, oracle_averages(t))
+    gold = [str(x) for x in np.load(os.path.join(HERE, "golden", "fout_text.npz"))["fss_s21"]]
+    assert len(got) == len(gold) and got[0] == gold[0]
+    g, m = np.loadtxt(gold[1:]), np.loadtxt(got[1:])
+    np.testing.assert_array_equal(m[:, 0], g[:, 0])
+    s21g, s21m = g[:, 5] + 1j * g[:, 6], m[:, 5] + 1j * m[:, 6]
+    assert np.max(np.abs(s21m - s21g) / np.abs(s21g)) < 2e-4
+    s11g, s11m = g[:, 1] + 1j * g[:, 2], m[:, 1] + 1j * m[:, 2]
+    assert np.max(np.abs(s11m - s11g)) < 2e-4
+    assert sum(a == b for a, b in zip(got, gold)) > 300
+
+
+@pytest.mark.gpu
+def test_gpu_fss_volume_averages_match_the_oracle(gpu_lib):
+    from ggi_tlm_b200 import capi
+
+    p, t = problem()
+    want = oracle_averages(t)
+    with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64) as g:
+        g.run(int(t["n_timesteps"]))
+        got = np.array(g.output_volumes())
+    assert got.shape == want.shape
+    assert np.linalg.norm(got - want) <= 1e-10 * np.linalg.norm(want)
