@@ -31,7 +31,14 @@ CASES = {
        for a, p in (("X", "Y"), ("X", "Z"), ("Y", "X"), ("Y", "Z"), ("Z", "X"), ("Z", "Y"))},
     "thin_layer_stability": "THIN_LAYER_STABILITY_TEST/PROBLEM_SPECIFICATION_FILES/cavity.field.tout_ref",
     "wrapping_Ex": "WRAPPING_BOUNDARY/PROBLEM_SPECIFICATION_FILES/Ex_centre.tout_ref",
+    # Debye and eps_r = 1.5 blocks with PEC and dispersive thin-layer sheets
+    "material_test_Ex": "MATERIAL_TEST/PROBLEM_SPECIFICATION_FILES/mat_test.field.tout_ref",
+    # volume average 1 of a wrapped cell with an FR4 slab, PEC patches and a Huygens plane
+    # (post-processor option 1 on the run's .volume_average_field.tout); first 20000 of 59958 steps kept
+    "resonant_absorber_Ey": "RESONANT_ABSORBER/PROBLEM_SPECIFICATION_FILES/Ey.tout_ref",
 }
+# cases whose golden series is cut to its first rows
+CASE_ROWS = {"resonant_absorber_Ey": 20000}
 
 
 # raw text of the reference's .tout files (header and every data line), kept
@@ -63,6 +70,8 @@ INP_CASES = {
     # a frequency selective surface: two square PEC loops in a cell wrapped in x and y, a normally
     # incident plane wave (the case's parameter set 4, which its S21.fout_4_ref is from)
     "fss_single_cell": "PARAMETERISED_FSS/PROBLEM_SPECIFICATION_FILES/single_cell.inp",
+    "material_test": "MATERIAL_TEST/PROBLEM_SPECIFICATION_FILES/mat_test.inp",
+    "resonant_absorber": "RESONANT_ABSORBER/PROBLEM_SPECIFICATION_FILES/TEM_cell.inp",
 }
 # the surface material files the thin-layer cases use, as text
 SMAT_CASES = ["Dispersive_sheet", "Anisotropic_sheet"]
@@ -110,7 +119,7 @@ def main():
     here = os.path.dirname(os.path.abspath(__file__))
     for name, rel in CASES.items():
         path = os.path.join(ref, "GGI_TLM", "TEST_DATA", rel)
-        d = np.loadtxt(path, comments="#")
+        d = np.loadtxt(path, comments="#")[:CASE_ROWS.get(name)]
         np.savez_compressed(os.path.join(here, name + ".npz"), time=d[:, 0], point=d[:, 1].astype(np.int32),
                             value=d[:, 2], source=rel)
         print(name, d.shape)

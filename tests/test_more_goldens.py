@@ -1,0 +1,103 @@
+"""Two more of the reference's known-answer cases read from their own input
+files and run on the oracle against their golden series:
+
+* MATERIAL_TEST (mat_test.field.tout_ref): eps_r = 1.5 and one-pole Debye
+  blocks with a PEC sheet and dispersive thin-layer sheets; the output
+  point's series on its output steps (output_timestep_information), as the
+  run's .field.tout writes it;
+* RESONANT_ABSORBER (Ey.tout_ref, the first 20000 of its 59958 steps): a
+  cell wrapped in x and y, an FR4 (fitted dispersive) slab under PEC
+  patches, a normally incident plane wave from a Huygens plane; the golden
+  file is volume average 1 as the post-processor extracts it from the run's
+  .volume_average_field.tout.
+
+GPU: the library against the oracle on the same tables."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from ggi_tlm_b200 import inp
+from ggi_tlm_b200.problem import build_tables, probe_series
+from ggi_tlm_b200.tout import field_rows
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import test_inp as T  # noqa: E402
+import test_thin_layer as TL  # noqa: E402
+import oracle  # noqa: E402
+
+TOL = 5e-7  # the golden files' E16.7
+RA_STEPS = 20000
+
+
+def material_test():
+    return inp.read_inp(T.inputs()["material_test"], T.materials, thin_layer=TL.thin_layer)
+
+
+def resonant_absorber():
+    p = inp.read_inp(T.inputs()["resonant_absorber"], T.materials)
+    return p, build_tables(p.spec)
+
+
+def golden(name):
+    return np.load(os.path.join(HERE, "golden", name + ".npz"))
+
+
+def test_material_test_reproduces_its_golden_series():
+    p = material_test()
+    t = build_tables(p.spec)
+    assert int(t["n_smat"]) == 1 and int(t["n_materials"]) == 2
+    centre = probe_series(t, oracle.Oracle(t).run(int(t["n_timesteps"])))
+    rows = np.array(field_rows(t, centre, np.zeros((0, int(t["n_timesteps"]))), timing=p.output_timing))
+    g = golden("material_test_Ex")
+    assert rows.shape == (len(g["value"]), 3)
+    np.testing.assert_allclose(rows[:, 0], g["time"], rtol=TOL)
+    v = np.where(np.abs(rows[:, 2]) < 1e-30, 0.0, rows[:, 2])
+    assert np.linalg.norm(v - g["value"]) / np.linalg.norm(g["value"]) < TOL
+
+
+def resonant_averages(t, steps, chunk=2000):
+    o = oracle.Oracle(t, threads=min(4, os.cpu_count() or 1))
+    out = []
+    for first in range(0, steps, chunk):
+        out.append(np.array(oracle.output_volumes(t, o.run(min(chunk, steps - first)))))
+    o.close()
+    return np.concatenate(out, axis=1)
+
+
+def test_resonant_absorber_reproduces_its_golden_series():
+    p, t = resonant_absorber()
+    assert p.spec.wrap == (1, 1, 0) and int(t["n_timesteps"]) == 59958
+    v = resonant_averages(t, RA_STEPS)[0]
+    g = golden("resonant_absorber_Ey")
+    v = np.where(np.abs(v) < 1e-30, 0.0, v)
+    assert len(v) == len(g["value"]) == RA_STEPS
+    assert np.linalg.norm(v - g["value"]) / np.linalg.norm(g["value"]) < TOL
+
+
+@pytest.mark.gpu
+def test_gpu_material_test_matches_the_oracle(gpu_lib):
+    from ggi_tlm_b200 import capi
+
+    t = build_tables(material_test().spec)
+    want = oracle.Oracle(t).run(int(t["n_timesteps"]))
+    with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64) as g:
+        g.run(int(t["n_timesteps"]))
+        got = g.cell_output()
+    keep = np.asarray(t["out_keep"]) == 1
+    assert np.linalg.norm(got - want[:, keep]) <= 1e-10 * np.linalg.norm(want[:, keep])
+
+
+@pytest.mark.gpu
+def test_gpu_resonant_absorber_matches_the_oracle(gpu_lib):
+    from ggi_tlm_b200 import capi
+
+    _, t = resonant_absorber()
+    want = resonant_averages(t, RA_STEPS)
+    with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64) as g:
+        g.run(RA_STEPS)
+        got = np.array([v[:RA_STEPS] for v in g.output_volumes()])
+    assert got.shape == want.shape
+    assert np.linalg.norm(got - want) <= 1e-10 * np.linalg.norm(want)
