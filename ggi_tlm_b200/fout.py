@@ -21,6 +21,7 @@ from typing import List, Sequence, Tuple
 
 import numpy as np
 
+from .problem import Z0
 from .tout import fortran_e
 
 HEADER = "# Frequency Domain Data"  # frequency_domain_output_file_header
@@ -192,6 +193,29 @@ def twoport_lines(freqs: Sequence[float], ft: Sequence[Sequence[complex]], d_por
                 20.0 * math.log10(abs(sb)), pr, pt, 1.0 - pr - pt)
         out.append("".join(fortran_e(v, 14, 5) for v in vals))
     return out
+
+
+def transmission_cross_section_lines(power_rows: np.ndarray, field_rows: np.ndarray, field: str = "e") -> List[str]:
+    """Post-processor option 15, transmission cross section
+    (POST_PROCESSOR/transmission_cross_section.F90): from the transmitted
+    power (|Re| of a power surface .fout, read_fout rows) and the cavity
+    field's spectrum (|V| of an E or H .fout): TCS = Pt / Si with
+    Si = 3 (|V|/sqrt 2)^2 scale / 2, scale 1/Z0 for E and Z0 for H.  The
+    reference stores TCS through CMPLX() without a kind, so the value is
+    rounded to single precision; the dB column is 10 log10 |TCS|."""
+    fp, fe = power_rows[:, 0], field_rows[:, 0]
+    if len(fp) != len(fe) or np.any(fp != fe):
+        raise ValueError("the power and field files need the same frequencies")
+    scale = 1.0 / Z0 if field.lower() == "e" else Z0
+    lines = header(1, len(fp))
+    for f, pw, mag in zip(fp, power_rows[:, 2], field_rows[:, 4]):
+        e_rms = mag / math.sqrt(2.0)
+        si = 3.0 * (e_rms ** 2) * scale / 2.0
+        tcs = float(np.float32(abs(pw) / si))  # CMPLX(TCS): default (single) precision
+        db = 10.0 * math.log10(abs(tcs)) if tcs != 0.0 else -math.inf
+        lines.append(fortran_e(f) + f"{1:5d}" +
+                     "".join(fortran_e(x) for x in (tcs, 0.0, abs(tcs), math.atan2(0.0, tcs), db)))
+    return lines
 
 
 def main(argv=None) -> int:

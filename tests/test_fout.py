@@ -211,3 +211,19 @@ def test_gpu_power_calcs_matches_reference_golden(gpu_lib):
         g.run(t["n_timesteps"])
         face, acc = g.face_output(), g.power_surfaces()
     check_power_calc(t, face, acc)
+
+
+def test_transmission_cross_section_reproduces_the_reference_file():
+    """POWER_CALCS's TCS.fout_ref (post-processor option 15), byte for byte:
+    the transmitted power from the case's golden power surface file over the
+    spectrum of its golden field series (option 3, 1 .. 600 MHz, 100
+    frequencies, as its post-processing input asks)."""
+    from ggi_tlm_b200 import fout
+
+    d = np.load(os.path.join(HERE, "golden", "fout_text.npz"))
+    g = np.load(os.path.join(HERE, "golden", "power_calc_Ex.npz"))
+    freqs = fout.frequencies(1e6, 600e6, 100, "lin")
+    sel = g["point"] == 1
+    field = fout.read_fout(fout.format_fout(freqs, fout.fourier_transform(g["time"][sel], g["value"][sel], freqs)))
+    power = fout.read_fout([str(x) for x in d["power_calc"]])
+    assert fout.transmission_cross_section_lines(power, field, "e") == [str(x) for x in d["power_calc_tcs"]]
