@@ -138,12 +138,14 @@ def power_surface_lines(freqs: Sequence[float], surface: Sequence[int], power: S
     return lines
 
 
-def oneport_calc(e1: complex, e2: complex, h1: complex, h2: complex, d: float) -> Tuple[complex, complex, complex]:
+def oneport_calc(e1: complex, e2: complex, h1: complex, h2: complex,
+                 d: float) -> Tuple[complex, complex, complex, complex]:
     """oneport_calc (POST_PROCESSOR/oneport.F90:206-249): from E and H at
     two output planes 2d apart in a uniform section, the propagation
-    constant beta (real part made non-negative) and the right- and
-    left-going waves Er, El at the first plane: the root P = exp(j beta d)
-    of a P^2 + b P + c = 0 with a = c = E2 H1 + E1 H2, b = -2 (E1 H1 + E2 H2)."""
+    constant beta (real part made non-negative), the right- and left-going
+    waves Er, El at the first plane and the wave impedance Z (real part made
+    non-negative): the root P = exp(j beta d) of a P^2 + b P + c = 0 with
+    a = c = E2 H1 + E1 H2, b = -2 (E1 H1 + E2 H2).  Returns (beta, Er, El, Z)."""
     a = e2 * h1 + e1 * h2
     b = -2.0 * (e1 * h1 + e2 * h2)
     c = e2 * h1 + e1 * h2
@@ -154,8 +156,37 @@ def oneport_calc(e1: complex, e2: complex, h1: complex, h2: complex, d: float) -
         beta = -beta
     p = cmath.exp(1j * beta * d)
     eit = (e2 * p - e1 * p * p * p) / (1.0 - p * p * p * p)
+    z = (2.0 * eit * p - e1) / h1
     ert = -eit * p * p + e1 * p
-    return beta, eit, ert
+    if z.real < 0.0:
+        z = -z
+    return beta, eit, ert, z
+
+
+def oneport_lines(freqs: Sequence[float], ft: Sequence[Sequence[complex]], d_port: float,
+                  l: float) -> Tuple[List[str], List[str]]:
+    """Post-processor option 9, one-port analysis (POST_PROCESSOR/oneport.F90:35-205):
+    ``ft`` holds E1, E2, H1, H2, the spectra on two planes ``d_port`` apart
+    whose midpoint is ``l`` from the interface.  Returns the lines of the
+    output file (per frequency, 11E14.5: f, beta, Z, the reflection
+    coefficient R = (El/Er) exp(2 j beta l) with |R| and its dB, Re(w/beta),
+    1 - |R|^2) and of its ``.Zs`` companion (f, the surface impedance
+    Z (1+R)/(1-R) and its magnitude)."""
+    E1, E2, H1, H2 = (np.asarray(x, dtype=np.complex128) for x in ft)
+    d = d_port / 2.0
+    out = ["    frequency       Re{Beta}     Im{Beta}       Re{Z}          Im{Z}"
+           "         Re{R}          Im{R}        |R|          |R|(dB)      Re{w/Beta}    1-|R|**2"]
+    zs_out = ["    frequency        Re{Zs}       Im{Zs}"]
+    for k, f in enumerate(freqs):
+        w = 2.0 * math.pi * f
+        beta, ei, er, z = oneport_calc(E1[k], E2[k], H1[k], H2[k], d)
+        r = (er / ei) * cmath.exp(2.0 * 1j * beta * l)
+        zs = z * (1.0 + r) / (1.0 - r)
+        vals = (f, beta.real, beta.imag, z.real, z.imag, r.real, r.imag, abs(r), 20.0 * math.log10(abs(r)),
+                (w / beta).real, 1.0 - abs(r) ** 2)
+        out.append("".join(fortran_e(v, 14, 5) for v in vals))
+        zs_out.append("".join(fortran_e(v, 14, 5) for v in (f, zs.real, zs.imag, abs(zs))))
+    return out, zs_out
 
 
 def twoport_lines(freqs: Sequence[float], ft: Sequence[Sequence[complex]], d_port1: float, l1: float,
@@ -179,8 +210,8 @@ def twoport_lines(freqs: Sequence[float], ft: Sequence[Sequence[complex]], d_por
     d1, d2 = d_port1 / 2.0, d_port2 / 2.0
     out = [title]
     for k, f in enumerate(freqs):
-        beta1, er1, el1 = oneport_calc(E11[k], E12[k], H11[k], H12[k], d1)
-        beta2, er2, el2 = oneport_calc(E22[k], E21[k], H22[k], H21[k], d2)
+        beta1, er1, el1, _ = oneport_calc(E11[k], E12[k], H11[k], H12[k], d1)
+        beta2, er2, el2, _ = oneport_calc(E22[k], E21[k], H22[k], H21[k], d2)
         if excitation_port == 1:
             sa = el1 * cmath.exp(1j * beta1 * l1) / (er1 * cmath.exp(-1j * beta1 * l1))  # S11
             sb = er2 * cmath.exp(1j * beta2 * l2) / (er1 * cmath.exp(-1j * beta1 * l1))  # S21

@@ -107,6 +107,8 @@ FOUT_CASES = {
     "box_slot": "SHIELDING_EFFECTIVENESS_BOX_SLOT/PROBLEM_SPECIFICATION_FILES/Shielding_effectiveness.fout_ref",
     # written by the solver itself (write_frequency_domain_power_surfaces)
     "power_calc": "POWER_CALCS/PROBLEM_SPECIFICATION_FILES/power_calc.frequency_domain_power_surface.fout_ref",
+    # four volume averages Fourier transformed (option 3), then the one-port analysis (option 9)
+    "resonant_absorber": "RESONANT_ABSORBER/PROBLEM_SPECIFICATION_FILES/Resonant_absorber.fout_ref",
     # option 15, transmission cross section, from the power surface file and the field spectrum
     "power_calc_tcs": "POWER_CALCS/PROBLEM_SPECIFICATION_FILES/TCS.fout_ref",
     # eight volume averages Fourier transformed (option 3), then the two-port analysis (option 10)

@@ -227,3 +227,27 @@ def test_transmission_cross_section_reproduces_the_reference_file():
     field = fout.read_fout(fout.format_fout(freqs, fout.fourier_transform(g["time"][sel], g["value"][sel], freqs)))
     power = fout.read_fout([str(x) for x in d["power_calc"]])
     assert fout.transmission_cross_section_lines(power, field, "e") == [str(x) for x in d["power_calc_tcs"]]
+
+
+def test_oneport_analysis_recovers_a_known_wave():
+    """Post-processor option 9 on the fields of one known wave in a uniform
+    section: E = a exp(-j beta x) + b exp(j beta x), H = (a exp(-j beta x) -
+    b exp(j beta x)) / Z on planes at x = -d, +d; the analysis returns beta,
+    Z and R = (b / a) exp(2 j beta l), the reflection at x = l."""
+    from ggi_tlm_b200 import fout
+
+    freqs = np.array([1e9, 5e9, 2e10])
+    d_port, l, z = 0.2e-3, 2.5e-3, 300.0 + 20.0j
+    beta = 2 * np.pi * freqs / 2.9e8 * (1.0 - 0.01j) * 1.3
+    a, b = 1.0 + 0.0j, 0.4 * np.exp(0.3j)
+    P = np.exp(1j * beta * d_port / 2)
+    ft = [a * P + b / P, a / P + b * P, (a * P - b / P) / z, (a / P - b * P) / z]
+    lines, zs_lines = fout.oneport_lines(freqs, ft, d_port, l)
+    assert lines[0].split()[:3] == ["frequency", "Re{Beta}", "Im{Beta}"] and len(lines) == 4 and len(zs_lines) == 4
+    rows = np.loadtxt(lines[1:])
+    r = b / a * np.exp(2j * beta * l)
+    want = np.column_stack([freqs, beta.real, beta.imag, np.full(3, z.real), np.full(3, z.imag), r.real, r.imag,
+                            np.abs(r), 20 * np.log10(np.abs(r)), (2 * np.pi * freqs / beta).real, 1 - np.abs(r) ** 2])
+    np.testing.assert_allclose(rows, want, rtol=1e-4, atol=1e-9)
+    zs = np.loadtxt(zs_lines[1:])
+    np.testing.assert_allclose(zs[:, 1] + 1j * zs[:, 2], z * (1 + r) / (1 - r), rtol=1e-4)
