@@ -258,6 +258,8 @@ class DistShard:
         self.slab = make(self.tab, device)
         nb = self.slab.halo_bytes()
         dev = torch.device(f"cuda:{device}") if dist.get_backend(group) == "nccl" else torch.device("cpu")
+        if dev.type == "cuda":  # NCCL point-to-point needs the rank's device current
+            torch.cuda.set_device(dev)
         self.bufs = {k: torch.empty(nb, dtype=torch.uint8, device=dev) for k in ("send_up", "send_dn", "recv_up",
                                                                                   "recv_dn")}
         self.on_gpu = dev.type == "cuda"
