@@ -140,6 +140,8 @@ int main(int argc, char **argv) {
   if (t.has("n_dft"))
     CALL(tlm_gpu_set_dft(h, t.n("n_dft"), t.dp("dft_freq"), t.ip("dft_comp"), t.ip("dft_face_ptr"),
                          t.ip("dft_face_out"), t.ip("dft_face_side")));
+  if (t.has("n_dft"))  // the surfaces' output steps (every step unless the input gives a timing block)
+    CALL(tlm_gpu_set_dft_gate(h, t.n("n_dft"), t.ip("dft_first"), t.ip("dft_last"), t.ip("dft_interval")));
   // the time loop, in chunks: after each chunk the output points are read
   // back (where the Fortran shim writes its .tout lines)
   const int n_steps = desc.n_timesteps, chunk = 100;

@@ -7,6 +7,7 @@ CPU: the driver compiles and links against the library, and without a GPU
 it stops with the library's error message and exit code 1, as the Fortran
 shim does.  GPU: its results equal the Python binding's bit for bit, and in
 FP64 the oracle's to 1e-10."""
+import dataclasses
 import os
 import subprocess
 import sys
@@ -25,7 +26,7 @@ INTS = ["cell_code", "sp_material", "sp_pml", "sp_excitation", "sp_output", "mat
         "mat_mu_exists", "mat_eps_order", "mat_mu_order", "pml_cell_param", "pt_cell", "pt_comp", "pt_fn", "pt_type",
         "face_cx", "face_cy", "face_cz", "face_dir", "face_exc", "face_out", "hs_face_exc", "hs_norm", "fpt_face",
         "fpt_comp", "fpt_fn", "fpt_type", "fprobe_face", "fprobe_side", "fprobe_comp", "dft_comp", "dft_face_ptr",
-        "dft_face_out", "dft_face_side"]
+        "dft_face_out", "dft_face_side", "dft_first", "dft_last", "dft_interval"]
 DOUBLES = ["R", "mat_Ys_eps_f", "mat_Zs_mu_f", "mat_Ge", "mat_Rm", "mat_eps_a", "mat_eps_b", "mat_mu_a", "mat_mu_b",
            "pml_params", "fn_value", "fn_value_face", "hs_offset", "hs_Ei", "hs_Hi", "dft_freq"]
 SCALARS = ["nx", "ny", "nz", "n_timesteps", "dl", "dt", "n_special", "n_materials", "n_pml_params", "n_pml_cells",
@@ -62,6 +63,7 @@ def compile_driver(tmp):
 
 def specs():
     a = cases.pml_spheres(n=24, pml=4, n_spheres=3, steps=230, n_probes=4, n_freq=3, dft_size=6, rmin=2.0, rmax=3.5)
+    a.dft_surfaces = [dataclasses.replace(d, first_step=20, last_step=200, interval=3) for d in a.dft_surfaces]
     b = cases.pml_point_source(18, pml=3, steps=150, n_probes=2)
     b.point_excitations.append(PointExcitation((9, 9, 6), "Ex", 1, face="zmin"))
     b.outputs.append(OutputPoint((9, 10, 11), "Hy", face="xmax"))
