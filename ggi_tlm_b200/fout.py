@@ -86,8 +86,13 @@ def read_fout(path_or_lines) -> np.ndarray:
 
 def spectrum(rows: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
     """(frequencies, complex values) of .fout rows [n, 7] (read_fout), as
-    read_frequency_domain_data takes them: from the printed Re and Im columns."""
-    return rows[:, 0], rows[:, 2] + 1j * rows[:, 3]
+    read_frequency_domain_data takes them
+    (POST_PROCESSOR/read_write_frequency_domain_data.F90:155-260): from the
+    printed Re and Im columns through CMPLX() without a kind, i.e. rounded
+    to single precision."""
+    re = rows[:, 2].astype(np.float32).astype(np.float64)
+    im = rows[:, 3].astype(np.float32).astype(np.float64)
+    return rows[:, 0], re + 1j * im
 
 
 def combine(f1: np.ndarray, f2: np.ndarray, a: float = 1.0, b: float = 1.0, c: float = 0.0) -> np.ndarray:

@@ -11,10 +11,11 @@ S21.fout_4_ref:
 * option 10, the two-port analysis (twoport.F90, oneport.F90:206-249).
 
 The S-parameters come from a nearly degenerate quadratic in each port's
-two planes (0.5 mm apart against wavelengths down to 10 cm), so the 7-digit
-files round their inputs hard: the oracle's S21 matches the golden file to
-1e-4 relative and a third of its lines byte for byte.  GPU: the library's
-volume averages against the oracle's."""
+two planes (0.5 mm apart against wavelengths down to 10 cm), which amplifies
+every rounding on the way; with the reference's own roundings (7-digit
+files, spectra read back in single precision) the oracle's S21 file equals
+the golden one byte for byte.  GPU: the library's volume averages against
+the oracle's."""
 import os
 import sys
 
@@ -73,17 +74,13 @@ def test_reader_takes_the_fss_input():
 
 
 def test_oracle_s21_matches_the_reference_file():
+    """Byte for byte: the oracle's time series, printed to 7 digits, Fourier
+    transformed, printed again and read back in single precision (as the
+    reference's read_frequency_domain_data does), give the golden S21 file."""
     p, t = problem()
     got = s21_lines(p, t, oracle_averages(t))
     gold = [str(x) for x in np.load(os.path.join(HERE, "golden", "fout_text.npz"))["fss_s21"]]
-    assert len(got) == len(gold) and got[0] == gold[0]
-    g, m = np.loadtxt(gold[1:]), np.loadtxt(got[1:])
-    np.testing.assert_array_equal(m[:, 0], g[:, 0])
-    s21g, s21m = g[:, 5] + 1j * g[:, 6], m[:, 5] + 1j * m[:, 6]
-    assert np.max(np.abs(s21m - s21g) / np.abs(s21g)) < 2e-4
-    s11g, s11m = g[:, 1] + 1j * g[:, 2], m[:, 1] + 1j * m[:, 2]
-    assert np.max(np.abs(s11m - s11g)) < 2e-4
-    assert sum(a == b for a, b in zip(got, gold)) > 300
+    assert got == gold
 
 
 @pytest.mark.gpu

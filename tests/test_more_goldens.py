@@ -108,11 +108,12 @@ def test_gpu_resonant_absorber_reflection_matches_the_reference_file(gpu_lib):
     """RESONANT_ABSORBER end to end: all 59958 steps on the GPU (FP64), the
     four volume averages as the run writes them (E16.7), post-processor
     option 3 on each (100 MHz .. 25 GHz, 1000 frequencies, written and read
-    back as .fout) and option 9, the one-port analysis of the two planes
-    0.2 mm apart, 2.5 mm from the absorber: Resonant_absorber.fout_ref.  The
-    analysis solves a quadratic whose roots nearly coincide at these plane
-    spacings, so it is compared to the golden file's 5 digits only where
-    that conditioning allows: |R| to 1e-4, R to 5e-3, beta and Z to 1 %."""
+    back as .fout, read in single precision as the reference does) and
+    option 9, the one-port analysis of the two planes 0.2 mm apart, 2.5 mm
+    from the absorber: Resonant_absorber.fout_ref.  The oracle's series give
+    that file byte for byte; the analysis solves a nearly degenerate
+    quadratic, so the GPU's lines are held to 95 % identical and the rest to
+    |R| 1e-4, R 1e-3, beta and Z 0.1 %."""
     from ggi_tlm_b200 import capi, fout, tout
     from ggi_tlm_b200 import run as runner
 
@@ -136,9 +137,12 @@ def test_gpu_resonant_absorber_reflection_matches_the_reference_file(gpu_lib):
     lines, _ = fout.oneport_lines(fr, [spec[3], spec[1], spec[4], spec[2]], 0.2e-3, 2.5e-3)
     gold = [str(x) for x in np.load(os.path.join(HERE, "golden", "fout_text.npz"))["resonant_absorber"]]
     assert lines[0] == gold[0] and len(lines) == len(gold)
+    # the oracle's series give the file byte for byte; the GPU's differ from them by ~1e-13, which can
+    # move a rare 7th printed digit, and the analysis amplifies that
+    assert sum(x == y for x, y in zip(lines, gold)) >= 0.95 * len(gold)
     a, b = np.loadtxt(lines[1:]), np.loadtxt(gold[1:])
     np.testing.assert_array_equal(a[:, 0], b[:, 0])
     np.testing.assert_allclose(a[:, 7], b[:, 7], rtol=1e-4)
-    assert np.max(np.abs((a[:, 5] + 1j * a[:, 6]) - (b[:, 5] + 1j * b[:, 6]))) < 5e-3
-    np.testing.assert_allclose(a[:, 1], b[:, 1], rtol=1e-2)
-    np.testing.assert_allclose(a[:, 3], b[:, 3], rtol=1e-2)
+    assert np.max(np.abs((a[:, 5] + 1j * a[:, 6]) - (b[:, 5] + 1j * b[:, 6]))) < 1e-3
+    np.testing.assert_allclose(a[:, 1], b[:, 1], rtol=1e-3)
+    np.testing.assert_allclose(a[:, 3], b[:, 3], rtol=1e-3)
