@@ -244,7 +244,8 @@ def transmission_cross_section_lines(power_rows: np.ndarray, field_rows: np.ndar
         raise ValueError("the power and field files need the same frequencies")
     scale = 1.0 / Z0 if field.lower() == "e" else Z0
     lines = header(1, len(fp))
-    for f, pw, mag in zip(fp, power_rows[:, 2], field_rows[:, 4]):
+    # the power value is read through CMPLX() (single precision), the magnitude as printed
+    for f, pw, mag in zip(fp, power_rows[:, 2].astype(np.float32).astype(np.float64), field_rows[:, 4]):
         e_rms = mag / math.sqrt(2.0)
         si = 3.0 * (e_rms ** 2) * scale / 2.0
         tcs = float(np.float32(abs(pw) / si))  # CMPLX(TCS): default (single) precision

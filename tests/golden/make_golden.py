@@ -91,6 +91,13 @@ RESULT_HEADS = {
 MESH_CASES = {
     "helix": "HELIX_ANTENNA/helix.mesh",
 }
+# the post-processor's input files of the cases whose post-processed results are golden, as text
+POST_CASES = {
+    "power_calc": "POWER_CALCS/PROBLEM_SPECIFICATION_FILES/GGI_TLM_post_process_in.txt",
+    "fss": "PARAMETERISED_FSS/PROBLEM_SPECIFICATION_FILES/GGI_TLM_post_process_in.txt",
+    "resonant_absorber": "RESONANT_ABSORBER/PROBLEM_SPECIFICATION_FILES/GGI_TLM_post_process_in.txt",
+    "box_slot": "SHIELDING_EFFECTIVENESS_BOX_SLOT/PROBLEM_SPECIFICATION_FILES/GGI_TLM_post_process_in.txt",
+}
 # data files the inputs name (excitation function samples), as text
 DATA_CASES = {
     "gaussian_from_file.dat": "EXCITATION_FUNCTION_TEST/PROBLEM_SPECIFICATION_FILES/gaussian_from_file.dat",
@@ -152,6 +159,12 @@ def main():
             inp[name] = np.array(f.read().splitlines())
     np.savez_compressed(os.path.join(here, "inp_text.npz"), **inp)
     print("inp_text", {k: len(v) for k, v in inp.items()})
+    pp = {}
+    for name, rel in POST_CASES.items():
+        with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", rel), encoding="latin-1") as f:
+            pp[name] = np.array(f.read().splitlines())
+    np.savez_compressed(os.path.join(here, "post_process_text.npz"), **pp)
+    print("post_process_text", {k: len(v) for k, v in pp.items()})
     data = {}
     for name, rel in DATA_CASES.items():
         with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", rel), encoding="latin-1") as f:
