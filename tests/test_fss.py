@@ -94,3 +94,33 @@ def test_gpu_fss_volume_averages_match_the_oracle(gpu_lib):
         got = np.array(g.output_volumes())
     assert got.shape == want.shape
     assert np.linalg.norm(got - want) <= 1e-10 * np.linalg.norm(want)
+
+
+@pytest.mark.gpu
+def test_gpu_fss_case_through_the_runner_and_the_post_processor(gpu_lib, tmp_path):
+    """The reference's workflow on the library: ``python -m
+    ggi_tlm_b200.run single_cell`` in a directory holding the case's input,
+    then ``python -m ggi_tlm_b200.post_process`` on its own post-processing
+    input.  The GPU's FP64 series differ from the oracle's by ~1e-13, which
+    can move a rare 7th printed digit that the two-port analysis amplifies,
+    so the S21 file is held to 90 % of its lines exact and S21 within 1e-4."""
+    import subprocess
+
+    d = str(tmp_path)
+    with open(os.path.join(d, "single_cell.inp"), "w", encoding="latin-1") as f:
+        f.write("\n".join(T.inputs()["fss_single_cell"]) + "\n")
+    post = [str(x) for x in np.load(os.path.join(HERE, "golden", "post_process_text.npz"))["fss"]]
+    with open(os.path.join(d, "GGI_TLM_post_process_in.txt"), "w") as f:
+        f.write("\n".join(post) + "\n")
+    env = dict(os.environ, PYTHONPATH=os.path.dirname(HERE))
+    for cmd in (["-m", "ggi_tlm_b200.run", "single_cell"],
+                ["-m", "ggi_tlm_b200.post_process", "GGI_TLM_post_process_in.txt"]):
+        res = subprocess.run([sys.executable, *cmd], cwd=d, env=env, capture_output=True, text=True, timeout=900)
+        assert res.returncode == 0, res.stderr[-2000:]
+    got = open(os.path.join(d, "S21.fout_4")).read().splitlines()
+    gold = [str(x) for x in np.load(os.path.join(HERE, "golden", "fout_text.npz"))["fss_s21"]]
+    assert got[0] == gold[0] and len(got) == len(gold)
+    assert sum(a == b for a, b in zip(got, gold)) >= 0.9 * len(gold)
+    a, b = np.loadtxt(got[1:]), np.loadtxt(gold[1:])
+    s21a, s21b = a[:, 5] + 1j * a[:, 6], b[:, 5] + 1j * b[:, 6]
+    assert np.max(np.abs(s21a - s21b) / np.abs(s21b)) < 1e-4
