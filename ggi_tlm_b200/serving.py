@@ -225,14 +225,19 @@ class GpuEngine:
 
     def advance(self, n_steps: int):
         self.wait()
+        # a precision whose membership changed keeps its batch (stream, graph
+        # resources, device buffers) and gets its new meshes; one left empty
+        # is closed
         for prec in list(self.dirty):
-            b = self.batches.pop(prec, None)
-            if b is not None:
-                b.close()
-        if self.dirty:
-            for g in self.retired:
-                g.close()
-            self.retired.clear()
+            members = [g for g in self.meshes.values() if g.precision == prec]
+            b = self.batches.get(prec)
+            if b is not None and members:
+                b.set_members(members)
+            elif b is not None:
+                self.batches.pop(prec).close()
+        for g in self.retired:
+            g.close()
+        self.retired.clear()
         self.dirty.clear()
         if not self.meshes:
             return

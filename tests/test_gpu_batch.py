@@ -56,3 +56,35 @@ def test_batch_rejects_mixed_precision(gpu_lib):
         capi.GpuBatch([a, b])
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("precision", [capi.TLM_PRECISION_FP32, capi.TLM_PRECISION_FP64])
+def test_batch_members_change_between_runs(gpu_lib, precision):
+    """Meshes leave and join a running batch (tlm_gpu_batch_set_members):
+    every mesh still gives its solo results bit for bit, a leaver can run on
+    its own, and the batch keeps working across the changes."""
+    tabs = uneven_tables(n=5, seed=4)
+    solo = []
+    for t in tabs:
+        with capi.GpuMesh(t, precision=precision) as g:
+            g.set_variant(1)
+            g.run(t["n_timesteps"])
+            solo.append(g.cell_output())
+    m = [capi.GpuMesh(t, precision=precision) for t in tabs]
+    for g in m:
+        g.set_variant(1)
+    with capi.GpuBatch(m[:3]) as b:
+        b.set_variant(1)
+        b.run(11)
+        b.set_members([m[1], m[2], m[3]])  # m0 leaves, m3 joins
+        m[0].run(5)  # the leaver runs alone
+        b.run(13)
+        b.set_members([m[0], m[2], m[3], m[4]])  # m0 back, m1 leaves, m4 joins
+        b.run(1000)
+        m[1].run(tabs[1]["n_timesteps"] - m[1].step)
+        b.synchronize()
+    for g, t, co in zip(m, tabs, solo):
+        assert g.step == t["n_timesteps"]
+        assert np.array_equal(g.cell_output(), co)
+    for g in m:
+        g.close()
