@@ -38,6 +38,7 @@ EXPORTS = [
     "tlm_gpu_num_variants", "tlm_gpu_fetch_links_noalloc", "tlm_gpu_batch_create", "tlm_gpu_batch_set_variant",
     "tlm_gpu_batch_run", "tlm_gpu_batch_synchronize", "tlm_gpu_batch_last_run", "tlm_gpu_batch_destroy",
     "tlm_gpu_set_small_to_zero", "tlm_gpu_set_pml_sigma", "tlm_gpu_set_face_excitation",
+    "tlm_gpu_set_face_excitation_side", "tlm_gpu_set_face_excitation_scale",
     "tlm_gpu_set_face_outputs", "tlm_gpu_fetch_face_output", "tlm_gpu_set_outer_huygens",
     "tlm_gpu_set_far_field", "tlm_gpu_fetch_far_field", "tlm_gpu_pool_release", "tlm_gpu_pool_cached_bytes",
     "tlm_gpu_prepare", "tlm_gpu_set_output_series", "tlm_gpu_set_volume_dft", "tlm_gpu_fetch_volume_dft",
@@ -47,7 +48,7 @@ EXPORTS = [
     "tlm_gpu_set_mode_outputs", "tlm_gpu_fetch_mode_outputs", "tlm_gpu_set_face_materials",
     "tlm_gpu_set_thin_layers", "tlm_gpu_set_face_thin_layers", "tlm_gpu_set_wrap",
     "tlm_gpu_halo_bytes", "tlm_gpu_halo_get", "tlm_gpu_halo_put", "tlm_gpu_set_test_wait_pad",
-    "tlm_gpu_set_dft_gate",
+    "tlm_gpu_set_dft_gate", "tlm_gpu_batch_set_members",
 ]
 
 
@@ -98,6 +99,8 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_set_pml": [i64, i32, _f64p, i32, _i32p],
         "tlm_gpu_set_pml_sigma": [i64, i32, _f64p],
         "tlm_gpu_set_face_excitation": [i64, i32, _i32p, _i32p, _i32p, _i32p],
+        "tlm_gpu_set_face_excitation_side": [i64, i32, _i32p],
+        "tlm_gpu_set_face_excitation_scale": [i64, i32, _f64p],
         "tlm_gpu_set_face_outputs": [i64, i32, _i32p, _i32p, _i32p],
         "tlm_gpu_set_outer_huygens": [i64, i32, _i32p, _f64p, _f64p, _f64p, C.c_double, C.c_double, i32],
         "tlm_gpu_set_far_field": [i64, i32, _f64p, _i32p, _i32p, _i32p],
@@ -153,6 +156,7 @@ def load_library(path: Optional[str] = None):
         "tlm_gpu_last_error": [C.c_char_p, i32],
         "tlm_gpu_batch_create": [C.POINTER(i64), i32, C.POINTER(i64)],
         "tlm_gpu_batch_set_variant": [i64, i32],
+        "tlm_gpu_batch_set_members": [i64, C.POINTER(i64), i32],
         "tlm_gpu_batch_run": [i64, i32],
         "tlm_gpu_batch_synchronize": [i64],
         "tlm_gpu_batch_last_run": [i64, C.POINTER(C.c_float), C.POINTER(i64), C.POINTER(i64)],
@@ -320,6 +324,12 @@ class GpuMesh:
         if int(t.get("n_face_points", 0)):
             fp = [_i32(t[k]) for k in ("fpt_face", "fpt_comp", "fpt_fn", "fpt_type")]
             _check(lib.tlm_gpu_set_face_excitation(self.h, int(t["n_face_points"]), *[_p(x) for x in fp]))
+            if "fpt_side" in t and np.any(np.asarray(t["fpt_side"]) != 0):
+                sd = _i32(t["fpt_side"])
+                _check(lib.tlm_gpu_set_face_excitation_side(self.h, int(t["n_face_points"]), _p(sd)))
+            if "fpt_scale" in t and np.any(np.asarray(t["fpt_scale"]) != 1.0):
+                sc = _f64(t["fpt_scale"])
+                _check(lib.tlm_gpu_set_face_excitation_scale(self.h, int(t["n_face_points"]), _p(sc)))
         if int(t.get("n_face_probes", 0)):
             fq = [_i32(t[k]) for k in ("fprobe_face", "fprobe_side", "fprobe_comp")]
             _check(lib.tlm_gpu_set_face_outputs(self.h, int(t["n_face_probes"]), *[_p(x) for x in fq]))
@@ -530,6 +540,14 @@ class GpuBatch:
 
     def set_variant(self, v: int):
         _check(_lib.tlm_gpu_batch_set_variant(self.h, v))
+
+    def set_members(self, meshes):
+        """Replace the batch's meshes (waits for its queued steps; the
+        leavers can then be used alone or closed)."""
+        meshes = list(meshes)
+        arr = (C.c_int64 * len(meshes))(*[m.h for m in meshes])
+        _check(_lib.tlm_gpu_batch_set_members(self.h, arr, len(meshes)))
+        self.meshes = meshes
 
     def run(self, n_steps: int, sync: bool = True):
         _check(_lib.tlm_gpu_batch_run(self.h, n_steps))

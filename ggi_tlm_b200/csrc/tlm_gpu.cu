@@ -253,6 +253,8 @@ struct Mesh {
   std::vector<tlm::ThinLayerDev> thin;  // thin-layer materials
   // point sources on faces (excitation face number, component 1..12, function, type)
   std::vector<int32_t> fpt_face, fpt_comp, fpt_fn, fpt_type;
+  std::vector<int32_t> fpt_side;  // per face source: 0 both sides, 1 or 2 that side alone; empty: all 0
+  std::vector<double> fpt_scale;  // per face source: factor on the function's value; empty: all 1
   // output points on faces (output face number, side 1/2, component 1..6)
   std::vector<int32_t> fpr_face, fpr_side, fpr_comp;
   int n_exc_faces = 0, n_out_faces = 0;
@@ -990,9 +992,14 @@ int finalize(Mesh *m) {
       src[exc_to_face[e]].x = 1;
     }
     // face point sources: one row of summed fields per excitation face that
-    // has any, tabulated for every step from the functions' value_face
+    // has any, side 1 then side 2, tabulated for every step from the
+    // functions' value_face
     std::vector<int> row_of(m->n_exc_faces + 1, -1);
     const int npt = (int)m->fpt_face.size();
+    if (!m->fpt_side.empty() && (int)m->fpt_side.size() != npt)
+      return fail(TLM_E_BADARG, "face source sides: %d given for %d face sources", (int)m->fpt_side.size(), npt);
+    if (!m->fpt_scale.empty() && (int)m->fpt_scale.size() != npt)
+      return fail(TLM_E_BADARG, "face source scales: %d given for %d face sources", (int)m->fpt_scale.size(), npt);
     m->n_pt_rows = 0;
     for (int e = 0; e < npt; e++) {
       const int fe = m->fpt_face[e], comp = m->fpt_comp[e], fn = m->fpt_fn[e], ty = m->fpt_type[e];
@@ -1000,6 +1007,8 @@ int finalize(Mesh *m) {
       if (comp < 1 || comp > 12) return fail(TLM_E_BADARG, "face point source %d: component %d out of range", e + 1, comp);
       if (fn < 1 || fn > m->n_fn) return fail(TLM_E_BADARG, "face point source %d: function out of range", e + 1);
       if (ty != 0 && ty != 1) return fail(TLM_E_BADARG, "face point source %d: source type must be 0 (hard) or 1 (soft)", e + 1);
+      if (!m->fpt_side.empty() && (m->fpt_side[e] < 0 || m->fpt_side[e] > 2))
+        return fail(TLM_E_BADARG, "face point source %d: side must be 0 (both), 1 or 2", e + 1);
       if (row_of[fe] < 0) row_of[fe] = m->n_pt_rows++;
       covered[fe]++;
     }
@@ -1009,15 +1018,23 @@ int finalize(Mesh *m) {
     }
     {
       const int R = std::max(m->n_pt_rows, 1);
-      std::vector<double> ptf((size_t)nsteps * R * 12, 0.0);
+      std::vector<double> ptf((size_t)nsteps * R * 24, 0.0);
       std::vector<int8_t> ptt((size_t)R * 6, 1);  // set_update_codes.F90:593, soft
       for (int e = 0; e < npt; e++) {
         const int r = row_of[m->fpt_face[e]], c = m->fpt_comp[e] - 1, fn = m->fpt_fn[e] - 1;
-        for (int t = 0; t < nsteps && t < m->n_fn_steps; t++) {
-          double &v = ptf[((size_t)t * R + r) * 12 + c];
-          v = v + m->fn_value_face[(size_t)fn * m->n_fn_steps + t];
+        const int only = m->fpt_side.empty() ? 0 : m->fpt_side[e];
+        const bool scaled = !m->fpt_scale.empty();
+        const double sc = scaled ? m->fpt_scale[e] : 1.0;
+        for (int sd = 0; sd < 2; sd++) {
+          if (only && sd != only - 1) continue;
+          for (int t = 0; t < nsteps && t < m->n_fn_steps; t++) {
+            const double fv = m->fn_value_face[(size_t)fn * m->n_fn_steps + t];
+            double &v = ptf[((size_t)t * R + r) * 24 + sd * 12 + c];
+            v = v + (scaled ? sc * fv : fv);  // Mode_excitation: face_excitation_field + mode_field*value
+          }
         }
-        if (c < 6) ptt[(size_t)r * 6 + c] = (int8_t)m->fpt_type[e];
+        // connect reads side 1's source types on both sides
+        if (c < 6 && only != 2) ptt[(size_t)r * 6 + c] = (int8_t)m->fpt_type[e];
       }
       if ((rc = upload(m, m->fpt_field_d, ptf)) || (rc = upload(m, m->fpt_type_d, ptt)) || (rc = upload(m, m->face_src, src)))
         return rc;
@@ -1848,6 +1865,26 @@ int tlm_gpu_set_face_excitation(int64_t h, int32_t n, const int32_t *face_exc, c
   return TLM_OK;
 }
 
+int tlm_gpu_set_face_excitation_side(int64_t h, int32_t n, const int32_t *side) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && !side)) return fail(TLM_E_BADARG, "bad face excitation side arguments");
+  m->fpt_side.assign(side, side + n);
+  return TLM_OK;
+}
+
+int tlm_gpu_set_face_excitation_scale(int64_t h, int32_t n, const double *scale) {
+  Mesh *m = get(h);
+  if (!m) return fail(TLM_E_BADARG, "bad handle");
+  if (m->finalized) return fail(TLM_E_STATE, "tables are fixed after the first run");
+  if (n < 0 || (n && !scale)) return fail(TLM_E_BADARG, "bad face excitation scale arguments");
+  for (int e = 0; e < n; e++)
+    if (!std::isfinite(scale[e])) return fail(TLM_E_BADARG, "face source %d: scale is not finite", e + 1);
+  m->fpt_scale.assign(scale, scale + n);
+  return TLM_OK;
+}
+
 int tlm_gpu_set_face_outputs(int64_t h, int32_t n, const int32_t *face_out, const int32_t *side, const int32_t *comp) {
   Mesh *m = get(h);
   if (!m) return fail(TLM_E_BADARG, "bad handle");
@@ -2606,13 +2643,23 @@ Batch *get_batch(int64_t h) {
   return it == g_batches.end() ? nullptr : it->second.get();
 }
 
+// Upload v into buf on the batch's stream.  A buffer that is large enough
+// is overwritten in place: the copy is ordered after the steps already
+// queued on that stream, which read the old lists, so a membership change
+// between segments needs no device-wide synchronisation (a fresh block
+// from the device cache may need one).  A buffer that is too small grows to
+// one and a half times what is needed.
 template <typename V>
 int bupload(Batch *b, DevBuf &buf, const std::vector<V> &v) {
-  if (buf.p) b->dev_bytes -= buf.bytes;
-  cudaError_t e = buf_alloc(buf, std::max<size_t>(v.size() * sizeof(V), 16));
-  if (e != cudaSuccess) return fail(TLM_E_OOM, "device allocation of %zu bytes failed: %s", buf.bytes, cudaGetErrorString(e));
-  b->dev_bytes += buf.bytes;
-  if (!v.empty()) CK(cudaMemcpy(buf.p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice));
+  const size_t need = std::max<size_t>(v.size() * sizeof(V), 16);
+  if (!buf.p || buf.cap < need) {
+    if (buf.p) b->dev_bytes -= buf.cap;
+    cudaError_t e = buf_alloc(buf, need + need / 2);
+    if (e != cudaSuccess) return fail(TLM_E_OOM, "device allocation of %zu bytes failed: %s", buf.bytes, cudaGetErrorString(e));
+    b->dev_bytes += buf.cap;
+  }
+  buf.bytes = need;
+  if (!v.empty()) CK(cudaMemcpyAsync(buf.p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice, b->stream));
   return TLM_OK;
 }
 
@@ -2967,6 +3014,38 @@ int tlm_gpu_batch_run(int64_t bh, int32_t n_steps) {
     left -= seg;
   }
   CK(cudaEventRecord(b->ev1, b->stream));
+  return TLM_OK;
+}
+
+int tlm_gpu_batch_set_members(int64_t bh, const int64_t *handles, int32_t n) {
+  Batch *b = get_batch(bh);
+  if (!b) return fail(TLM_E_BADARG, "bad batch handle");
+  if (!handles || n < 1) return fail(TLM_E_BADARG, "bad batch arguments");
+  for (int i = 0; i < n; i++) {
+    Mesh *m = get(handles[i]);
+    if (!m) return fail(TLM_E_BADARG, "bad handle at position %d", i);
+    const bool member = std::find(b->handles.begin(), b->handles.end(), handles[i]) != b->handles.end();
+    if (m->batch_stream && !member) return fail(TLM_E_STATE, "mesh %d belongs to another batch", i);
+    if (m->fp64 != b->fp64 || m->desc.device != b->device)
+      return fail(TLM_E_BADARG, "all meshes of a batch need the same precision and device");
+    for (int j = 0; j < i; j++)
+      if (handles[j] == handles[i]) return fail(TLM_E_BADARG, "mesh listed twice");
+  }
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  for (int i = 0; i < n; i++) {
+    Mesh *m = get(handles[i]);
+    int rc = finalize(m);
+    if (rc) return rc;
+    if (m->stream) CK(cudaStreamSynchronize(m->stream));
+  }
+  for (int64_t h : b->handles) {  // leavers run alone again
+    Mesh *m = get(h);
+    if (m && std::find(handles, handles + n, h) == handles + n) m->batch_stream = nullptr;
+  }
+  b->handles.assign(handles, handles + n);
+  for (int i = 0; i < n; i++) get(handles[i])->batch_stream = b->stream;
+  b->active.clear();  // the next run rebuilds the work lists and the graph
   return TLM_OK;
 }
 

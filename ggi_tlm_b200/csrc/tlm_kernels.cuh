@@ -1542,7 +1542,7 @@ struct FaceDev {
   int n_timesteps;
   double *face_field;      // [n_out_faces][2][6]
   const int2 *face_src;    // per special face: (Huygens patch 0/1, face point-source row or -1)
-  const double *pt_field;  // [n_timesteps][n_pt_rows][12] summed face point sources (E, H, J, M)
+  const double *pt_field;  // [n_timesteps][n_pt_rows][2 sides][12] summed face sources (E, H, J, M)
   const int8_t *pt_type;   // [n_pt_rows][6] hard (0) / soft (1) source factor of E, H
   int n_pt_rows;
   const int8_t *mat;       // per special face: surface material 0 none, 1 PEC, 2 PMC, 3 thin layer, 4 free space
@@ -1728,26 +1728,39 @@ __device__ __forceinline__ void face_body(const MeshDev<T> &m, const FaceDev &fd
     thin_layer_update(L, pol2, sm > 0, w + 4 * kMaxOrder, b2, a2, B_max, B_min);
   }  // 0 and 4 (a free-space surface material): the plain sum
   if (io.x >= 0) {
-    // face_excitation_field / face_excitation_type of this face: point
-    // sources first (excitation_points.F90:286-323, the same value on both
-    // sides), then the Huygens J, M (huygens_surface.F90:734-848)
+    // face_excitation_field / face_excitation_type of this face, side 1
+    // (min) and side 2 (max): point sources on both sides
+    // (excitation_points.F90:286-323), one-sided or two-sided excitation
+    // surfaces (excitation_surfaces.F90:218-275), then the Huygens J, M on
+    // both sides (huygens_surface.F90:734-848)
     const int2 src = fd.face_src[f];
-    double fld[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double fld[2][6], Js[2][3], Ms[2][3];
     double hsf[6] = {1.0, 1.0, 1.0, 1.0, 1.0, 1.0};
-    double Js[3] = {0.0, 0.0, 0.0}, Ms[3] = {0.0, 0.0, 0.0};
-    if (src.y >= 0) {
-      const double *pf = fd.pt_field + ((size_t)(t - 1) * fd.n_pt_rows + src.y) * 12;
-      const int8_t *ty = fd.pt_type + (size_t)src.y * 6;
 #pragma unroll
-      for (int k = 0; k < 6; k++) {
-        fld[k] = pf[k];
-        hsf[k] = double(ty[k]);
-      }
+    for (int sd = 0; sd < 2; sd++) {
+#pragma unroll
+      for (int k = 0; k < 6; k++) fld[sd][k] = 0.0;
 #pragma unroll
       for (int k = 0; k < 3; k++) {
-        Js[k] = pf[6 + k];
-        Ms[k] = pf[9 + k];
+        Js[sd][k] = 0.0;
+        Ms[sd][k] = 0.0;
       }
+    }
+    if (src.y >= 0) {
+      const double *pf = fd.pt_field + ((size_t)(t - 1) * fd.n_pt_rows + src.y) * 24;
+      const int8_t *ty = fd.pt_type + (size_t)src.y * 6;
+#pragma unroll
+      for (int sd = 0; sd < 2; sd++) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) fld[sd][k] = pf[sd * 12 + k];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          Js[sd][k] = pf[sd * 12 + 6 + k];
+          Ms[sd][k] = pf[sd * 12 + 9 + k];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 6; k++) hsf[k] = double(ty[k]);
     }
     if (src.x) {
       // get_interpolated_excitation_value (excitation.F90:645-690)
@@ -1763,30 +1776,40 @@ __device__ __forceinline__ void face_body(const MeshDev<T> &m, const FaceDev &fd
       const double value = v1 + delta_t * (v2 - v1) / dt;
       const double nx_ = h.y, ny_ = h.z, nz_ = h.w;
       const double *Hi = fd.Hi, *Ei = fd.Ei;
-      Js[0] = Js[0] + (ny_ * value * (Hi[2]) - nz_ * value * (Hi[1]));
-      Js[1] = Js[1] + (nz_ * value * (Hi[0]) - nx_ * value * (Hi[2]));
-      Js[2] = Js[2] + (nx_ * value * (Hi[1]) - ny_ * value * (Hi[0]));
-      Ms[0] = Ms[0] + -(ny_ * value * (Ei[2]) - nz_ * value * (Ei[1]));
-      Ms[1] = Ms[1] + -(nz_ * value * (Ei[0]) - nx_ * value * (Ei[2]));
-      Ms[2] = Ms[2] + -(nx_ * value * (Ei[1]) - ny_ * value * (Ei[0]));
+      const double j0 = (ny_ * value * (Hi[2]) - nz_ * value * (Hi[1]));
+      const double j1 = (nz_ * value * (Hi[0]) - nx_ * value * (Hi[2]));
+      const double j2 = (nx_ * value * (Hi[1]) - ny_ * value * (Hi[0]));
+      const double m0 = -(ny_ * value * (Ei[2]) - nz_ * value * (Ei[1]));
+      const double m1 = -(nz_ * value * (Ei[0]) - nx_ * value * (Ei[2]));
+      const double m2 = -(nx_ * value * (Ei[1]) - ny_ * value * (Ei[0]));
+#pragma unroll
+      for (int sd = 0; sd < 2; sd++) {
+        Js[sd][0] = Js[sd][0] + j0;
+        Js[sd][1] = Js[sd][1] + j1;
+        Js[sd][2] = Js[sd][2] + j2;
+        Ms[sd][0] = Ms[sd][0] + m0;
+        Ms[sd][1] = Ms[sd][1] + m1;
+        Ms[sd][2] = Ms[sd][2] + m2;
+      }
     }
     const double dl = fd.dl, Z0 = kZ0;
+    const double *fn = fld[0], *fx = fld[1], *Jn = Js[0], *Jx = Js[1], *Mn = Ms[0], *Mx = Ms[1];
     // connect_normal_to_{x,y,z}.F90: the side-1 source types act on both sides
     if (dir == 1) {  // connect_normal_to_x.F90:301-305
-      A_min = A_min * hsf[1] - fld[1] * dl - fld[5] * Z0 * dl + Js[1] * dl * Z0 / 2.0 + Ms[2] * dl / 2.0;
-      A_max = A_max * hsf[1] - fld[1] * dl + fld[5] * Z0 * dl + Js[1] * dl * Z0 / 2.0 - Ms[2] * dl / 2.0;
-      B_min = B_min * hsf[2] - fld[2] * dl + fld[4] * Z0 * dl + Js[2] * dl * Z0 / 2.0 - Ms[1] * dl / 2.0;
-      B_max = B_max * hsf[2] - fld[2] * dl - fld[4] * Z0 * dl + Js[2] * dl * Z0 / 2.0 + Ms[1] * dl / 2.0;
+      A_min = A_min * hsf[1] - fn[1] * dl - fn[5] * Z0 * dl + Jn[1] * dl * Z0 / 2.0 + Mn[2] * dl / 2.0;
+      A_max = A_max * hsf[1] - fx[1] * dl + fx[5] * Z0 * dl + Jx[1] * dl * Z0 / 2.0 - Mx[2] * dl / 2.0;
+      B_min = B_min * hsf[2] - fn[2] * dl + fn[4] * Z0 * dl + Jn[2] * dl * Z0 / 2.0 - Mn[1] * dl / 2.0;
+      B_max = B_max * hsf[2] - fx[2] * dl - fx[4] * Z0 * dl + Jx[2] * dl * Z0 / 2.0 + Mx[1] * dl / 2.0;
     } else if (dir == 2) {  // connect_normal_to_y.F90:304-308
-      A_min = A_min * hsf[0] - fld[0] * dl + fld[5] * Z0 * dl + Js[0] * dl * Z0 / 2.0 - Ms[2] * dl / 2.0;
-      A_max = A_max * hsf[0] - fld[0] * dl - fld[5] * Z0 * dl + Js[0] * dl * Z0 / 2.0 + Ms[2] * dl / 2.0;
-      B_min = B_min * hsf[2] - fld[2] * dl - fld[3] * Z0 * dl + Js[2] * dl * Z0 / 2.0 + Ms[0] * dl / 2.0;
-      B_max = B_max * hsf[2] - fld[2] * dl + fld[3] * Z0 * dl + Js[2] * dl * Z0 / 2.0 - Ms[0] * dl / 2.0;
+      A_min = A_min * hsf[0] - fn[0] * dl + fn[5] * Z0 * dl + Jn[0] * dl * Z0 / 2.0 - Mn[2] * dl / 2.0;
+      A_max = A_max * hsf[0] - fx[0] * dl - fx[5] * Z0 * dl + Jx[0] * dl * Z0 / 2.0 + Mx[2] * dl / 2.0;
+      B_min = B_min * hsf[2] - fn[2] * dl - fn[3] * Z0 * dl + Jn[2] * dl * Z0 / 2.0 + Mn[0] * dl / 2.0;
+      B_max = B_max * hsf[2] - fx[2] * dl + fx[3] * Z0 * dl + Jx[2] * dl * Z0 / 2.0 - Mx[0] * dl / 2.0;
     } else {  // connect_normal_to_z.F90:302-306
-      A_min = A_min * hsf[0] - fld[0] * dl - fld[4] * Z0 * dl + Js[0] * dl * Z0 / 2.0 + Ms[1] * dl / 2.0;
-      A_max = A_max * hsf[0] - fld[0] * dl + fld[4] * Z0 * dl + Js[0] * dl * Z0 / 2.0 - Ms[1] * dl / 2.0;
-      B_min = B_min * hsf[1] - fld[1] * dl + fld[3] * Z0 * dl + Js[1] * dl * Z0 / 2.0 - Ms[0] * dl / 2.0;
-      B_max = B_max * hsf[1] - fld[1] * dl - fld[3] * Z0 * dl + Js[1] * dl * Z0 / 2.0 + Ms[0] * dl / 2.0;
+      A_min = A_min * hsf[0] - fn[0] * dl - fn[4] * Z0 * dl + Jn[0] * dl * Z0 / 2.0 + Mn[1] * dl / 2.0;
+      A_max = A_max * hsf[0] - fx[0] * dl + fx[4] * Z0 * dl + Jx[0] * dl * Z0 / 2.0 - Mx[1] * dl / 2.0;
+      B_min = B_min * hsf[1] - fn[1] * dl + fn[3] * Z0 * dl + Jn[1] * dl * Z0 / 2.0 - Mn[0] * dl / 2.0;
+      B_max = B_max * hsf[1] - fx[1] * dl - fx[3] * Z0 * dl + Jx[1] * dl * Z0 / 2.0 + Mx[0] * dl / 2.0;
     }
   }
   // new incident pulses: + cell pulls its min port from the - cell's max-port

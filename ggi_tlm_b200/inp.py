@@ -37,7 +37,8 @@ import numpy as np
 
 from .meshfile import MeshFile, check_cells, connect_faces, pml_cells_from_mesh, read_mesh
 from .problem import (C0, MAT_PEC, MAT_PMC, SOURCE_HARD, SOURCE_SOFT, Block, CellList, DFTSurface, ExcitationFunction,
-                      FarFieldSurface, FrequencyOutputVolume, HuygensBox, HuygensOuter, HuygensPlane, OutputPoint,
+                      FarFieldSurface, FrequencyOutputVolume, HuygensBox, HuygensOuter, HuygensPlane, ModeOutput,
+                      OutputPoint,
                       OutputSurface, OutputVolume, PointExcitation, PowerSurface, ProblemSpec, RCSSurface, SARVolume,
                       SurfaceMaterial, SurfaceSheet, UnsupportedFeature, VolumeMaterial, Z0, _region_mask, nint)
 
@@ -69,18 +70,18 @@ NEUTRAL = {"new_mesh_generation", "no_geometry_vtk_files", "compress_output_file
            "inductance_equivalent_radius_factor", "lc_correction_type_geometry_scale",
            "lc_correction_type_subtract_cell_inductance", "max_cable_bundle_diameter_factor"}
 # packets of other parts of the reference the GPU path does not run
-UNSUPPORTED = {"periodic_boundary", "excitation_surface_list", "excitation_volume_list",
-               "ngspice_node_output_list", "periodic_boundary_far_field_surface", "excitation_mode_list",
+UNSUPPORTED = {"periodic_boundary",
+               "ngspice_node_output_list", "periodic_boundary_far_field_surface",
                "mode_stir_surface_list", "ngspice_timestep_factor",
                "ngspice_lpf_alpha", "cable_geometry_list", "cable_list", "cable_junction_list", "cable_output_list"}
-# run by the GPU path but not read here: a mode output's profile comes from a
-# separate mode field file (ModeOutput takes the profile directly)
-NOT_READ = {"output_mode_list"}
+# run by the GPU path but not read here
+NOT_READ = set()
 # packets read_inp turns into the spec
 HANDLED = {"wrapping_boundary_conditions", "mesh_outer_boundary_dimension", "mesh_cell_dimension", "mesh_dimensions_in_cells", "pml",
            "volume_list", "surface_list", "point_list", "simulation_time", "volume_material_list",
            "surface_material_list", "outer_boundary_reflection_coefficient", "excitation_function_list",
-           "excitation_point_list", "huygens_surface", "output_point_list", "output_surface_list",
+           "excitation_point_list", "excitation_surface_list", "excitation_volume_list", "excitation_mode_list",
+           "huygens_surface", "output_point_list", "output_surface_list", "output_mode_list",
            "output_volume_list", "output_volume_average_list", "output_volume_peak_list",
            "frequency_output_volume_list", "frequency_output_volume_list_xyz", "frequency_output_surface_list",
            "far_field_surface_list", "rcs_surface", "frequency_domain_power_surface_list", "sar_volume_list",
@@ -94,6 +95,7 @@ _FIELD = {"ex": "Ex", "ey": "Ey", "ez": "Ez", "hx": "Hx", "hy": "Hy", "hz": "Hz"
 _FIELD_OR_CURRENT = {**_FIELD, "jx": "Jx", "jy": "Jy", "jz": "Jz"}
 _SURFACE_FIELD = {**_FIELD_OR_CURRENT, "em": "Em", "hm": "Hm", "jm": "Jm"}
 _FACES = {"centre", "xmin", "xmax", "ymin", "ymax", "zmin", "zmax"}  # read_centre_or_face
+_FACE_OF_CODE = {1: "xmin", 2: "ymin", 3: "zmin", 4: "xmax", 5: "ymax", 6: "zmax"}  # Mesh_Modules.F90:40-46
 # parameters per geometry type (read_volume_list.F90:107-159, read_surface_list.F90:108-220);
 # the types marked with a file name read that line before the parameters
 _VOLUME_PARAMS = {"rectangular_block2": 6, "rectangular_block": 3, "cylinder": 2, "sphere": 1, "tet": 12, "hex": 24,
@@ -549,6 +551,57 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
             raise UnsupportedFeature(f"{what} on a volume of type {s.kind!r}")
         return _block_cells(mesh, s.par, s.tr, s.kind)
 
+    def mode_faces(surf: int, side: int, name: str, cols: Sequence[int], what: str):
+        """The faces of a mode excitation or output and their mode field
+        (set_mode_excitations_in_mesh, mode_excitation.F90:35-250, and
+        set_mode_outputs_in_mesh, output_modes.F90:35-250): the mode file's
+        samples in file order, moved by the offset between the bounding
+        cells of the samples and of the surface's faces, each on the
+        surface's (single) face code, taken from the other side of the face
+        unless ``side`` is 1."""
+        if open_file is None:
+            raise UnsupportedFeature(f"{what} from the mode file {name!r}: no file opener")
+        xcol, ycol, zcol, mcol = cols
+        if sorted((xcol, ycol, zcol)) != [1, 2, 3] or mcol < 4:
+            raise ValueError(f"{what}: mode file columns {cols} (x, y, z among 1..3, the data column above 3)")
+        samples = []
+        for ln in open_file(name):
+            f = ln.replace(",", " ").split()
+            if not f:
+                continue
+            if len(f) < mcol:
+                raise ValueError(f"{what}: mode file {name!r}: a line with fewer than {mcol} values")
+            c = (int(f[0]), int(f[1]), int(f[2]))
+            samples.append(((c[xcol - 1], c[ycol - 1], c[zcol - 1]), fortran_real(f[mcol - 1])))
+        geo, orient = surface_geo(surf, what, 1)
+        faces = FarFieldSurface([], side=orient, **geo).faces()  # the surface's own face list
+        if not faces or not samples:
+            return []
+        codes = {code for _, code in faces}
+        if len(codes) != 1:
+            raise ValueError(f"{what}: surface {surf} has faces of more than one orientation")
+        code = codes.pop()
+        lo_s = [min(c[a] for c, _ in faces) for a in range(3)]
+        hi_s = [max(c[a] for c, _ in faces) for a in range(3)]
+        lo_m = [min(c[a] for c, _ in samples) for a in range(3)]
+        hi_m = [max(c[a] for c, _ in samples) for a in range(3)]
+        n_s = [h - l + 1 for l, h in zip(lo_s, hi_s)]
+        n_m = [h - l + 1 for l, h in zip(lo_m, hi_m)]
+        if n_s != n_m:
+            raise ValueError(f"{what}: the mode's extent {n_m} differs from surface {surf}'s {n_s}")
+        if n_m[(code - 1) % 3] != 1:
+            raise ValueError(f"{what}: the mode is not planar along its surface's normal")
+        off = [a - b for a, b in zip(lo_s, lo_m)]
+        flip = {1: (0, -1, 4), 2: (1, -1, 5), 3: (2, -1, 6), 4: (0, 1, 1), 5: (1, 1, 2), 6: (2, 1, 3)}
+        out = []
+        for c, field in samples:
+            cell, fc = [c[a] + off[a] for a in range(3)], code
+            if side != 1:  # the face seen from the neighbouring cell
+                ax, d, fc = flip[code]
+                cell[ax] += d
+            out.append((tuple(cell), fc, field))
+        return out
+
     def surface_geo(surf: int, what: str, side: int) -> Tuple[dict, int]:
         """box=, plane= or (with a mesh file) records= of a surface, and the
         side in the spec's convention: the packet's side times the plane's
@@ -612,6 +665,84 @@ def read_inp(lines: Sequence[str], material: Callable[[str], VolumeMaterial],
                 raise ValueError(f"Excitation_point_list packet: source type {kind!r}")
             spec.point_excitations.append(PointExcitation(point_cell(pt), comp, fn,
                                                           SOURCE_SOFT if kind == "soft" else SOURCE_HARD, face=face))
+    # excitation surfaces and volumes (read_excitation_surface_list.F90:66-120,
+    # read_excitation_volume_list.F90): Surface_excitation and Volume_excitation
+    # (excitation_surfaces.F90, excitation_volumes.F90) add the function's value
+    # on every face side / cell of the geometry to the same field tables as the
+    # excitation points, after them, so each face side or cell becomes a face
+    # or centre point excitation appended after the packet's points
+    if "excitation_surface_list" in rec:
+        r = rec["excitation_surface_list"]
+        for k in range(1, r.ints(1)[0] + 1):
+            if r.ints(1)[0] != k:
+                raise ValueError("Excitation_surface_list packet: surfaces must be numbered in order")
+            fn, surf, side = r.ints(1)[0], r.ints(1)[0], r.ints(1)[0]
+            if side not in (1, -1, 0):
+                raise ValueError("Excitation_surface_list packet: the side must be 1, -1 or 0")
+            comp = _component(r, _FIELD)
+            kind = r.text()
+            if kind not in ("soft", "hard"):
+                raise ValueError(f"Excitation_surface_list packet: source type {kind!r}")
+            # side 0 takes each face from the other side (as -1) and excites both of its sides;
+            # otherwise the side of the face the (possibly flipped) face code names
+            geo, eff = surface_geo(surf, "an excitation surface", -1 if side == 0 else side)
+            for cell, code in FarFieldSurface([], side=eff, **geo).faces():
+                spec.point_excitations.append(PointExcitation(
+                    tuple(cell), comp, fn, SOURCE_SOFT if kind == "soft" else SOURCE_HARD,
+                    face=_FACE_OF_CODE[code], one_side=side != 0))
+    if "excitation_volume_list" in rec:
+        r = rec["excitation_volume_list"]
+        for k in range(1, r.ints(1)[0] + 1):
+            if r.ints(1)[0] != k:
+                raise ValueError("Excitation_volume_list packet: volumes must be numbered in order")
+            fn, v = r.ints(1)[0], r.ints(1)[0]
+            comp = _component(r, _FIELD)
+            kind = r.text()
+            if kind not in ("soft", "hard"):
+                raise ValueError(f"Excitation_volume_list packet: source type {kind!r}")
+            region = volume_block(v, "an excitation volume")
+            zz, yy, xx = np.nonzero(FrequencyOutputVolume(region, [], comp).mask(spec))
+            for x, y, z in zip(xx, yy, zz):  # the volume's cells in traversal order
+                spec.point_excitations.append(PointExcitation(
+                    (int(x) + 1, int(y) + 1, int(z) + 1), comp, fn, SOURCE_SOFT if kind == "soft" else SOURCE_HARD))
+    # mode excitations (read_excitation_mode_list.F90:52-110, Mode_excitation,
+    # mode_excitation.F90:330-420): the function's value times each face's
+    # mode field on one side of the face, or half of it on both sides for
+    # side 0 (E and H only: the Huygens surface's J, M, added before them in
+    # the step, touch other components)
+    if "excitation_mode_list" in rec:
+        r = rec["excitation_mode_list"]
+        for k in range(1, r.ints(1)[0] + 1):
+            if r.ints(1)[0] != k:
+                raise ValueError("Excitation_mode_list packet: modes must be numbered in order")
+            fn, surf, side = r.ints(1)[0], r.ints(1)[0], r.ints(1)[0]
+            if side not in (1, -1, 0):
+                raise ValueError("Excitation_mode_list packet: the side must be 1, -1 or 0")
+            comp = _component(r, _FIELD)
+            kind = r.text()
+            if kind not in ("soft", "hard"):
+                raise ValueError(f"Excitation_mode_list packet: source type {kind!r}")
+            name = r.line().strip()
+            cols = [r.ints(1)[0] for _ in range(4)]
+            for cell, code, field in mode_faces(surf, side, name, cols, "an excitation mode"):
+                spec.point_excitations.append(PointExcitation(
+                    cell, comp, fn, SOURCE_SOFT if kind == "soft" else SOURCE_HARD, face=_FACE_OF_CODE[code],
+                    one_side=side != 0, scale=field if side != 0 else field / 2.0))
+    # mode outputs (read_output_mode_list.F90:50-90, Mode_output,
+    # output_modes.F90:546-620)
+    if "output_mode_list" in rec:
+        r = rec["output_mode_list"]
+        for k in range(1, r.ints(1)[0] + 1):
+            if r.ints(1)[0] != k:
+                raise ValueError("Output_mode_list packet: modes must be numbered in order")
+            surf, side = r.ints(1)[0], r.ints(1)[0]
+            if side not in (1, -1):
+                raise ValueError("Output_mode_list packet: the side must be 1 or -1")
+            comp = _component(r, _FIELD)
+            name = r.line().strip()
+            cols = [r.ints(1)[0] for _ in range(4)]
+            spec.mode_outputs.append(ModeOutput(comp, None, None, samples=mode_faces(surf, side, name, cols,
+                                                                                      "an output mode")))
     # the Huygens surface, read_huygens_surface.F90:89-200
     if "huygens_surface" in rec:
         r = rec["huygens_surface"]

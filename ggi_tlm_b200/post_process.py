@@ -21,6 +21,8 @@ option here takes the same answers in the same order:
   ``.Zs`` companion);
 * 10 two-port analysis (twoport.F90): eight spectra, separation and
   distance of port 1 and of port 2, excitation port, output file;
+* 13 extract a mode from a frequency output surface file (extract_mode.F90):
+  file, then surface numbers each followed by its mode file, ended by 0;
 * 15 transmission cross section (transmission_cross_section.F90): power
   spectrum, field spectrum, e|h, output file.
 
@@ -82,6 +84,39 @@ def _spectrum(a: _Answers, directory: str):
     return fout.spectrum(rows)
 
 
+def read_frequency_output_surfaces(path: str) -> List[np.ndarray]:
+    """The faces' data of each surface of a ``.frequency_output_surface.fout``
+    as extract_mode.F90:120-196 reads it: per surface [faces] rows of cx, cy,
+    cz and the phasor, the phasor held in single precision (``cmplx`` of
+    default kind)."""
+    with open(path) as f:
+        lines = [ln for ln in f.read().splitlines()]
+    pos = 1
+    n_surfaces = int(lines[pos].split()[0]); pos += 1
+    out = []
+    for _ in range(n_surfaces):
+        pos += 2
+        n_points = int(lines[pos].split()[0]); pos += 2
+        n_quads = int(lines[pos].split()[0]); pos += 2
+        pos += 1 + n_points + n_quads  # frame count, corners, quads
+        rows = np.loadtxt(lines[pos:pos + n_quads], ndmin=2)
+        pos += n_quads
+        out.append(rows)
+    return out
+
+
+def mode_lines(rows: np.ndarray) -> List[str]:
+    """A mode file (extract_mode.F90:226-236, format(3I10,3E16.7)): cell,
+    real and imaginary part and magnitude of each face's phasor, the parts
+    rounded to single precision (``cmplx`` of default kind) and stored in a
+    double complex (post_process_modules.F90:70), whose magnitude is taken
+    in double precision."""
+    z = rows[:, 3].astype(np.float32).astype(np.float64) + 1j * rows[:, 4].astype(np.float32).astype(np.float64)
+    mag = np.abs(z)
+    return ["".join(f"{int(c):10d}" for c in r[:3]) + tout.fortran_e(float(v.real), 16, 7) +
+            tout.fortran_e(float(v.imag), 16, 7) + tout.fortran_e(float(m), 16, 7) for r, v, m in zip(rows, z, mag)]
+
+
 def _write(path: str, lines: Sequence[str]) -> None:
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
@@ -132,6 +167,17 @@ def run(lines: Sequence[str], directory: str = ".") -> List[str]:
             out = os.path.join(directory, a.name())
             _write(out, fout.twoport_lines(spec[0][0], [s[1] for s in spec], d1, l1, d2, l2, port))
             written.append(out)
+        elif option == 13:
+            surfaces = read_frequency_output_surfaces(os.path.join(directory, a.name()))
+            while True:
+                k = a.integer()
+                if k == 0:
+                    break
+                if not 1 <= k <= len(surfaces):
+                    raise ValueError(f"extract mode: surface {k} is not between 1 and {len(surfaces)}")
+                out = os.path.join(directory, a.name())
+                _write(out, mode_lines(surfaces[k - 1]))
+                written.append(out)
         elif option == 15:
             power_path, power_point = os.path.join(directory, a.name()), a.integer()
             field_path, field_point = os.path.join(directory, a.name()), a.integer()

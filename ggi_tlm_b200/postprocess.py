@@ -189,6 +189,14 @@ def sar_values(spec, t: dict, acc: np.ndarray, densities: Sequence[float]) -> Li
     return rows
 
 
+def check_sar_volumes(spec) -> None:
+    """Raise unless every SAR volume lies in a material of constant
+    permittivity without magnetic conductivity (initialise_SAR_volumes,
+    SAR_volumes.F90:150-190, stops the run otherwise)."""
+    for sv in spec.sar_volumes:
+        _sar_material(spec, sv)
+
+
 def _sar_material(spec, sv):
     """The volume material whose cells the SAR volume covers."""
     from .problem import _region_mask
@@ -346,6 +354,42 @@ def surface_field_template(number: int, spec, faces, n_frames: int) -> List[str]
     out += [f"{4:3d}" + "".join(f"{4 * k + j:12d}" for j in range(4)) for k in range(len(faces))]
     out.append(f"# END SURFACE FIELD FILE TEMPLATE, OUTPUT SURFACE NUMBER:{number:5d}")
     return out
+
+
+def frequency_output_surface_lines(spec, t: dict, dft: np.ndarray) -> List[str]:
+    """``.frequency_output_surface.fout``: the entry count
+    (frequency_output_surfaces.F90:265-268), then per entry (one surface and
+    frequency) its template (:646-677; the four corners of every face after
+    the side flip, 24 frames) and each face's cell and phasor, real,
+    imaginary and magnitude (:679-696).  ``dft`` is [faces, 2] in the
+    tables' entry order."""
+    entries = [ds for ds in spec.dft_surfaces for _ in ds.frequencies]
+    ptr = np.asarray(t["dft_face_ptr"]) if len(entries) else np.zeros(1, dtype=np.int32)
+    out = ["# NUMBER OF FREQUENCY OUTPUT SURFACES:", f"{len(entries):10d}"]
+    for d, ds in enumerate(entries):
+        faces = ds.faces()
+        if len(faces) != int(ptr[d + 1] - ptr[d]):
+            raise ValueError(f"frequency output surface {d + 1}: {len(faces)} faces, tables hold {ptr[d + 1] - ptr[d]}")
+        out += [f"# START SURFACE FIELD FILE TEMPLATE, OUTPUT SURFACE NUMBER:{d + 1:10d}",
+                "# Number of points:", f"{4 * len(faces):10d}", "# Number of faces:", f"{len(faces):10d}",
+                "# Number of frames:", f"{24:10d}"]
+        for cell, code in faces:
+            out += [_xyz_line(_corner(spec.origin, spec.dl, cell, off)) for off in _FACE_CORNERS[code]]
+        out += [f"{4:3d}" + "".join(f"{4 * k + j:12d}" for j in range(4)) for k in range(len(faces))]
+        for (cell, _), (re, im) in zip(faces, dft[ptr[d]:ptr[d + 1]]):
+            out.append("".join(f"{int(c):8d}" for c in cell) +  # format(3I8,3E16.8)
+                       fortran_e(re, 16, 8) + fortran_e(im, 16, 8) + fortran_e(abs(complex(re, im)), 16, 8))
+    return out
+
+
+def write_frequency_output_surfaces(name: str, spec, t: dict, dft: np.ndarray, directory: str = ".") -> List[str]:
+    if not spec.dft_surfaces:
+        return []
+    path = os.path.join(directory, name + ".frequency_output_surface.fout")
+    with open(path, "w") as f:
+        for line in frequency_output_surface_lines(spec, t, dft):
+            f.write(line + "\n")
+    return [path]
 
 
 def _output_steps(first: int, last: Optional[int], interval: int, n: int) -> List[int]:

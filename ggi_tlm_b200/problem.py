@@ -472,6 +472,13 @@ class PointExcitation:
     function: int  # 1-based function number
     source_type: int = SOURCE_SOFT
     face: str = "centre"  # or xmin, xmax, ymin, ymax, zmin, zmax: a point source on that face of the cell
+    # a face source on that side of the face alone (side 1 for a min face, 2 for a max face), as
+    # Surface_excitation applies a one-sided surface (excitation_surfaces.F90:236-262); a point
+    # source on a face reaches both sides (excitation_points.F90:286-323)
+    one_side: bool = False
+    # the function's value times this factor: a mode excitation's mode field, halved when it
+    # excites both sides (mode_excitation.F90:393-411)
+    scale: float = 1.0
 
 
 @dataclass
@@ -691,15 +698,25 @@ class PowerSurface:
 class ModeOutput:
     """A mode output (OUTPUT/output_modes.F90): every step the sum over the
     faces of a plane patch of one field component on each face's side
-    times the mode field ``profile(i, j, k)`` of the face's cell."""
+    times the mode field ``profile(i, j, k)`` of the face's cell, or over
+    ``samples`` (cell, face code, mode field) in their order, as the reader
+    takes them from a mode file (set_mode_outputs_in_mesh)."""
 
     component: str
-    plane: Tuple[int, int, Tuple[int, int], Tuple[int, int]]
+    plane: Optional[Tuple[int, int, Tuple[int, int], Tuple[int, int]]]
     profile: object
     side: int = 1
+    samples: Optional[List[Tuple[Tuple[int, int, int], int, float]]] = None
 
     def faces(self) -> List[Tuple[Tuple[int, int, int], int]]:
+        if self.samples is not None:
+            return [(tuple(int(v) for v in c), int(code)) for c, code, _ in self.samples]
         return FarFieldSurface([], None, self.plane, self.side).faces()
+
+    def weights(self) -> List[float]:
+        if self.samples is not None:
+            return [float(w) for _, _, w in self.samples]
+        return [float(self.profile(*c)) for c, _ in self.faces()]
 
 
 @dataclass
@@ -1030,6 +1047,8 @@ def build_tables(spec: ProblemSpec) -> dict:
         if q.face != "centre" and q.face not in FACE_POINT:
             raise ValueError(f"unknown face {q.face!r}")
     centre_pts = [q for q in spec.point_excitations if q.face == "centre"]
+    if any(q.scale != 1.0 or q.one_side for q in centre_pts):
+        raise ValueError("a centre point excitation takes neither a scale nor a side")
     centre_outs = [q for q in spec.outputs if q.face == "centre"]
     cell_exc = np.zeros((nz, ny, nx), dtype=bool)
     for pe in centre_pts:
@@ -1243,6 +1262,12 @@ def build_tables(spec: ProblemSpec) -> dict:
         for key, sg in zip(sh.face_keys(), sh.face_signs()):  # the last sheet on a face wins
             face_mat[key] = SURFACE_SHEET_TYPES[sh.kind]
             face_smat[key] = sg * sh.material if sh.kind == "dispersive" else 0
+    # connect visits the internal faces only (connect.F90:180-213: cx, cy,
+    # cz .ne. 1), so a surface material on a face of the outer boundary
+    # changes nothing: such faces are dropped
+    for key in [k for k in face_mat if not 1 < k[0][k[1] - 1] <= (nx, ny, nz)[k[1] - 1]]:
+        del face_mat[key]
+        face_smat.pop(key, None)
     keys = set(face_exc) | set(face_out) | set(face_mat)
     for (c, axis) in keys:
         if c[axis - 1] <= 1 or c[axis - 1] > (nx, ny, nz)[axis - 1]:
@@ -1271,6 +1296,8 @@ def build_tables(spec: ProblemSpec) -> dict:
         fpt_comp=np.array([COMPONENTS[q.component] for q, _, _ in face_pts], dtype=np.int32),
         fpt_fn=np.array([q.function for q, _, _ in face_pts], dtype=np.int32),
         fpt_type=np.array([q.source_type for q, _, _ in face_pts], dtype=np.int32),
+        fpt_side=np.array([side if q.one_side else 0 for q, _, side in face_pts], dtype=np.int32),
+        fpt_scale=np.array([q.scale for q, _, _ in face_pts], dtype=np.float64),
         n_face_probes=len(face_probes),
         fprobe_face=np.array([fout_num[k] for _, k, _ in face_probes], dtype=np.int32),
         fprobe_side=np.array([sd for _, _, sd in face_probes], dtype=np.int32),
@@ -1494,10 +1521,10 @@ def build_tables(spec: ProblemSpec) -> dict:
         if COMPONENTS.get(mo.component, 0) not in range(1, 7):
             raise ValueError("a mode output samples Ex..Hz")
         mc.append(COMPONENTS[mo.component])
-        for c, code in fl:
+        for (c, code), w in zip(fl, mo.weights()):
             mfo.append(fout_num[connect_key(c, code)])
             mfc.append(code)
-            mw.append(float(mo.profile(*c)))
+            mw.append(w)
         mptr.append(len(mfo))
     tables.update(n_modes=len(mc), mode_comp=np.array(mc, dtype=np.int32), mode_face_ptr=np.array(mptr, dtype=np.int32),
                   mode_face_out=np.array(mfo, dtype=np.int32), mode_face_code=np.array(mfc, dtype=np.int32),

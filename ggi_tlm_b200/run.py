@@ -74,13 +74,16 @@ def write_results(name: str, p: InpProblem, t: dict, cell_out: np.ndarray, face_
                   volumes: Optional[List[np.ndarray]] = None, directory: str = ".",
                   power: Optional[np.ndarray] = None, far_field: Optional[np.ndarray] = None,
                   sar: Optional[np.ndarray] = None, rcs: Optional[np.ndarray] = None,
-                  surfaces: Optional[List[np.ndarray]] = None) -> List[str]:
+                  surfaces: Optional[List[np.ndarray]] = None, dft: Optional[np.ndarray] = None,
+                  modes: Optional[np.ndarray] = None) -> List[str]:
     """Write the result files of a finished run; returns the paths written.
     ``cell_out`` is [steps, n_kept, 6], ``face_out`` [n_face_points, steps],
     ``volumes`` the output volume results, ``power`` the power surface
     accumulators [faces, 4], ``far_field`` the far-field accumulators
     [faces, 6], ``sar`` the SAR accumulators [cells, 3], ``rcs`` the RCS
-    far field [4, points] and ``surfaces`` the output surface frames."""
+    far field [4, points], ``surfaces`` the output surface frames, ``dft``
+    the frequency output surfaces' phasors [faces, 2] and ``modes`` the mode
+    outputs [modes, steps]."""
     written = []
     n = int(t["n_timesteps"])
     if int(t["n_functions"]):
@@ -107,6 +110,16 @@ def write_results(name: str, p: InpProblem, t: dict, cell_out: np.ndarray, face_
     if p.spec.rcs_surface is not None and rcs is not None:
         written += postprocess.write_rcs(name, t, rcs, p.post["rcs"], int(t["hs_fn"]), directory)
     written += postprocess.write_field_files(name, p.spec, t, surfaces, volumes, directory)
+    if p.spec.dft_surfaces and dft is not None:
+        written += postprocess.write_frequency_output_surfaces(name, p.spec, t, dft, directory)
+    if p.spec.mode_outputs and modes is not None:
+        # Mode_output (output_modes.F90:546-620): every step after connect, at time (timestep-1)*dt + dt/2
+        dt = float(t["dt"])
+        rows = [((ts - 1) * dt + dt / 2.0, k + 1, float(modes[k, ts - 1]))
+                for ts in range(1, n + 1) for k in range(len(p.spec.mode_outputs))]
+        path = os.path.join(directory, name + ".mode.tout")
+        _write(path, header(len(p.spec.mode_outputs), n), rows)
+        written.append(path)
     for kind, extn in (("average", ".volume_average_field.tout"), ("peak", ".volume_peak_field.tout")):
         if any(v.kind == kind for v in p.spec.output_volumes):
             rows, count = _volume_rows(t, p.spec, volumes, kind)
@@ -134,6 +147,7 @@ def run(name: str, precision: int = capi.TLM_PRECISION_FP64, device: int = 0, ch
             print("left out", item)
     t = build_tables(p.spec)
     n = int(t["n_timesteps"])
+    postprocess.check_sar_volumes(p.spec)  # the reference stops here, before time stepping
     with capi.GpuMesh(t, precision=precision, device=device) as g:
         cells, faces = [], []
         for first in range(1, n + 1, chunk):
@@ -149,7 +163,10 @@ def run(name: str, precision: int = capi.TLM_PRECISION_FP64, device: int = 0, ch
         sar = g.sar_volumes() if p.spec.sar_volumes else None
         rcs = g.rcs() if p.spec.rcs_surface is not None else None
         surfaces = g.output_surfaces() if p.spec.output_surfaces else None
-    return write_results(name, p, t, cell_out, face_out, volumes, directory, power, far_field, sar, rcs, surfaces)
+        dft = g.dft() if p.spec.dft_surfaces else None
+        modes = g.mode_outputs(1, n) if p.spec.mode_outputs else None
+    return write_results(name, p, t, cell_out, face_out, volumes, directory, power, far_field, sar, rcs, surfaces,
+                         dft, modes)
 
 
 def main(argv: Optional[Sequence[str]] = None) -> int:

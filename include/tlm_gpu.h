@@ -193,6 +193,22 @@ int tlm_gpu_set_outer_huygens(int64_t handle, int32_t n_faces, const int32_t *ce
 int tlm_gpu_set_face_excitation(int64_t handle, int32_t n_points, const int32_t *face_exc, const int32_t *component,
                                 const int32_t *function, const int32_t *source_type);
 
+/* Excitation surfaces (SRC/EXCITATION/excitation_surfaces.F90:218-275) as
+   face sources, listed after the point sources: per entry of
+   tlm_gpu_set_face_excitation 0 (both sides, a point source or a surface
+   with side 0) or the one side, 1 (min) or 2 (max), that receives the
+   value; a source type set on side 2 alone does not reach connect, which
+   reads side 1's types on both sides.  Optional: without it every entry
+   reaches both sides.  Replaces Surface_excitation's face loop. */
+int tlm_gpu_set_face_excitation_side(int64_t handle, int32_t n_points, const int32_t *side);
+
+/* Mode excitations (SRC/EXCITATION/mode_excitation.F90:330-420) as face
+   sources listed last: per entry of tlm_gpu_set_face_excitation the factor
+   on the function's value, the face's mode field on one side, or half of it
+   on both sides (side 0 of the packet).  Optional: without it every factor
+   is 1.  Replaces Mode_excitation's face loop. */
+int tlm_gpu_set_face_excitation_scale(int64_t handle, int32_t n_points, const double *scale);
+
 /* Output points on cell faces (SRC/OUTPUT/output_points.F90:255-444):
    1-based output face number, side (1 = the min-side field, face_xmin/ymin/
    zmin; 2 = the max side) and component 1..6 of face_output_field after
@@ -473,6 +489,13 @@ int tlm_gpu_destroy(int64_t handle);
    while it does. */
 int tlm_gpu_batch_create(const int64_t *handles, int32_t n_meshes, int64_t *batch);
 int tlm_gpu_batch_set_variant(int64_t batch, int32_t variant);
+/* Replace the meshes of a batch (same precision and device; a mesh may stay,
+   leave or join).  The batch first waits for its queued steps; meshes that
+   leave can then be run alone, read or destroyed, and the work lists are
+   rebuilt at the next tlm_gpu_batch_run.  The batch keeps its stream, graph
+   resources and device buffers, so a serving loop changes membership
+   without destroying and creating batches. */
+int tlm_gpu_batch_set_members(int64_t batch, const int64_t *handles, int32_t n_meshes);
 /* Advance every unfinished mesh by up to n_steps steps (asynchronous). */
 int tlm_gpu_batch_run(int64_t batch, int32_t n_steps);
 int tlm_gpu_batch_synchronize(int64_t batch);

@@ -54,7 +54,7 @@ class _Problem(C.Structure):
         ("ff_face_code", _i32p), ("face_mat", _i32p),
         ("face_smat", _i32p), ("n_smat", C.c_int32), ("smat_f", _f64p), ("smat_a", _f64p), ("smat_b", _f64p),
         ("smat_order", _i32p), ("wrap", C.c_int32 * 3), ("slab", C.c_int32 * 2),
-        ("dft_gate", _i32p),
+        ("dft_gate", _i32p), ("fpt_side", _i32p), ("fpt_scale", _f64p),
     ]
 
 
@@ -157,9 +157,11 @@ class Oracle:
             for k in ("smat_f", "smat_a", "smat_b"):
                 setattr(p, k, arr(k, np.float64))
             p.smat_order = arr("smat_order", np.int32)
-        for k in ("fpt_face", "fpt_comp", "fpt_fn", "fpt_type", "fprobe_face", "fprobe_side", "fprobe_comp",
-                  "hs_cell"):
+        for k in ("fpt_face", "fpt_comp", "fpt_fn", "fpt_type", "fpt_side", "fprobe_face", "fprobe_side",
+                  "fprobe_comp", "hs_cell"):
             setattr(p, k, arr(k, np.int32) if k in t else arr_empty())
+        if "fpt_scale" in t and int(t.get("n_face_points", 0)):
+            p.fpt_scale = arr("fpt_scale", np.float64)
         if int(t.get("n_pml_material_cells", 0)):
             p.pml_sigma = arr("pml_sigma", np.float64)
         p.n_small_to_zero = int(t.get("n_small_to_zero", 0))

@@ -266,11 +266,19 @@ static void excitation(tlm_oracle_state *s, int timestep) {
     if (comp < 6) s->cell_exc_type[cell * 6 + comp] = p->pt_type[e];
   }
   /* Point_excitation, face points (excitation_points.F90:286-323): the value
-     goes to both sides of the face, the source type too (components 1..6) */
+     goes to both sides of the face, the source type too (components 1..6);
+     then Surface_excitation (excitation_surfaces.F90:218-275), whose faces
+     follow the points in the list: one side, or both; Mode_excitation's
+     faces (mode_excitation.F90:370-415) come last, each value times its
+     mode field (E and H only, so the Huygens J, M added below are not
+     reordered against them) */
   for (int e = 0; e < p->n_face_points; e++) {
     int face = p->fpt_face[e] - 1, comp = p->fpt_comp[e] - 1;
     double value = p->fn_value_face[(size_t)(p->fpt_fn[e] - 1) * p->n_timesteps + (timestep - 1)];
+    if (p->fpt_scale) value = p->fpt_scale[e] * value;
+    int only = p->fpt_side ? p->fpt_side[e] : 0;
     for (int side = 0; side < 2; side++) {
+      if (only && side != only - 1) continue;
       double *fe = s->face_exc + (size_t)face * 24 + side * 12;
       fe[comp] = fe[comp] + value;
       if (comp < 6) s->face_exc_type[(size_t)face * 12 + side * 6 + comp] = p->fpt_type[e];

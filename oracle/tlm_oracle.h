@@ -165,6 +165,16 @@ typedef struct {
      first, last, interval (get_output_flag, OUTPUT/output.F90:564-598);
      NULL: every step */
   const int32_t *dft_gate;
+
+  /* the side of each face point source: 0 both (a point excitation,
+     excitation_points.F90:286-323), 1 or 2 that side alone (a one-sided
+     excitation surface, excitation_surfaces.F90:236-262); NULL: all 0 */
+  const int32_t *fpt_side;
+
+  /* the factor on the function's value of each face point source: a mode
+     excitation's mode field, halved on both sides (Mode_excitation,
+     mode_excitation.F90:393-411); NULL: all 1 */
+  const double *fpt_scale;
 } tlm_oracle_problem;
 
 typedef struct tlm_oracle_state tlm_oracle_state;

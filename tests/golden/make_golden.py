@@ -72,9 +72,16 @@ INP_CASES = {
     "fss_single_cell": "PARAMETERISED_FSS/PROBLEM_SPECIFICATION_FILES/single_cell.inp",
     "material_test": "MATERIAL_TEST/PROBLEM_SPECIFICATION_FILES/mat_test.inp",
     "resonant_absorber": "RESONANT_ABSORBER/PROBLEM_SPECIFICATION_FILES/TEM_cell.inp",
+    # a PEC waveguide cavity driven by a soft Ex excitation surface across its cross section
+    "waveguide": "WAVEGUIDE_RESONATOR/PROBLEM_SPECIFICATION_FILES/waveguide.inp",
+    # WR90 waveguides driven by a TE10 mode excitation from a mode file, ended by mode-impedance
+    # thin layers: straight, with a PML, and with an iris
+    "waveguide_straight": "WAVEGUIDE_STRAIGHT/PROBLEM_SPECIFICATION_FILES/waveguide_straight.inp",
+    "waveguide_pml": "WAVEGUIDE_PML/PROBLEM_SPECIFICATION_FILES/waveguide_pml.inp",
+    "waveguide_iris": "WAVEGUIDE_IRIS/PROBLEM_SPECIFICATION_FILES/waveguide_iris.inp",
 }
 # the surface material files the thin-layer cases use, as text
-SMAT_CASES = ["Dispersive_sheet", "Anisotropic_sheet"]
+SMAT_CASES = ["Dispersive_sheet", "Anisotropic_sheet", "WR90_mode_impedance"]
 # result files the solver writes after the run (write_SAR_volumes), as text
 RESULT_CASES = {
     "sar_test": "SAR_TEST/PROBLEM_SPECIFICATION_FILES/SAR_test.SAR.fout_ref",
@@ -86,6 +93,12 @@ RESULT_HEADS = {
     # HELIX_ANTENNA's surface field file: the template of its one output
     # surface and the first data frame (output_surfaces.F90:326-927)
     "helix_surface_field": ("HELIX_ANTENNA/helix.surface_field.tout", 10603),
+    # the mode-excited waveguides' time-domain results, whole
+    "waveguide_straight_mode": ("WAVEGUIDE_STRAIGHT/PROBLEM_SPECIFICATION_FILES/waveguide_straight.mode.tout_ref", None),
+    "waveguide_straight_field": ("WAVEGUIDE_STRAIGHT/PROBLEM_SPECIFICATION_FILES/waveguide_straight.field.tout_ref",
+                                 None),
+    "waveguide_pml_Ex1": ("WAVEGUIDE_PML/PROBLEM_SPECIFICATION_FILES/Ex1.tout_ref", None),
+    "waveguide_iris_field": ("WAVEGUIDE_IRIS/PROBLEM_SPECIFICATION_FILES/waveguide_iris.field.tout_ref", None),
 }
 # mesh files written by the reference's mesher (MESH/write_mesh.F90), as text
 MESH_CASES = {
@@ -97,10 +110,18 @@ POST_CASES = {
     "fss": "PARAMETERISED_FSS/PROBLEM_SPECIFICATION_FILES/GGI_TLM_post_process_in.txt",
     "resonant_absorber": "RESONANT_ABSORBER/PROBLEM_SPECIFICATION_FILES/GGI_TLM_post_process_in.txt",
     "box_slot": "SHIELDING_EFFECTIVENESS_BOX_SLOT/PROBLEM_SPECIFICATION_FILES/GGI_TLM_post_process_in.txt",
+    "waveguide": "WAVEGUIDE_RESONATOR/PROBLEM_SPECIFICATION_FILES/GGI_TLM_post_process_in.txt",
+    "waveguide_straight": "WAVEGUIDE_STRAIGHT/PROBLEM_SPECIFICATION_FILES/GGI_TLM_post_process_in.txt",
+    "waveguide_pml": "WAVEGUIDE_PML/PROBLEM_SPECIFICATION_FILES/GGI_TLM_post_process_in.txt",
+    "waveguide_iris": "WAVEGUIDE_IRIS/PROBLEM_SPECIFICATION_FILES/GGI_TLM_post_process_in.txt",
 }
 # data files the inputs name (excitation function samples), as text
 DATA_CASES = {
     "gaussian_from_file.dat": "EXCITATION_FUNCTION_TEST/PROBLEM_SPECIFICATION_FILES/gaussian_from_file.dat",
+    # each waveguide case's own mode file (NAME@case)
+    "WR90.mode@waveguide_straight": "WAVEGUIDE_STRAIGHT/PROBLEM_SPECIFICATION_FILES/WR90.mode",
+    "WR90.mode@waveguide_pml": "WAVEGUIDE_PML/PROBLEM_SPECIFICATION_FILES/WR90.mode",
+    "WR90.mode@waveguide_iris": "WAVEGUIDE_IRIS/PROBLEM_SPECIFICATION_FILES/WR90.mode",
 }
 # the post-processor's Fourier transforms of those four cases' output point
 # (GGI_TLM_post_process_in.txt beside each: option 3, point 1, lin 1 MHz to
@@ -120,6 +141,15 @@ FOUT_CASES = {
     "power_calc_tcs": "POWER_CALCS/PROBLEM_SPECIFICATION_FILES/TCS.fout_ref",
     # eight volume averages Fourier transformed (option 3), then the two-port analysis (option 10)
     "fss_s21": "PARAMETERISED_FSS/PROBLEM_SPECIFICATION_FILES/S21.fout_4_ref",
+    # option 3 on output point 1 (8 GHz to 12 GHz, 800 frequencies), then option 13: the mode on
+    # the frequency output surface
+    "waveguide": "WAVEGUIDE_RESONATOR/PROBLEM_SPECIFICATION_FILES/waveguide.field.fout_ref",
+    "waveguide_mode": "WAVEGUIDE_RESONATOR/PROBLEM_SPECIFICATION_FILES/WR90.mode_ref",
+    # the mode-excited waveguides: four mode outputs Fourier transformed (option 3), then the one-port
+    # (option 9) or, for the iris, eight, then the two-port analysis (option 10)
+    "waveguide_straight": "WAVEGUIDE_STRAIGHT/PROBLEM_SPECIFICATION_FILES/waveguide_straight.fout_ref",
+    "waveguide_pml": "WAVEGUIDE_PML/PROBLEM_SPECIFICATION_FILES/waveguide_pml.fout_ref",
+    "waveguide_iris": "WAVEGUIDE_IRIS/PROBLEM_SPECIFICATION_FILES/waveguide_iris.fout_ref",
 }
 
 
@@ -183,7 +213,7 @@ def main():
             rs[name] = np.array(f.read().splitlines())
     for name, (rel, n_lines) in RESULT_HEADS.items():
         with open(os.path.join(ref, "GGI_TLM", "TEST_DATA", rel)) as f:
-            rs[name] = np.array(f.read().splitlines()[:n_lines])
+            rs[name] = np.array(f.read().splitlines()[:n_lines])  # None: every line
     np.savez_compressed(os.path.join(here, "result_text.npz"), **rs)
     print("result_text", {k: len(v) for k, v in rs.items()})
     me = {}

@@ -319,7 +319,7 @@ Ez
     ("Surface_list\n1\n1\nrectangle\n1.0 1.0\n0 0 0\n0.5 0.5 0.5\nSurface_material_list\n1\n1\nDISPERSIVE\n"
      "MATERIAL_DIRECTORY/sheet\n1\n1\n1\n", "no surface material file resolver"),
     ("Cable_list\n0\n", "cable_list packet"),
-    ("Output_mode_list\n0\n", "ModeOutput"),
+    ("Output_mode_list\n1\n1\n1\n1\nEx\nWR90.mode\n1\n2\n3\n6\n", "no file opener"),          # mode file
     ("Frequency_scale_flag\nT\n2.0\n", "frequency scale"),
     ("Bicubic_warp_flag\n.true.\n", "bicubic"),
     ("Excitation_function_list\n1\n1\nnoise\n1.0\n", "function 'noise'"),

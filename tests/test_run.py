@@ -47,7 +47,12 @@ def oracle_files(tmp, name, lines):
     vols = oracle.output_volumes(t, cell) if p.spec.output_volumes else None
     power = oracle.power_surfaces(t) if p.spec.power_surfaces else None
     surfs = oracle.output_surfaces(t) if p.spec.output_surfaces else None
-    return runner.write_results(name, p, t, cell, face, vols, tmp, power, surfaces=surfs), p, t
+    dft = o.dft() if p.spec.dft_surfaces else None
+    far = o.far_field() if p.spec.far_field_surfaces else None
+    rcs = oracle.rcs(t) if p.spec.rcs_surface is not None else None
+    modes = oracle.mode_outputs(t) if p.spec.mode_outputs else None
+    return runner.write_results(name, p, t, cell, face, vols, tmp, power, far, rcs=rcs, surfaces=surfs, dft=dft,
+                                modes=modes), p, t
 
 
 # ALL_OUTPUTS with an output surface (the rectangle at z = 0.7, Ez on output
@@ -119,8 +124,9 @@ def test_volume_average_and_peak_files(tmp_path):
     lines = test_inp.ALL_OUTPUTS.splitlines()
     paths, p, t = oracle_files(str(tmp_path), "all", lines)
     names = sorted(os.path.basename(x) for x in paths)
-    assert names == ["all.excitation.tout", "all.field.tout", "all.frequency_domain_power_surface.fout",
-                     "all.volume_average_field.tout", "all.volume_peak_field.tout"]
+    assert names == ["all.excitation.tout", "all.far_field.fout.1", "all.field.tout",
+                     "all.frequency_domain_power_surface.fout", "all.frequency_output_surface.fout",
+                     "all.rcs.fout", "all.rcs.tout", "all.volume_average_field.tout", "all.volume_peak_field.tout"]
     pw = [x for x in open(os.path.join(str(tmp_path), "all.frequency_domain_power_surface.fout")).read().splitlines()]
     assert pw[:3] == ["# Frequency Domain Data", "# Number of data points:         1",
                       "# Number of frequencies:         3"] and len(pw) == 6
@@ -133,6 +139,15 @@ def test_volume_average_and_peak_files(tmp_path):
     want = oracle.output_volumes(t, oracle.Oracle(t).run(t["n_timesteps"]))
     np.testing.assert_allclose(avg[:, 2], want[0], rtol=TOL, atol=1e-30)
     np.testing.assert_allclose(peak[:, 2], want[1], rtol=TOL, atol=1e-30)
+
+
+def test_runner_refuses_sar_in_a_dispersive_material_before_running(tmp_path):
+    """SAR only in a material of constant permittivity without magnetic
+    conductivity: the reference stops at initialisation
+    (SAR_volumes.F90:150-190), and so does the runner, before it needs a GPU."""
+    problem_dir(str(tmp_path), "sar", test_inp.ALL_OUTPUTS.splitlines())
+    with pytest.raises(ValueError, match="SAR in a dispersive dielectric material"):
+        runner.run("sar", directory=str(tmp_path))
 
 
 def test_runner_stops_cleanly_without_a_gpu(tmp_path):
@@ -155,8 +170,9 @@ def test_runner_stops_cleanly_without_a_gpu(tmp_path):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name, text", [("huygens_test", None), ("all", "all"), ("fields", "fields")])
 def test_gpu_runner_files_match_oracle_files(gpu_lib, tmp_path, name, text):
+    # without the SAR volume, which sits in a Debye material (refused, as the reference stops on it)
     lines = (test_inp.inputs()["huygens_box"] if text is None else
-             (FIELDS if text == "fields" else test_inp.ALL_OUTPUTS).splitlines())
+             (FIELDS if text == "fields" else test_inp.ALL_OUTPUTS).split("SAR_volume_list")[0].splitlines())
     run_dir, ref_dir = str(tmp_path / "run"), str(tmp_path / "oracle")
     os.makedirs(run_dir)
     os.makedirs(ref_dir)
@@ -172,10 +188,27 @@ def test_gpu_runner_files_match_oracle_files(gpu_lib, tmp_path, name, text):
         if a.endswith("_field.tout") and (".surface_" in a or ".volume_field" in a):
             # templates and framing line for line; values to the file's 5 digits
             num = [k for k, x in enumerate(la) if not x.startswith("#") and len(x.split()) == 1 and "." in x]
-            assert [x for k, x in enumerate(la) if k not in set(num)] == \
-                [x for k, x in enumerate(lb) if k not in set(num)]
+            skip = set(num)
+            assert [x for k, x in enumerate(la) if k not in skip] == [x for k, x in enumerate(lb) if k not in skip]
             va, vb = np.array([float(la[k]) for k in num]), np.array([float(lb[k]) for k in num])
             np.testing.assert_allclose(vb, va, rtol=1.01e-5, atol=1e-9 * max(np.abs(va).max(), 1e-300))
+            continue
+        if a.endswith(".frequency_output_surface.fout"):
+            # template line for line; each face's cell, then its phasor to the file's 8 digits
+            num = [k for k, x in enumerate(la) if len(x.split()) == 6]
+            skip = set(num)
+            assert [x for k, x in enumerate(la) if k not in skip] == [x for k, x in enumerate(lb) if k not in skip]
+            da, db = np.loadtxt([la[k] for k in num], ndmin=2), np.loadtxt([lb[k] for k in num], ndmin=2)
+            assert np.array_equal(da[:, :3], db[:, :3])
+            np.testing.assert_allclose(db[:, 3:5], da[:, 3:5], rtol=1.01e-7, atol=1e-9 * np.abs(da[:, 3:5]).max())
+            continue
+        if ".far_field.fout" in a or ".rcs." in a:
+            # comment lines as they are; the numbers to the files' printed digits
+            ka = [k for k, x in enumerate(la) if x.lstrip().startswith("#")]
+            assert [la[k] for k in ka] == [lb[k] for k in ka]
+            da = np.loadtxt([x for x in la if not x.lstrip().startswith("#")], ndmin=2)
+            db = np.loadtxt([x for x in lb if not x.lstrip().startswith("#")], ndmin=2)
+            np.testing.assert_allclose(db, da, rtol=1.01e-5, atol=1e-9 * np.abs(da).max())
             continue
         if a.endswith(".fout"):
             da, db = np.loadtxt(la, comments="#", ndmin=2), np.loadtxt(lb, comments="#", ndmin=2)
