@@ -106,8 +106,13 @@ def test_gpu_fp32_and_batch_equals_solo(gpu_lib):
 def test_gpu_rejects_other_surface_materials(gpu_lib):
     t = build_tables(spec_with(FULL_PEC, steps=10))
     t["face_mat"] = t["face_mat"].copy()
-    t["face_mat"][0] = 3  # a dispersive (thin-layer) surface material
+    t["face_mat"][0] = 5  # a surface material type outside PEC, PMC, thin layer and free space (a diode)
     with pytest.raises(capi.TLMError) as e:
         with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64) as g:
             g.run(1)
     assert "TLM_E_UNSUPPORTED" in str(e.value)
+    t["face_mat"][0] = 3  # a thin layer without its thin-layer material
+    with pytest.raises(capi.TLMError) as e:
+        with capi.GpuMesh(t, precision=capi.TLM_PRECISION_FP64) as g:
+            g.run(1)
+    assert "TLM_E_BADARG" in str(e.value)
