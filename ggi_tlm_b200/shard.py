@@ -21,9 +21,12 @@ per slab (NCCL over NVLink between GPUs; gloo on the CPU for the tests);
 ``LocalShards`` holds every slab in one process.
 
 Supported: the cell-centred path (free space, PML, volume materials, point
-sources, probes, the denormal flush).  Special faces (Huygens surfaces,
-surface sheets, face points, surface outputs) and z wrapping are refused
-with ``UnsupportedFeature``.
+sources, probes, the denormal flush) and the special faces inside a slab
+(Huygens surfaces, surface sheets and thin layers, face sources, face
+probes, frequency output surfaces).  A special face on a z-face between two
+slabs, the outer-boundary Huygens surface, whole-surface and volume outputs
+(far field, output surfaces and volumes, power, modes, RCS, SAR) and z
+wrapping are refused with ``UnsupportedFeature``.
 """
 from __future__ import annotations
 
@@ -33,9 +36,8 @@ import numpy as np
 
 from .problem import UnsupportedFeature
 
-# tables whose non-empty presence needs faces or whole-mesh outputs
-_REFUSED_COUNTS = ("n_faces", "hs_n", "n_face_points", "n_face_probes", "n_dft", "n_ff", "n_osurf", "n_ps",
-                   "n_modes", "rcs_on", "n_sar", "n_ovol", "n_vdft", "n_smat")
+# tables whose non-empty presence needs whole-mesh outputs or the outer boundary
+_REFUSED_COUNTS = ("n_ff", "n_osurf", "n_ps", "n_modes", "rcs_on", "n_sar", "n_ovol", "n_vdft", "hs_outer")
 
 
 def slab_bounds(nz: int, parts: int) -> List[Tuple[int, int]]:
@@ -54,7 +56,8 @@ def slab_bounds(nz: int, parts: int) -> List[Tuple[int, int]]:
 def check_shardable(t: dict):
     for k in _REFUSED_COUNTS:
         if int(np.sum(t.get(k, 0))):
-            raise UnsupportedFeature(f"z-slab sharding of a mesh with {k} > 0 (special faces or surface outputs)")
+            raise UnsupportedFeature(f"z-slab sharding of a mesh with {k} > 0 (whole-surface or volume outputs, "
+                                     "or the outer-boundary Huygens surface)")
     if int(np.asarray(t.get("wrap", (0, 0, 0)))[2]):
         raise UnsupportedFeature("z-slab sharding of a mesh that wraps in z")
 
@@ -131,12 +134,93 @@ def slab_tables(t: dict, z0: int, z1: int) -> dict:
     below, above = z0 > 0, z1 < nz
     s["slab"] = np.array([int(below), int(above)], dtype=np.int32)
     s["slab_z0"] = z0
+    _slab_faces(t, s, z0, z1)
     if "pml_depth" in t:
         d = np.asarray(t["pml_depth"]).copy()
         d[4] = max(0, int(d[4]) - z0) if not below else 0
         d[5] = max(0, int(d[5]) - (nz - z1)) if not above else 0
         s["pml_depth"] = d
     return s
+
+
+def _slab_faces(t: dict, s: dict, z0: int, z1: int) -> None:
+    """The special faces of planes [z0, z1) (connect.F90 order: cz, cy, cx,
+    then the x-, y-, z-face, so a slab's faces are one run of the list, and
+    so are its excitation and output face numbers), with the sources,
+    probes, sheets and frequency output surface entries on them renumbered.
+    ``slab_face_probes`` and ``slab_dft`` give the global positions of the
+    slab's face probes and DFT faces, for the gathers."""
+    n = int(t.get("n_faces", 0))
+    cz = np.asarray(t.get("face_cz", []), dtype=np.int64)
+    fdir = np.asarray(t.get("face_dir", []), dtype=np.int64)
+    keep = (cz > z0) & (cz <= z1)
+    if n and np.any(keep & (fdir == 3) & (cz == z0 + 1) & (z0 > 0)):
+        raise UnsupportedFeature("z-slab sharding with a special face on the z-faces between two slabs")
+    fe = np.asarray(t.get("face_exc", []), dtype=np.int64)
+    fo = np.asarray(t.get("face_out", []), dtype=np.int64)
+    ea = int(np.count_nonzero(fe[~keep & (cz <= z0)])) if n else 0
+    oa = int(np.count_nonzero(fo[~keep & (cz <= z0)])) if n else 0
+    ne, no = (int(np.count_nonzero(fe[keep])), int(np.count_nonzero(fo[keep]))) if n else (0, 0)
+    s["n_faces"] = int(np.count_nonzero(keep))
+    for k in ("face_cx", "face_cy", "face_dir", "face_mat", "face_smat"):
+        if k in t:
+            s[k] = np.asarray(t[k])[keep].astype(np.int32) if n else np.asarray(t[k]).copy()
+    s["face_cz"] = (cz[keep] - z0).astype(np.int32)
+    s["face_exc"] = np.where(fe[keep] != 0, fe[keep] - ea, 0).astype(np.int32)
+    s["face_out"] = np.where(fo[keep] != 0, fo[keep] - oa, 0).astype(np.int32)
+    s["n_exc_faces"], s["n_out_faces"] = ne, no
+
+    def in_exc(a):
+        a = np.asarray(a, dtype=np.int64)
+        return (a > ea) & (a <= ea + ne)
+
+    def in_out(a):
+        a = np.asarray(a, dtype=np.int64)
+        return (a > oa) & (a <= oa + no)
+
+    # Huygens patches (their offsets stay the global ones)
+    hk = in_exc(t.get("hs_face_exc", []))
+    if int(t.get("hs_n", 0)):
+        s["hs_face_exc"] = (np.asarray(t["hs_face_exc"])[hk] - ea).astype(np.int32)
+        s["hs_norm"] = np.asarray(t["hs_norm"]).reshape(-1, 3)[hk].reshape(-1).astype(np.int32)
+        s["hs_offset"] = np.asarray(t["hs_offset"])[hk].copy()
+        s["hs_n"] = int(hk.sum())
+    # face sources
+    pk = in_exc(t.get("fpt_face", []))
+    s["fpt_face"] = (np.asarray(t.get("fpt_face", []), dtype=np.int64)[pk] - ea).astype(np.int32)
+    for k in ("fpt_comp", "fpt_fn", "fpt_type", "fpt_side", "fpt_scale"):
+        if k in t:
+            s[k] = np.asarray(t[k])[pk].copy()
+    s["n_face_points"] = int(pk.sum())
+    # face probes
+    qk = in_out(t.get("fprobe_face", []))
+    s["fprobe_face"] = (np.asarray(t.get("fprobe_face", []), dtype=np.int64)[qk] - oa).astype(np.int32)
+    for k in ("fprobe_side", "fprobe_comp", "fprobe_point_no"):
+        if k in t:
+            s[k] = np.asarray(t[k])[qk].copy()
+    s["n_face_probes"] = int(qk.sum())
+    s["slab_face_probes"] = np.nonzero(qk)[0].astype(np.int32)
+    # frequency output surfaces: every entry, with the slab's faces of each
+    if int(t.get("n_dft", 0)):
+        ptr = np.asarray(t["dft_face_ptr"], dtype=np.int64)
+        dk = in_out(t["dft_face_out"])
+        s["dft_face_out"] = (np.asarray(t["dft_face_out"], dtype=np.int64)[dk] - oa).astype(np.int32)
+        s["dft_face_side"] = np.asarray(t["dft_face_side"])[dk].copy()
+        s["dft_face_ptr"] = np.array([int(np.count_nonzero(dk[:p])) for p in ptr], dtype=np.int32)
+        s["slab_dft"] = np.nonzero(dk)[0].astype(np.int32)
+    else:
+        s["slab_dft"] = np.zeros(0, dtype=np.int32)
+
+
+def gather_rows(n_rows: int, slabs: List[dict], key: str, parts: List[np.ndarray]) -> np.ndarray:
+    """Global rows (face probe series, DFT phasors) from each slab's rows,
+    placed by the slab's ``key`` positions."""
+    shape = next((np.asarray(p).shape[1:] for p in parts if np.asarray(p).size), ())
+    out = np.zeros((n_rows,) + tuple(shape))
+    for tab, rows in zip(slabs, parts):
+        for k, g in enumerate(np.asarray(tab[key])):
+            out[int(g)] = rows[k]
+    return out
 
 
 def _shift_z(xyz: np.ndarray, z0: int) -> np.ndarray:
@@ -192,6 +276,14 @@ class GpuSlab:
         self.mesh.synchronize()
         return probe_series(self.t, self.mesh.cell_output())
 
+    def face_probes(self) -> np.ndarray:
+        self.mesh.synchronize()
+        return self.mesh.face_output()
+
+    def dft(self) -> np.ndarray:
+        self.mesh.synchronize()
+        return self.mesh.dft()
+
     def close(self):
         self.mesh.close()
 
@@ -229,6 +321,16 @@ class LocalShards:
 
     def probes(self) -> np.ndarray:
         return gather_series(self.t, self.tables, [s.probes() for s in self.slabs])
+
+    def face_probes(self) -> np.ndarray:
+        """Face probe series [n_face_probes, steps] of the global mesh."""
+        return gather_rows(int(self.t.get("n_face_probes", 0)), self.tables, "slab_face_probes",
+                           [s.face_probes() for s in self.slabs])
+
+    def dft(self) -> np.ndarray:
+        """Frequency output surface phasors [faces, 2] in the global entry order."""
+        n = int(np.asarray(self.t["dft_face_ptr"])[-1]) if int(self.t.get("n_dft", 0)) else 0
+        return gather_rows(n, self.tables, "slab_dft", [s.dft() for s in self.slabs])
 
     def close(self):
         for s in self.slabs:
@@ -309,6 +411,22 @@ class DistShard:
             for k, g in enumerate(pts):
                 out[int(g)] = ser[k]
         return out
+
+    def _gather(self, key: str, rows: np.ndarray, n_rows: int):
+        parts = [None] * self.world if self.rank == 0 else None
+        self.dist.gather_object((self.tab[key].tolist(), rows), parts, dst=self._peer(0), group=self.group)
+        if self.rank != 0:
+            return None
+        return gather_rows(n_rows, [{key: p[0]} for p in parts], key, [p[1] for p in parts])
+
+    def face_probes(self):
+        """Global face probe series on rank 0, None elsewhere."""
+        return self._gather("slab_face_probes", self.slab.face_probes(), int(self.t.get("n_face_probes", 0)))
+
+    def dft(self):
+        """Global frequency output surface phasors on rank 0, None elsewhere."""
+        n = int(np.asarray(self.t["dft_face_ptr"])[-1]) if int(self.t.get("n_dft", 0)) else 0
+        return self._gather("slab_dft", self.slab.dft(), n)
 
     def close(self):
         self.slab.close()
